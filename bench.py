@@ -1,0 +1,329 @@
+"""Throughput of the trace -> deposit -> merge -> update hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload iliev64]
+                    [--ticks T] [--impl ours|reference]
+
+A step is one batch of T ticks of the workload: all rays of those ticks are
+traced, sorted and deposited, and every particle they hit is updated once
+per tick, as run_epoch() does (loop.c:128-147). The metric is ray-particle
+hits per second (hits = stat.total_deposit_count, the summed hit-list
+lengths), over the whole pipeline -- a stricter clock than the reference's
+own hits/s, which counts only trace + deposit time.
+
+Workloads (seeded synthetic fields; no dataset is involved):
+  iliev64       64^3 uniform particles in a 6.6 kpc box, one corner source of
+                5e48 photons/s at 13.6 eV, 1024 rays/tick, isothermal 1e4 K
+  iliev32       32^3, 32 rays/tick (the reference's CPU-sized case)
+  lognormal128  128^3 particles on a log-normal field (sigma 1), 16 sources,
+                8192 rays/tick, 8-bin 1e5 K blackbody, non-isothermal
+
+--gpus N under torchrun runs N independent replicas, one per GPU (the path
+is single-GPU; no data crosses GPUs), barrier + max over ranks for time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DEFAULT_TICKS = {"iliev32": 400, "iliev64": 100, "lognormal128": 8}
+BYTES_PER_HIT = 36       # pos 12 + sml 4 + lambdaH 8 + mass 4 + FP64 absorbed photons 8
+BYTES_PER_HIT_TRACE = 36  # trace fill: pos+sml 16 read, (ipar 4, d 8, b 8) written
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    def __init__(self, device: int):
+        self.proc = None
+        self.device = device
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make(workload: str):
+    from psphray_b200 import fields
+    return fields.make_workload(workload)
+
+
+def cpu_baseline_reference(w, seconds: float = 15.0, threads: int | None = None, ticks=None):
+    """The reference's own CPU code (oracle/_ref) on a bounded sample of the
+    same workload: hits/s over its trace + deposit time, as its stat counters
+    define it, with all host threads. Falls back to the C restatement."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    threads = threads or os.cpu_count()
+    try:
+        from refpy import LIB_PATH, Reference
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(LIB_PATH)
+        from psphray_b200.api import RATES_HUI
+        ref = Reference(RATES_HUI, w.field.units, isothermal=w.isothermal, threads=threads)
+        ref.load(w.field)
+        ref.build_tree(8)
+        ref.reset_stats()
+        t0 = time.time()
+        n = 0
+        while (time.time() - t0 < seconds and (ticks is None or n < ticks)) or n == 0:
+            n += 1
+            ref.tick(w.schedule.rays_for_tick(n), n, w.tick_time)
+        st = ref.stats()
+        hits_s = st["hits"] / (st["raytrace_time"] + st["deposit_time"])
+        full = (st["raytrace_time"] + st["deposit_time"] + st["merge_time"] + st["update_time"])
+        return {"value": hits_s, "unit": "hits/s", "cores": threads, "kind": "reference",
+                "sample": f"{n} ticks x {w.schedule.nray} rays of {w.name}, trace+deposit clock "
+                          f"({st['hits']:.0f} hits); whole tick incl. LSODA update: "
+                          f"{st['hits'] / full:.4g} hits/s, {full / n * 1e3:.3g} ms/tick"}
+    except FileNotFoundError:
+        from oracle import Oracle
+        from psphray_b200 import api
+        phys = api.Physics(w.field.units, isothermal=w.isothermal)
+        orc = Oracle(w.field, phys, isothermal=w.isothermal)
+        orc.build_tree(8)
+        t0 = time.time()
+        n = hits = 0
+        while time.time() - t0 < seconds or n == 0:
+            n += 1
+            hits += orc.tick(w.schedule.rays_for_tick(n), n, w.tick_time)["hits"]
+        dt = time.time() - t0
+        return {"value": hits / dt, "unit": "hits/s", "cores": 1, "kind": "port",
+                "sample": f"{n} ticks x {w.schedule.nray} rays of {w.name}, whole tick, 1 thread"}
+
+
+def dist_setup(gpus: int):
+    if gpus <= 1 or "RANK" not in os.environ:
+        return 0, 1, 0, None
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ["RANK"]); world = int(os.environ["WORLD_SIZE"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    import torch
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return rank, world, local, dist
+
+
+def run_reference(args):
+    rank, world, local, dist = dist_setup(args.gpus)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    w = make(args.workload)
+    per_step = max(1, args.ref_ticks)
+    vals = []
+    base = None
+    for k in range(args.warmup + args.steps):
+        b = cpu_baseline_reference(w, seconds=1e9, ticks=per_step) if base is None else None
+        if base is None:
+            base = b
+        vals.append(b["value"] if b else base["value"])
+    v = base["value"]
+    line = {"impl": "reference", "metric": "ray-particle hits/s", "value": v, "unit": "hits/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload},
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": "hits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="iliev64")
+    ap.add_argument("--ticks", type=int, default=0, help="ticks per step (default per workload)")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-ticks", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    dev = local
+    torch.cuda.set_device(dev)
+    from psphray_b200 import api
+    from psphray_b200.fields import RAY_DTYPE
+
+    w = make(args.workload)
+    T = args.ticks or DEFAULT_TICKS[args.workload]
+    R = w.schedule.nray
+    nsteps = args.warmup + args.steps
+    phys = api.Physics(w.field.units, isothermal=w.isothermal)
+    ctx = api.Context(dev)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_physics(phys)
+    ctx.load(w.field)
+    ctx.build_tree(8)
+    tinfo = ctx.tree_info()
+
+    # rays of every step, resident in HBM before timing (inputs of `value`)
+    host_rays = [w.schedule.rays_for_ticks(1 + s * T, T) for s in range(nsteps)]
+    dev_rays = [torch.from_numpy(r.view(np.uint8)).to(f"cuda:{dev}") for r in host_rays]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")   # > 126 MB L2
+    torch.cuda.synchronize(dev)
+
+    ctx.set_timing(True)
+    for s in range(args.warmup):
+        ctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
+    torch.cuda.synchronize(dev)
+
+    clocks = Clocks(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    total_ms, hits, launches = 0.0, 0.0, 0.0
+    kms = {k: 0.0 for k in api.KERNELS}
+    kn = {k: 0.0 for k in api.KERNELS}
+    for s in range(args.warmup, nsteps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = ctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        hits += st["hits"]
+        launches += st["launches"]
+        for k in api.KERNELS:
+            kms[k] += st["kernel_ms"][k]
+            kn[k] += st["kernel_launches"][k]
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    t_local = total_ms / 1e3
+    if dist:
+        t = torch.tensor([t_local], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        h = torch.tensor([hits], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(h)
+        hits_all = float(h.item())
+    else:
+        t_max, hits_all = t_local, hits
+    value = hits_all / t_max
+    sim_myr = args.steps * T * w.tick_time / w.field.units.MYR
+    ctx.set_timing(False)
+
+    # e2e: the public host-buffer call, pinned host rays, result read back
+    pinned = [torch.from_numpy(r.view(np.uint8)).pin_memory() for r in host_rays[args.warmup:]]
+    e2e_hits = 0.0
+    lam = np.zeros(w.field.n)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for i, pr in enumerate(pinned):
+        s = args.warmup + i
+        rays = np.frombuffer(pr.numpy(), dtype=RAY_DTYPE)
+        st = ctx.run_ticks(rays, R, T, 1 + (nsteps + i) * T, w.tick_time)
+        lam = ctx.state()["lambdaH"]
+        e2e_hits += st["hits"]
+    torch.cuda.synchronize(dev)
+    e2e_t = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_t], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+        h = torch.tensor([e2e_hits], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(h)
+        e2e_hits = float(h.item())
+
+    # roofline of the dominant kernel group
+    peak, peak_kind = peaks()
+    dom = max(api.KERNELS, key=lambda k: kms[k])
+    per_hit = {"trace_count": 16, "trace_fill": BYTES_PER_HIT_TRACE, "sort": 60, "slots": 48,
+               "deposit": 32, "update": 4}
+    achieved = hits * per_hit[dom] / (kms[dom] / 1e3) / 1e9 if kms[dom] > 0 else None
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"{dom}_{args.workload}_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+
+    line = {"metric": "ray-particle hits/s", "value": value, "unit": "hits/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "particles": w.field.n, "rays_per_tick": R,
+                       "ticks_per_step": T, "hits_per_step": hits / args.steps,
+                       "tree_cells": tinfo["ncells"], "l2": "256 MiB buffer zeroed between steps",
+                       "parallelism": f"replicas{world}"},
+            "gpu_s_per_sim_myr": t_max / sim_myr,
+            "gpu_launches": launches,
+            "kernel_ms_per_step": {k: kms[k] / args.steps for k in api.KERNELS},
+            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "bytes_per_hit": per_hit[dom]},
+            "clocks": clk,
+            "e2e": {"value": e2e_hits / e2e_t, "unit": "hits/s",
+                    "h2d_bytes_per_step": int(host_rays[0].nbytes),
+                    "d2h_bytes_per_step": int(24 * w.field.n)}}
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_reference(make(args.workload), seconds=args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,220 @@
+/* psg.h -- C ABI of the B200 trace -> deposit -> solve library (libpsg.so).
+ *
+ * Drop-in for the hot path of psphray (rainwoodman/psphray). Each entry
+ * point names the reference function it replaces. Conventions:
+ *   - every call returns PSG_OK (0) or a negative PSG_E_* code; nothing traps
+ *     (the reference raises SIGTRAP through ERROR(), support/messages.h:17);
+ *     psg_last_error() gives the message of the last failure of a context;
+ *   - host buffers belong to the caller, device buffers to the library;
+ *   - one host thread per context; calls on one context are serialised on the
+ *     context's own CUDA stream;
+ *   - particles keep the caller's order: particle index ipar is the position
+ *     in the arrays given to psg_load_particles().
+ */
+#ifndef PSG_H
+#define PSG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSG_OK 0
+#define PSG_E_INVAL (-1)     /* bad argument or call order */
+#define PSG_E_CUDA (-2)      /* CUDA runtime error */
+#define PSG_E_NOMEM (-3)     /* device or host allocation failed */
+#define PSG_E_OVERFLOW (-4)  /* a fixed capacity was exceeded (tree depth, table size) */
+#define PSG_E_IO (-5)        /* file missing or malformed */
+#define PSG_E_DEVICE (-6)    /* a kernel raised its status word (NaN, solver failure) */
+
+/* ---- units: units_init() src/units.c:66-104, defaults src/config.c:15-23 -- */
+typedef struct {
+	double h;            /* cosmology.h */
+	double hmf;          /* cosmology.hmf, hydrogen mass fraction */
+	double length_cmh;   /* units.lengthCMh */
+	double mass_gramh;   /* units.massGramh */
+	double time_sh;      /* units.timeSh */
+} psg_unit_params;
+
+typedef struct {
+	double CM, GRAM, SEC, M, KM, KPC, YR, MYR, KG, MSUN, MPROTON, KELVIN;
+	double BOLTZMANN, J, EV, ERG, RY_ENG;
+	double H_PER_MASS, HE_PER_MASS, HI_ENERGY, HEI_ENERGY, HEII_ENERGY;
+	double MPROTON_OVER_BOLTZMANN, BOLTZMANN_OVER_MPROTON;
+	double hmf, hemf;
+} psg_units;
+
+/* Fills *u from *p. Replaces units_init() units.c:66. */
+int psg_units_init(const psg_unit_params *p, psg_units *u);
+
+/* ---- atomic-rate table: tabfun_init() src/tabfun.c:60-130 + ar_init()
+ * src/atomic-rate.c:66-87. Columns, after unit scaling: */
+enum {
+	PSG_AR_HI_CI = 0, PSG_AR_HII_RC_A, PSG_AR_HII_RC_B, PSG_AR_HII_RCC_A, PSG_AR_HII_RCC_B,
+	PSG_AR_HI_CIC, PSG_AR_HI_CEC, PSG_AR_E_BREMC, PSG_AR_E_COMPC,
+	PSG_AR_HEI_CI, PSG_AR_HEII_CI, PSG_AR_HEII_RC_A, PSG_AR_HEII_RC_B, PSG_AR_HEIII_RC_A,
+	PSG_AR_HEIII_RC_B, PSG_AR_NCOLS
+};
+typedef struct {
+	int nrows;
+	double min, max, step, step_inv;
+	double *logT;                 /* first column of the file, nrows */
+	double *col[PSG_AR_NCOLS];    /* scaled to internal units, nrows each */
+} psg_rate_table;
+
+/* Parses the 14-character fixed-width table at path. Replaces ar_init(). */
+int psg_rate_table_load(const char *path, const psg_units *u, psg_rate_table *t);
+void psg_rate_table_free(psg_rate_table *t);
+/* ar_get() atomic-rate.c:89 / tabfun_get() tabfun.c:38-58. */
+double psg_ar_get(const psg_rate_table *t, int col, double logT);
+
+/* ---- cross sections: xs_init(NULL) atomic-rate.c:93-124 with the analytic
+ * fits of src/verner.F90, 16384 rows over 1-100 Ry. */
+enum { PSG_XS_HI = 0, PSG_XS_HEI, PSG_XS_HEII, PSG_XS_NSPECIES };
+typedef struct {
+	int nrows;
+	double min, max, step, step_inv;
+	double *eng;
+	double *sigma[PSG_XS_NSPECIES];
+	double cut[PSG_XS_NSPECIES];
+} psg_xs_table;
+int psg_xs_table_build(const psg_units *u, psg_xs_table *t);
+void psg_xs_table_free(psg_xs_table *t);
+/* xs_get() atomic-rate.c:126-131. */
+double psg_xs_get(const psg_xs_table *t, int species, double freq);
+
+/* ---- SPH column-depth table (src/kernel.akline format: one double per line,
+ * trailing comma). *n receives the count (4096 for the reference table). */
+int psg_kernel_table_load(const char *path, double *out, int cap, int *n);
+/* sph_depth() src/sph-depth.c:26-33. */
+double psg_sph_depth(const double *table, int n, double r_h);
+
+/* ---- context -------------------------------------------------------------- */
+typedef struct psg_context psg_context;
+
+int psg_create(psg_context **ctx, int device);
+void psg_destroy(psg_context *ctx);
+const char *psg_last_error(const psg_context *ctx);
+/* With on != 0, psg_run_ticks*() bracket every kernel launch with CUDA
+ * events on the context's stream and report per-kernel device time. */
+int psg_set_timing(psg_context *ctx, int on);
+/* Run the context's work on the caller's CUDA stream (a cudaStream_t passed
+ * as void*; NULL restores the context's own stream). No reference
+ * counterpart: the reference has no device. */
+int psg_set_stream(psg_context *ctx, void *stream);
+
+/* Physics switches, the config.c flags that the path reads. */
+typedef struct {
+	int isothermal;          /* psphray.isothermal */
+	int on_the_spot;         /* psphray.onTheSpot */
+	int h_only;              /* psphray.HOnly (only 1 is supported) */
+	int adiabatic;           /* psphray.adiabatic */
+} psg_flags;
+
+/* Upload units, tables and flags. Must precede psg_load_particles(). */
+int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_rate_table *ar,
+		const psg_xs_table *xs, const double *kernel, int kernel_n, const psg_flags *flags);
+
+/* Particle arrays (reference storage types, psystem.h:32-78). xHI and ye are
+ * the snapshot blocks; lambdaH and yeMET are derived as psystem_read_epoch()
+ * psystem.c:340-356 does. flag may be NULL (bit 0 = PF_INVALID). */
+typedef struct {
+	size_t n;
+	const float *pos;    /* [n][3] */
+	const float *mass, *sml, *rho, *ie, *xHI, *ye;
+	const int8_t *flag;
+	double boxsize;
+} psg_particles;
+int psg_load_particles(psg_context *ctx, const psg_particles *p);
+
+/* Octree over [0, boxsize)^3 with at most ppc particles per leaf, built on
+ * the device. Replaces rt_switch_epoch() raytrace.c:41-151 (same cells, same
+ * leaf boxes). */
+int psg_build_tree(psg_context *ctx, int ppc);
+
+typedef struct {
+	size_t ncells, nleaves, skipped;
+	int depth;
+} psg_tree_info;
+int psg_get_tree_info(psg_context *ctx, psg_tree_info *info);
+/* Cells in depth-first order (children 0..7): boxes, the index just past each
+ * cell's subtree, and the first particle (in leaf order) of each cell; and
+ * the leaf-order particle permutation. Arrays sized from psg_get_tree_info;
+ * pstart has ncells+1 entries. Any pointer may be NULL. */
+int psg_get_tree(psg_context *ctx, float *bot, float *top, int32_t *skip, int32_t *pstart,
+		int32_t *order);
+
+/* ---- rays and hits --------------------------------------------------------- */
+typedef struct {
+	float s[3];
+	float dir[3];
+	double Nph;
+	double freq;
+	double length;
+} psg_ray;                  /* struct r_t loop.c:21-35 without the bookkeeping */
+
+typedef struct {
+	int64_t ipar;
+	double d;
+	double b;
+} psg_xtype;                /* Xtype psystem.h:108-112 */
+
+/* One ray, rt_trace() raytrace.c:153 signature plus the context: hits sorted
+ * by (d, ipar) -- the reference's trace() order (loop.c:383) with ties made
+ * deterministic. *x is (re)allocated with malloc as in the reference (caller
+ * frees); returns the hit count, or (size_t)-1 on error. */
+size_t psg_rt_trace(psg_context *ctx, const float s[3], const float dir[3], const float dist,
+		psg_xtype **x, size_t *size);
+
+/* Many rays at once, host buffers: offsets[nray+1] and hits in *x (grown with
+ * realloc as needed, size in *size). Replaces trace() loop.c:375-386. */
+int psg_trace(psg_context *ctx, const psg_ray *rays, size_t nray, int64_t *offsets,
+		psg_xtype **x, size_t *size);
+
+/* ---- ticks ----------------------------------------------------------------- */
+/* Kernels timed by psg_tick_stats when timing is on (psg_set_timing). */
+enum { PSG_K_TRACE_COUNT = 0, PSG_K_TRACE_FILL, PSG_K_SORT, PSG_K_SLOTS, PSG_K_DEPOSIT,
+	PSG_K_UPDATE, PSG_K_NKERNELS };
+typedef struct {
+	double hits;            /* sum of hit-list lengths, stat.total_deposit_count */
+	double saturated;       /* deposits capped at the neutral atoms, loop.c:482-485 */
+	double active;          /* particle updates, stat.evolve_count */
+	double lost_photons;    /* photons left in rays at their end */
+	double trace_ms, tick_ms;   /* device time: trace+sort+slots, then the tick loop */
+	double launches;        /* kernels of this library launched by the call */
+	double kernel_ms[PSG_K_NKERNELS];        /* per kernel group, with timing on */
+	double kernel_launches[PSG_K_NKERNELS];
+} psg_tick_stats;
+
+/* Runs nticks ticks; rays holds nray_per_tick rays for each tick, tick by
+ * tick (host buffer). Tick k (0-based) is the reference's psys.tick =
+ * first_tick + k. Per tick: trace, deposit, merge, update -- run_epoch()
+ * loop.c:128-147 without emit_rays(). stats may be NULL. */
+int psg_run_ticks(psg_context *ctx, const psg_ray *rays, size_t nray_per_tick, size_t nticks,
+		int64_t first_tick, double tick_time, psg_tick_stats *stats);
+/* Same with rays already in device memory. */
+int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, size_t nray_per_tick,
+		size_t nticks, int64_t first_tick, double tick_time, psg_tick_stats *stats);
+
+/* Particle state, caller order. Any pointer may be NULL. */
+int psg_get_state(psg_context *ctx, double *lambdaH, float *ie, int32_t *hits, int64_t *lasthit);
+int psg_set_state(psg_context *ctx, const double *lambdaH, const float *ie, const int64_t *lasthit);
+
+/* ---- solver ---------------------------------------------------------------- */
+typedef struct {
+	double lambdaH, lambdaHeI, lambdaHeII, ie, yeMET, yGdepHI, yGdepHeI, yGdepHeII, heat;
+	double time, nH, T, yGrecHII, yGrecHeII, yGrecHeIII, step_remain;
+	int refined;
+	int64_t ipar;
+} psg_step;                 /* Step psystem.h:84-105 */
+
+/* step_evolve() solve.c:317 for n independent steps, on the device; steps
+ * are updated in place (host buffer). */
+int psg_step_evolve(psg_context *ctx, psg_step *steps, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

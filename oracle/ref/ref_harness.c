@@ -184,9 +184,12 @@ int ref_load_particles(size_t n, const float *pos, const float *mass,
 	return 0;
 }
 
+/* rt_switch_epoch(0) sizes its pool and next[] from the loaded particle
+ * count, so every build here takes that path (the arrays of an earlier
+ * build are simply dropped). */
 int ref_build_tree(int ppc) {
 	CFG_OCTTREE_PPC = ppc;
-	rt_switch_epoch(tree_built ? 1 : 0);
+	rt_switch_epoch(0);
 	tree_built = 1;
 	return 0;
 }

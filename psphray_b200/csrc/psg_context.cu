@@ -1,0 +1,250 @@
+// Context lifetime, error reporting, physics tables and particle upload.
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "psg_internal.cuh"
+
+int psg_fail(psg_context *ctx, int code, const char *fmt, ...) {
+	if (ctx) {
+		va_list ap;
+		va_start(ap, fmt);
+		vsnprintf(ctx->err, sizeof(ctx->err), fmt, ap);
+		va_end(ap);
+	}
+	return code;
+}
+
+int psg_cuda_fail(psg_context *ctx, cudaError_t e, const char *what, const char *file, int line) {
+	const int code = (e == cudaErrorMemoryAllocation) ? PSG_E_NOMEM : PSG_E_CUDA;
+	return psg_fail(ctx, code, "%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+}
+
+void *psg_scratch(psg_context *ctx, int slot, size_t bytes) {
+	psg_buf &b = ctx->scratch[slot];
+	if (b.bytes >= bytes && b.p) return b.p;
+	if (b.p) cudaFree(b.p);
+	b.p = nullptr;
+	b.bytes = 0;
+	size_t want = bytes + bytes / 4 + 256;
+	if (cudaMalloc(&b.p, want) != cudaSuccess) {
+		cudaGetLastError();
+		b.p = nullptr;
+		psg_fail(ctx, PSG_E_NOMEM, "device allocation of %zu bytes failed (scratch %d)", want, slot);
+		return nullptr;
+	}
+	b.bytes = want;
+	return b.p;
+}
+
+extern "C" int psg_create(psg_context **out, int device) {
+	if (!out) return PSG_E_INVAL;
+	*out = nullptr;
+	int ndev = 0;
+	cudaError_t e = cudaGetDeviceCount(&ndev);
+	if (e != cudaSuccess || ndev == 0) {
+		cudaGetLastError();
+		return PSG_E_CUDA;
+	}
+	if (device < 0 || device >= ndev) return PSG_E_INVAL;
+	psg_context *ctx = new psg_context();
+	ctx->device = device;
+	if (cudaSetDevice(device) != cudaSuccess ||
+			cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+			cudaMalloc(&ctx->d_status, sizeof(uint32_t)) != cudaSuccess ||
+			cudaMemset(ctx->d_status, 0, sizeof(uint32_t)) != cudaSuccess) {
+		cudaGetLastError();
+		delete ctx;
+		return PSG_E_CUDA;
+	}
+	ctx->stream = ctx->own_stream;
+	for (auto &ev : ctx->ev) cudaEventCreate(&ev);
+	*out = ctx;
+	return PSG_OK;
+}
+
+static void free_particles(psg_context *ctx) {
+	void *ptrs[] = {ctx->d_psml, ctx->d_mass, ctx->d_rho, ctx->d_yeMET, ctx->d_ie, ctx->d_flag,
+		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit};
+	for (void *p : ptrs) if (p) cudaFree(p);
+	ctx->d_psml = nullptr; ctx->d_mass = ctx->d_rho = ctx->d_yeMET = ctx->d_ie = nullptr;
+	ctx->d_flag = nullptr; ctx->d_lambdaH = nullptr; ctx->d_hits = nullptr; ctx->d_lasthit = nullptr;
+	ctx->n = 0;
+}
+
+static void free_tree(psg_context *ctx) {
+	void *ptrs[] = {ctx->d_cell_lo, ctx->d_cell_hi, ctx->d_leaf_psml, ctx->d_leaf_idx};
+	for (void *p : ptrs) if (p) cudaFree(p);
+	ctx->d_cell_lo = ctx->d_cell_hi = ctx->d_leaf_psml = nullptr;
+	ctx->d_leaf_idx = nullptr;
+	ctx->have_tree = 0;
+}
+
+extern "C" void psg_destroy(psg_context *ctx) {
+	if (!ctx) return;
+	cudaSetDevice(ctx->device);
+	cudaStreamSynchronize(ctx->stream);
+	free_particles(ctx);
+	free_tree(ctx);
+	if (ctx->d_ar) cudaFree(ctx->d_ar);
+	if (ctx->d_xs) cudaFree(ctx->d_xs);
+	if (ctx->d_kernel) cudaFree(ctx->d_kernel);
+	if (ctx->d_status) cudaFree(ctx->d_status);
+	for (auto &b : ctx->scratch) if (b.p) cudaFree(b.p);
+	for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
+	for (auto &ev : ctx->kev) if (ev) cudaEventDestroy(ev);
+	cudaStreamDestroy(ctx->own_stream);
+	delete ctx;
+}
+
+extern "C" const char *psg_last_error(const psg_context *ctx) {
+	return ctx ? ctx->err : "no context";
+}
+
+extern "C" int psg_set_timing(psg_context *ctx, int on) {
+	if (!ctx) return PSG_E_INVAL;
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	if (on && !ctx->kev[0])
+		for (auto &e : ctx->kev) PSG_CUDA(cudaEventCreate(&e));
+	ctx->timing = on ? 1 : 0;
+	return PSG_OK;
+}
+
+extern "C" int psg_set_stream(psg_context *ctx, void *stream) {
+	if (!ctx) return PSG_E_INVAL;
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+	return PSG_OK;
+}
+
+extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_rate_table *ar,
+		const psg_xs_table *xs, const double *kernel, int kernel_n, const psg_flags *flags) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!u || !ar || !xs || !kernel || kernel_n <= 0 || !flags || ar->nrows < 2 || xs->nrows < 2)
+		return psg_fail(ctx, PSG_E_INVAL, "psg_set_physics: missing or empty table");
+	if (!flags->h_only)
+		return psg_fail(ctx, PSG_E_INVAL, "psg_set_physics: only hydrogen-only runs (HOnly) are supported");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	if (ctx->d_ar) cudaFree(ctx->d_ar);
+	if (ctx->d_xs) cudaFree(ctx->d_xs);
+	if (ctx->d_kernel) cudaFree(ctx->d_kernel);
+	ctx->d_ar = ctx->d_xs = ctx->d_kernel = nullptr;
+	const size_t nr = (size_t)ar->nrows;
+	PSG_CUDA(cudaMalloc(&ctx->d_ar, sizeof(double) * nr * (PSG_AR_NCOLS + 1)));
+	PSG_CUDA(cudaMemcpy(ctx->d_ar, ar->logT, sizeof(double) * nr, cudaMemcpyHostToDevice));
+	for (int c = 0; c < PSG_AR_NCOLS; c++)
+		PSG_CUDA(cudaMemcpy(ctx->d_ar + nr * (c + 1), ar->col[c], sizeof(double) * nr,
+				cudaMemcpyHostToDevice));
+	const size_t nx = (size_t)xs->nrows;
+	PSG_CUDA(cudaMalloc(&ctx->d_xs, sizeof(double) * nx * 2));
+	PSG_CUDA(cudaMemcpy(ctx->d_xs, xs->eng, sizeof(double) * nx, cudaMemcpyHostToDevice));
+	PSG_CUDA(cudaMemcpy(ctx->d_xs + nx, xs->sigma[PSG_XS_HI], sizeof(double) * nx,
+			cudaMemcpyHostToDevice));
+	PSG_CUDA(cudaMalloc(&ctx->d_kernel, sizeof(double) * kernel_n));
+	PSG_CUDA(cudaMemcpy(ctx->d_kernel, kernel, sizeof(double) * kernel_n, cudaMemcpyHostToDevice));
+	ctx->u = *u;
+	ctx->flags = *flags;
+	ctx->ar_nrows = ar->nrows;
+	ctx->ar_min = ar->min;
+	ctx->ar_step_inv = ar->step_inv;
+	ctx->xs_nrows = xs->nrows;
+	ctx->xs_min = xs->min;
+	ctx->xs_step_inv = xs->step_inv;
+	ctx->xs_cut_HI = xs->cut[PSG_XS_HI];
+	ctx->kernel_n = kernel_n;
+	ctx->have_physics = 1;
+	return PSG_OK;
+}
+
+// lambdaH and yeMET from the snapshot's xHI and ye, psystem.c:340-356 with
+// psys_set_lambdaH() psystem.h:156-160 (hydrogen-only branch).
+__global__ void k_init_particles(size_t n, const float *pos, const float *sml, const float *xHI,
+		const float *ye, float4 *psml, double *lambdaH, float *yeMET) {
+	const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	psml[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], sml[i]);
+	const double xhi = xHI[i];
+	const double xhii = rn_dsub(1.0, xhi);
+	double lam;
+	if (xhi >= 1.0 || xhii <= 0.0) lam = 1.0;
+	else if (xhi <= 0.0 || xhii >= 1.0) lam = 0.0;
+	else lam = xhi;
+	lambdaH[i] = lam;
+	yeMET[i] = (float)fdim((double)ye[i], xhii);
+}
+
+extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!p || p->n == 0 || !p->pos || !p->mass || !p->sml || !p->rho || !p->ie || !p->xHI || !p->ye)
+		return psg_fail(ctx, PSG_E_INVAL, "psg_load_particles: missing array");
+	if (p->n >= (size_t)PSG_INVALID_BIT)
+		return psg_fail(ctx, PSG_E_OVERFLOW, "psg_load_particles: at most 2^31-1 particles");
+	if (!(p->boxsize > 0))
+		return psg_fail(ctx, PSG_E_INVAL, "psg_load_particles: boxsize must be positive");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	free_particles(ctx);
+	free_tree(ctx);
+	const size_t n = p->n;
+	ctx->n = n;
+	ctx->boxsize = p->boxsize;
+	PSG_CUDA(cudaMalloc(&ctx->d_psml, sizeof(float4) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_mass, sizeof(float) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_rho, sizeof(float) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_yeMET, sizeof(float) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_ie, sizeof(float) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_flag, n));
+	PSG_CUDA(cudaMalloc(&ctx->d_lambdaH, sizeof(double) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_hits, sizeof(int32_t) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_lasthit, sizeof(int64_t) * n));
+	float *d_pos = (float *)psg_scratch(ctx, S_MISC, sizeof(float) * n * 7);
+	if (!d_pos) return PSG_E_NOMEM;
+	float *d_sml = d_pos + 3 * n, *d_xHI = d_pos + 4 * n, *d_ye = d_pos + 5 * n;
+	cudaStream_t s = ctx->stream;
+	PSG_CUDA(cudaMemcpyAsync(d_pos, p->pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
+	PSG_CUDA(cudaMemcpyAsync(d_sml, p->sml, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+	PSG_CUDA(cudaMemcpyAsync(d_xHI, p->xHI, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+	PSG_CUDA(cudaMemcpyAsync(d_ye, p->ye, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+	PSG_CUDA(cudaMemcpyAsync(ctx->d_mass, p->mass, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+	PSG_CUDA(cudaMemcpyAsync(ctx->d_rho, p->rho, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+	PSG_CUDA(cudaMemcpyAsync(ctx->d_ie, p->ie, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+	if (p->flag) PSG_CUDA(cudaMemcpyAsync(ctx->d_flag, p->flag, n, cudaMemcpyHostToDevice, s));
+	else PSG_CUDA(cudaMemsetAsync(ctx->d_flag, 0, n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_hits, 0, sizeof(int32_t) * n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_lasthit, 0, sizeof(int64_t) * n, s));
+	const int bs = 256;
+	k_init_particles<<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(n, d_pos, d_sml, d_xHI, d_ye,
+			ctx->d_psml, ctx->d_lambdaH, ctx->d_yeMET);
+	PSG_CHECK_LAUNCH();
+	PSG_CUDA(cudaStreamSynchronize(s));
+	return PSG_OK;
+}
+
+extern "C" int psg_get_state(psg_context *ctx, double *lambdaH, float *ie, int32_t *hits,
+		int64_t *lasthit) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_get_state: no particles loaded");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	cudaStream_t s = ctx->stream;
+	const size_t n = ctx->n;
+	if (lambdaH) PSG_CUDA(cudaMemcpyAsync(lambdaH, ctx->d_lambdaH, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+	if (ie) PSG_CUDA(cudaMemcpyAsync(ie, ctx->d_ie, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+	if (hits) PSG_CUDA(cudaMemcpyAsync(hits, ctx->d_hits, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+	if (lasthit) PSG_CUDA(cudaMemcpyAsync(lasthit, ctx->d_lasthit, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, s));
+	PSG_CUDA(cudaStreamSynchronize(s));
+	return PSG_OK;
+}
+
+extern "C" int psg_set_state(psg_context *ctx, const double *lambdaH, const float *ie,
+		const int64_t *lasthit) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_set_state: no particles loaded");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	cudaStream_t s = ctx->stream;
+	const size_t n = ctx->n;
+	if (lambdaH) PSG_CUDA(cudaMemcpyAsync(ctx->d_lambdaH, lambdaH, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+	if (ie) PSG_CUDA(cudaMemcpyAsync(ctx->d_ie, ie, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+	if (lasthit) PSG_CUDA(cudaMemcpyAsync(ctx->d_lasthit, lasthit, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s));
+	PSG_CUDA(cudaStreamSynchronize(s));
+	return PSG_OK;
+}

@@ -1,0 +1,121 @@
+// Internal declarations shared by the libpsg CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "psg.h"
+
+// Octree keys: 3 bits per level, child k = xbit | ybit<<1 | zbit<<2 as in
+// split() raytrace.c:282-287; level 1 in the top bits. 21 levels fit 63 bits.
+#define PSG_MAX_LEVELS 21
+#define PSG_KEY_OUTSIDE 0xFFFFFFFFFFFFFFFFull
+#define PSG_INVALID_BIT 0x80000000u
+
+// Bits of the device status word.
+#define PSG_ST_NAN 1u          // NaN/inf reached a particle state
+#define PSG_ST_SOLVER 2u       // the general integrator hit its step limit
+#define PSG_ST_IE_NEG 4u       // internal energy would turn negative (solve.c:137-139)
+
+struct psg_buf {
+	void *p = nullptr;
+	size_t bytes = 0;
+};
+
+struct psg_context {
+	int device = 0;
+	cudaStream_t stream = nullptr;       // the stream all work is issued on
+	cudaStream_t own_stream = nullptr;   // created with the context
+	char err[512] = {0};
+
+	// physics
+	int have_physics = 0;
+	psg_units u{};
+	psg_flags flags{};
+	double *d_ar = nullptr;      // [PSG_AR_NCOLS + 1][ar_nrows]: logT first
+	int ar_nrows = 0;
+	double ar_min = 0, ar_step_inv = 0;
+	double *d_xs = nullptr;      // [2][xs_nrows]: energy, sigma_HI
+	int xs_nrows = 0;
+	double xs_min = 0, xs_step_inv = 0, xs_cut_HI = 0;
+	double *d_kernel = nullptr;
+	int kernel_n = 0;
+
+	// particles, caller order
+	size_t n = 0;
+	double boxsize = 0;
+	float4 *d_psml = nullptr;    // x, y, z, sml
+	float *d_mass = nullptr, *d_rho = nullptr, *d_yeMET = nullptr, *d_ie = nullptr;
+	int8_t *d_flag = nullptr;
+	double *d_lambdaH = nullptr;
+	int32_t *d_hits = nullptr;
+	int64_t *d_lasthit = nullptr;
+
+	// octree, depth-first order
+	int have_tree = 0;
+	size_t ncell = 0, nleaf = 0, skipped = 0, nvalid = 0;
+	int depth = 0;
+	float4 *d_cell_lo = nullptr;  // bot.xyz, w = index past the subtree (int bits)
+	float4 *d_cell_hi = nullptr;  // top.xyz, w = first particle in leaf order (int bits)
+	float4 *d_leaf_psml = nullptr; // particles in leaf order
+	uint32_t *d_leaf_idx = nullptr; // caller index, PSG_INVALID_BIT if flagged
+
+	uint32_t *d_status = nullptr;
+
+	// scratch, grown on demand
+	psg_buf scratch[16];
+	cudaEvent_t ev[8] = {};
+	int timing = 0;
+	cudaEvent_t kev[2 * 4096] = {};      // per-launch events when timing is on
+	int nkev = 0;
+	int kev_kind[4096] = {};
+	long launches = 0;                   // kernels of this library launched
+};
+
+// error helpers ---------------------------------------------------------------
+int psg_fail(psg_context *ctx, int code, const char *fmt, ...);
+int psg_cuda_fail(psg_context *ctx, cudaError_t e, const char *what, const char *file, int line);
+#define PSG_CUDA(call)                                                               \
+	do {                                                                             \
+		cudaError_t e_ = (call);                                                     \
+		if (e_ != cudaSuccess) return psg_cuda_fail(ctx, e_, #call, __FILE__, __LINE__); \
+	} while (0)
+#define PSG_CHECK_LAUNCH() PSG_CUDA(cudaGetLastError())
+
+// scratch buffer slot `slot` with at least `bytes`; returns nullptr on failure
+void *psg_scratch(psg_context *ctx, int slot, size_t bytes);
+
+// scratch slots
+enum {
+	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
+	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC
+};
+
+// Per-launch timing: mark_begin/mark_end bracket a group of launches of one
+// kind with events on the context's stream (only when timing is on).
+inline void psg_mark_begin(psg_context *ctx, int kind) {
+	if (ctx->timing && ctx->nkev < 4096) {
+		cudaEventRecord(ctx->kev[2 * ctx->nkev], ctx->stream);
+		ctx->kev_kind[ctx->nkev] = kind;
+	}
+}
+inline void psg_mark_end(psg_context *ctx) {
+	if (ctx->timing && ctx->nkev < 4096) {
+		cudaEventRecord(ctx->kev[2 * ctx->nkev + 1], ctx->stream);
+		ctx->nkev++;
+	}
+}
+
+// tree / trace entry points used across units
+int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_db);
+
+// ---- device helpers ------------------------------------------------------------
+// Single-rounding float/double ops: the reference is compiled for x86-64 SSE
+// without FMA, so each product and sum rounds separately.
+__device__ __forceinline__ float rn_fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rn_fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rn_fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rn_dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rn_dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rn_dsub(double a, double b) { return __dsub_rn(a, b); }

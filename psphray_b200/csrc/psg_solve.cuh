@@ -1,0 +1,194 @@
+// Per-particle ionisation update on the device; replaces step_evolve()
+// solve.c:317 (LSODA over the 7-variable system of solve.c:76-141).
+//
+// Hydrogen-only, so only lambdaH (= xHI) and, when not isothermal, the
+// internal energy ie move. Normalised time s in [0,1] as in the reference
+// (every derivative multiplied by the step length, solve.c:120-121).
+//
+// Isothermal: with ye = 1 + m - lambda (m = yeMET plus the frozen helium
+// electrons), d(lambda)/ds = -g + tau*ye*(alpha*(1-lambda) - gamma*lambda) is
+// a Riccati equation with constant coefficients,
+//     d(lambda)/ds = a*lambda^2 - b*lambda + c,
+// solved exactly about its stable root p1 in FP64, carried in lambda = 1-x so
+// it stays accurate near full ionisation:
+//     y(1) = y0*e^-k / (1 - a*y0*phi(k)),  y = lambda - p1,
+//     k = sqrt(q^2 + 4*a*g), q = tau*(gamma*(1+m) + alpha*m), phi = (1-e^-k)/k,
+//     p1 = 2c/(b + k).
+// Not isothermal: adaptive Dormand-Prince 5(4) in FP64 over (lambda, ie).
+#pragma once
+
+#include "psg_internal.cuh"
+
+struct PhysParams {
+	const double *ar;      // [PSG_AR_NCOLS+1][ar_nrows], logT first
+	int ar_nrows;
+	double ar_min, ar_step_inv;
+	const double *xs;      // [2][xs_nrows]: energy, sigma_HI
+	int xs_nrows;
+	double xs_min, xs_step_inv, xs_cut_HI;
+	const double *kernel;
+	int kernel_n;
+	double H_PER_MASS, HI_ENERGY, MPROTON_OVER_BOLTZMANN, BOLTZMANN_OVER_MPROTON, hmf, hemf;
+	double he_e;           // helium electrons per H, helium frozen (psystem.h:134-137)
+	int isothermal, on_the_spot, adiabatic;
+};
+
+// tabfun_get() tabfun.c:38-58
+__device__ __forceinline__ double tab_get(int nrows, double min, double step_inv,
+		const double *__restrict__ x, const double *__restrict__ y, double v) {
+	const long long idx = (long long)rn_dmul(rn_dsub(v, min), step_inv);
+	if (idx < 0) return y[0];
+	if (idx >= nrows - 1) return y[nrows - 1];
+	const double lw = rn_dsub(x[idx + 1], v);
+	const double rw = rn_dsub(v, x[idx]);
+	return rn_dmul(rn_dadd(rn_dmul(lw, y[idx]), rn_dmul(rw, y[idx + 1])), step_inv);
+}
+
+__device__ __forceinline__ double ar_get(const PhysParams &P, int col, double logT) {
+	return tab_get(P.ar_nrows, P.ar_min, P.ar_step_inv, P.ar, P.ar + (size_t)P.ar_nrows * (col + 1), logT);
+}
+
+// xs_get() atomic-rate.c:126-131 for HI
+__device__ __forceinline__ double xs_get_HI(const PhysParams &P, double freq) {
+	if (freq < P.xs_cut_HI) return 0.0;
+	return tab_get(P.xs_nrows, P.xs_min, P.xs_step_inv, P.xs, P.xs + P.xs_nrows, freq);
+}
+
+// sph_depth() sph-depth.c:26-33
+__device__ __forceinline__ double sph_depth(const PhysParams &P, double r_h) {
+	const double x = rn_dmul((double)P.kernel_n, r_h);
+	if (!(x < (double)P.kernel_n) || !(x > -1.0)) return 0.0;
+	const int n = (int)x;
+	if (n < P.kernel_n && n >= 0) return P.kernel[n];
+	return 0.0;
+}
+
+// ieye2T() / Tye2ie() config.h:106-114
+__device__ __forceinline__ double ieye2T(const PhysParams &P, double ie, double ye) {
+	const double den = rn_dadd(rn_dadd(rn_dmul(P.hemf, 0.25), P.hmf), rn_dmul(P.hmf, ye));
+	return __ddiv_rn(rn_dmul(__ddiv_rn(rn_dmul(P.MPROTON_OVER_BOLTZMANN, ie), den), 2.0), 3.0);
+}
+__device__ __forceinline__ double Tye2ie(const PhysParams &P, double T, double ye) {
+	const double den = rn_dadd(rn_dadd(rn_dmul(P.hemf, 0.25), P.hmf), rn_dmul(P.hmf, ye));
+	return rn_dmul(__ddiv_rn(rn_dmul(rn_dmul(T, P.BOLTZMANN_OVER_MPROTON), den), 2.0), 3.0);
+}
+
+__device__ __forceinline__ double phi_k(double k) {
+	if (k > 1e-6) return -expm1(-k) / k;
+	return 1.0 - k * (0.5 - k / 6.0);
+}
+
+__device__ __forceinline__ double riccati_step(double lam0, double a, double b, double q, double c, double g) {
+	if (!(a > 0.0)) {
+		if (b > 0.0) {
+			const double eq = c / b;
+			return eq + (lam0 - eq) * exp(-b);
+		}
+		return lam0 + c;
+	}
+	const double k = sqrt(q * q + 4.0 * a * g);
+	const double p1 = 2.0 * c / (b + k);
+	const double y0 = lam0 - p1;
+	return p1 + y0 * exp(-k) / (1.0 - a * y0 * phi_k(k));
+}
+
+struct RhsCtx {
+	double yeMET, g, heat, time, nH, T;
+};
+
+// function() solve.c:76-141, hydrogen-only branch.
+__device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const double x[2], double dx[2]) {
+	const double xHI = x[0], xHII = 1.0 - x[0];
+	const double ye = xHII + P.he_e + cx.yeMET;
+	const double T = P.isothermal ? cx.T : ieye2T(P, x[1], ye);
+	const double logT = log10(T);
+	const double nH = cx.nH;
+	const double gamma = ar_get(P, PSG_AR_HI_CI, logT) * nH;
+	const double alpha = ar_get(P, P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A, logT) * nH;
+	dx[0] = (-cx.g / cx.time + (-gamma * ye * xHI + alpha * ye * xHII)) * cx.time;
+	if (P.isothermal || P.adiabatic) {
+		dx[1] = 0.0;
+	} else {
+		const double eta = ar_get(P, P.on_the_spot ? PSG_AR_HII_RCC_B : PSG_AR_HII_RCC_A, logT) * nH;
+		const double psi = ar_get(P, PSG_AR_HI_CEC, logT) * nH;
+		const double zeta = ar_get(P, PSG_AR_HI_CIC, logT) * nH;
+		const double beta = ar_get(P, PSG_AR_E_BREMC, logT) * nH;
+		const double chi = ar_get(P, PSG_AR_E_COMPC, logT);
+		const double L = P.H_PER_MASS * ((zeta + psi) * ye * xHI + eta * ye * xHII + beta * ye * xHII + chi * ye);
+		dx[1] = (cx.heat / cx.time - L) * cx.time;
+	}
+}
+
+// Adaptive Dormand-Prince 5(4); returns false if the step limit is reached.
+__device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2], int max_steps) {
+	const double a21 = 1. / 5, a31 = 3. / 40, a32 = 9. / 40, a41 = 44. / 45, a42 = -56. / 15, a43 = 32. / 9;
+	const double a51 = 19372. / 6561, a52 = -25360. / 2187, a53 = 64448. / 6561, a54 = -212. / 729;
+	const double a61 = 9017. / 3168, a62 = -355. / 33, a63 = 46732. / 5247, a64 = 49. / 176, a65 = -5103. / 18656;
+	const double b1 = 35. / 384, b3 = 500. / 1113, b4 = 125. / 192, b5 = -2187. / 6784, b6 = 11. / 84;
+	const double e1 = 71. / 57600, e3 = -71. / 16695, e4 = 71. / 1920, e5 = -17253. / 339200, e6 = 22. / 525, e7 = -1. / 40;
+	const double rtol = 1e-8;
+	const double atol0 = 1e-12, atol1 = 1e-10 * fabs(x[1]) + 1e-300;
+	double t = 0.0, h = 0.05;
+	double k1[2], k2[2], k3[2], k4[2], k5[2], k6[2], k7[2], y[2], yn[2];
+	rhs(P, cx, x, k1);
+	for (int it = 0; it < max_steps; it++) {
+		if (t >= 1.0) return true;
+		if (t + h > 1.0) h = 1.0 - t;
+		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a21 * k1[i]);
+		rhs(P, cx, y, k2);
+		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a31 * k1[i] + a32 * k2[i]);
+		rhs(P, cx, y, k3);
+		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+		rhs(P, cx, y, k4);
+		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i] + a54 * k4[i]);
+		rhs(P, cx, y, k5);
+		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i] + a64 * k4[i] + a65 * k5[i]);
+		rhs(P, cx, y, k6);
+		for (int i = 0; i < 2; i++) yn[i] = x[i] + h * (b1 * k1[i] + b3 * k3[i] + b4 * k4[i] + b5 * k5[i] + b6 * k6[i]);
+		rhs(P, cx, yn, k7);
+		double err = 0.0;
+		for (int i = 0; i < 2; i++) {
+			const double e = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i] + e6 * k6[i] + e7 * k7[i]);
+			const double sc = (i == 0 ? atol0 : atol1) + rtol * fmax(fabs(x[i]), fabs(yn[i]));
+			err += (e / sc) * (e / sc);
+		}
+		err = sqrt(0.5 * err);
+		if (err <= 1.0) {
+			t += h;
+			x[0] = yn[0]; x[1] = yn[1];
+			k1[0] = k7[0]; k1[1] = k7[1];
+		}
+		double fac = err > 0 ? 0.9 * pow(err, -0.2) : 5.0;
+		fac = fmin(5.0, fmax(0.2, fac));
+		h = fmax(h * fac, 1e-14);
+	}
+	return t >= 1.0;
+}
+
+// One particle step. lambdaH is clamped to [0,1] as solve.c:208 does.
+// Returns a PSG_ST_* bit on trouble, 0 otherwise.
+__device__ inline uint32_t solve_step(const PhysParams &P, double &lambdaH, double &ie, double yeMET,
+		double g, double heat, double time, double nH, double T) {
+	uint32_t st = 0;
+	if (P.isothermal) {
+		const double logT = log10(T);
+		const double gamma = ar_get(P, PSG_AR_HI_CI, logT) * nH;
+		const double alpha = ar_get(P, P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A, logT) * nH;
+		const double m = yeMET + P.he_e;
+		const double a = time * (alpha + gamma);
+		const double b = time * (alpha + (alpha + gamma) * (1.0 + m));
+		const double q = time * (gamma * (1.0 + m) + alpha * m);
+		const double c = time * alpha * (1.0 + m) - g;
+		lambdaH = riccati_step(lambdaH, a, b, q, c, g);
+	} else {
+		RhsCtx cx{yeMET, g, heat, time, nH, T};
+		double x[2] = {lambdaH, ie};
+		if (!dopri(P, cx, x, 200000)) st |= PSG_ST_SOLVER;
+		lambdaH = x[0];
+		ie = x[1];
+		if (!(ie >= 0.0)) st |= PSG_ST_IE_NEG;
+	}
+	if (!isfinite(lambdaH) || !isfinite(ie)) st |= PSG_ST_NAN;
+	lambdaH = fmin(1.0, fmax(0.0, lambdaH));
+	return st;
+}

@@ -1,0 +1,324 @@
+// Ray traversal; replaces rt_trace() raytrace.c:153-210 and the per-ray
+// sort of trace() loop.c:375-386.
+//
+// Cells are stored depth first with a skip pointer (the index just past the
+// subtree), so the reference's parent/sibling walk becomes a loop over one
+// index: a crossed cell continues at i+1 (its first child, or the next cell
+// after a leaf), a missed cell jumps to its skip pointer. The visiting order
+// and the set of crossed cells are the reference's. Hit lists are produced in
+// two passes (count, then fill at scanned offsets) and sorted per ray by
+// (d, ipar).
+#include <cub/cub.cuh>
+
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "psg_internal.cuh"
+
+namespace {
+
+// pluecker_() pluecker-sse.c:28-198. The reference's 8 hand-written sign
+// classes reduce to one rule per axis and per axis pair (selected by the
+// signs of dir); every product and difference rounds once, in float.
+__device__ __forceinline__ bool segment_hits_box(const float dir[3], float dist, const float s2b[3],
+		const float s2t[3]) {
+	bool up[3];
+#pragma unroll
+	for (int a = 0; a < 3; a++) {
+		up[a] = dir[a] > 0.0f;
+		const float step = rn_fmul(dist, dir[a]);
+		const float e2t = rn_fsub(s2t[a], step);
+		const float e2b = rn_fsub(s2b[a], step);
+		if (up[a] ? (s2t[a] < 0.0f) : (s2b[a] > 0.0f)) return false;
+		if (up[a] ? (e2b > 0.0f) : (e2t < 0.0f)) return false;
+	}
+#pragma unroll
+	for (int q = 0; q < 3; q++) {
+		const int i = q == 2 ? 1 : 0;
+		const int j = q == 0 ? 1 : 2;
+		const float P = up[i] ? s2t[j] : s2b[j];
+		const float R = up[i] ? s2b[j] : s2t[j];
+		const float Q = up[j] ? s2b[i] : s2t[i];
+		const float S = up[j] ? s2t[i] : s2b[i];
+		if (rn_fmul(dir[i], P) < rn_fmul(dir[j], Q) || rn_fmul(dir[i], R) > rn_fmul(dir[j], S)) return false;
+	}
+	return true;
+}
+
+struct RayGeom {
+	float s[3], dir[3], dist;
+};
+
+__device__ __forceinline__ RayGeom load_ray(const psg_ray *__restrict__ rays, size_t r) {
+	RayGeom g;
+	const psg_ray &ry = rays[r];
+#pragma unroll
+	for (int d = 0; d < 3; d++) { g.s[d] = ry.s[d]; g.dir[d] = ry.dir[d]; }
+	g.dist = (float)ry.length;      // rt_trace() takes the length as float
+	return g;
+}
+
+// The line test of raytrace.c:168-195: float differences and products,
+// double sums; accepted iff sml^2 >= (dc - proj)(dc + proj).
+__device__ __forceinline__ bool line_hits_particle(const RayGeom &g, float4 q, double &dc, double &r2) {
+	const float dx = rn_fsub(q.x, g.s[0]), dy = rn_fsub(q.y, g.s[1]), dz = rn_fsub(q.z, g.s[2]);
+	double proj = (double)rn_fmul(dx, g.dir[0]);
+	proj = rn_dadd(proj, (double)rn_fmul(dy, g.dir[1]));
+	proj = rn_dadd(proj, (double)rn_fmul(dz, g.dir[2]));
+	double d2 = (double)rn_fmul(dx, dx);
+	d2 = rn_dadd(d2, (double)rn_fmul(dy, dy));
+	d2 = rn_dadd(d2, (double)rn_fmul(dz, dz));
+	dc = __dsqrt_rn(d2);
+	r2 = rn_dmul(rn_dsub(dc, proj), rn_dadd(dc, proj));
+	return !((double)rn_fmul(q.w, q.w) < r2);
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(128) k_trace(const psg_ray *__restrict__ rays, size_t nray,
+		const float4 *__restrict__ cell_lo, const float4 *__restrict__ cell_hi, int ncell,
+		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx,
+		uint32_t *__restrict__ count, const int64_t *__restrict__ offsets,
+		uint32_t *__restrict__ out_ipar, double *__restrict__ out_d, double *__restrict__ out_b) {
+	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (r >= nray) return;
+	const RayGeom g = load_ray(rays, r);
+	uint32_t nh = 0;
+	int64_t o = FILL ? offsets[r] : 0;
+	int i = 0;
+	while (i < ncell) {
+		const float4 lo = __ldg(&cell_lo[i]);
+		const float4 hi = __ldg(&cell_hi[i]);
+		const int skip = __float_as_int(lo.w);
+		if (skip <= i) break;     // a well-formed tree always advances; never loop
+		const float s2b[3] = {rn_fsub(lo.x, g.s[0]), rn_fsub(lo.y, g.s[1]), rn_fsub(lo.z, g.s[2])};
+		const float s2t[3] = {rn_fsub(hi.x, g.s[0]), rn_fsub(hi.y, g.s[1]), rn_fsub(hi.z, g.s[2])};
+		if (segment_hits_box(g.dir, g.dist, s2b, s2t)) {
+			if (skip == i + 1) {
+				const int p0 = __float_as_int(hi.w);
+				const int p1 = __float_as_int(__ldg(&cell_hi[i + 1]).w);
+				for (int p = p0; p < p1; p++) {
+					const uint32_t idx = __ldg(&lidx[p]);
+					if (idx & PSG_INVALID_BIT) continue;
+					double dc, r2;
+					if (line_hits_particle(g, __ldg(&lpsml[p]), dc, r2)) {
+						if (FILL) {
+							out_ipar[o] = idx;
+							out_d[o] = dc;
+							out_b[o] = __dsqrt_rn(fabs(r2));
+							o++;
+						}
+						nh++;
+					}
+				}
+			}
+			i++;
+		} else {
+			i = skip;
+		}
+	}
+	if (!FILL) count[r] = nh;
+}
+
+__global__ void k_offsets64(const uint32_t *__restrict__ scan32, const uint32_t *__restrict__ count,
+		size_t nray, int64_t *__restrict__ off64, int32_t *__restrict__ off32) {
+	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (r > nray) return;
+	// scan32 holds the exclusive scan over nray+1 entries (count[nray] = 0)
+	off64[r] = scan32[r];
+	off32[r] = (int32_t)scan32[r];
+	(void)count;
+}
+
+__global__ void k_sort_keys(size_t nhit, const double *__restrict__ d, unsigned long long *__restrict__ keys,
+		uint32_t *__restrict__ vals) {
+	const size_t h = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (h >= nhit) return;
+	keys[h] = (unsigned long long)__double_as_longlong(d[h]);   // d >= 0: bit order is value order
+	vals[h] = (uint32_t)h;
+}
+
+__global__ void k_gather_sorted(size_t nhit, const uint32_t *__restrict__ perm,
+		const uint32_t *__restrict__ raw_ipar, const double *__restrict__ raw_d,
+		const double *__restrict__ raw_b, uint32_t *__restrict__ ipar, double *__restrict__ d,
+		double *__restrict__ b) {
+	const size_t h = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (h >= nhit) return;
+	const uint32_t j = perm[h];
+	ipar[h] = raw_ipar[j];
+	d[h] = raw_d[j];
+	b[h] = raw_b[j];
+}
+
+// Runs of equal d inside a ray are put in ipar order (the reference leaves
+// their order to qsort); insertion sort, runs are almost always length 1.
+__global__ void k_break_ties(size_t nray, const int64_t *__restrict__ off, uint32_t *__restrict__ ipar,
+		double *__restrict__ d, double *__restrict__ b) {
+	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (r >= nray) return;
+	const int64_t h0 = off[r], h1 = off[r + 1];
+	for (int64_t h = h0 + 1; h < h1; h++) {
+		if (d[h] != d[h - 1]) continue;
+		int64_t k = h;
+		while (k > h0 && d[k - 1] == d[k] && ipar[k - 1] > ipar[k]) {
+			const uint32_t ti = ipar[k]; ipar[k] = ipar[k - 1]; ipar[k - 1] = ti;
+			const double tb = b[k]; b[k] = b[k - 1]; b[k - 1] = tb;
+			k--;
+		}
+	}
+}
+
+inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+}  // namespace
+
+// Traces nray device-resident rays. Leaves in scratch: S_OFFSETS (int64
+// offsets[nray+1], then int32 offsets[nray+1]), S_HIT_IPAR (sorted caller
+// indices), S_RAW_D (sorted d) and S_HIT_KERN (sorted b).
+int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_db) {
+	(void)want_db;
+	if (!ctx->have_tree) return psg_fail(ctx, PSG_E_INVAL, "trace: no tree (psg_build_tree first)");
+	cudaStream_t st = ctx->stream;
+	uint32_t *count = (uint32_t *)psg_scratch(ctx, S_COUNT, sizeof(uint32_t) * 2 * (nray + 1));
+	char *offmem = (char *)psg_scratch(ctx, S_OFFSETS, (sizeof(int64_t) + sizeof(int32_t)) * (nray + 1) + 256);
+	if (!count || !offmem) return PSG_E_NOMEM;
+	uint32_t *scan = count + (nray + 1);
+	int64_t *off64 = (int64_t *)offmem;
+	int32_t *off32 = (int32_t *)(offmem + sizeof(int64_t) * (nray + 1));
+	const int ncell = (int)ctx->ncell;
+	PSG_CUDA(cudaMemsetAsync(count + nray, 0, sizeof(uint32_t), st));
+	psg_mark_begin(ctx, PSG_K_TRACE_COUNT);
+	if (nray) ctx->launches++;
+	if (nray)
+		k_trace<false><<<blocks(nray, 128), 128, 0, st>>>(d_rays, nray, ctx->d_cell_lo, ctx->d_cell_hi,
+				ncell, ctx->d_leaf_psml, ctx->d_leaf_idx, count, nullptr, nullptr, nullptr, nullptr);
+	PSG_CHECK_LAUNCH();
+	psg_mark_end(ctx);
+	size_t tmp = 0;
+	PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, count, scan, (int)(nray + 1), st));
+	void *dt = psg_scratch(ctx, S_CUB, tmp);
+	if (!dt) return PSG_E_NOMEM;
+	PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, count, scan, (int)(nray + 1), st));
+	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32);
+	PSG_CHECK_LAUNCH();
+	ctx->launches++;
+	uint32_t total32 = 0;
+	PSG_CUDA(cudaMemcpyAsync(&total32, scan + nray, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
+	const size_t nhit = total32;
+	if (nhit >= (size_t)INT32_MAX)
+		return psg_fail(ctx, PSG_E_OVERFLOW, "trace: %zu hits in one batch exceed 2^31", nhit);
+	const size_t hb = nhit ? nhit : 1;
+	uint32_t *raw_ipar = (uint32_t *)psg_scratch(ctx, S_RAW_IPAR, sizeof(uint32_t) * hb);
+	double *raw_d = (double *)psg_scratch(ctx, S_RAW_D, sizeof(double) * 2 * hb);
+	double *raw_b = (double *)psg_scratch(ctx, S_RAW_B, sizeof(double) * hb);
+	unsigned long long *keys = (unsigned long long *)psg_scratch(ctx, S_KEYS, sizeof(unsigned long long) * 2 * hb);
+	uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
+	uint32_t *hit_ipar = (uint32_t *)psg_scratch(ctx, S_HIT_IPAR, sizeof(uint32_t) * hb);
+	double *hit_b = (double *)psg_scratch(ctx, S_HIT_KERN, sizeof(double) * hb);
+	if (!raw_ipar || !raw_d || !raw_b || !keys || !vals || !hit_ipar || !hit_b) return PSG_E_NOMEM;
+	double *hit_d = raw_d + hb;
+	psg_mark_begin(ctx, PSG_K_TRACE_FILL);
+	if (nray) ctx->launches++;
+	if (nray)
+		k_trace<true><<<blocks(nray, 128), 128, 0, st>>>(d_rays, nray, ctx->d_cell_lo, ctx->d_cell_hi,
+				ncell, ctx->d_leaf_psml, ctx->d_leaf_idx, nullptr, off64, raw_ipar, raw_d, raw_b);
+	PSG_CHECK_LAUNCH();
+	psg_mark_end(ctx);
+	if (nhit) {
+		psg_mark_begin(ctx, PSG_K_SORT);
+		ctx->launches += 3;
+		k_sort_keys<<<blocks(nhit, 256), 256, 0, st>>>(nhit, raw_d, keys, vals);
+		PSG_CHECK_LAUNCH();
+		size_t stmp = 0;
+		PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, stmp, keys, keys + hb, vals, vals + hb,
+				(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
+		void *dst = psg_scratch(ctx, S_CUB, stmp);
+		if (!dst) return PSG_E_NOMEM;
+		PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(dst, stmp, keys, keys + hb, vals, vals + hb,
+				(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
+		k_gather_sorted<<<blocks(nhit, 256), 256, 0, st>>>(nhit, vals + hb, raw_ipar, raw_d, raw_b,
+				hit_ipar, hit_d, hit_b);
+		PSG_CHECK_LAUNCH();
+		k_break_ties<<<blocks(nray, 128), 128, 0, st>>>(nray, off64, hit_ipar, hit_d, hit_b);
+		PSG_CHECK_LAUNCH();
+		psg_mark_end(ctx);
+	}
+	return PSG_OK;
+}
+
+// copies the traced hit lists to host Xtype records
+static int download_hits(psg_context *ctx, size_t nray, int64_t *offsets, psg_xtype **x, size_t *size,
+		size_t *nhit_out) {
+	cudaStream_t st = ctx->stream;
+	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
+	std::vector<int64_t> off(nray + 1);
+	PSG_CUDA(cudaMemcpyAsync(off.data(), off64, sizeof(int64_t) * (nray + 1), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
+	const size_t nhit = (size_t)off[nray];
+	if (offsets) memcpy(offsets, off.data(), sizeof(int64_t) * (nray + 1));
+	if (*x == nullptr || *size < nhit) {
+		size_t want = *size ? *size : 1000;
+		while (want < nhit) want *= 2;
+		psg_xtype *nx = (psg_xtype *)realloc(*x, sizeof(psg_xtype) * want);
+		if (!nx) return psg_fail(ctx, PSG_E_NOMEM, "trace: host allocation failed");
+		*x = nx;
+		*size = want;
+	}
+	if (nhit) {
+		std::vector<uint32_t> ip(nhit);
+		std::vector<double> d(nhit), b(nhit);
+		const size_t hb = nhit;
+		double *hit_d = (double *)ctx->scratch[S_RAW_D].p + hb;
+		PSG_CUDA(cudaMemcpyAsync(ip.data(), ctx->scratch[S_HIT_IPAR].p, sizeof(uint32_t) * nhit, cudaMemcpyDeviceToHost, st));
+		PSG_CUDA(cudaMemcpyAsync(d.data(), hit_d, sizeof(double) * nhit, cudaMemcpyDeviceToHost, st));
+		PSG_CUDA(cudaMemcpyAsync(b.data(), ctx->scratch[S_HIT_KERN].p, sizeof(double) * nhit, cudaMemcpyDeviceToHost, st));
+		PSG_CUDA(cudaStreamSynchronize(st));
+		for (size_t h = 0; h < nhit; h++) {
+			(*x)[h].ipar = ip[h];
+			(*x)[h].d = d[h];
+			(*x)[h].b = b[h];
+		}
+	}
+	*nhit_out = nhit;
+	return PSG_OK;
+}
+
+static int upload_rays(psg_context *ctx, const psg_ray *rays, size_t nray, psg_ray **d_rays) {
+	psg_ray *d = (psg_ray *)psg_scratch(ctx, S_RAYS, sizeof(psg_ray) * (nray ? nray : 1));
+	if (!d) return PSG_E_NOMEM;
+	if (nray) PSG_CUDA(cudaMemcpyAsync(d, rays, sizeof(psg_ray) * nray, cudaMemcpyHostToDevice, ctx->stream));
+	*d_rays = d;
+	return PSG_OK;
+}
+
+extern "C" int psg_trace(psg_context *ctx, const psg_ray *rays, size_t nray, int64_t *offsets,
+		psg_xtype **x, size_t *size) {
+	if (!ctx) return PSG_E_INVAL;
+	if ((nray && !rays) || !x || !size) return psg_fail(ctx, PSG_E_INVAL, "psg_trace: null argument");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	psg_ray *d_rays = nullptr;
+	int rc = upload_rays(ctx, rays, nray, &d_rays);
+	if (rc) return rc;
+	rc = psg_trace_internal(ctx, d_rays, nray, 1);
+	if (rc) return rc;
+	size_t nhit = 0;
+	return download_hits(ctx, nray, offsets, x, size, &nhit);
+}
+
+extern "C" size_t psg_rt_trace(psg_context *ctx, const float s[3], const float dir[3], const float dist,
+		psg_xtype **x, size_t *size) {
+	if (!ctx || !s || !dir || !x || !size) return (size_t)-1;
+	psg_ray ray;
+	memset(&ray, 0, sizeof(ray));
+	for (int d = 0; d < 3; d++) { ray.s[d] = s[d]; ray.dir[d] = dir[d]; }
+	ray.length = dist;
+	if (cudaSetDevice(ctx->device) != cudaSuccess) return (size_t)-1;
+	psg_ray *d_rays = nullptr;
+	if (upload_rays(ctx, &ray, 1, &d_rays)) return (size_t)-1;
+	if (psg_trace_internal(ctx, d_rays, 1, 1)) return (size_t)-1;
+	size_t nhit = 0;
+	if (download_hits(ctx, 1, nullptr, x, size, &nhit)) return (size_t)-1;
+	return nhit;
+}
