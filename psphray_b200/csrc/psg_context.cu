@@ -52,7 +52,8 @@ extern "C" int psg_create(psg_context **out, int device) {
 	if (cudaSetDevice(device) != cudaSuccess ||
 			cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
 			cudaMalloc(&ctx->d_status, sizeof(uint32_t)) != cudaSuccess ||
-			cudaMemset(ctx->d_status, 0, sizeof(uint32_t)) != cudaSuccess) {
+			cudaMemset(ctx->d_status, 0, sizeof(uint32_t)) != cudaSuccess ||
+			cudaMalloc(&ctx->d_counters, 8 * sizeof(unsigned long long)) != cudaSuccess) {
 		cudaGetLastError();
 		delete ctx;
 		return PSG_E_CUDA;
@@ -90,6 +91,7 @@ extern "C" void psg_destroy(psg_context *ctx) {
 	if (ctx->d_xs) cudaFree(ctx->d_xs);
 	if (ctx->d_kernel) cudaFree(ctx->d_kernel);
 	if (ctx->d_status) cudaFree(ctx->d_status);
+	if (ctx->d_counters) cudaFree(ctx->d_counters);
 	for (auto &b : ctx->scratch) if (b.p) cudaFree(b.p);
 	for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
 	for (auto &ev : ctx->kev) if (ev) cudaEventDestroy(ev);

@@ -62,9 +62,12 @@ struct psg_context {
 	uint32_t *d_leaf_idx = nullptr; // caller index, PSG_INVALID_BIT if flagged
 
 	uint32_t *d_status = nullptr;
+	unsigned long long *d_counters = nullptr;   // 8 device counters (records, deposits capped, ...)
 
 	// scratch, grown on demand
-	psg_buf scratch[16];
+	psg_buf scratch[20];
+	size_t rec_cap = 0;   // capacity of the traversal's hit-record buffer
+	int ppc = 8;          // leaf capacity of the current tree
 	cudaEvent_t ev[8] = {};
 	int timing = 0;
 	cudaEvent_t kev[2 * 4096] = {};      // per-launch events when timing is on
@@ -89,7 +92,7 @@ void *psg_scratch(psg_context *ctx, int slot, size_t bytes);
 // scratch slots
 enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
-	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC
+	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64
 };
 
 // Per-launch timing: mark_begin/mark_end bracket a group of launches of one

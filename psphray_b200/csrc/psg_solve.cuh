@@ -165,6 +165,23 @@ __device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2],
 	return t >= 1.0;
 }
 
+// Isothermal step only (the closed form), for the kernels specialised on it.
+__device__ inline uint32_t solve_step_iso(const PhysParams &P, double &lambdaH, double yeMET, double g,
+		double time, double nH, double T) {
+	const double logT = log10(T);
+	const double gamma = ar_get(P, PSG_AR_HI_CI, logT) * nH;
+	const double alpha = ar_get(P, P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A, logT) * nH;
+	const double m = yeMET + P.he_e;
+	const double a = time * (alpha + gamma);
+	const double b = time * (alpha + (alpha + gamma) * (1.0 + m));
+	const double q = time * (gamma * (1.0 + m) + alpha * m);
+	const double c = time * alpha * (1.0 + m) - g;
+	lambdaH = riccati_step(lambdaH, a, b, q, c, g);
+	const uint32_t st = isfinite(lambdaH) ? 0u : PSG_ST_NAN;
+	lambdaH = fmin(1.0, fmax(0.0, lambdaH));
+	return st;
+}
+
 // One particle step. lambdaH is clamped to [0,1] as solve.c:208 does.
 // Returns a PSG_ST_* bit on trouble, 0 otherwise.
 __device__ inline uint32_t solve_step(const PhysParams &P, double &lambdaH, double &ie, double yeMET,

@@ -128,15 +128,25 @@ __device__ __forceinline__ bool below_cutoff(double TM, double Nph) {
 	return TM < 0.0 || __ddiv_rn(TM, Nph) < 1e-10;
 }
 
-__global__ void __launch_bounds__(128) k_deposit(const psg_ray *__restrict__ rays, size_t ray0, int nray,
+// One block of DEP_THREADS per ray; hits are taken DEP_THREADS at a time.
+// Within a chunk, optical depths are summed with a block-wide FP64 scan; the
+// first hit whose absorption exceeds its neutral atoms (loop.c:482-485) or
+// after which TM/Nph < 1e-10 (loop.c:585) is found with a block min, settled
+// by its own thread, and the scan restarts after it.
+#define DEP_THREADS 256
+#define DEP_WARPS (DEP_THREADS / 32)
+
+__global__ void __launch_bounds__(DEP_THREADS) k_deposit(const psg_ray *__restrict__ rays, size_t ray0, int nray,
 		const int64_t *__restrict__ off, const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
 		const uint32_t *__restrict__ slot, const double *__restrict__ lambdaH, const float *__restrict__ mass,
 		PhysParams P, int want_heat, double *__restrict__ acc, double *__restrict__ acc_heat,
 		unsigned long long *__restrict__ n_sat, double *__restrict__ lost) {
-	const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int lane = threadIdx.x & 31;
-	if (w >= nray) return;
-	const size_t r = ray0 + w;
+	__shared__ double s_wsum[DEP_WARPS];
+	__shared__ int s_first;
+	__shared__ double s_tm;
+	const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+	const size_t r = ray0 + blockIdx.x;
+	if (blockIdx.x >= (unsigned)nray) return;
 	const int64_t h0 = off[r], h1 = off[r + 1];
 	if (h1 == h0) return;
 	const double Nph = rays[r].Nph;
@@ -147,8 +157,8 @@ __global__ void __launch_bounds__(128) k_deposit(const psg_ray *__restrict__ ray
 	double TM = Nph;
 	bool done = skip_ray;
 	unsigned nsat = 0;
-	for (int64_t base = h0; base < h1; base += 32) {
-		const int64_t h = base + lane;
+	for (int64_t base = h0; base < h1; base += DEP_THREADS) {
+		const int64_t h = base + tid;
 		const bool valid = h < h1;
 		double tau = 0.0, NHI = 0.0, NH_inv = 0.0, delta = -1.0;
 		if (valid && !done) {
@@ -159,51 +169,74 @@ __global__ void __launch_bounds__(128) k_deposit(const psg_ray *__restrict__ ray
 			NH_inv = __ddiv_rn(1.0, NH);
 		}
 		int start = 0;
-		while (!done && start < 32) {
-			const bool part = valid && lane >= start && tau != 0.0;
+		while (!done && start < DEP_THREADS) {
+			const bool part = valid && tid >= start && tau != 0.0;
 			const double my_tau = part ? tau : 0.0;
-			const double incl = warp_incl_sum(my_tau, lane);
-			double excl = __shfl_up_sync(0xffffffffu, incl, 1);
-			if (lane == 0) excl = 0.0;
+			// block scan: warp scan, then the warp totals
+			double wi = my_tau;
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				const double u = __shfl_up_sync(0xffffffffu, wi, o);
+				if (lane >= o) wi += u;
+			}
+			double we = __shfl_up_sync(0xffffffffu, wi, 1);
+			if (lane == 0) we = 0.0;
+			if (lane == 31) s_wsum[wid] = wi;
+			if (tid == 0) s_first = DEP_THREADS;
+			__syncthreads();
+			double woff = 0.0, total = 0.0;
+			for (int k = 0; k < DEP_WARPS; k++) {
+				const double v = s_wsum[k];
+				if (k < wid) woff += v;
+				total += v;
+			}
+			const double incl = woff + wi, excl = woff + we;
 			const double TMj = TM * exp(-excl);
 			double absorb = TMj * -expm1(-my_tau);
 			const double TMafter = TM * exp(-incl);
 			const bool capped = part && absorb > NHI;
 			const bool cut = part && below_cutoff(TMafter, Nph);
-			const unsigned ev = __ballot_sync(0xffffffffu, capped || cut);
-			const int f = ev ? __ffs(ev) - 1 : 32;
-			if (part && lane < f) delta = rn_dmul(absorb, NH_inv);
-			if (f == 32) {
-				TM = TM * exp(-__shfl_sync(0xffffffffu, incl, 31));
+			if (capped || cut) atomicMin(&s_first, tid);
+			__syncthreads();
+			const int f = s_first;
+			if (part && tid < f) delta = rn_dmul(absorb, NH_inv);
+			if (f == DEP_THREADS) {
+				TM = TM * exp(-total);
+				__syncthreads();     // s_wsum / s_first are rewritten by the next chunk
 				break;
 			}
-			double TMnew = TMafter;
-			if (lane == f) {
+			if (tid == f) {
+				double TMnew = TMafter;
 				if (capped) {
 					absorb = NHI;
 					TMnew = TMj - NHI;
+					nsat++;
 				}
 				delta = rn_dmul(absorb, NH_inv);
+				s_tm = TMnew;
 			}
-			nsat += (lane == f && capped) ? 1u : 0u;
-			TM = __shfl_sync(0xffffffffu, TMnew, f);
+			__syncthreads();
+			TM = s_tm;
 			if (below_cutoff(TM, Nph)) done = true;
 			start = f + 1;
+			__syncthreads();
 		}
 		if (valid) {
-			const uint32_t s = slot[h];
-			acc[s] = delta;
-			if (want_heat) acc_heat[s] = delta >= 0.0 ? rn_dmul(heat_factor, delta) : 0.0;
+			const uint32_t sl = slot[h];
+			acc[sl] = delta;
+			if (want_heat) acc_heat[sl] = delta >= 0.0 ? rn_dmul(heat_factor, delta) : 0.0;
 		}
 	}
 	for (int o = 16; o > 0; o >>= 1) nsat += __shfl_down_sync(0xffffffffu, nsat, o);
-	if (lane == 0) {
-		if (nsat) atomicAdd(n_sat, (unsigned long long)nsat);
-		if (!skip_ray) atomicAdd(lost, TM);
-	}
+	if (lane == 0 && nsat) atomicAdd(n_sat, (unsigned long long)nsat);
+	if (tid == 0 && !skip_ray) atomicAdd(lost, TM);
 }
 
-// update_pars() loop.c:653-770 for the particles hit in tick t.
+// update_pars() loop.c:653-770 for the particles hit in tick t, one thread
+// per particle. A particle's deposits are summed in slot order; segments
+// longer than a warp (particles next to a source are hit by nearly every
+// ray) are summed by the whole warp, lanes strided, then a fixed butterfly.
+template <bool ISO>
 __global__ void __launch_bounds__(256) k_update(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
 		const double *__restrict__ acc, const double *__restrict__ acc_heat, int want_heat,
@@ -211,12 +244,20 @@ __global__ void __launch_bounds__(256) k_update(int t, const int32_t *__restrict
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
 		PhysParams P, int64_t tick, double tick_time, uint32_t *__restrict__ status) {
 	const int lo = tick_act[t], hi = tick_act[t + 1];
-	uint32_t st = 0;
-	for (int a = lo + blockIdx.x * blockDim.x + threadIdx.x; a < hi; a += gridDim.x * blockDim.x) {
-		const uint32_t p = act_ipar[a];
-		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
-		double g = 0.0, heat = 0.0;
-		int nh = 0;
+	const int lane = threadIdx.x & 31;
+	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
+	const bool mine = a < hi;
+	if (__all_sync(0xffffffffu, !mine)) return;
+	uint32_t p = 0, s0 = 0, s1 = 0;
+	if (mine) {
+		p = act_ipar[a];
+		s0 = act_seg[a];
+		s1 = act_seg[a + 1];
+	}
+	double g = 0.0, heat = 0.0;
+	int nh = 0;
+	const bool longseg = mine && (s1 - s0) > 32;
+	if (mine && !longseg) {
 		for (uint32_t k = s0; k < s1; k++) {
 			const double d = acc[k];
 			if (d >= 0.0) {
@@ -225,22 +266,48 @@ __global__ void __launch_bounds__(256) k_update(int t, const int32_t *__restrict
 				nh++;
 			}
 		}
-		const double time = rn_dmul((double)(tick - lasthit[p]), tick_time);
-		const double lam0 = lambdaH[p];
-		const double ie0 = (double)ie[p];
-		const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, lam0), P.he_e));
-		const double nH = rn_dmul(P.H_PER_MASS, (double)rho[p]);
-		double lam = lam0, e = ie0;
-		st |= solve_step(P, lam, e, (double)yeMET[p], g, heat, time, nH, T);
-		lambdaH[p] = lam;
-		if (P.isothermal) {
-			ie[p] = (float)Tye2ie(P, T, rn_dadd(rn_dsub(1.0, lam), P.he_e));
-		} else if (!P.adiabatic) {
-			ie[p] = (float)e;
-		}
-		lasthit[p] = tick;
-		hits[p] += nh;
 	}
+	unsigned lm = __ballot_sync(0xffffffffu, longseg);
+	while (lm) {
+		const int l = __ffs(lm) - 1;
+		lm &= lm - 1;
+		const uint32_t b0 = __shfl_sync(0xffffffffu, s0, l), b1 = __shfl_sync(0xffffffffu, s1, l);
+		double sg = 0.0, sh = 0.0;
+		int sn = 0;
+		for (uint32_t k = b0 + lane; k < b1; k += 32) {
+			const double d = acc[k];
+			if (d >= 0.0) {
+				sg += d;
+				if (want_heat) sh += acc_heat[k];
+				sn++;
+			}
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			sg += __shfl_xor_sync(0xffffffffu, sg, o);
+			sh += __shfl_xor_sync(0xffffffffu, sh, o);
+			sn += __shfl_xor_sync(0xffffffffu, sn, o);
+		}
+		if (lane == l) { g = sg; heat = sh; nh = sn; }
+	}
+	if (!mine) return;
+	const double time = rn_dmul((double)(tick - lasthit[p]), tick_time);
+	const double lam0 = lambdaH[p];
+	const double ie0 = (double)ie[p];
+	const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, lam0), P.he_e));
+	const double nH = rn_dmul(P.H_PER_MASS, (double)rho[p]);
+	double lam = lam0, e = ie0;
+	uint32_t st;
+	if (ISO) st = solve_step_iso(P, lam, (double)yeMET[p], g, time, nH, T);
+	else st = solve_step(P, lam, e, (double)yeMET[p], g, heat, time, nH, T);
+	lambdaH[p] = lam;
+	if (ISO) {
+		ie[p] = (float)Tye2ie(P, T, rn_dadd(rn_dsub(1.0, lam), P.he_e));
+	} else if (!P.adiabatic) {
+		ie[p] = (float)e;
+	}
+	lasthit[p] = tick;
+	hits[p] += nh;
 	if (st) atomicOr(status, st);
 }
 
@@ -353,29 +420,37 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	PSG_CHECK_LAUNCH();
 	ctx->launches++;
 	psg_mark_end(ctx);
-	unsigned long long *d_nsat = (unsigned long long *)psg_scratch(ctx, S_MISC, 64);
-	if (!d_nsat) return PSG_E_NOMEM;
-	double *d_lost = (double *)(d_nsat + 1);
+	unsigned long long *d_nsat = ctx->d_counters + 1;
+	double *d_lost = (double *)(ctx->d_counters + 2);
 	PSG_CUDA(cudaMemsetAsync(d_nsat, 0, 16, st));
 	PSG_CUDA(cudaEventRecord(ctx->ev[1], st));
 
 	// the tick loop
-	int dev_sms = 148;
-	cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
-	const unsigned upd_grid = (unsigned)(dev_sms * 8);
+	std::vector<int32_t> h_tick_act(K + 1);
+	PSG_CUDA(cudaMemcpyAsync(h_tick_act.data(), tick_act, sizeof(int32_t) * (K + 1), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
 	for (size_t t = 0; t < K; t++) {
 		psg_mark_begin(ctx, PSG_K_DEPOSIT);
-		k_deposit<<<blocks(R * 32, 128), 128, 0, st>>>(d_rays, t * R, (int)R, off64, hit_ipar, hit_kern,
+		k_deposit<<<(unsigned)R, DEP_THREADS, 0, st>>>(d_rays, t * R, (int)R, off64, hit_ipar, hit_kern,
 				slot, ctx->d_lambdaH, ctx->d_mass, P, want_heat, acc, acc_heat, d_nsat, d_lost);
 		PSG_CHECK_LAUNCH();
 		psg_mark_end(ctx);
+		const int nact_t = h_tick_act[t + 1] - h_tick_act[t];
 		psg_mark_begin(ctx, PSG_K_UPDATE);
-		k_update<<<upd_grid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat,
-				ctx->d_lambdaH, ctx->d_ie, ctx->d_hits, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P,
-				first_tick + (int64_t)t, tick_time, ctx->d_status);
-		PSG_CHECK_LAUNCH();
+		if (nact_t > 0) {
+			if (ctx->flags.isothermal)
+				k_update<true><<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
+						acc_heat, want_heat, ctx->d_lambdaH, ctx->d_ie, ctx->d_hits, ctx->d_lasthit, ctx->d_rho,
+						ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, ctx->d_status);
+			else
+				k_update<false><<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
+						acc_heat, want_heat, ctx->d_lambdaH, ctx->d_ie, ctx->d_hits, ctx->d_lasthit, ctx->d_rho,
+						ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, ctx->d_status);
+			PSG_CHECK_LAUNCH();
+			ctx->launches++;
+		}
 		psg_mark_end(ctx);
-		ctx->launches += 2;
+		ctx->launches++;
 	}
 	PSG_CUDA(cudaEventRecord(ctx->ev[2], st));
 	rc = check_status(ctx);

@@ -75,50 +75,116 @@ __device__ __forceinline__ bool line_hits_particle(const RayGeom &g, float4 q, d
 	return !((double)rn_fmul(q.w, q.w) < r2);
 }
 
-template <bool FILL>
-__global__ void __launch_bounds__(128) k_trace(const psg_ray *__restrict__ rays, size_t nray,
+// One warp per ray. The warp tests 32 consecutive cells of the depth-first
+// array at once. A cell is inside a missed cell's subtree iff some missed
+// cell k before it in the window has skip_k > j; a warp max-scan of the
+// missed cells' skip pointers decides that for all 32 lanes. Crossed leaves
+// of the window list their particles in shared memory and the lanes test
+// them 32 at a time. The next window starts after the window or after the
+// furthest missed subtree, whichever is later, so every window advances by
+// at least 32 cells. Accepted hits are appended with one atomic per warp
+// round; each record carries its ray and its rank within the ray (the
+// traversal order), so the scatter into per-ray lists is deterministic.
+__global__ void __launch_bounds__(128) k_trace_warp(const psg_ray *__restrict__ rays, size_t nray,
 		const float4 *__restrict__ cell_lo, const float4 *__restrict__ cell_hi, int ncell,
-		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx,
-		uint32_t *__restrict__ count, const int64_t *__restrict__ offsets,
-		uint32_t *__restrict__ out_ipar, double *__restrict__ out_d, double *__restrict__ out_b) {
-	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx, int ppc,
+		uint32_t *__restrict__ count, unsigned long long *__restrict__ nrec, size_t cap,
+		uint32_t *__restrict__ rec_ipar, uint32_t *__restrict__ rec_ray, uint32_t *__restrict__ rec_pos,
+		double *__restrict__ rec_d, double *__restrict__ rec_b) {
+	extern __shared__ int list_all[];
+	const int lane = threadIdx.x & 31;
+	const int wib = threadIdx.x >> 5;
+	int *list = list_all + wib * 32 * ppc;
+	const size_t r = (size_t)blockIdx.x * (blockDim.x >> 5) + wib;
 	if (r >= nray) return;
 	const RayGeom g = load_ray(rays, r);
+	const unsigned lt_mask = (1u << lane) - 1u;
 	uint32_t nh = 0;
-	int64_t o = FILL ? offsets[r] : 0;
 	int i = 0;
 	while (i < ncell) {
-		const float4 lo = __ldg(&cell_lo[i]);
-		const float4 hi = __ldg(&cell_hi[i]);
+		const int j = i + lane;
+		const bool valid = j < ncell;
+		float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+		if (valid) lo = __ldg(&cell_lo[j]);
+		if (j <= ncell) hi = __ldg(&cell_hi[j]);     // the sentinel closes the last leaf
 		const int skip = __float_as_int(lo.w);
-		if (skip <= i) break;     // a well-formed tree always advances; never loop
-		const float s2b[3] = {rn_fsub(lo.x, g.s[0]), rn_fsub(lo.y, g.s[1]), rn_fsub(lo.z, g.s[2])};
-		const float s2t[3] = {rn_fsub(hi.x, g.s[0]), rn_fsub(hi.y, g.s[1]), rn_fsub(hi.z, g.s[2])};
-		if (segment_hits_box(g.dir, g.dist, s2b, s2t)) {
-			if (skip == i + 1) {
-				const int p0 = __float_as_int(hi.w);
-				const int p1 = __float_as_int(__ldg(&cell_hi[i + 1]).w);
-				for (int p = p0; p < p1; p++) {
-					const uint32_t idx = __ldg(&lidx[p]);
-					if (idx & PSG_INVALID_BIT) continue;
-					double dc, r2;
-					if (line_hits_particle(g, __ldg(&lpsml[p]), dc, r2)) {
-						if (FILL) {
-							out_ipar[o] = idx;
-							out_d[o] = dc;
-							out_b[o] = __dsqrt_rn(fabs(r2));
-							o++;
-						}
-						nh++;
+		bool hit = false;
+		if (valid) {
+			const float s2b[3] = {rn_fsub(lo.x, g.s[0]), rn_fsub(lo.y, g.s[1]), rn_fsub(lo.z, g.s[2])};
+			const float s2t[3] = {rn_fsub(hi.x, g.s[0]), rn_fsub(hi.y, g.s[1]), rn_fsub(hi.z, g.s[2])};
+			hit = segment_hits_box(g.dir, g.dist, s2b, s2t);
+		}
+		int m = (valid && !hit) ? skip : 0;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int t = __shfl_up_sync(0xffffffffu, m, o);
+			if (lane >= o) m = max(m, t);
+		}
+		int cover = __shfl_up_sync(0xffffffffu, m, 1);
+		if (lane == 0) cover = 0;
+		const bool live = valid && cover <= j;
+		const bool leaf = live && hit && skip == j + 1;
+		const int ps = __float_as_int(hi.w);
+		int pe = __shfl_down_sync(0xffffffffu, ps, 1);
+		if (lane == 31 && j + 1 <= ncell) pe = __float_as_int(__ldg(&cell_hi[j + 1]).w);
+		const int cnt = leaf ? min(max(pe - ps, 0), ppc) : 0;
+		int c = cnt;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int t = __shfl_up_sync(0xffffffffu, c, o);
+			if (lane >= o) c += t;
+		}
+		const int total = __shfl_sync(0xffffffffu, c, 31);
+		const int base = c - cnt;
+		for (int k = 0; k < cnt; k++) list[base + k] = ps + k;
+		__syncwarp();
+		for (int k0 = 0; k0 < total; k0 += 32) {
+			const int k = k0 + lane;
+			bool acc = false;
+			double dc = 0.0, r2 = 0.0;
+			uint32_t idx = 0;
+			if (k < total) {
+				const int p = list[k];
+				idx = __ldg(&lidx[p]);
+				if (!(idx & PSG_INVALID_BIT)) acc = line_hits_particle(g, __ldg(&lpsml[p]), dc, r2);
+			}
+			const unsigned bal = __ballot_sync(0xffffffffu, acc);
+			if (bal) {
+				const unsigned n = __popc(bal);
+				unsigned long long q0 = 0;
+				if (lane == 0) q0 = atomicAdd(nrec, (unsigned long long)n);
+				q0 = __shfl_sync(0xffffffffu, q0, 0);
+				if (acc) {
+					const unsigned rank = __popc(bal & lt_mask);
+					const unsigned long long q = q0 + rank;
+					if (q < cap) {
+						rec_ipar[q] = idx;
+						rec_ray[q] = (uint32_t)r;
+						rec_pos[q] = nh + rank;
+						rec_d[q] = dc;
+						rec_b[q] = __dsqrt_rn(fabs(r2));
 					}
 				}
+				nh += n;
 			}
-			i++;
-		} else {
-			i = skip;
 		}
+		__syncwarp();
+		i = max(i + 32, __shfl_sync(0xffffffffu, m, 31));
 	}
-	if (!FILL) count[r] = nh;
+	if (lane == 0) count[r] = nh;
+}
+
+// Records into per-ray lists at offsets[ray] + rank: CSR in traversal order.
+__global__ void k_scatter(size_t nrec, const int64_t *__restrict__ off, const uint32_t *__restrict__ rec_ipar,
+		const uint32_t *__restrict__ rec_ray, const uint32_t *__restrict__ rec_pos,
+		const double *__restrict__ rec_d, const double *__restrict__ rec_b, uint32_t *__restrict__ ipar,
+		double *__restrict__ d, double *__restrict__ b) {
+	const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (q >= nrec) return;
+	const int64_t dst = off[rec_ray[q]] + rec_pos[q];
+	ipar[dst] = rec_ipar[q];
+	d[dst] = rec_d[q];
+	b[dst] = rec_b[q];
 }
 
 __global__ void k_offsets64(const uint32_t *__restrict__ scan32, const uint32_t *__restrict__ count,
@@ -182,19 +248,46 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	cudaStream_t st = ctx->stream;
 	uint32_t *count = (uint32_t *)psg_scratch(ctx, S_COUNT, sizeof(uint32_t) * 2 * (nray + 1));
 	char *offmem = (char *)psg_scratch(ctx, S_OFFSETS, (sizeof(int64_t) + sizeof(int32_t)) * (nray + 1) + 256);
+	unsigned long long *d_nrec = ctx->d_counters;
 	if (!count || !offmem) return PSG_E_NOMEM;
 	uint32_t *scan = count + (nray + 1);
 	int64_t *off64 = (int64_t *)offmem;
 	int32_t *off32 = (int32_t *)(offmem + sizeof(int64_t) * (nray + 1));
 	const int ncell = (int)ctx->ncell;
-	PSG_CUDA(cudaMemsetAsync(count + nray, 0, sizeof(uint32_t), st));
-	psg_mark_begin(ctx, PSG_K_TRACE_COUNT);
-	if (nray) ctx->launches++;
-	if (nray)
-		k_trace<false><<<blocks(nray, 128), 128, 0, st>>>(d_rays, nray, ctx->d_cell_lo, ctx->d_cell_hi,
-				ncell, ctx->d_leaf_psml, ctx->d_leaf_idx, count, nullptr, nullptr, nullptr, nullptr);
-	PSG_CHECK_LAUNCH();
-	psg_mark_end(ctx);
+	const int ppc = ctx->ppc;
+	const int wpb = 4;
+	const size_t smem = sizeof(int) * 32 * (size_t)ppc * wpb;
+	if (smem > 48 * 1024)
+		PSG_CUDA(cudaFuncSetAttribute(k_trace_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	// single traversal; if the record buffer was too small, grow it and rerun
+	size_t nrec = 0, cap = 0;
+	for (int attempt = 0; attempt < 2; attempt++) {
+		cap = ctx->rec_cap ? ctx->rec_cap : nray * 64 + 1024;
+		uint32_t *rec_u32 = (uint32_t *)psg_scratch(ctx, S_REC_U32, sizeof(uint32_t) * 3 * cap);
+		double *rec_f64 = (double *)psg_scratch(ctx, S_REC_F64, sizeof(double) * 2 * cap);
+		if (!rec_u32 || !rec_f64) return PSG_E_NOMEM;
+		PSG_CUDA(cudaMemsetAsync(d_nrec, 0, sizeof(unsigned long long), st));
+		PSG_CUDA(cudaMemsetAsync(count + nray, 0, sizeof(uint32_t), st));
+		psg_mark_begin(ctx, PSG_K_TRACE_FILL);
+		if (nray) {
+			k_trace_warp<<<blocks(nray, wpb), 32 * wpb, smem, st>>>(d_rays, nray, ctx->d_cell_lo,
+					ctx->d_cell_hi, ncell, ctx->d_leaf_psml, ctx->d_leaf_idx, ppc, count, d_nrec, cap,
+					rec_u32, rec_u32 + cap, rec_u32 + 2 * cap, rec_f64, rec_f64 + cap);
+			ctx->launches++;
+		}
+		PSG_CHECK_LAUNCH();
+		psg_mark_end(ctx);
+		unsigned long long got = 0;
+		PSG_CUDA(cudaMemcpyAsync(&got, d_nrec, sizeof(got), cudaMemcpyDeviceToHost, st));
+		PSG_CUDA(cudaStreamSynchronize(st));
+		nrec = (size_t)got;
+		if (nrec <= cap) break;
+		ctx->rec_cap = nrec + nrec / 8 + 1024;
+		if (attempt == 1) return psg_fail(ctx, PSG_E_OVERFLOW, "trace: hit records grew between passes");
+	}
+	if (nrec >= (size_t)INT32_MAX)
+		return psg_fail(ctx, PSG_E_OVERFLOW, "trace: %zu hits in one batch exceed 2^31", nrec);
+	if (!ctx->rec_cap || nrec > ctx->rec_cap) ctx->rec_cap = nrec + nrec / 8 + 1024;
 	size_t tmp = 0;
 	PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, count, scan, (int)(nray + 1), st));
 	void *dt = psg_scratch(ctx, S_CUB, tmp);
@@ -203,12 +296,7 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32);
 	PSG_CHECK_LAUNCH();
 	ctx->launches++;
-	uint32_t total32 = 0;
-	PSG_CUDA(cudaMemcpyAsync(&total32, scan + nray, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-	PSG_CUDA(cudaStreamSynchronize(st));
-	const size_t nhit = total32;
-	if (nhit >= (size_t)INT32_MAX)
-		return psg_fail(ctx, PSG_E_OVERFLOW, "trace: %zu hits in one batch exceed 2^31", nhit);
+	const size_t nhit = nrec;
 	const size_t hb = nhit ? nhit : 1;
 	uint32_t *raw_ipar = (uint32_t *)psg_scratch(ctx, S_RAW_IPAR, sizeof(uint32_t) * hb);
 	double *raw_d = (double *)psg_scratch(ctx, S_RAW_D, sizeof(double) * 2 * hb);
@@ -219,16 +307,15 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	double *hit_b = (double *)psg_scratch(ctx, S_HIT_KERN, sizeof(double) * hb);
 	if (!raw_ipar || !raw_d || !raw_b || !keys || !vals || !hit_ipar || !hit_b) return PSG_E_NOMEM;
 	double *hit_d = raw_d + hb;
-	psg_mark_begin(ctx, PSG_K_TRACE_FILL);
-	if (nray) ctx->launches++;
-	if (nray)
-		k_trace<true><<<blocks(nray, 128), 128, 0, st>>>(d_rays, nray, ctx->d_cell_lo, ctx->d_cell_hi,
-				ncell, ctx->d_leaf_psml, ctx->d_leaf_idx, nullptr, off64, raw_ipar, raw_d, raw_b);
-	PSG_CHECK_LAUNCH();
-	psg_mark_end(ctx);
 	if (nhit) {
 		psg_mark_begin(ctx, PSG_K_SORT);
-		ctx->launches += 3;
+		uint32_t *rec_u32 = (uint32_t *)ctx->scratch[S_REC_U32].p;
+		double *rec_f64 = (double *)ctx->scratch[S_REC_F64].p;
+		const size_t c = cap;     // the layout the traversal wrote with
+		k_scatter<<<blocks(nhit, 256), 256, 0, st>>>(nhit, off64, rec_u32, rec_u32 + c, rec_u32 + 2 * c,
+				rec_f64, rec_f64 + c, raw_ipar, raw_d, raw_b);
+		PSG_CHECK_LAUNCH();
+		ctx->launches += 4;
 		k_sort_keys<<<blocks(nhit, 256), 256, 0, st>>>(nhit, raw_d, keys, vals);
 		PSG_CHECK_LAUNCH();
 		size_t stmp = 0;

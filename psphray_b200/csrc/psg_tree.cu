@@ -242,7 +242,7 @@ inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs);
 extern "C" int psg_build_tree(psg_context *ctx, int ppc) {
 	if (!ctx) return PSG_E_INVAL;
 	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_build_tree: no particles loaded");
-	if (ppc < 1) return psg_fail(ctx, PSG_E_INVAL, "psg_build_tree: ppc must be >= 1");
+	if (ppc < 1 || ppc > 255) return psg_fail(ctx, PSG_E_INVAL, "psg_build_tree: ppc must be in 1..255");
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	cudaStream_t st = ctx->stream;
 	const size_t n = ctx->n;
@@ -387,6 +387,7 @@ extern "C" int psg_build_tree(psg_context *ctx, int ppc) {
 	ctx->nvalid = nvalid;
 	ctx->skipped = n - nvalid;
 	ctx->depth = nlevels - 1;
+	ctx->ppc = ppc;
 	ctx->have_tree = 1;
 	return PSG_OK;
 }
