@@ -50,31 +50,49 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    """nvidia-smi sampled every 100 ms on a reader thread; start() returns once
+    the first sample has arrived so the samples cover the timed region."""
 
     def __init__(self, device: int):
         self.proc = None
         self.device = device
+        self.lines = []
+        self.t_start = None
 
     def start(self):
+        import threading
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return
+
+        def reader():
+            for line in self.proc.stdout:
+                self.lines.append((time.time(), line))
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 5:
+            time.sleep(0.01)
+        self.t_start = time.time()
 
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t_end = time.time()
+        time.sleep(0.15)
         self.proc.terminate()
-        out, _ = self.proc.communicate(timeout=10)
+        self.thread.join(timeout=5)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        window = [l for t, l in self.lines if self.t_start - 0.1 <= t <= t_end + 0.1] or [l for _, l in self.lines]
+        for line in window:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -181,7 +199,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="iliev64")
     ap.add_argument("--ticks", type=int, default=0, help="ticks per step (default per workload)")
@@ -229,7 +247,8 @@ def main():
         dist.barrier()
     torch.cuda.synchronize(dev)
     clocks.start()
-    total_ms, hits, launches = 0.0, 0.0, 0.0
+    total_ms, hits, launches, sat = 0.0, 0.0, 0.0, 0.0
+    per_step = []
     kms = {k: 0.0 for k in api.KERNELS}
     kn = {k: 0.0 for k in api.KERNELS}
     for s in range(args.warmup, nsteps):
@@ -241,6 +260,8 @@ def main():
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
         hits += st["hits"]
+        sat += st["saturated"]
+        per_step.append(round(e0.elapsed_time(e1), 3))
         launches += st["launches"]
         for k in api.KERNELS:
             kms[k] += st["kernel_ms"][k]
@@ -307,6 +328,8 @@ def main():
                        "parallelism": f"replicas{world}"},
             "gpu_s_per_sim_myr": t_max / sim_myr,
             "gpu_launches": launches,
+            "saturated_deposits_per_step": sat / args.steps,
+            "step_ms": per_step,
             "kernel_ms_per_step": {k: kms[k] / args.steps for k in api.KERNELS},
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,

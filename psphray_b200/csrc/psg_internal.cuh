@@ -12,6 +12,9 @@
 #define PSG_MAX_LEVELS 21
 #define PSG_KEY_OUTSIDE 0xFFFFFFFFFFFFFFFFull
 #define PSG_INVALID_BIT 0x80000000u
+// Longest hit list sorted in shared memory (16 bytes per hit); longer lists
+// take the library segmented sort.
+#define PSG_SORT_MAX 8192
 
 // Bits of the device status word.
 #define PSG_ST_NAN 1u          // NaN/inf reached a particle state
@@ -66,7 +69,7 @@ struct psg_context {
 
 	// scratch, grown on demand
 	psg_buf scratch[20];
-	size_t rec_cap = 0;   // capacity of the traversal's hit-record buffer
+	size_t slab_cap = 0;  // hits each ray can hold in the traversal's output slabs
 	int ppc = 8;          // leaf capacity of the current tree
 	cudaEvent_t ev[8] = {};
 	int timing = 0;
@@ -92,7 +95,7 @@ void *psg_scratch(psg_context *ctx, int slot, size_t bytes);
 // scratch slots
 enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
-	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64
+	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST
 };
 
 // Per-launch timing: mark_begin/mark_end bracket a group of launches of one

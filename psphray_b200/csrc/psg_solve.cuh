@@ -33,6 +33,8 @@ struct PhysParams {
 	int isothermal, on_the_spot, adiabatic;
 };
 
+PhysParams psg_phys_params(const psg_context *ctx);
+
 // tabfun_get() tabfun.c:38-58
 __device__ __forceinline__ double tab_get(int nrows, double min, double step_inv,
 		const double *__restrict__ x, const double *__restrict__ y, double v) {

@@ -22,11 +22,7 @@
 #include "psg_internal.cuh"
 #include "psg_solve.cuh"
 
-namespace {
-
-inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
-
-PhysParams phys_params(const psg_context *ctx) {
+PhysParams psg_phys_params(const psg_context *ctx) {
 	PhysParams P{};
 	P.ar = ctx->d_ar;
 	P.ar_nrows = ctx->ar_nrows;
@@ -53,63 +49,63 @@ PhysParams phys_params(const psg_context *ctx) {
 	return P;
 }
 
-// Column-density factor of each hit, kernel = sph_depth(b/h) / h^2
-// (loop.c:429-445), computed once per batch; b is overwritten.
-__global__ void k_hit_kernel(size_t nhit, const uint32_t *__restrict__ ipar, const float4 *__restrict__ psml,
-		double *__restrict__ b_to_kern, PhysParams P) {
-	const size_t h = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (h >= nhit) return;
-	const double sml = (double)psml[ipar[h]].w;
-	const double sml_inv = __ddiv_rn(1.0, sml);
-	const double r_h = rn_dmul(b_to_kern[h], sml_inv);
-	b_to_kern[h] = rn_dmul(sph_depth(P, r_h), rn_dmul(sml_inv, sml_inv));
-}
+namespace {
 
-// (tick, ipar) keys for the by-particle order; one warp per ray.
-__global__ void k_slot_keys(size_t nray, int nray_per_tick, const int64_t *__restrict__ off,
-		const uint32_t *__restrict__ ipar, unsigned long long *__restrict__ keys,
-		uint32_t *__restrict__ vals) {
+inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+
+// (tick, ipar) keys for the by-particle order, tick in the bits above
+// `shift`; one warp per ray. KT is 32-bit whenever both fit.
+template <typename KT>
+__global__ void k_slot_keys(size_t nray, int nray_per_tick, int shift, const int64_t *__restrict__ off,
+		const uint32_t *__restrict__ ipar, KT *__restrict__ keys, uint32_t *__restrict__ vals) {
 	const size_t r = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32;
 	const int lane = threadIdx.x & 31;
 	if (r >= nray) return;
-	const unsigned long long t = (unsigned long long)(r / (size_t)nray_per_tick);
+	const KT t = (KT)(r / (size_t)nray_per_tick);
 	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32) {
-		keys[h] = (t << 32) | ipar[h];
+		keys[h] = (t << shift) | (KT)ipar[h];
 		vals[h] = (uint32_t)h;
 	}
 }
 
-__global__ void k_slots(size_t nhit, const unsigned long long *__restrict__ skeys,
-		const uint32_t *__restrict__ svals, uint32_t *__restrict__ slot, int32_t *__restrict__ head) {
+template <typename KT>
+__global__ void k_slots(size_t nhit, const KT *__restrict__ skeys, const uint32_t *__restrict__ svals,
+		uint32_t *__restrict__ slot, int32_t *__restrict__ head) {
 	const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (k >= nhit) return;
 	slot[svals[k]] = (uint32_t)k;
 	head[k] = (k == 0 || skeys[k] != skeys[k - 1]) ? 1 : 0;
 }
 
-__global__ void k_active(size_t nhit, const unsigned long long *__restrict__ skeys,
-		const int32_t *__restrict__ head, const int32_t *__restrict__ scan,
-		uint32_t *__restrict__ act_ipar, uint32_t *__restrict__ act_seg,
-		unsigned long long *__restrict__ act_key) {
+template <typename KT>
+__global__ void k_active(size_t nhit, int shift, const KT *__restrict__ skeys, const int32_t *__restrict__ head,
+		const int32_t *__restrict__ scan, uint32_t *__restrict__ act_ipar, uint32_t *__restrict__ act_seg,
+		KT *__restrict__ act_key) {
 	const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (k >= nhit) return;
 	if (!head[k]) return;
 	const int a = scan[k];
-	act_ipar[a] = (uint32_t)(skeys[k] & 0xFFFFFFFFull);
+	act_ipar[a] = (uint32_t)(skeys[k] & (((KT)1 << shift) - 1));
 	act_seg[a] = (uint32_t)k;
 	act_key[a] = skeys[k];
 }
 
 // first active entry of every tick (and the total at index nticks)
-__global__ void k_tick_bounds(int nticks, const unsigned long long *__restrict__ act_key, int nact,
+template <typename KT>
+__global__ void k_tick_bounds(int nticks, int shift, const KT *__restrict__ act_key, int nact,
 		uint32_t *__restrict__ act_seg, uint32_t nhit, int32_t *__restrict__ tick_act) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t > nticks) return;
-	const unsigned long long want = (unsigned long long)t << 32;
 	int lo = 0, hi = nact;
-	while (lo < hi) {
-		const int mid = (lo + hi) / 2;
-		if (act_key[mid] < want) lo = mid + 1; else hi = mid;
+	if (t < nticks) {
+		const KT want = (KT)t << shift;
+		while (lo < hi) {
+			const int mid = (lo + hi) / 2;
+			if (act_key[mid] < want) lo = mid + 1; else hi = mid;
+		}
+	} else {
+		lo = nact;
 	}
 	tick_act[t] = lo;
 	if (t == nticks) act_seg[nact] = nhit;
@@ -128,108 +124,200 @@ __device__ __forceinline__ bool below_cutoff(double TM, double Nph) {
 	return TM < 0.0 || __ddiv_rn(TM, Nph) < 1e-10;
 }
 
-// One block of DEP_THREADS per ray; hits are taken DEP_THREADS at a time.
-// Within a chunk, optical depths are summed with a block-wide FP64 scan; the
-// first hit whose absorption exceeds its neutral atoms (loop.c:482-485) or
-// after which TM/Nph < 1e-10 (loop.c:585) is found with a block min, settled
-// by its own thread, and the scan restarts after it.
-#define DEP_THREADS 256
-#define DEP_WARPS (DEP_THREADS / 32)
+// Deposit of one ray by a group of NT threads (a warp, or a whole block):
+// hits are taken NT at a time; optical depths are summed with an FP64 scan
+// over the group; the first hit whose absorption exceeds its neutral atoms
+// (loop.c:482-485) or after which TM/Nph < 1e-10 (loop.c:585) is found with
+// a group min, settled by its own thread, and the scan restarts after it.
+// Transmitted photons before hit j are TM*exp(-(sum of earlier tau)); after
+// it, TM_j minus the absorbed photons, as loop.c:580 updates TM. Each hit
+// writes photons/NH to its slot, or -1 where the reference deposits nothing.
+struct DepShared {
+	double wsum[32];
+	double tm;
+	int first;
+};
 
-__global__ void __launch_bounds__(DEP_THREADS) k_deposit(const psg_ray *__restrict__ rays, size_t ray0, int nray,
-		const int64_t *__restrict__ off, const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
-		const uint32_t *__restrict__ slot, const double *__restrict__ lambdaH, const float *__restrict__ mass,
-		PhysParams P, int want_heat, double *__restrict__ acc, double *__restrict__ acc_heat,
-		unsigned long long *__restrict__ n_sat, double *__restrict__ lost) {
-	__shared__ double s_wsum[DEP_WARPS];
-	__shared__ int s_first;
-	__shared__ double s_tm;
-	const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-	const size_t r = ray0 + blockIdx.x;
-	if (blockIdx.x >= (unsigned)nray) return;
-	const int64_t h0 = off[r], h1 = off[r + 1];
-	if (h1 == h0) return;
-	const double Nph = rays[r].Nph;
-	const double freq = rays[r].freq;
+template <int NT>
+__device__ __forceinline__ void group_sync() {
+	if (NT == 32) __syncwarp(); else __syncthreads();
+}
+
+template <int NT>
+__device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
+		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern, const uint32_t *__restrict__ slot,
+		const double *__restrict__ lambdaH, const float *__restrict__ mass, const PhysParams &P, int want_heat,
+		double *__restrict__ acc, double *__restrict__ acc_heat, DepShared &sh, unsigned &nsat, double &lost) {
+	const int lane = t & 31, wid = t >> 5;
+	constexpr int NW = NT / 32;
+	const double Nph = ray.Nph;
+	const double freq = ray.freq;
 	const bool skip_ray = (Nph == 0.0);
 	const double sigma = xs_get_HI(P, freq);
 	const double heat_factor = rn_dmul(P.H_PER_MASS, fdim(freq, P.HI_ENERGY));
 	double TM = Nph;
 	bool done = skip_ray;
-	unsigned nsat = 0;
-	for (int64_t base = h0; base < h1; base += DEP_THREADS) {
-		const int64_t h = base + tid;
+	// the next step's loads are issued one step ahead
+	uint32_t np_slot = 0;
+	double np_kern = 0.0, np_lam = 0.0;
+	float np_mass = 1.0f;
+	{
+		const int64_t h = h0 + t;
+		if (h < h1) {
+			const uint32_t p = hipar[h];
+			np_kern = hkern[h];
+			np_slot = slot[h];
+			if (!done) { np_lam = lambdaH[p]; np_mass = mass[p]; }
+		}
+	}
+	for (int64_t base = h0; base < h1; base += NT) {
+		const int64_t h = base + t;
 		const bool valid = h < h1;
+		const double kern_c = np_kern, lam_c = np_lam;
+		const float mass_c = np_mass;
+		const uint32_t slot_c = np_slot;
+		{
+			const int64_t hn = h + NT;
+			if (hn < h1) {
+				const uint32_t p = hipar[hn];
+				np_kern = hkern[hn];
+				np_slot = slot[hn];
+				if (!done) { np_lam = lambdaH[p]; np_mass = mass[p]; }
+			}
+		}
 		double tau = 0.0, NHI = 0.0, NH_inv = 0.0, delta = -1.0;
 		if (valid && !done) {
-			const uint32_t p = hipar[h];
-			const double NH = rn_dmul((double)mass[p], P.H_PER_MASS);
-			NHI = rn_dmul(lambdaH[p], NH);
-			tau = rn_dmul(sigma, rn_dmul(hkern[h], NHI));
+			const double NH = rn_dmul((double)mass_c, P.H_PER_MASS);
+			NHI = rn_dmul(lam_c, NH);
+			tau = rn_dmul(sigma, rn_dmul(kern_c, NHI));
 			NH_inv = __ddiv_rn(1.0, NH);
 		}
 		int start = 0;
-		while (!done && start < DEP_THREADS) {
-			const bool part = valid && tid >= start && tau != 0.0;
+		while (!done && start < NT) {
+			const bool part = valid && t >= start && tau != 0.0;
 			const double my_tau = part ? tau : 0.0;
-			// block scan: warp scan, then the warp totals
 			double wi = my_tau;
 #pragma unroll
 			for (int o = 1; o < 32; o <<= 1) {
-				const double u = __shfl_up_sync(0xffffffffu, wi, o);
-				if (lane >= o) wi += u;
+				const double v = __shfl_up_sync(0xffffffffu, wi, o);
+				if (lane >= o) wi += v;
 			}
-			double we = __shfl_up_sync(0xffffffffu, wi, 1);
-			if (lane == 0) we = 0.0;
-			if (lane == 31) s_wsum[wid] = wi;
-			if (tid == 0) s_first = DEP_THREADS;
-			__syncthreads();
-			double woff = 0.0, total = 0.0;
-			for (int k = 0; k < DEP_WARPS; k++) {
-				const double v = s_wsum[k];
-				if (k < wid) woff += v;
-				total += v;
+			double woff = 0.0, total;
+			if (NW == 1) {
+				total = __shfl_sync(0xffffffffu, wi, 31);
+			} else {
+				if (lane == 31) sh.wsum[wid] = wi;
+				if (t == 0) sh.first = NT;
+				group_sync<NT>();
+				total = 0.0;
+#pragma unroll
+				for (int k = 0; k < NW; k++) {
+					const double v = sh.wsum[k];
+					if (k < wid) woff += v;
+					total += v;
+				}
 			}
-			const double incl = woff + wi, excl = woff + we;
-			const double TMj = TM * exp(-excl);
-			double absorb = TMj * -expm1(-my_tau);
-			const double TMafter = TM * exp(-incl);
-			const bool capped = part && absorb > NHI;
-			const bool cut = part && below_cutoff(TMafter, Nph);
-			if (capped || cut) atomicMin(&s_first, tid);
-			__syncthreads();
-			const int f = s_first;
-			if (part && tid < f) delta = rn_dmul(absorb, NH_inv);
-			if (f == DEP_THREADS) {
+			double TMj = 0.0, absorb = 0.0, TMafter = 0.0;
+			bool capped = false, cut = false;
+			if (part) {
+				const double excl = (woff + wi) - my_tau;
+				TMj = TM * exp(-excl);
+				absorb = TMj * -expm1(-my_tau);
+				TMafter = TMj - absorb;
+				capped = absorb > NHI;
+				cut = below_cutoff(TMafter, Nph);
+			}
+			int f;
+			if (NW == 1) {
+				const unsigned ev = __ballot_sync(0xffffffffu, capped || cut);
+				f = ev ? __ffs(ev) - 1 : NT;
+			} else {
+				if (capped || cut) atomicMin(&sh.first, t);
+				group_sync<NT>();
+				f = sh.first;
+			}
+			if (part && t < f) delta = rn_dmul(absorb, NH_inv);
+			if (f == NT) {
 				TM = TM * exp(-total);
-				__syncthreads();     // s_wsum / s_first are rewritten by the next chunk
+				group_sync<NT>();       // shared words are rewritten by the next step
 				break;
 			}
-			if (tid == f) {
-				double TMnew = TMafter;
+			double TMnew = 0.0;
+			if (t == f) {
+				TMnew = TMafter;
 				if (capped) {
 					absorb = NHI;
 					TMnew = TMj - NHI;
 					nsat++;
 				}
 				delta = rn_dmul(absorb, NH_inv);
-				s_tm = TMnew;
+				if (NW > 1) sh.tm = TMnew;
 			}
-			__syncthreads();
-			TM = s_tm;
+			if (NW == 1) {
+				TM = __shfl_sync(0xffffffffu, TMnew, f);
+			} else {
+				group_sync<NT>();
+				TM = sh.tm;
+			}
 			if (below_cutoff(TM, Nph)) done = true;
 			start = f + 1;
-			__syncthreads();
+			group_sync<NT>();
 		}
 		if (valid) {
-			const uint32_t sl = slot[h];
-			acc[sl] = delta;
-			if (want_heat) acc_heat[sl] = delta >= 0.0 ? rn_dmul(heat_factor, delta) : 0.0;
+			acc[slot_c] = delta;
+			if (want_heat) acc_heat[slot_c] = delta >= 0.0 ? rn_dmul(heat_factor, delta) : 0.0;
+		}
+	}
+	if (t == 0 && !skip_ray) lost += TM;
+}
+
+// Blocks [0, nlong) take one long ray each with all DEP_THREADS threads; the
+// remaining blocks take DEP_THREADS/32 short rays, one per warp.
+#define DEP_THREADS 512
+#define DEP_LONG 96
+
+__global__ void __launch_bounds__(DEP_THREADS) k_deposit(const psg_ray *__restrict__ rays,
+		const uint32_t *__restrict__ long_rays, int nlong, const uint32_t *__restrict__ short_rays, int nshort,
+		const int64_t *__restrict__ off, const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
+		const uint32_t *__restrict__ slot, const double *__restrict__ lambdaH, const float *__restrict__ mass,
+		PhysParams P, int want_heat, double *__restrict__ acc, double *__restrict__ acc_heat,
+		unsigned long long *__restrict__ n_sat, double *__restrict__ lost) {
+	__shared__ DepShared sh_block;
+	__shared__ DepShared sh_warp[DEP_THREADS / 32];
+	const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+	unsigned nsat = 0;
+	double tm_lost = 0.0;
+	if ((int)blockIdx.x < nlong) {
+		const uint32_t r = long_rays[blockIdx.x];
+		deposit_ray<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P, want_heat,
+				acc, acc_heat, sh_block, nsat, tm_lost);
+	} else {
+		const int w = ((int)blockIdx.x - nlong) * (DEP_THREADS / 32) + wid;
+		if (w < nshort) {
+			const uint32_t r = short_rays[w];
+			if (off[r + 1] > off[r])
+				deposit_ray<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P, want_heat,
+						acc, acc_heat, sh_warp[wid], nsat, tm_lost);
 		}
 	}
 	for (int o = 16; o > 0; o >>= 1) nsat += __shfl_down_sync(0xffffffffu, nsat, o);
 	if (lane == 0 && nsat) atomicAdd(n_sat, (unsigned long long)nsat);
-	if (tid == 0 && !skip_ray) atomicAdd(lost, TM);
+	if (lane == 0 && tm_lost != 0.0) atomicAdd(lost, tm_lost);
+}
+
+// Rays of the batch split into long and short lists (ray order kept).
+__global__ void k_ray_class(size_t nray, const int64_t *__restrict__ off, int32_t *__restrict__ is_long) {
+	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (r >= nray) return;
+	is_long[r] = (off[r + 1] - off[r]) > DEP_LONG ? 1 : 0;
+}
+
+__global__ void k_ray_lists(size_t nray, const int32_t *__restrict__ is_long, const int32_t *__restrict__ scan,
+		uint32_t *__restrict__ long_rays, uint32_t *__restrict__ short_rays) {
+	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (r >= nray) return;
+	if (is_long[r]) long_rays[scan[r]] = (uint32_t)r;
+	else short_rays[r - scan[r]] = (uint32_t)r;
 }
 
 // update_pars() loop.c:653-770 for the particles hit in tick t, one thread
@@ -274,7 +362,22 @@ __global__ void __launch_bounds__(256) k_update(int t, const int32_t *__restrict
 		const uint32_t b0 = __shfl_sync(0xffffffffu, s0, l), b1 = __shfl_sync(0xffffffffu, s1, l);
 		double sg = 0.0, sh = 0.0;
 		int sn = 0;
-		for (uint32_t k = b0 + lane; k < b1; k += 32) {
+		// eight independent loads in flight per lane and round
+		uint32_t k = b0 + lane;
+		for (; k + 7 * 32 < b1; k += 8 * 32) {
+			double v[8];
+#pragma unroll
+			for (int u = 0; u < 8; u++) v[u] = acc[k + 32 * u];
+#pragma unroll
+			for (int u = 0; u < 8; u++) {
+				if (v[u] >= 0.0) {
+					sg += v[u];
+					if (want_heat) sh += acc_heat[k + 32 * u];
+					sn++;
+				}
+			}
+		}
+		for (; k < b1; k += 32) {
 			const double d = acc[k];
 			if (d >= 0.0) {
 				sg += d;
@@ -340,6 +443,62 @@ static int check_status(psg_context *ctx) {
 	return PSG_OK;
 }
 
+// The per-batch by-particle order: sort (tick, ipar) keys of all hits,
+// give every hit its slot, list the distinct (tick, particle) pairs with the
+// first slot of each, and the first pair of every tick. Layout of S_ACT:
+// head, scan, act_ipar, act_seg (hb+1 each), tick_act (K+1, 16-aligned),
+// act_key (hb+1, 16-aligned).
+template <typename KT>
+static int build_slots(psg_context *ctx, size_t nray, size_t R, size_t K, size_t nhit, int shift, int tbits,
+		const int64_t *off64, const uint32_t *hit_ipar, int want_heat, int *nact_out) {
+	cudaStream_t st = ctx->stream;
+	const size_t hb = nhit ? nhit : 1;
+	KT *keys = (KT *)psg_scratch(ctx, S_KEYS, sizeof(KT) * 2 * hb);
+	uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
+	uint32_t *slot = (uint32_t *)psg_scratch(ctx, S_SLOT, sizeof(uint32_t) * hb);
+	double *acc = (double *)psg_scratch(ctx, S_ACC, sizeof(double) * hb * (want_heat ? 2 : 1));
+	char *actm = (char *)psg_scratch(ctx, S_ACT, sizeof(int32_t) * 4 * (hb + 1) + sizeof(int32_t) * (K + 2)
+			+ sizeof(KT) * (hb + 1) + 1024);
+	if (!keys || !vals || !slot || !acc || !actm) return PSG_E_NOMEM;
+	int32_t *head = (int32_t *)actm;
+	int32_t *hscan = head + (hb + 1);
+	uint32_t *act_ipar = (uint32_t *)(hscan + (hb + 1));
+	uint32_t *act_seg = act_ipar + (hb + 1);
+	int32_t *tick_act = (int32_t *)(((uintptr_t)(act_seg + hb + 1) + 15) & ~(uintptr_t)15);
+	KT *act_key = (KT *)(((uintptr_t)(tick_act + K + 1) + 15) & ~(uintptr_t)15);
+	int nact = 0;
+	if (nhit) {
+		k_slot_keys<KT><<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, shift, off64, hit_ipar, keys, vals);
+		PSG_CHECK_LAUNCH();
+		const int endbit = shift + tbits;
+		size_t tmp = 0;
+		PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, keys + hb, vals, vals + hb, (int64_t)nhit, 0, endbit, st));
+		void *dt = psg_scratch(ctx, S_CUB, tmp);
+		if (!dt) return PSG_E_NOMEM;
+		PSG_CUDA(cub::DeviceRadixSort::SortPairs(dt, tmp, keys, keys + hb, vals, vals + hb, (int64_t)nhit, 0, endbit, st));
+		k_slots<KT><<<blocks(nhit, 256), 256, 0, st>>>(nhit, keys + hb, vals + hb, slot, head);
+		PSG_CHECK_LAUNCH();
+		tmp = 0;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, head, hscan, (int)nhit, st));
+		dt = psg_scratch(ctx, S_CUB, tmp);
+		if (!dt) return PSG_E_NOMEM;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, head, hscan, (int)nhit, st));
+		k_active<KT><<<blocks(nhit, 256), 256, 0, st>>>(nhit, shift, keys + hb, head, hscan, act_ipar, act_seg, act_key);
+		PSG_CHECK_LAUNCH();
+		ctx->launches += 3;
+		int last_scan = 0, last_head = 0;
+		PSG_CUDA(cudaMemcpyAsync(&last_scan, hscan + nhit - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+		PSG_CUDA(cudaMemcpyAsync(&last_head, head + nhit - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+		PSG_CUDA(cudaStreamSynchronize(st));
+		nact = last_scan + last_head;
+	}
+	k_tick_bounds<KT><<<blocks(K + 1, 128), 128, 0, st>>>((int)K, shift, act_key, nact, act_seg, (uint32_t)nhit, tick_act);
+	PSG_CHECK_LAUNCH();
+	ctx->launches++;
+	*nact_out = nact;
+	return PSG_OK;
+}
+
 extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K,
 		int64_t first_tick, double tick_time, psg_tick_stats *stats) {
 	if (!ctx) return PSG_E_INVAL;
@@ -351,13 +510,13 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	cudaStream_t st = ctx->stream;
 	const size_t nray = R * K;
-	const PhysParams P = phys_params(ctx);
+	const PhysParams P = psg_phys_params(ctx);
 	const int want_heat = !ctx->flags.isothermal;
 
 	ctx->nkev = 0;
 	ctx->launches = 0;
 	PSG_CUDA(cudaEventRecord(ctx->ev[0], st));
-	int rc = psg_trace_internal(ctx, d_rays, nray, 0);
+	int rc = psg_trace_internal(ctx, d_rays, nray, 1);
 	if (rc) return rc;
 	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
 	int64_t nhit64 = 0;
@@ -368,71 +527,69 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	uint32_t *hit_ipar = (uint32_t *)ctx->scratch[S_HIT_IPAR].p;
 	double *hit_kern = (double *)ctx->scratch[S_HIT_KERN].p;
 	psg_mark_begin(ctx, PSG_K_SLOTS);
-	if (nhit) {
-		k_hit_kernel<<<blocks(nhit, 256), 256, 0, st>>>(nhit, hit_ipar, ctx->d_psml, hit_kern, P);
-		PSG_CHECK_LAUNCH();
-		ctx->launches++;
-	}
-
 	// by-particle order of all hits
-	unsigned long long *keys = (unsigned long long *)psg_scratch(ctx, S_KEYS, sizeof(unsigned long long) * 2 * hb);
-	uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
-	uint32_t *slot = (uint32_t *)psg_scratch(ctx, S_SLOT, sizeof(uint32_t) * hb);
-	double *acc = (double *)psg_scratch(ctx, S_ACC, sizeof(double) * hb * (want_heat ? 2 : 1));
-	char *actm = (char *)psg_scratch(ctx, S_ACT, (sizeof(int32_t) * 2 + sizeof(uint32_t) * 2 + 8) * (hb + 1)
-			+ sizeof(int32_t) * (K + 2) + 1024);
-	if (!keys || !vals || !slot || !acc || !actm) return PSG_E_NOMEM;
+	int shift = 1;
+	while (shift < 32 && (1ull << shift) < (unsigned long long)ctx->n) shift++;
+	int tbits = 0;
+	while ((1ull << tbits) < (unsigned long long)K) tbits++;
+	int nact = 0;
+	int rc2 = (shift + tbits <= 32) ? build_slots<uint32_t>(ctx, nray, R, K, nhit, shift, tbits, off64, hit_ipar,
+			want_heat, &nact)
+		: build_slots<unsigned long long>(ctx, nray, R, K, nhit, shift, tbits, off64, hit_ipar, want_heat, &nact);
+	if (rc2) return rc2;
+	double *acc = (double *)ctx->scratch[S_ACC].p;
 	double *acc_heat = want_heat ? acc + hb : nullptr;
+	uint32_t *slot = (uint32_t *)ctx->scratch[S_SLOT].p;
+	char *actm = (char *)ctx->scratch[S_ACT].p;
 	int32_t *head = (int32_t *)actm;
 	int32_t *hscan = head + (hb + 1);
 	uint32_t *act_ipar = (uint32_t *)(hscan + (hb + 1));
 	uint32_t *act_seg = act_ipar + (hb + 1);
-	unsigned long long *act_key = (unsigned long long *)(((uintptr_t)(act_seg + hb + 1) + 15) & ~(uintptr_t)15);
-	int32_t *tick_act = (int32_t *)(act_key + hb + 1);
-	int nact = 0;
-	if (nhit) {
-		k_slot_keys<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, off64, hit_ipar, keys, vals);
-		PSG_CHECK_LAUNCH();
-		int endbit = 32;
-		while ((1ull << (endbit - 32)) < (unsigned long long)K) endbit++;
-		size_t tmp = 0;
-		PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, keys + hb, vals, vals + hb, (int64_t)nhit, 0, endbit, st));
-		void *dt = psg_scratch(ctx, S_CUB, tmp);
-		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceRadixSort::SortPairs(dt, tmp, keys, keys + hb, vals, vals + hb, (int64_t)nhit, 0, endbit, st));
-		k_slots<<<blocks(nhit, 256), 256, 0, st>>>(nhit, keys + hb, vals + hb, slot, head);
-		PSG_CHECK_LAUNCH();
-		tmp = 0;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, head, hscan, (int)nhit, st));
-		dt = psg_scratch(ctx, S_CUB, tmp);
-		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, head, hscan, (int)nhit, st));
-		k_active<<<blocks(nhit, 256), 256, 0, st>>>(nhit, keys + hb, head, hscan, act_ipar, act_seg, act_key);
-		PSG_CHECK_LAUNCH();
-		ctx->launches += 3;
-		int last_scan = 0, last_head = 0;
-		PSG_CUDA(cudaMemcpyAsync(&last_scan, hscan + nhit - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-		PSG_CUDA(cudaMemcpyAsync(&last_head, head + nhit - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-		PSG_CUDA(cudaStreamSynchronize(st));
-		nact = last_scan + last_head;
-	}
-	k_tick_bounds<<<blocks(K + 1, 128), 128, 0, st>>>((int)K, act_key, nact, act_seg, (uint32_t)nhit, tick_act);
-	PSG_CHECK_LAUNCH();
-	ctx->launches++;
-	psg_mark_end(ctx);
+	int32_t *tick_act = (int32_t *)(((uintptr_t)(act_seg + hb + 1) + 15) & ~(uintptr_t)15);
+	(void)head;
 	unsigned long long *d_nsat = ctx->d_counters + 1;
 	double *d_lost = (double *)(ctx->d_counters + 2);
 	PSG_CUDA(cudaMemsetAsync(d_nsat, 0, 16, st));
+	psg_mark_end(ctx);
 	PSG_CUDA(cudaEventRecord(ctx->ev[1], st));
 
 	// the tick loop
 	std::vector<int32_t> h_tick_act(K + 1);
 	PSG_CUDA(cudaMemcpyAsync(h_tick_act.data(), tick_act, sizeof(int32_t) * (K + 1), cudaMemcpyDeviceToHost, st));
+	// long / short ray lists of the batch (ray order, so each tick's rays are a run)
+	int32_t *is_long = (int32_t *)psg_scratch(ctx, S_COUNT, sizeof(int32_t) * 2 * (nray + 1));
+	uint32_t *ray_lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * (nray + 1));
+	if (!is_long || !ray_lists) return PSG_E_NOMEM;
+	int32_t *long_scan = is_long + (nray + 1);
+	k_ray_class<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, is_long);
+	PSG_CHECK_LAUNCH();
+	{
+		size_t tmp = 0;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, is_long, long_scan, (int)nray, st));
+		void *dt = psg_scratch(ctx, S_CUB, tmp);
+		if (!dt) return PSG_E_NOMEM;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, is_long, long_scan, (int)nray, st));
+	}
+	std::vector<int32_t> h_scan(nray), h_last(1);
+	PSG_CUDA(cudaMemcpyAsync(h_scan.data(), long_scan, sizeof(int32_t) * nray, cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaMemcpyAsync(h_last.data(), is_long + nray - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
 	PSG_CUDA(cudaStreamSynchronize(st));
+	const int nlong_all = h_scan[nray - 1] + h_last[0];
+	uint32_t *long_rays = ray_lists, *short_rays = ray_lists + nlong_all;
+	k_ray_lists<<<blocks(nray, 256), 256, 0, st>>>(nray, is_long, long_scan, long_rays, short_rays);
+	PSG_CHECK_LAUNCH();
+	ctx->launches += 2;
 	for (size_t t = 0; t < K; t++) {
+		const int l0 = h_scan[t * R];
+		const int l1 = (t + 1 < K) ? h_scan[(t + 1) * R] : nlong_all;
+		const int nlong = l1 - l0;
+		const int s0 = (int)(t * R) - l0;
+		const int nshort = (int)R - nlong;
+		const unsigned grid = (unsigned)(nlong + (nshort + DEP_THREADS / 32 - 1) / (DEP_THREADS / 32));
 		psg_mark_begin(ctx, PSG_K_DEPOSIT);
-		k_deposit<<<(unsigned)R, DEP_THREADS, 0, st>>>(d_rays, t * R, (int)R, off64, hit_ipar, hit_kern,
-				slot, ctx->d_lambdaH, ctx->d_mass, P, want_heat, acc, acc_heat, d_nsat, d_lost);
+		if (grid)
+			k_deposit<<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, short_rays + s0, nshort, off64,
+					hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P, want_heat, acc, acc_heat, d_nsat, d_lost);
 		PSG_CHECK_LAUNCH();
 		psg_mark_end(ctx);
 		const int nact_t = h_tick_act[t + 1] - h_tick_act[t];
@@ -503,7 +660,7 @@ extern "C" int psg_step_evolve(psg_context *ctx, psg_step *steps, size_t n) {
 	if (!d) return PSG_E_NOMEM;
 	cudaStream_t st = ctx->stream;
 	PSG_CUDA(cudaMemcpyAsync(d, steps, sizeof(psg_step) * n, cudaMemcpyHostToDevice, st));
-	k_step_evolve<<<blocks(n, 128), 128, 0, st>>>(d, n, phys_params(ctx), ctx->d_status);
+	k_step_evolve<<<blocks(n, 128), 128, 0, st>>>(d, n, psg_phys_params(ctx), ctx->d_status);
 	PSG_CHECK_LAUNCH();
 	PSG_CUDA(cudaMemcpyAsync(steps, d, sizeof(psg_step) * n, cudaMemcpyDeviceToHost, st));
 	PSG_CUDA(cudaStreamSynchronize(st));

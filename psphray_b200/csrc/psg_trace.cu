@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "psg_internal.cuh"
+#include "psg_solve.cuh"
 
 namespace {
 
@@ -82,15 +83,14 @@ __device__ __forceinline__ bool line_hits_particle(const RayGeom &g, float4 q, d
 // of the window list their particles in shared memory and the lanes test
 // them 32 at a time. The next window starts after the window or after the
 // furthest missed subtree, whichever is later, so every window advances by
-// at least 32 cells. Accepted hits are appended with one atomic per warp
-// round; each record carries its ray and its rank within the ray (the
-// traversal order), so the scatter into per-ray lists is deterministic.
+// at least 32 cells. Accepted hits are written in traversal order straight
+// into the ray's own slab of scap entries; the true count is returned even
+// when it exceeds scap, so the caller can grow the slabs and run again.
 __global__ void __launch_bounds__(128) k_trace_warp(const psg_ray *__restrict__ rays, size_t nray,
 		const float4 *__restrict__ cell_lo, const float4 *__restrict__ cell_hi, int ncell,
 		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx, int ppc,
-		uint32_t *__restrict__ count, unsigned long long *__restrict__ nrec, size_t cap,
-		uint32_t *__restrict__ rec_ipar, uint32_t *__restrict__ rec_ray, uint32_t *__restrict__ rec_pos,
-		double *__restrict__ rec_d, double *__restrict__ rec_b) {
+		uint32_t *__restrict__ count, size_t scap, uint32_t *__restrict__ slab_ipar,
+		double *__restrict__ slab_d, double *__restrict__ slab_b) {
 	extern __shared__ int list_all[];
 	const int lane = threadIdx.x & 31;
 	const int wib = threadIdx.x >> 5;
@@ -149,24 +149,16 @@ __global__ void __launch_bounds__(128) k_trace_warp(const psg_ray *__restrict__ 
 				if (!(idx & PSG_INVALID_BIT)) acc = line_hits_particle(g, __ldg(&lpsml[p]), dc, r2);
 			}
 			const unsigned bal = __ballot_sync(0xffffffffu, acc);
-			if (bal) {
-				const unsigned n = __popc(bal);
-				unsigned long long q0 = 0;
-				if (lane == 0) q0 = atomicAdd(nrec, (unsigned long long)n);
-				q0 = __shfl_sync(0xffffffffu, q0, 0);
-				if (acc) {
-					const unsigned rank = __popc(bal & lt_mask);
-					const unsigned long long q = q0 + rank;
-					if (q < cap) {
-						rec_ipar[q] = idx;
-						rec_ray[q] = (uint32_t)r;
-						rec_pos[q] = nh + rank;
-						rec_d[q] = dc;
-						rec_b[q] = __dsqrt_rn(fabs(r2));
-					}
+			if (acc) {
+				const size_t q = nh + __popc(bal & lt_mask);
+				if (q < scap) {
+					const size_t o = r * scap + q;
+					slab_ipar[o] = idx;
+					slab_d[o] = dc;
+					slab_b[o] = __dsqrt_rn(fabs(r2));
 				}
-				nh += n;
 			}
+			nh += __popc(bal);
 		}
 		__syncwarp();
 		i = max(i + 32, __shfl_sync(0xffffffffu, m, 31));
@@ -174,27 +166,30 @@ __global__ void __launch_bounds__(128) k_trace_warp(const psg_ray *__restrict__ 
 	if (lane == 0) count[r] = nh;
 }
 
-// Records into per-ray lists at offsets[ray] + rank: CSR in traversal order.
-__global__ void k_scatter(size_t nrec, const int64_t *__restrict__ off, const uint32_t *__restrict__ rec_ipar,
-		const uint32_t *__restrict__ rec_ray, const uint32_t *__restrict__ rec_pos,
-		const double *__restrict__ rec_d, const double *__restrict__ rec_b, uint32_t *__restrict__ ipar,
-		double *__restrict__ d, double *__restrict__ b) {
-	const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (q >= nrec) return;
-	const int64_t dst = off[rec_ray[q]] + rec_pos[q];
-	ipar[dst] = rec_ipar[q];
-	d[dst] = rec_d[q];
-	b[dst] = rec_b[q];
+// Slabs into contiguous per-ray lists (traversal order), for the library
+// sort taken when a ray is longer than the shared-memory sort.
+__global__ void k_compact_slabs(size_t nray, size_t scap, const int64_t *__restrict__ off,
+		const uint32_t *__restrict__ slab_ipar, const double *__restrict__ slab_d, const double *__restrict__ slab_b,
+		uint32_t *__restrict__ ipar, double *__restrict__ d, double *__restrict__ b) {
+	const size_t r = blockIdx.x;
+	const int64_t h0 = off[r];
+	const int n = (int)(off[r + 1] - h0);
+	for (int i = threadIdx.x; i < n; i += blockDim.x) {
+		ipar[h0 + i] = slab_ipar[r * scap + i];
+		d[h0 + i] = slab_d[r * scap + i];
+		b[h0 + i] = slab_b[r * scap + i];
+	}
 }
 
 __global__ void k_offsets64(const uint32_t *__restrict__ scan32, const uint32_t *__restrict__ count,
-		size_t nray, int64_t *__restrict__ off64, int32_t *__restrict__ off32) {
+		size_t nray, int64_t *__restrict__ off64, int32_t *__restrict__ off32,
+		unsigned long long *__restrict__ maxcount) {
 	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (r > nray) return;
 	// scan32 holds the exclusive scan over nray+1 entries (count[nray] = 0)
 	off64[r] = scan32[r];
 	off32[r] = (int32_t)scan32[r];
-	(void)count;
+	if (r < nray) atomicMax(maxcount, (unsigned long long)count[r]);
 }
 
 __global__ void k_sort_keys(size_t nhit, const double *__restrict__ d, unsigned long long *__restrict__ keys,
@@ -217,6 +212,18 @@ __global__ void k_gather_sorted(size_t nhit, const uint32_t *__restrict__ perm,
 	b[h] = raw_b[j];
 }
 
+// Column-density factor of each hit, kernel = sph_depth(b/h) / h^2
+// (loop.c:429-445); b is overwritten.
+__global__ void k_hit_kernel(size_t nhit, const uint32_t *__restrict__ ipar, const float4 *__restrict__ psml,
+		double *__restrict__ b_to_kern, PhysParams P) {
+	const size_t h = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (h >= nhit) return;
+	const double sml = (double)psml[ipar[h]].w;
+	const double sml_inv = __ddiv_rn(1.0, sml);
+	const double r_h = rn_dmul(b_to_kern[h], sml_inv);
+	b_to_kern[h] = rn_dmul(sph_depth(P, r_h), rn_dmul(sml_inv, sml_inv));
+}
+
 // Runs of equal d inside a ray are put in ipar order (the reference leaves
 // their order to qsort); insertion sort, runs are almost always length 1.
 __global__ void k_break_ties(size_t nray, const int64_t *__restrict__ off, uint32_t *__restrict__ ipar,
@@ -235,6 +242,71 @@ __global__ void k_break_ties(size_t nray, const int64_t *__restrict__ off, uint3
 	}
 }
 
+// Per-ray sort by (d, ipar) in shared memory, one block per ray: a bitonic
+// network over the next power of two of the ray's hit count (padding keys
+// sort last). The comparison is the reference's d order (loop.c:783-787)
+// with ties broken by particle index. With want_kern the b column is
+// replaced by the column-density factor sph_depth(b/h)/h^2 of loop.c:429-445.
+__global__ void __launch_bounds__(256) k_sort_rays(size_t nray, const int64_t *__restrict__ off, size_t scap,
+		const uint32_t *__restrict__ slab_ipar, const double *__restrict__ slab_d, const double *__restrict__ slab_b,
+		uint32_t *__restrict__ out_ipar, double *__restrict__ out_d, double *__restrict__ out_b, int want_kern,
+		const float4 *__restrict__ psml, PhysParams P) {
+	extern __shared__ unsigned long long sk[];
+	const size_t r = blockIdx.x;
+	const int64_t h0 = off[r];
+	const int n = (int)(off[r + 1] - h0);
+	if (n == 0) return;
+	int p2 = 1;
+	while (p2 < n) p2 <<= 1;
+	uint32_t *si = (uint32_t *)(sk + p2);
+	uint32_t *sp = si + p2;
+	const uint32_t *raw_ipar = slab_ipar + r * scap;
+	const double *raw_d = slab_d + r * scap, *raw_b = slab_b + r * scap;
+	for (int i = threadIdx.x; i < p2; i += blockDim.x) {
+		if (i < n) {
+			sk[i] = (unsigned long long)__double_as_longlong(raw_d[i]);
+			si[i] = raw_ipar[i];
+			sp[i] = (uint32_t)i;
+		} else {
+			sk[i] = ~0ull;
+			si[i] = ~0u;
+			sp[i] = 0;
+		}
+	}
+	__syncthreads();
+	for (int k = 2; k <= p2; k <<= 1) {
+		for (int j = k >> 1; j > 0; j >>= 1) {
+			for (int i = threadIdx.x; i < p2; i += blockDim.x) {
+				const int l = i ^ j;
+				if (l > i) {
+					const unsigned long long a = sk[i], b = sk[l];
+					const uint32_t ia = si[i], ib = si[l];
+					const bool gt = a > b || (a == b && ia > ib);
+					if (gt == ((i & k) == 0)) {
+						sk[i] = b; sk[l] = a;
+						si[i] = ib; si[l] = ia;
+						const uint32_t t = sp[i]; sp[i] = sp[l]; sp[l] = t;
+					}
+				}
+			}
+			__syncthreads();
+		}
+	}
+	for (int i = threadIdx.x; i < n; i += blockDim.x) {
+		const uint32_t ip = si[i];
+		const double b = raw_b[sp[i]];
+		out_ipar[h0 + i] = ip;
+		out_d[h0 + i] = __longlong_as_double((long long)sk[i]);
+		if (want_kern) {
+			const double sml = (double)psml[ip].w;
+			const double inv = __ddiv_rn(1.0, sml);
+			out_b[h0 + i] = rn_dmul(sph_depth(P, rn_dmul(b, inv)), rn_dmul(inv, inv));
+		} else {
+			out_b[h0 + i] = b;
+		}
+	}
+}
+
 inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 }  // namespace
@@ -242,94 +314,121 @@ inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs);
 // Traces nray device-resident rays. Leaves in scratch: S_OFFSETS (int64
 // offsets[nray+1], then int32 offsets[nray+1]), S_HIT_IPAR (sorted caller
 // indices), S_RAW_D (sorted d) and S_HIT_KERN (sorted b).
-int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_db) {
-	(void)want_db;
+int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_kern) {
 	if (!ctx->have_tree) return psg_fail(ctx, PSG_E_INVAL, "trace: no tree (psg_build_tree first)");
 	cudaStream_t st = ctx->stream;
 	uint32_t *count = (uint32_t *)psg_scratch(ctx, S_COUNT, sizeof(uint32_t) * 2 * (nray + 1));
 	char *offmem = (char *)psg_scratch(ctx, S_OFFSETS, (sizeof(int64_t) + sizeof(int32_t)) * (nray + 1) + 256);
-	unsigned long long *d_nrec = ctx->d_counters;
 	if (!count || !offmem) return PSG_E_NOMEM;
 	uint32_t *scan = count + (nray + 1);
 	int64_t *off64 = (int64_t *)offmem;
 	int32_t *off32 = (int32_t *)(offmem + sizeof(int64_t) * (nray + 1));
+	unsigned long long *d_max = ctx->d_counters + 4;
 	const int ncell = (int)ctx->ncell;
 	const int ppc = ctx->ppc;
 	const int wpb = 4;
 	const size_t smem = sizeof(int) * 32 * (size_t)ppc * wpb;
 	if (smem > 48 * 1024)
 		PSG_CUDA(cudaFuncSetAttribute(k_trace_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-	// single traversal; if the record buffer was too small, grow it and rerun
-	size_t nrec = 0, cap = 0;
+	// one traversal into per-ray slabs; if a ray outgrew its slab, grow and rerun
+	size_t scap = 0;
+	unsigned long long maxcount = 0;
 	for (int attempt = 0; attempt < 2; attempt++) {
-		cap = ctx->rec_cap ? ctx->rec_cap : nray * 64 + 1024;
-		uint32_t *rec_u32 = (uint32_t *)psg_scratch(ctx, S_REC_U32, sizeof(uint32_t) * 3 * cap);
-		double *rec_f64 = (double *)psg_scratch(ctx, S_REC_F64, sizeof(double) * 2 * cap);
-		if (!rec_u32 || !rec_f64) return PSG_E_NOMEM;
-		PSG_CUDA(cudaMemsetAsync(d_nrec, 0, sizeof(unsigned long long), st));
+		scap = ctx->slab_cap ? ctx->slab_cap : 1024;
+		const size_t slots = nray * scap;
+		uint32_t *slab_ipar = (uint32_t *)psg_scratch(ctx, S_REC_U32, sizeof(uint32_t) * (slots ? slots : 1));
+		double *slab_f64 = (double *)psg_scratch(ctx, S_REC_F64, sizeof(double) * 2 * (slots ? slots : 1));
+		if (!slab_ipar || !slab_f64) return PSG_E_NOMEM;
 		PSG_CUDA(cudaMemsetAsync(count + nray, 0, sizeof(uint32_t), st));
+		PSG_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st));
 		psg_mark_begin(ctx, PSG_K_TRACE_FILL);
 		if (nray) {
 			k_trace_warp<<<blocks(nray, wpb), 32 * wpb, smem, st>>>(d_rays, nray, ctx->d_cell_lo,
-					ctx->d_cell_hi, ncell, ctx->d_leaf_psml, ctx->d_leaf_idx, ppc, count, d_nrec, cap,
-					rec_u32, rec_u32 + cap, rec_u32 + 2 * cap, rec_f64, rec_f64 + cap);
+					ctx->d_cell_hi, ncell, ctx->d_leaf_psml, ctx->d_leaf_idx, ppc, count, scap, slab_ipar,
+					slab_f64, slab_f64 + slots);
 			ctx->launches++;
 		}
 		PSG_CHECK_LAUNCH();
 		psg_mark_end(ctx);
-		unsigned long long got = 0;
-		PSG_CUDA(cudaMemcpyAsync(&got, d_nrec, sizeof(got), cudaMemcpyDeviceToHost, st));
+		size_t tmp = 0;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, count, scan, (int)(nray + 1), st));
+		void *dt = psg_scratch(ctx, S_CUB, tmp);
+		if (!dt) return PSG_E_NOMEM;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, count, scan, (int)(nray + 1), st));
+		k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32, d_max);
+		PSG_CHECK_LAUNCH();
+		ctx->launches++;
+		PSG_CUDA(cudaMemcpyAsync(&maxcount, d_max, sizeof(maxcount), cudaMemcpyDeviceToHost, st));
 		PSG_CUDA(cudaStreamSynchronize(st));
-		nrec = (size_t)got;
-		if (nrec <= cap) break;
-		ctx->rec_cap = nrec + nrec / 8 + 1024;
-		if (attempt == 1) return psg_fail(ctx, PSG_E_OVERFLOW, "trace: hit records grew between passes");
+		if (maxcount <= scap) break;
+		size_t want = 1024;
+		while (want < maxcount + maxcount / 4) want <<= 1;
+		ctx->slab_cap = want;
+		if (attempt == 1) return psg_fail(ctx, PSG_E_OVERFLOW, "trace: hit lists grew between passes");
 	}
-	if (nrec >= (size_t)INT32_MAX)
-		return psg_fail(ctx, PSG_E_OVERFLOW, "trace: %zu hits in one batch exceed 2^31", nrec);
-	if (!ctx->rec_cap || nrec > ctx->rec_cap) ctx->rec_cap = nrec + nrec / 8 + 1024;
-	size_t tmp = 0;
-	PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, count, scan, (int)(nray + 1), st));
-	void *dt = psg_scratch(ctx, S_CUB, tmp);
-	if (!dt) return PSG_E_NOMEM;
-	PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, count, scan, (int)(nray + 1), st));
-	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32);
-	PSG_CHECK_LAUNCH();
-	ctx->launches++;
-	const size_t nhit = nrec;
+	if (!ctx->slab_cap) ctx->slab_cap = scap;
+	int64_t nhit64 = 0;
+	PSG_CUDA(cudaMemcpyAsync(&nhit64, off64 + nray, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
+	const size_t nhit = (size_t)nhit64;
+	if (nhit >= (size_t)INT32_MAX)
+		return psg_fail(ctx, PSG_E_OVERFLOW, "trace: %zu hits in one batch exceed 2^31", nhit);
 	const size_t hb = nhit ? nhit : 1;
-	uint32_t *raw_ipar = (uint32_t *)psg_scratch(ctx, S_RAW_IPAR, sizeof(uint32_t) * hb);
-	double *raw_d = (double *)psg_scratch(ctx, S_RAW_D, sizeof(double) * 2 * hb);
-	double *raw_b = (double *)psg_scratch(ctx, S_RAW_B, sizeof(double) * hb);
-	unsigned long long *keys = (unsigned long long *)psg_scratch(ctx, S_KEYS, sizeof(unsigned long long) * 2 * hb);
-	uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
 	uint32_t *hit_ipar = (uint32_t *)psg_scratch(ctx, S_HIT_IPAR, sizeof(uint32_t) * hb);
+	double *hit_db = (double *)psg_scratch(ctx, S_RAW_D, sizeof(double) * 2 * hb);
 	double *hit_b = (double *)psg_scratch(ctx, S_HIT_KERN, sizeof(double) * hb);
-	if (!raw_ipar || !raw_d || !raw_b || !keys || !vals || !hit_ipar || !hit_b) return PSG_E_NOMEM;
-	double *hit_d = raw_d + hb;
+	if (!hit_ipar || !hit_db || !hit_b) return PSG_E_NOMEM;
+	double *hit_d = hit_db + hb;
+	const size_t slots = nray * scap;
+	uint32_t *slab_ipar = (uint32_t *)ctx->scratch[S_REC_U32].p;
+	double *slab_d = (double *)ctx->scratch[S_REC_F64].p;
+	double *slab_b = slab_d + slots;
 	if (nhit) {
 		psg_mark_begin(ctx, PSG_K_SORT);
-		uint32_t *rec_u32 = (uint32_t *)ctx->scratch[S_REC_U32].p;
-		double *rec_f64 = (double *)ctx->scratch[S_REC_F64].p;
-		const size_t c = cap;     // the layout the traversal wrote with
-		k_scatter<<<blocks(nhit, 256), 256, 0, st>>>(nhit, off64, rec_u32, rec_u32 + c, rec_u32 + 2 * c,
-				rec_f64, rec_f64 + c, raw_ipar, raw_d, raw_b);
-		PSG_CHECK_LAUNCH();
-		ctx->launches += 4;
-		k_sort_keys<<<blocks(nhit, 256), 256, 0, st>>>(nhit, raw_d, keys, vals);
-		PSG_CHECK_LAUNCH();
-		size_t stmp = 0;
-		PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, stmp, keys, keys + hb, vals, vals + hb,
-				(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
-		void *dst = psg_scratch(ctx, S_CUB, stmp);
-		if (!dst) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(dst, stmp, keys, keys + hb, vals, vals + hb,
-				(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
-		k_gather_sorted<<<blocks(nhit, 256), 256, 0, st>>>(nhit, vals + hb, raw_ipar, raw_d, raw_b,
-				hit_ipar, hit_d, hit_b);
-		PSG_CHECK_LAUNCH();
-		k_break_ties<<<blocks(nray, 128), 128, 0, st>>>(nray, off64, hit_ipar, hit_d, hit_b);
-		PSG_CHECK_LAUNCH();
+		if (maxcount <= PSG_SORT_MAX) {
+			int p2 = 1;
+			while ((unsigned long long)p2 < maxcount) p2 <<= 1;
+			const size_t ssm = (size_t)p2 * 16;
+			if (ssm > 48 * 1024)
+				PSG_CUDA(cudaFuncSetAttribute(k_sort_rays, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+			const int bs = p2 >= 512 ? 256 : (p2 >= 64 ? p2 / 2 : 32);
+			k_sort_rays<<<(unsigned)nray, bs, ssm, st>>>(nray, off64, scap, slab_ipar, slab_d, slab_b, hit_ipar,
+					hit_d, hit_b, want_kern, ctx->d_psml, psg_phys_params(ctx));
+			PSG_CHECK_LAUNCH();
+			ctx->launches++;
+		} else {
+			// a ray longer than the shared-memory sort takes: library segmented sort
+			uint32_t *raw_ipar = (uint32_t *)psg_scratch(ctx, S_RAW_IPAR, sizeof(uint32_t) * hb);
+			double *raw_db = (double *)psg_scratch(ctx, S_RAW_B, sizeof(double) * 2 * hb);
+			unsigned long long *keys = (unsigned long long *)psg_scratch(ctx, S_KEYS, sizeof(unsigned long long) * 2 * hb);
+			uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
+			if (!raw_ipar || !raw_db || !keys || !vals) return PSG_E_NOMEM;
+			double *raw_d = raw_db, *raw_b = raw_db + hb;
+			k_compact_slabs<<<(unsigned)nray, 128, 0, st>>>(nray, scap, off64, slab_ipar, slab_d, slab_b,
+					raw_ipar, raw_d, raw_b);
+			PSG_CHECK_LAUNCH();
+			k_sort_keys<<<blocks(nhit, 256), 256, 0, st>>>(nhit, raw_d, keys, vals);
+			PSG_CHECK_LAUNCH();
+			size_t stmp = 0;
+			PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, stmp, keys, keys + hb, vals, vals + hb,
+					(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
+			void *dst = psg_scratch(ctx, S_CUB, stmp);
+			if (!dst) return PSG_E_NOMEM;
+			PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(dst, stmp, keys, keys + hb, vals, vals + hb,
+					(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
+			k_gather_sorted<<<blocks(nhit, 256), 256, 0, st>>>(nhit, vals + hb, raw_ipar, raw_d, raw_b,
+					hit_ipar, hit_d, hit_b);
+			PSG_CHECK_LAUNCH();
+			k_break_ties<<<blocks(nray, 128), 128, 0, st>>>(nray, off64, hit_ipar, hit_d, hit_b);
+			PSG_CHECK_LAUNCH();
+			ctx->launches += 4;
+			if (want_kern) {
+				k_hit_kernel<<<blocks(nhit, 256), 256, 0, st>>>(nhit, hit_ipar, ctx->d_psml, hit_b,
+						psg_phys_params(ctx));
+				PSG_CHECK_LAUNCH();
+				ctx->launches++;
+			}
+		}
 		psg_mark_end(ctx);
 	}
 	return PSG_OK;
@@ -388,7 +487,7 @@ extern "C" int psg_trace(psg_context *ctx, const psg_ray *rays, size_t nray, int
 	psg_ray *d_rays = nullptr;
 	int rc = upload_rays(ctx, rays, nray, &d_rays);
 	if (rc) return rc;
-	rc = psg_trace_internal(ctx, d_rays, nray, 1);
+	rc = psg_trace_internal(ctx, d_rays, nray, 0);
 	if (rc) return rc;
 	size_t nhit = 0;
 	return download_hits(ctx, nray, offsets, x, size, &nhit);
@@ -404,7 +503,7 @@ extern "C" size_t psg_rt_trace(psg_context *ctx, const float s[3], const float d
 	if (cudaSetDevice(ctx->device) != cudaSuccess) return (size_t)-1;
 	psg_ray *d_rays = nullptr;
 	if (upload_rays(ctx, &ray, 1, &d_rays)) return (size_t)-1;
-	if (psg_trace_internal(ctx, d_rays, 1, 1)) return (size_t)-1;
+	if (psg_trace_internal(ctx, d_rays, 1, 0)) return (size_t)-1;
 	size_t nhit = 0;
 	if (download_hits(ctx, 1, nullptr, x, size, &nhit)) return (size_t)-1;
 	return nhit;

@@ -205,3 +205,25 @@ def test_errors_are_reported_not_trapped(gpu_ctx, phys):
     # the context stays usable
     _gpu(gpu_ctx, f, phys)
     gpu_ctx.run_ticks(g["rays"][:16], 16, 1, 1, float(g["tick_time"]))
+
+
+def test_capped_deposits_vs_oracle(gpu_ctx, phys):
+    """Rays carrying 1e3x the photons saturate particles (the cap of
+    loop.c:482-485) and end early on the 1e-10 cut: both settled exactly
+    as the sequential restatement settles them."""
+    g = load_golden("uniform16.npz")
+    f = golden_field(g)
+    _gpu(gpu_ctx, f, phys)
+    orc = Oracle(f, phys)
+    orc.build_tree(8)
+    R = int(g["nray"])
+    rays = g["rays"][:4 * R].copy()
+    rays["Nph"] *= 1e3
+    st = gpu_ctx.run_ticks(rays, R, 4, 1, float(g["tick_time"]))
+    sat = 0
+    for k in range(4):
+        sat += orc.tick(rays[k * R:(k + 1) * R], k + 1, float(g["tick_time"]))["saturated"]
+    assert sat > 0 and st["saturated"] == sat
+    gs = gpu_ctx.state()
+    assert np.array_equal(gs["hits"], orc.hits)
+    assert np.max(np.abs(gs["lambdaH"] - orc.lambdaH)) < 1e-9
