@@ -124,7 +124,12 @@ def cpu_baseline_reference(w, seconds: float = 15.0, threads: int | None = None,
         if not os.path.exists(LIB_PATH):
             raise FileNotFoundError(LIB_PATH)
         from psphray_b200.api import RATES_HUI
-        ref = Reference(RATES_HUI, w.field.units, isothermal=w.isothermal, threads=threads)
+        # The reference's non-isothermal solver raises SIGTRAP (solve.c:137-139)
+        # wherever one step of cooling exceeds the internal energy, which the
+        # dense cells of the log-normal field reach; its hits/s clock covers
+        # trace + deposit only, which do not depend on the solver, so the
+        # sample runs its isothermal solver.
+        ref = Reference(RATES_HUI, w.field.units, isothermal=True, threads=threads)
         ref.load(w.field)
         ref.build_tree(8)
         ref.reset_stats()
@@ -137,7 +142,8 @@ def cpu_baseline_reference(w, seconds: float = 15.0, threads: int | None = None,
         hits_s = st["hits"] / (st["raytrace_time"] + st["deposit_time"])
         full = (st["raytrace_time"] + st["deposit_time"] + st["merge_time"] + st["update_time"])
         return {"value": hits_s, "unit": "hits/s", "cores": threads, "kind": "reference",
-                "sample": f"{n} ticks x {w.schedule.nray} rays of {w.name}, trace+deposit clock "
+                "sample": f"{n} ticks x {w.schedule.nray} rays of {w.name}"
+                          f"{'' if w.isothermal else ' (isothermal solver; see bench.py)'}, trace+deposit clock "
                           f"({st['hits']:.0f} hits); whole tick incl. LSODA update: "
                           f"{st['hits'] / full:.4g} hits/s, {full / n * 1e3:.3g} ms/tick"}
     except FileNotFoundError:

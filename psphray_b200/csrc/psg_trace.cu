@@ -242,61 +242,77 @@ __global__ void k_break_ties(size_t nray, const int64_t *__restrict__ off, uint3
 	}
 }
 
-// Per-ray sort by (d, ipar) in shared memory, one block per ray: a bitonic
-// network over the next power of two of the ray's hit count (padding keys
-// sort last). The comparison is the reference's d order (loop.c:783-787)
-// with ties broken by particle index. With want_kern the b column is
-// replaced by the column-density factor sph_depth(b/h)/h^2 of loop.c:429-445.
-__global__ void __launch_bounds__(256) k_sort_rays(size_t nray, const int64_t *__restrict__ off, size_t scap,
-		const uint32_t *__restrict__ slab_ipar, const double *__restrict__ slab_d, const double *__restrict__ slab_b,
-		uint32_t *__restrict__ out_ipar, double *__restrict__ out_d, double *__restrict__ out_b, int want_kern,
-		const float4 *__restrict__ psml, PhysParams P) {
-	extern __shared__ unsigned long long sk[];
-	const size_t r = blockIdx.x;
+// Per-ray sort by (d, ipar), one ray per block of TPR threads holding IPT
+// hits each: a block radix sort (8 passes of 4 bits) on the float image of
+// d, which preserves the order of d >= 0; the few runs where distinct
+// doubles round to one float are then insertion-sorted on the exact (d,
+// ipar) -- the reference's d order (loop.c:783-787) with ties broken by
+// particle index. With want_kern the b column is replaced by the
+// column-density factor sph_depth(b/h)/h^2 of loop.c:429-445.
+template <int TPR, int IPT>
+__global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__ list, int nlist,
+		const int64_t *__restrict__ off, size_t scap, const uint32_t *__restrict__ slab_ipar,
+		const double *__restrict__ slab_d, const double *__restrict__ slab_b, uint32_t *__restrict__ out_ipar,
+		double *__restrict__ out_d, double *__restrict__ out_b, int want_kern, const float4 *__restrict__ psml,
+		PhysParams P) {
+	constexpr int NMAX = TPR * IPT;
+	using Sort = cub::BlockRadixSort<uint32_t, TPR, IPT, uint32_t, 4>;
+	struct Smem {
+		typename Sort::TempStorage sort;
+		uint32_t key[NMAX];
+		uint32_t pos[NMAX];
+	};
+	extern __shared__ __align__(16) char sort_smem[];
+	Smem &sm = *reinterpret_cast<Smem *>(sort_smem);
+	if ((int)blockIdx.x >= nlist) return;
+	const size_t r = list[blockIdx.x];
 	const int64_t h0 = off[r];
 	const int n = (int)(off[r + 1] - h0);
-	if (n == 0) return;
-	int p2 = 1;
-	while (p2 < n) p2 <<= 1;
-	uint32_t *si = (uint32_t *)(sk + p2);
-	uint32_t *sp = si + p2;
 	const uint32_t *raw_ipar = slab_ipar + r * scap;
 	const double *raw_d = slab_d + r * scap, *raw_b = slab_b + r * scap;
-	for (int i = threadIdx.x; i < p2; i += blockDim.x) {
-		if (i < n) {
-			sk[i] = (unsigned long long)__double_as_longlong(raw_d[i]);
-			si[i] = raw_ipar[i];
-			sp[i] = (uint32_t)i;
-		} else {
-			sk[i] = ~0ull;
-			si[i] = ~0u;
-			sp[i] = 0;
+	uint32_t k[IPT], v[IPT];
+#pragma unroll
+	for (int u = 0; u < IPT; u++) {
+		const int i = threadIdx.x * IPT + u;
+		k[u] = i < n ? __float_as_uint((float)raw_d[i]) : 0xFFFFFFFFu;
+		v[u] = (uint32_t)i;
+	}
+	Sort(sm.sort).Sort(k, v, 0, 32);
+	__syncthreads();
+#pragma unroll
+	for (int u = 0; u < IPT; u++) {
+		const int i = threadIdx.x * IPT + u;
+		sm.key[i] = k[u];
+		sm.pos[i] = v[u];
+	}
+	__syncthreads();
+	// exact order inside runs of equal float keys
+	for (int i = threadIdx.x; i + 1 < n; i += TPR) {
+		if (sm.key[i] != sm.key[i + 1] || (i > 0 && sm.key[i - 1] == sm.key[i])) continue;
+		int e = i + 1;
+		while (e + 1 < n && sm.key[e + 1] == sm.key[i]) e++;
+		for (int a = i + 1; a <= e; a++) {
+			const uint32_t pa = sm.pos[a];
+			const double da = raw_d[pa];
+			const uint32_t ia = raw_ipar[pa];
+			int c = a;
+			while (c > i) {
+				const uint32_t pc = sm.pos[c - 1];
+				const double dc = raw_d[pc];
+				if (dc < da || (dc == da && raw_ipar[pc] < ia)) break;
+				sm.pos[c] = pc;
+				c--;
+			}
+			sm.pos[c] = pa;
 		}
 	}
 	__syncthreads();
-	for (int k = 2; k <= p2; k <<= 1) {
-		for (int j = k >> 1; j > 0; j >>= 1) {
-			for (int i = threadIdx.x; i < p2; i += blockDim.x) {
-				const int l = i ^ j;
-				if (l > i) {
-					const unsigned long long a = sk[i], b = sk[l];
-					const uint32_t ia = si[i], ib = si[l];
-					const bool gt = a > b || (a == b && ia > ib);
-					if (gt == ((i & k) == 0)) {
-						sk[i] = b; sk[l] = a;
-						si[i] = ib; si[l] = ia;
-						const uint32_t t = sp[i]; sp[i] = sp[l]; sp[l] = t;
-					}
-				}
-			}
-			__syncthreads();
-		}
-	}
-	for (int i = threadIdx.x; i < n; i += blockDim.x) {
-		const uint32_t ip = si[i];
-		const double b = raw_b[sp[i]];
+	for (int i = threadIdx.x; i < n; i += TPR) {
+		const uint32_t p = sm.pos[i];
+		const uint32_t ip = raw_ipar[p];
+		const double b = raw_b[p];
 		out_ipar[h0 + i] = ip;
-		out_d[h0 + i] = __longlong_as_double((long long)sk[i]);
+		out_d[h0 + i] = raw_d[p];
 		if (want_kern) {
 			const double sml = (double)psml[ip].w;
 			const double inv = __ddiv_rn(1.0, sml);
@@ -305,6 +321,27 @@ __global__ void __launch_bounds__(256) k_sort_rays(size_t nray, const int64_t *_
 			out_b[h0 + i] = b;
 		}
 	}
+}
+
+template <int TPR, int IPT>
+size_t sort_smem_bytes() {
+	return sizeof(typename cub::BlockRadixSort<uint32_t, TPR, IPT, uint32_t, 4>::TempStorage) + 8 * TPR * IPT + 64;
+}
+
+// Size classes of the ray sort: class c holds rays with at most
+// kSortClassMax[c] hits (and more than the previous class's bound).
+__constant__ int kSortBounds[4] = {64, 512, 2048, PSG_SORT_MAX};   // 32x2, 128x4, 256x8, 512x16
+
+__global__ void k_sort_classify(size_t nray, const int64_t *__restrict__ off, uint32_t *__restrict__ lists,
+		size_t stride, unsigned long long *__restrict__ nclass) {
+	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (r >= nray) return;
+	const int64_t n = off[r + 1] - off[r];
+	if (n == 0) return;
+	int c = 0;
+	while (c < 3 && n > kSortBounds[c]) c++;
+	const unsigned long long k = atomicAdd(&nclass[c], 1ull);
+	lists[c * stride + k] = (uint32_t)r;
 }
 
 inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -386,16 +423,34 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	if (nhit) {
 		psg_mark_begin(ctx, PSG_K_SORT);
 		if (maxcount <= PSG_SORT_MAX) {
-			int p2 = 1;
-			while ((unsigned long long)p2 < maxcount) p2 <<= 1;
-			const size_t ssm = (size_t)p2 * 16;
-			if (ssm > 48 * 1024)
-				PSG_CUDA(cudaFuncSetAttribute(k_sort_rays, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
-			const int bs = p2 >= 512 ? 256 : (p2 >= 64 ? p2 / 2 : 32);
-			k_sort_rays<<<(unsigned)nray, bs, ssm, st>>>(nray, off64, scap, slab_ipar, slab_d, slab_b, hit_ipar,
-					hit_d, hit_b, want_kern, ctx->d_psml, psg_phys_params(ctx));
+			uint32_t *lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * 4 * (nray + 1));
+			if (!lists) return PSG_E_NOMEM;
+			unsigned long long *d_ncls = ctx->d_counters + 4;
+			PSG_CUDA(cudaMemsetAsync(d_ncls, 0, 4 * sizeof(unsigned long long), st));
+			k_sort_classify<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, lists, nray + 1, d_ncls);
 			PSG_CHECK_LAUNCH();
-			ctx->launches++;
+			unsigned long long ncls[4];
+			PSG_CUDA(cudaMemcpyAsync(ncls, d_ncls, sizeof(ncls), cudaMemcpyDeviceToHost, st));
+			PSG_CUDA(cudaStreamSynchronize(st));
+			const PhysParams PP = psg_phys_params(ctx);
+			const size_t stride = nray + 1;
+			auto launch_block = [&](auto kern, int tpr, size_t smem, const uint32_t *lst, unsigned long long nl) -> int {
+				if (!nl) return PSG_OK;
+				if (smem > 48 * 1024)
+					PSG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+				kern<<<(unsigned)nl, tpr, smem, st>>>(lst, (int)nl, off64, scap, slab_ipar, slab_d, slab_b, hit_ipar,
+						hit_d, hit_b, want_kern, ctx->d_psml, PP);
+				PSG_CHECK_LAUNCH();
+				return PSG_OK;
+			};
+			int rcs = launch_block(k_sort_block<32, 2>, 32, sort_smem_bytes<32, 2>(), lists, ncls[0]);
+			if (!rcs) rcs = launch_block(k_sort_block<128, 4>, 128, sort_smem_bytes<128, 4>(), lists + stride, ncls[1]);
+			if (!rcs) rcs = launch_block(k_sort_block<256, 8>, 256, sort_smem_bytes<256, 8>(), lists + 2 * stride,
+					ncls[2]);
+			if (!rcs) rcs = launch_block(k_sort_block<512, 16>, 512, sort_smem_bytes<512, 16>(), lists + 3 * stride,
+					ncls[3]);
+			if (rcs) return rcs;
+			ctx->launches += 1 + (ncls[0] > 0) + (ncls[1] > 0) + (ncls[2] > 0) + (ncls[3] > 0);
 		} else {
 			// a ray longer than the shared-memory sort takes: library segmented sort
 			uint32_t *raw_ipar = (uint32_t *)psg_scratch(ctx, S_RAW_IPAR, sizeof(uint32_t) * hb);
