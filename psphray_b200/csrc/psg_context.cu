@@ -132,12 +132,19 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 	if (ctx->d_xs) cudaFree(ctx->d_xs);
 	if (ctx->d_kernel) cudaFree(ctx->d_kernel);
 	ctx->d_ar = ctx->d_xs = ctx->d_kernel = nullptr;
+	// rows of 16 doubles (one 128-byte line): log T, then the 15 rate columns
 	const size_t nr = (size_t)ar->nrows;
-	PSG_CUDA(cudaMalloc(&ctx->d_ar, sizeof(double) * nr * (PSG_AR_NCOLS + 1)));
-	PSG_CUDA(cudaMemcpy(ctx->d_ar, ar->logT, sizeof(double) * nr, cudaMemcpyHostToDevice));
-	for (int c = 0; c < PSG_AR_NCOLS; c++)
-		PSG_CUDA(cudaMemcpy(ctx->d_ar + nr * (c + 1), ar->col[c], sizeof(double) * nr,
-				cudaMemcpyHostToDevice));
+	static_assert(PSG_AR_NCOLS + 1 == 16, "one rate row is one 128-byte line");
+	double *rows = (double *)malloc(sizeof(double) * nr * 16);
+	if (!rows) return psg_fail(ctx, PSG_E_NOMEM, "psg_set_physics: host allocation failed");
+	for (size_t j = 0; j < nr; j++) {
+		rows[16 * j] = ar->logT[j];
+		for (int c = 0; c < PSG_AR_NCOLS; c++) rows[16 * j + 1 + c] = ar->col[c][j];
+	}
+	cudaError_t e1 = cudaMalloc(&ctx->d_ar, sizeof(double) * nr * 16);
+	if (e1 == cudaSuccess) e1 = cudaMemcpy(ctx->d_ar, rows, sizeof(double) * nr * 16, cudaMemcpyHostToDevice);
+	free(rows);
+	PSG_CUDA(e1);
 	const size_t nx = (size_t)xs->nrows;
 	PSG_CUDA(cudaMalloc(&ctx->d_xs, sizeof(double) * nx * 2));
 	PSG_CUDA(cudaMemcpy(ctx->d_xs, xs->eng, sizeof(double) * nx, cudaMemcpyHostToDevice));

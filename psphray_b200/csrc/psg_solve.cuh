@@ -20,7 +20,7 @@
 #include "psg_internal.cuh"
 
 struct PhysParams {
-	const double *ar;      // [PSG_AR_NCOLS+1][ar_nrows], logT first
+	const double *ar;      // [ar_nrows][16]: log T, then the PSG_AR_* columns
 	int ar_nrows;
 	double ar_min, ar_step_inv;
 	const double *xs;      // [2][xs_nrows]: energy, sigma_HI
@@ -46,8 +46,43 @@ __device__ __forceinline__ double tab_get(int nrows, double min, double step_inv
 	return rn_dmul(rn_dadd(rn_dmul(lw, y[idx]), rn_dmul(rw, y[idx + 1])), step_inv);
 }
 
+// ar_get() atomic-rate.c:89 for several columns at one log T: the row index
+// and the interpolation weights of tabfun_get() are computed once.
+struct RateAt {
+	const double *r0, *r1;
+	double lw, rw, step_inv;
+	int clamp;            // 0 interpolate, 1 first row, 2 last row
+	__device__ __forceinline__ double operator()(int col) const {
+		if (clamp == 1) return r0[1 + col];
+		if (clamp == 2) return r1[1 + col];
+		return rn_dmul(rn_dadd(rn_dmul(lw, r0[1 + col]), rn_dmul(rw, r1[1 + col])), step_inv);
+	}
+};
+
+__device__ __forceinline__ RateAt rates_at(const PhysParams &P, double logT) {
+	RateAt a;
+	a.step_inv = P.ar_step_inv;
+	const long long idx = (long long)rn_dmul(rn_dsub(logT, P.ar_min), P.ar_step_inv);
+	if (idx < 0) {
+		a.clamp = 1;
+		a.r0 = a.r1 = P.ar;
+		a.lw = a.rw = 0.0;
+	} else if (idx >= P.ar_nrows - 1) {
+		a.clamp = 2;
+		a.r0 = a.r1 = P.ar + (size_t)(P.ar_nrows - 1) * 16;
+		a.lw = a.rw = 0.0;
+	} else {
+		a.clamp = 0;
+		a.r0 = P.ar + (size_t)idx * 16;
+		a.r1 = a.r0 + 16;
+		a.lw = rn_dsub(a.r1[0], logT);
+		a.rw = rn_dsub(logT, a.r0[0]);
+	}
+	return a;
+}
+
 __device__ __forceinline__ double ar_get(const PhysParams &P, int col, double logT) {
-	return tab_get(P.ar_nrows, P.ar_min, P.ar_step_inv, P.ar, P.ar + (size_t)P.ar_nrows * (col + 1), logT);
+	return rates_at(P, logT)(col);
 }
 
 // xs_get() atomic-rate.c:126-131 for HI
@@ -103,19 +138,19 @@ __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const
 	const double xHI = x[0], xHII = 1.0 - x[0];
 	const double ye = xHII + P.he_e + cx.yeMET;
 	const double T = P.isothermal ? cx.T : ieye2T(P, x[1], ye);
-	const double logT = log10(T);
+	const RateAt R = rates_at(P, log10(T));
 	const double nH = cx.nH;
-	const double gamma = ar_get(P, PSG_AR_HI_CI, logT) * nH;
-	const double alpha = ar_get(P, P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A, logT) * nH;
+	const double gamma = R(PSG_AR_HI_CI) * nH;
+	const double alpha = R(P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A) * nH;
 	dx[0] = (-cx.g / cx.time + (-gamma * ye * xHI + alpha * ye * xHII)) * cx.time;
 	if (P.isothermal || P.adiabatic) {
 		dx[1] = 0.0;
 	} else {
-		const double eta = ar_get(P, P.on_the_spot ? PSG_AR_HII_RCC_B : PSG_AR_HII_RCC_A, logT) * nH;
-		const double psi = ar_get(P, PSG_AR_HI_CEC, logT) * nH;
-		const double zeta = ar_get(P, PSG_AR_HI_CIC, logT) * nH;
-		const double beta = ar_get(P, PSG_AR_E_BREMC, logT) * nH;
-		const double chi = ar_get(P, PSG_AR_E_COMPC, logT);
+		const double eta = R(P.on_the_spot ? PSG_AR_HII_RCC_B : PSG_AR_HII_RCC_A) * nH;
+		const double psi = R(PSG_AR_HI_CEC) * nH;
+		const double zeta = R(PSG_AR_HI_CIC) * nH;
+		const double beta = R(PSG_AR_E_BREMC) * nH;
+		const double chi = R(PSG_AR_E_COMPC);
 		const double L = P.H_PER_MASS * ((zeta + psi) * ye * xHI + eta * ye * xHII + beta * ye * xHII + chi * ye);
 		dx[1] = (cx.heat / cx.time - L) * cx.time;
 	}
@@ -128,11 +163,21 @@ __device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2],
 	const double a61 = 9017. / 3168, a62 = -355. / 33, a63 = 46732. / 5247, a64 = 49. / 176, a65 = -5103. / 18656;
 	const double b1 = 35. / 384, b3 = 500. / 1113, b4 = 125. / 192, b5 = -2187. / 6784, b6 = 11. / 84;
 	const double e1 = 71. / 57600, e3 = -71. / 16695, e4 = 71. / 1920, e5 = -17253. / 339200, e6 = 22. / 525, e7 = -1. / 40;
-	const double rtol = 1e-8;
-	const double atol0 = 1e-12, atol1 = 1e-10 * fabs(x[1]) + 1e-300;
-	double t = 0.0, h = 0.05;
+	// LSODA runs the reference at rtol 1e-4 (solve.c:151-152); 1e-6 here
+	const double rtol = 1e-6;
+	const double atol0 = 1e-10, atol1 = 1e-8 * fabs(x[1]) + 1e-300;
+	double t = 0.0;
 	double k1[2], k2[2], k3[2], k4[2], k5[2], k6[2], k7[2], y[2], yn[2];
 	rhs(P, cx, x, k1);
+	// first step from the derivatives: about a 1% change of each component
+	// (components near zero measured against atol/rtol)
+	double h = 1.0;
+	for (int i = 0; i < 2; i++) {
+		const double scale = fabs(x[i]) + (i == 0 ? atol0 : atol1) / rtol;
+		const double f = fabs(k1[i]);
+		if (f > 0.0) h = fmin(h, 0.01 * scale / f);
+	}
+	h = fmax(h, 1e-8);
 	for (int it = 0; it < max_steps; it++) {
 		if (t >= 1.0) return true;
 		if (t + h > 1.0) h = 1.0 - t;
@@ -170,9 +215,9 @@ __device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2],
 // Isothermal step only (the closed form), for the kernels specialised on it.
 __device__ inline uint32_t solve_step_iso(const PhysParams &P, double &lambdaH, double yeMET, double g,
 		double time, double nH, double T) {
-	const double logT = log10(T);
-	const double gamma = ar_get(P, PSG_AR_HI_CI, logT) * nH;
-	const double alpha = ar_get(P, P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A, logT) * nH;
+	const RateAt R = rates_at(P, log10(T));
+	const double gamma = R(PSG_AR_HI_CI) * nH;
+	const double alpha = R(P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A) * nH;
 	const double m = yeMET + P.he_e;
 	const double a = time * (alpha + gamma);
 	const double b = time * (alpha + (alpha + gamma) * (1.0 + m));

@@ -158,8 +158,8 @@ def test_step_evolve_vs_oracle(gpu_ctx, phys):
 
 
 def test_step_evolve_noniso_vs_oracle(gpu_ctx, phys_noniso):
-    """Not isothermal: lambdaH and ie integrated together; GPU (rtol 1e-8)
-    against the restatement (rtol 1e-10)."""
+    """Not isothermal: lambdaH and ie integrated together; GPU (rtol 1e-6;
+    the reference's LSODA runs at 1e-4) against the restatement (rtol 1e-10)."""
     from psphray_b200.api import STEP_DTYPE
     g = load_golden("uniform16.npz")
     f = golden_field(g)
@@ -179,10 +179,10 @@ def test_step_evolve_noniso_vs_oracle(gpu_ctx, phys_noniso):
     for s, o in zip(steps, out):
         lam, ie, rc = orc.solve(s["lambdaH"], s["ie"], 0.0, s["yGdepHI"], s["heat"], s["time"], s["nH"], s["T"])
         assert rc == 0
-        assert abs(o["lambdaH"] - lam) < 1e-6
+        assert abs(o["lambdaH"] - lam) < 1e-5
         # rate tables are linear in log T, so the right-hand side is only
-        # continuous: two adaptive integrations agree to ~1e-6, not to rtol
-        assert abs(o["ie"] - ie) / ie < 1e-5
+        # continuous: the integrations agree to ~1e-5, not to rtol
+        assert abs(o["ie"] - ie) / ie < 1e-4
 
 
 def test_errors_are_reported_not_trapped(gpu_ctx, phys):
