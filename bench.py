@@ -1,6 +1,6 @@
 """Throughput of the trace -> deposit -> merge -> update hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload iliev64]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload lognormal128]
                     [--ticks T] [--impl ours|reference]
 
 A step is one batch of T ticks of the workload: all rays of those ticks are
@@ -10,7 +10,8 @@ hits per second (hits = stat.total_deposit_count, the summed hit-list
 lengths), over the whole pipeline -- a stricter clock than the reference's
 own hits/s, which counts only trace + deposit time.
 
-Workloads (seeded synthetic fields; no dataset is involved):
+Workloads (seeded synthetic fields; no dataset is involved; the default is
+lognormal128, the 2M-particle case the hits/s target is stated at):
   iliev64       64^3 uniform particles in a 6.6 kpc box, one corner source of
                 5e48 photons/s at 13.6 eV, 1024 rays/tick, isothermal 1e4 K
   iliev32       32^3, 32 rays/tick (the reference's CPU-sized case)
@@ -36,6 +37,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 DEFAULT_TICKS = {"iliev32": 400, "iliev64": 100, "lognormal128": 8}
+REF_TICKS = {"iliev32": 40, "iliev64": 4, "lognormal128": 1}   # per step of --impl reference
 BYTES_PER_HIT = 36       # pos 12 + sml 4 + lambdaH 8 + mass 4 + FP64 absorbed photons 8
 BYTES_PER_HIT_TRACE = 36  # trace fill: pos+sml 16 read, (ipar 4, d 8, b 8) written
 
@@ -162,6 +164,18 @@ def cpu_baseline_reference(w, seconds: float = 15.0, threads: int | None = None,
                 "sample": f"{n} ticks x {w.schedule.nray} rays of {w.name}, whole tick, 1 thread"}
 
 
+def reduce_over_ranks(t_local: float, hits: float, dist, device):
+    """Max of the ranks' times and sum of their hits (all ranks get both)."""
+    import torch
+    if dist is None:
+        return t_local, hits
+    t = torch.tensor([t_local], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    h = torch.tensor([hits], device=device, dtype=torch.float64)
+    dist.all_reduce(h)
+    return float(t.item()), float(h.item())
+
+
 def dist_setup(gpus: int):
     if gpus <= 1 or "RANK" not in os.environ:
         return 0, 1, 0, None
@@ -176,25 +190,48 @@ def dist_setup(gpus: int):
 
 
 def run_reference(args):
+    """--impl reference: the reference's own CPU code (oracle/_ref) on the
+    same workload, all host threads, each step a bounded sample of ticks;
+    hits/s on the reference's own clock (trace + deposit, stat.h:49-55)."""
     rank, world, local, dist = dist_setup(args.gpus)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from refpy import LIB_PATH, Reference
     w = make(args.workload)
-    per_step = max(1, args.ref_ticks)
-    vals = []
-    base = None
+    if not os.path.exists(LIB_PATH):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpsphray_ref.so not built "
+                          "(it is compiled from the reference sources by oracle/Makefile)"}), flush=True)
+        return
+    from psphray_b200.api import RATES_HUI
+    threads = os.cpu_count()
+    # isothermal solver: the reference's non-isothermal one traps on the
+    # log-normal field (solve.c:137-139); the clock below excludes the solver
+    ref = Reference(RATES_HUI, w.field.units, isothermal=True, threads=threads)
+    ref.load(w.field)
+    ref.build_tree(8)
+    per = args.ref_ticks or REF_TICKS[args.workload]
+    tick = 0
+    hits = clock = 0.0
     for k in range(args.warmup + args.steps):
-        b = cpu_baseline_reference(w, seconds=1e9, ticks=per_step) if base is None else None
-        if base is None:
-            base = b
-        vals.append(b["value"] if b else base["value"])
-    v = base["value"]
+        ref.reset_stats()
+        for _ in range(per):
+            tick += 1
+            ref.tick(w.schedule.rays_for_tick(tick), tick, w.tick_time)
+        st = ref.stats()
+        if k >= args.warmup:
+            hits += st["hits"]
+            clock += st["raytrace_time"] + st["deposit_time"]
+    v = hits / clock
+    base = {"value": v, "unit": "hits/s", "cores": threads, "kind": "reference",
+            "sample": f"{args.steps} steps x {per} ticks x {w.schedule.nray} rays of {args.workload}, "
+                      f"trace+deposit clock, {hits:.0f} hits"}
     line = {"impl": "reference", "metric": "ray-particle hits/s", "value": v, "unit": "hits/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload},
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": clock / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "ticks_per_step": per},
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": "hits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -207,10 +244,10 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="iliev64")
+    ap.add_argument("--workload", default="lognormal128")
     ap.add_argument("--ticks", type=int, default=0, help="ticks per step (default per workload)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-ticks", type=int, default=10)
+    ap.add_argument("--ref-ticks", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -274,16 +311,7 @@ def main():
             kn[k] += st["kernel_launches"][k]
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
-    t_local = total_ms / 1e3
-    if dist:
-        t = torch.tensor([t_local], device=f"cuda:{dev}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-        h = torch.tensor([hits], device=f"cuda:{dev}", dtype=torch.float64)
-        dist.all_reduce(h)
-        hits_all = float(h.item())
-    else:
-        t_max, hits_all = t_local, hits
+    t_max, hits_all = reduce_over_ranks(total_ms / 1e3, hits, dist, torch.device("cuda", dev))
     value = hits_all / t_max
     sim_myr = args.steps * T * w.tick_time / w.field.units.MYR
     ctx.set_timing(False)
@@ -303,14 +331,7 @@ def main():
         lam = ctx.state()["lambdaH"]
         e2e_hits += st["hits"]
     torch.cuda.synchronize(dev)
-    e2e_t = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_t], device=f"cuda:{dev}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
-        h = torch.tensor([e2e_hits], device=f"cuda:{dev}", dtype=torch.float64)
-        dist.all_reduce(h)
-        e2e_hits = float(h.item())
+    e2e_t, e2e_hits = reduce_over_ranks(time.perf_counter() - t0, e2e_hits, dist, torch.device("cuda", dev))
 
     # roofline of the dominant kernel group
     peak, peak_kind = peaks()

@@ -131,18 +131,21 @@ __device__ __forceinline__ double riccati_step(double lam0, double a, double b, 
 
 struct RhsCtx {
 	double yeMET, g, heat, time, nH, T;
+	double g_rate, heat_rate;    // g/time and heat/time, constant over the step
+	double T_num;                // MPROTON_OVER_BOLTZMANN*2/3: T = T_num*ie/(hemf/4+hmf+hmf*ye)
 };
 
-// function() solve.c:76-141, hydrogen-only branch.
+// function() solve.c:76-141, hydrogen-only branch (used inside the
+// integrator, where the last bit of T does not matter: T takes one division).
 __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const double x[2], double dx[2]) {
 	const double xHI = x[0], xHII = 1.0 - x[0];
 	const double ye = xHII + P.he_e + cx.yeMET;
-	const double T = P.isothermal ? cx.T : ieye2T(P, x[1], ye);
+	const double T = P.isothermal ? cx.T : cx.T_num * x[1] / (P.hemf * 0.25 + P.hmf + P.hmf * ye);
 	const RateAt R = rates_at(P, log10(T));
 	const double nH = cx.nH;
 	const double gamma = R(PSG_AR_HI_CI) * nH;
 	const double alpha = R(P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A) * nH;
-	dx[0] = (-cx.g / cx.time + (-gamma * ye * xHI + alpha * ye * xHII)) * cx.time;
+	dx[0] = (-cx.g_rate + ye * (alpha * xHII - gamma * xHI)) * cx.time;
 	if (P.isothermal || P.adiabatic) {
 		dx[1] = 0.0;
 	} else {
@@ -151,8 +154,8 @@ __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const
 		const double zeta = R(PSG_AR_HI_CIC) * nH;
 		const double beta = R(PSG_AR_E_BREMC) * nH;
 		const double chi = R(PSG_AR_E_COMPC);
-		const double L = P.H_PER_MASS * ((zeta + psi) * ye * xHI + eta * ye * xHII + beta * ye * xHII + chi * ye);
-		dx[1] = (cx.heat / cx.time - L) * cx.time;
+		const double L = P.H_PER_MASS * ye * ((zeta + psi) * xHI + (eta + beta) * xHII + chi);
+		dx[1] = (cx.heat_rate - L) * cx.time;
 	}
 }
 
@@ -205,9 +208,9 @@ __device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2],
 			x[0] = yn[0]; x[1] = yn[1];
 			k1[0] = k7[0]; k1[1] = k7[1];
 		}
-		double fac = err > 0 ? 0.9 * pow(err, -0.2) : 5.0;
-		fac = fmin(5.0, fmax(0.2, fac));
-		h = fmax(h * fac, 1e-14);
+		// step-size control needs no double precision
+		const float fac = err > 0.0 ? fminf(5.0f, fmaxf(0.2f, 0.9f * __powf((float)err, -0.2f))) : 5.0f;
+		h = fmax(h * (double)fac, 1e-14);
 	}
 	return t >= 1.0;
 }
@@ -245,7 +248,7 @@ __device__ inline uint32_t solve_step(const PhysParams &P, double &lambdaH, doub
 		const double c = time * alpha * (1.0 + m) - g;
 		lambdaH = riccati_step(lambdaH, a, b, q, c, g);
 	} else {
-		RhsCtx cx{yeMET, g, heat, time, nH, T};
+		RhsCtx cx{yeMET, g, heat, time, nH, T, g / time, heat / time, P.MPROTON_OVER_BOLTZMANN * 2.0 / 3.0};
 		double x[2] = {lambdaH, ie};
 		if (!dopri(P, cx, x, 200000)) st |= PSG_ST_SOLVER;
 		lambdaH = x[0];
