@@ -328,7 +328,7 @@ def main():
         s = args.warmup + i
         rays = np.frombuffer(pr.numpy(), dtype=RAY_DTYPE)
         st = ctx.run_ticks(rays, R, T, 1 + (nsteps + i) * T, w.tick_time)
-        lam = ctx.state()["lambdaH"]
+        lam = ctx.lambdaH()
         e2e_hits += st["hits"]
     torch.cuda.synchronize(dev)
     e2e_t, e2e_hits = reduce_over_ranks(time.perf_counter() - t0, e2e_hits, dist, torch.device("cuda", dev))
@@ -365,7 +365,7 @@ def main():
             "clocks": clk,
             "e2e": {"value": e2e_hits / e2e_t, "unit": "hits/s",
                     "h2d_bytes_per_step": int(host_rays[0].nbytes),
-                    "d2h_bytes_per_step": int(24 * w.field.n)}}
+                    "d2h_bytes_per_step": int(lam.nbytes)}}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_reference(make(args.workload), seconds=args.cpu_seconds)
     if rank == 0:

@@ -338,6 +338,12 @@ class Context:
                                         lh.ctypes.data), "psg_get_state")
         return dict(lambdaH=lam, ie=ie, hits=hits, lasthit=lh)
 
+    def lambdaH(self) -> np.ndarray:
+        """x_HI of every particle (the result a tick produces)."""
+        lam = np.zeros(self.n)
+        self._check(lib().psg_get_state(self.h, lam.ctypes.data, None, None, None), "psg_get_state")
+        return lam
+
     def set_state(self, lambdaH=None, ie=None, lasthit=None):
         keep = [None if lambdaH is None else np.ascontiguousarray(lambdaH, np.float64),
                 None if ie is None else np.ascontiguousarray(ie, np.float32),

@@ -95,7 +95,7 @@ void *psg_scratch(psg_context *ctx, int slot, size_t bytes);
 // scratch slots
 enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
-	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST
+	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD
 };
 
 // Per-launch timing: mark_begin/mark_end bracket a group of launches of one

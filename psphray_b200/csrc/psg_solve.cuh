@@ -135,6 +135,16 @@ struct RhsCtx {
 	double T_num;                // MPROTON_OVER_BOLTZMANN*2/3: T = T_num*ie/(hemf/4+hmf+hmf*ye)
 };
 
+__device__ __forceinline__ RhsCtx make_rhs_ctx(const PhysParams &P, double yeMET, double g, double heat,
+		double time, double nH, double T) {
+	RhsCtx c;
+	c.yeMET = yeMET; c.g = g; c.heat = heat; c.time = time; c.nH = nH; c.T = T;
+	c.g_rate = g / time;
+	c.heat_rate = heat / time;
+	c.T_num = P.MPROTON_OVER_BOLTZMANN * 2.0 / 3.0;
+	return c;
+}
+
 // function() solve.c:76-141, hydrogen-only branch (used inside the
 // integrator, where the last bit of T does not matter: T takes one division).
 __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const double x[2], double dx[2]) {
@@ -159,60 +169,89 @@ __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const
 	}
 }
 
-// Adaptive Dormand-Prince 5(4); returns false if the step limit is reached.
-__device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2], int max_steps) {
+// Adaptive Dormand-Prince 5(4) over s in [0,1]. LSODA runs the reference at
+// rtol 1e-4 (solve.c:151-152); 1e-6 here. The state of one integration is a
+// DPState; dp_init() evaluates the first derivative and picks the first step
+// (about a 1% change of each component, components near zero measured
+// against atol/rtol), dp_step() attempts one step.
+struct DPState {
+	double x[2], k1[2];
+	double t, h;
+	int steps;
+};
+
+#define DP_RTOL 1e-6
+#define DP_ATOL0 1e-10
+#define DP_ATOL1_REL 1e-8
+
+__device__ __forceinline__ void dp_init(const PhysParams &P, const RhsCtx &cx, DPState &S) {
+	rhs(P, cx, S.x, S.k1);
+	S.t = 0.0;
+	S.steps = 0;
+	double h = 1.0;
+	const double atol1 = DP_ATOL1_REL * fabs(S.x[1]) + 1e-300;
+	for (int i = 0; i < 2; i++) {
+		const double scale = fabs(S.x[i]) + (i == 0 ? DP_ATOL0 : atol1) / DP_RTOL;
+		const double f = fabs(S.k1[i]);
+		if (f > 0.0) h = fmin(h, 0.01 * scale / f);
+	}
+	S.h = fmax(h, 1e-8);
+}
+
+// One attempted step; returns true once s = 1 is reached.
+__device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, DPState &S, double atol1) {
 	const double a21 = 1. / 5, a31 = 3. / 40, a32 = 9. / 40, a41 = 44. / 45, a42 = -56. / 15, a43 = 32. / 9;
 	const double a51 = 19372. / 6561, a52 = -25360. / 2187, a53 = 64448. / 6561, a54 = -212. / 729;
 	const double a61 = 9017. / 3168, a62 = -355. / 33, a63 = 46732. / 5247, a64 = 49. / 176, a65 = -5103. / 18656;
 	const double b1 = 35. / 384, b3 = 500. / 1113, b4 = 125. / 192, b5 = -2187. / 6784, b6 = 11. / 84;
 	const double e1 = 71. / 57600, e3 = -71. / 16695, e4 = 71. / 1920, e5 = -17253. / 339200, e6 = 22. / 525, e7 = -1. / 40;
-	// LSODA runs the reference at rtol 1e-4 (solve.c:151-152); 1e-6 here
-	const double rtol = 1e-6;
-	const double atol0 = 1e-10, atol1 = 1e-8 * fabs(x[1]) + 1e-300;
-	double t = 0.0;
-	double k1[2], k2[2], k3[2], k4[2], k5[2], k6[2], k7[2], y[2], yn[2];
-	rhs(P, cx, x, k1);
-	// first step from the derivatives: about a 1% change of each component
-	// (components near zero measured against atol/rtol)
-	double h = 1.0;
+	double h = S.h;
+	if (S.t + h > 1.0) h = 1.0 - S.t;
+	double k2[2], k3[2], k4[2], k5[2], k6[2], k7[2], y[2], yn[2];
+	const double *x = S.x, *k1 = S.k1;
+	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a21 * k1[i]);
+	rhs(P, cx, y, k2);
+	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a31 * k1[i] + a32 * k2[i]);
+	rhs(P, cx, y, k3);
+	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+	rhs(P, cx, y, k4);
+	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i] + a54 * k4[i]);
+	rhs(P, cx, y, k5);
+	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i] + a64 * k4[i] + a65 * k5[i]);
+	rhs(P, cx, y, k6);
+	for (int i = 0; i < 2; i++) yn[i] = x[i] + h * (b1 * k1[i] + b3 * k3[i] + b4 * k4[i] + b5 * k5[i] + b6 * k6[i]);
+	rhs(P, cx, yn, k7);
+	double err = 0.0;
 	for (int i = 0; i < 2; i++) {
-		const double scale = fabs(x[i]) + (i == 0 ? atol0 : atol1) / rtol;
-		const double f = fabs(k1[i]);
-		if (f > 0.0) h = fmin(h, 0.01 * scale / f);
+		const double e = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i] + e6 * k6[i] + e7 * k7[i]);
+		const double sc = (i == 0 ? DP_ATOL0 : atol1) + DP_RTOL * fmax(fabs(x[i]), fabs(yn[i]));
+		err += (e / sc) * (e / sc);
 	}
-	h = fmax(h, 1e-8);
-	for (int it = 0; it < max_steps; it++) {
-		if (t >= 1.0) return true;
-		if (t + h > 1.0) h = 1.0 - t;
-		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a21 * k1[i]);
-		rhs(P, cx, y, k2);
-		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a31 * k1[i] + a32 * k2[i]);
-		rhs(P, cx, y, k3);
-		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
-		rhs(P, cx, y, k4);
-		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i] + a54 * k4[i]);
-		rhs(P, cx, y, k5);
-		for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i] + a64 * k4[i] + a65 * k5[i]);
-		rhs(P, cx, y, k6);
-		for (int i = 0; i < 2; i++) yn[i] = x[i] + h * (b1 * k1[i] + b3 * k3[i] + b4 * k4[i] + b5 * k5[i] + b6 * k6[i]);
-		rhs(P, cx, yn, k7);
-		double err = 0.0;
-		for (int i = 0; i < 2; i++) {
-			const double e = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i] + e6 * k6[i] + e7 * k7[i]);
-			const double sc = (i == 0 ? atol0 : atol1) + rtol * fmax(fabs(x[i]), fabs(yn[i]));
-			err += (e / sc) * (e / sc);
-		}
-		err = sqrt(0.5 * err);
-		if (err <= 1.0) {
-			t += h;
-			x[0] = yn[0]; x[1] = yn[1];
-			k1[0] = k7[0]; k1[1] = k7[1];
-		}
-		// step-size control needs no double precision
-		const float fac = err > 0.0 ? fminf(5.0f, fmaxf(0.2f, 0.9f * __powf((float)err, -0.2f))) : 5.0f;
-		h = fmax(h * (double)fac, 1e-14);
+	err = sqrt(0.5 * err);
+	if (err <= 1.0) {
+		S.t += h;
+		S.x[0] = yn[0]; S.x[1] = yn[1];
+		S.k1[0] = k7[0]; S.k1[1] = k7[1];
 	}
-	return t >= 1.0;
+	// step-size control needs no double precision
+	const float fac = err > 0.0 ? fminf(5.0f, fmaxf(0.2f, 0.9f * __powf((float)err, -0.2f))) : 5.0f;
+	S.h = fmax(h * (double)fac, 1e-14);
+	S.steps++;
+	return S.t >= 1.0;
+}
+
+// Whole integration on one thread; returns false if the step limit is reached.
+__device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2], int max_steps) {
+	DPState S;
+	S.x[0] = x[0];
+	S.x[1] = x[1];
+	const double atol1 = DP_ATOL1_REL * fabs(x[1]) + 1e-300;
+	dp_init(P, cx, S);
+	bool done = false;
+	while (!done && S.steps < max_steps) done = dp_step(P, cx, S, atol1);
+	x[0] = S.x[0];
+	x[1] = S.x[1];
+	return done;
 }
 
 // Isothermal step only (the closed form), for the kernels specialised on it.
@@ -248,7 +287,7 @@ __device__ inline uint32_t solve_step(const PhysParams &P, double &lambdaH, doub
 		const double c = time * alpha * (1.0 + m) - g;
 		lambdaH = riccati_step(lambdaH, a, b, q, c, g);
 	} else {
-		RhsCtx cx{yeMET, g, heat, time, nH, T, g / time, heat / time, P.MPROTON_OVER_BOLTZMANN * 2.0 / 3.0};
+		RhsCtx cx = make_rhs_ctx(P, yeMET, g, heat, time, nH, T);
 		double x[2] = {lambdaH, ie};
 		if (!dopri(P, cx, x, 200000)) st |= PSG_ST_SOLVER;
 		lambdaH = x[0];

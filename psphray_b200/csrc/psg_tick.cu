@@ -17,6 +17,7 @@
 //     and advances (lambdaH, ie) by the step since its last hit.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <vector>
 
 #include "psg_internal.cuh"
@@ -109,15 +110,6 @@ __global__ void k_tick_bounds(int nticks, int shift, const KT *__restrict__ act_
 	}
 	tick_act[t] = lo;
 	if (t == nticks) act_seg[nact] = nhit;
-}
-
-__device__ __forceinline__ double warp_incl_sum(double v, int lane) {
-#pragma unroll
-	for (int o = 1; o < 32; o <<= 1) {
-		const double u = __shfl_up_sync(0xffffffffu, v, o);
-		if (lane >= o) v += u;
-	}
-	return v;
 }
 
 __device__ __forceinline__ bool below_cutoff(double TM, double Nph) {
@@ -276,7 +268,7 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 #define DEP_THREADS 512
 #define DEP_LONG 96
 
-__global__ void __launch_bounds__(DEP_THREADS) k_deposit(const psg_ray *__restrict__ rays,
+__global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__restrict__ rays,
 		const uint32_t *__restrict__ long_rays, int nlong, const uint32_t *__restrict__ short_rays, int nshort,
 		const int64_t *__restrict__ off, const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
 		const uint32_t *__restrict__ slot, const double *__restrict__ lambdaH, const float *__restrict__ mass,
@@ -411,6 +403,127 @@ __global__ void __launch_bounds__(256) k_update(int t, const int32_t *__restrict
 	}
 	lasthit[p] = tick;
 	hits[p] += nh;
+	if (st) atomicOr(status, st);
+}
+
+// Per-particle sums of one tick's deposits (photons/NH, heat, deposit count),
+// in slot order; segments longer than a warp are summed by the whole warp.
+__global__ void __launch_bounds__(256) k_reduce_acc(int t, const int32_t *__restrict__ tick_act,
+		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
+		const double *__restrict__ acc, const double *__restrict__ acc_heat, int want_heat,
+		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat) {
+	const int lo = tick_act[t], hi = tick_act[t + 1];
+	const int lane = threadIdx.x & 31;
+	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
+	const bool mine = a < hi;
+	if (__all_sync(0xffffffffu, !mine)) return;
+	uint32_t s0 = 0, s1 = 0;
+	if (mine) { s0 = act_seg[a]; s1 = act_seg[a + 1]; }
+	double g = 0.0, heat = 0.0;
+	int nh = 0;
+	const bool longseg = mine && (s1 - s0) > 32;
+	if (mine && !longseg) {
+		for (uint32_t k = s0; k < s1; k++) {
+			const double d = acc[k];
+			if (d >= 0.0) { g += d; if (want_heat) heat += acc_heat[k]; nh++; }
+		}
+	}
+	unsigned lm = __ballot_sync(0xffffffffu, longseg);
+	while (lm) {
+		const int l = __ffs(lm) - 1;
+		lm &= lm - 1;
+		const uint32_t b0 = __shfl_sync(0xffffffffu, s0, l), b1 = __shfl_sync(0xffffffffu, s1, l);
+		double sg = 0.0, sh = 0.0;
+		int sn = 0;
+		uint32_t k = b0 + lane;
+		for (; k + 7 * 32 < b1; k += 8 * 32) {
+			double v[8];
+#pragma unroll
+			for (int u = 0; u < 8; u++) v[u] = acc[k + 32 * u];
+#pragma unroll
+			for (int u = 0; u < 8; u++)
+				if (v[u] >= 0.0) { sg += v[u]; if (want_heat) sh += acc_heat[k + 32 * u]; sn++; }
+		}
+		for (; k < b1; k += 32) {
+			const double d = acc[k];
+			if (d >= 0.0) { sg += d; if (want_heat) sh += acc_heat[k]; sn++; }
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			sg += __shfl_xor_sync(0xffffffffu, sg, o);
+			sh += __shfl_xor_sync(0xffffffffu, sh, o);
+			sn += __shfl_xor_sync(0xffffffffu, sn, o);
+		}
+		if (lane == l) { g = sg; heat = sh; nh = sn; }
+	}
+	if (!mine) return;
+	act_g[a] = g;
+	act_heat[a] = heat;
+	hits[act_ipar[a]] += nh;
+}
+
+// update_pars() loop.c:653-770, not isothermal: every lane integrates one
+// particle at a time with the Dormand-Prince step; a lane whose particle is
+// done takes the next one of the tick from a shared cursor, so the warp keeps
+// all lanes on integrator steps (particles need 1 to a few hundred steps).
+#define UPD_MAX_STEPS 200000
+__global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__restrict__ tick_act,
+		const uint32_t *__restrict__ act_ipar, const double *__restrict__ act_g,
+		const double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
+		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
+		PhysParams P, int64_t tick, double tick_time, unsigned *__restrict__ cursor,
+		uint32_t *__restrict__ status) {
+	const int lo = tick_act[t], hi = tick_act[t + 1];
+	const unsigned n = (unsigned)(hi - lo);
+	const int lane = threadIdx.x & 31;
+	const unsigned lt_mask = (1u << lane) - 1u;
+	DPState S;
+	RhsCtx cx;
+	double atol1 = 0.0;
+	uint32_t p = 0;
+	bool have = false, drained = false;
+	uint32_t st = 0;
+	for (;;) {
+		const unsigned need = __ballot_sync(0xffffffffu, !have);
+		if (need && !drained) {
+			unsigned base = 0;
+			if (lane == 0) base = atomicAdd(cursor, (unsigned)__popc(need));
+			base = __shfl_sync(0xffffffffu, base, 0);
+			if (base + __popc(need) >= n) drained = true;
+			if (!have) {
+				const unsigned k = base + __popc(need & lt_mask);
+				if (k < n) {
+					const int a = lo + (int)k;
+					p = act_ipar[a];
+					const double time = rn_dmul((double)(tick - lasthit[p]), tick_time);
+					const double lam0 = lambdaH[p];
+					const double ie0 = (double)ie[p];
+					const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, lam0), P.he_e));
+					const double nH = rn_dmul(P.H_PER_MASS, (double)rho[p]);
+					cx = make_rhs_ctx(P, (double)yeMET[p], act_g[a], act_heat[a], time, nH, T);
+					S.x[0] = lam0;
+					S.x[1] = ie0;
+					atol1 = DP_ATOL1_REL * fabs(ie0) + 1e-300;
+					dp_init(P, cx, S);
+					have = true;
+				}
+			}
+		}
+		if (!__any_sync(0xffffffffu, have)) break;
+		if (have) {
+			const bool done = dp_step(P, cx, S, atol1);
+			if (done || S.steps >= UPD_MAX_STEPS) {
+				if (!done) st |= PSG_ST_SOLVER;
+				const double lam = S.x[0], e = S.x[1];
+				if (!(e >= 0.0)) st |= PSG_ST_IE_NEG;
+				if (!isfinite(lam) || !isfinite(e)) st |= PSG_ST_NAN;
+				lambdaH[p] = fmin(1.0, fmax(0.0, lam));
+				if (!P.adiabatic) ie[p] = (float)e;
+				lasthit[p] = tick;
+				have = false;
+			}
+		}
+	}
 	if (st) atomicOr(status, st);
 }
 
@@ -579,6 +692,20 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	k_ray_lists<<<blocks(nray, 256), 256, 0, st>>>(nray, is_long, long_scan, long_rays, short_rays);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 2;
+	// non-isothermal: per-particle sums and the integrator's work cursors
+	double *act_g = nullptr, *act_heat = nullptr;
+	unsigned *cursors = nullptr;
+	int dev_sms = 148;
+	cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+	if (!ctx->flags.isothermal) {
+		const size_t na = (size_t)(h_tick_act[K] > 0 ? h_tick_act[K] : 1);
+		char *m = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * (K + 1) + 256);
+		if (!m) return PSG_E_NOMEM;
+		act_g = (double *)m;
+		act_heat = act_g + na;
+		cursors = (unsigned *)(act_heat + na);
+		PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * (K + 1), st));
+	}
 	for (size_t t = 0; t < K; t++) {
 		const int l0 = h_scan[t * R];
 		const int l1 = (t + 1 < K) ? h_scan[(t + 1) * R] : nlong_all;
@@ -599,10 +726,16 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 				k_update<true><<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
 						acc_heat, want_heat, ctx->d_lambdaH, ctx->d_ie, ctx->d_hits, ctx->d_lasthit, ctx->d_rho,
 						ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, ctx->d_status);
-			else
-				k_update<false><<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
-						acc_heat, want_heat, ctx->d_lambdaH, ctx->d_ie, ctx->d_hits, ctx->d_lasthit, ctx->d_rho,
-						ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, ctx->d_status);
+			else {
+				k_reduce_acc<<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat,
+						want_heat, ctx->d_hits, act_g, act_heat);
+				PSG_CHECK_LAUNCH();
+				const unsigned qgrid = (unsigned)std::min<size_t>(blocks(nact_t, 256), (size_t)dev_sms * 8);
+				k_update_queue<<<qgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_g, act_heat, ctx->d_lambdaH,
+						ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time,
+						cursors + t, ctx->d_status);
+				ctx->launches++;
+			}
 			PSG_CHECK_LAUNCH();
 			ctx->launches++;
 		}

@@ -227,3 +227,28 @@ def test_capped_deposits_vs_oracle(gpu_ctx, phys):
     gs = gpu_ctx.state()
     assert np.array_equal(gs["hits"], orc.hits)
     assert np.max(np.abs(gs["lambdaH"] - orc.lambdaH)) < 1e-9
+
+
+def test_ticks_noniso_vs_oracle(gpu_ctx, phys_noniso):
+    """Not isothermal, 8-bin blackbody rays (photo-heating on): 6 ticks on
+    the log-normal field through the work-queue integrator against the
+    restatement's tight integration; counters exact, state to the
+    integrator's tolerance."""
+    from psphray_b200 import fields
+    w = fields.make_workload("lognormal128", n_side=16, nray=64, seed=21)
+    f = w.field
+    _gpu(gpu_ctx, f, phys_noniso)
+    orc = Oracle(f, phys_noniso, isothermal=False)
+    orc.build_tree(8)
+    rays = w.schedule.rays_for_ticks(1, 6)
+    assert np.any(rays["freq"] > 13.7 * f.units.EV)
+    gpu_ctx.run_ticks(rays[:3 * 64], 64, 3, 1, w.tick_time)
+    gpu_ctx.run_ticks(rays[3 * 64:], 64, 3, 4, w.tick_time)
+    for k in range(6):
+        assert orc.tick(rays[k * 64:(k + 1) * 64], k + 1, w.tick_time)["rc"] == 0
+    gs = gpu_ctx.state()
+    assert np.array_equal(gs["lasthit"], orc.lasthit)
+    assert np.array_equal(gs["hits"], orc.hits)
+    assert np.max(np.abs(gs["lambdaH"] - orc.lambdaH)) < 1e-4
+    assert np.max(np.abs(gs["ie"] - orc.ie) / orc.ie) < 1e-4
+    assert np.max(np.abs(gs["ie"] - f.ie) / f.ie) > 1e-3     # the gas did heat or cool
