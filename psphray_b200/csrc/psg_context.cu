@@ -74,9 +74,9 @@ static void free_particles(psg_context *ctx) {
 }
 
 static void free_tree(psg_context *ctx) {
-	void *ptrs[] = {ctx->d_cell_lo, ctx->d_cell_hi, ctx->d_leaf_psml, ctx->d_leaf_idx};
+	void *ptrs[] = {ctx->d_cell_lo, ctx->d_cell_hi, ctx->d_wide_lo, ctx->d_wide_hi, ctx->d_leaf_psml, ctx->d_leaf_idx};
 	for (void *p : ptrs) if (p) cudaFree(p);
-	ctx->d_cell_lo = ctx->d_cell_hi = ctx->d_leaf_psml = nullptr;
+	ctx->d_cell_lo = ctx->d_cell_hi = ctx->d_wide_lo = ctx->d_wide_hi = ctx->d_leaf_psml = nullptr;
 	ctx->d_leaf_idx = nullptr;
 	ctx->have_tree = 0;
 }

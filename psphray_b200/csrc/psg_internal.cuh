@@ -20,6 +20,7 @@
 #define PSG_ST_NAN 1u          // NaN/inf reached a particle state
 #define PSG_ST_SOLVER 2u       // the general integrator hit its step limit
 #define PSG_ST_IE_NEG 4u       // internal energy would turn negative (solve.c:137-139)
+#define PSG_ST_STACK 8u        // traversal stack overflow
 
 struct psg_buf {
 	void *p = nullptr;
@@ -61,6 +62,8 @@ struct psg_context {
 	int depth = 0;
 	float4 *d_cell_lo = nullptr;  // bot.xyz, w = index past the subtree (int bits)
 	float4 *d_cell_hi = nullptr;  // top.xyz, w = first particle in leaf order (int bits)
+	float4 *d_wide_lo = nullptr;  // level order (siblings contiguous): bot.xyz, w = first child or -1-count
+	float4 *d_wide_hi = nullptr;  // top.xyz, w = first particle in leaf order
 	float4 *d_leaf_psml = nullptr; // particles in leaf order
 	uint32_t *d_leaf_idx = nullptr; // caller index, PSG_INVALID_BIT if flagged
 

@@ -63,8 +63,19 @@ __device__ __forceinline__ RayGeom load_ray(const psg_ray *__restrict__ rays, si
 
 // The line test of raytrace.c:168-195: float differences and products,
 // double sums; accepted iff sml^2 >= (dc - proj)(dc + proj).
+// Candidates that miss by a wide margin are rejected in float first: the
+// float estimate r2f = d2f - projf^2 carries at most ~12 roundings of
+// relative size 2^-24 of d2 (about 7.2e-7 d2), so r2f - sml^2 > 1e-5 d2f
+// guarantees the exact test rejects too; everything closer takes the exact
+// double path, so the accepted set is the reference's.
 __device__ __forceinline__ bool line_hits_particle(const RayGeom &g, float4 q, double &dc, double &r2) {
 	const float dx = rn_fsub(q.x, g.s[0]), dy = rn_fsub(q.y, g.s[1]), dz = rn_fsub(q.z, g.s[2]);
+	{
+		const float pf = __fadd_rn(__fadd_rn(rn_fmul(dx, g.dir[0]), rn_fmul(dy, g.dir[1])), rn_fmul(dz, g.dir[2]));
+		const float d2f = __fadd_rn(__fadd_rn(rn_fmul(dx, dx), rn_fmul(dy, dy)), rn_fmul(dz, dz));
+		const float r2f = __fsub_rn(d2f, rn_fmul(pf, pf));
+		if (__fsub_rn(r2f, rn_fmul(q.w, q.w)) > 1e-5f * d2f) return false;
+	}
 	double proj = (double)rn_fmul(dx, g.dir[0]);
 	proj = rn_dadd(proj, (double)rn_fmul(dy, g.dir[1]));
 	proj = rn_dadd(proj, (double)rn_fmul(dz, g.dir[2]));
@@ -164,6 +175,131 @@ __global__ void __launch_bounds__(128) k_trace_warp(const psg_ray *__restrict__ 
 		i = max(i + 32, __shfl_sync(0xffffffffu, m, 31));
 	}
 	if (lane == 0) count[r] = nh;
+}
+
+// Candidates listed in shared memory (leaf-order particle positions), tested
+// 32 at a time; accepted hits go to the ray's slab in order of discovery.
+__device__ __forceinline__ void test_candidates(const RayGeom &g, const int *list, int total,
+		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx, size_t r, size_t scap,
+		uint32_t *__restrict__ slab_ipar, double *__restrict__ slab_d, double *__restrict__ slab_b,
+		uint32_t &nh, int lane, unsigned lt_mask) {
+	for (int k0 = 0; k0 < total; k0 += 32) {
+		const int k = k0 + lane;
+		bool acc = false;
+		double dc = 0.0, r2 = 0.0;
+		uint32_t idx = 0;
+		if (k < total) {
+			const int p = list[k];
+			idx = __ldg(&lidx[p]);
+			if (!(idx & PSG_INVALID_BIT)) acc = line_hits_particle(g, __ldg(&lpsml[p]), dc, r2);
+		}
+		const unsigned bal = __ballot_sync(0xffffffffu, acc);
+		if (acc) {
+			const size_t q = nh + __popc(bal & lt_mask);
+			if (q < scap) {
+				const size_t o = r * scap + q;
+				slab_ipar[o] = idx;
+				slab_d[o] = dc;
+				slab_b[o] = __dsqrt_rn(fabs(r2));
+			}
+		}
+		nh += __popc(bal);
+	}
+}
+
+// One warp per ray over the level-order tree, whose 8 children of a cell are
+// contiguous. The warp keeps a stack (shared memory) of crossed internal
+// cells; each step pops up to 4 of them and tests their 32 children at once,
+// one per lane, with the reference's segment-box test; crossed internal
+// children are pushed, crossed leaves list their particles for the line
+// test. The cells tested are exactly the children of crossed cells, as in
+// the reference's walk (raytrace.c:160-208); only the order differs, and the
+// per-ray sort makes the output independent of it. The stack cannot exceed
+// 4 + 28 entries per tree level; TR_STACK leaves room for 21 levels and an
+// overflow would raise PSG_ST_STACK instead of losing cells.
+#define TR_STACK 1024
+#define TR_WARPS 4
+
+__global__ void __launch_bounds__(32 * TR_WARPS) k_trace_stack(const psg_ray *__restrict__ rays, size_t nray,
+		const float4 *__restrict__ wlo, const float4 *__restrict__ whi,
+		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx, int ppc,
+		uint32_t *__restrict__ count, size_t scap, uint32_t *__restrict__ slab_ipar,
+		double *__restrict__ slab_d, double *__restrict__ slab_b, uint32_t *__restrict__ status) {
+	extern __shared__ int tr_smem[];
+	const int lane = threadIdx.x & 31;
+	const int wib = threadIdx.x >> 5;
+	int *stack = tr_smem + wib * (TR_STACK + 32 * ppc);
+	int *list = stack + TR_STACK;
+	const size_t r = (size_t)blockIdx.x * TR_WARPS + wib;
+	if (r >= nray) return;
+	const RayGeom g = load_ray(rays, r);
+	const unsigned lt_mask = (1u << lane) - 1u;
+	uint32_t nh = 0;
+	int sp = 0;
+	bool overflow = false;
+	{
+		const float4 lo = __ldg(&wlo[0]), hi = __ldg(&whi[0]);
+		const float s2b[3] = {rn_fsub(lo.x, g.s[0]), rn_fsub(lo.y, g.s[1]), rn_fsub(lo.z, g.s[2])};
+		const float s2t[3] = {rn_fsub(hi.x, g.s[0]), rn_fsub(hi.y, g.s[1]), rn_fsub(hi.z, g.s[2])};
+		if (segment_hits_box(g.dir, g.dist, s2b, s2t)) {
+			const int w = __float_as_int(lo.w);
+			if (w >= 0) {
+				if (lane == 0) stack[0] = w;
+				sp = 1;
+			} else {
+				const int cnt = min(-1 - w, ppc), ps = __float_as_int(hi.w);
+				for (int k = lane; k < cnt; k += 32) list[k] = ps + k;
+				__syncwarp();
+				test_candidates(g, list, cnt, lpsml, lidx, r, scap, slab_ipar, slab_d, slab_b, nh, lane, lt_mask);
+			}
+		}
+	}
+	__syncwarp();
+	while (sp > 0) {
+		const int k = min(sp, 4);
+		const int node = lane >> 3;
+		const bool valid = node < k;
+		const int c = valid ? stack[sp - k + node] + (lane & 7) : 0;
+		__syncwarp();
+		sp -= k;
+		float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+		bool hit = false;
+		if (valid) {
+			lo = __ldg(&wlo[c]);
+			hi = __ldg(&whi[c]);
+			const float s2b[3] = {rn_fsub(lo.x, g.s[0]), rn_fsub(lo.y, g.s[1]), rn_fsub(lo.z, g.s[2])};
+			const float s2t[3] = {rn_fsub(hi.x, g.s[0]), rn_fsub(hi.y, g.s[1]), rn_fsub(hi.z, g.s[2])};
+			hit = segment_hits_box(g.dir, g.dist, s2b, s2t);
+		}
+		const int w = __float_as_int(lo.w);
+		const bool internal = hit && w >= 0;
+		const unsigned bi = __ballot_sync(0xffffffffu, internal);
+		if (internal) {
+			const int pos = sp + __popc(bi & lt_mask);
+			if (pos < TR_STACK) stack[pos] = w;
+		}
+		sp += __popc(bi);
+		if (sp > TR_STACK) { overflow = true; sp = TR_STACK; }
+		const int cnt = (hit && w < 0) ? min(-1 - w, ppc) : 0;
+		int cs = cnt;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int t = __shfl_up_sync(0xffffffffu, cs, o);
+			if (lane >= o) cs += t;
+		}
+		const int total = __shfl_sync(0xffffffffu, cs, 31);
+		if (cnt) {
+			const int ps = __float_as_int(hi.w), base = cs - cnt;
+			for (int q = 0; q < cnt; q++) list[base + q] = ps + q;
+		}
+		__syncwarp();
+		test_candidates(g, list, total, lpsml, lidx, r, scap, slab_ipar, slab_d, slab_b, nh, lane, lt_mask);
+		__syncwarp();
+	}
+	if (lane == 0) {
+		count[r] = nh;
+		if (overflow) atomicOr(status, PSG_ST_STACK);
+	}
 }
 
 // Slabs into contiguous per-ray lists (traversal order), for the library
@@ -363,10 +499,9 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	unsigned long long *d_max = ctx->d_counters + 4;
 	const int ncell = (int)ctx->ncell;
 	const int ppc = ctx->ppc;
-	const int wpb = 4;
-	const size_t smem = sizeof(int) * 32 * (size_t)ppc * wpb;
+	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ppc) * TR_WARPS;
 	if (smem > 48 * 1024)
-		PSG_CUDA(cudaFuncSetAttribute(k_trace_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		PSG_CUDA(cudaFuncSetAttribute(k_trace_stack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 	// one traversal into per-ray slabs; if a ray outgrew its slab, grow and rerun
 	size_t scap = 0;
 	unsigned long long maxcount = 0;
@@ -380,9 +515,9 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 		PSG_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st));
 		psg_mark_begin(ctx, PSG_K_TRACE_FILL);
 		if (nray) {
-			k_trace_warp<<<blocks(nray, wpb), 32 * wpb, smem, st>>>(d_rays, nray, ctx->d_cell_lo,
-					ctx->d_cell_hi, ncell, ctx->d_leaf_psml, ctx->d_leaf_idx, ppc, count, scap, slab_ipar,
-					slab_f64, slab_f64 + slots);
+			k_trace_stack<<<blocks(nray, TR_WARPS), 32 * TR_WARPS, smem, st>>>(d_rays, nray, ctx->d_wide_lo,
+					ctx->d_wide_hi, ctx->d_leaf_psml, ctx->d_leaf_idx, ppc, count, scap, slab_ipar,
+					slab_f64, slab_f64 + slots, ctx->d_status);
 			ctx->launches++;
 		}
 		PSG_CHECK_LAUNCH();
@@ -396,7 +531,13 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 		PSG_CHECK_LAUNCH();
 		ctx->launches++;
 		PSG_CUDA(cudaMemcpyAsync(&maxcount, d_max, sizeof(maxcount), cudaMemcpyDeviceToHost, st));
+		uint32_t stw = 0;
+		PSG_CUDA(cudaMemcpyAsync(&stw, ctx->d_status, sizeof(stw), cudaMemcpyDeviceToHost, st));
 		PSG_CUDA(cudaStreamSynchronize(st));
+		if (stw & PSG_ST_STACK) {
+			PSG_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), st));
+			return psg_fail(ctx, PSG_E_OVERFLOW, "trace: traversal stack overflow (tree deeper than supported)");
+		}
 		if (maxcount <= scap) break;
 		size_t want = 1024;
 		while (want < maxcount + maxcount / 4) want <<= 1;

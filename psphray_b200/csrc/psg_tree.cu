@@ -225,6 +225,19 @@ __global__ void k_emit(Cells c, int ncell, uint32_t nvalid, float4 *__restrict__
 	out_hi[i] = make_float4(z.x, z.y, z.z, __int_as_float((int)c.start[cell]));
 }
 
+// Level-order layout for the stack traversal: cells as built, the 8 children
+// of a cell contiguous. lo.w = index of the first child, or -1-count for a
+// leaf of `count` particles; hi.w = first particle of the cell (leaf order).
+__global__ void k_emit_wide(Cells c, int ncell, float4 *__restrict__ out_lo, float4 *__restrict__ out_hi) {
+	const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+	if (cell >= ncell) return;
+	const float4 a = c.lo[cell], z = c.hi[cell];
+	const int fc = c.fchild[cell];
+	const int w = fc >= 0 ? fc : -1 - (int)(c.end[cell] - c.start[cell]);
+	out_lo[cell] = make_float4(a.x, a.y, a.z, __int_as_float(w));
+	out_hi[cell] = make_float4(z.x, z.y, z.z, __int_as_float((int)c.start[cell]));
+}
+
 __global__ void k_gather_particles(size_t nvalid, const uint32_t *__restrict__ order,
 		const float4 *__restrict__ psml, const int8_t *__restrict__ flag,
 		float4 *__restrict__ lpsml, uint32_t *__restrict__ lidx) {
@@ -380,6 +393,13 @@ extern "C" int psg_build_tree(psg_context *ctx, int ppc) {
 	PSG_CUDA(cudaMalloc(&ctx->d_cell_lo, sizeof(float4) * (ncell + 1)));
 	PSG_CUDA(cudaMalloc(&ctx->d_cell_hi, sizeof(float4) * (ncell + 1)));
 	k_emit<<<blocks(ncell + 1, 256), 256, 0, st>>>(c, (int)ncell, (uint32_t)nvalid, ctx->d_cell_lo, ctx->d_cell_hi);
+	PSG_CHECK_LAUNCH();
+	if (ctx->d_wide_lo) cudaFree(ctx->d_wide_lo);
+	if (ctx->d_wide_hi) cudaFree(ctx->d_wide_hi);
+	ctx->d_wide_lo = ctx->d_wide_hi = nullptr;
+	PSG_CUDA(cudaMalloc(&ctx->d_wide_lo, sizeof(float4) * ncell));
+	PSG_CUDA(cudaMalloc(&ctx->d_wide_hi, sizeof(float4) * ncell));
+	k_emit_wide<<<blocks(ncell, 256), 256, 0, st>>>(c, (int)ncell, ctx->d_wide_lo, ctx->d_wide_hi);
 	PSG_CHECK_LAUNCH();
 	PSG_CUDA(cudaStreamSynchronize(st));
 	ctx->ncell = ncell;
