@@ -240,6 +240,78 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 	return S.t >= 1.0;
 }
 
+// Stiff finish: particles whose cooling time is far below the step make the
+// explicit method crawl. After DP_SWITCH steps such a particle continues
+// with a Rosenbrock method (the L-stable second-order W-method with
+// third-order error estimate of Shampine & Reichelt's ode23s), Jacobian by
+// finite differences, rtol RB_RTOL.
+#define DP_SWITCH 32
+#define RB_RTOL 1e-5
+
+__device__ inline bool rosenbrock(const PhysParams &P, const RhsCtx &cx, double x[2], double t, double h,
+		int max_steps) {
+	const double d = 1.0 / (2.0 + 1.4142135623730951), e32 = 6.0 + 1.4142135623730951;
+	const double atol[2] = {DP_ATOL0, DP_ATOL1_REL * fabs(x[1]) + 1e-300};
+	double F0[2];
+	rhs(P, cx, x, F0);
+	h = fmin(fmax(h, 1e-10), 1.0);
+	for (int it = 0; it < max_steps; it++) {
+		if (t >= 1.0) return true;
+		if (t + h > 1.0) h = 1.0 - t;
+		// Jacobian by forward differences
+		double J[2][2];
+		for (int j = 0; j < 2; j++) {
+			const double del = 1e-7 * fmax(fabs(x[j]), atol[j] / RB_RTOL);
+			double y[2] = {x[0], x[1]}, Fj[2];
+			y[j] += del;
+			rhs(P, cx, y, Fj);
+			J[0][j] = (Fj[0] - F0[0]) / del;
+			J[1][j] = (Fj[1] - F0[1]) / del;
+		}
+		const double a00 = 1.0 - h * d * J[0][0], a01 = -h * d * J[0][1];
+		const double a10 = -h * d * J[1][0], a11 = 1.0 - h * d * J[1][1];
+		const double det = a00 * a11 - a01 * a10;
+		auto solve = [&](const double b[2], double out[2]) {
+			out[0] = (a11 * b[0] - a01 * b[1]) / det;
+			out[1] = (a00 * b[1] - a10 * b[0]) / det;
+		};
+		double k1[2], k2[2], k3[2], F1[2], F2[2], y[2], yn[2], b[2];
+		solve(F0, k1);
+		y[0] = x[0] + 0.5 * h * k1[0];
+		y[1] = x[1] + 0.5 * h * k1[1];
+		rhs(P, cx, y, F1);
+		b[0] = F1[0] - k1[0];
+		b[1] = F1[1] - k1[1];
+		solve(b, k2);
+		k2[0] += k1[0];
+		k2[1] += k1[1];
+		yn[0] = x[0] + h * k2[0];
+		yn[1] = x[1] + h * k2[1];
+		rhs(P, cx, yn, F2);
+		b[0] = F2[0] - e32 * (k2[0] - F1[0]) - 2.0 * (k1[0] - F0[0]);
+		b[1] = F2[1] - e32 * (k2[1] - F1[1]) - 2.0 * (k1[1] - F0[1]);
+		solve(b, k3);
+		double err = 0.0;
+		for (int i = 0; i < 2; i++) {
+			const double e = h / 6.0 * (k1[i] - 2.0 * k2[i] + k3[i]);
+			const double sc = atol[i] + RB_RTOL * fmax(fabs(x[i]), fabs(yn[i]));
+			err += (e / sc) * (e / sc);
+		}
+		err = sqrt(0.5 * err);
+		if (err <= 1.0 && isfinite(err)) {
+			t += h;
+			x[0] = yn[0];
+			x[1] = yn[1];
+			F0[0] = F2[0];
+			F0[1] = F2[1];
+		}
+		const float fac = (err > 0.0 && isfinite(err))
+				? fminf(5.0f, fmaxf(0.2f, 0.9f * __powf((float)err, -1.0f / 3.0f))) : (isfinite(err) ? 5.0f : 0.2f);
+		h = fmax(h * (double)fac, 1e-14);
+	}
+	return t >= 1.0;
+}
+
 // Whole integration on one thread; returns false if the step limit is reached.
 __device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2], int max_steps) {
 	DPState S;
@@ -248,10 +320,11 @@ __device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2],
 	const double atol1 = DP_ATOL1_REL * fabs(x[1]) + 1e-300;
 	dp_init(P, cx, S);
 	bool done = false;
-	while (!done && S.steps < max_steps) done = dp_step(P, cx, S, atol1);
+	while (!done && S.steps < DP_SWITCH) done = dp_step(P, cx, S, atol1);
 	x[0] = S.x[0];
 	x[1] = S.x[1];
-	return done;
+	if (done) return true;
+	return rosenbrock(P, cx, x, S.t, S.h, max_steps);
 }
 
 // Isothermal step only (the closed form), for the kernels specialised on it.

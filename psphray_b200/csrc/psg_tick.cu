@@ -467,12 +467,16 @@ __global__ void __launch_bounds__(256) k_reduce_acc(int t, const int32_t *__rest
 // done takes the next one of the tick from a shared cursor, so the warp keeps
 // all lanes on integrator steps (particles need 1 to a few hundred steps).
 #define UPD_MAX_STEPS 200000
+struct StiffItem {
+	double t, h, x0, x1, yeMET, g, heat, time, nH, T;
+	uint32_t p;
+};
 __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const double *__restrict__ act_g,
 		const double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
 		PhysParams P, int64_t tick, double tick_time, unsigned *__restrict__ cursor,
-		uint32_t *__restrict__ status) {
+		StiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff, uint32_t *__restrict__ status) {
 	const int lo = tick_act[t], hi = tick_act[t + 1];
 	const unsigned n = (unsigned)(hi - lo);
 	const int lane = threadIdx.x & 31;
@@ -512,8 +516,15 @@ __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__re
 		if (!__any_sync(0xffffffffu, have)) break;
 		if (have) {
 			const bool done = dp_step(P, cx, S, atol1);
-			if (done || S.steps >= UPD_MAX_STEPS) {
-				if (!done) st |= PSG_ST_SOLVER;
+			if (!done && S.steps >= DP_SWITCH) {
+				// stiff: hand the particle to k_update_stiff and free the lane
+				const unsigned q = atomicAdd(nstiff, 1u);
+				StiffItem it;
+				it.p = p; it.t = S.t; it.h = S.h; it.x0 = S.x[0]; it.x1 = S.x[1];
+				it.yeMET = cx.yeMET; it.g = cx.g; it.heat = cx.heat; it.time = cx.time; it.nH = cx.nH; it.T = cx.T;
+				stiff[q] = it;
+				have = false;
+			} else if (done) {
 				const double lam = S.x[0], e = S.x[1];
 				if (!(e >= 0.0)) st |= PSG_ST_IE_NEG;
 				if (!isfinite(lam) || !isfinite(e)) st |= PSG_ST_NAN;
@@ -523,6 +534,27 @@ __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__re
 				have = false;
 			}
 		}
+	}
+	if (st) atomicOr(status, st);
+}
+
+// The stiff particles of a tick, one thread each (their number is read on
+// the device): Rosenbrock from where the explicit steps stopped.
+__global__ void __launch_bounds__(64) k_update_stiff(const StiffItem *__restrict__ stiff,
+		const unsigned *__restrict__ nstiff, double *__restrict__ lambdaH, float *__restrict__ ie,
+		int64_t *__restrict__ lasthit, PhysParams P, int64_t tick, uint32_t *__restrict__ status) {
+	const unsigned n = *nstiff;
+	uint32_t st = 0;
+	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		const StiffItem it = stiff[i];
+		const RhsCtx cx = make_rhs_ctx(P, it.yeMET, it.g, it.heat, it.time, it.nH, it.T);
+		double x[2] = {it.x0, it.x1};
+		if (!rosenbrock(P, cx, x, it.t, it.h, UPD_MAX_STEPS)) st |= PSG_ST_SOLVER;
+		if (!(x[1] >= 0.0)) st |= PSG_ST_IE_NEG;
+		if (!isfinite(x[0]) || !isfinite(x[1])) st |= PSG_ST_NAN;
+		lambdaH[it.p] = fmin(1.0, fmax(0.0, x[0]));
+		if (!P.adiabatic) ie[it.p] = (float)x[1];
+		lasthit[it.p] = tick;
 	}
 	if (st) atomicOr(status, st);
 }
@@ -694,17 +726,24 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	ctx->launches += 2;
 	// non-isothermal: per-particle sums and the integrator's work cursors
 	double *act_g = nullptr, *act_heat = nullptr;
-	unsigned *cursors = nullptr;
+	unsigned *cursors = nullptr, *nstiff = nullptr;
+	StiffItem *stiff = nullptr;
 	int dev_sms = 148;
 	cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
 	if (!ctx->flags.isothermal) {
 		const size_t na = (size_t)(h_tick_act[K] > 0 ? h_tick_act[K] : 1);
-		char *m = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * (K + 1) + 256);
+		// the stiff list of a tick can hold every particle of the tick
+		size_t maxt = 1;
+		for (size_t t = 0; t < K; t++) maxt = std::max<size_t>(maxt, (size_t)(h_tick_act[t + 1] - h_tick_act[t]));
+		char *m = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * 2 * (K + 1)
+				+ sizeof(StiffItem) * maxt + 512);
 		if (!m) return PSG_E_NOMEM;
 		act_g = (double *)m;
 		act_heat = act_g + na;
 		cursors = (unsigned *)(act_heat + na);
-		PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * (K + 1), st));
+		nstiff = cursors + (K + 1);
+		stiff = (StiffItem *)(((uintptr_t)(nstiff + K + 1) + 15) & ~(uintptr_t)15);
+		PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * 2 * (K + 1), st));
 	}
 	for (size_t t = 0; t < K; t++) {
 		const int l0 = h_scan[t * R];
@@ -733,8 +772,11 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 				const unsigned qgrid = (unsigned)std::min<size_t>(blocks(nact_t, 256), (size_t)dev_sms * 8);
 				k_update_queue<<<qgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_g, act_heat, ctx->d_lambdaH,
 						ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time,
-						cursors + t, ctx->d_status);
-				ctx->launches++;
+						cursors + t, stiff, nstiff + t, ctx->d_status);
+				PSG_CHECK_LAUNCH();
+				k_update_stiff<<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
+						P, first_tick + (int64_t)t, ctx->d_status);
+				ctx->launches += 2;
 			}
 			PSG_CHECK_LAUNCH();
 			ctx->launches++;
@@ -799,3 +841,4 @@ extern "C" int psg_step_evolve(psg_context *ctx, psg_step *steps, size_t n) {
 	PSG_CUDA(cudaStreamSynchronize(st));
 	return check_status(ctx);
 }
+
