@@ -214,6 +214,15 @@ typedef struct {
  * are updated in place (host buffer). */
 int psg_step_evolve(psg_context *ctx, psg_step *steps, size_t n);
 
+/* psg_step_evolve without any device allocation (no counterpart in the
+ * reference): the steps are staged in a fixed buffer inside the library,
+ * one per device, of PSG_NOALLOC_MAX_STEPS (16384) steps; larger n is
+ * rejected with PSG_E_INVAL. The first call on each device looks the buffer
+ * up (cudaGetSymbolAddress) and should come before any stream capture on
+ * that device. Calls that overlap in time on one device race on the buffer. */
+#define PSG_NOALLOC_MAX_STEPS 16384
+int psg_step_evolve_noalloc(psg_context *ctx, psg_step *steps, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "psg_internal.cuh"
@@ -842,3 +843,74 @@ extern "C" int psg_step_evolve(psg_context *ctx, psg_step *steps, size_t n) {
 	return check_status(ctx);
 }
 
+// ---- step_evolve without allocation -----------------------------------------
+// psg_step_evolve_noalloc stages the steps in a fixed buffer that is part of
+// the library's device image instead of the context's growable scratch, so
+// the call itself never allocates or frees device memory. It is meant for
+// hosts that cannot allocate while a time step is under way: a code whose
+// own pool allocator has already taken the device's free memory (cudaMalloc
+// would fail there), or one that must not pay the device-wide
+// synchronisation that cudaMalloc and cudaFree can imply while its other
+// streams are busy. The buffer holds PSG_NOALLOC_MAX_STEPS steps (2.25 MiB)
+// plus a status word; every device gets its own copy. There is one buffer per
+// device, not per context: calls that overlap in time on the same device
+// (two host threads, two contexts or two streams) race on it, and the caller
+// must serialise them.
+#define PSG_NOALLOC_MAX_DEVICES 64
+static constexpr size_t kNoallocStatusOffset = (size_t)PSG_NOALLOC_MAX_STEPS * sizeof(psg_step);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocStatusOffset + 256];
+
+static std::mutex g_noalloc_mutex;
+static unsigned char *g_noalloc_base[PSG_NOALLOC_MAX_DEVICES];
+
+// Device address of the static buffer on ctx->device, looked up on the first
+// call for that device (with the device current) and cached afterwards.
+static int noalloc_buffer(psg_context *ctx, unsigned char **base) {
+	if (ctx->device < 0 || ctx->device >= PSG_NOALLOC_MAX_DEVICES)
+		return psg_fail(ctx, PSG_E_INVAL, "psg_step_evolve_noalloc: device %d beyond the %d supported", ctx->device,
+				PSG_NOALLOC_MAX_DEVICES);
+	std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+	if (!g_noalloc_base[ctx->device]) {
+		void *p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		if (e != cudaSuccess || !p)
+			return psg_cuda_fail(ctx, e != cudaSuccess ? e : cudaErrorInvalidSymbol,
+					"cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+		g_noalloc_base[ctx->device] = (unsigned char *)p;
+	}
+	*base = g_noalloc_base[ctx->device];
+	return PSG_OK;
+}
+
+extern "C" int psg_step_evolve_noalloc(psg_context *ctx, psg_step *steps, size_t n) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!ctx->have_physics) return psg_fail(ctx, PSG_E_INVAL, "psg_step_evolve_noalloc: set physics first");
+	if (n > PSG_NOALLOC_MAX_STEPS)
+		return psg_fail(ctx, PSG_E_INVAL,
+				"psg_step_evolve_noalloc: %zu steps exceed its fixed buffer of %d; split the call or use "
+				"psg_step_evolve", n, PSG_NOALLOC_MAX_STEPS);
+	if (n == 0) return PSG_OK;
+	if (!steps) return psg_fail(ctx, PSG_E_INVAL, "psg_step_evolve_noalloc: null steps");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	unsigned char *base = nullptr;
+	const int rc = noalloc_buffer(ctx, &base);
+	if (rc) return rc;
+	psg_step *d = (psg_step *)base;
+	uint32_t *d_status = (uint32_t *)(base + kNoallocStatusOffset);
+	cudaStream_t st = ctx->stream;
+	// the status word is OR-ed into by the kernel: it must start at zero
+	PSG_CUDA(cudaMemsetAsync(d_status, 0, sizeof(uint32_t), st));
+	PSG_CUDA(cudaMemcpyAsync(d, steps, sizeof(psg_step) * n, cudaMemcpyHostToDevice, st));
+	k_step_evolve<<<blocks(n, 128), 128, 0, st>>>(d, n, psg_phys_params(ctx), d_status);
+	PSG_CHECK_LAUNCH();
+	PSG_CUDA(cudaMemcpyAsync(steps, d, sizeof(psg_step) * n, cudaMemcpyDeviceToHost, st));
+	uint32_t status = 0;
+	PSG_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
+	if (status)
+		return psg_fail(ctx, PSG_E_DEVICE, "device status 0x%x:%s%s%s", status,
+				(status & PSG_ST_NAN) ? " non-finite state" : "",
+				(status & PSG_ST_SOLVER) ? " integrator step limit" : "",
+				(status & PSG_ST_IE_NEG) ? " negative internal energy" : "");
+	return PSG_OK;
+}
