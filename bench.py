@@ -38,8 +38,16 @@ sys.path.insert(0, ROOT)
 
 DEFAULT_TICKS = {"iliev32": 400, "iliev64": 100, "lognormal128": 8}
 REF_TICKS = {"iliev32": 40, "iliev64": 4, "lognormal128": 1}   # per step of --impl reference
-BYTES_PER_HIT = 36       # pos 12 + sml 4 + lambdaH 8 + mass 4 + FP64 absorbed photons 8
-BYTES_PER_HIT_TRACE = 36  # trace fill: pos+sml 16 read, (ipar 4, d 8, b 8) written
+# Algorithmic bytes. Per hit (the whole path): pos 12 + sml 4 + lambdaH 8 +
+# mass 4 + FP64 absorbed photons 8. Per kernel group, per unit it processes:
+# trace fill reads pos+sml (16) and writes (ipar 4, d 8, b 8) per hit; the
+# sort reads and writes (ipar, d, b) and writes the kernel value; slots read
+# ipar and write a slot per hit; deposit reads the slot's particle state and
+# writes an FP64 sum per hit; the update reads ~60 B and writes ~40 B of
+# particle state per active (tick, particle) pair.
+BYTES_PER_HIT = 36
+GROUP_BYTES = {"trace_count": (16, "hit"), "trace_fill": (36, "hit"), "sort": (60, "hit"),
+               "slots": (48, "hit"), "deposit": (32, "hit"), "update": (100, "active particle")}
 
 
 def peaks():
@@ -290,7 +298,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize(dev)
     clocks.start()
-    total_ms, hits, launches, sat = 0.0, 0.0, 0.0, 0.0
+    total_ms, hits, launches, sat, active = 0.0, 0.0, 0.0, 0.0, 0.0
     per_step = []
     kms = {k: 0.0 for k in api.KERNELS}
     kn = {k: 0.0 for k in api.KERNELS}
@@ -304,6 +312,7 @@ def main():
         total_ms += e0.elapsed_time(e1)
         hits += st["hits"]
         sat += st["saturated"]
+        active += st["active"]
         per_step.append(round(e0.elapsed_time(e1), 3))
         launches += st["launches"]
         for k in api.KERNELS:
@@ -336,9 +345,10 @@ def main():
     # roofline of the dominant kernel group
     peak, peak_kind = peaks()
     dom = max(api.KERNELS, key=lambda k: kms[k])
-    per_hit = {"trace_count": 16, "trace_fill": BYTES_PER_HIT_TRACE, "sort": 60, "slots": 48,
-               "deposit": 32, "update": 4}
-    achieved = hits * per_hit[dom] / (kms[dom] / 1e3) / 1e9 if kms[dom] > 0 else None
+    unit_bytes, unit_name = GROUP_BYTES[dom]
+    units = active if unit_name == "active particle" else hits
+    achieved = units * unit_bytes / (kms[dom] / 1e3) / 1e9 if kms[dom] > 0 else None
+    path_gbs = value / world * BYTES_PER_HIT / 1e9    # per GPU, over the whole step
     traffic = None
     prof = os.path.join(ROOT, "profiles", f"{dom}_{args.workload}_traffic.json")
     if os.path.exists(prof):
@@ -361,7 +371,10 @@ def main():
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "peak_source": peak_kind,
-                         "bytes_per_hit": per_hit[dom]},
+                         "bytes_per_unit": unit_bytes, "unit_counted": unit_name,
+                         "units_per_step": units / args.steps,
+                         "path_achieved_gbs": path_gbs,
+                         "path_frac": path_gbs / peak},
             "clocks": clk,
             "e2e": {"value": e2e_hits / e2e_t, "unit": "hits/s",
                     "h2d_bytes_per_step": int(host_rays[0].nbytes),

@@ -66,10 +66,11 @@ extern "C" int psg_create(psg_context **out, int device) {
 
 static void free_particles(psg_context *ctx) {
 	void *ptrs[] = {ctx->d_psml, ctx->d_mass, ctx->d_rho, ctx->d_yeMET, ctx->d_ie, ctx->d_flag,
-		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit};
+		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep};
 	for (void *p : ptrs) if (p) cudaFree(p);
 	ctx->d_psml = nullptr; ctx->d_mass = ctx->d_rho = ctx->d_yeMET = ctx->d_ie = nullptr;
 	ctx->d_flag = nullptr; ctx->d_lambdaH = nullptr; ctx->d_hits = nullptr; ctx->d_lasthit = nullptr;
+	ctx->d_hstep = nullptr;
 	ctx->n = 0;
 }
 
@@ -206,6 +207,7 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMalloc(&ctx->d_lambdaH, sizeof(double) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_hits, sizeof(int32_t) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_lasthit, sizeof(int64_t) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_hstep, sizeof(float) * n));
 	float *d_pos = (float *)psg_scratch(ctx, S_MISC, sizeof(float) * n * 7);
 	if (!d_pos) return PSG_E_NOMEM;
 	float *d_sml = d_pos + 3 * n, *d_xHI = d_pos + 4 * n, *d_ye = d_pos + 5 * n;
@@ -221,6 +223,7 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	else PSG_CUDA(cudaMemsetAsync(ctx->d_flag, 0, n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_hits, 0, sizeof(int32_t) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_lasthit, 0, sizeof(int64_t) * n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_hstep, 0, sizeof(float) * n, s));
 	const int bs = 256;
 	k_init_particles<<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(n, d_pos, d_sml, d_xHI, d_ye,
 			ctx->d_psml, ctx->d_lambdaH, ctx->d_yeMET);

@@ -55,6 +55,7 @@ struct psg_context {
 	double *d_lambdaH = nullptr;
 	int32_t *d_hits = nullptr;
 	int64_t *d_lasthit = nullptr;
+	float *d_hstep = nullptr;    // last integrator step proposal, seconds (0: none yet)
 
 	// octree, depth-first order
 	int have_tree = 0;

@@ -177,6 +177,7 @@ __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const
 struct DPState {
 	double x[2], k1[2];
 	double t, h;
+	float hnext;     // proposal for a step beyond s = 1 (the interval end truncates h)
 	int steps;
 };
 
@@ -196,6 +197,7 @@ __device__ __forceinline__ void dp_init(const PhysParams &P, const RhsCtx &cx, D
 		if (f > 0.0) h = fmin(h, 0.01 * scale / f);
 	}
 	S.h = fmax(h, 1e-8);
+	S.hnext = 0.0f;
 }
 
 // One attempted step; returns true once s = 1 is reached.
@@ -206,7 +208,8 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 	const double b1 = 35. / 384, b3 = 500. / 1113, b4 = 125. / 192, b5 = -2187. / 6784, b6 = 11. / 84;
 	const double e1 = 71. / 57600, e3 = -71. / 16695, e4 = 71. / 1920, e5 = -17253. / 339200, e6 = 22. / 525, e7 = -1. / 40;
 	double h = S.h;
-	if (S.t + h > 1.0) h = 1.0 - S.t;
+	const bool cut = S.t + h > 1.0;
+	if (cut) h = 1.0 - S.t;
 	double k2[2], k3[2], k4[2], k5[2], k6[2], k7[2], y[2], yn[2];
 	const double *x = S.x, *k1 = S.k1;
 	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a21 * k1[i]);
@@ -235,6 +238,7 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 	}
 	// step-size control needs no double precision
 	const float fac = err > 0.0 ? fminf(5.0f, fmaxf(0.2f, 0.9f * __powf((float)err, -0.2f))) : 5.0f;
+	S.hnext = (cut && err <= 1.0) ? fmaxf((float)S.h, (float)h * fac) : (float)h * fac;
 	S.h = fmax(h * (double)fac, 1e-14);
 	S.steps++;
 	return S.t >= 1.0;

@@ -476,7 +476,7 @@ __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__re
 		const uint32_t *__restrict__ act_ipar, const double *__restrict__ act_g,
 		const double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
-		PhysParams P, int64_t tick, double tick_time, unsigned *__restrict__ cursor,
+		float *__restrict__ hstep, PhysParams P, int64_t tick, double tick_time, unsigned *__restrict__ cursor,
 		StiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff, uint32_t *__restrict__ status) {
 	const int lo = tick_act[t], hi = tick_act[t + 1];
 	const unsigned n = (unsigned)(hi - lo);
@@ -510,6 +510,10 @@ __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__re
 					S.x[1] = ie0;
 					atol1 = DP_ATOL1_REL * fabs(ie0) + 1e-300;
 					dp_init(P, cx, S);
+					// the particle's last step proposal is a better first
+					// step than the derivative estimate
+					const float hp = hstep[p];
+					if (hp > 0.0f) S.h = fmin(1.0, fmax((double)hp / time, 1e-8));
 					have = true;
 				}
 			}
@@ -524,6 +528,7 @@ __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__re
 				it.p = p; it.t = S.t; it.h = S.h; it.x0 = S.x[0]; it.x1 = S.x[1];
 				it.yeMET = cx.yeMET; it.g = cx.g; it.heat = cx.heat; it.time = cx.time; it.nH = cx.nH; it.T = cx.T;
 				stiff[q] = it;
+				hstep[p] = 0.0f;
 				have = false;
 			} else if (done) {
 				const double lam = S.x[0], e = S.x[1];
@@ -532,6 +537,7 @@ __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__re
 				lambdaH[p] = fmin(1.0, fmax(0.0, lam));
 				if (!P.adiabatic) ie[p] = (float)e;
 				lasthit[p] = tick;
+				hstep[p] = (float)((double)S.hnext * cx.time);
 				have = false;
 			}
 		}
@@ -772,7 +778,8 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 				PSG_CHECK_LAUNCH();
 				const unsigned qgrid = (unsigned)std::min<size_t>(blocks(nact_t, 256), (size_t)dev_sms * 8);
 				k_update_queue<<<qgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_g, act_heat, ctx->d_lambdaH,
-						ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time,
+						ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, P, first_tick + (int64_t)t,
+						tick_time,
 						cursors + t, stiff, nstiff + t, ctx->d_status);
 				PSG_CHECK_LAUNCH();
 				k_update_stiff<<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,

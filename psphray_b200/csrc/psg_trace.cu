@@ -1,13 +1,11 @@
 // Ray traversal; replaces rt_trace() raytrace.c:153-210 and the per-ray
 // sort of trace() loop.c:375-386.
 //
-// Cells are stored depth first with a skip pointer (the index just past the
-// subtree), so the reference's parent/sibling walk becomes a loop over one
-// index: a crossed cell continues at i+1 (its first child, or the next cell
-// after a leaf), a missed cell jumps to its skip pointer. The visiting order
-// and the set of crossed cells are the reference's. Hit lists are produced in
-// two passes (count, then fill at scanned offsets) and sorted per ray by
-// (d, ipar).
+// The traversal walks the level-order copy of the octree (the 8 children of
+// a cell contiguous), one warp per ray with a stack of crossed cells in
+// shared memory; the set of crossed cells and the hits are the reference's
+// parent/sibling walk's, found in another order. Hits go to per-ray slabs in
+// discovery order and are then sorted per ray by (d, ipar).
 #include <cub/cub.cuh>
 
 #include <stdlib.h>
@@ -85,96 +83,6 @@ __device__ __forceinline__ bool line_hits_particle(const RayGeom &g, float4 q, d
 	dc = __dsqrt_rn(d2);
 	r2 = rn_dmul(rn_dsub(dc, proj), rn_dadd(dc, proj));
 	return !((double)rn_fmul(q.w, q.w) < r2);
-}
-
-// One warp per ray. The warp tests 32 consecutive cells of the depth-first
-// array at once. A cell is inside a missed cell's subtree iff some missed
-// cell k before it in the window has skip_k > j; a warp max-scan of the
-// missed cells' skip pointers decides that for all 32 lanes. Crossed leaves
-// of the window list their particles in shared memory and the lanes test
-// them 32 at a time. The next window starts after the window or after the
-// furthest missed subtree, whichever is later, so every window advances by
-// at least 32 cells. Accepted hits are written in traversal order straight
-// into the ray's own slab of scap entries; the true count is returned even
-// when it exceeds scap, so the caller can grow the slabs and run again.
-__global__ void __launch_bounds__(128) k_trace_warp(const psg_ray *__restrict__ rays, size_t nray,
-		const float4 *__restrict__ cell_lo, const float4 *__restrict__ cell_hi, int ncell,
-		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx, int ppc,
-		uint32_t *__restrict__ count, size_t scap, uint32_t *__restrict__ slab_ipar,
-		double *__restrict__ slab_d, double *__restrict__ slab_b) {
-	extern __shared__ int list_all[];
-	const int lane = threadIdx.x & 31;
-	const int wib = threadIdx.x >> 5;
-	int *list = list_all + wib * 32 * ppc;
-	const size_t r = (size_t)blockIdx.x * (blockDim.x >> 5) + wib;
-	if (r >= nray) return;
-	const RayGeom g = load_ray(rays, r);
-	const unsigned lt_mask = (1u << lane) - 1u;
-	uint32_t nh = 0;
-	int i = 0;
-	while (i < ncell) {
-		const int j = i + lane;
-		const bool valid = j < ncell;
-		float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
-		if (valid) lo = __ldg(&cell_lo[j]);
-		if (j <= ncell) hi = __ldg(&cell_hi[j]);     // the sentinel closes the last leaf
-		const int skip = __float_as_int(lo.w);
-		bool hit = false;
-		if (valid) {
-			const float s2b[3] = {rn_fsub(lo.x, g.s[0]), rn_fsub(lo.y, g.s[1]), rn_fsub(lo.z, g.s[2])};
-			const float s2t[3] = {rn_fsub(hi.x, g.s[0]), rn_fsub(hi.y, g.s[1]), rn_fsub(hi.z, g.s[2])};
-			hit = segment_hits_box(g.dir, g.dist, s2b, s2t);
-		}
-		int m = (valid && !hit) ? skip : 0;
-#pragma unroll
-		for (int o = 1; o < 32; o <<= 1) {
-			const int t = __shfl_up_sync(0xffffffffu, m, o);
-			if (lane >= o) m = max(m, t);
-		}
-		int cover = __shfl_up_sync(0xffffffffu, m, 1);
-		if (lane == 0) cover = 0;
-		const bool live = valid && cover <= j;
-		const bool leaf = live && hit && skip == j + 1;
-		const int ps = __float_as_int(hi.w);
-		int pe = __shfl_down_sync(0xffffffffu, ps, 1);
-		if (lane == 31 && j + 1 <= ncell) pe = __float_as_int(__ldg(&cell_hi[j + 1]).w);
-		const int cnt = leaf ? min(max(pe - ps, 0), ppc) : 0;
-		int c = cnt;
-#pragma unroll
-		for (int o = 1; o < 32; o <<= 1) {
-			const int t = __shfl_up_sync(0xffffffffu, c, o);
-			if (lane >= o) c += t;
-		}
-		const int total = __shfl_sync(0xffffffffu, c, 31);
-		const int base = c - cnt;
-		for (int k = 0; k < cnt; k++) list[base + k] = ps + k;
-		__syncwarp();
-		for (int k0 = 0; k0 < total; k0 += 32) {
-			const int k = k0 + lane;
-			bool acc = false;
-			double dc = 0.0, r2 = 0.0;
-			uint32_t idx = 0;
-			if (k < total) {
-				const int p = list[k];
-				idx = __ldg(&lidx[p]);
-				if (!(idx & PSG_INVALID_BIT)) acc = line_hits_particle(g, __ldg(&lpsml[p]), dc, r2);
-			}
-			const unsigned bal = __ballot_sync(0xffffffffu, acc);
-			if (acc) {
-				const size_t q = nh + __popc(bal & lt_mask);
-				if (q < scap) {
-					const size_t o = r * scap + q;
-					slab_ipar[o] = idx;
-					slab_d[o] = dc;
-					slab_b[o] = __dsqrt_rn(fabs(r2));
-				}
-			}
-			nh += __popc(bal);
-		}
-		__syncwarp();
-		i = max(i + 32, __shfl_sync(0xffffffffu, m, 31));
-	}
-	if (lane == 0) count[r] = nh;
 }
 
 // Candidates listed in shared memory (leaf-order particle positions), tested
@@ -497,7 +405,6 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	int64_t *off64 = (int64_t *)offmem;
 	int32_t *off32 = (int32_t *)(offmem + sizeof(int64_t) * (nray + 1));
 	unsigned long long *d_max = ctx->d_counters + 4;
-	const int ncell = (int)ctx->ncell;
 	const int ppc = ctx->ppc;
 	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ppc) * TR_WARPS;
 	if (smem > 48 * 1024)
