@@ -131,42 +131,60 @@ __device__ __forceinline__ double riccati_step(double lam0, double a, double b, 
 
 struct RhsCtx {
 	double yeMET, g, heat, time, nH, T;
-	double g_rate, heat_rate;    // g/time and heat/time, constant over the step
-	double T_num;                // MPROTON_OVER_BOLTZMANN*2/3: T = T_num*ie/(hemf/4+hmf+hmf*ye)
+	double nHt;                  // nH*time: rates per unit normalised time
+	double hpt;                  // H_PER_MASS*time
+	double T_num;                // MPROTON_OVER_BOLTZMANN*2/3: T = T_num*ie/(T_den0 + hmf*ye)
+	double T_den0;               // hemf/4 + hmf
 };
 
 __device__ __forceinline__ RhsCtx make_rhs_ctx(const PhysParams &P, double yeMET, double g, double heat,
 		double time, double nH, double T) {
 	RhsCtx c;
 	c.yeMET = yeMET; c.g = g; c.heat = heat; c.time = time; c.nH = nH; c.T = T;
-	c.g_rate = g / time;
-	c.heat_rate = heat / time;
+	c.nHt = nH * time;
+	c.hpt = P.H_PER_MASS * time;
 	c.T_num = P.MPROTON_OVER_BOLTZMANN * 2.0 / 3.0;
+	c.T_den0 = P.hemf * 0.25 + P.hmf;
 	return c;
 }
 
-// function() solve.c:76-141, hydrogen-only branch (used inside the
-// integrator, where the last bit of T does not matter: T takes one division).
+// function() solve.c:76-141, hydrogen-only branch, for the integrators (not
+// isothermal): the same equations with the step length folded into the
+// rates, and fused multiply-adds (the last bits of an integrator's stage do
+// not matter; the isothermal closed form keeps the reference's roundings).
 __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const double x[2], double dx[2]) {
 	const double xHI = x[0], xHII = 1.0 - x[0];
 	const double ye = xHII + P.he_e + cx.yeMET;
-	const double T = P.isothermal ? cx.T : cx.T_num * x[1] / (P.hemf * 0.25 + P.hmf + P.hmf * ye);
-	const RateAt R = rates_at(P, log10(T));
-	const double nH = cx.nH;
-	const double gamma = R(PSG_AR_HI_CI) * nH;
-	const double alpha = R(P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A) * nH;
-	dx[0] = (-cx.g_rate + ye * (alpha * xHII - gamma * xHI)) * cx.time;
+	const double T = cx.T_num * x[1] / __fma_rn(P.hmf, ye, cx.T_den0);
+	// row and weights of tabfun_get() (clamped rows: weight 1 on one row)
+	const double logT = log10(T);
+	const long long idx = (long long)((logT - P.ar_min) * P.ar_step_inv);
+	const double *r0, *r1;
+	double w0, w1;
+	if (idx >= 0 && idx < P.ar_nrows - 1) {
+		r0 = P.ar + (size_t)idx * 16;
+		r1 = r0 + 16;
+		w0 = (r1[0] - logT) * P.ar_step_inv;
+		w1 = (logT - r0[0]) * P.ar_step_inv;
+	} else {
+		r0 = r1 = P.ar + (idx < 0 ? (size_t)0 : (size_t)(P.ar_nrows - 1) * 16);
+		w0 = 1.0;
+		w1 = 0.0;
+	}
+#define PSG_RATE(col) __fma_rn(w0, r0[1 + (col)], w1 * r1[1 + (col)])
+	const double gamma = PSG_RATE(PSG_AR_HI_CI) * cx.nHt;
+	const double alpha = PSG_RATE(P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A) * cx.nHt;
+	dx[0] = __fma_rn(ye, __fma_rn(alpha, xHII, -gamma * xHI), -cx.g);
 	if (P.isothermal || P.adiabatic) {
 		dx[1] = 0.0;
 	} else {
-		const double eta = R(P.on_the_spot ? PSG_AR_HII_RCC_B : PSG_AR_HII_RCC_A) * nH;
-		const double psi = R(PSG_AR_HI_CEC) * nH;
-		const double zeta = R(PSG_AR_HI_CIC) * nH;
-		const double beta = R(PSG_AR_E_BREMC) * nH;
-		const double chi = R(PSG_AR_E_COMPC);
-		const double L = P.H_PER_MASS * ye * ((zeta + psi) * xHI + (eta + beta) * xHII + chi);
-		dx[1] = (cx.heat_rate - L) * cx.time;
+		const double ion = PSG_RATE(P.on_the_spot ? PSG_AR_HII_RCC_B : PSG_AR_HII_RCC_A) + PSG_RATE(PSG_AR_E_BREMC);
+		const double neu = PSG_RATE(PSG_AR_HI_CEC) + PSG_RATE(PSG_AR_HI_CIC);
+		const double chi = PSG_RATE(PSG_AR_E_COMPC);
+		const double L = __fma_rn(cx.nH, __fma_rn(neu, xHI, ion * xHII), chi);
+		dx[1] = __fma_rn(-cx.hpt * ye, L, cx.heat);
 	}
+#undef PSG_RATE
 }
 
 // Adaptive Dormand-Prince 5(4) over s in [0,1]. LSODA runs the reference at
@@ -212,24 +230,27 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 	if (cut) h = 1.0 - S.t;
 	double k2[2], k3[2], k4[2], k5[2], k6[2], k7[2], y[2], yn[2];
 	const double *x = S.x, *k1 = S.k1;
-	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a21 * k1[i]);
+#define F __fma_rn
+	for (int i = 0; i < 2; i++) y[i] = F(h, a21 * k1[i], x[i]);
 	rhs(P, cx, y, k2);
-	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a31 * k1[i] + a32 * k2[i]);
+	for (int i = 0; i < 2; i++) y[i] = F(h, F(a32, k2[i], a31 * k1[i]), x[i]);
 	rhs(P, cx, y, k3);
-	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+	for (int i = 0; i < 2; i++) y[i] = F(h, F(a43, k3[i], F(a42, k2[i], a41 * k1[i])), x[i]);
 	rhs(P, cx, y, k4);
-	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i] + a54 * k4[i]);
+	for (int i = 0; i < 2; i++) y[i] = F(h, F(a54, k4[i], F(a53, k3[i], F(a52, k2[i], a51 * k1[i]))), x[i]);
 	rhs(P, cx, y, k5);
-	for (int i = 0; i < 2; i++) y[i] = x[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i] + a64 * k4[i] + a65 * k5[i]);
+	for (int i = 0; i < 2; i++)
+		y[i] = F(h, F(a65, k5[i], F(a64, k4[i], F(a63, k3[i], F(a62, k2[i], a61 * k1[i])))), x[i]);
 	rhs(P, cx, y, k6);
-	for (int i = 0; i < 2; i++) yn[i] = x[i] + h * (b1 * k1[i] + b3 * k3[i] + b4 * k4[i] + b5 * k5[i] + b6 * k6[i]);
+	for (int i = 0; i < 2; i++) yn[i] = F(h, F(b6, k6[i], F(b5, k5[i], F(b4, k4[i], F(b3, k3[i], b1 * k1[i])))), x[i]);
 	rhs(P, cx, yn, k7);
 	double err = 0.0;
 	for (int i = 0; i < 2; i++) {
-		const double e = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i] + e6 * k6[i] + e7 * k7[i]);
+		const double e = h * F(e7, k7[i], F(e6, k6[i], F(e5, k5[i], F(e4, k4[i], F(e3, k3[i], e1 * k1[i])))));
 		const double sc = (i == 0 ? DP_ATOL0 : atol1) + DP_RTOL * fmax(fabs(x[i]), fabs(yn[i]));
 		err += (e / sc) * (e / sc);
 	}
+#undef F
 	err = sqrt(0.5 * err);
 	if (err <= 1.0) {
 		S.t += h;
