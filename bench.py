@@ -349,6 +349,9 @@ def main():
     units = active if unit_name == "active particle" else hits
     achieved = units * unit_bytes / (kms[dom] / 1e3) / 1e9 if kms[dom] > 0 else None
     path_gbs = value / world * BYTES_PER_HIT / 1e9    # per GPU, over the whole step
+    # groups launched once per tick (deposit, update) vs once per step
+    per_tick = dom in ("deposit", "update")
+    alg_per_launch = units * unit_bytes / (args.steps * (T if per_tick else 1))
     traffic = None
     prof = os.path.join(ROOT, "profiles", f"{dom}_{args.workload}_traffic.json")
     if os.path.exists(prof):
@@ -372,6 +375,8 @@ def main():
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "peak_source": peak_kind,
                          "bytes_per_unit": unit_bytes, "unit_counted": unit_name,
+                         "launch": "one tick" if per_tick else "one step",
+                         "algorithmic_bytes_per_launch": alg_per_launch,
                          "units_per_step": units / args.steps,
                          "path_achieved_gbs": path_gbs,
                          "path_frac": path_gbs / peak},
