@@ -24,6 +24,7 @@ is single-GPU; no data crosses GPUs), barrier + max over ranks for time.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -342,6 +343,25 @@ def main():
     torch.cuda.synchronize(dev)
     e2e_t, e2e_hits = reduce_over_ranks(time.perf_counter() - t0, e2e_hits, dist, torch.device("cuda", dev))
 
+    # the same through psg_run_ticks_emit: rays emitted on the device from the
+    # workload's sources (no rays cross the bus), state read back every step
+    sch = w.schedule
+    t1 = 1 + 2 * nsteps * T
+    srcs = [dataclasses.replace(src, lastemit=t1 - 1) for src in sch.sources]   # one tick's photons at t1
+    ctx.set_sources(srcs, [(sch.energies, sch.eweights)], seed=sch.seed)
+    ctx.run_ticks_emit(R, T, t1, w.tick_time)
+    em_hits = 0.0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        st = ctx.run_ticks_emit(R, T, t1 + (i + 1) * T, w.tick_time)
+        lam = ctx.lambdaH()
+        em_hits += st["hits"]
+    torch.cuda.synchronize(dev)
+    em_t, em_hits = reduce_over_ranks(time.perf_counter() - t0, em_hits, dist, torch.device("cuda", dev))
+
     # roofline of the dominant kernel group
     peak, peak_kind = peaks()
     dom = max(api.KERNELS, key=lambda k: kms[k])
@@ -381,6 +401,8 @@ def main():
                          "path_achieved_gbs": path_gbs,
                          "path_frac": path_gbs / peak},
             "clocks": clk,
+            "e2e_device_emission": {"value": em_hits / em_t, "unit": "hits/s", "h2d_bytes_per_step": 0,
+                                    "d2h_bytes_per_step": int(lam.nbytes)},
             "e2e": {"value": e2e_hits / e2e_t, "unit": "hits/s",
                     "h2d_bytes_per_step": int(host_rays[0].nbytes),
                     "d2h_bytes_per_step": int(lam.nbytes)}}

@@ -176,7 +176,7 @@ int psg_trace(psg_context *ctx, const psg_ray *rays, size_t nray, int64_t *offse
 /* ---- ticks ----------------------------------------------------------------- */
 /* Kernels timed by psg_tick_stats when timing is on (psg_set_timing). */
 enum { PSG_K_TRACE_COUNT = 0, PSG_K_TRACE_FILL, PSG_K_SORT, PSG_K_SLOTS, PSG_K_DEPOSIT,
-	PSG_K_UPDATE, PSG_K_NKERNELS };
+	PSG_K_UPDATE, PSG_K_EMIT, PSG_K_NKERNELS };
 typedef struct {
 	double hits;            /* sum of hit-list lengths, stat.total_deposit_count */
 	double saturated;       /* deposits capped at the neutral atoms, loop.c:482-485 */
@@ -197,6 +197,55 @@ int psg_run_ticks(psg_context *ctx, const psg_ray *rays, size_t nray_per_tick, s
 /* Same with rays already in device memory. */
 int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, size_t nray_per_tick,
 		size_t nticks, int64_t first_tick, double tick_time, psg_tick_stats *stats);
+
+/* ---- sources and ray emission on the device -------------------------------- */
+/* Source rays of emit_rays() loop.c:163-373 (recombination rays are not
+ * emitted). A source is psystem.h's Source: position, type, spectrum and its
+ * luminosity history (Ngamma_dot from ticks[k] on, sources.c:58-66). */
+#define PSG_SRC_PLANE 0     /* PSYS_SRC_PLANE psystem.h:4 */
+#define PSG_SRC_POINT 1     /* PSYS_SRC_POINT psystem.h:5 */
+typedef struct {
+	int type;               /* PSG_SRC_POINT or PSG_SRC_PLANE */
+	int specid;             /* index into the spectra of psg_set_sources */
+	double pos[3];
+	double dir[3];          /* plane sources: the direction of every ray */
+	double a[3], b[3];      /* plane sources: unit vectors spanning the plane */
+	double radius;          /* plane sources: half side of the emitting square */
+	const int64_t *ticks;   /* luminosity history: from tick ticks[k] on, */
+	const double *ngamma_dot;   /* photons per unit time ngamma_dot[k] */
+	int nhist;              /* entries in the history (>= 1) */
+	int64_t lastemit;       /* tick of the last emission (Source.lastemit) */
+} psg_source;
+typedef struct {
+	const double *eng;      /* photon energies (internal units), spectra.c */
+	const double *weight;   /* photon-number weight of each energy */
+	int n;                  /* 1: monochromatic (spec type 1) */
+} psg_spectrum;
+#define PSG_MAX_SOURCES 4096
+
+/* Copies the sources, their histories and the spectra to the device and
+ * keys the counter-based generator (Philox4x32-10) with seed. Replaces the
+ * source and spectrum set-up of psystem_read_source() sources.c and
+ * spec_init() spectra.c; the reference's GSL generator has no device
+ * counterpart, so the draws are this library's own stream. */
+int psg_set_sources(psg_context *ctx, const psg_source *srcs, int nsrc, const psg_spectrum *specs,
+		int nspec, uint64_t seed);
+/* lastemit and history cursor of every source (after emissions). */
+int psg_get_sources(psg_context *ctx, int64_t *lastemit, int32_t *cursor);
+
+/* Emits nray_per_tick source rays for each of nticks ticks into a host
+ * buffer (nticks*nray_per_tick rays, tick by tick), advancing the sources'
+ * state as the ticks would: per tick, weights = Ngamma_dot*(tick-lastemit)*
+ * tick_time (psystem_weight_srcs() sources.c:67-78), a source per ray drawn
+ * by weight, the source's photons split evenly over its rays of the tick
+ * (loop.c:305-320), isotropic directions for point sources, a uniform point
+ * of the square for plane sources, a spectrum energy per ray, length twice
+ * the box. */
+int psg_emit_rays(psg_context *ctx, size_t nray_per_tick, size_t nticks, int64_t first_tick,
+		double tick_time, psg_ray *rays);
+/* emit_rays() + the ticks, all on the device (no rays cross the bus). */
+int psg_run_ticks_emit(psg_context *ctx, size_t nray_per_tick, size_t nticks, int64_t first_tick,
+		double tick_time, psg_tick_stats *stats);
 
 /* Particle state, caller order. Any pointer may be NULL. */
 int psg_get_state(psg_context *ctx, double *lambdaH, float *ie, int32_t *hits, int64_t *lasthit);

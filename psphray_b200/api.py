@@ -81,7 +81,20 @@ class TreeInfo(C.Structure):
                 ("depth", C.c_int)]
 
 
-KERNELS = ["trace_count", "trace_fill", "sort", "slots", "deposit", "update"]
+KERNELS = ["trace_count", "trace_fill", "sort", "slots", "deposit", "update", "emit"]
+
+SRC_PLANE, SRC_POINT = 0, 1
+
+
+class CSource(C.Structure):
+    _fields_ = [("type", C.c_int), ("specid", C.c_int), ("pos", C.c_double * 3), ("dir", C.c_double * 3),
+                ("a", C.c_double * 3), ("b", C.c_double * 3), ("radius", C.c_double),
+                ("ticks", C.c_void_p), ("ngamma_dot", C.c_void_p), ("nhist", C.c_int),
+                ("lastemit", C.c_int64)]
+
+
+class CSpectrum(C.Structure):
+    _fields_ = [("eng", C.c_void_p), ("weight", C.c_void_p), ("n", C.c_int)]
 
 
 class TickStats(C.Structure):
@@ -143,6 +156,10 @@ def lib() -> C.CDLL:
         "psg_get_state": ([vp, vp, vp, vp, vp], C.c_int),
         "psg_set_state": ([vp, vp, vp, vp], C.c_int),
         "psg_step_evolve": ([vp, vp, sz], C.c_int),
+        "psg_set_sources": ([vp, vp, C.c_int, vp, C.c_int, C.c_uint64], C.c_int),
+        "psg_get_sources": ([vp, vp, vp], C.c_int),
+        "psg_emit_rays": ([vp, sz, sz, i64, dbl, vp], C.c_int),
+        "psg_run_ticks_emit": ([vp, sz, sz, i64, dbl, C.POINTER(TickStats)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -326,6 +343,54 @@ class Context:
         st = TickStats()
         self._check(lib().psg_run_ticks_device(self.h, C.c_void_p(d_rays_ptr), nray_per_tick, nticks,
                                                first_tick, tick_time, C.byref(st)), "psg_run_ticks_device")
+        return _stats(st)
+
+    def set_sources(self, sources, spectra, seed: int):
+        """sources: objects with pos, ngamma_dot (or a history: ticks +
+        ngamma_dots), lastemit and optionally type/specid/dir/a/b/radius;
+        spectra: list of (energies, weights)."""
+        keep = []
+        cs = (CSource * len(sources))()
+        for c, src in zip(cs, sources):
+            ticks = np.ascontiguousarray(getattr(src, "ticks", None) if getattr(src, "ticks", None) is not None
+                                         else [0], np.int64)
+            ngd = np.ascontiguousarray(getattr(src, "ngamma_dots", None) if getattr(src, "ngamma_dots", None)
+                                       is not None else [src.ngamma_dot], np.float64)
+            keep += [ticks, ngd]
+            c.type = int(getattr(src, "type", SRC_POINT))
+            c.specid = int(getattr(src, "specid", 0))
+            c.pos[:] = [float(v) for v in src.pos]
+            for name in ("dir", "a", "b"):
+                v = getattr(src, name, None)
+                if v is not None:
+                    getattr(c, name)[:] = [float(x) for x in v]
+            c.radius = float(getattr(src, "radius", 0.0))
+            c.ticks, c.ngamma_dot, c.nhist = ticks.ctypes.data, ngd.ctypes.data, len(ticks)
+            c.lastemit = int(src.lastemit)
+        sp = (CSpectrum * len(spectra))()
+        for c, (eng, wt) in zip(sp, spectra):
+            e = np.ascontiguousarray(eng, np.float64); w = np.ascontiguousarray(wt, np.float64)
+            keep += [e, w]
+            c.eng, c.weight, c.n = e.ctypes.data, w.ctypes.data, len(e)
+        self._check(lib().psg_set_sources(self.h, C.cast(cs, C.c_void_p), len(sources), C.cast(sp, C.c_void_p),
+                                          len(spectra), C.c_uint64(seed)), "psg_set_sources")
+        self.nsrc = len(sources)
+
+    def sources_state(self):
+        lastemit = np.zeros(self.nsrc, np.int64); cursor = np.zeros(self.nsrc, np.int32)
+        self._check(lib().psg_get_sources(self.h, lastemit.ctypes.data, cursor.ctypes.data), "psg_get_sources")
+        return lastemit, cursor
+
+    def emit_rays(self, nray_per_tick: int, nticks: int, first_tick: int, tick_time: float) -> np.ndarray:
+        out = np.zeros(nray_per_tick * nticks, RAY_DTYPE)
+        self._check(lib().psg_emit_rays(self.h, nray_per_tick, nticks, first_tick, tick_time, out.ctypes.data),
+                    "psg_emit_rays")
+        return out
+
+    def run_ticks_emit(self, nray_per_tick: int, nticks: int, first_tick: int, tick_time: float) -> dict:
+        st = TickStats()
+        self._check(lib().psg_run_ticks_emit(self.h, nray_per_tick, nticks, first_tick, tick_time, C.byref(st)),
+                    "psg_run_ticks_emit")
         return _stats(st)
 
     def set_timing(self, on: bool):

@@ -20,7 +20,7 @@ INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpsg.so")
 
-CU_SOURCES = ["psg_context.cu", "psg_tree.cu", "psg_trace.cu", "psg_tick.cu"]
+CU_SOURCES = ["psg_context.cu", "psg_tree.cu", "psg_trace.cu", "psg_tick.cu", "psg_emit.cu"]
 C_SOURCES = ["psg_host.c"]
 HEADERS = ["psg_internal.cuh", "psg_solve.cuh"]
 

@@ -93,6 +93,7 @@ extern "C" void psg_destroy(psg_context *ctx) {
 	if (ctx->d_kernel) cudaFree(ctx->d_kernel);
 	if (ctx->d_status) cudaFree(ctx->d_status);
 	if (ctx->d_counters) cudaFree(ctx->d_counters);
+	if (ctx->d_emit) cudaFree(ctx->d_emit);
 	for (auto &b : ctx->scratch) if (b.p) cudaFree(b.p);
 	for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
 	for (auto &ev : ctx->kev) if (ev) cudaEventDestroy(ev);

@@ -68,11 +68,16 @@ struct psg_context {
 	float4 *d_leaf_psml = nullptr; // particles in leaf order
 	uint32_t *d_leaf_idx = nullptr; // caller index, PSG_INVALID_BIT if flagged
 
+	// sources for device emission: one allocation, layout in psg_emit.cu
+	void *d_emit = nullptr;
+	int nsrc = 0, nspec = 0, nhist_total = 0, nspec_total = 0;
+	uint64_t emit_seed = 0;
+
 	uint32_t *d_status = nullptr;
 	unsigned long long *d_counters = nullptr;   // 8 device counters (records, deposits capped, ...)
 
 	// scratch, grown on demand
-	psg_buf scratch[20];
+	psg_buf scratch[24];
 	size_t slab_cap = 0;  // hits each ray can hold in the traversal's output slabs
 	int ppc = 8;          // leaf capacity of the current tree
 	cudaEvent_t ev[8] = {};
@@ -99,7 +104,8 @@ void *psg_scratch(psg_context *ctx, int slot, size_t bytes);
 // scratch slots
 enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
-	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD
+	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
+	S_EMIT
 };
 
 // Per-launch timing: mark_begin/mark_end bracket a group of launches of one

@@ -108,7 +108,7 @@ def lognormal_field(n_side: int, seed: int, sigma: float = 1.0, box_kpc: float =
     amp = np.sqrt(1.0 / k2)          # sqrt(P(k)) with P ~ k^-2
     amp[0, 0, 0] = 0.0
     noise = np.fft.rfftn(rng.standard_normal((g, g, g)))
-    gauss = np.fft.irfftn(noise * amp, s=(g, g, g))
+    gauss = np.fft.irfftn(noise * amp, s=(g, g, g), axes=(0, 1, 2))
     gauss = (gauss - gauss.mean()) / gauss.std()
     dens = np.exp(sigma * gauss - 0.5 * sigma * sigma)
     dens /= dens.mean()
