@@ -66,11 +66,11 @@ extern "C" int psg_create(psg_context **out, int device) {
 
 static void free_particles(psg_context *ctx) {
 	void *ptrs[] = {ctx->d_psml, ctx->d_mass, ctx->d_rho, ctx->d_yeMET, ctx->d_ie, ctx->d_flag,
-		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep};
+		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep, ctx->d_order};
 	for (void *p : ptrs) if (p) cudaFree(p);
 	ctx->d_psml = nullptr; ctx->d_mass = ctx->d_rho = ctx->d_yeMET = ctx->d_ie = nullptr;
 	ctx->d_flag = nullptr; ctx->d_lambdaH = nullptr; ctx->d_hits = nullptr; ctx->d_lasthit = nullptr;
-	ctx->d_hstep = nullptr;
+	ctx->d_hstep = nullptr; ctx->d_order = nullptr;
 	ctx->n = 0;
 }
 
@@ -233,18 +233,112 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	return PSG_OK;
 }
 
+// ---- particle order ----------------------------------------------------------
+// After psg_build_tree the per-particle arrays are kept in the tree's leaf
+// order (internal position k holds the caller's particle d_order[k]), so the
+// particles a ray meets one after another sit next to each other in memory.
+// The caller only ever sees its own order: the state calls and the hit lists
+// map through d_order.
+template <typename T>
+__global__ void k_gather(size_t n, const uint32_t *__restrict__ g, const T *__restrict__ in, T *__restrict__ out) {
+	const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (k < n) out[k] = in[g[k]];
+}
+template <typename T>
+__global__ void k_scatter(size_t n, const uint32_t *__restrict__ g, const T *__restrict__ in, T *__restrict__ out) {
+	const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (k < n) out[g[k]] = in[k];
+}
+
+template <typename T>
+static int permute_array(psg_context *ctx, T *&arr, const uint32_t *g) {
+	const size_t n = ctx->n;
+	T *out = nullptr;
+	PSG_CUDA(cudaMalloc(&out, sizeof(T) * n));
+	k_gather<T><<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, g, arr, out);
+	const cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) {
+		cudaFree(out);
+		return psg_cuda_fail(ctx, e, "k_gather", __FILE__, __LINE__);
+	}
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	PSG_CUDA(cudaFree(arr));
+	arr = out;
+	return PSG_OK;
+}
+
+int psg_permute_particles(psg_context *ctx, const uint32_t *g) {
+	int rc = 0;
+	if ((rc = permute_array(ctx, ctx->d_psml, g)) || (rc = permute_array(ctx, ctx->d_mass, g)) ||
+			(rc = permute_array(ctx, ctx->d_rho, g)) || (rc = permute_array(ctx, ctx->d_yeMET, g)) ||
+			(rc = permute_array(ctx, ctx->d_ie, g)) || (rc = permute_array(ctx, ctx->d_flag, g)) ||
+			(rc = permute_array(ctx, ctx->d_lambdaH, g)) || (rc = permute_array(ctx, ctx->d_hits, g)) ||
+			(rc = permute_array(ctx, ctx->d_lasthit, g)) || (rc = permute_array(ctx, ctx->d_hstep, g)))
+		return rc;
+	// the caller index of every new position: through the previous order
+	const size_t n = ctx->n;
+	uint32_t *order = nullptr;
+	PSG_CUDA(cudaMalloc(&order, sizeof(uint32_t) * n));
+	if (ctx->d_order) {
+		k_gather<uint32_t><<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, g, ctx->d_order, order);
+		PSG_CHECK_LAUNCH();
+		PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+		PSG_CUDA(cudaFree(ctx->d_order));
+	} else {
+		PSG_CUDA(cudaMemcpyAsync(order, g, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+		PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	}
+	ctx->d_order = order;
+	return PSG_OK;
+}
+
+// device array (internal order) -> host array (caller order)
+template <typename T>
+static int to_caller(psg_context *ctx, T *host, const T *dev) {
+	const size_t n = ctx->n;
+	cudaStream_t s = ctx->stream;
+	if (!ctx->d_order) {
+		PSG_CUDA(cudaMemcpyAsync(host, dev, sizeof(T) * n, cudaMemcpyDeviceToHost, s));
+		return PSG_OK;
+	}
+	T *tmp = (T *)psg_scratch(ctx, S_MAP, sizeof(T) * n);
+	if (!tmp) return PSG_E_NOMEM;
+	k_scatter<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, ctx->d_order, dev, tmp);
+	PSG_CHECK_LAUNCH();
+	PSG_CUDA(cudaMemcpyAsync(host, tmp, sizeof(T) * n, cudaMemcpyDeviceToHost, s));
+	PSG_CUDA(cudaStreamSynchronize(s));
+	return PSG_OK;
+}
+
+// host array (caller order) -> device array (internal order)
+template <typename T>
+static int from_caller(psg_context *ctx, T *dev, const T *host) {
+	const size_t n = ctx->n;
+	cudaStream_t s = ctx->stream;
+	if (!ctx->d_order) {
+		PSG_CUDA(cudaMemcpyAsync(dev, host, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+		return PSG_OK;
+	}
+	T *tmp = (T *)psg_scratch(ctx, S_MAP, sizeof(T) * n);
+	if (!tmp) return PSG_E_NOMEM;
+	PSG_CUDA(cudaMemcpyAsync(tmp, host, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+	k_gather<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, ctx->d_order, tmp, dev);
+	PSG_CHECK_LAUNCH();
+	PSG_CUDA(cudaStreamSynchronize(s));
+	return PSG_OK;
+}
+
 extern "C" int psg_get_state(psg_context *ctx, double *lambdaH, float *ie, int32_t *hits,
 		int64_t *lasthit) {
 	if (!ctx) return PSG_E_INVAL;
 	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_get_state: no particles loaded");
 	PSG_CUDA(cudaSetDevice(ctx->device));
-	cudaStream_t s = ctx->stream;
-	const size_t n = ctx->n;
-	if (lambdaH) PSG_CUDA(cudaMemcpyAsync(lambdaH, ctx->d_lambdaH, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-	if (ie) PSG_CUDA(cudaMemcpyAsync(ie, ctx->d_ie, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
-	if (hits) PSG_CUDA(cudaMemcpyAsync(hits, ctx->d_hits, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
-	if (lasthit) PSG_CUDA(cudaMemcpyAsync(lasthit, ctx->d_lasthit, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, s));
-	PSG_CUDA(cudaStreamSynchronize(s));
+	int rc = 0;
+	if (lambdaH && (rc = to_caller(ctx, lambdaH, ctx->d_lambdaH))) return rc;
+	if (ie && (rc = to_caller(ctx, ie, ctx->d_ie))) return rc;
+	if (hits && (rc = to_caller(ctx, hits, ctx->d_hits))) return rc;
+	if (lasthit && (rc = to_caller(ctx, lasthit, ctx->d_lasthit))) return rc;
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
 	return PSG_OK;
 }
 
@@ -253,11 +347,10 @@ extern "C" int psg_set_state(psg_context *ctx, const double *lambdaH, const floa
 	if (!ctx) return PSG_E_INVAL;
 	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_set_state: no particles loaded");
 	PSG_CUDA(cudaSetDevice(ctx->device));
-	cudaStream_t s = ctx->stream;
-	const size_t n = ctx->n;
-	if (lambdaH) PSG_CUDA(cudaMemcpyAsync(ctx->d_lambdaH, lambdaH, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-	if (ie) PSG_CUDA(cudaMemcpyAsync(ctx->d_ie, ie, sizeof(float) * n, cudaMemcpyHostToDevice, s));
-	if (lasthit) PSG_CUDA(cudaMemcpyAsync(ctx->d_lasthit, lasthit, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s));
-	PSG_CUDA(cudaStreamSynchronize(s));
+	int rc = 0;
+	if (lambdaH && (rc = from_caller(ctx, ctx->d_lambdaH, lambdaH))) return rc;
+	if (ie && (rc = from_caller(ctx, ctx->d_ie, ie))) return rc;
+	if (lasthit && (rc = from_caller(ctx, ctx->d_lasthit, lasthit))) return rc;
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
 	return PSG_OK;
 }

@@ -46,7 +46,7 @@ struct psg_context {
 	double *d_kernel = nullptr;
 	int kernel_n = 0;
 
-	// particles, caller order
+	// particles (caller order until the first tree build, leaf order after it)
 	size_t n = 0;
 	double boxsize = 0;
 	float4 *d_psml = nullptr;    // x, y, z, sml
@@ -56,6 +56,8 @@ struct psg_context {
 	int32_t *d_hits = nullptr;
 	int64_t *d_lasthit = nullptr;
 	float *d_hstep = nullptr;    // last integrator step proposal, seconds (0: none yet)
+	uint32_t *d_order = nullptr; // after a tree build the arrays above are in leaf order:
+	                             // position k holds the caller's particle d_order[k] (null: caller order)
 
 	// octree, depth-first order
 	int have_tree = 0;
@@ -105,7 +107,7 @@ void *psg_scratch(psg_context *ctx, int slot, size_t bytes);
 enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
 	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
-	S_EMIT
+	S_EMIT, S_MAP, S_ALONG
 };
 
 // Per-launch timing: mark_begin/mark_end bracket a group of launches of one
@@ -122,6 +124,9 @@ inline void psg_mark_end(psg_context *ctx) {
 		ctx->nkev++;
 	}
 }
+
+// permutes every per-particle array by g (new[k] = old[g[k]]) and composes d_order
+int psg_permute_particles(psg_context *ctx, const uint32_t *g);
 
 // tree / trace entry points used across units
 int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_db);

@@ -313,127 +313,74 @@ __global__ void k_ray_lists(size_t nray, const int32_t *__restrict__ is_long, co
 	else short_rays[r - scan[r]] = (uint32_t)r;
 }
 
-// update_pars() loop.c:653-770 for the particles hit in tick t, one thread
-// per particle. A particle's deposits are summed in slot order; segments
-// longer than a warp (particles next to a source are hit by nearly every
-// ray) are summed by the whole warp, lanes strided, then a fixed butterfly.
+// Active particles of the batch whose deposit segment is longer than a warp
+// (particles next to a source are hit by nearly every ray); flag[na] = 0 so
+// that the scan's last entry is the total.
+__global__ void k_act_class(size_t na, const uint32_t *__restrict__ act_seg, int32_t *__restrict__ flag) {
+	const size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (a > na) return;
+	flag[a] = (a < na && act_seg[a + 1] - act_seg[a] > 32) ? 1 : 0;
+}
+__global__ void k_act_lists(size_t na, const int32_t *__restrict__ flag, const int32_t *__restrict__ scan,
+		uint32_t *__restrict__ long_act) {
+	const size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (a < na && flag[a]) long_act[scan[a]] = (uint32_t)a;
+}
+// first long entry of every tick
+__global__ void k_tick_long(int K, const int32_t *__restrict__ tick_act, const int32_t *__restrict__ scan,
+		int32_t *__restrict__ out) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t <= K) out[t] = scan[tick_act[t]];
+}
+
+// The particle's summed deposits of the tick: isothermal, the closed-form
+// update_pars() step (loop.c:653-770); otherwise the sums for the integrator.
 template <bool ISO>
-__global__ void __launch_bounds__(256) k_update(int t, const int32_t *__restrict__ tick_act,
-		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
-		const double *__restrict__ acc, const double *__restrict__ acc_heat, int want_heat,
-		double *__restrict__ lambdaH, float *__restrict__ ie, int32_t *__restrict__ hits,
+__device__ __forceinline__ void finish_particle(int a, double g, double heat, int nh,
+		const uint32_t *__restrict__ act_ipar, int32_t *__restrict__ hits, double *__restrict__ act_g,
+		double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
-		PhysParams P, int64_t tick, double tick_time, uint32_t *__restrict__ status) {
-	const int lo = tick_act[t], hi = tick_act[t + 1];
-	const int lane = threadIdx.x & 31;
-	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
-	const bool mine = a < hi;
-	if (__all_sync(0xffffffffu, !mine)) return;
-	uint32_t p = 0, s0 = 0, s1 = 0;
-	if (mine) {
-		p = act_ipar[a];
-		s0 = act_seg[a];
-		s1 = act_seg[a + 1];
+		const PhysParams &P, int64_t tick, double tick_time, uint32_t *__restrict__ status) {
+	const uint32_t p = act_ipar[a];
+	hits[p] += nh;
+	if (!ISO) {
+		act_g[a] = g;
+		act_heat[a] = heat;
+		return;
 	}
-	double g = 0.0, heat = 0.0;
-	int nh = 0;
-	const bool longseg = mine && (s1 - s0) > 32;
-	if (mine && !longseg) {
-		for (uint32_t k = s0; k < s1; k++) {
-			const double d = acc[k];
-			if (d >= 0.0) {
-				g += d;
-				if (want_heat) heat += acc_heat[k];
-				nh++;
-			}
-		}
-	}
-	unsigned lm = __ballot_sync(0xffffffffu, longseg);
-	while (lm) {
-		const int l = __ffs(lm) - 1;
-		lm &= lm - 1;
-		const uint32_t b0 = __shfl_sync(0xffffffffu, s0, l), b1 = __shfl_sync(0xffffffffu, s1, l);
-		double sg = 0.0, sh = 0.0;
-		int sn = 0;
-		// eight independent loads in flight per lane and round
-		uint32_t k = b0 + lane;
-		for (; k + 7 * 32 < b1; k += 8 * 32) {
-			double v[8];
-#pragma unroll
-			for (int u = 0; u < 8; u++) v[u] = acc[k + 32 * u];
-#pragma unroll
-			for (int u = 0; u < 8; u++) {
-				if (v[u] >= 0.0) {
-					sg += v[u];
-					if (want_heat) sh += acc_heat[k + 32 * u];
-					sn++;
-				}
-			}
-		}
-		for (; k < b1; k += 32) {
-			const double d = acc[k];
-			if (d >= 0.0) {
-				sg += d;
-				if (want_heat) sh += acc_heat[k];
-				sn++;
-			}
-		}
-#pragma unroll
-		for (int o = 16; o > 0; o >>= 1) {
-			sg += __shfl_xor_sync(0xffffffffu, sg, o);
-			sh += __shfl_xor_sync(0xffffffffu, sh, o);
-			sn += __shfl_xor_sync(0xffffffffu, sn, o);
-		}
-		if (lane == l) { g = sg; heat = sh; nh = sn; }
-	}
-	if (!mine) return;
 	const double time = rn_dmul((double)(tick - lasthit[p]), tick_time);
 	const double lam0 = lambdaH[p];
-	const double ie0 = (double)ie[p];
-	const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, lam0), P.he_e));
+	const double T = ieye2T(P, (double)ie[p], rn_dadd(rn_dsub(1.0, lam0), P.he_e));
 	const double nH = rn_dmul(P.H_PER_MASS, (double)rho[p]);
-	double lam = lam0, e = ie0;
-	uint32_t st;
-	if (ISO) st = solve_step_iso(P, lam, (double)yeMET[p], g, time, nH, T);
-	else st = solve_step(P, lam, e, (double)yeMET[p], g, heat, time, nH, T);
+	double lam = lam0;
+	const uint32_t st = solve_step_iso(P, lam, (double)yeMET[p], g, time, nH, T);
 	lambdaH[p] = lam;
-	if (ISO) {
-		ie[p] = (float)Tye2ie(P, T, rn_dadd(rn_dsub(1.0, lam), P.he_e));
-	} else if (!P.adiabatic) {
-		ie[p] = (float)e;
-	}
+	ie[p] = (float)Tye2ie(P, T, rn_dadd(rn_dsub(1.0, lam), P.he_e));
 	lasthit[p] = tick;
-	hits[p] += nh;
 	if (st) atomicOr(status, st);
 }
 
-// Per-particle sums of one tick's deposits (photons/NH, heat, deposit count),
-// in slot order; segments longer than a warp are summed by the whole warp.
-__global__ void __launch_bounds__(256) k_reduce_acc(int t, const int32_t *__restrict__ tick_act,
+// Per-particle sums of one tick's deposits (photons/NH, heat, deposit count)
+// in slot order. The first long_blocks blocks take the tick's long segments,
+// a warp each: lanes strided over the segment (eight loads in flight per
+// lane), then a fixed butterfly. The other blocks take the short ones, a
+// thread each. Particles are in leaf order, so the long ones are neighbours;
+// giving each its own warp keeps them from piling up on a few warps.
+template <bool ISO>
+__global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
 		const double *__restrict__ acc, const double *__restrict__ acc_heat, int want_heat,
-		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat) {
-	const int lo = tick_act[t], hi = tick_act[t + 1];
-	const int lane = threadIdx.x & 31;
-	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
-	const bool mine = a < hi;
-	if (__all_sync(0xffffffffu, !mine)) return;
-	uint32_t s0 = 0, s1 = 0;
-	if (mine) { s0 = act_seg[a]; s1 = act_seg[a + 1]; }
-	double g = 0.0, heat = 0.0;
-	int nh = 0;
-	const bool longseg = mine && (s1 - s0) > 32;
-	if (mine && !longseg) {
-		for (uint32_t k = s0; k < s1; k++) {
-			const double d = acc[k];
-			if (d >= 0.0) { g += d; if (want_heat) heat += acc_heat[k]; nh++; }
-		}
-	}
-	unsigned lm = __ballot_sync(0xffffffffu, longseg);
-	while (lm) {
-		const int l = __ffs(lm) - 1;
-		lm &= lm - 1;
-		const uint32_t b0 = __shfl_sync(0xffffffffu, s0, l), b1 = __shfl_sync(0xffffffffu, s1, l);
+		const uint32_t *__restrict__ long_act, int nlong, int long_blocks,
+		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat,
+		double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit,
+		const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P, int64_t tick,
+		double tick_time, uint32_t *__restrict__ status) {
+	if ((int)blockIdx.x < long_blocks) {
+		const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
+		const int lane = threadIdx.x & 31;
+		if (e >= nlong) return;
+		const int a = (int)long_act[e];
+		const uint32_t b0 = act_seg[a], b1 = act_seg[a + 1];
 		double sg = 0.0, sh = 0.0;
 		int sn = 0;
 		uint32_t k = b0 + lane;
@@ -455,12 +402,23 @@ __global__ void __launch_bounds__(256) k_reduce_acc(int t, const int32_t *__rest
 			sh += __shfl_xor_sync(0xffffffffu, sh, o);
 			sn += __shfl_xor_sync(0xffffffffu, sn, o);
 		}
-		if (lane == l) { g = sg; heat = sh; nh = sn; }
+		if (lane == 0)
+			finish_particle<ISO>(a, sg, sh, sn, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
+					P, tick, tick_time, status);
+		return;
 	}
-	if (!mine) return;
-	act_g[a] = g;
-	act_heat[a] = heat;
-	hits[act_ipar[a]] += nh;
+	const int a = tick_act[t] + (blockIdx.x - long_blocks) * blockDim.x + threadIdx.x;
+	if (a >= tick_act[t + 1]) return;
+	const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
+	if (s1 - s0 > 32) return;
+	double g = 0.0, heat = 0.0;
+	int nh = 0;
+	for (uint32_t k = s0; k < s1; k++) {
+		const double d = acc[k];
+		if (d >= 0.0) { g += d; if (want_heat) heat += acc_heat[k]; nh++; }
+	}
+	finish_particle<ISO>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET, P,
+			tick, tick_time, status);
 }
 
 // update_pars() loop.c:653-770, not isothermal: every lane integrates one
@@ -731,27 +689,45 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	k_ray_lists<<<blocks(nray, 256), 256, 0, st>>>(nray, is_long, long_scan, long_rays, short_rays);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 2;
-	// non-isothermal: per-particle sums and the integrator's work cursors
-	double *act_g = nullptr, *act_heat = nullptr;
-	unsigned *cursors = nullptr, *nstiff = nullptr;
-	StiffItem *stiff = nullptr;
+	// per-particle sums, the long-segment lists and (not isothermal) the
+	// integrator's work cursors and stiff lists
 	int dev_sms = 148;
 	cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
-	if (!ctx->flags.isothermal) {
-		const size_t na = (size_t)(h_tick_act[K] > 0 ? h_tick_act[K] : 1);
-		// the stiff list of a tick can hold every particle of the tick
-		size_t maxt = 1;
-		for (size_t t = 0; t < K; t++) maxt = std::max<size_t>(maxt, (size_t)(h_tick_act[t + 1] - h_tick_act[t]));
-		char *m = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * 2 * (K + 1)
-				+ sizeof(StiffItem) * maxt + 512);
-		if (!m) return PSG_E_NOMEM;
-		act_g = (double *)m;
-		act_heat = act_g + na;
-		cursors = (unsigned *)(act_heat + na);
-		nstiff = cursors + (K + 1);
-		stiff = (StiffItem *)(((uintptr_t)(nstiff + K + 1) + 15) & ~(uintptr_t)15);
-		PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * 2 * (K + 1), st));
+	const bool iso = ctx->flags.isothermal != 0;
+	const size_t na = (size_t)(h_tick_act[K] > 0 ? h_tick_act[K] : 1);
+	size_t maxt = 1;
+	for (size_t t = 0; t < K; t++) maxt = std::max<size_t>(maxt, (size_t)(h_tick_act[t + 1] - h_tick_act[t]));
+	char *um = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * 2 * (K + 1)
+			+ (iso ? 0 : sizeof(StiffItem) * maxt) + 512);
+	int32_t *aflag = (int32_t *)psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (3 * (na + 1) + K + 1) + 512);
+	if (!um || !aflag) return PSG_E_NOMEM;
+	double *act_g = (double *)um;
+	double *act_heat = act_g + na;
+	unsigned *cursors = (unsigned *)(act_heat + na);
+	unsigned *nstiff = cursors + (K + 1);
+	StiffItem *stiff = (StiffItem *)(((uintptr_t)(nstiff + K + 1) + 15) & ~(uintptr_t)15);
+	PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * 2 * (K + 1), st));
+	// the long segments of the batch, listed in order, and each tick's first
+	int32_t *ascan = aflag + (na + 1);
+	uint32_t *long_act = (uint32_t *)(ascan + (na + 1));
+	int32_t *tick_long = (int32_t *)(long_act + (na + 1));
+	k_act_class<<<blocks(na + 1, 256), 256, 0, st>>>(na, act_seg, aflag);
+	PSG_CHECK_LAUNCH();
+	{
+		size_t tmp = 0;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, aflag, ascan, (int)(na + 1), st));
+		void *dt = psg_scratch(ctx, S_CUB, tmp);
+		if (!dt) return PSG_E_NOMEM;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, aflag, ascan, (int)(na + 1), st));
 	}
+	k_act_lists<<<blocks(na, 256), 256, 0, st>>>(na, aflag, ascan, long_act);
+	PSG_CHECK_LAUNCH();
+	k_tick_long<<<blocks(K + 1, 256), 256, 0, st>>>((int)K, tick_act, ascan, tick_long);
+	PSG_CHECK_LAUNCH();
+	ctx->launches += 4;
+	std::vector<int32_t> h_tick_long(K + 1);
+	PSG_CUDA(cudaMemcpyAsync(h_tick_long.data(), tick_long, sizeof(int32_t) * (K + 1), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
 	for (size_t t = 0; t < K; t++) {
 		const int l0 = h_scan[t * R];
 		const int l1 = (t + 1 < K) ? h_scan[(t + 1) * R] : nlong_all;
@@ -768,26 +744,31 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 		const int nact_t = h_tick_act[t + 1] - h_tick_act[t];
 		psg_mark_begin(ctx, PSG_K_UPDATE);
 		if (nact_t > 0) {
-			if (ctx->flags.isothermal)
-				k_update<true><<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
-						acc_heat, want_heat, ctx->d_lambdaH, ctx->d_ie, ctx->d_hits, ctx->d_lasthit, ctx->d_rho,
-						ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, ctx->d_status);
-			else {
-				k_reduce_acc<<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat,
-						want_heat, ctx->d_hits, act_g, act_heat);
-				PSG_CHECK_LAUNCH();
+			const int64_t tick = first_tick + (int64_t)t;
+			const int nl = h_tick_long[t + 1] - h_tick_long[t];
+			const int lb = (nl + 7) / 8;
+			const unsigned rgrid = (unsigned)(lb + (int)blocks(nact_t, 256));
+			if (iso)
+				k_reduce<true><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat,
+						long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,
+						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, tick, tick_time, ctx->d_status);
+			else
+				k_reduce<false><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat,
+						long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,
+						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, tick, tick_time, ctx->d_status);
+			PSG_CHECK_LAUNCH();
+			ctx->launches++;
+			if (!iso) {
 				const unsigned qgrid = (unsigned)std::min<size_t>(blocks(nact_t, 256), (size_t)dev_sms * 8);
 				k_update_queue<<<qgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_g, act_heat, ctx->d_lambdaH,
-						ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, P, first_tick + (int64_t)t,
-						tick_time,
+						ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, P, tick, tick_time,
 						cursors + t, stiff, nstiff + t, ctx->d_status);
 				PSG_CHECK_LAUNCH();
 				k_update_stiff<<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
-						P, first_tick + (int64_t)t, ctx->d_status);
+						P, tick, ctx->d_status);
+				PSG_CHECK_LAUNCH();
 				ctx->launches += 2;
 			}
-			PSG_CHECK_LAUNCH();
-			ctx->launches++;
 		}
 		psg_mark_end(ctx);
 		ctx->launches++;

@@ -268,17 +268,24 @@ __global__ void k_hit_kernel(size_t nhit, const uint32_t *__restrict__ ipar, con
 	b_to_kern[h] = rn_dmul(sph_depth(P, r_h), rn_dmul(sml_inv, sml_inv));
 }
 
-// Runs of equal d inside a ray are put in ipar order (the reference leaves
-// their order to qsort); insertion sort, runs are almost always length 1.
+// The caller's index of internal particle i (order: null when the arrays
+// are still in caller order); ties in d are broken by it.
+__device__ __forceinline__ uint32_t caller_index(const uint32_t *__restrict__ order, uint32_t i) {
+	return order ? order[i] : i;
+}
+
+// Runs of equal d inside a ray are put in the caller's ipar order (the
+// reference leaves their order to qsort); insertion sort, runs are almost
+// always length 1.
 __global__ void k_break_ties(size_t nray, const int64_t *__restrict__ off, uint32_t *__restrict__ ipar,
-		double *__restrict__ d, double *__restrict__ b) {
+		double *__restrict__ d, double *__restrict__ b, const uint32_t *__restrict__ order) {
 	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (r >= nray) return;
 	const int64_t h0 = off[r], h1 = off[r + 1];
 	for (int64_t h = h0 + 1; h < h1; h++) {
 		if (d[h] != d[h - 1]) continue;
 		int64_t k = h;
-		while (k > h0 && d[k - 1] == d[k] && ipar[k - 1] > ipar[k]) {
+		while (k > h0 && d[k - 1] == d[k] && caller_index(order, ipar[k - 1]) > caller_index(order, ipar[k])) {
 			const uint32_t ti = ipar[k]; ipar[k] = ipar[k - 1]; ipar[k - 1] = ti;
 			const double tb = b[k]; b[k] = b[k - 1]; b[k - 1] = tb;
 			k--;
@@ -298,7 +305,7 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 		const int64_t *__restrict__ off, size_t scap, const uint32_t *__restrict__ slab_ipar,
 		const double *__restrict__ slab_d, const double *__restrict__ slab_b, uint32_t *__restrict__ out_ipar,
 		double *__restrict__ out_d, double *__restrict__ out_b, int want_kern, const float4 *__restrict__ psml,
-		PhysParams P) {
+		PhysParams P, const uint32_t *__restrict__ order) {
 	constexpr int NMAX = TPR * IPT;
 	using Sort = cub::BlockRadixSort<uint32_t, TPR, IPT, uint32_t, 4>;
 	struct Smem {
@@ -338,12 +345,12 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 		for (int a = i + 1; a <= e; a++) {
 			const uint32_t pa = sm.pos[a];
 			const double da = raw_d[pa];
-			const uint32_t ia = raw_ipar[pa];
+			const uint32_t ia = caller_index(order, raw_ipar[pa]);
 			int c = a;
 			while (c > i) {
 				const uint32_t pc = sm.pos[c - 1];
 				const double dc = raw_d[pc];
-				if (dc < da || (dc == da && raw_ipar[pc] < ia)) break;
+				if (dc < da || (dc == da && caller_index(order, raw_ipar[pc]) < ia)) break;
 				sm.pos[c] = pc;
 				c--;
 			}
@@ -487,7 +494,7 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 				if (smem > 48 * 1024)
 					PSG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 				kern<<<(unsigned)nl, tpr, smem, st>>>(lst, (int)nl, off64, scap, slab_ipar, slab_d, slab_b, hit_ipar,
-						hit_d, hit_b, want_kern, ctx->d_psml, PP);
+						hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order);
 				PSG_CHECK_LAUNCH();
 				return PSG_OK;
 			};
@@ -522,7 +529,7 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 			k_gather_sorted<<<blocks(nhit, 256), 256, 0, st>>>(nhit, vals + hb, raw_ipar, raw_d, raw_b,
 					hit_ipar, hit_d, hit_b);
 			PSG_CHECK_LAUNCH();
-			k_break_ties<<<blocks(nray, 128), 128, 0, st>>>(nray, off64, hit_ipar, hit_d, hit_b);
+			k_break_ties<<<blocks(nray, 128), 128, 0, st>>>(nray, off64, hit_ipar, hit_d, hit_b, ctx->d_order);
 			PSG_CHECK_LAUNCH();
 			ctx->launches += 4;
 			if (want_kern) {
@@ -535,6 +542,12 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 		psg_mark_end(ctx);
 	}
 	return PSG_OK;
+}
+
+__global__ void k_caller_index(size_t n, const uint32_t *__restrict__ in, const uint32_t *__restrict__ order,
+		uint32_t *__restrict__ out) {
+	const size_t h = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (h < n) out[h] = order[in[h]];
 }
 
 // copies the traced hit lists to host Xtype records
@@ -560,7 +573,16 @@ static int download_hits(psg_context *ctx, size_t nray, int64_t *offsets, psg_xt
 		std::vector<double> d(nhit), b(nhit);
 		const size_t hb = nhit;
 		double *hit_d = (double *)ctx->scratch[S_RAW_D].p + hb;
-		PSG_CUDA(cudaMemcpyAsync(ip.data(), ctx->scratch[S_HIT_IPAR].p, sizeof(uint32_t) * nhit, cudaMemcpyDeviceToHost, st));
+		// hits carry internal particle positions: the caller's indices
+		const uint32_t *hit_ipar = (const uint32_t *)ctx->scratch[S_HIT_IPAR].p;
+		if (ctx->d_order) {
+			uint32_t *mapped = (uint32_t *)psg_scratch(ctx, S_MAP, sizeof(uint32_t) * nhit);
+			if (!mapped) return PSG_E_NOMEM;
+			k_caller_index<<<(unsigned)((nhit + 255) / 256), 256, 0, st>>>(nhit, hit_ipar, ctx->d_order, mapped);
+			PSG_CHECK_LAUNCH();
+			hit_ipar = mapped;
+		}
+		PSG_CUDA(cudaMemcpyAsync(ip.data(), hit_ipar, sizeof(uint32_t) * nhit, cudaMemcpyDeviceToHost, st));
 		PSG_CUDA(cudaMemcpyAsync(d.data(), hit_d, sizeof(double) * nhit, cudaMemcpyDeviceToHost, st));
 		PSG_CUDA(cudaMemcpyAsync(b.data(), ctx->scratch[S_HIT_KERN].p, sizeof(double) * nhit, cudaMemcpyDeviceToHost, st));
 		PSG_CUDA(cudaStreamSynchronize(st));

@@ -238,14 +238,15 @@ __global__ void k_emit_wide(Cells c, int ncell, float4 *__restrict__ out_lo, flo
 	out_hi[cell] = make_float4(z.x, z.y, z.z, __int_as_float((int)c.start[cell]));
 }
 
-__global__ void k_gather_particles(size_t nvalid, const uint32_t *__restrict__ order,
-		const float4 *__restrict__ psml, const int8_t *__restrict__ flag,
+// The traversal's copy of the particles in the box (the first nvalid of the
+// leaf order, which the particle arrays are already in) and their index,
+// marked when flagged PF_INVALID (psystem.h:28).
+__global__ void k_gather_particles(size_t nvalid, const float4 *__restrict__ psml, const int8_t *__restrict__ flag,
 		float4 *__restrict__ lpsml, uint32_t *__restrict__ lidx) {
 	const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (k >= nvalid) return;
-	const uint32_t i = order[k];
-	lpsml[k] = psml[i];
-	lidx[k] = i | ((flag[i] & 1) ? PSG_INVALID_BIT : 0u);
+	lpsml[k] = psml[k];
+	lidx[k] = (uint32_t)k | ((flag[k] & 1) ? PSG_INVALID_BIT : 0u);
 }
 
 inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -282,6 +283,12 @@ extern "C" int psg_build_tree(psg_context *ctx, int ppc) {
 	PSG_CUDA(cudaMemcpyAsync(&nvalid, d_nvalid, sizeof(nvalid), cudaMemcpyDeviceToHost, st));
 	PSG_CUDA(cudaStreamSynchronize(st));
 
+	// every per-particle array into the leaf order of this tree (vals_s
+	// holds the current positions sorted by key, the particles outside the
+	// box last)
+	int prc = psg_permute_particles(ctx, vals_s);
+	if (prc) return prc;
+
 	// particles in leaf order
 	if (ctx->d_leaf_psml) cudaFree(ctx->d_leaf_psml);
 	if (ctx->d_leaf_idx) cudaFree(ctx->d_leaf_idx);
@@ -291,8 +298,8 @@ extern "C" int psg_build_tree(psg_context *ctx, int ppc) {
 	PSG_CUDA(cudaMalloc(&ctx->d_leaf_psml, sizeof(float4) * (nvalid + 1)));
 	PSG_CUDA(cudaMalloc(&ctx->d_leaf_idx, sizeof(uint32_t) * (nvalid + 1)));
 	if (nvalid)
-		k_gather_particles<<<blocks(nvalid, 256), 256, 0, st>>>(nvalid, vals_s, ctx->d_psml,
-				ctx->d_flag, ctx->d_leaf_psml, ctx->d_leaf_idx);
+		k_gather_particles<<<blocks(nvalid, 256), 256, 0, st>>>(nvalid, ctx->d_psml, ctx->d_flag,
+				ctx->d_leaf_psml, ctx->d_leaf_idx);
 	PSG_CHECK_LAUNCH();
 
 	// 3: cells level by level. A run of more than ppc equal level-L prefixes
@@ -439,9 +446,10 @@ extern "C" int psg_get_tree(psg_context *ctx, float *bot, float *top, int32_t *s
 	if (pstart)
 		for (size_t i = 0; i <= nc; i++) memcpy(&pstart[i], &hi[i].w, sizeof(int32_t));
 	if (order && ctx->nvalid) {
+		// leaf order as the caller's particle indices
 		std::vector<uint32_t> idx(ctx->nvalid);
-		PSG_CUDA(cudaMemcpy(idx.data(), ctx->d_leaf_idx, sizeof(uint32_t) * ctx->nvalid, cudaMemcpyDeviceToHost));
-		for (size_t k = 0; k < ctx->nvalid; k++) order[k] = (int32_t)(idx[k] & ~PSG_INVALID_BIT);
+		PSG_CUDA(cudaMemcpy(idx.data(), ctx->d_order, sizeof(uint32_t) * ctx->nvalid, cudaMemcpyDeviceToHost));
+		for (size_t k = 0; k < ctx->nvalid; k++) order[k] = (int32_t)idx[k];
 	}
 	return PSG_OK;
 }
