@@ -362,6 +362,48 @@ def main():
     torch.cuda.synchronize(dev)
     em_t, em_hits = reduce_over_ranks(time.perf_counter() - t0, em_hits, dist, torch.device("cuda", dev))
 
+    # chemistry surrogate (not isothermal): the same steps from one state,
+    # on the integrator and with the network (trained weights shipped in
+    # psphray_b200/data), GPU s per simulated Myr and the x_HII difference
+    surrogate = None
+    surr_path = os.path.join(ROOT, "psphray_b200", "data", f"surrogate_{args.workload}.npz")
+    if not w.isothermal and os.path.exists(surr_path):
+        from psphray_b200.surrogate import Surrogate
+        net = Surrogate.load(surr_path)
+        nsurr, tol = 4, 1e-3
+        ts = t1 + (args.steps + 2) * T
+        s_rays = [torch.from_numpy(w.schedule.rays_for_ticks(ts + i * T, T).view(np.uint8)).to(f"cuda:{dev}")
+                  for i in range(nsurr)]
+        st0 = ctx.state()
+        keep = {k: st0[k] for k in ("lambdaH", "ie", "lasthit")}
+        res = {}
+        for mode in ("plain", "surrogate"):
+            ctx.set_state(**keep)
+            if mode == "surrogate":
+                net.install(ctx, tol=tol)
+            ms, acc, act = 0.0, 0.0, 0.0
+            for i in range(nsurr):
+                e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                st = ctx.run_ticks_device(s_rays[i].data_ptr(), R, T, ts + i * T, w.tick_time)
+                e1.record(stream)
+                e1.synchronize()
+                ms += e0.elapsed_time(e1)
+                acc += st["surrogate_accepted"]
+                act += st["active"]
+            res[mode] = (ms, acc / max(act, 1.0), 1.0 - ctx.lambdaH())
+            if mode == "surrogate":
+                Surrogate.uninstall(ctx)
+        myr = nsurr * T * w.tick_time / w.field.units.MYR
+        xp, xs = res["plain"][2], res["surrogate"][2]
+        rel = np.abs(xs - xp) / np.maximum(xp, 1e-6)
+        surrogate = {"tol": tol, "steps": nsurr, "ticks_per_step": T,
+                     "gpu_s_per_sim_myr_plain": res["plain"][0] / 1e3 / myr,
+                     "gpu_s_per_sim_myr_surrogate": res["surrogate"][0] / 1e3 / myr,
+                     "accepted_fraction": res["surrogate"][1],
+                     "x_HII_rel_diff": {"p50": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),
+                                        "max": float(rel.max())}}
+
     # roofline of the dominant kernel group
     peak, peak_kind = peaks()
     dom = max(api.KERNELS, key=lambda k: kms[k])
@@ -401,6 +443,7 @@ def main():
                          "path_achieved_gbs": path_gbs,
                          "path_frac": path_gbs / peak},
             "clocks": clk,
+            "surrogate": surrogate,
             "e2e_device_emission": {"value": em_hits / em_t, "unit": "hits/s", "h2d_bytes_per_step": 0,
                                     "d2h_bytes_per_step": int(lam.nbytes)},
             "e2e": {"value": e2e_hits / e2e_t, "unit": "hits/s",

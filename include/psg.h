@@ -186,6 +186,7 @@ typedef struct {
 	double launches;        /* kernels of this library launched by the call */
 	double kernel_ms[PSG_K_NKERNELS];        /* per kernel group, with timing on */
 	double kernel_launches[PSG_K_NKERNELS];
+	double surrogate_accepted;  /* particle updates taken from the surrogate (psg_set_surrogate) */
 } psg_tick_stats;
 
 /* Runs nticks ticks; rays holds nray_per_tick rays for each tick, tick by
@@ -271,6 +272,43 @@ int psg_step_evolve(psg_context *ctx, psg_step *steps, size_t n);
  * that device. Calls that overlap in time on one device race on the buffer. */
 #define PSG_NOALLOC_MAX_STEPS 16384
 int psg_step_evolve_noalloc(psg_context *ctx, psg_step *steps, size_t n);
+
+/* ---- chemistry surrogate: the network and its training ------------------- */
+/* No counterpart in the reference (it integrates every particle with LSODA):
+ * a 6 -> 64 -> 64 -> 2 perceptron with SiLU activations learns the
+ * non-isothermal update of one particle over one step. Parameters are one
+ * flat FP32 array: W1[64][8], b1[64], W2[64][64], b2[64], W3[2][64], b3[2]
+ * (inputs padded to 8). All pointers are device pointers. */
+#define PSG_MLP_NIN 8
+#define PSG_MLP_NPARAM 4866
+/* y[n][2] = net(x[n][8]) in FP32. */
+int psg_mlp_forward(psg_context *ctx, const float *params, const float *x, size_t n, float *y);
+/* grad[PSG_MLP_NPARAM + 1]: the gradient of the mean over the n samples of
+ * the summed squared error, then the summed squared error itself (also
+ * copied to *loss if loss is not NULL). Deterministic. */
+int psg_mlp_grad(psg_context *ctx, const float *params, const float *x, const float *t, size_t n,
+		float *grad, float *loss);
+/* Update log: while set, every non-isothermal tick appends one row of 8
+ * floats per particle update to rows (device, cap rows; *count, a device
+ * counter the caller zeroes, counts the updates offered): the surrogate's 5
+ * inputs (psg_surrogate.cuh: log nH*time, log T, logit lambdaH, log g,
+ * log heat/ie), its 2 targets (change of logit lambdaH and of log T) and a
+ * zero. rows = NULL switches it off. */
+int psg_set_update_log(psg_context *ctx, float *rows, size_t cap, unsigned long long *count);
+/* Installs a trained network for the non-isothermal ticks (params as for
+ * psg_mlp_forward; x_mu/x_sd[5] normalise the inputs, y_mu/y_sd[2]
+ * de-normalise the outputs). Every active particle's step is predicted on
+ * the tensor cores (BF16, FP32 accumulation); a prediction whose trapezoid
+ * residual exceeds tol (relative, see psg_surrogate.cu) is redone by the
+ * integrator. params = NULL switches the surrogate off. */
+int psg_set_surrogate(psg_context *ctx, const float *params, const float *x_mu, const float *x_sd,
+		const float *y_mu, const float *y_sd, float tol);
+/* The installed network on rows of raw inputs (device x[n][8], 5 used):
+ * y[n][2] de-normalised outputs, computed exactly as inside the ticks. */
+int psg_surrogate_forward(psg_context *ctx, const float *x, size_t n, float *y);
+/* One Adam step (step counts from 1). */
+int psg_mlp_adam(psg_context *ctx, float *params, const float *grad, float *m, float *v, float lr,
+		float beta1, float beta2, float eps, int step);
 
 #ifdef __cplusplus
 }

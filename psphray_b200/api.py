@@ -100,13 +100,15 @@ class CSpectrum(C.Structure):
 class TickStats(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("hits", "saturated", "active", "lost_photons",
                                           "trace_ms", "tick_ms", "launches")] + [
-        ("kernel_ms", C.c_double * len(KERNELS)), ("kernel_launches", C.c_double * len(KERNELS))]
+        ("kernel_ms", C.c_double * len(KERNELS)), ("kernel_launches", C.c_double * len(KERNELS)),
+        ("surrogate_accepted", C.c_double)]
 
 
 def _stats(st: TickStats) -> dict:
     d = {k: getattr(st, k) for k, _ in TickStats._fields_[:7]}
     d["kernel_ms"] = dict(zip(KERNELS, list(st.kernel_ms)))
     d["kernel_launches"] = dict(zip(KERNELS, list(st.kernel_launches)))
+    d["surrogate_accepted"] = st.surrogate_accepted
     return d
 
 
@@ -160,6 +162,12 @@ def lib() -> C.CDLL:
         "psg_get_sources": ([vp, vp, vp], C.c_int),
         "psg_emit_rays": ([vp, sz, sz, i64, dbl, vp], C.c_int),
         "psg_run_ticks_emit": ([vp, sz, sz, i64, dbl, C.POINTER(TickStats)], C.c_int),
+        "psg_mlp_forward": ([vp, vp, vp, sz, vp], C.c_int),
+        "psg_mlp_grad": ([vp, vp, vp, vp, sz, vp, vp], C.c_int),
+        "psg_mlp_adam": ([vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int], C.c_int),
+        "psg_set_update_log": ([vp, vp, sz, vp], C.c_int),
+        "psg_set_surrogate": ([vp, vp, vp, vp, vp, vp, C.c_float], C.c_int),
+        "psg_surrogate_forward": ([vp, vp, sz, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -245,6 +253,7 @@ class Context:
             raise PsgError(rc, f"psg_create(device={device}): no usable CUDA device")
         self.h = h
         self.n = 0
+        self.device = device
 
     def close(self):
         if getattr(self, "h", None):

@@ -21,6 +21,7 @@ int psg_cuda_fail(psg_context *ctx, cudaError_t e, const char *what, const char 
 }
 
 void *psg_scratch(psg_context *ctx, int slot, size_t bytes) {
+	if (slot < 0 || slot >= S_NSLOTS) return nullptr;
 	psg_buf &b = ctx->scratch[slot];
 	if (b.bytes >= bytes && b.p) return b.p;
 	if (b.p) cudaFree(b.p);
@@ -53,7 +54,7 @@ extern "C" int psg_create(psg_context **out, int device) {
 			cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
 			cudaMalloc(&ctx->d_status, sizeof(uint32_t)) != cudaSuccess ||
 			cudaMemset(ctx->d_status, 0, sizeof(uint32_t)) != cudaSuccess ||
-			cudaMalloc(&ctx->d_counters, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+			cudaMalloc(&ctx->d_counters, 16 * sizeof(unsigned long long)) != cudaSuccess) {
 		cudaGetLastError();
 		delete ctx;
 		return PSG_E_CUDA;
@@ -94,6 +95,7 @@ extern "C" void psg_destroy(psg_context *ctx) {
 	if (ctx->d_status) cudaFree(ctx->d_status);
 	if (ctx->d_counters) cudaFree(ctx->d_counters);
 	if (ctx->d_emit) cudaFree(ctx->d_emit);
+	if (ctx->d_surr) cudaFree(ctx->d_surr);
 	for (auto &b : ctx->scratch) if (b.p) cudaFree(b.p);
 	for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
 	for (auto &ev : ctx->kev) if (ev) cudaEventDestroy(ev);

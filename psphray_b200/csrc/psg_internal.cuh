@@ -5,6 +5,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <algorithm>
+
 #include "psg.h"
 
 // Octree keys: 3 bits per level, child k = xbit | ybit<<1 | zbit<<2 as in
@@ -21,6 +23,15 @@
 #define PSG_ST_SOLVER 2u       // the general integrator hit its step limit
 #define PSG_ST_IE_NEG 4u       // internal energy would turn negative (solve.c:137-139)
 #define PSG_ST_STACK 8u        // traversal stack overflow
+#define PSG_ST_SURR 16u        // a surrogate tile's tensor-core step did not complete
+
+// scratch slots
+enum {
+	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
+	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
+	S_EMIT, S_MAP, S_ALONG, S_MLP, S_LOG, S_SURR,
+	S_NSLOTS
+};
 
 struct psg_buf {
 	void *p = nullptr;
@@ -75,11 +86,22 @@ struct psg_context {
 	int nsrc = 0, nspec = 0, nhist_total = 0, nspec_total = 0;
 	uint64_t emit_seed = 0;
 
+	// chemistry surrogate (not isothermal): weight blob, residual tolerance
+	void *d_surr = nullptr;
+	float surr_tol = 0.f;
+	int surr_on = 0;
+
+	// update log (surrogate training data), caller-owned device buffers
+	float *log_buf = nullptr;
+	size_t log_cap = 0;
+	unsigned long long *log_count = nullptr;
+
 	uint32_t *d_status = nullptr;
-	unsigned long long *d_counters = nullptr;   // 8 device counters (records, deposits capped, ...)
+	unsigned long long *d_counters = nullptr;   // 16 device counters: 1 capped deposits, 2 lost photons,
+	                                            // 4-7 trace/sort, 8 surrogate accepts
 
 	// scratch, grown on demand
-	psg_buf scratch[24];
+	psg_buf scratch[S_NSLOTS];
 	size_t slab_cap = 0;  // hits each ray can hold in the traversal's output slabs
 	int ppc = 8;          // leaf capacity of the current tree
 	cudaEvent_t ev[8] = {};
@@ -103,12 +125,6 @@ int psg_cuda_fail(psg_context *ctx, cudaError_t e, const char *what, const char 
 // scratch buffer slot `slot` with at least `bytes`; returns nullptr on failure
 void *psg_scratch(psg_context *ctx, int slot, size_t bytes);
 
-// scratch slots
-enum {
-	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
-	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
-	S_EMIT, S_MAP, S_ALONG
-};
 
 // Per-launch timing: mark_begin/mark_end bracket a group of launches of one
 // kind with events on the context's stream (only when timing is on).
@@ -127,6 +143,12 @@ inline void psg_mark_end(psg_context *ctx) {
 
 // permutes every per-particle array by g (new[k] = old[g[k]]) and composes d_order
 int psg_permute_particles(psg_context *ctx, const uint32_t *g);
+
+// the surrogate's tick (psg_surrogate.cu)
+struct PhysParams;
+int psg_surrogate_tick(psg_context *ctx, int t, int nact_t, const int32_t *tick_act, const uint32_t *act_ipar,
+		const double *act_g, const double *act_heat, const PhysParams &P, int64_t tick, double tick_time,
+		uint32_t *rej, unsigned *nrej, int sms);
 
 // tree / trace entry points used across units
 int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_db);

@@ -23,6 +23,7 @@
 
 #include "psg_internal.cuh"
 #include "psg_solve.cuh"
+#include "psg_surrogate.cuh"
 
 PhysParams psg_phys_params(const psg_context *ctx) {
 	PhysParams P{};
@@ -435,9 +436,11 @@ __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__re
 		const double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
 		float *__restrict__ hstep, PhysParams P, int64_t tick, double tick_time, unsigned *__restrict__ cursor,
-		StiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff, uint32_t *__restrict__ status) {
+		StiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff, const uint32_t *__restrict__ alist,
+		const unsigned *__restrict__ nalist, uint32_t *__restrict__ status) {
+	// the tick's particles, or only those listed in alist (the surrogate's rejects)
 	const int lo = tick_act[t], hi = tick_act[t + 1];
-	const unsigned n = (unsigned)(hi - lo);
+	const unsigned n = alist ? *nalist : (unsigned)(hi - lo);
 	const int lane = threadIdx.x & 31;
 	const unsigned lt_mask = (1u << lane) - 1u;
 	DPState S;
@@ -456,7 +459,7 @@ __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__re
 			if (!have) {
 				const unsigned k = base + __popc(need & lt_mask);
 				if (k < n) {
-					const int a = lo + (int)k;
+					const int a = alist ? (int)alist[k] : lo + (int)k;
 					p = act_ipar[a];
 					const double time = rn_dmul((double)(tick - lasthit[p]), tick_time);
 					const double lam0 = lambdaH[p];
@@ -522,6 +525,49 @@ __global__ void __launch_bounds__(64) k_update_stiff(const StiffItem *__restrict
 		lasthit[it.p] = tick;
 	}
 	if (st) atomicOr(status, st);
+}
+
+// Update log (training data of the surrogate): the inputs of every active
+// particle's step before the update, the outputs after it.
+__global__ void k_log_pre(int t, const int32_t *__restrict__ tick_act, const uint32_t *__restrict__ act_ipar,
+		const double *__restrict__ act_g, const double *__restrict__ act_heat, const double *__restrict__ lambdaH,
+		const float *__restrict__ ie, const int64_t *__restrict__ lasthit, const float *__restrict__ rho,
+		const float *__restrict__ yeMET, PhysParams P, int64_t tick, double tick_time, float *__restrict__ feat) {
+	const int lo = tick_act[t];
+	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
+	if (a >= tick_act[t + 1]) return;
+	const uint32_t p = act_ipar[a];
+	const double time = rn_dmul((double)(tick - lasthit[p]), tick_time);
+	const double lam0 = lambdaH[p], ie0 = (double)ie[p];
+	const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, lam0), P.he_e));
+	const RhsCtx cx = make_rhs_ctx(P, (double)yeMET[p], act_g[a], act_heat[a], time,
+			rn_dmul(P.H_PER_MASS, (double)rho[p]), T);
+	float f[PSG_SURR_NFEAT];
+	surr_features(cx, lam0, ie0, f);
+	for (int i = 0; i < PSG_SURR_NFEAT; i++) feat[(size_t)(a - lo) * 8 + i] = f[i];
+}
+
+__global__ void k_log_post(int t, const int32_t *__restrict__ tick_act, const uint32_t *__restrict__ act_ipar,
+		const double *__restrict__ lambdaH, const float *__restrict__ ie, const float *__restrict__ yeMET,
+		PhysParams P, const float *__restrict__ feat, float *__restrict__ out, size_t cap,
+		unsigned long long *__restrict__ count) {
+	const int lo = tick_act[t];
+	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
+	if (a >= tick_act[t + 1]) return;
+	const uint32_t p = act_ipar[a];
+	const double lam1 = lambdaH[p];
+	const double T1 = ieye2T(P, (double)ie[p], rn_dadd(rn_dsub(1.0, lam1), P.he_e));
+	const float *f = feat + (size_t)(a - lo) * 8;
+	const float y0 = (float)(surr_logit(lam1) - (double)f[2]);
+	const float y1 = (float)(log10(fmax(T1, 1e-300)) - (double)f[1]);
+	if (!isfinite(y0) || !isfinite(y1)) return;
+	const unsigned long long row = atomicAdd(count, 1ull);
+	if (row >= cap) return;
+	float *o = out + row * 8;
+	for (int i = 0; i < PSG_SURR_NFEAT; i++) o[i] = f[i];
+	o[5] = y0;
+	o[6] = y1;
+	o[7] = 0.0f;
 }
 
 __global__ void k_step_evolve(psg_step *steps, size_t n, PhysParams P, uint32_t *status) {
@@ -697,16 +743,25 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	const size_t na = (size_t)(h_tick_act[K] > 0 ? h_tick_act[K] : 1);
 	size_t maxt = 1;
 	for (size_t t = 0; t < K; t++) maxt = std::max<size_t>(maxt, (size_t)(h_tick_act[t + 1] - h_tick_act[t]));
-	char *um = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * 2 * (K + 1)
-			+ (iso ? 0 : sizeof(StiffItem) * maxt) + 512);
+	const bool surr = !iso && ctx->surr_on && !ctx->flags.adiabatic;
+	char *um = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * 3 * (K + 1)
+			+ (iso ? 0 : sizeof(StiffItem) * maxt) + (surr ? sizeof(uint32_t) * maxt : 0) + 512);
 	int32_t *aflag = (int32_t *)psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (3 * (na + 1) + K + 1) + 512);
 	if (!um || !aflag) return PSG_E_NOMEM;
 	double *act_g = (double *)um;
 	double *act_heat = act_g + na;
 	unsigned *cursors = (unsigned *)(act_heat + na);
 	unsigned *nstiff = cursors + (K + 1);
-	StiffItem *stiff = (StiffItem *)(((uintptr_t)(nstiff + K + 1) + 15) & ~(uintptr_t)15);
-	PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * 2 * (K + 1), st));
+	unsigned *nrej = nstiff + (K + 1);
+	StiffItem *stiff = (StiffItem *)(((uintptr_t)(nrej + K + 1) + 15) & ~(uintptr_t)15);
+	uint32_t *rej = (uint32_t *)(stiff + (iso ? 0 : maxt));
+	PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * 3 * (K + 1), st));
+	if (surr) PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 8, 0, sizeof(unsigned long long), st));
+	float *feat = nullptr;
+	if (ctx->log_buf && !iso) {
+		feat = (float *)psg_scratch(ctx, S_LOG, sizeof(float) * 8 * maxt);
+		if (!feat) return PSG_E_NOMEM;
+	}
 	// the long segments of the batch, listed in order, and each tick's first
 	int32_t *ascan = aflag + (na + 1);
 	uint32_t *long_act = (uint32_t *)(ascan + (na + 1));
@@ -760,14 +815,32 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 			ctx->launches++;
 			if (!iso) {
 				const unsigned qgrid = (unsigned)std::min<size_t>(blocks(nact_t, 256), (size_t)dev_sms * 8);
+				if (feat) {
+					k_log_pre<<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_g, act_heat,
+							ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, tick, tick_time, feat);
+					PSG_CHECK_LAUNCH();
+				}
+				if (surr) {
+					// the network first; the integrator takes its rejects
+					rc = psg_surrogate_tick(ctx, (int)t, nact_t, tick_act, act_ipar, act_g, act_heat, P, tick,
+							tick_time, rej, nrej + t, dev_sms);
+					if (rc) return rc;
+					ctx->launches++;
+				}
 				k_update_queue<<<qgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_g, act_heat, ctx->d_lambdaH,
 						ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, P, tick, tick_time,
-						cursors + t, stiff, nstiff + t, ctx->d_status);
+						cursors + t, stiff, nstiff + t, surr ? rej : nullptr, surr ? nrej + t : nullptr,
+						ctx->d_status);
 				PSG_CHECK_LAUNCH();
 				k_update_stiff<<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
 						P, tick, ctx->d_status);
 				PSG_CHECK_LAUNCH();
 				ctx->launches += 2;
+				if (feat) {
+					k_log_post<<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, ctx->d_lambdaH,
+							ctx->d_ie, ctx->d_yeMET, P, feat, ctx->log_buf, ctx->log_cap, ctx->log_count);
+					PSG_CHECK_LAUNCH();
+				}
 			}
 		}
 		psg_mark_end(ctx);
@@ -792,6 +865,13 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 		stats->trace_ms = trace_ms;
 		stats->tick_ms = tick_ms;
 		stats->launches = (double)ctx->launches;
+		stats->surrogate_accepted = 0.0;
+		if (surr) {
+			unsigned long long acc_n = 0;
+			PSG_CUDA(cudaMemcpyAsync(&acc_n, ctx->d_counters + 8, sizeof(acc_n), cudaMemcpyDeviceToHost, st));
+			PSG_CUDA(cudaStreamSynchronize(st));
+			stats->surrogate_accepted = (double)acc_n;
+		}
 		for (int k = 0; k < PSG_K_NKERNELS; k++) stats->kernel_ms[k] = stats->kernel_launches[k] = 0.0;
 		for (int i = 0; i < ctx->nkev; i++) {
 			float ms = 0.f;
@@ -900,5 +980,14 @@ extern "C" int psg_step_evolve_noalloc(psg_context *ctx, psg_step *steps, size_t
 				(status & PSG_ST_NAN) ? " non-finite state" : "",
 				(status & PSG_ST_SOLVER) ? " integrator step limit" : "",
 				(status & PSG_ST_IE_NEG) ? " negative internal energy" : "");
+	return PSG_OK;
+}
+
+extern "C" int psg_set_update_log(psg_context *ctx, float *d_rows, size_t cap, unsigned long long *d_count) {
+	if (!ctx) return PSG_E_INVAL;
+	if (d_rows && (!d_count || cap == 0)) return psg_fail(ctx, PSG_E_INVAL, "psg_set_update_log: need a counter and capacity");
+	ctx->log_buf = d_rows;
+	ctx->log_cap = d_rows ? cap : 0;
+	ctx->log_count = d_rows ? d_count : nullptr;
 	return PSG_OK;
 }

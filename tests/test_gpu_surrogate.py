@@ -1,0 +1,141 @@
+"""The chemistry surrogate on the GPU: the training kernels against the
+float64 oracle (oracle/mlp.py), the tensor-core network against the FP32
+one, training that learns, and the ticks with the surrogate against the
+plain integrator -- identical when every prediction is rejected, close in
+x_HII when predictions are accepted."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from mlp import NPARAM, forward, init_params, loss_and_grad
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _rows(rng, n):
+    x = np.zeros((n, 8), np.float32)
+    x[:, :5] = rng.normal(size=(n, 5))
+    return x
+
+
+def test_mlp_grad_and_forward_vs_oracle(gpu_ctx):
+    from psphray_b200 import api
+    rng = np.random.default_rng(0)
+    p = (init_params(2) + rng.normal(0, 0.05, NPARAM)).astype(np.float32)
+    x = _rows(rng, 3001)
+    t = rng.normal(size=(3001, 2)).astype(np.float32)
+    dp, dx, dt = _t(p), _t(x), _t(t)
+    grad = _t(np.zeros(NPARAM + 1))
+    y = _t(np.zeros((3001, 2)))
+    L = api.lib()
+    gpu_ctx._check(L.psg_mlp_grad(gpu_ctx.h, _p(dp), _p(dx), _p(dt), 3001, _p(grad), None), "grad")
+    gpu_ctx._check(L.psg_mlp_forward(gpu_ctx.h, _p(dp), _p(dx), 3001, _p(y)), "forward")
+    sse, g = loss_and_grad(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64))
+    gg = grad.cpu().numpy().astype(np.float64)
+    # FP32 sums of 3001 samples against float64
+    assert np.linalg.norm(gg[:NPARAM] - g) <= 1e-4 * np.linalg.norm(g)
+    assert abs(gg[NPARAM] - sse) <= 1e-5 * sse
+    assert np.max(np.abs(y.cpu().numpy() - forward(p.astype(np.float64), x.astype(np.float64)))) < 1e-4
+    # deterministic: the same call gives the same bits
+    grad2 = _t(np.zeros(NPARAM + 1))
+    gpu_ctx._check(L.psg_mlp_grad(gpu_ctx.h, _p(dp), _p(dx), _p(dt), 3001, _p(grad2), None), "grad")
+    assert np.array_equal(grad.cpu().numpy(), grad2.cpu().numpy())
+
+
+def test_adam_step(gpu_ctx):
+    from psphray_b200 import api
+    rng = np.random.default_rng(1)
+    p, g = rng.normal(size=NPARAM).astype(np.float32), rng.normal(size=NPARAM + 1).astype(np.float32)
+    m, v = rng.normal(size=NPARAM).astype(np.float32) * 0.1, rng.random(NPARAM).astype(np.float32) * 0.1
+    dp, dg, dm, dv = _t(p), _t(g), _t(m), _t(v)
+    gpu_ctx._check(api.lib().psg_mlp_adam(gpu_ctx.h, _p(dp), _p(dg), _p(dm), _p(dv), C.c_float(1e-3), C.c_float(0.9),
+                                          C.c_float(0.999), C.c_float(1e-8), 3), "adam")
+    m1 = 0.9 * m + 0.1 * g[:NPARAM]
+    v1 = 0.999 * v + 0.001 * g[:NPARAM] ** 2
+    p1 = p - 1e-3 * (m1 / (1 - 0.9 ** 3)) / (np.sqrt(v1 / (1 - 0.999 ** 3)) + 1e-8)
+    assert np.allclose(dp.cpu().numpy(), p1, rtol=1e-5, atol=1e-7)
+
+
+def test_tensor_core_network_vs_fp32(gpu_ctx, phys_noniso):
+    """psg_surrogate_forward (BF16 tcgen05, normalisation folded into layer 1)
+    against the float64 network on the normalised inputs."""
+    from psphray_b200.surrogate import Surrogate
+    rng = np.random.default_rng(5)
+    p = (init_params(7) + rng.normal(0, 0.02, NPARAM)).astype(np.float32)
+    x_mu = rng.normal(size=5).astype(np.float32)
+    x_sd = (0.5 + rng.random(5)).astype(np.float32)
+    y_mu, y_sd = np.array([0.1, -0.2], np.float32), np.array([0.5, 2.0], np.float32)
+    s = Surrogate(p, x_mu, x_sd, y_mu, y_sd)
+    gpu_ctx.set_physics(phys_noniso)
+    s.install(gpu_ctx, tol=1e-3)
+    n = 1000                                     # 8 tiles, the last one partial
+    raw = np.zeros((n, 8), np.float32)
+    raw[:, :5] = x_mu + x_sd * rng.normal(size=(n, 5)).astype(np.float32)
+    y = s.predict(gpu_ctx, _t(raw)).cpu().numpy().astype(np.float64)
+    xn = np.zeros((n, 8))
+    xn[:, :5] = (raw[:, :5] - x_mu) / x_sd
+    ref = forward(p.astype(np.float64), xn) * y_sd + y_mu
+    err = (y - ref) / y_sd                       # in units of the output scale
+    # BF16 operands (8-bit mantissa), FP32 accumulation: about 1% of the scale
+    assert np.sqrt(np.mean(err ** 2)) < 0.02
+    assert np.max(np.abs(err)) < 0.1
+    Surrogate.uninstall(gpu_ctx)
+
+
+def _noniso_ctx(phys_noniso, n_side=24):
+    from psphray_b200 import api, fields
+    w = fields.make_workload("lognormal128", n_side=n_side, nray=256, seed=3)
+    ctx = api.Context(0)
+    ctx.set_physics(phys_noniso)
+    ctx.load(w.field)
+    ctx.build_tree(8)
+    return ctx, w
+
+
+def test_surrogate_ticks(phys_noniso):
+    """Logged updates -> training on the GPU -> ticks with the surrogate."""
+    from psphray_b200.surrogate import Surrogate, collect, fit
+    a, w = _noniso_ctx(phys_noniso)
+    b, _ = _noniso_ctx(phys_noniso)
+    c, _ = _noniso_ctx(phys_noniso)
+    try:
+        rays = w.schedule.rays_for_ticks
+        rows, tick = collect(a, rays, 256, 4, 3, 1, w.tick_time, 2_000_000)
+        assert rows.shape[0] > 1000
+        s, hist = fit(a, rows, epochs=25, batch=512, lr=3e-3, log=lambda *_: None)
+        assert hist[-1] < 0.05      # it learns: most of the targets' variance explained
+        # b: the same ticks on the plain integrator; c: with the surrogate
+        rb = rays(1, 12)
+        b.run_ticks(rb, 256, 12, 1, w.tick_time)
+        # every prediction rejected (tolerance 0+): identical to the plain path
+        s.install(c, tol=1e-30)
+        st = c.run_ticks(rb, 256, 12, 1, w.tick_time)
+        assert st["surrogate_accepted"] == 0
+        sb, sc = b.state(), c.state()
+        for k in ("lambdaH", "ie", "hits", "lasthit"):
+            assert np.array_equal(sb[k], sc[k]), k
+        # accepting predictions: x_HII within 1% of the integrator's
+        s.install(c, tol=1e-3)
+        rb2 = rays(13, 8)
+        st = c.run_ticks(rb2, 256, 8, 13, w.tick_time)
+        b.run_ticks(rb2, 256, 8, 13, w.tick_time)
+        assert st["surrogate_accepted"] > 0
+        xb, xc = 1.0 - b.state()["lambdaH"], 1.0 - c.state()["lambdaH"]
+        rel = np.abs(xc - xb) / np.maximum(xb, 1e-6)
+        # the residual tolerance bounds each accepted step to about 1e-3;
+        # over 8 ticks most particles stay far inside 1%
+        assert np.median(rel) < 1e-3
+        assert np.percentile(rel, 99) < 2e-2
+    finally:
+        for ctx in (a, b, c):
+            ctx.close()
