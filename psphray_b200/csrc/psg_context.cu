@@ -1,4 +1,5 @@
 // Context lifetime, error reporting, physics tables and particle upload.
+#include <math.h>
 #include <stdarg.h>
 #include <stdlib.h>
 #include <string.h>
@@ -90,6 +91,7 @@ extern "C" void psg_destroy(psg_context *ctx) {
 	free_particles(ctx);
 	free_tree(ctx);
 	if (ctx->d_ar) cudaFree(ctx->d_ar);
+	if (ctx->d_ar_ni) cudaFree(ctx->d_ar_ni);
 	if (ctx->d_xs) cudaFree(ctx->d_xs);
 	if (ctx->d_kernel) cudaFree(ctx->d_kernel);
 	if (ctx->d_status) cudaFree(ctx->d_status);
@@ -133,9 +135,11 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 		return psg_fail(ctx, PSG_E_INVAL, "psg_set_physics: only hydrogen-only runs (HOnly) are supported");
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	if (ctx->d_ar) cudaFree(ctx->d_ar);
+	if (ctx->d_ar_ni) cudaFree(ctx->d_ar_ni);
 	if (ctx->d_xs) cudaFree(ctx->d_xs);
 	if (ctx->d_kernel) cudaFree(ctx->d_kernel);
 	ctx->d_ar = ctx->d_xs = ctx->d_kernel = nullptr;
+	ctx->d_ar_ni = nullptr;
 	// rows of 16 doubles (one 128-byte line): log T, then the 15 rate columns
 	const size_t nr = (size_t)ar->nrows;
 	static_assert(PSG_AR_NCOLS + 1 == 16, "one rate row is one 128-byte line");
@@ -149,6 +153,36 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 	if (e1 == cudaSuccess) e1 = cudaMemcpy(ctx->d_ar, rows, sizeof(double) * nr * 16, cudaMemcpyHostToDevice);
 	free(rows);
 	PSG_CUDA(e1);
+	// The non-isothermal right-hand side needs 7 columns at one log T: one
+	// 64-byte row per table row, the 7 values and their slopes per unit log T
+	// in FP32, so a lookup is four 16-byte loads. Linear interpolation from
+	// value and slope is the same line as tabfun_get()'s two-point form.
+	{
+		const int cols[7] = {PSG_AR_HI_CI, flags->on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A,
+				flags->on_the_spot ? PSG_AR_HII_RCC_B : PSG_AR_HII_RCC_A, PSG_AR_HI_CEC, PSG_AR_HI_CIC,
+				PSG_AR_E_BREMC, PSG_AR_E_COMPC};
+		float *ni = (float *)calloc(nr * 16, sizeof(float));
+		if (!ni) return psg_fail(ctx, PSG_E_NOMEM, "psg_set_physics: host allocation failed");
+		// internal-unit rates (1e-140 .. 1e-56) are far below FP32's range:
+		// each column is stored divided by its largest magnitude
+		for (int c = 0; c < 7; c++) {
+			double m = 0.0;
+			for (size_t j = 0; j < nr; j++) m = fmax(m, fabs(ar->col[cols[c]][j]));
+			ctx->ar_ni_scale[c] = m > 0.0 ? m : 1.0;
+		}
+		for (size_t j = 0; j < nr; j++)
+			for (int c = 0; c < 7; c++) {
+				const double sc = ctx->ar_ni_scale[c];
+				const double v = ar->col[cols[c]][j] / sc;
+				const double s = j + 1 < nr ? (ar->col[cols[c]][j + 1] / sc - v) * ar->step_inv : 0.0;
+				ni[16 * j + c] = (float)v;
+				ni[16 * j + 8 + c] = (float)s;
+			}
+		cudaError_t e2 = cudaMalloc(&ctx->d_ar_ni, sizeof(float) * nr * 16);
+		if (e2 == cudaSuccess) e2 = cudaMemcpy(ctx->d_ar_ni, ni, sizeof(float) * nr * 16, cudaMemcpyHostToDevice);
+		free(ni);
+		PSG_CUDA(e2);
+	}
 	const size_t nx = (size_t)xs->nrows;
 	PSG_CUDA(cudaMalloc(&ctx->d_xs, sizeof(double) * nx * 2));
 	PSG_CUDA(cudaMemcpy(ctx->d_xs, xs->eng, sizeof(double) * nx, cudaMemcpyHostToDevice));
@@ -161,6 +195,7 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 	ctx->ar_nrows = ar->nrows;
 	ctx->ar_min = ar->min;
 	ctx->ar_step_inv = ar->step_inv;
+	ctx->ar_step = ar->step;
 	ctx->xs_nrows = xs->nrows;
 	ctx->xs_min = xs->min;
 	ctx->xs_step_inv = xs->step_inv;

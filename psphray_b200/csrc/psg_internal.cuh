@@ -29,7 +29,7 @@
 enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
 	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
-	S_EMIT, S_MAP, S_ALONG, S_MLP, S_LOG, S_SURR,
+	S_EMIT, S_MAP, S_ALONG, S_MLP, S_LOG, S_SURR, S_REC,
 	S_NSLOTS
 };
 
@@ -48,7 +48,11 @@ struct psg_context {
 	int have_physics = 0;
 	psg_units u{};
 	psg_flags flags{};
-	double *d_ar = nullptr;      // [PSG_AR_NCOLS + 1][ar_nrows]: logT first
+	double *d_ar = nullptr;      // [ar_nrows][16]: logT, then the PSG_AR_* columns
+	float4 *d_ar_ni = nullptr;   // [ar_nrows][4]: the 7 rates of the non-isothermal
+	                             // right-hand side, values then slopes per log T
+	double ar_step = 0;
+	double ar_ni_scale[7] = {};  // each d_ar_ni column is stored divided by this
 	int ar_nrows = 0;
 	double ar_min = 0, ar_step_inv = 0;
 	double *d_xs = nullptr;      // [2][xs_nrows]: energy, sigma_HI

@@ -21,8 +21,10 @@
 
 struct PhysParams {
 	const double *ar;      // [ar_nrows][16]: log T, then the PSG_AR_* columns
+	const float4 *ar_ni;   // [ar_nrows][4]: the right-hand side's 7 rates, values and slopes
+	double ar_ni_scale[7]; // ... each column divided by its largest magnitude
 	int ar_nrows;
-	double ar_min, ar_step_inv;
+	double ar_min, ar_step_inv, ar_step;
 	const double *xs;      // [2][xs_nrows]: energy, sigma_HI
 	int xs_nrows;
 	double xs_min, xs_step_inv, xs_cut_HI;
@@ -156,35 +158,35 @@ __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const
 	const double xHI = x[0], xHII = 1.0 - x[0];
 	const double ye = xHII + P.he_e + cx.yeMET;
 	const double T = cx.T_num * x[1] / __fma_rn(P.hmf, ye, cx.T_den0);
-	// row and weights of tabfun_get() (clamped rows: weight 1 on one row)
+	// the row of tabfun_get() and the offset into it (clamped rows: offset 0)
 	const double logT = log10(T);
-	const long long idx = (long long)((logT - P.ar_min) * P.ar_step_inv);
-	const double *r0, *r1;
-	double w0, w1;
-	if (idx >= 0 && idx < P.ar_nrows - 1) {
-		r0 = P.ar + (size_t)idx * 16;
-		r1 = r0 + 16;
-		w0 = (r1[0] - logT) * P.ar_step_inv;
-		w1 = (logT - r0[0]) * P.ar_step_inv;
+	long long idx = (long long)((logT - P.ar_min) * P.ar_step_inv);
+	double du;
+	if (idx < 0) {
+		idx = 0;
+		du = 0.0;
+	} else if (idx >= P.ar_nrows - 1) {
+		idx = P.ar_nrows - 1;
+		du = 0.0;
 	} else {
-		r0 = r1 = P.ar + (idx < 0 ? (size_t)0 : (size_t)(P.ar_nrows - 1) * 16);
-		w0 = 1.0;
-		w1 = 0.0;
+		du = logT - __fma_rn((double)idx, P.ar_step, P.ar_min);
 	}
-#define PSG_RATE(col) __fma_rn(w0, r0[1 + (col)], w1 * r1[1 + (col)])
-	const double gamma = PSG_RATE(PSG_AR_HI_CI) * cx.nHt;
-	const double alpha = PSG_RATE(P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A) * cx.nHt;
+	const float4 *row = P.ar_ni + 4 * idx;
+	const float4 v0 = row[0], v1 = row[1], s0 = row[2], s1 = row[3];
+#define PSG_LIN(v, s, c) (__fma_rn((double)(s), du, (double)(v)) * P.ar_ni_scale[c])
+	const double gamma = PSG_LIN(v0.x, s0.x, 0) * cx.nHt;
+	const double alpha = PSG_LIN(v0.y, s0.y, 1) * cx.nHt;       // case B on the spot, else A
 	dx[0] = __fma_rn(ye, __fma_rn(alpha, xHII, -gamma * xHI), -cx.g);
 	if (P.isothermal || P.adiabatic) {
 		dx[1] = 0.0;
 	} else {
-		const double ion = PSG_RATE(P.on_the_spot ? PSG_AR_HII_RCC_B : PSG_AR_HII_RCC_A) + PSG_RATE(PSG_AR_E_BREMC);
-		const double neu = PSG_RATE(PSG_AR_HI_CEC) + PSG_RATE(PSG_AR_HI_CIC);
-		const double chi = PSG_RATE(PSG_AR_E_COMPC);
+		const double ion = PSG_LIN(v0.z, s0.z, 2) + PSG_LIN(v1.y, s1.y, 5);     // recombination + bremsstrahlung
+		const double neu = PSG_LIN(v0.w, s0.w, 3) + PSG_LIN(v1.x, s1.x, 4);     // excitation + ionisation
+		const double chi = PSG_LIN(v1.z, s1.z, 6);                           // Compton
 		const double L = __fma_rn(cx.nH, __fma_rn(neu, xHI, ion * xHII), chi);
 		dx[1] = __fma_rn(-cx.hpt * ye, L, cx.heat);
 	}
-#undef PSG_RATE
+#undef PSG_LIN
 }
 
 // Adaptive Dormand-Prince 5(4) over s in [0,1]. LSODA runs the reference at
@@ -202,6 +204,21 @@ struct DPState {
 #define DP_RTOL 1e-6
 #define DP_ATOL0 1e-10
 #define DP_ATOL1_REL 1e-8
+
+// First step from the derivative S.k1 = f(S.x), already evaluated.
+__device__ __forceinline__ void dp_init_k1(DPState &S) {
+	S.t = 0.0;
+	S.steps = 0;
+	double h = 1.0;
+	const double atol1 = DP_ATOL1_REL * fabs(S.x[1]) + 1e-300;
+	for (int i = 0; i < 2; i++) {
+		const double scale = fabs(S.x[i]) + (i == 0 ? DP_ATOL0 : atol1) / DP_RTOL;
+		const double f = fabs(S.k1[i]);
+		if (f > 0.0) h = fmin(h, 0.01 * scale / f);
+	}
+	S.h = fmax(h, 1e-8);
+	S.hnext = 0.0f;
+}
 
 __device__ __forceinline__ void dp_init(const PhysParams &P, const RhsCtx &cx, DPState &S) {
 	rhs(P, cx, S.x, S.k1);

@@ -28,6 +28,9 @@
 PhysParams psg_phys_params(const psg_context *ctx) {
 	PhysParams P{};
 	P.ar = ctx->d_ar;
+	P.ar_ni = ctx->d_ar_ni;
+	for (int c = 0; c < 7; c++) P.ar_ni_scale[c] = ctx->ar_ni_scale[c];
+	P.ar_step = ctx->ar_step;
 	P.ar_nrows = ctx->ar_nrows;
 	P.ar_min = ctx->ar_min;
 	P.ar_step_inv = ctx->ar_step_inv;
@@ -334,6 +337,17 @@ __global__ void k_tick_long(int K, const int32_t *__restrict__ tick_act, const i
 	if (t <= K) out[t] = scan[tick_act[t]];
 }
 
+// One active particle's non-isothermal update, prepared by k_reduce<false>
+// so that the integrator reads one contiguous record instead of gathering
+// the particle's state: the inputs of the step and f(x0). 80 bytes, a
+// multiple of 16 for cp.async.
+struct __align__(16) UpdRec {
+	double time, lam0, g, heat, k0, k1;
+	float ie0, rho, yeMET, hstep;
+	uint32_t p, pad0, pad1, pad2;
+};
+static_assert(sizeof(UpdRec) == 80, "UpdRec layout");
+
 // The particle's summed deposits of the tick: isothermal, the closed-form
 // update_pars() step (loop.c:653-770); otherwise the sums for the integrator.
 template <bool ISO>
@@ -341,12 +355,33 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 		const uint32_t *__restrict__ act_ipar, int32_t *__restrict__ hits, double *__restrict__ act_g,
 		double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
-		const PhysParams &P, int64_t tick, double tick_time, uint32_t *__restrict__ status) {
+		const float *__restrict__ hstep, UpdRec *__restrict__ rec, int lo, const PhysParams &P, int64_t tick,
+		double tick_time, uint32_t *__restrict__ status) {
 	const uint32_t p = act_ipar[a];
 	hits[p] += nh;
 	if (!ISO) {
 		act_g[a] = g;
 		act_heat[a] = heat;
+		UpdRec r;
+		r.time = rn_dmul((double)(tick - lasthit[p]), tick_time);
+		r.lam0 = lambdaH[p];
+		r.g = g;
+		r.heat = heat;
+		r.ie0 = ie[p];
+		r.rho = rho[p];
+		r.yeMET = yeMET[p];
+		r.hstep = hstep[p];
+		r.p = p;
+		r.pad0 = r.pad1 = r.pad2 = 0u;
+		const double ie0 = (double)r.ie0;
+		const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, r.lam0), P.he_e));
+		const RhsCtx cx = make_rhs_ctx(P, (double)r.yeMET, g, heat, r.time, rn_dmul(P.H_PER_MASS, (double)r.rho), T);
+		const double x0[2] = {r.lam0, ie0};
+		double f0[2];
+		rhs(P, cx, x0, f0);
+		r.k0 = f0[0];
+		r.k1 = f0[1];
+		rec[a - lo] = r;    // records of one tick, from its first active particle
 		return;
 	}
 	const double time = rn_dmul((double)(tick - lasthit[p]), tick_time);
@@ -374,8 +409,8 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		const uint32_t *__restrict__ long_act, int nlong, int long_blocks,
 		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat,
 		double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit,
-		const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P, int64_t tick,
-		double tick_time, uint32_t *__restrict__ status) {
+		const float *__restrict__ rho, const float *__restrict__ yeMET, const float *__restrict__ hstep,
+		UpdRec *__restrict__ rec, PhysParams P, int64_t tick, double tick_time, uint32_t *__restrict__ status) {
 	if ((int)blockIdx.x < long_blocks) {
 		const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
 		const int lane = threadIdx.x & 31;
@@ -405,7 +440,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		}
 		if (lane == 0)
 			finish_particle<ISO>(a, sg, sh, sn, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
-					P, tick, tick_time, status);
+					hstep, rec, tick_act[t], P, tick, tick_time, status);
 		return;
 	}
 	const int a = tick_act[t] + (blockIdx.x - long_blocks) * blockDim.x + threadIdx.x;
@@ -418,8 +453,8 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		const double d = acc[k];
 		if (d >= 0.0) { g += d; if (want_heat) heat += acc_heat[k]; nh++; }
 	}
-	finish_particle<ISO>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET, P,
-			tick, tick_time, status);
+	finish_particle<ISO>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET, hstep,
+			rec, tick_act[t], P, tick, tick_time, status);
 }
 
 // update_pars() loop.c:653-770, not isothermal: every lane integrates one
@@ -431,53 +466,98 @@ struct StiffItem {
 	double t, h, x0, x1, yeMET, g, heat, time, nH, T;
 	uint32_t p;
 };
-__global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__restrict__ tick_act,
-		const uint32_t *__restrict__ act_ipar, const double *__restrict__ act_g,
-		const double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
-		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
-		float *__restrict__ hstep, PhysParams P, int64_t tick, double tick_time, unsigned *__restrict__ cursor,
-		StiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff, const uint32_t *__restrict__ alist,
-		const unsigned *__restrict__ nalist, uint32_t *__restrict__ status) {
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+			"l"(gmem_src)
+			: "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+#define UPD_WARPS 8
+// Every warp owns two buffers of 32 records in shared memory: it claims
+// chunks of 32 particles from the tick's cursor and copies their records
+// with cp.async one chunk ahead, so a lane whose particle is done takes the
+// next one from shared memory without waiting on a gather.
+__global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const int32_t *__restrict__ tick_act,
+		const UpdRec *__restrict__ rec, double *__restrict__ lambdaH, float *__restrict__ ie,
+		int64_t *__restrict__ lasthit, float *__restrict__ hstep, PhysParams P, int64_t tick,
+		unsigned *__restrict__ cursor, StiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff,
+		const uint32_t *__restrict__ alist, const unsigned *__restrict__ nalist, uint32_t *__restrict__ status) {
+	__shared__ UpdRec buf[UPD_WARPS][2][32];
 	// the tick's particles, or only those listed in alist (the surrogate's rejects)
 	const int lo = tick_act[t], hi = tick_act[t + 1];
 	const unsigned n = alist ? *nalist : (unsigned)(hi - lo);
 	const int lane = threadIdx.x & 31;
 	const unsigned lt_mask = (1u << lane) - 1u;
+	UpdRec (*B)[32] = buf[threadIdx.x >> 5];
+	auto fetch = [&](int b) -> int {
+		unsigned base = 0;
+		if (lane == 0) base = atomicAdd(cursor, 32u);
+		base = __shfl_sync(0xffffffffu, base, 0);
+		const int cnt = base >= n ? 0 : (int)min(32u, n - base);
+		if (lane < cnt) {
+			const unsigned k = base + lane;
+			const int a = alist ? (int)alist[k] : lo + (int)k;
+			const char *src = (const char *)(rec + (a - lo));
+			char *dst = (char *)&B[b][lane];
+#pragma unroll
+			for (int q = 0; q < 5; q++) cp_async16(dst + 16 * q, src + 16 * q);
+		}
+		cp_async_commit();
+		return cnt;
+	};
+	int avail[2];
+	avail[0] = fetch(0);
+	avail[1] = fetch(1);
+	cp_async_wait<1>();
+	__syncwarp();
+	int cur = 0, used = 0;
+	bool exhausted = false;
 	DPState S;
 	RhsCtx cx;
 	double atol1 = 0.0;
 	uint32_t p = 0;
-	bool have = false, drained = false;
+	bool have = false;
 	uint32_t st = 0;
 	for (;;) {
-		const unsigned need = __ballot_sync(0xffffffffu, !have);
-		if (need && !drained) {
-			unsigned base = 0;
-			if (lane == 0) base = atomicAdd(cursor, (unsigned)__popc(need));
-			base = __shfl_sync(0xffffffffu, base, 0);
-			if (base + __popc(need) >= n) drained = true;
-			if (!have) {
-				const unsigned k = base + __popc(need & lt_mask);
-				if (k < n) {
-					const int a = alist ? (int)alist[k] : lo + (int)k;
-					p = act_ipar[a];
-					const double time = rn_dmul((double)(tick - lasthit[p]), tick_time);
-					const double lam0 = lambdaH[p];
-					const double ie0 = (double)ie[p];
-					const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, lam0), P.he_e));
-					const double nH = rn_dmul(P.H_PER_MASS, (double)rho[p]);
-					cx = make_rhs_ctx(P, (double)yeMET[p], act_g[a], act_heat[a], time, nH, T);
-					S.x[0] = lam0;
-					S.x[1] = ie0;
-					atol1 = DP_ATOL1_REL * fabs(ie0) + 1e-300;
-					dp_init(P, cx, S);
-					// the particle's last step proposal is a better first
-					// step than the derivative estimate
-					const float hp = hstep[p];
-					if (hp > 0.0f) S.h = fmin(1.0, fmax((double)hp / time, 1e-8));
-					have = true;
+		unsigned need = __ballot_sync(0xffffffffu, !have);
+		while (need && !exhausted) {
+			const int left = avail[cur] - used;
+			if (left <= 0) {
+				if (avail[cur ^ 1] == 0) {
+					exhausted = true;
+					break;
 				}
+				cp_async_wait<0>();
+				__syncwarp();
+				cur ^= 1;
+				used = 0;
+				avail[cur ^ 1] = fetch(cur ^ 1);
+				continue;
 			}
+			const int rank = __popc(need & lt_mask);
+			const int take = min(__popc(need), left);
+			if (!have && rank < take) {
+				const UpdRec &r = B[cur][used + rank];
+				p = r.p;
+				const double ie0 = (double)r.ie0;
+				const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, r.lam0), P.he_e));
+				cx = make_rhs_ctx(P, (double)r.yeMET, r.g, r.heat, r.time, rn_dmul(P.H_PER_MASS, (double)r.rho), T);
+				S.x[0] = r.lam0;
+				S.x[1] = ie0;
+				S.k1[0] = r.k0;
+				S.k1[1] = r.k1;
+				atol1 = DP_ATOL1_REL * fabs(ie0) + 1e-300;
+				dp_init_k1(S);
+				// the particle's last step proposal is a better first
+				// step than the derivative estimate
+				if (r.hstep > 0.0f) S.h = fmin(1.0, fmax((double)r.hstep / r.time, 1e-8));
+				have = true;
+			}
+			used += take;
+			need = __ballot_sync(0xffffffffu, !have);
 		}
 		if (!__any_sync(0xffffffffu, have)) break;
 		if (have) {
@@ -503,6 +583,7 @@ __global__ void __launch_bounds__(256) k_update_queue(int t, const int32_t *__re
 			}
 		}
 	}
+	cp_async_wait<0>();
 	if (st) atomicOr(status, st);
 }
 
@@ -757,6 +838,11 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	uint32_t *rej = (uint32_t *)(stiff + (iso ? 0 : maxt));
 	PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * 3 * (K + 1), st));
 	if (surr) PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 8, 0, sizeof(unsigned long long), st));
+	UpdRec *urec = nullptr;
+	if (!iso) {
+		urec = (UpdRec *)psg_scratch(ctx, S_REC, sizeof(UpdRec) * maxt);
+		if (!urec) return PSG_E_NOMEM;
+	}
 	float *feat = nullptr;
 	if (ctx->log_buf && !iso) {
 		feat = (float *)psg_scratch(ctx, S_LOG, sizeof(float) * 8 * maxt);
@@ -806,11 +892,13 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 			if (iso)
 				k_reduce<true><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat,
 						long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,
-						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, tick, tick_time, ctx->d_status);
+						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, P, tick, tick_time,
+						ctx->d_status);
 			else
 				k_reduce<false><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat,
 						long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,
-						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, tick, tick_time, ctx->d_status);
+						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, P, tick, tick_time,
+						ctx->d_status);
 			PSG_CHECK_LAUNCH();
 			ctx->launches++;
 			if (!iso) {
@@ -827,10 +915,9 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 					if (rc) return rc;
 					ctx->launches++;
 				}
-				k_update_queue<<<qgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_g, act_heat, ctx->d_lambdaH,
-						ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, P, tick, tick_time,
-						cursors + t, stiff, nstiff + t, surr ? rej : nullptr, surr ? nrej + t : nullptr,
-						ctx->d_status);
+				k_update_queue<<<qgrid, 32 * UPD_WARPS, 0, st>>>((int)t, tick_act, urec, ctx->d_lambdaH, ctx->d_ie,
+						ctx->d_lasthit, ctx->d_hstep, P, tick, cursors + t, stiff, nstiff + t, surr ? rej : nullptr,
+						surr ? nrej + t : nullptr, ctx->d_status);
 				PSG_CHECK_LAUNCH();
 				k_update_stiff<<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
 						P, tick, ctx->d_status);
