@@ -412,9 +412,11 @@ class Context:
                                         lh.ctypes.data), "psg_get_state")
         return dict(lambdaH=lam, ie=ie, hits=hits, lasthit=lh)
 
-    def lambdaH(self) -> np.ndarray:
-        """x_HI of every particle (the result a tick produces)."""
-        lam = np.zeros(self.n)
+    def lambdaH(self, out: np.ndarray | None = None) -> np.ndarray:
+        """x_HI of every particle (the result a tick produces), into `out`
+        (float64[n], e.g. a view of pinned host memory) if given."""
+        lam = np.zeros(self.n) if out is None else out
+        assert lam.dtype == np.float64 and lam.shape == (self.n,) and lam.flags["C_CONTIGUOUS"]
         self._check(lib().psg_get_state(self.h, lam.ctypes.data, None, None, None), "psg_get_state")
         return lam
 

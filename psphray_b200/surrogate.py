@@ -162,13 +162,54 @@ def fit(ctx: api.Context, rows, epochs: int = 8, batch: int = 8192, lr: float = 
     return s, hist
 
 
+FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 16)     # the three tensor-core layers as padded
+
+
+def forward_bench(n: int, reps: int = 20):
+    """Times the shipped network on the tensor cores (psg_surrogate_forward)
+    over n rows of inputs drawn around the training distribution."""
+    import torch
+    s = Surrogate.load()
+    from .units import Units
+    ctx = api.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)     # events and kernels on one stream
+    ctx.set_physics(api.Physics(Units(hmf=1.0), isothermal=False))
+    s.install(ctx)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    rows = torch.zeros((n, 8), dtype=torch.float32, device="cuda")
+    rows[:, :NFEAT] = torch.from_numpy(s.x_mu).cuda() + torch.from_numpy(s.x_sd).cuda() * torch.randn(
+        (n, NFEAT), generator=g, device="cuda")
+    y = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    run = lambda: ctx._check(api.lib().psg_surrogate_forward(ctx.h, C.c_void_p(rows.data_ptr()), n,
+                                                             C.c_void_p(y.data_ptr())), "psg_surrogate_forward")
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    ms = 0.0
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run()
+        e1.record()
+        e1.synchronize()
+        ms += e0.elapsed_time(e1) / reps
+    print(json.dumps({"rows": n, "ms": ms, "rows_per_s": n / ms * 1e3,
+                      "tflops": n * FLOP_PER_ROW / ms / 1e9, "flop_per_row": FLOP_PER_ROW}))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--out", default=DEFAULT_PATH)
+    ap.add_argument("--forward-bench", type=int, default=0, help="time the shipped network on N rows and exit")
     ap.add_argument("--calls", type=int, default=4, help="batches of 8 ticks logged")
     ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--cap", type=int, default=60_000_000)
     args = ap.parse_args()
+    if args.forward_bench:
+        forward_bench(args.forward_bench)
+        return
     from . import fields
     w = fields.make_workload("lognormal128")
     phys = api.Physics(w.field.units, isothermal=False)
