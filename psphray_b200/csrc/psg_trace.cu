@@ -294,11 +294,10 @@ __global__ void k_break_ties(size_t nray, const int64_t *__restrict__ off, uint3
 }
 
 // Per-ray sort by (d, ipar), one ray per block of TPR threads holding IPT
-// hits each: a block radix sort (8 passes of 4 bits) on the float image of
-// d, which preserves the order of d >= 0; the few runs where distinct
-// doubles round to one float are then insertion-sorted on the exact (d,
-// ipar) -- the reference's d order (loop.c:783-787) with ties broken by
-// particle index. With want_kern the b column is replaced by the
+// hits each: a block radix sort (6 passes of 4 bits) on d mapped to 24 bits
+// over the ray's own range of d (a monotone map); the few runs of equal keys
+// are then insertion-sorted on the exact (d, ipar) -- the reference's d
+// order (loop.c:783-787) with ties broken by the caller's particle index. With want_kern the b column is replaced by the
 // column-density factor sph_depth(b/h)/h^2 of loop.c:429-445.
 template <int TPR, int IPT>
 __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__ list, int nlist,
@@ -312,6 +311,7 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 		typename Sort::TempStorage sort;
 		uint32_t key[NMAX];
 		uint32_t pos[NMAX];
+		double lo[TPR / 32], hi[TPR / 32];
 	};
 	extern __shared__ __align__(16) char sort_smem[];
 	Smem &sm = *reinterpret_cast<Smem *>(sort_smem);
@@ -321,14 +321,45 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 	const int n = (int)(off[r + 1] - h0);
 	const uint32_t *raw_ipar = slab_ipar + r * scap;
 	const double *raw_d = slab_d + r * scap, *raw_b = slab_b + r * scap;
+	// keys: d mapped onto 24 bits over the ray's [min, max] (monotone, so
+	// equal keys only ever hide an order the fix-up below restores)
+	double dv[IPT];
+	double dlo = 1e300, dhi = -1e300;
+#pragma unroll
+	for (int u = 0; u < IPT; u++) {
+		const int i = threadIdx.x * IPT + u;
+		dv[u] = i < n ? raw_d[i] : 0.0;
+		if (i < n) {
+			dlo = fmin(dlo, dv[u]);
+			dhi = fmax(dhi, dv[u]);
+		}
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		dlo = fmin(dlo, __shfl_xor_sync(0xffffffffu, dlo, o));
+		dhi = fmax(dhi, __shfl_xor_sync(0xffffffffu, dhi, o));
+	}
+	if ((threadIdx.x & 31) == 0) {
+		sm.lo[threadIdx.x >> 5] = dlo;
+		sm.hi[threadIdx.x >> 5] = dhi;
+	}
+	__syncthreads();
+#pragma unroll
+	for (int w = 0; w < TPR / 32; w++) {
+		dlo = fmin(dlo, sm.lo[w]);
+		dhi = fmax(dhi, sm.hi[w]);
+	}
+	const double scale = dhi > dlo ? 16777215.0 / (dhi - dlo) : 0.0;
 	uint32_t k[IPT], v[IPT];
 #pragma unroll
 	for (int u = 0; u < IPT; u++) {
 		const int i = threadIdx.x * IPT + u;
-		k[u] = i < n ? __float_as_uint((float)raw_d[i]) : 0xFFFFFFFFu;
+		// padding takes the largest key; the sort is stable and padding
+		// follows every real item, so it stays behind them
+		k[u] = i < n ? (uint32_t)((dv[u] - dlo) * scale) : 16777215u;
 		v[u] = (uint32_t)i;
 	}
-	Sort(sm.sort).Sort(k, v, 0, 32);
+	Sort(sm.sort).Sort(k, v, 0, 24);
 	__syncthreads();
 #pragma unroll
 	for (int u = 0; u < IPT; u++) {
@@ -376,7 +407,8 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 
 template <int TPR, int IPT>
 size_t sort_smem_bytes() {
-	return sizeof(typename cub::BlockRadixSort<uint32_t, TPR, IPT, uint32_t, 4>::TempStorage) + 8 * TPR * IPT + 64;
+	return sizeof(typename cub::BlockRadixSort<uint32_t, TPR, IPT, uint32_t, 4>::TempStorage) + 8 * TPR * IPT +
+			16 * (TPR / 32) + 128;
 }
 
 // Size classes of the ray sort: class c holds rays with at most
