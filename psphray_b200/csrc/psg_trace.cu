@@ -136,14 +136,14 @@ __global__ void __launch_bounds__(32 * TR_WARPS) k_trace_stack(const psg_ray *__
 	extern __shared__ int tr_smem[];
 	const int lane = threadIdx.x & 31;
 	const int wib = threadIdx.x >> 5;
-	int *stack = tr_smem + wib * (TR_STACK + 32 * ppc);
-	int *list = stack + TR_STACK;
+	int *stack = tr_smem + wib * (TR_STACK + 32 * ppc + 32);
+	int *list = stack + TR_STACK;      // candidates waiting for a full round of 32
 	const size_t r = (size_t)blockIdx.x * TR_WARPS + wib;
 	if (r >= nray) return;
 	const RayGeom g = load_ray(rays, r);
 	const unsigned lt_mask = (1u << lane) - 1u;
 	uint32_t nh = 0;
-	int sp = 0;
+	int sp = 0, nbuf = 0;
 	bool overflow = false;
 	{
 		const float4 lo = __ldg(&wlo[0]), hi = __ldg(&whi[0]);
@@ -197,13 +197,24 @@ __global__ void __launch_bounds__(32 * TR_WARPS) k_trace_stack(const psg_ray *__
 		}
 		const int total = __shfl_sync(0xffffffffu, cs, 31);
 		if (cnt) {
-			const int ps = __float_as_int(hi.w), base = cs - cnt;
+			const int ps = __float_as_int(hi.w), base = nbuf + cs - cnt;
 			for (int q = 0; q < cnt; q++) list[base + q] = ps + q;
 		}
+		nbuf += total;
 		__syncwarp();
-		test_candidates(g, list, total, lpsml, lidx, r, scap, slab_ipar, slab_d, slab_b, nh, lane, lt_mask);
-		__syncwarp();
+		// line tests only in full rounds of 32; the rest waits in the list
+		if (nbuf >= 32) {
+			const int full = nbuf & ~31, rem = nbuf - full;
+			test_candidates(g, list, full, lpsml, lidx, r, scap, slab_ipar, slab_d, slab_b, nh, lane, lt_mask);
+			__syncwarp();
+			const int keep = lane < rem ? list[full + lane] : 0;
+			__syncwarp();
+			if (lane < rem) list[lane] = keep;
+			nbuf = rem;
+			__syncwarp();
+		}
 	}
+	if (nbuf) test_candidates(g, list, nbuf, lpsml, lidx, r, scap, slab_ipar, slab_d, slab_b, nh, lane, lt_mask);
 	if (lane == 0) {
 		count[r] = nh;
 		if (overflow) atomicOr(status, PSG_ST_STACK);
@@ -445,7 +456,7 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	int32_t *off32 = (int32_t *)(offmem + sizeof(int64_t) * (nray + 1));
 	unsigned long long *d_max = ctx->d_counters + 4;
 	const int ppc = ctx->ppc;
-	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ppc) * TR_WARPS;
+	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ppc + 32) * TR_WARPS;
 	if (smem > 48 * 1024)
 		PSG_CUDA(cudaFuncSetAttribute(k_trace_stack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 	// one traversal into per-ray slabs; if a ray outgrew its slab, grow and rerun
