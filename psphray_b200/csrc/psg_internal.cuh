@@ -102,7 +102,7 @@ struct psg_context {
 
 	uint32_t *d_status = nullptr;
 	unsigned long long *d_counters = nullptr;   // 16 device counters: 1 capped deposits, 2 lost photons,
-	                                            // 4-7 trace/sort, 8 surrogate accepts
+	                                            // 4-7 trace/sort, 8 surrogate accepts, 9 trace ray cursor
 
 	// scratch, grown on demand
 	psg_buf scratch[S_NSLOTS];

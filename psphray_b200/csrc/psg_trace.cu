@@ -132,14 +132,21 @@ __global__ void __launch_bounds__(32 * TR_WARPS) k_trace_stack(const psg_ray *__
 		const float4 *__restrict__ wlo, const float4 *__restrict__ whi,
 		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx, int ppc,
 		uint32_t *__restrict__ count, size_t scap, uint32_t *__restrict__ slab_ipar,
-		double *__restrict__ slab_d, double *__restrict__ slab_b, uint32_t *__restrict__ status) {
+		double *__restrict__ slab_d, double *__restrict__ slab_b, unsigned long long *__restrict__ next_ray,
+		uint32_t *__restrict__ status) {
 	extern __shared__ int tr_smem[];
 	const int lane = threadIdx.x & 31;
 	const int wib = threadIdx.x >> 5;
 	int *stack = tr_smem + wib * (TR_STACK + 32 * ppc + 32);
 	int *list = stack + TR_STACK;      // candidates waiting for a full round of 32
-	const size_t r = (size_t)blockIdx.x * TR_WARPS + wib;
-	if (r >= nray) return;
+	// persistent warps: each takes the next ray from a shared counter, so a
+	// block never idles behind its longest ray
+	for (;;) {
+	unsigned long long rr = 0;
+	if (lane == 0) rr = atomicAdd(next_ray, 1ull);
+	rr = __shfl_sync(0xffffffffu, rr, 0);
+	if (rr >= nray) break;
+	const size_t r = (size_t)rr;
 	const RayGeom g = load_ray(rays, r);
 	const unsigned lt_mask = (1u << lane) - 1u;
 	uint32_t nh = 0;
@@ -218,6 +225,8 @@ __global__ void __launch_bounds__(32 * TR_WARPS) k_trace_stack(const psg_ray *__
 	if (lane == 0) {
 		count[r] = nh;
 		if (overflow) atomicOr(status, PSG_ST_STACK);
+	}
+	__syncwarp();
 	}
 }
 
@@ -455,6 +464,9 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	int64_t *off64 = (int64_t *)offmem;
 	int32_t *off32 = (int32_t *)(offmem + sizeof(int64_t) * (nray + 1));
 	unsigned long long *d_max = ctx->d_counters + 4;
+	unsigned long long *next_ray = ctx->d_counters + 9;
+	int sms = 148;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
 	const int ppc = ctx->ppc;
 	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ppc + 32) * TR_WARPS;
 	if (smem > 48 * 1024)
@@ -472,9 +484,13 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 		PSG_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st));
 		psg_mark_begin(ctx, PSG_K_TRACE_FILL);
 		if (nray) {
-			k_trace_stack<<<blocks(nray, TR_WARPS), 32 * TR_WARPS, smem, st>>>(d_rays, nray, ctx->d_wide_lo,
+			PSG_CUDA(cudaMemsetAsync(next_ray, 0, sizeof(unsigned long long), st));
+			int per_sm = 1;
+			PSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_stack, 32 * TR_WARPS, smem));
+			const unsigned tgrid = (unsigned)std::min<size_t>(blocks(nray, TR_WARPS), (size_t)std::max(per_sm, 1) * sms);
+			k_trace_stack<<<tgrid, 32 * TR_WARPS, smem, st>>>(d_rays, nray, ctx->d_wide_lo,
 					ctx->d_wide_hi, ctx->d_leaf_psml, ctx->d_leaf_idx, ppc, count, scap, slab_ipar,
-					slab_f64, slab_f64 + slots, ctx->d_status);
+					slab_f64, slab_f64 + slots, next_ray, ctx->d_status);
 			ctx->launches++;
 		}
 		PSG_CHECK_LAUNCH();
