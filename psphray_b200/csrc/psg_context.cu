@@ -55,7 +55,7 @@ extern "C" int psg_create(psg_context **out, int device) {
 			cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
 			cudaMalloc(&ctx->d_status, sizeof(uint32_t)) != cudaSuccess ||
 			cudaMemset(ctx->d_status, 0, sizeof(uint32_t)) != cudaSuccess ||
-			cudaMalloc(&ctx->d_counters, 16 * sizeof(unsigned long long)) != cudaSuccess) {
+			cudaMalloc(&ctx->d_counters, 32 * sizeof(unsigned long long)) != cudaSuccess) {
 		cudaGetLastError();
 		delete ctx;
 		return PSG_E_CUDA;

@@ -101,8 +101,9 @@ struct psg_context {
 	unsigned long long *log_count = nullptr;
 
 	uint32_t *d_status = nullptr;
-	unsigned long long *d_counters = nullptr;   // 16 device counters: 1 capped deposits, 2 lost photons,
-	                                            // 4-7 trace/sort, 8 surrogate accepts, 9 trace ray cursor
+	unsigned long long *d_counters = nullptr;   // 32 device counters: 1 capped deposits, 2 lost photons,
+	                                            // 4 longest hit list, 8 surrogate accepts, 9 trace ray
+	                                            // cursor, 16-23 sort size classes
 
 	// scratch, grown on demand
 	psg_buf scratch[S_NSLOTS];

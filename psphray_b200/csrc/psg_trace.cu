@@ -433,7 +433,10 @@ size_t sort_smem_bytes() {
 
 // Size classes of the ray sort: class c holds rays with at most
 // kSortClassMax[c] hits (and more than the previous class's bound).
-__constant__ int kSortBounds[4] = {64, 512, 2048, PSG_SORT_MAX};   // 32x2, 128x4, 256x8, 512x16
+// size classes of the per-ray sort (threads x items per thread):
+// 32x2, 32x4, 64x4, 128x4, 128x8, 256x8, 256x16, 512x16
+#define SORT_NCLS 8
+__constant__ int kSortBounds[SORT_NCLS] = {64, 128, 256, 512, 1024, 2048, 4096, PSG_SORT_MAX};
 
 __global__ void k_sort_classify(size_t nray, const int64_t *__restrict__ off, uint32_t *__restrict__ lists,
 		size_t stride, unsigned long long *__restrict__ nclass) {
@@ -442,7 +445,7 @@ __global__ void k_sort_classify(size_t nray, const int64_t *__restrict__ off, ui
 	const int64_t n = off[r + 1] - off[r];
 	if (n == 0) return;
 	int c = 0;
-	while (c < 3 && n > kSortBounds[c]) c++;
+	while (c < SORT_NCLS - 1 && n > kSortBounds[c]) c++;
 	const unsigned long long k = atomicAdd(&nclass[c], 1ull);
 	lists[c * stride + k] = (uint32_t)r;
 }
@@ -537,34 +540,38 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	if (nhit) {
 		psg_mark_begin(ctx, PSG_K_SORT);
 		if (maxcount <= PSG_SORT_MAX) {
-			uint32_t *lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * 4 * (nray + 1));
+			uint32_t *lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * SORT_NCLS * (nray + 1));
 			if (!lists) return PSG_E_NOMEM;
-			unsigned long long *d_ncls = ctx->d_counters + 4;
-			PSG_CUDA(cudaMemsetAsync(d_ncls, 0, 4 * sizeof(unsigned long long), st));
+			unsigned long long *d_ncls = ctx->d_counters + 16;
+			PSG_CUDA(cudaMemsetAsync(d_ncls, 0, SORT_NCLS * sizeof(unsigned long long), st));
 			k_sort_classify<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, lists, nray + 1, d_ncls);
 			PSG_CHECK_LAUNCH();
-			unsigned long long ncls[4];
+			unsigned long long ncls[SORT_NCLS];
 			PSG_CUDA(cudaMemcpyAsync(ncls, d_ncls, sizeof(ncls), cudaMemcpyDeviceToHost, st));
 			PSG_CUDA(cudaStreamSynchronize(st));
 			const PhysParams PP = psg_phys_params(ctx);
 			const size_t stride = nray + 1;
-			auto launch_block = [&](auto kern, int tpr, size_t smem, const uint32_t *lst, unsigned long long nl) -> int {
+			auto launch_block = [&](auto kern, int tpr, size_t smem, int c) -> int {
+				const unsigned long long nl = ncls[c];
 				if (!nl) return PSG_OK;
 				if (smem > 48 * 1024)
 					PSG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-				kern<<<(unsigned)nl, tpr, smem, st>>>(lst, (int)nl, off64, scap, slab_ipar, slab_d, slab_b, hit_ipar,
-						hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order);
+				kern<<<(unsigned)nl, tpr, smem, st>>>(lists + c * stride, (int)nl, off64, scap, slab_ipar, slab_d,
+						slab_b, hit_ipar, hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order);
 				PSG_CHECK_LAUNCH();
+				ctx->launches++;
 				return PSG_OK;
 			};
-			int rcs = launch_block(k_sort_block<32, 2>, 32, sort_smem_bytes<32, 2>(), lists, ncls[0]);
-			if (!rcs) rcs = launch_block(k_sort_block<128, 4>, 128, sort_smem_bytes<128, 4>(), lists + stride, ncls[1]);
-			if (!rcs) rcs = launch_block(k_sort_block<256, 8>, 256, sort_smem_bytes<256, 8>(), lists + 2 * stride,
-					ncls[2]);
-			if (!rcs) rcs = launch_block(k_sort_block<512, 16>, 512, sort_smem_bytes<512, 16>(), lists + 3 * stride,
-					ncls[3]);
+			int rcs = launch_block(k_sort_block<32, 2>, 32, sort_smem_bytes<32, 2>(), 0);
+			if (!rcs) rcs = launch_block(k_sort_block<32, 4>, 32, sort_smem_bytes<32, 4>(), 1);
+			if (!rcs) rcs = launch_block(k_sort_block<64, 4>, 64, sort_smem_bytes<64, 4>(), 2);
+			if (!rcs) rcs = launch_block(k_sort_block<128, 4>, 128, sort_smem_bytes<128, 4>(), 3);
+			if (!rcs) rcs = launch_block(k_sort_block<128, 8>, 128, sort_smem_bytes<128, 8>(), 4);
+			if (!rcs) rcs = launch_block(k_sort_block<256, 8>, 256, sort_smem_bytes<256, 8>(), 5);
+			if (!rcs) rcs = launch_block(k_sort_block<256, 16>, 256, sort_smem_bytes<256, 16>(), 6);
+			if (!rcs) rcs = launch_block(k_sort_block<512, 16>, 512, sort_smem_bytes<512, 16>(), 7);
 			if (rcs) return rcs;
-			ctx->launches += 1 + (ncls[0] > 0) + (ncls[1] > 0) + (ncls[2] > 0) + (ncls[3] > 0);
+			ctx->launches++;
 		} else {
 			// a ray longer than the shared-memory sort takes: library segmented sort
 			uint32_t *raw_ipar = (uint32_t *)psg_scratch(ctx, S_RAW_IPAR, sizeof(uint32_t) * hb);
