@@ -135,16 +135,21 @@ struct DepShared {
 	int first;
 };
 
+// The threads of one ray: a warp, a 128-thread quarter of a block (named
+// barrier `bar`, 1..4) or the whole block (bar 0).
 template <int NT>
-__device__ __forceinline__ void group_sync() {
-	if (NT == 32) __syncwarp(); else __syncthreads();
+__device__ __forceinline__ void group_sync(int bar) {
+	if (NT == 32) __syncwarp();
+	else if (bar == 0) __syncthreads();
+	else asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(NT) : "memory");
 }
 
 template <int NT>
 __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern, const uint32_t *__restrict__ slot,
 		const double *__restrict__ lambdaH, const float *__restrict__ mass, const PhysParams &P, int want_heat,
-		double *__restrict__ acc, double *__restrict__ acc_heat, DepShared &sh, unsigned &nsat, double &lost) {
+		double *__restrict__ acc, double *__restrict__ acc_heat, DepShared &sh, unsigned &nsat, double &lost,
+		int bar) {
 	const int lane = t & 31, wid = t >> 5;
 	constexpr int NW = NT / 32;
 	const double Nph = ray.Nph;
@@ -205,7 +210,7 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 			} else {
 				if (lane == 31) sh.wsum[wid] = wi;
 				if (t == 0) sh.first = NT;
-				group_sync<NT>();
+				group_sync<NT>(bar);
 				total = 0.0;
 #pragma unroll
 				for (int k = 0; k < NW; k++) {
@@ -230,13 +235,13 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 				f = ev ? __ffs(ev) - 1 : NT;
 			} else {
 				if (capped || cut) atomicMin(&sh.first, t);
-				group_sync<NT>();
+				group_sync<NT>(bar);
 				f = sh.first;
 			}
 			if (part && t < f) delta = rn_dmul(absorb, NH_inv);
 			if (f == NT) {
 				TM = TM * exp(-total);
-				group_sync<NT>();       // shared words are rewritten by the next step
+				group_sync<NT>(bar);       // shared words are rewritten by the next step
 				break;
 			}
 			double TMnew = 0.0;
@@ -253,12 +258,12 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 			if (NW == 1) {
 				TM = __shfl_sync(0xffffffffu, TMnew, f);
 			} else {
-				group_sync<NT>();
+				group_sync<NT>(bar);
 				TM = sh.tm;
 			}
 			if (below_cutoff(TM, Nph)) done = true;
 			start = f + 1;
-			group_sync<NT>();
+			group_sync<NT>(bar);
 		}
 		if (valid) {
 			acc[slot_c] = delta;
@@ -268,33 +273,46 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 	if (t == 0 && !skip_ray) lost += TM;
 }
 
-// Blocks [0, nlong) take one long ray each with all DEP_THREADS threads; the
+// Blocks [0, nlong) take one long ray each with all DEP_THREADS threads;
+// the next nmid_blocks take four middle rays each, 128 threads per ray; the
 // remaining blocks take DEP_THREADS/32 short rays, one per warp.
 #define DEP_THREADS 512
-#define DEP_LONG 96
+#define DEP_LONG 96       // more hits than this: a group of threads, else a warp
+#define DEP_MID 384       // more hits than this: the whole block, else a 128-thread quarter
 
 __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__restrict__ rays,
-		const uint32_t *__restrict__ long_rays, int nlong, const uint32_t *__restrict__ short_rays, int nshort,
+		const uint32_t *__restrict__ long_rays, int nlong, const uint32_t *__restrict__ mid_rays, int nmid,
+		const uint32_t *__restrict__ short_rays, int nshort,
 		const int64_t *__restrict__ off, const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
 		const uint32_t *__restrict__ slot, const double *__restrict__ lambdaH, const float *__restrict__ mass,
 		PhysParams P, int want_heat, double *__restrict__ acc, double *__restrict__ acc_heat,
 		unsigned long long *__restrict__ n_sat, double *__restrict__ lost) {
 	__shared__ DepShared sh_block;
+	__shared__ DepShared sh_quarter[4];
 	__shared__ DepShared sh_warp[DEP_THREADS / 32];
 	const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 	unsigned nsat = 0;
 	double tm_lost = 0.0;
+	const int nmid_blocks = (nmid + 3) / 4;
 	if ((int)blockIdx.x < nlong) {
 		const uint32_t r = long_rays[blockIdx.x];
 		deposit_ray<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P, want_heat,
-				acc, acc_heat, sh_block, nsat, tm_lost);
+				acc, acc_heat, sh_block, nsat, tm_lost, 0);
+	} else if ((int)blockIdx.x < nlong + nmid_blocks) {
+		const int q = tid >> 7;
+		const int m = ((int)blockIdx.x - nlong) * 4 + q;
+		if (m < nmid) {
+			const uint32_t r = mid_rays[m];
+			deposit_ray<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
+					want_heat, acc, acc_heat, sh_quarter[q], nsat, tm_lost, 1 + q);
+		}
 	} else {
-		const int w = ((int)blockIdx.x - nlong) * (DEP_THREADS / 32) + wid;
+		const int w = ((int)blockIdx.x - nlong - nmid_blocks) * (DEP_THREADS / 32) + wid;
 		if (w < nshort) {
 			const uint32_t r = short_rays[w];
 			if (off[r + 1] > off[r])
 				deposit_ray<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P, want_heat,
-						acc, acc_heat, sh_warp[wid], nsat, tm_lost);
+						acc, acc_heat, sh_warp[wid], nsat, tm_lost, 0);
 		}
 	}
 	for (int o = 16; o > 0; o >>= 1) nsat += __shfl_down_sync(0xffffffffu, nsat, o);
@@ -302,19 +320,25 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 	if (lane == 0 && tm_lost != 0.0) atomicAdd(lost, tm_lost);
 }
 
-// Rays of the batch split into long and short lists (ray order kept).
-__global__ void k_ray_class(size_t nray, const int64_t *__restrict__ off, int32_t *__restrict__ is_long) {
+// Rays of the batch split into long, middle and short lists (ray order
+// kept): cls = 1 for long, 1 << 32 for middle, so one scan counts both.
+__global__ void k_ray_class(size_t nray, const int64_t *__restrict__ off, unsigned long long *__restrict__ cls) {
 	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (r >= nray) return;
-	is_long[r] = (off[r + 1] - off[r]) > DEP_LONG ? 1 : 0;
+	const int64_t n = off[r + 1] - off[r];
+	cls[r] = n > DEP_MID ? 1ull : (n > DEP_LONG ? (1ull << 32) : 0ull);
 }
 
-__global__ void k_ray_lists(size_t nray, const int32_t *__restrict__ is_long, const int32_t *__restrict__ scan,
-		uint32_t *__restrict__ long_rays, uint32_t *__restrict__ short_rays) {
+__global__ void k_ray_lists(size_t nray, const unsigned long long *__restrict__ cls,
+		const unsigned long long *__restrict__ scan, uint32_t *__restrict__ long_rays,
+		uint32_t *__restrict__ mid_rays, uint32_t *__restrict__ short_rays) {
 	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (r >= nray) return;
-	if (is_long[r]) long_rays[scan[r]] = (uint32_t)r;
-	else short_rays[r - scan[r]] = (uint32_t)r;
+	const unsigned long long sc = scan[r];
+	const uint32_t nl = (uint32_t)sc, nm = (uint32_t)(sc >> 32);
+	if (cls[r] == 1ull) long_rays[nl] = (uint32_t)r;
+	else if (cls[r]) mid_rays[nm] = (uint32_t)r;
+	else short_rays[r - nl - nm] = (uint32_t)r;
 }
 
 // Active particles of the batch whose deposit segment is longer than a warp
@@ -793,27 +817,29 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	// the tick loop
 	std::vector<int32_t> h_tick_act(K + 1);
 	PSG_CUDA(cudaMemcpyAsync(h_tick_act.data(), tick_act, sizeof(int32_t) * (K + 1), cudaMemcpyDeviceToHost, st));
-	// long / short ray lists of the batch (ray order, so each tick's rays are a run)
-	int32_t *is_long = (int32_t *)psg_scratch(ctx, S_COUNT, sizeof(int32_t) * 2 * (nray + 1));
+	// long / middle / short ray lists of the batch (ray order, so each tick's
+	// rays are a run)
+	unsigned long long *cls = (unsigned long long *)psg_scratch(ctx, S_COUNT, sizeof(unsigned long long) * 2 * (nray + 1));
 	uint32_t *ray_lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * (nray + 1));
-	if (!is_long || !ray_lists) return PSG_E_NOMEM;
-	int32_t *long_scan = is_long + (nray + 1);
-	k_ray_class<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, is_long);
+	if (!cls || !ray_lists) return PSG_E_NOMEM;
+	unsigned long long *cls_scan = cls + (nray + 1);
+	k_ray_class<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, cls);
 	PSG_CHECK_LAUNCH();
 	{
 		size_t tmp = 0;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, is_long, long_scan, (int)nray, st));
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cls, cls_scan, (int)nray, st));
 		void *dt = psg_scratch(ctx, S_CUB, tmp);
 		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, is_long, long_scan, (int)nray, st));
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, cls, cls_scan, (int)nray, st));
 	}
-	std::vector<int32_t> h_scan(nray), h_last(1);
-	PSG_CUDA(cudaMemcpyAsync(h_scan.data(), long_scan, sizeof(int32_t) * nray, cudaMemcpyDeviceToHost, st));
-	PSG_CUDA(cudaMemcpyAsync(h_last.data(), is_long + nray - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+	std::vector<unsigned long long> h_scan(nray), h_last(1);
+	PSG_CUDA(cudaMemcpyAsync(h_scan.data(), cls_scan, sizeof(unsigned long long) * nray, cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaMemcpyAsync(h_last.data(), cls + nray - 1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
 	PSG_CUDA(cudaStreamSynchronize(st));
-	const int nlong_all = h_scan[nray - 1] + h_last[0];
-	uint32_t *long_rays = ray_lists, *short_rays = ray_lists + nlong_all;
-	k_ray_lists<<<blocks(nray, 256), 256, 0, st>>>(nray, is_long, long_scan, long_rays, short_rays);
+	const unsigned long long tot = h_scan[nray - 1] + h_last[0];
+	const int nlong_all = (int)(uint32_t)tot, nmid_all = (int)(uint32_t)(tot >> 32);
+	uint32_t *long_rays = ray_lists, *mid_rays = ray_lists + nlong_all, *short_rays = mid_rays + nmid_all;
+	k_ray_lists<<<blocks(nray, 256), 256, 0, st>>>(nray, cls, cls_scan, long_rays, mid_rays, short_rays);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 2;
 	// per-particle sums, the long-segment lists and (not isothermal) the
@@ -870,16 +896,17 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	PSG_CUDA(cudaMemcpyAsync(h_tick_long.data(), tick_long, sizeof(int32_t) * (K + 1), cudaMemcpyDeviceToHost, st));
 	PSG_CUDA(cudaStreamSynchronize(st));
 	for (size_t t = 0; t < K; t++) {
-		const int l0 = h_scan[t * R];
-		const int l1 = (t + 1 < K) ? h_scan[(t + 1) * R] : nlong_all;
-		const int nlong = l1 - l0;
-		const int s0 = (int)(t * R) - l0;
-		const int nshort = (int)R - nlong;
-		const unsigned grid = (unsigned)(nlong + (nshort + DEP_THREADS / 32 - 1) / (DEP_THREADS / 32));
+		const unsigned long long c0 = h_scan[t * R], c1 = (t + 1 < K) ? h_scan[(t + 1) * R] : tot;
+		const int l0 = (int)(uint32_t)c0, m0 = (int)(uint32_t)(c0 >> 32);
+		const int nlong = (int)(uint32_t)c1 - l0, nmid = (int)(uint32_t)(c1 >> 32) - m0;
+		const int s0 = (int)(t * R) - l0 - m0;
+		const int nshort = (int)R - nlong - nmid;
+		const unsigned grid = (unsigned)(nlong + (nmid + 3) / 4 + (nshort + DEP_THREADS / 32 - 1) / (DEP_THREADS / 32));
 		psg_mark_begin(ctx, PSG_K_DEPOSIT);
 		if (grid)
-			k_deposit<<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, short_rays + s0, nshort, off64,
-					hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P, want_heat, acc, acc_heat, d_nsat, d_lost);
+			k_deposit<<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0, nmid,
+					short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+					want_heat, acc, acc_heat, d_nsat, d_lost);
 		PSG_CHECK_LAUNCH();
 		psg_mark_end(ctx);
 		const int nact_t = h_tick_act[t + 1] - h_tick_act[t];
