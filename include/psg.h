@@ -273,6 +273,36 @@ int psg_step_evolve(psg_context *ctx, psg_step *steps, size_t n);
 #define PSG_NOALLOC_MAX_STEPS 16384
 int psg_step_evolve_noalloc(psg_context *ctx, psg_step *steps, size_t n);
 
+/* ---- snapshots: psystem_write_output() psystem.c:598-690 ------------------ */
+/* One psphray-format file (reader-psphray.inc): gas (type 0) and sources
+ * (type 5). Array pointers may be NULL: written as zeros, skipped on read. */
+typedef struct {
+	size_t ngas, nsrc;
+	double time;                /* scale factor 1/(1+z) of the output */
+	double redshift, boxsize, OmegaM, OmegaL, OmegaB, h;
+	float *pos;                 /* [ngas][3] */
+	int64_t *id;
+	float *mass, *ie, *rho, *ye, *xHI, *sml, *xHeI, *xHeII, *gammaHI;
+	int64_t *lasthit;
+	int32_t *hits;
+	float *src_pos;             /* [nsrc][3] */
+	double *ngammas;            /* [nsrc] photons per unit time */
+} psg_snapshot;
+int psg_snapshot_write(const char *filename, const psg_snapshot *s);
+/* counts and constants of a file into s (arrays untouched) */
+int psg_snapshot_read_header(const char *filename, psg_snapshot *s);
+/* the arrays of a file into the non-NULL pointers of s (s->ngas, s->nsrc
+ * must match the file's) */
+int psg_snapshot_read(const char *filename, psg_snapshot *s);
+/* psystem_write_output(): the particle state on the device, in the caller's
+ * order, written with meta's constants, ids and sources (meta->ngas must be
+ * the particle count; NULL ids write 0..n-1). xHI = lambdaH, ye = x_HII plus
+ * the frozen helium electrons (psys_ye() psystem.h:177), xHeI = xHeII = 0
+ * and gammaHI = 0 (hydrogen only, on the spot). */
+int psg_write_output(psg_context *ctx, const char *filename, const psg_snapshot *meta);
+/* Per-particle deposit counters (psys.hits), caller order; for a resumed run. */
+int psg_set_hits(psg_context *ctx, const int32_t *hits);
+
 /* ---- chemistry surrogate: the network and its training ------------------- */
 /* No counterpart in the reference (it integrates every particle with LSODA):
  * a 6 -> 64 -> 64 -> 2 perceptron with SiLU activations learns the

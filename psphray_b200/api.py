@@ -93,6 +93,61 @@ class CSource(C.Structure):
                 ("lastemit", C.c_int64)]
 
 
+class CSnapshot(C.Structure):
+    _fields_ = [("ngas", C.c_size_t), ("nsrc", C.c_size_t)] + [
+        (n, C.c_double) for n in ("time", "redshift", "boxsize", "OmegaM", "OmegaL", "OmegaB", "h")] + [
+        (n, C.c_void_p) for n in ("pos", "id", "mass", "ie", "rho", "ye", "xHI", "sml", "xHeI", "xHeII",
+                                  "gammaHI", "lasthit", "hits", "src_pos", "ngammas")]
+
+
+SNAP_ARRAYS = {"pos": (np.float32, 3), "id": (np.int64, 1), "mass": (np.float32, 1), "ie": (np.float32, 1),
+               "rho": (np.float32, 1), "ye": (np.float32, 1), "xHI": (np.float32, 1), "sml": (np.float32, 1),
+               "xHeI": (np.float32, 1), "xHeII": (np.float32, 1), "gammaHI": (np.float32, 1),
+               "lasthit": (np.int64, 1), "hits": (np.int32, 1)}
+SNAP_CONSTS = ("time", "redshift", "boxsize", "OmegaM", "OmegaL", "OmegaB", "h")
+
+
+def write_snapshot(path: str, ngas: int, arrays: dict, src_pos=None, ngammas=None, **consts):
+    """psphray-format file from host arrays (missing ones written as zeros)."""
+    s = CSnapshot(ngas=ngas, nsrc=0 if src_pos is None else len(src_pos))
+    for k in SNAP_CONSTS:
+        setattr(s, k, float(consts.get(k, 0.0)))
+    keep = []
+    for k, (dt, _) in SNAP_ARRAYS.items():
+        if arrays.get(k) is not None:
+            a = np.ascontiguousarray(arrays[k], dt)
+            keep.append(a)
+            setattr(s, k, a.ctypes.data)
+    if src_pos is not None:
+        sp = np.ascontiguousarray(src_pos, np.float32); ng = np.ascontiguousarray(ngammas, np.float64)
+        keep += [sp, ng]
+        s.src_pos, s.ngammas = sp.ctypes.data, ng.ctypes.data
+    rc = lib().psg_snapshot_write(path.encode(), C.byref(s))
+    if rc != PSG_OK:
+        raise PsgError(rc, f"psg_snapshot_write({path})")
+
+
+def read_snapshot(path: str) -> dict:
+    """Every block of a psphray-format file: arrays and constants."""
+    s = CSnapshot()
+    rc = lib().psg_snapshot_read_header(path.encode(), C.byref(s))
+    if rc != PSG_OK:
+        raise PsgError(rc, f"psg_snapshot_read_header({path})")
+    out = {k: getattr(s, k) for k in SNAP_CONSTS}
+    out["ngas"], out["nsrc"] = s.ngas, s.nsrc
+    for k, (dt, w) in SNAP_ARRAYS.items():
+        a = np.zeros((s.ngas, w) if w > 1 else s.ngas, dt)
+        out[k] = a
+        setattr(s, k, a.ctypes.data)
+    out["src_pos"] = np.zeros((s.nsrc, 3), np.float32)
+    out["ngammas"] = np.zeros(s.nsrc, np.float64)
+    s.src_pos, s.ngammas = out["src_pos"].ctypes.data, out["ngammas"].ctypes.data
+    rc = lib().psg_snapshot_read(path.encode(), C.byref(s))
+    if rc != PSG_OK:
+        raise PsgError(rc, f"psg_snapshot_read({path})")
+    return out
+
+
 class CSpectrum(C.Structure):
     _fields_ = [("eng", C.c_void_p), ("weight", C.c_void_p), ("n", C.c_int)]
 
@@ -168,6 +223,11 @@ def lib() -> C.CDLL:
         "psg_set_update_log": ([vp, vp, sz, vp], C.c_int),
         "psg_set_surrogate": ([vp, vp, vp, vp, vp, vp, C.c_float], C.c_int),
         "psg_surrogate_forward": ([vp, vp, sz, vp], C.c_int),
+        "psg_snapshot_write": ([C.c_char_p, C.POINTER(CSnapshot)], C.c_int),
+        "psg_snapshot_read_header": ([C.c_char_p, C.POINTER(CSnapshot)], C.c_int),
+        "psg_snapshot_read": ([C.c_char_p, C.POINTER(CSnapshot)], C.c_int),
+        "psg_write_output": ([vp, C.c_char_p, C.POINTER(CSnapshot)], C.c_int),
+        "psg_set_hits": ([vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -425,6 +485,23 @@ class Context:
                 None if ie is None else np.ascontiguousarray(ie, np.float32),
                 None if lasthit is None else np.ascontiguousarray(lasthit, np.int64)]
         self._check(lib().psg_set_state(self.h, *[_ptr(a) for a in keep]), "psg_set_state")
+
+    def write_output(self, path: str, ids=None, src_pos=None, ngammas=None, **consts):
+        """psystem_write_output(): the device state as a psphray-format file."""
+        s = CSnapshot(ngas=self.n, nsrc=0 if src_pos is None else len(src_pos))
+        for k in SNAP_CONSTS:
+            setattr(s, k, float(consts.get(k, 0.0)))
+        keep = []
+        if ids is not None:
+            keep.append(np.ascontiguousarray(ids, np.int64)); s.id = keep[-1].ctypes.data
+        if src_pos is not None:
+            keep += [np.ascontiguousarray(src_pos, np.float32), np.ascontiguousarray(ngammas, np.float64)]
+            s.src_pos, s.ngammas = keep[-2].ctypes.data, keep[-1].ctypes.data
+        self._check(lib().psg_write_output(self.h, path.encode(), C.byref(s)), "psg_write_output")
+
+    def set_hits(self, hits):
+        h = np.ascontiguousarray(hits, np.int32)
+        self._check(lib().psg_set_hits(self.h, h.ctypes.data), "psg_set_hits")
 
     def step_evolve(self, steps: np.ndarray) -> np.ndarray:
         steps = np.ascontiguousarray(steps, STEP_DTYPE)

@@ -21,7 +21,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpsg.so")
 
 CU_SOURCES = ["psg_context.cu", "psg_tree.cu", "psg_trace.cu", "psg_tick.cu", "psg_emit.cu", "psg_mlp.cu", "psg_surrogate.cu"]
-C_SOURCES = ["psg_host.c"]
+C_SOURCES = ["psg_host.c", "psg_snapshot.c"]
 HEADERS = ["psg_internal.cuh", "psg_solve.cuh", "psg_surrogate.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -4,6 +4,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <vector>
+
 #include "psg_internal.cuh"
 
 int psg_fail(psg_context *ctx, int code, const char *fmt, ...) {
@@ -389,5 +391,68 @@ extern "C" int psg_set_state(psg_context *ctx, const double *lambdaH, const floa
 	if (ie && (rc = from_caller(ctx, ctx->d_ie, ie))) return rc;
 	if (lasthit && (rc = from_caller(ctx, ctx->d_lasthit, lasthit))) return rc;
 	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	return PSG_OK;
+}
+
+extern "C" int psg_set_hits(psg_context *ctx, const int32_t *hits) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!ctx->n || !hits) return psg_fail(ctx, PSG_E_INVAL, "psg_set_hits: no particles or no counters");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	const int rc = from_caller(ctx, ctx->d_hits, hits);
+	if (rc) return rc;
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	return PSG_OK;
+}
+
+extern "C" int psg_write_output(psg_context *ctx, const char *filename, const psg_snapshot *meta) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!filename || !meta || meta->ngas != ctx->n || !ctx->n)
+		return psg_fail(ctx, PSG_E_INVAL, "psg_write_output: meta->ngas must equal the loaded particle count");
+	if (!ctx->have_physics) return psg_fail(ctx, PSG_E_INVAL, "psg_write_output: set physics first");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	const size_t n = ctx->n;
+	std::vector<float4> psml(n);
+	std::vector<float> pos(3 * n), sml(n), mass(n), rho(n), ie(n), xHI(n), ye(n), zero(n, 0.0f);
+	std::vector<double> lam(n);
+	std::vector<int32_t> hits(n);
+	std::vector<int64_t> lasthit(n), ids;
+	int rc = 0;
+	if ((rc = to_caller(ctx, psml.data(), ctx->d_psml)) || (rc = to_caller(ctx, mass.data(), ctx->d_mass)) ||
+			(rc = to_caller(ctx, rho.data(), ctx->d_rho)) || (rc = to_caller(ctx, ie.data(), ctx->d_ie)) ||
+			(rc = to_caller(ctx, lam.data(), ctx->d_lambdaH)) || (rc = to_caller(ctx, hits.data(), ctx->d_hits)) ||
+			(rc = to_caller(ctx, lasthit.data(), ctx->d_lasthit)))
+		return rc;
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	// helium frozen fully ionised in hydrogen-only runs (lambdaHeI = lambdaHeII = 0)
+	const double he_e = ctx->u.hemf / ctx->u.hmf * 0.25 * 2.0;
+	for (size_t i = 0; i < n; i++) {
+		pos[3 * i] = psml[i].x;
+		pos[3 * i + 1] = psml[i].y;
+		pos[3 * i + 2] = psml[i].z;
+		sml[i] = psml[i].w;
+		xHI[i] = (float)lam[i];
+		ye[i] = (float)((1.0 - lam[i]) + he_e);
+	}
+	psg_snapshot s = *meta;
+	if (!s.id) {
+		ids.resize(n);
+		for (size_t i = 0; i < n; i++) ids[i] = (int64_t)i;
+		s.id = ids.data();
+	}
+	s.pos = pos.data();
+	s.sml = sml.data();
+	s.mass = mass.data();
+	s.rho = rho.data();
+	s.ie = ie.data();
+	s.xHI = xHI.data();
+	s.ye = ye.data();
+	s.xHeI = zero.data();
+	s.xHeII = zero.data();
+	s.gammaHI = zero.data();
+	s.lasthit = lasthit.data();
+	s.hits = hits.data();
+	if (s.boxsize == 0.0) s.boxsize = ctx->boxsize;
+	rc = psg_snapshot_write(filename, &s);
+	if (rc) return psg_fail(ctx, rc, "psg_write_output: writing %s failed", filename);
 	return PSG_OK;
 }
