@@ -111,6 +111,8 @@ typedef struct {
 	int on_the_spot;         /* psphray.onTheSpot */
 	int h_only;              /* psphray.HOnly (only 1 is supported) */
 	int adiabatic;           /* psphray.adiabatic */
+	int euler;               /* step_evolve_euler() solve.c:225-316 (a build without
+	                            USE_LSODA) instead of the adaptive integrator */
 } psg_flags;
 
 /* Upload units, tables and flags. Must precede psg_load_particles(). */

@@ -11,6 +11,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libpsphray_ref.so")
+EULER_LIB_PATH = os.path.join(HERE, "_ref", "libpsphray_ref_euler.so")   # solve.c without USE_LSODA
 
 
 class Xtype(C.Structure):
@@ -33,16 +34,16 @@ def _p(a, ct):
 class Reference:
     """One process-wide instance: the reference keeps its state in globals."""
 
-    _lib = None
+    _libs = {}
 
     def __init__(self, rates_path: str, units, isothermal=True, on_the_spot=True,
-                 h_only=True, adiabatic=False, threads: int | None = None):
-        if Reference._lib is not None:
-            raise RuntimeError("the reference harness holds global state; one instance per process")
-        if not os.path.exists(LIB_PATH):
-            raise FileNotFoundError(f"{LIB_PATH} missing: run `make -C oracle ref`")
-        lib = C.CDLL(LIB_PATH)
-        Reference._lib = lib
+                 h_only=True, adiabatic=False, threads: int | None = None, lib_path: str = LIB_PATH):
+        if lib_path in Reference._libs:
+            raise RuntimeError("the reference harness holds global state; one instance per library and process")
+        if not os.path.exists(lib_path):
+            raise FileNotFoundError(f"{lib_path} missing: run `make -C oracle ref`")
+        lib = C.CDLL(lib_path)
+        Reference._libs[lib_path] = lib
         self.lib = lib
         lib.ref_setup.argtypes = [C.c_char_p] + [C.c_double] * 5 + [C.c_int] * 4
         lib.ref_sph_depth.restype = C.c_double

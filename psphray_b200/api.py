@@ -67,7 +67,7 @@ class XsTable(C.Structure):
 
 class Flags(C.Structure):
     _fields_ = [("isothermal", C.c_int), ("on_the_spot", C.c_int), ("h_only", C.c_int),
-                ("adiabatic", C.c_int)]
+                ("adiabatic", C.c_int), ("euler", C.c_int)]
 
 
 class Particles(C.Structure):
@@ -246,7 +246,7 @@ class Physics:
     file formats (units_init, ar_init, xs_init, kernel.akline)."""
 
     def __init__(self, units, rates_path: str = RATES_HUI, kernel_path: str = KERNEL_AKLINE,
-                 isothermal=True, on_the_spot=True, h_only=True, adiabatic=False):
+                 isothermal=True, on_the_spot=True, h_only=True, adiabatic=False, euler=False):
         L = lib()
         self.units = units
         p = UnitParams(units.h, units.hmf, units.length_cmh, units.mass_gramh, units.time_sh)
@@ -262,7 +262,7 @@ class Physics:
         self._check(L.psg_kernel_table_load(kernel_path.encode(), self.kernel.ctypes.data, 65536, C.byref(n)),
                     f"psg_kernel_table_load({kernel_path})")
         self.kernel = self.kernel[: n.value].copy()
-        self.flags = Flags(int(isothermal), int(on_the_spot), int(h_only), int(adiabatic))
+        self.flags = Flags(int(isothermal), int(on_the_spot), int(h_only), int(adiabatic), int(euler))
 
     @staticmethod
     def _check(rc, what):

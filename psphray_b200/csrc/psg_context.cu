@@ -70,11 +70,11 @@ extern "C" int psg_create(psg_context **out, int device) {
 
 static void free_particles(psg_context *ctx) {
 	void *ptrs[] = {ctx->d_psml, ctx->d_mass, ctx->d_rho, ctx->d_yeMET, ctx->d_ie, ctx->d_flag,
-		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep, ctx->d_order};
+		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep, ctx->d_order, ctx->d_gcarry};
 	for (void *p : ptrs) if (p) cudaFree(p);
 	ctx->d_psml = nullptr; ctx->d_mass = ctx->d_rho = ctx->d_yeMET = ctx->d_ie = nullptr;
 	ctx->d_flag = nullptr; ctx->d_lambdaH = nullptr; ctx->d_hits = nullptr; ctx->d_lasthit = nullptr;
-	ctx->d_hstep = nullptr; ctx->d_order = nullptr;
+	ctx->d_hstep = nullptr; ctx->d_order = nullptr; ctx->d_gcarry = nullptr;
 	ctx->n = 0;
 }
 
@@ -248,6 +248,7 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMalloc(&ctx->d_hits, sizeof(int32_t) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_lasthit, sizeof(int64_t) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_hstep, sizeof(float) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_gcarry, sizeof(double) * n));
 	float *d_pos = (float *)psg_scratch(ctx, S_MISC, sizeof(float) * n * 7);
 	if (!d_pos) return PSG_E_NOMEM;
 	float *d_sml = d_pos + 3 * n, *d_xHI = d_pos + 4 * n, *d_ye = d_pos + 5 * n;
@@ -264,6 +265,7 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMemsetAsync(ctx->d_hits, 0, sizeof(int32_t) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_lasthit, 0, sizeof(int64_t) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_hstep, 0, sizeof(float) * n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_gcarry, 0, sizeof(double) * n, s));
 	const int bs = 256;
 	k_init_particles<<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(n, d_pos, d_sml, d_xHI, d_ye,
 			ctx->d_psml, ctx->d_lambdaH, ctx->d_yeMET);
@@ -312,7 +314,8 @@ int psg_permute_particles(psg_context *ctx, const uint32_t *g) {
 			(rc = permute_array(ctx, ctx->d_rho, g)) || (rc = permute_array(ctx, ctx->d_yeMET, g)) ||
 			(rc = permute_array(ctx, ctx->d_ie, g)) || (rc = permute_array(ctx, ctx->d_flag, g)) ||
 			(rc = permute_array(ctx, ctx->d_lambdaH, g)) || (rc = permute_array(ctx, ctx->d_hits, g)) ||
-			(rc = permute_array(ctx, ctx->d_lasthit, g)) || (rc = permute_array(ctx, ctx->d_hstep, g)))
+			(rc = permute_array(ctx, ctx->d_lasthit, g)) || (rc = permute_array(ctx, ctx->d_hstep, g)) ||
+			(rc = permute_array(ctx, ctx->d_gcarry, g)))
 		return rc;
 	// the caller index of every new position: through the previous order
 	const size_t n = ctx->n;

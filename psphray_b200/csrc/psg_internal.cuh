@@ -71,6 +71,7 @@ struct psg_context {
 	int32_t *d_hits = nullptr;
 	int64_t *d_lasthit = nullptr;
 	float *d_hstep = nullptr;    // last integrator step proposal, seconds (0: none yet)
+	double *d_gcarry = nullptr;  // absorbed photons per H left over by an explicit step
 	uint32_t *d_order = nullptr; // after a tree build the arrays above are in leaf order:
 	                             // position k holds the caller's particle d_order[k] (null: caller order)
 

@@ -32,7 +32,7 @@ struct PhysParams {
 	int kernel_n;
 	double H_PER_MASS, HI_ENERGY, MPROTON_OVER_BOLTZMANN, BOLTZMANN_OVER_MPROTON, hmf, hemf;
 	double he_e;           // helium electrons per H, helium frozen (psystem.h:134-137)
-	int isothermal, on_the_spot, adiabatic;
+	int isothermal, on_the_spot, adiabatic, euler;
 };
 
 PhysParams psg_phys_params(const psg_context *ctx);
@@ -157,7 +157,7 @@ __device__ __forceinline__ RhsCtx make_rhs_ctx(const PhysParams &P, double yeMET
 __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const double x[2], double dx[2]) {
 	const double xHI = x[0], xHII = 1.0 - x[0];
 	const double ye = xHII + P.he_e + cx.yeMET;
-	const double T = cx.T_num * x[1] / __fma_rn(P.hmf, ye, cx.T_den0);
+	const double T = P.isothermal ? cx.T : cx.T_num * x[1] / __fma_rn(P.hmf, ye, cx.T_den0);
 	// the row of tabfun_get() and the offset into it (clamped rows: offset 0)
 	const double logT = log10(T);
 	long long idx = (long long)((logT - P.ar_min) * P.ar_step_inv);
@@ -367,6 +367,48 @@ __device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2],
 	x[1] = S.x[1];
 	if (done) return true;
 	return rosenbrock(P, cx, x, S.t, S.h, max_steps);
+}
+
+// step_evolve_euler() solve.c:225-316, hydrogen only: nsteps explicit Euler
+// steps of the normalised system, the internal step a 200th of the shorter
+// of the recombination and ionisation times at the start (rates of
+// FETCH_VARS, solve.c:42-73), at most 10000 steps; the walk stops one step
+// after lambdaH leaves [0, 1] and reports the unused fraction of the step
+// (step_remain = 1 - (float)k / nsteps). Returns PSG_ST_* bits.
+__device__ inline uint32_t euler_step(const PhysParams &P, const RhsCtx &cx, double x[2], double &step_remain,
+		int &refined) {
+	const double ye = (1.0 - x[0]) + P.he_e + cx.yeMET;
+	const double T = P.isothermal ? cx.T : ieye2T(P, x[1], ye);
+	const RateAt R = rates_at(P, log10(T));
+	const double alphaA = R(PSG_AR_HII_RC_A) * cx.nH;
+	const double gamma = R(PSG_AR_HI_CI) * cx.nH;
+	double internal = fmin(1.0 / alphaA, 1.0 / gamma) / 200.0;
+	internal = fmin(internal, cx.time);
+	int nsteps = (int)(cx.time / internal);
+	if (nsteps > 10000) nsteps = 10000;
+	if (nsteps < 1) nsteps = 1;
+	const double h = 1.0 / nsteps;
+	refined = nsteps > 1;
+	uint32_t st = 0;
+	int k;
+	for (k = 0; k < nsteps; k++) {
+		double dx[2];
+		rhs(P, cx, x, dx);
+		if (!(x[1] + dx[1] >= 0.0)) st |= PSG_ST_IE_NEG;      // function()'s check, solve.c:137-139
+		x[0] += dx[0] * h;
+		x[1] += dx[1] * h;
+		if (!isfinite(x[0]) || !isfinite(x[1])) {
+			st |= PSG_ST_NAN;
+			k++;
+			break;
+		}
+		if (x[0] < 0.0 || x[0] > 1.0) {
+			k++;
+			break;
+		}
+	}
+	step_remain = 1.0 - (double)((float)k / (float)nsteps);
+	return st;
 }
 
 // Isothermal step only (the closed form), for the kernels specialised on it.

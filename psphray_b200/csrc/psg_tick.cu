@@ -52,6 +52,7 @@ PhysParams psg_phys_params(const psg_context *ctx) {
 	P.isothermal = ctx->flags.isothermal;
 	P.on_the_spot = ctx->flags.on_the_spot;
 	P.adiabatic = ctx->flags.adiabatic;
+	P.euler = ctx->flags.euler;
 	return P;
 }
 
@@ -379,10 +380,11 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 		const uint32_t *__restrict__ act_ipar, int32_t *__restrict__ hits, double *__restrict__ act_g,
 		double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
-		const float *__restrict__ hstep, UpdRec *__restrict__ rec, int lo, const PhysParams &P, int64_t tick,
-		double tick_time, uint32_t *__restrict__ status) {
+		const float *__restrict__ hstep, UpdRec *__restrict__ rec, int lo, const double *__restrict__ gcarry,
+		const PhysParams &P, int64_t tick, double tick_time, uint32_t *__restrict__ status) {
 	const uint32_t p = act_ipar[a];
 	hits[p] += nh;
+	if (gcarry) g += gcarry[p];      // photons left over by an earlier explicit step (loop.c:745)
 	if (!ISO) {
 		act_g[a] = g;
 		act_heat[a] = heat;
@@ -434,7 +436,8 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat,
 		double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit,
 		const float *__restrict__ rho, const float *__restrict__ yeMET, const float *__restrict__ hstep,
-		UpdRec *__restrict__ rec, PhysParams P, int64_t tick, double tick_time, uint32_t *__restrict__ status) {
+		UpdRec *__restrict__ rec, const double *__restrict__ gcarry, PhysParams P, int64_t tick, double tick_time,
+		uint32_t *__restrict__ status) {
 	if ((int)blockIdx.x < long_blocks) {
 		const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
 		const int lane = threadIdx.x & 31;
@@ -464,7 +467,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		}
 		if (lane == 0)
 			finish_particle<ISO>(a, sg, sh, sn, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
-					hstep, rec, tick_act[t], P, tick, tick_time, status);
+					hstep, rec, tick_act[t], gcarry, P, tick, tick_time, status);
 		return;
 	}
 	const int a = tick_act[t] + (blockIdx.x - long_blocks) * blockDim.x + threadIdx.x;
@@ -478,7 +481,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		if (d >= 0.0) { g += d; if (want_heat) heat += acc_heat[k]; nh++; }
 	}
 	finish_particle<ISO>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET, hstep,
-			rec, tick_act[t], P, tick, tick_time, status);
+			rec, tick_act[t], gcarry, P, tick, tick_time, status);
 }
 
 // update_pars() loop.c:653-770, not isothermal: every lane integrates one
@@ -632,6 +635,33 @@ __global__ void __launch_bounds__(64) k_update_stiff(const StiffItem *__restrict
 	if (st) atomicOr(status, st);
 }
 
+// update_pars() with step_evolve_euler(): one thread per active particle
+// from its record; the unused fraction of the absorbed photons is carried
+// to the particle's next update (loop.c:745), heat is not (loop.c:769).
+__global__ void __launch_bounds__(128) k_update_euler(int t, const int32_t *__restrict__ tick_act,
+		const UpdRec *__restrict__ rec, double *__restrict__ lambdaH, float *__restrict__ ie,
+		int64_t *__restrict__ lasthit, double *__restrict__ gcarry, PhysParams P, int64_t tick,
+		uint32_t *__restrict__ status) {
+	const int lo = tick_act[t];
+	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
+	if (a >= tick_act[t + 1]) return;
+	const UpdRec r = rec[a - lo];
+	const double ie0 = (double)r.ie0;
+	const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, r.lam0), P.he_e));
+	const RhsCtx cx = make_rhs_ctx(P, (double)r.yeMET, r.g, r.heat, r.time, rn_dmul(P.H_PER_MASS, (double)r.rho), T);
+	double x[2] = {r.lam0, ie0};
+	double remain = 0.0;
+	int refined = 0;
+	uint32_t st = euler_step(P, cx, x, remain, refined);
+	const double lam = fmin(1.0, fmax(0.0, x[0]));
+	lambdaH[r.p] = lam;
+	if (P.isothermal) ie[r.p] = (float)Tye2ie(P, T, rn_dadd(rn_dsub(1.0, lam), P.he_e));
+	else if (!P.adiabatic) ie[r.p] = (float)x[1];
+	lasthit[r.p] = tick;
+	gcarry[r.p] = r.g * remain;
+	if (st) atomicOr(status, st);
+}
+
 // Update log (training data of the surrogate): the inputs of every active
 // particle's step before the update, the outputs after it.
 __global__ void k_log_pre(int t, const int32_t *__restrict__ tick_act, const uint32_t *__restrict__ act_ipar,
@@ -679,6 +709,22 @@ __global__ void k_step_evolve(psg_step *steps, size_t n, PhysParams P, uint32_t 
 	const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	psg_step s = steps[i];
+	if (P.euler) {
+		// step_evolve_euler(): no clamping here (update_pars clamps), the
+		// unused fraction of the step and whether it was subdivided
+		const RhsCtx cx = make_rhs_ctx(P, s.yeMET, s.yGdepHI, s.heat, s.time, s.nH, s.T);
+		double x[2] = {s.lambdaH, s.ie};
+		double remain = 0.0;
+		int refined = 0;
+		const uint32_t st = euler_step(P, cx, x, remain, refined);
+		s.lambdaH = x[0];
+		s.ie = x[1];
+		s.step_remain = remain;
+		s.refined = refined;
+		steps[i] = s;
+		if (st) atomicOr(status, st);
+		return;
+	}
 	double lam = s.lambdaH, e = s.ie;
 	const uint32_t st = solve_step(P, lam, e, s.yeMET, s.yGdepHI, s.heat, s.time, s.nH, s.T);
 	s.lambdaH = lam;
@@ -850,7 +896,8 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	const size_t na = (size_t)(h_tick_act[K] > 0 ? h_tick_act[K] : 1);
 	size_t maxt = 1;
 	for (size_t t = 0; t < K; t++) maxt = std::max<size_t>(maxt, (size_t)(h_tick_act[t + 1] - h_tick_act[t]));
-	const bool surr = !iso && ctx->surr_on && !ctx->flags.adiabatic;
+	const bool euler = ctx->flags.euler != 0;
+	const bool surr = !iso && !euler && ctx->surr_on && !ctx->flags.adiabatic;
 	char *um = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * 3 * (K + 1)
 			+ (iso ? 0 : sizeof(StiffItem) * maxt) + (surr ? sizeof(uint32_t) * maxt : 0) + 512);
 	int32_t *aflag = (int32_t *)psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (3 * (na + 1) + K + 1) + 512);
@@ -865,7 +912,7 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * 3 * (K + 1), st));
 	if (surr) PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 8, 0, sizeof(unsigned long long), st));
 	UpdRec *urec = nullptr;
-	if (!iso) {
+	if (!iso || euler) {
 		urec = (UpdRec *)psg_scratch(ctx, S_REC, sizeof(UpdRec) * maxt);
 		if (!urec) return PSG_E_NOMEM;
 	}
@@ -916,19 +963,25 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 			const int nl = h_tick_long[t + 1] - h_tick_long[t];
 			const int lb = (nl + 7) / 8;
 			const unsigned rgrid = (unsigned)(lb + (int)blocks(nact_t, 256));
-			if (iso)
+			const double *gcarry = euler ? ctx->d_gcarry : nullptr;
+			if (iso && !euler)
 				k_reduce<true><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat,
 						long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,
-						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, P, tick, tick_time,
+						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, tick, tick_time,
 						ctx->d_status);
 			else
 				k_reduce<false><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat,
 						long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,
-						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, P, tick, tick_time,
+						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, tick, tick_time,
 						ctx->d_status);
 			PSG_CHECK_LAUNCH();
 			ctx->launches++;
-			if (!iso) {
+			if (euler) {
+				k_update_euler<<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, urec, ctx->d_lambdaH, ctx->d_ie,
+						ctx->d_lasthit, ctx->d_gcarry, P, tick, ctx->d_status);
+				PSG_CHECK_LAUNCH();
+				ctx->launches++;
+			} else if (!iso) {
 				const unsigned qgrid = (unsigned)std::min<size_t>(blocks(nact_t, 256), (size_t)dev_sms * 8);
 				if (feat) {
 					k_log_pre<<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_g, act_heat,
