@@ -409,6 +409,31 @@ def main():
                      "x_HII_rel_diff": {"p50": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),
                                         "max": float(rel.max())}}
 
+    # recombination rays (onTheSpot = false): the same rays on a context
+    # with case-A recombination, nrec = 100 recombination rays per tick
+    # emitted on the device; the ticks then run one at a time
+    rctx = api.Context(dev)
+    rctx.set_stream(stream.cuda_stream)
+    rctx.set_physics(api.Physics(w.field.units, isothermal=w.isothermal, on_the_spot=False))
+    rctx.load(w.field)
+    rctx.build_tree(8)
+    rctx.set_recombination(nrec=100)
+    nrs = min(3, nsteps - 1)
+    rctx.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
+    r_ms, r_hits, r_rays = 0.0, 0.0, 0.0
+    for s in range(1, 1 + nrs):
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = rctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
+        e1.record(stream)
+        e1.synchronize()
+        r_ms += e0.elapsed_time(e1)
+        r_hits += st["hits"]
+        r_rays += st["rec_rays"]
+    rctx.close()
+    recombination = {"value": r_hits / (r_ms / 1e3), "unit": "hits/s", "ms_per_tick": r_ms / (nrs * T),
+                     "rec_rays_per_tick": r_rays / (nrs * T), "steps": nrs, "ticks_per_step": T}
+
     # roofline of the dominant kernel group
     peak, peak_kind = peaks()
     dom = max(api.KERNELS, key=lambda k: kms[k])
@@ -449,6 +474,7 @@ def main():
                          "path_frac": path_gbs / peak},
             "clocks": clk,
             "surrogate": surrogate,
+            "recombination": recombination,
             "e2e_device_emission": {"value": em_hits / em_t, "unit": "hits/s", "h2d_bytes_per_step": 0,
                                     "d2h_bytes_per_step": int(lam.nbytes)},
             "e2e": {"value": e2e_hits / e2e_t, "unit": "hits/s",

@@ -108,7 +108,9 @@ int psg_set_stream(psg_context *ctx, void *stream);
 /* Physics switches, the config.c flags that the path reads. */
 typedef struct {
 	int isothermal;          /* psphray.isothermal */
-	int on_the_spot;         /* psphray.onTheSpot */
+	int on_the_spot;         /* psphray.onTheSpot; 0: case-A recombination, the photons
+	                            collected in yGrecHII and re-emitted as recombination
+	                            rays (psg_set_recombination) */
 	int h_only;              /* psphray.HOnly (only 1 is supported) */
 	int adiabatic;           /* psphray.adiabatic */
 	int euler;               /* step_evolve_euler() solve.c:225-316 (a build without
@@ -189,21 +191,51 @@ typedef struct {
 	double kernel_ms[PSG_K_NKERNELS];        /* per kernel group, with timing on */
 	double kernel_launches[PSG_K_NKERNELS];
 	double surrogate_accepted;  /* particle updates taken from the surrogate (psg_set_surrogate) */
+	double rec_rays;        /* recombination rays emitted (stat.rec_ray_count) */
+	double rec_photons;     /* photons they carried (stat.rec_photon_count) */
 } psg_tick_stats;
 
 /* Runs nticks ticks; rays holds nray_per_tick rays for each tick, tick by
  * tick (host buffer). Tick k (0-based) is the reference's psys.tick =
  * first_tick + k. Per tick: trace, deposit, merge, update -- run_epoch()
- * loop.c:128-147 without emit_rays(). stats may be NULL. */
+ * loop.c:128-147 without the source half of emit_rays(). Not on the spot,
+ * each tick also emits its recombination rays on the device first (see
+ * psg_set_recombination) and the ticks run one at a time. stats may be
+ * NULL. */
 int psg_run_ticks(psg_context *ctx, const psg_ray *rays, size_t nray_per_tick, size_t nticks,
 		int64_t first_tick, double tick_time, psg_tick_stats *stats);
 /* Same with rays already in device memory. */
 int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, size_t nray_per_tick,
 		size_t nticks, int64_t first_tick, double tick_time, psg_tick_stats *stats);
 
+/* ---- recombination rays (psphray.onTheSpot = false) ---------------------- */
+/* The recombination half of emit_rays() loop.c:197-232, 273-300, 322-368:
+ * from the second tick on, the particles hit in the previous tick by its
+ * source rays (and by its first recombination ray, merge_pars()
+ * loop.c:628-630) emit nrec rays per tick, each drawing its particle with
+ * weight yGrecHII/xHI; a ray starts at the particle, goes in an isotropic
+ * direction for 0.2 box sides, carries the particle's yGrecHII*NH split
+ * evenly over the rays that drew it, and has an energy drawn from
+ * lte_gen_freq() lte.c:36-44 at the particle's temperature (or the HI edge
+ * with disable_lte, psphray.disableLTE). The photons leave yGrecHII. With
+ * nrec < 0 every such particle with yGrecHII > threshold
+ * (psphray.recombineThreshold) emits one ray; with nrec = 0 none is emitted
+ * and the photons stay in yGrecHII. Defaults: nrec 100 (epoch
+ * nrec, epochs.c:29), threshold 0.1, LTE on, seed 0. The draws are this
+ * library's own stream (Philox4x32-10, streams 4-6). */
+int psg_set_recombination(psg_context *ctx, int nrec, double threshold, int disable_lte, uint64_t seed);
+/* The recombination rays of the last tick run, in the order they were
+ * traced (by emitting particle), with each emitter's caller index; *n
+ * receives their number (rays and ipar may be NULL). */
+int psg_get_rec_rays(psg_context *ctx, psg_ray *rays, int64_t *ipar, size_t cap, size_t *n);
+/* yGrecHII (psystem.h:56) and the tick each particle was last hit by a
+ * source ray (-1: never; the next tick's emitters are those of the
+ * previous tick), caller order. Any pointer may be NULL. */
+int psg_get_rec_state(psg_context *ctx, float *yGrecHII, int32_t *srcmark);
+int psg_set_rec_state(psg_context *ctx, const float *yGrecHII, const int32_t *srcmark);
+
 /* ---- sources and ray emission on the device -------------------------------- */
-/* Source rays of emit_rays() loop.c:163-373 (recombination rays are not
- * emitted). A source is psystem.h's Source: position, type, spectrum and its
+/* Source rays of emit_rays() loop.c:163-373. A source is psystem.h's Source: position, type, spectrum and its
  * luminosity history (Ngamma_dot from ticks[k] on, sources.c:58-66). */
 #define PSG_SRC_PLANE 0     /* PSYS_SRC_PLANE psystem.h:4 */
 #define PSG_SRC_POINT 1     /* PSYS_SRC_POINT psystem.h:5 */

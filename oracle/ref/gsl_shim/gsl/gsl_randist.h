@@ -4,7 +4,13 @@
 #define ORACLE_GSL_RANDIST_H
 #include <stddef.h>
 #include <gsl/gsl_rng.h>
-typedef struct gsl_ran_discrete_t gsl_ran_discrete_t;
+/* A discrete distribution keeps its weights; a draw inverts their running
+ * sum at the uniform set by oracle_shim_set_uniform() (gsl_shim.c). */
+typedef struct gsl_ran_discrete_t {
+	size_t K;
+	double *P;
+} gsl_ran_discrete_t;
+void oracle_shim_set_uniform(double u);
 gsl_ran_discrete_t *gsl_ran_discrete_preproc(size_t K, const double *P);
 size_t gsl_ran_discrete(const gsl_rng *r, const gsl_ran_discrete_t *g);
 void gsl_ran_discrete_free(gsl_ran_discrete_t *g);

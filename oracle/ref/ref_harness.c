@@ -49,9 +49,8 @@ double C_H = 0.72;
 double C_HMF = 0.76;
 double C_HEMF = 0.24;
 Epoch *EPOCHS = NULL;
-/* Table column ids owned by lte.c and secion.c, which are not linked (their
- * callers are on bypassed paths). */
-int LTE_FREQ_HI = -1, LTE_FREQ_HEI = -1, LTE_FREQ_HEII = -1;
+/* Table column ids owned by secion.c, which is not linked (its callers are
+ * on bypassed paths). lte.c is built in ref_lte.c. */
 int SECION_PHI_HI = -1, SECION_PHI_HEI = -1, SECION_EH = -1;
 int N_EPOCHS = 0;
 PSystem psys = {0};
@@ -78,7 +77,6 @@ void stat_stop() { bypassed("stat_stop"); }
 void psystem_write_output(int n) { (void)n; bypassed("psystem_write_output"); }
 void psystem_weight_srcs(double w[]) { (void)w; bypassed("psystem_weight_srcs"); }
 double spec_gen_freq(const int id) { (void)id; bypassed("spec_gen_freq"); return 0; }
-double lte_gen_freq(const int id, const double logT) { (void)id; (void)logT; bypassed("lte_gen_freq"); return 0; }
 double secion_get(int id, double E, double x) { (void)id; (void)E; (void)x; bypassed("secion_get"); return 0; }
 double eos_get_cloud_fraction(const double d) { (void)d; bypassed("eos_get_cloud_fraction"); return 0; }
 double eos_get_egyhot(const double d) { (void)d; bypassed("eos_get_egyhot"); return 0; }
@@ -238,6 +236,15 @@ size_t ref_ray_hits(size_t i, int64_t *ipar, double *d, double *b) {
 size_t ref_active_count(void) { return active_set_length; }
 void ref_active(int64_t *out) {
 	for (size_t i = 0; i < active_set_length; i++) out[i] = active_set[i];
+}
+
+/* yGrecHII (psystem.h:56): the recombination photons of runs not on the
+ * spot, which update_pars() carries through step_evolve() (loop.c:680,756). */
+void ref_get_ygrec(float *out) {
+	for (size_t i = 0; i < psys.npar; i++) out[i] = psys.yGrecHII[i];
+}
+void ref_set_ygrec(const float *in) {
+	for (size_t i = 0; i < psys.npar; i++) psys.yGrecHII[i] = in[i];
 }
 
 void ref_get_state(double *lambdaH, float *ie, float *yGdepHI, float *heat,

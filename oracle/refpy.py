@@ -66,6 +66,12 @@ class Reference:
         lib.ref_tree_ncells.restype = C.c_size_t
         lib.ref_step_evolve.argtypes = [C.c_void_p, C.c_size_t]
         lib.ref_sizeof_step.restype = C.c_size_t
+        lib.ref_get_ygrec.argtypes = [C.c_void_p]
+        lib.ref_set_ygrec.argtypes = [C.c_void_p]
+        lib.ref_lte_row.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        lib.ref_lte_row.restype = C.c_int
+        lib.ref_lte_gen_freq.argtypes = [C.c_double, C.c_double]
+        lib.ref_lte_gen_freq.restype = C.c_double
         assert lib.ref_sizeof_step() == C.sizeof(Step)
         self.units = units
         lib.ref_setup(rates_path.encode(), units.h, units.hmf, units.length_cmh,
@@ -160,6 +166,30 @@ class Reference:
                 np.ascontiguousarray(ie, np.float32) if ie is not None else None,
                 np.ascontiguousarray(lasthit, np.int64) if lasthit is not None else None]
         self.lib.ref_set_state(*[a.ctypes.data_as(C.c_void_p) if a is not None else None for a in keep])
+
+    def ygrec(self) -> np.ndarray:
+        """yGrecHII of every particle (runs not on the spot)."""
+        out = np.zeros(self.n, np.float32)
+        self.lib.ref_get_ygrec(out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def set_ygrec(self, yg) -> None:
+        a = np.ascontiguousarray(yg, np.float32)
+        self.lib.ref_set_ygrec(a.ctypes.data_as(C.c_void_p))
+
+    def lte_init(self) -> None:
+        """lte_init() src/lte.c:30-34: the LTE recombination spectra."""
+        self.lib.ref_lte_init()
+
+    def lte_row(self, row: int):
+        """(energies, weights) of the HI table's row (lte_fill() src/lte.c:46-72)."""
+        f = np.zeros(1024); w = np.zeros(1024)
+        n = self.lib.ref_lte_row(int(row), f.ctypes.data_as(C.c_void_p), w.ctypes.data_as(C.c_void_p))
+        return f[:n], w[:n]
+
+    def lte_gen_freq(self, logT: float, u: float) -> float:
+        """lte_gen_freq(LTE_FREQ_HI, logT) src/lte.c:36-44 drawing at uniform u."""
+        return self.lib.ref_lte_gen_freq(float(logT), float(u))
 
     def stats(self) -> dict:
         out = np.zeros(8)

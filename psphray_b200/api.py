@@ -156,7 +156,7 @@ class TickStats(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("hits", "saturated", "active", "lost_photons",
                                           "trace_ms", "tick_ms", "launches")] + [
         ("kernel_ms", C.c_double * len(KERNELS)), ("kernel_launches", C.c_double * len(KERNELS)),
-        ("surrogate_accepted", C.c_double)]
+        ("surrogate_accepted", C.c_double), ("rec_rays", C.c_double), ("rec_photons", C.c_double)]
 
 
 def _stats(st: TickStats) -> dict:
@@ -164,6 +164,8 @@ def _stats(st: TickStats) -> dict:
     d["kernel_ms"] = dict(zip(KERNELS, list(st.kernel_ms)))
     d["kernel_launches"] = dict(zip(KERNELS, list(st.kernel_launches)))
     d["surrogate_accepted"] = st.surrogate_accepted
+    d["rec_rays"] = st.rec_rays
+    d["rec_photons"] = st.rec_photons
     return d
 
 
@@ -228,6 +230,10 @@ def lib() -> C.CDLL:
         "psg_snapshot_read": ([C.c_char_p, C.POINTER(CSnapshot)], C.c_int),
         "psg_write_output": ([vp, C.c_char_p, C.POINTER(CSnapshot)], C.c_int),
         "psg_set_hits": ([vp, vp], C.c_int),
+        "psg_set_recombination": ([vp, C.c_int, dbl, C.c_int, C.c_uint64], C.c_int),
+        "psg_get_rec_rays": ([vp, vp, vp, sz, C.POINTER(sz)], C.c_int),
+        "psg_get_rec_state": ([vp, vp, vp], C.c_int),
+        "psg_set_rec_state": ([vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -502,6 +508,33 @@ class Context:
     def set_hits(self, hits):
         h = np.ascontiguousarray(hits, np.int32)
         self._check(lib().psg_set_hits(self.h, h.ctypes.data), "psg_set_hits")
+
+    def set_recombination(self, nrec: int = 100, threshold: float = 0.1, disable_lte: bool = False, seed: int = 0):
+        """Recombination rays when not on the spot (epoch nrec,
+        psphray.recombineThreshold, psphray.disableLTE)."""
+        self._check(lib().psg_set_recombination(self.h, int(nrec), float(threshold), int(bool(disable_lte)),
+                                                C.c_uint64(seed)), "psg_set_recombination")
+
+    def rec_rays(self):
+        """The last tick's recombination rays and their emitters (caller index)."""
+        n = C.c_size_t(0)
+        self._check(lib().psg_get_rec_rays(self.h, None, None, 0, C.byref(n)), "psg_get_rec_rays")
+        rays = np.zeros(n.value, RAY_DTYPE); ipar = np.zeros(n.value, np.int64)
+        if n.value:
+            self._check(lib().psg_get_rec_rays(self.h, rays.ctypes.data, ipar.ctypes.data, n.value, C.byref(n)),
+                        "psg_get_rec_rays")
+        return rays, ipar
+
+    def rec_state(self):
+        """yGrecHII and the tick each particle was last hit by a source ray."""
+        yg = np.zeros(self.n, np.float32); mark = np.zeros(self.n, np.int32)
+        self._check(lib().psg_get_rec_state(self.h, yg.ctypes.data, mark.ctypes.data), "psg_get_rec_state")
+        return yg, mark
+
+    def set_rec_state(self, yGrecHII=None, srcmark=None):
+        keep = [None if yGrecHII is None else np.ascontiguousarray(yGrecHII, np.float32),
+                None if srcmark is None else np.ascontiguousarray(srcmark, np.int32)]
+        self._check(lib().psg_set_rec_state(self.h, *[_ptr(a) for a in keep]), "psg_set_rec_state")
 
     def step_evolve(self, steps: np.ndarray) -> np.ndarray:
         steps = np.ascontiguousarray(steps, STEP_DTYPE)

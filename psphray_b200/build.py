@@ -20,9 +20,10 @@ INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpsg.so")
 
-CU_SOURCES = ["psg_context.cu", "psg_tree.cu", "psg_trace.cu", "psg_tick.cu", "psg_emit.cu", "psg_mlp.cu", "psg_surrogate.cu"]
+CU_SOURCES = ["psg_context.cu", "psg_tree.cu", "psg_trace.cu", "psg_tick.cu", "psg_emit.cu", "psg_mlp.cu", "psg_surrogate.cu",
+              "psg_recomb.cu"]
 C_SOURCES = ["psg_host.c", "psg_snapshot.c"]
-HEADERS = ["psg_internal.cuh", "psg_solve.cuh", "psg_surrogate.cuh"]
+HEADERS = ["psg_internal.cuh", "psg_solve.cuh", "psg_surrogate.cuh", "psg_philox.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

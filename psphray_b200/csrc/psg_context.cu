@@ -70,11 +70,14 @@ extern "C" int psg_create(psg_context **out, int device) {
 
 static void free_particles(psg_context *ctx) {
 	void *ptrs[] = {ctx->d_psml, ctx->d_mass, ctx->d_rho, ctx->d_yeMET, ctx->d_ie, ctx->d_flag,
-		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep, ctx->d_order, ctx->d_gcarry};
+		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep, ctx->d_order, ctx->d_gcarry, ctx->d_ygrec,
+		ctx->d_srcmark};
 	for (void *p : ptrs) if (p) cudaFree(p);
 	ctx->d_psml = nullptr; ctx->d_mass = ctx->d_rho = ctx->d_yeMET = ctx->d_ie = nullptr;
 	ctx->d_flag = nullptr; ctx->d_lambdaH = nullptr; ctx->d_hits = nullptr; ctx->d_lasthit = nullptr;
-	ctx->d_hstep = nullptr; ctx->d_order = nullptr; ctx->d_gcarry = nullptr;
+	ctx->d_hstep = nullptr; ctx->d_order = nullptr; ctx->d_gcarry = nullptr; ctx->d_ygrec = nullptr;
+	ctx->d_srcmark = nullptr;
+	ctx->rec_last = ctx->rec_last_R = 0;
 	ctx->n = 0;
 }
 
@@ -100,6 +103,7 @@ extern "C" void psg_destroy(psg_context *ctx) {
 	if (ctx->d_counters) cudaFree(ctx->d_counters);
 	if (ctx->d_emit) cudaFree(ctx->d_emit);
 	if (ctx->d_surr) cudaFree(ctx->d_surr);
+	if (ctx->d_lte) cudaFree(ctx->d_lte);
 	for (auto &b : ctx->scratch) if (b.p) cudaFree(b.p);
 	for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
 	for (auto &ev : ctx->kev) if (ev) cudaEventDestroy(ev);
@@ -160,20 +164,24 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 	// in FP32, so a lookup is four 16-byte loads. Linear interpolation from
 	// value and slope is the same line as tabfun_get()'s two-point form.
 	{
-		const int cols[7] = {PSG_AR_HI_CI, flags->on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A,
+		// (an eighth column, alpha_B, for the recombination photons when
+		// not on the spot: alpha_AB = fdim(alpha_A, alpha_B), solve.c:59)
+		const int ncol = flags->on_the_spot ? 7 : 8;
+		const int cols[8] = {PSG_AR_HI_CI, flags->on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A,
 				flags->on_the_spot ? PSG_AR_HII_RCC_B : PSG_AR_HII_RCC_A, PSG_AR_HI_CEC, PSG_AR_HI_CIC,
-				PSG_AR_E_BREMC, PSG_AR_E_COMPC};
+				PSG_AR_E_BREMC, PSG_AR_E_COMPC, PSG_AR_HII_RC_B};
 		float *ni = (float *)calloc(nr * 16, sizeof(float));
 		if (!ni) return psg_fail(ctx, PSG_E_NOMEM, "psg_set_physics: host allocation failed");
 		// internal-unit rates (1e-140 .. 1e-56) are far below FP32's range:
 		// each column is stored divided by its largest magnitude
-		for (int c = 0; c < 7; c++) {
+		for (int c = 0; c < 8; c++) ctx->ar_ni_scale[c] = 1.0;
+		for (int c = 0; c < ncol; c++) {
 			double m = 0.0;
 			for (size_t j = 0; j < nr; j++) m = fmax(m, fabs(ar->col[cols[c]][j]));
 			ctx->ar_ni_scale[c] = m > 0.0 ? m : 1.0;
 		}
 		for (size_t j = 0; j < nr; j++)
-			for (int c = 0; c < 7; c++) {
+			for (int c = 0; c < ncol; c++) {
 				const double sc = ctx->ar_ni_scale[c];
 				const double v = ar->col[cols[c]][j] / sc;
 				const double s = j + 1 < nr ? (ar->col[cols[c]][j + 1] / sc - v) * ar->step_inv : 0.0;
@@ -203,6 +211,10 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 	ctx->xs_step_inv = xs->step_inv;
 	ctx->xs_cut_HI = xs->cut[PSG_XS_HI];
 	ctx->kernel_n = kernel_n;
+	if (!flags->on_the_spot) {
+		const int rc = psg_build_lte(ctx, xs);
+		if (rc) return rc;
+	}
 	ctx->have_physics = 1;
 	return PSG_OK;
 }
@@ -249,6 +261,8 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMalloc(&ctx->d_lasthit, sizeof(int64_t) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_hstep, sizeof(float) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_gcarry, sizeof(double) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_ygrec, sizeof(float) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_srcmark, sizeof(int32_t) * n));
 	float *d_pos = (float *)psg_scratch(ctx, S_MISC, sizeof(float) * n * 7);
 	if (!d_pos) return PSG_E_NOMEM;
 	float *d_sml = d_pos + 3 * n, *d_xHI = d_pos + 4 * n, *d_ye = d_pos + 5 * n;
@@ -266,6 +280,8 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMemsetAsync(ctx->d_lasthit, 0, sizeof(int64_t) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_hstep, 0, sizeof(float) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_gcarry, 0, sizeof(double) * n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_ygrec, 0, sizeof(float) * n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_srcmark, 0xff, sizeof(int32_t) * n, s));
 	const int bs = 256;
 	k_init_particles<<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(n, d_pos, d_sml, d_xHI, d_ye,
 			ctx->d_psml, ctx->d_lambdaH, ctx->d_yeMET);
@@ -315,7 +331,8 @@ int psg_permute_particles(psg_context *ctx, const uint32_t *g) {
 			(rc = permute_array(ctx, ctx->d_ie, g)) || (rc = permute_array(ctx, ctx->d_flag, g)) ||
 			(rc = permute_array(ctx, ctx->d_lambdaH, g)) || (rc = permute_array(ctx, ctx->d_hits, g)) ||
 			(rc = permute_array(ctx, ctx->d_lasthit, g)) || (rc = permute_array(ctx, ctx->d_hstep, g)) ||
-			(rc = permute_array(ctx, ctx->d_gcarry, g)))
+			(rc = permute_array(ctx, ctx->d_gcarry, g)) || (rc = permute_array(ctx, ctx->d_ygrec, g)) ||
+			(rc = permute_array(ctx, ctx->d_srcmark, g)))
 		return rc;
 	// the caller index of every new position: through the previous order
 	const size_t n = ctx->n;
@@ -403,6 +420,28 @@ extern "C" int psg_set_hits(psg_context *ctx, const int32_t *hits) {
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	const int rc = from_caller(ctx, ctx->d_hits, hits);
 	if (rc) return rc;
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	return PSG_OK;
+}
+
+extern "C" int psg_get_rec_state(psg_context *ctx, float *yGrecHII, int32_t *srcmark) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_get_rec_state: no particles loaded");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	int rc = 0;
+	if (yGrecHII && (rc = to_caller(ctx, yGrecHII, ctx->d_ygrec))) return rc;
+	if (srcmark && (rc = to_caller(ctx, srcmark, ctx->d_srcmark))) return rc;
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	return PSG_OK;
+}
+
+extern "C" int psg_set_rec_state(psg_context *ctx, const float *yGrecHII, const int32_t *srcmark) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_set_rec_state: no particles loaded");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	int rc = 0;
+	if (yGrecHII && (rc = from_caller(ctx, ctx->d_ygrec, yGrecHII))) return rc;
+	if (srcmark && (rc = from_caller(ctx, ctx->d_srcmark, srcmark))) return rc;
 	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
 	return PSG_OK;
 }

@@ -29,7 +29,7 @@
 enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
 	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
-	S_EMIT, S_MAP, S_ALONG, S_MLP, S_LOG, S_SURR, S_REC,
+	S_EMIT, S_MAP, S_ALONG, S_MLP, S_LOG, S_SURR, S_REC, S_RECW, S_RECK, S_RECRAYS,
 	S_NSLOTS
 };
 
@@ -52,7 +52,7 @@ struct psg_context {
 	float4 *d_ar_ni = nullptr;   // [ar_nrows][4]: the 7 rates of the non-isothermal
 	                             // right-hand side, values then slopes per log T
 	double ar_step = 0;
-	double ar_ni_scale[7] = {};  // each d_ar_ni column is stored divided by this
+	double ar_ni_scale[8] = {};  // each d_ar_ni column is stored divided by this
 	int ar_nrows = 0;
 	double ar_min = 0, ar_step_inv = 0;
 	double *d_xs = nullptr;      // [2][xs_nrows]: energy, sigma_HI
@@ -72,6 +72,9 @@ struct psg_context {
 	int64_t *d_lasthit = nullptr;
 	float *d_hstep = nullptr;    // last integrator step proposal, seconds (0: none yet)
 	double *d_gcarry = nullptr;  // absorbed photons per H left over by an explicit step
+	float *d_ygrec = nullptr;    // yGrecHII: recombination photons per H not yet emitted
+	int32_t *d_srcmark = nullptr; // last tick a source ray (or the tick's first recombination
+	                             // ray) hit the particle, -1 never: the emitters of the next tick
 	uint32_t *d_order = nullptr; // after a tree build the arrays above are in leaf order:
 	                             // position k holds the caller's particle d_order[k] (null: caller order)
 
@@ -90,6 +93,17 @@ struct psg_context {
 	void *d_emit = nullptr;
 	int nsrc = 0, nspec = 0, nhist_total = 0, nspec_total = 0;
 	uint64_t emit_seed = 0;
+
+	// recombination rays (not on the spot), psg_recomb.cu
+	int rec_nrec = 100;          // epoch nrec (epochs.c:29); < 0: every particle above the threshold, 0: none
+	double rec_threshold = 0.1;  // psphray.recombineThreshold (config.c:37)
+	int rec_disable_lte = 0;     // psphray.disableLTE (config.c:33)
+	uint64_t rec_seed = 0;
+	double *d_lte = nullptr;     // [PSG_LTE_NLOGT][PSG_LTE_NFREQ] cumulative weights
+	double lte_freq_min = 0, lte_freq_step = 0;
+	size_t rec_last = 0;         // recombination rays of the last tick (after the source rays in S_RECRAYS)
+	size_t rec_last_R = 0;       // source rays of that tick
+	size_t rec_last_kmax = 0;    // capacity of that tick's key arrays (S_RECK)
 
 	// chemistry surrogate (not isothermal): weight blob, residual tolerance
 	void *d_surr = nullptr;
@@ -155,6 +169,14 @@ struct PhysParams;
 int psg_surrogate_tick(psg_context *ctx, int t, int nact_t, const int32_t *tick_act, const uint32_t *act_ipar,
 		const double *act_g, const double *act_heat, const PhysParams &P, int64_t tick, double tick_time,
 		uint32_t *rej, unsigned *nrej, int sms);
+
+// recombination rays (psg_recomb.cu): the tick-by-tick loop used by
+// psg_run_ticks_device when not on the spot, and the LTE table build
+int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K, int64_t first_tick,
+		double tick_time, psg_tick_stats *stats);
+int psg_build_lte(psg_context *ctx, const psg_xs_table *xs);
+#define PSG_LTE_NLOGT 128
+#define PSG_LTE_NFREQ 1024
 
 // tree / trace entry points used across units
 int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_db);

@@ -1,0 +1,380 @@
+// Recombination rays on the device (psphray.onTheSpot = false, hydrogen
+// only); replaces the recombination half of emit_rays() loop.c:197-232,
+// 273-300, 305-320 and 322-368, with lte_gen_freq() lte.c:36-44 and
+// lte_fill() lte.c:46-72.
+//
+// From the second tick on (loop.c:197), the particles that the previous
+// tick's source rays hit -- and those of that tick's first recombination
+// ray, which merge_pars() loop.c:628-630 counts in as well -- emit nrec
+// rays: each ray draws its particle with weight yGrecHII/xHI (xHI = 0
+// counts as 1e-10, loop.c:207-211), starts at the particle, goes in an
+// isotropic direction for a tenth of twice the box (loop.c:169), carries
+// the particle's recombination photons yGrecHII*NH split evenly over the
+// rays that drew it (loop.c:305-320), and has an energy drawn from the
+// Lyman-continuum spectrum sigma(E) E^3 exp(-(E - E_HI)/kT) at the
+// particle's temperature (lte.c:60-70). The emitted photons leave the
+// particle's yGrecHII (loop.c:345-356). With nrec < 0 every such particle
+// above the recombine threshold emits one ray instead (loop.c:221-230; the
+// reference reaches that branch through a negative epoch nrec); with nrec
+// = 0 none is emitted and the photons stay in yGrecHII (loop.c:180,197).
+//
+// Emission depends on the previous tick's update, so with recombination
+// rays the ticks of a batch run one at a time: emit, then trace, deposit,
+// merge and update the tick's source rays and recombination rays together.
+//
+// Random numbers: psg_philox.cuh, streams 4-6, keyed by the seed of
+// psg_set_recombination. The reference draws from GSL's MT19937 and its
+// Walker tables (gsl_ran_discrete); the draws here are inverse-CDF draws
+// of the same distributions.
+#include <cub/cub.cuh>
+
+#include <math.h>
+
+#include <vector>
+
+#include "psg_internal.cuh"
+#include "psg_philox.cuh"
+#include "psg_solve.cuh"
+
+int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K, int64_t first_tick,
+		double tick_time, psg_tick_stats *stats);
+
+namespace {
+
+inline unsigned nblocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+__device__ __forceinline__ uint32_t caller_of(const uint32_t *__restrict__ order, uint32_t i) {
+	return order ? order[i] : i;
+}
+
+// first i in [lo, hi) with cdf[i] >= target, or hi
+__device__ __forceinline__ int lower_index(const double *cdf, int lo, int hi, double target) {
+	while (lo < hi) {
+		const int mid = (lo + hi) >> 1;
+		if (cdf[mid] >= target) hi = mid;
+		else lo = mid + 1;
+	}
+	return lo;
+}
+
+// The emitters' weights (loop.c:207-211): particles marked in the previous
+// tick, yGrecHII / xHI, placed in the caller's particle order (so that the
+// draws do not depend on the device's leaf order), and the caller -> leaf
+// map.
+__global__ void k_rec_weight(size_t n, int32_t prev, const int32_t *__restrict__ mark,
+		const float *__restrict__ ygrec, const double *__restrict__ lambdaH, const uint32_t *__restrict__ order,
+		double *__restrict__ w, uint32_t *__restrict__ leaf_of) {
+	const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	double x = lambdaH[p];
+	if (x == 0.0) x = 1e-10;
+	const uint32_t c = caller_of(order, (uint32_t)p);
+	w[c] = mark[p] == prev ? __ddiv_rn((double)ygrec[p], x) : 0.0;
+	leaf_of[c] = (uint32_t)p;
+}
+
+// nrec draws from the cumulative weights (caller order): key = caller index
+// << 24 | draw, value = the particle (leaf order); *count = nrec, or 0 when
+// no weight is positive.
+__global__ void k_rec_draw(size_t n, int nrec, const double *__restrict__ cdf, int64_t tick, uint64_t seed,
+		const uint32_t *__restrict__ leaf_of, unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals,
+		unsigned *__restrict__ count) {
+	const double total = cdf[n - 1];
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k == 0) *count = total > 0.0 ? (unsigned)nrec : 0u;
+	if (k >= nrec || !(total > 0.0)) return;
+	uint32_t x[4];
+	draw(x, (uint32_t)k, tick, 4u, seed);
+	const double target = rn_dmul(u01(x[0], x[1]), total);
+	int c = upper_index(cdf, 0, (int)n, target);
+	if (c >= (int)n) c = lower_index(cdf, 0, (int)n, total);   // the last particle with weight
+	keys[k] = ((unsigned long long)c << 24) | (unsigned long long)k;
+	vals[k] = leaf_of[c];
+}
+
+// Threshold mode (loop.c:221-230): every marked particle above the threshold.
+__global__ void k_rec_flag(size_t n, int32_t prev, const int32_t *__restrict__ mark,
+		const float *__restrict__ ygrec, double threshold, uint32_t *__restrict__ flag) {
+	const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	flag[p] = (mark[p] == prev && (double)ygrec[p] > threshold) ? 1u : 0u;
+}
+
+__global__ void k_rec_compact(size_t n, const uint32_t *__restrict__ flag, const uint32_t *__restrict__ pos,
+		const uint32_t *__restrict__ order, unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals,
+		unsigned *__restrict__ count) {
+	const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	if (p == n - 1) *count = pos[p] + flag[p];
+	if (!flag[p]) return;
+	keys[pos[p]] = (unsigned long long)caller_of(order, (uint32_t)p) << 24;
+	vals[pos[p]] = (uint32_t)p;
+}
+
+struct LteView {
+	const double *cdf;        // [PSG_LTE_NLOGT][PSG_LTE_NFREQ], cumulative weights per row
+	double freq_min, freq_step;
+	int disabled;
+};
+
+// The rays, in (caller index, draw) order -- the reference sorts its rays
+// by (type, ipar), loop.c:236. Each ray's photons: yGrecHII*NH of its
+// particle, split over the run of rays that drew it (loop.c:305-320).
+__global__ void k_rec_rays(int M, const uint32_t *__restrict__ vals, int64_t tick, uint64_t seed,
+		const float4 *__restrict__ psml, const float *__restrict__ mass, const float *__restrict__ ygrec,
+		const double *__restrict__ lambdaH, const float *__restrict__ ie, PhysParams P, LteView L, double length,
+		psg_ray *__restrict__ out, double *__restrict__ nph_sum) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= M) return;
+	const uint32_t p = vals[i];
+	int c = 1;
+	for (int j = i - 1; j >= 0 && vals[j] == p; j--) c++;
+	for (int j = i + 1; j < M && vals[j] == p; j++) c++;
+	const double NH = rn_dmul((double)mass[p], P.H_PER_MASS);
+	psg_ray r;
+	r.Nph = rn_dmul(rn_dmul((double)ygrec[p], NH), __ddiv_rn(1.0, (double)c));
+	const float4 q = psml[p];
+	r.s[0] = q.x;
+	r.s[1] = q.y;
+	r.s[2] = q.z;
+	r.length = length;
+	uint32_t x[4];
+	draw(x, (uint32_t)i, tick, 5u, seed);
+	const double cz = rn_dsub(rn_dmul(2.0, u01(x[0], x[1])), 1.0);
+	const double phi = rn_dmul(2.0 * 3.141592653589793, u01(x[2], x[3]));
+	const double st = __dsqrt_rn(fmax(0.0, rn_dsub(1.0, rn_dmul(cz, cz))));
+	double sp, cp;
+	sincos(phi, &sp, &cp);
+	r.dir[0] = (float)rn_dmul(st, cp);
+	r.dir[1] = (float)rn_dmul(st, sp);
+	r.dir[2] = (float)cz;
+	if (L.disabled) {
+		r.freq = L.freq_min;
+	} else {
+		// psys_T() psystem.h:180-182: T from ie and ye without yeMET
+		const double T = ieye2T(P, (double)ie[p], rn_dadd(rn_dsub(1.0, lambdaH[p]), P.he_e));
+		const double logT = log10(T);
+		int row = (int)__ddiv_rn(rn_dsub(logT, 3.0), 7.0 / PSG_LTE_NLOGT);
+		if (row < 0) row = 0;
+		if (row >= PSG_LTE_NLOGT) row = PSG_LTE_NLOGT - 1;
+		const double *cdf = L.cdf + (size_t)row * PSG_LTE_NFREQ;
+		draw(x, (uint32_t)i, tick, 6u, seed);
+		const double total = cdf[PSG_LTE_NFREQ - 1];
+		int j = upper_index(cdf, 0, PSG_LTE_NFREQ, rn_dmul(u01(x[0], x[1]), total));
+		if (j >= PSG_LTE_NFREQ) j = lower_index(cdf, 0, PSG_LTE_NFREQ, total);
+		r.freq = rn_dadd(L.freq_min, rn_dmul(L.freq_step, (double)j));
+	}
+	out[i] = r;
+	atomicAdd(nph_sum, r.Nph);
+}
+
+// The photons leave the emitter (loop.c:345-356): once per run, ray by ray
+// in float as the reference's compound assignment rounds, never below 0.
+__global__ void k_rec_purge(int M, const uint32_t *__restrict__ vals, const psg_ray *__restrict__ rays,
+		const float *__restrict__ mass, float *__restrict__ ygrec, PhysParams P) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= M) return;
+	const uint32_t p = vals[i];
+	if (i > 0 && vals[i - 1] == p) return;
+	const double NH = rn_dmul((double)mass[p], P.H_PER_MASS);
+	float y = ygrec[p];
+	for (int j = i; j < M && vals[j] == p; j++) {
+		y = (float)rn_dsub((double)y, __ddiv_rn(rays[j].Nph, NH));
+		if (y < 0.0f) y = 0.0f;
+	}
+	ygrec[p] = y;
+}
+
+// The emitters of the next tick: every particle on the hit lists of the
+// tick's first nmark rays (its source rays and its first recombination ray).
+__global__ void k_rec_mark(int nmark, const int64_t *__restrict__ off, const uint32_t *__restrict__ hit_ipar,
+		int32_t tick, int32_t *__restrict__ mark) {
+	const int64_t end = off[nmark];
+	for (int64_t h = off[0] + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < end;
+			h += (int64_t)gridDim.x * blockDim.x)
+		mark[hit_ipar[h]] = tick;
+}
+
+// The tick's recombination rays into out (at most cap); *M_out their number.
+int emit_rec(psg_context *ctx, int64_t tick, size_t cap, psg_ray *out, size_t *M_out) {
+	cudaStream_t st = ctx->stream;
+	const size_t n = ctx->n;
+	const PhysParams P = psg_phys_params(ctx);
+	const int threshold_mode = ctx->rec_nrec < 0;
+	const size_t kmax = threshold_mode ? n : (size_t)ctx->rec_nrec;
+	char *wm = (char *)psg_scratch(ctx, S_RECW, sizeof(double) * 2 * n + sizeof(uint32_t) * n + 512);
+	char *km = (char *)psg_scratch(ctx, S_RECK, (sizeof(unsigned long long) + sizeof(uint32_t)) * 2 * kmax + 1024);
+	if (!wm || !km) return PSG_E_NOMEM;
+	unsigned long long *keys = (unsigned long long *)km;
+	uint32_t *vals = (uint32_t *)(keys + 2 * kmax);
+	unsigned *d_count = (unsigned *)(ctx->d_counters + 11);
+	double *d_nph = (double *)(ctx->d_counters + 10);
+	const int32_t prev = (int32_t)(tick - 1);
+	if (!threshold_mode) {
+		double *w = (double *)wm, *cdf = w + n;
+		uint32_t *leaf_of = (uint32_t *)(cdf + n);
+		k_rec_weight<<<nblocks(n, 256), 256, 0, st>>>(n, prev, ctx->d_srcmark, ctx->d_ygrec, ctx->d_lambdaH,
+				ctx->d_order, w, leaf_of);
+		PSG_CHECK_LAUNCH();
+		size_t tmp = 0;
+		PSG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, w, cdf, (int64_t)n, st));
+		void *dt = psg_scratch(ctx, S_CUB, tmp);
+		if (!dt) return PSG_E_NOMEM;
+		PSG_CUDA(cub::DeviceScan::InclusiveSum(dt, tmp, w, cdf, (int64_t)n, st));
+		k_rec_draw<<<nblocks(kmax, 128), 128, 0, st>>>(n, (int)kmax, cdf, tick, ctx->rec_seed, leaf_of,
+				keys, vals, d_count);
+		PSG_CHECK_LAUNCH();
+	} else {
+		uint32_t *flag = (uint32_t *)wm, *pos = flag + n;
+		k_rec_flag<<<nblocks(n, 256), 256, 0, st>>>(n, prev, ctx->d_srcmark, ctx->d_ygrec, ctx->rec_threshold, flag);
+		PSG_CHECK_LAUNCH();
+		size_t tmp = 0;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag, pos, (int64_t)n, st));
+		void *dt = psg_scratch(ctx, S_CUB, tmp);
+		if (!dt) return PSG_E_NOMEM;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, flag, pos, (int64_t)n, st));
+		k_rec_compact<<<nblocks(n, 256), 256, 0, st>>>(n, flag, pos, ctx->d_order, keys, vals, d_count);
+		PSG_CHECK_LAUNCH();
+	}
+	ctx->launches += 3;
+	unsigned M = 0;
+	PSG_CUDA(cudaMemcpyAsync(&M, d_count, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
+	if (M > cap) return psg_fail(ctx, PSG_E_OVERFLOW, "recombination rays: %u > capacity %zu", M, cap);
+	*M_out = M;
+	if (M == 0) return PSG_OK;
+	int nbits = 24;
+	while (nbits < 64 && (1ull << (nbits - 24)) < (unsigned long long)n) nbits++;
+	size_t tmp = 0;
+	PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, keys + kmax, vals, vals + kmax, (int64_t)M, 0, nbits, st));
+	void *dt = psg_scratch(ctx, S_CUB, tmp);
+	if (!dt) return PSG_E_NOMEM;
+	PSG_CUDA(cub::DeviceRadixSort::SortPairs(dt, tmp, keys, keys + kmax, vals, vals + kmax, (int64_t)M, 0, nbits, st));
+	const LteView L{ctx->d_lte, ctx->lte_freq_min, ctx->lte_freq_step, ctx->rec_disable_lte};
+	const double length = ctx->boxsize * 2.0 * 0.1;     // MAX_REC_RAY_LENGTH, loop.c:169
+	k_rec_rays<<<nblocks(M, 128), 128, 0, st>>>((int)M, vals + kmax, tick, ctx->rec_seed, ctx->d_psml, ctx->d_mass,
+			ctx->d_ygrec, ctx->d_lambdaH, ctx->d_ie, P, L, length, out, d_nph);
+	PSG_CHECK_LAUNCH();
+	k_rec_purge<<<nblocks(M, 128), 128, 0, st>>>((int)M, vals + kmax, out, ctx->d_mass, ctx->d_ygrec, P);
+	PSG_CHECK_LAUNCH();
+	ctx->launches += 2;
+	return PSG_OK;
+}
+
+}  // namespace
+
+// lte_fill() lte.c:46-72 for hydrogen: 128 rows of log T from 3 to 10, 1024
+// energies from E_HI up to 16 E_HI; the weights summed in order per row.
+int psg_build_lte(psg_context *ctx, const psg_xs_table *xs) {
+	const double fmin_ = ctx->u.HI_ENERGY, fmax_ = 16.0 * ctx->u.HI_ENERGY;
+	const double fstep = (fmax_ - fmin_) / PSG_LTE_NFREQ;
+	const double tstep = (10.0 - 3.0) / PSG_LTE_NLOGT;
+	std::vector<double> cdf((size_t)PSG_LTE_NLOGT * PSG_LTE_NFREQ), freq(PSG_LTE_NFREQ);
+	for (int j = 0; j < PSG_LTE_NFREQ; j++) freq[j] = fmin_ + fstep * j;
+	for (int i = 0; i < PSG_LTE_NLOGT; i++) {
+		const double logT = 3.0 + tstep * i;
+		const double kT = ctx->u.BOLTZMANN * exp10(logT);
+		double acc = 0.0;
+		for (int j = 0; j < PSG_LTE_NFREQ; j++) {
+			const double f = freq[j];
+			acc += psg_xs_get(xs, PSG_XS_HI, f) * f * f * f * exp(-(f - fmin_) / kT);
+			cdf[(size_t)i * PSG_LTE_NFREQ + j] = acc;
+		}
+	}
+	if (!ctx->d_lte) PSG_CUDA(cudaMalloc(&ctx->d_lte, sizeof(double) * cdf.size()));
+	PSG_CUDA(cudaMemcpy(ctx->d_lte, cdf.data(), sizeof(double) * cdf.size(), cudaMemcpyHostToDevice));
+	ctx->lte_freq_min = fmin_;
+	ctx->lte_freq_step = fstep;
+	return PSG_OK;
+}
+
+int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K, int64_t first_tick,
+		double tick_time, psg_tick_stats *stats) {
+	cudaStream_t st = ctx->stream;
+	const size_t cap = ctx->rec_nrec > 0 ? (size_t)ctx->rec_nrec : ctx->rec_nrec < 0 ? ctx->n : 0;
+	if (R + cap >= (size_t)INT32_MAX) return psg_fail(ctx, PSG_E_OVERFLOW, "psg_run_ticks: batch too large");
+	psg_ray *buf = (psg_ray *)psg_scratch(ctx, S_RECRAYS, sizeof(psg_ray) * (R + cap));
+	if (!buf) return PSG_E_NOMEM;
+	double *d_nph = (double *)(ctx->d_counters + 10);
+	PSG_CUDA(cudaMemsetAsync(d_nph, 0, sizeof(double), st));
+	psg_tick_stats acc{}, one{};
+	double rec_rays = 0.0;
+	long launches = 0;
+	for (size_t k = 0; k < K; k++) {
+		const int64_t tick = first_tick + (int64_t)k;
+		PSG_CUDA(cudaMemcpyAsync(buf, d_rays + k * R, sizeof(psg_ray) * R, cudaMemcpyDeviceToDevice, st));
+		ctx->launches = 0;
+		size_t M = 0;
+		if (tick > 1 && ctx->rec_nrec != 0) {      // loop.c:197
+			const int rc = emit_rec(ctx, tick, cap, buf + R, &M);
+			if (rc) return rc;
+		}
+		const long emit_launches = ctx->launches;
+		ctx->rec_last = M;
+		ctx->rec_last_R = R;
+		ctx->rec_last_kmax = cap;
+		rec_rays += (double)M;
+		int rc = psg_run_ticks_core(ctx, buf, R + M, 1, tick, tick_time, &one);
+		if (rc) return rc;
+		const int nmark = (int)(R + (M > 0 ? 1 : 0));
+		k_rec_mark<<<4 * 148, 256, 0, st>>>(nmark, (const int64_t *)ctx->scratch[S_OFFSETS].p,
+				(const uint32_t *)ctx->scratch[S_HIT_IPAR].p, (int32_t)tick, ctx->d_srcmark);
+		PSG_CHECK_LAUNCH();
+		launches += emit_launches + (long)one.launches + 1;
+		acc.hits += one.hits;
+		acc.saturated += one.saturated;
+		acc.active += one.active;
+		acc.lost_photons += one.lost_photons;
+		acc.trace_ms += one.trace_ms;
+		acc.tick_ms += one.tick_ms;
+		for (int g = 0; g < PSG_K_NKERNELS; g++) {
+			acc.kernel_ms[g] += one.kernel_ms[g];
+			acc.kernel_launches[g] += one.kernel_launches[g];
+		}
+	}
+	double nph = 0.0;
+	PSG_CUDA(cudaMemcpyAsync(&nph, d_nph, sizeof(double), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
+	ctx->launches = launches;
+	if (stats) {
+		acc.launches = (double)launches;
+		acc.rec_rays = rec_rays;
+		acc.rec_photons = nph;
+		*stats = acc;
+	}
+	return PSG_OK;
+}
+
+extern "C" int psg_set_recombination(psg_context *ctx, int nrec, double threshold, int disable_lte,
+		uint64_t seed) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!(threshold >= 0.0)) return psg_fail(ctx, PSG_E_INVAL, "psg_set_recombination: threshold must be >= 0");
+	if (nrec >= (1 << 24)) return psg_fail(ctx, PSG_E_INVAL, "psg_set_recombination: nrec must be below 2^24");
+	ctx->rec_nrec = nrec;
+	ctx->rec_threshold = threshold;
+	ctx->rec_disable_lte = disable_lte != 0;
+	ctx->rec_seed = seed;
+	return PSG_OK;
+}
+
+extern "C" int psg_get_rec_rays(psg_context *ctx, psg_ray *rays, int64_t *ipar, size_t cap, size_t *n) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!n) return psg_fail(ctx, PSG_E_INVAL, "psg_get_rec_rays: null count");
+	*n = ctx->rec_last;
+	if (ctx->rec_last == 0 || (!rays && !ipar)) return PSG_OK;
+	if (cap < ctx->rec_last) return psg_fail(ctx, PSG_E_INVAL, "psg_get_rec_rays: %zu rays, capacity %zu", ctx->rec_last, cap);
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	const size_t M = ctx->rec_last;
+	const size_t kmax = ctx->rec_last_kmax;
+	if (rays)
+		PSG_CUDA(cudaMemcpyAsync(rays, (psg_ray *)ctx->scratch[S_RECRAYS].p + ctx->rec_last_R, sizeof(psg_ray) * M,
+				cudaMemcpyDeviceToHost, ctx->stream));
+	std::vector<unsigned long long> keys(M);
+	if (ipar)
+		PSG_CUDA(cudaMemcpyAsync(keys.data(), (unsigned long long *)ctx->scratch[S_RECK].p + kmax,
+				sizeof(unsigned long long) * M, cudaMemcpyDeviceToHost, ctx->stream));
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	if (ipar)
+		for (size_t i = 0; i < M; i++) ipar[i] = (int64_t)(keys[i] >> 24);
+	return PSG_OK;
+}

@@ -15,14 +15,26 @@
 //     k = sqrt(q^2 + 4*a*g), q = tau*(gamma*(1+m) + alpha*m), phi = (1-e^-k)/k,
 //     p1 = 2c/(b + k).
 // Not isothermal: adaptive Dormand-Prince 5(4) in FP64 over (lambda, ie).
+//
+// Recombination photons (onTheSpot = false): the case-A rate drives lambda
+// and the recombination photons per H, d(yGrecHII)/ds = tau*alpha_AB*ye*x_HII
+// (solve.c:83-86, alpha_AB = fdim(alpha_A, alpha_B)), are integrated beside
+// it. Nothing depends on them, so the integrators carry them as a
+// quadrature over the same stages (REC template flag), outside the error
+// control; the isothermal closed form integrates them exactly:
+//     int_0^1 lambda ds = p1 + y0*phi(k)*L(z),  z = a*y0*phi(k),
+//     L(z) = -log(1-z)/z,
+//     int_0^1 lambda^2 ds = (lambda(1) - lambda0 + b*int lambda - c)/a
+// (the Riccati equation itself, a*lambda^2 = lambda' + b*lambda - c).
 #pragma once
 
 #include "psg_internal.cuh"
 
 struct PhysParams {
 	const double *ar;      // [ar_nrows][16]: log T, then the PSG_AR_* columns
-	const float4 *ar_ni;   // [ar_nrows][4]: the right-hand side's 7 rates, values and slopes
-	double ar_ni_scale[7]; // ... each column divided by its largest magnitude
+	const float4 *ar_ni;   // [ar_nrows][4]: the right-hand side's 7 rates (+ alpha_B when not
+	                       // on the spot), values and slopes
+	double ar_ni_scale[8]; // ... each column divided by its largest magnitude
 	int ar_nrows;
 	double ar_min, ar_step_inv, ar_step;
 	const double *xs;      // [2][xs_nrows]: energy, sigma_HI
@@ -33,6 +45,7 @@ struct PhysParams {
 	double H_PER_MASS, HI_ENERGY, MPROTON_OVER_BOLTZMANN, BOLTZMANN_OVER_MPROTON, hmf, hemf;
 	double he_e;           // helium electrons per H, helium frozen (psystem.h:134-137)
 	int isothermal, on_the_spot, adiabatic, euler;
+	float *ygrec;          // yGrecHII per particle (leaf order), when not on the spot
 };
 
 PhysParams psg_phys_params(const psg_context *ctx);
@@ -117,18 +130,37 @@ __device__ __forceinline__ double phi_k(double k) {
 	return 1.0 - k * (0.5 - k / 6.0);
 }
 
-__device__ __forceinline__ double riccati_step(double lam0, double a, double b, double q, double c, double g) {
+// lambda(1); with I1 != NULL also int_0^1 lambda ds.
+__device__ __forceinline__ double riccati_step(double lam0, double a, double b, double q, double c, double g,
+		double *I1 = nullptr) {
 	if (!(a > 0.0)) {
 		if (b > 0.0) {
 			const double eq = c / b;
+			if (I1) *I1 = eq + (lam0 - eq) * phi_k(b);
 			return eq + (lam0 - eq) * exp(-b);
 		}
+		if (I1) *I1 = lam0 + 0.5 * c;
 		return lam0 + c;
 	}
 	const double k = sqrt(q * q + 4.0 * a * g);
 	const double p1 = 2.0 * c / (b + k);
 	const double y0 = lam0 - p1;
-	return p1 + y0 * exp(-k) / (1.0 - a * y0 * phi_k(k));
+	const double ph = phi_k(k);
+	if (I1) {
+		const double z = a * y0 * ph;
+		const double L = fabs(z) < 1e-4 ? 1.0 + z * (0.5 + z * (1.0 / 3.0 + 0.25 * z)) : -log1p(-z) / z;
+		*I1 = p1 + y0 * ph * L;
+	}
+	return p1 + y0 * exp(-k) / (1.0 - a * y0 * ph);
+}
+
+// Recombination photons per H of one isothermal step: tau*alpha_AB times
+// int_0^1 ye*x_HII ds, ye*x_HII = (1+m-lambda)(1-lambda), from the closed
+// form's integrals (ar = alpha_AB/(alpha+gamma), the step's tau cancels).
+__device__ __forceinline__ double riccati_rec(double lam0, double lam1, double I1, double a, double b, double c,
+		double m, double tau_ab, double ar) {
+	if (!(a > 0.0)) return 0.0;
+	return tau_ab * ((1.0 + m) - (2.0 + m) * I1) + ar * (lam1 - lam0 + b * I1 - c);
 }
 
 struct RhsCtx {
@@ -154,7 +186,10 @@ __device__ __forceinline__ RhsCtx make_rhs_ctx(const PhysParams &P, double yeMET
 // isothermal): the same equations with the step length folded into the
 // rates, and fused multiply-adds (the last bits of an integrator's stage do
 // not matter; the isothermal closed form keeps the reference's roundings).
-__device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const double x[2], double dx[2]) {
+// With REC, *rec receives d(yGrecHII)/ds.
+template <bool REC = false>
+__device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const double x[2], double dx[2],
+		double *rec = nullptr) {
 	const double xHI = x[0], xHII = 1.0 - x[0];
 	const double ye = xHII + P.he_e + cx.yeMET;
 	const double T = P.isothermal ? cx.T : cx.T_num * x[1] / __fma_rn(P.hmf, ye, cx.T_den0);
@@ -177,6 +212,10 @@ __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const
 	const double gamma = PSG_LIN(v0.x, s0.x, 0) * cx.nHt;
 	const double alpha = PSG_LIN(v0.y, s0.y, 1) * cx.nHt;       // case B on the spot, else A
 	dx[0] = __fma_rn(ye, __fma_rn(alpha, xHII, -gamma * xHI), -cx.g);
+	if (REC) {
+		const double alphaB = PSG_LIN(v1.w, s1.w, 7) * cx.nHt;
+		*rec = fdim(alpha, alphaB) * ye * xHII;
+	}
 	if (P.isothermal || P.adiabatic) {
 		dx[1] = 0.0;
 	} else {
@@ -196,6 +235,7 @@ __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const
 // against atol/rtol), dp_step() attempts one step.
 struct DPState {
 	double x[2], k1[2];
+	double rec, krec;   // REC: yGrecHII gained so far, and its derivative at x
 	double t, h;
 	float hnext;     // proposal for a step beyond s = 1 (the interval end truncates h)
 	int steps;
@@ -220,8 +260,10 @@ __device__ __forceinline__ void dp_init_k1(DPState &S) {
 	S.hnext = 0.0f;
 }
 
+template <bool REC = false>
 __device__ __forceinline__ void dp_init(const PhysParams &P, const RhsCtx &cx, DPState &S) {
-	rhs(P, cx, S.x, S.k1);
+	S.rec = 0.0;
+	rhs<REC>(P, cx, S.x, S.k1, &S.krec);
 	S.t = 0.0;
 	S.steps = 0;
 	double h = 1.0;
@@ -236,6 +278,7 @@ __device__ __forceinline__ void dp_init(const PhysParams &P, const RhsCtx &cx, D
 }
 
 // One attempted step; returns true once s = 1 is reached.
+template <bool REC = false>
 __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, DPState &S, double atol1) {
 	const double a21 = 1. / 5, a31 = 3. / 40, a32 = 9. / 40, a41 = 44. / 45, a42 = -56. / 15, a43 = 32. / 9;
 	const double a51 = 19372. / 6561, a52 = -25360. / 2187, a53 = 64448. / 6561, a54 = -212. / 729;
@@ -246,21 +289,22 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 	const bool cut = S.t + h > 1.0;
 	if (cut) h = 1.0 - S.t;
 	double k2[2], k3[2], k4[2], k5[2], k6[2], k7[2], y[2], yn[2];
+	double r2 = 0.0, r3 = 0.0, r4 = 0.0, r5 = 0.0, r6 = 0.0, r7 = 0.0;
 	const double *x = S.x, *k1 = S.k1;
 #define F __fma_rn
 	for (int i = 0; i < 2; i++) y[i] = F(h, a21 * k1[i], x[i]);
-	rhs(P, cx, y, k2);
+	rhs<REC>(P, cx, y, k2, &r2);
 	for (int i = 0; i < 2; i++) y[i] = F(h, F(a32, k2[i], a31 * k1[i]), x[i]);
-	rhs(P, cx, y, k3);
+	rhs<REC>(P, cx, y, k3, &r3);
 	for (int i = 0; i < 2; i++) y[i] = F(h, F(a43, k3[i], F(a42, k2[i], a41 * k1[i])), x[i]);
-	rhs(P, cx, y, k4);
+	rhs<REC>(P, cx, y, k4, &r4);
 	for (int i = 0; i < 2; i++) y[i] = F(h, F(a54, k4[i], F(a53, k3[i], F(a52, k2[i], a51 * k1[i]))), x[i]);
-	rhs(P, cx, y, k5);
+	rhs<REC>(P, cx, y, k5, &r5);
 	for (int i = 0; i < 2; i++)
 		y[i] = F(h, F(a65, k5[i], F(a64, k4[i], F(a63, k3[i], F(a62, k2[i], a61 * k1[i])))), x[i]);
-	rhs(P, cx, y, k6);
+	rhs<REC>(P, cx, y, k6, &r6);
 	for (int i = 0; i < 2; i++) yn[i] = F(h, F(b6, k6[i], F(b5, k5[i], F(b4, k4[i], F(b3, k3[i], b1 * k1[i])))), x[i]);
-	rhs(P, cx, yn, k7);
+	rhs<REC>(P, cx, yn, k7, &r7);
 	double err = 0.0;
 	for (int i = 0; i < 2; i++) {
 		const double e = h * F(e7, k7[i], F(e6, k6[i], F(e5, k5[i], F(e4, k4[i], F(e3, k3[i], e1 * k1[i])))));
@@ -273,6 +317,10 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 		S.t += h;
 		S.x[0] = yn[0]; S.x[1] = yn[1];
 		S.k1[0] = k7[0]; S.k1[1] = k7[1];
+		if (REC) {
+			S.rec = __fma_rn(h, __fma_rn(b6, r6, __fma_rn(b5, r5, __fma_rn(b4, r4, __fma_rn(b3, r3, b1 * S.krec)))), S.rec);
+			S.krec = r7;
+		}
 	}
 	// step-size control needs no double precision
 	const float fac = err > 0.0 ? fminf(5.0f, fmaxf(0.2f, 0.9f * __powf((float)err, -0.2f))) : 5.0f;
@@ -290,25 +338,30 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 #define DP_SWITCH 32
 #define RB_RTOL 1e-5
 
+// With REC, *rec accumulates yGrecHII: the third component of the augmented
+// system, whose Jacobian column is zero, so W's last row only adds
+// h*d*(J20*k0 + J21*k1) to its stage values; it stays out of the error norm.
+template <bool REC = false>
 __device__ inline bool rosenbrock(const PhysParams &P, const RhsCtx &cx, double x[2], double t, double h,
-		int max_steps) {
+		int max_steps, double *rec = nullptr) {
 	const double d = 1.0 / (2.0 + 1.4142135623730951), e32 = 6.0 + 1.4142135623730951;
 	const double atol[2] = {DP_ATOL0, DP_ATOL1_REL * fabs(x[1]) + 1e-300};
-	double F0[2];
-	rhs(P, cx, x, F0);
+	double F0[2], R0 = 0.0;
+	rhs<REC>(P, cx, x, F0, &R0);
 	h = fmin(fmax(h, 1e-10), 1.0);
 	for (int it = 0; it < max_steps; it++) {
 		if (t >= 1.0) return true;
 		if (t + h > 1.0) h = 1.0 - t;
 		// Jacobian by forward differences
-		double J[2][2];
+		double J[2][2], JR[2] = {0.0, 0.0};
 		for (int j = 0; j < 2; j++) {
 			const double del = 1e-7 * fmax(fabs(x[j]), atol[j] / RB_RTOL);
-			double y[2] = {x[0], x[1]}, Fj[2];
+			double y[2] = {x[0], x[1]}, Fj[2], Rj = 0.0;
 			y[j] += del;
-			rhs(P, cx, y, Fj);
+			rhs<REC>(P, cx, y, Fj, &Rj);
 			J[0][j] = (Fj[0] - F0[0]) / del;
 			J[1][j] = (Fj[1] - F0[1]) / del;
+			if (REC) JR[j] = (Rj - R0) / del;
 		}
 		const double a00 = 1.0 - h * d * J[0][0], a01 = -h * d * J[0][1];
 		const double a10 = -h * d * J[1][0], a11 = 1.0 - h * d * J[1][1];
@@ -317,19 +370,21 @@ __device__ inline bool rosenbrock(const PhysParams &P, const RhsCtx &cx, double 
 			out[0] = (a11 * b[0] - a01 * b[1]) / det;
 			out[1] = (a00 * b[1] - a10 * b[0]) / det;
 		};
-		double k1[2], k2[2], k3[2], F1[2], F2[2], y[2], yn[2], b[2];
+		double k1[2], k2[2], k3[2], F1[2], F2[2], y[2], yn[2], b[2], R1 = 0.0, R2 = 0.0;
 		solve(F0, k1);
+		const double kr1 = REC ? R0 + h * d * (JR[0] * k1[0] + JR[1] * k1[1]) : 0.0;
 		y[0] = x[0] + 0.5 * h * k1[0];
 		y[1] = x[1] + 0.5 * h * k1[1];
-		rhs(P, cx, y, F1);
+		rhs<REC>(P, cx, y, F1, &R1);
 		b[0] = F1[0] - k1[0];
 		b[1] = F1[1] - k1[1];
 		solve(b, k2);
+		const double kr2 = REC ? (R1 - kr1) + h * d * (JR[0] * k2[0] + JR[1] * k2[1]) + kr1 : 0.0;
 		k2[0] += k1[0];
 		k2[1] += k1[1];
 		yn[0] = x[0] + h * k2[0];
 		yn[1] = x[1] + h * k2[1];
-		rhs(P, cx, yn, F2);
+		rhs<REC>(P, cx, yn, F2, &R2);
 		b[0] = F2[0] - e32 * (k2[0] - F1[0]) - 2.0 * (k1[0] - F0[0]);
 		b[1] = F2[1] - e32 * (k2[1] - F1[1]) - 2.0 * (k1[1] - F0[1]);
 		solve(b, k3);
@@ -346,6 +401,10 @@ __device__ inline bool rosenbrock(const PhysParams &P, const RhsCtx &cx, double 
 			x[1] = yn[1];
 			F0[0] = F2[0];
 			F0[1] = F2[1];
+			if (REC) {
+				*rec += h * kr2;
+				R0 = R2;
+			}
 		}
 		const float fac = (err > 0.0 && isfinite(err))
 				? fminf(5.0f, fmaxf(0.2f, 0.9f * __powf((float)err, -1.0f / 3.0f))) : (isfinite(err) ? 5.0f : 0.2f);
@@ -354,19 +413,23 @@ __device__ inline bool rosenbrock(const PhysParams &P, const RhsCtx &cx, double 
 	return t >= 1.0;
 }
 
-// Whole integration on one thread; returns false if the step limit is reached.
-__device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2], int max_steps) {
+// Whole integration on one thread; returns false if the step limit is
+// reached. With REC, *rec receives the yGrecHII gained.
+template <bool REC = false>
+__device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2], int max_steps,
+		double *rec = nullptr) {
 	DPState S;
 	S.x[0] = x[0];
 	S.x[1] = x[1];
 	const double atol1 = DP_ATOL1_REL * fabs(x[1]) + 1e-300;
-	dp_init(P, cx, S);
+	dp_init<REC>(P, cx, S);
 	bool done = false;
-	while (!done && S.steps < DP_SWITCH) done = dp_step(P, cx, S, atol1);
+	while (!done && S.steps < DP_SWITCH) done = dp_step<REC>(P, cx, S, atol1);
 	x[0] = S.x[0];
 	x[1] = S.x[1];
+	if (REC) *rec = S.rec;
 	if (done) return true;
-	return rosenbrock(P, cx, x, S.t, S.h, max_steps);
+	return rosenbrock<REC>(P, cx, x, S.t, S.h, max_steps, rec);
 }
 
 // step_evolve_euler() solve.c:225-316, hydrogen only: nsteps explicit Euler
@@ -375,8 +438,10 @@ __device__ inline bool dopri(const PhysParams &P, const RhsCtx &cx, double x[2],
 // FETCH_VARS, solve.c:42-73), at most 10000 steps; the walk stops one step
 // after lambdaH leaves [0, 1] and reports the unused fraction of the step
 // (step_remain = 1 - (float)k / nsteps). Returns PSG_ST_* bits.
+// With REC, *rec receives the yGrecHII gained (solve.c:256-300, x[3]).
+template <bool REC = false>
 __device__ inline uint32_t euler_step(const PhysParams &P, const RhsCtx &cx, double x[2], double &step_remain,
-		int &refined) {
+		int &refined, double *rec = nullptr) {
 	const double ye = (1.0 - x[0]) + P.he_e + cx.yeMET;
 	const double T = P.isothermal ? cx.T : ieye2T(P, x[1], ye);
 	const RateAt R = rates_at(P, log10(T));
@@ -391,12 +456,14 @@ __device__ inline uint32_t euler_step(const PhysParams &P, const RhsCtx &cx, dou
 	refined = nsteps > 1;
 	uint32_t st = 0;
 	int k;
+	double acc = 0.0;
 	for (k = 0; k < nsteps; k++) {
-		double dx[2];
-		rhs(P, cx, x, dx);
+		double dx[2], r = 0.0;
+		rhs<REC>(P, cx, x, dx, &r);
 		if (!(x[1] + dx[1] >= 0.0)) st |= PSG_ST_IE_NEG;      // function()'s check, solve.c:137-139
 		x[0] += dx[0] * h;
 		x[1] += dx[1] * h;
+		if (REC) acc += r * h;
 		if (!isfinite(x[0]) || !isfinite(x[1])) {
 			st |= PSG_ST_NAN;
 			k++;
@@ -408,12 +475,14 @@ __device__ inline uint32_t euler_step(const PhysParams &P, const RhsCtx &cx, dou
 		}
 	}
 	step_remain = 1.0 - (double)((float)k / (float)nsteps);
+	if (REC) *rec = acc;
 	return st;
 }
 
-// Isothermal step only (the closed form), for the kernels specialised on it.
+// Isothermal step only (the closed form), for the kernels specialised on
+// it. Not on the spot, *grec (if not NULL) receives the yGrecHII gained.
 __device__ inline uint32_t solve_step_iso(const PhysParams &P, double &lambdaH, double yeMET, double g,
-		double time, double nH, double T) {
+		double time, double nH, double T, double *grec = nullptr) {
 	const RateAt R = rates_at(P, log10(T));
 	const double gamma = R(PSG_AR_HI_CI) * nH;
 	const double alpha = R(P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A) * nH;
@@ -422,31 +491,37 @@ __device__ inline uint32_t solve_step_iso(const PhysParams &P, double &lambdaH, 
 	const double b = time * (alpha + (alpha + gamma) * (1.0 + m));
 	const double q = time * (gamma * (1.0 + m) + alpha * m);
 	const double c = time * alpha * (1.0 + m) - g;
-	lambdaH = riccati_step(lambdaH, a, b, q, c, g);
-	const uint32_t st = isfinite(lambdaH) ? 0u : PSG_ST_NAN;
+	const double lam0 = lambdaH;
+	if (grec && !P.on_the_spot) {
+		double I1 = 0.0;
+		lambdaH = riccati_step(lam0, a, b, q, c, g, &I1);
+		const double alpha_ab = fdim(alpha, R(PSG_AR_HII_RC_B) * nH);
+		*grec = riccati_rec(lam0, lambdaH, I1, a, b, c, m, time * alpha_ab,
+				alpha + gamma > 0.0 ? alpha_ab / (alpha + gamma) : 0.0);
+	} else {
+		lambdaH = riccati_step(lam0, a, b, q, c, g);
+	}
+	uint32_t st = isfinite(lambdaH) ? 0u : PSG_ST_NAN;
+	if (grec && !isfinite(*grec)) st |= PSG_ST_NAN;
 	lambdaH = fmin(1.0, fmax(0.0, lambdaH));
 	return st;
 }
 
-// One particle step. lambdaH is clamped to [0,1] as solve.c:208 does.
-// Returns a PSG_ST_* bit on trouble, 0 otherwise.
+// One particle step. lambdaH is clamped to [0,1] as solve.c:208 does. Not
+// on the spot, *grec (if not NULL) receives the yGrecHII gained. Returns a
+// PSG_ST_* bit on trouble, 0 otherwise.
 __device__ inline uint32_t solve_step(const PhysParams &P, double &lambdaH, double &ie, double yeMET,
-		double g, double heat, double time, double nH, double T) {
+		double g, double heat, double time, double nH, double T, double *grec = nullptr) {
 	uint32_t st = 0;
 	if (P.isothermal) {
-		const double logT = log10(T);
-		const double gamma = ar_get(P, PSG_AR_HI_CI, logT) * nH;
-		const double alpha = ar_get(P, P.on_the_spot ? PSG_AR_HII_RC_B : PSG_AR_HII_RC_A, logT) * nH;
-		const double m = yeMET + P.he_e;
-		const double a = time * (alpha + gamma);
-		const double b = time * (alpha + (alpha + gamma) * (1.0 + m));
-		const double q = time * (gamma * (1.0 + m) + alpha * m);
-		const double c = time * alpha * (1.0 + m) - g;
-		lambdaH = riccati_step(lambdaH, a, b, q, c, g);
+		st = solve_step_iso(P, lambdaH, yeMET, g, time, nH, T, grec);
 	} else {
 		RhsCtx cx = make_rhs_ctx(P, yeMET, g, heat, time, nH, T);
 		double x[2] = {lambdaH, ie};
-		if (!dopri(P, cx, x, 200000)) st |= PSG_ST_SOLVER;
+		double r = 0.0;
+		const bool ok = (grec && !P.on_the_spot) ? dopri<true>(P, cx, x, 200000, &r) : dopri<false>(P, cx, x, 200000);
+		if (!ok) st |= PSG_ST_SOLVER;
+		if (grec) *grec = r;
 		lambdaH = x[0];
 		ie = x[1];
 		if (!(ie >= 0.0)) st |= PSG_ST_IE_NEG;

@@ -29,7 +29,7 @@ PhysParams psg_phys_params(const psg_context *ctx) {
 	PhysParams P{};
 	P.ar = ctx->d_ar;
 	P.ar_ni = ctx->d_ar_ni;
-	for (int c = 0; c < 7; c++) P.ar_ni_scale[c] = ctx->ar_ni_scale[c];
+	for (int c = 0; c < 8; c++) P.ar_ni_scale[c] = ctx->ar_ni_scale[c];
 	P.ar_step = ctx->ar_step;
 	P.ar_nrows = ctx->ar_nrows;
 	P.ar_min = ctx->ar_min;
@@ -53,6 +53,7 @@ PhysParams psg_phys_params(const psg_context *ctx) {
 	P.on_the_spot = ctx->flags.on_the_spot;
 	P.adiabatic = ctx->flags.adiabatic;
 	P.euler = ctx->flags.euler;
+	P.ygrec = ctx->flags.on_the_spot ? nullptr : ctx->d_ygrec;
 	return P;
 }
 
@@ -364,18 +365,20 @@ __global__ void k_tick_long(int K, const int32_t *__restrict__ tick_act, const i
 
 // One active particle's non-isothermal update, prepared by k_reduce<false>
 // so that the integrator reads one contiguous record instead of gathering
-// the particle's state: the inputs of the step and f(x0). 80 bytes, a
-// multiple of 16 for cp.async.
+// the particle's state: the inputs of the step and f(x0) (with the
+// recombination photons' rate when not on the spot). 80 bytes, a multiple
+// of 16 for cp.async.
 struct __align__(16) UpdRec {
 	double time, lam0, g, heat, k0, k1;
 	float ie0, rho, yeMET, hstep;
-	uint32_t p, pad0, pad1, pad2;
+	uint32_t p, pad0;
+	double krec;
 };
 static_assert(sizeof(UpdRec) == 80, "UpdRec layout");
 
 // The particle's summed deposits of the tick: isothermal, the closed-form
 // update_pars() step (loop.c:653-770); otherwise the sums for the integrator.
-template <bool ISO>
+template <bool ISO, bool REC>
 __device__ __forceinline__ void finish_particle(int a, double g, double heat, int nh,
 		const uint32_t *__restrict__ act_ipar, int32_t *__restrict__ hits, double *__restrict__ act_g,
 		double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
@@ -398,13 +401,14 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 		r.yeMET = yeMET[p];
 		r.hstep = hstep[p];
 		r.p = p;
-		r.pad0 = r.pad1 = r.pad2 = 0u;
+		r.pad0 = 0u;
+		r.krec = 0.0;
 		const double ie0 = (double)r.ie0;
 		const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, r.lam0), P.he_e));
 		const RhsCtx cx = make_rhs_ctx(P, (double)r.yeMET, g, heat, r.time, rn_dmul(P.H_PER_MASS, (double)r.rho), T);
 		const double x0[2] = {r.lam0, ie0};
 		double f0[2];
-		rhs(P, cx, x0, f0);
+		rhs<REC>(P, cx, x0, f0, &r.krec);
 		r.k0 = f0[0];
 		r.k1 = f0[1];
 		rec[a - lo] = r;    // records of one tick, from its first active particle
@@ -414,9 +418,10 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 	const double lam0 = lambdaH[p];
 	const double T = ieye2T(P, (double)ie[p], rn_dadd(rn_dsub(1.0, lam0), P.he_e));
 	const double nH = rn_dmul(P.H_PER_MASS, (double)rho[p]);
-	double lam = lam0;
-	const uint32_t st = solve_step_iso(P, lam, (double)yeMET[p], g, time, nH, T);
+	double lam = lam0, grec = 0.0;
+	const uint32_t st = solve_step_iso(P, lam, (double)yeMET[p], g, time, nH, T, REC ? &grec : nullptr);
 	lambdaH[p] = lam;
+	if (REC) P.ygrec[p] = (float)((double)P.ygrec[p] + grec);     // x[3], solve.c:183,218
 	ie[p] = (float)Tye2ie(P, T, rn_dadd(rn_dsub(1.0, lam), P.he_e));
 	lasthit[p] = tick;
 	if (st) atomicOr(status, st);
@@ -428,7 +433,7 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 // lane), then a fixed butterfly. The other blocks take the short ones, a
 // thread each. Particles are in leaf order, so the long ones are neighbours;
 // giving each its own warp keeps them from piling up on a few warps.
-template <bool ISO>
+template <bool ISO, bool REC>
 __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
 		const double *__restrict__ acc, const double *__restrict__ acc_heat, int want_heat,
@@ -466,7 +471,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 			sn += __shfl_xor_sync(0xffffffffu, sn, o);
 		}
 		if (lane == 0)
-			finish_particle<ISO>(a, sg, sh, sn, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
+			finish_particle<ISO, REC>(a, sg, sh, sn, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
 					hstep, rec, tick_act[t], gcarry, P, tick, tick_time, status);
 		return;
 	}
@@ -480,7 +485,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		const double d = acc[k];
 		if (d >= 0.0) { g += d; if (want_heat) heat += acc_heat[k]; nh++; }
 	}
-	finish_particle<ISO>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET, hstep,
+	finish_particle<ISO, REC>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET, hstep,
 			rec, tick_act[t], gcarry, P, tick, tick_time, status);
 }
 
@@ -490,7 +495,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 // all lanes on integrator steps (particles need 1 to a few hundred steps).
 #define UPD_MAX_STEPS 200000
 struct StiffItem {
-	double t, h, x0, x1, yeMET, g, heat, time, nH, T;
+	double t, h, x0, x1, yeMET, g, heat, time, nH, T, rec;
 	uint32_t p;
 };
 __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
@@ -507,6 +512,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // chunks of 32 particles from the tick's cursor and copies their records
 // with cp.async one chunk ahead, so a lane whose particle is done takes the
 // next one from shared memory without waiting on a gather.
+template <bool REC>
 __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const int32_t *__restrict__ tick_act,
 		const UpdRec *__restrict__ rec, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, float *__restrict__ hstep, PhysParams P, int64_t tick,
@@ -576,6 +582,8 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 				S.x[1] = ie0;
 				S.k1[0] = r.k0;
 				S.k1[1] = r.k1;
+				S.rec = 0.0;
+				S.krec = r.krec;
 				atol1 = DP_ATOL1_REL * fabs(ie0) + 1e-300;
 				dp_init_k1(S);
 				// the particle's last step proposal is a better first
@@ -588,13 +596,14 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 		}
 		if (!__any_sync(0xffffffffu, have)) break;
 		if (have) {
-			const bool done = dp_step(P, cx, S, atol1);
+			const bool done = dp_step<REC>(P, cx, S, atol1);
 			if (!done && S.steps >= DP_SWITCH) {
 				// stiff: hand the particle to k_update_stiff and free the lane
 				const unsigned q = atomicAdd(nstiff, 1u);
 				StiffItem it;
 				it.p = p; it.t = S.t; it.h = S.h; it.x0 = S.x[0]; it.x1 = S.x[1];
 				it.yeMET = cx.yeMET; it.g = cx.g; it.heat = cx.heat; it.time = cx.time; it.nH = cx.nH; it.T = cx.T;
+				it.rec = S.rec;
 				stiff[q] = it;
 				hstep[p] = 0.0f;
 				have = false;
@@ -604,6 +613,7 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 				if (!isfinite(lam) || !isfinite(e)) st |= PSG_ST_NAN;
 				lambdaH[p] = fmin(1.0, fmax(0.0, lam));
 				if (!P.adiabatic) ie[p] = (float)e;
+				if (REC) P.ygrec[p] = (float)((double)P.ygrec[p] + S.rec);
 				lasthit[p] = tick;
 				hstep[p] = (float)((double)S.hnext * cx.time);
 				have = false;
@@ -616,6 +626,7 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 
 // The stiff particles of a tick, one thread each (their number is read on
 // the device): Rosenbrock from where the explicit steps stopped.
+template <bool REC>
 __global__ void __launch_bounds__(64) k_update_stiff(const StiffItem *__restrict__ stiff,
 		const unsigned *__restrict__ nstiff, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, PhysParams P, int64_t tick, uint32_t *__restrict__ status) {
@@ -625,7 +636,9 @@ __global__ void __launch_bounds__(64) k_update_stiff(const StiffItem *__restrict
 		const StiffItem it = stiff[i];
 		const RhsCtx cx = make_rhs_ctx(P, it.yeMET, it.g, it.heat, it.time, it.nH, it.T);
 		double x[2] = {it.x0, it.x1};
-		if (!rosenbrock(P, cx, x, it.t, it.h, UPD_MAX_STEPS)) st |= PSG_ST_SOLVER;
+		double rec = it.rec;
+		if (!rosenbrock<REC>(P, cx, x, it.t, it.h, UPD_MAX_STEPS, &rec)) st |= PSG_ST_SOLVER;
+		if (REC) P.ygrec[it.p] = (float)((double)P.ygrec[it.p] + rec);
 		if (!(x[1] >= 0.0)) st |= PSG_ST_IE_NEG;
 		if (!isfinite(x[0]) || !isfinite(x[1])) st |= PSG_ST_NAN;
 		lambdaH[it.p] = fmin(1.0, fmax(0.0, x[0]));
@@ -650,9 +663,10 @@ __global__ void __launch_bounds__(128) k_update_euler(int t, const int32_t *__re
 	const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, r.lam0), P.he_e));
 	const RhsCtx cx = make_rhs_ctx(P, (double)r.yeMET, r.g, r.heat, r.time, rn_dmul(P.H_PER_MASS, (double)r.rho), T);
 	double x[2] = {r.lam0, ie0};
-	double remain = 0.0;
+	double remain = 0.0, grec = 0.0;
 	int refined = 0;
-	uint32_t st = euler_step(P, cx, x, remain, refined);
+	uint32_t st = P.ygrec ? euler_step<true>(P, cx, x, remain, refined, &grec) : euler_step<false>(P, cx, x, remain, refined);
+	if (P.ygrec) P.ygrec[r.p] = (float)((double)P.ygrec[r.p] + grec);
 	const double lam = fmin(1.0, fmax(0.0, x[0]));
 	lambdaH[r.p] = lam;
 	if (P.isothermal) ie[r.p] = (float)Tye2ie(P, T, rn_dadd(rn_dsub(1.0, lam), P.he_e));
@@ -714,21 +728,24 @@ __global__ void k_step_evolve(psg_step *steps, size_t n, PhysParams P, uint32_t 
 		// unused fraction of the step and whether it was subdivided
 		const RhsCtx cx = make_rhs_ctx(P, s.yeMET, s.yGdepHI, s.heat, s.time, s.nH, s.T);
 		double x[2] = {s.lambdaH, s.ie};
-		double remain = 0.0;
+		double remain = 0.0, grec = 0.0;
 		int refined = 0;
-		const uint32_t st = euler_step(P, cx, x, remain, refined);
+		const uint32_t st = P.on_the_spot ? euler_step<false>(P, cx, x, remain, refined)
+			: euler_step<true>(P, cx, x, remain, refined, &grec);
 		s.lambdaH = x[0];
 		s.ie = x[1];
+		s.yGrecHII += grec;
 		s.step_remain = remain;
 		s.refined = refined;
 		steps[i] = s;
 		if (st) atomicOr(status, st);
 		return;
 	}
-	double lam = s.lambdaH, e = s.ie;
-	const uint32_t st = solve_step(P, lam, e, s.yeMET, s.yGdepHI, s.heat, s.time, s.nH, s.T);
+	double lam = s.lambdaH, e = s.ie, grec = 0.0;
+	const uint32_t st = solve_step(P, lam, e, s.yeMET, s.yGdepHI, s.heat, s.time, s.nH, s.T, &grec);
 	s.lambdaH = lam;
 	s.ie = e;
+	s.yGrecHII += grec;      // x[3] of solve.c:183,218; unchanged on the spot
 	s.step_remain = 0.0;
 	steps[i] = s;
 	if (st) atomicOr(status, st);
@@ -806,7 +823,9 @@ static int build_slots(psg_context *ctx, size_t nray, size_t R, size_t K, size_t
 	return PSG_OK;
 }
 
-extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K,
+// One batch of K ticks of R rays each, rays already traced together: the
+// path on the spot (and the per-tick step of the recombination loop).
+int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K,
 		int64_t first_tick, double tick_time, psg_tick_stats *stats) {
 	if (!ctx) return PSG_E_INVAL;
 	if (!ctx->have_physics || !ctx->have_tree)
@@ -897,7 +916,8 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 	size_t maxt = 1;
 	for (size_t t = 0; t < K; t++) maxt = std::max<size_t>(maxt, (size_t)(h_tick_act[t + 1] - h_tick_act[t]));
 	const bool euler = ctx->flags.euler != 0;
-	const bool surr = !iso && !euler && ctx->surr_on && !ctx->flags.adiabatic;
+	// (the network does not model the recombination photons: on the spot only)
+	const bool surr = !iso && !euler && ctx->surr_on && !ctx->flags.adiabatic && ctx->flags.on_the_spot;
 	char *um = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * 3 * (K + 1)
 			+ (iso ? 0 : sizeof(StiffItem) * maxt) + (surr ? sizeof(uint32_t) * maxt : 0) + 512);
 	int32_t *aflag = (int32_t *)psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (3 * (na + 1) + K + 1) + 512);
@@ -964,16 +984,19 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 			const int lb = (nl + 7) / 8;
 			const unsigned rgrid = (unsigned)(lb + (int)blocks(nact_t, 256));
 			const double *gcarry = euler ? ctx->d_gcarry : nullptr;
-			if (iso && !euler)
-				k_reduce<true><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat,
-						long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,
-						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, tick, tick_time,
-						ctx->d_status);
-			else
-				k_reduce<false><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat,
-						long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,
-						ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, tick, tick_time,
-						ctx->d_status);
+#define PSG_REDUCE(ISO_, REC_)                                                                              \
+	k_reduce<ISO_, REC_><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat, \
+			long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,        \
+			ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, tick, tick_time,          \
+			ctx->d_status)
+			if (iso && !euler) {
+				if (P.ygrec) PSG_REDUCE(true, true);
+				else PSG_REDUCE(true, false);
+			} else {
+				if (P.ygrec) PSG_REDUCE(false, true);
+				else PSG_REDUCE(false, false);
+			}
+#undef PSG_REDUCE
 			PSG_CHECK_LAUNCH();
 			ctx->launches++;
 			if (euler) {
@@ -995,12 +1018,21 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 					if (rc) return rc;
 					ctx->launches++;
 				}
-				k_update_queue<<<qgrid, 32 * UPD_WARPS, 0, st>>>((int)t, tick_act, urec, ctx->d_lambdaH, ctx->d_ie,
-						ctx->d_lasthit, ctx->d_hstep, P, tick, cursors + t, stiff, nstiff + t, surr ? rej : nullptr,
-						surr ? nrej + t : nullptr, ctx->d_status);
-				PSG_CHECK_LAUNCH();
-				k_update_stiff<<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
-						P, tick, ctx->d_status);
+				if (P.ygrec) {
+					k_update_queue<true><<<qgrid, 32 * UPD_WARPS, 0, st>>>((int)t, tick_act, urec, ctx->d_lambdaH,
+							ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, tick, cursors + t, stiff, nstiff + t, nullptr,
+							nullptr, ctx->d_status);
+					PSG_CHECK_LAUNCH();
+					k_update_stiff<true><<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie,
+							ctx->d_lasthit, P, tick, ctx->d_status);
+				} else {
+					k_update_queue<false><<<qgrid, 32 * UPD_WARPS, 0, st>>>((int)t, tick_act, urec, ctx->d_lambdaH,
+							ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, tick, cursors + t, stiff, nstiff + t,
+							surr ? rej : nullptr, surr ? nrej + t : nullptr, ctx->d_status);
+					PSG_CHECK_LAUNCH();
+					k_update_stiff<false><<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie,
+							ctx->d_lasthit, P, tick, ctx->d_status);
+				}
 				PSG_CHECK_LAUNCH();
 				ctx->launches += 2;
 				if (feat) {
@@ -1033,6 +1065,7 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 		stats->tick_ms = tick_ms;
 		stats->launches = (double)ctx->launches;
 		stats->surrogate_accepted = 0.0;
+		stats->rec_rays = stats->rec_photons = 0.0;
 		if (surr) {
 			unsigned long long acc_n = 0;
 			PSG_CUDA(cudaMemcpyAsync(&acc_n, ctx->d_counters + 8, sizeof(acc_n), cudaMemcpyDeviceToHost, st));
@@ -1048,6 +1081,19 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 		}
 	}
 	return PSG_OK;
+}
+
+extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K,
+		int64_t first_tick, double tick_time, psg_tick_stats *stats) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!ctx->have_physics || !ctx->have_tree)
+		return psg_fail(ctx, PSG_E_INVAL, "psg_run_ticks: set physics, load particles and build the tree first");
+	if (R == 0 || K == 0 || !d_rays) return psg_fail(ctx, PSG_E_INVAL, "psg_run_ticks: empty batch");
+	if (!ctx->flags.on_the_spot) {
+		PSG_CUDA(cudaSetDevice(ctx->device));
+		return psg_run_ticks_rec(ctx, d_rays, R, K, first_tick, tick_time, stats);
+	}
+	return psg_run_ticks_core(ctx, d_rays, R, K, first_tick, tick_time, stats);
 }
 
 extern "C" int psg_run_ticks(psg_context *ctx, const psg_ray *rays, size_t R, size_t K,
