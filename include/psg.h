@@ -111,13 +111,28 @@ typedef struct {
 	int on_the_spot;         /* psphray.onTheSpot; 0: case-A recombination, the photons
 	                            collected in yGrecHII and re-emitted as recombination
 	                            rays (psg_set_recombination) */
-	int h_only;              /* psphray.HOnly (only 1 is supported) */
+	int h_only;              /* psphray.HOnly; 0: helium as well (HeI, HeII, HeIII) */
 	int adiabatic;           /* psphray.adiabatic */
 	int euler;               /* step_evolve_euler() solve.c:225-316 (a build without
 	                            USE_LSODA) instead of the adaptive integrator */
+	int secondary_ionization;   /* psphray.secondaryIonization: the deposit's
+	                            secondary ionisation and heating (loop.c:513-552) */
 } psg_flags;
 
-/* Upload units, tables and flags. Must precede psg_load_particles(). */
+/* secion_init() secion.c:74-98: the secondary-ionisation fractions of
+ * Ricotti, Gnedin & Shull (2002, ApJ 575, 33) -- PhiHI, PhiHeI and the
+ * heating fraction Eh -- tabulated on PSG_SECION_NE energies above
+ * threshold (10 to 200 eV) by PSG_SECION_NX values of log10 x_e (-8 to 0):
+ * out[3][PSG_SECION_NE][PSG_SECION_NX]. Used by psg_set_physics with
+ * secondary_ionization; exposed for tests. */
+#define PSG_SECION_NE 4096
+#define PSG_SECION_NX 1024
+int psg_secion_table_build(const psg_units *u, double *out);
+
+/* Upload units, tables and flags. Must precede psg_load_particles().
+ * Helium (h_only = 0) runs on the spot only (recombination rays of helium
+ * are not emitted), and its ticks use the adaptive integrator (euler = 1
+ * is accepted by psg_step_evolve only). */
 int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_rate_table *ar,
 		const psg_xs_table *xs, const double *kernel, int kernel_n, const psg_flags *flags);
 
@@ -285,6 +300,13 @@ int psg_run_ticks_emit(psg_context *ctx, size_t nray_per_tick, size_t nticks, in
 /* Particle state, caller order. Any pointer may be NULL. */
 int psg_get_state(psg_context *ctx, double *lambdaH, float *ie, int32_t *hits, int64_t *lasthit);
 int psg_set_state(psg_context *ctx, const double *lambdaH, const float *ie, const int64_t *lasthit);
+/* Helium state, caller order: lambdaHeI = x_HeI, lambdaHeII = x_HeII
+ * (psystem.h:35-36) and yeMET (the electrons from metals, after the
+ * hydrogen and helium ones are taken out of the ye block at load,
+ * psystem.c:340-358). With HOnly both fractions stay 0 (x_HeIII = 1), as
+ * in the reference. Any pointer may be NULL. */
+int psg_get_he_state(psg_context *ctx, double *lambdaHeI, double *lambdaHeII, float *yeMET);
+int psg_set_he_state(psg_context *ctx, const double *lambdaHeI, const double *lambdaHeII);
 
 /* ---- solver ---------------------------------------------------------------- */
 typedef struct {
@@ -330,9 +352,10 @@ int psg_snapshot_read_header(const char *filename, psg_snapshot *s);
 int psg_snapshot_read(const char *filename, psg_snapshot *s);
 /* psystem_write_output(): the particle state on the device, in the caller's
  * order, written with meta's constants, ids and sources (meta->ngas must be
- * the particle count; NULL ids write 0..n-1). xHI = lambdaH, ye = x_HII plus
- * the frozen helium electrons (psys_ye() psystem.h:177), xHeI = xHeII = 0
- * and gammaHI = 0 (hydrogen only, on the spot). */
+ * the particle count; NULL ids write 0..n-1). xHI = lambdaH, xHeI and xHeII
+ * the helium fractions, ye = psys_ye() psystem.h:177 (hydrogen and helium
+ * electrons; with HOnly helium counts as fully ionised), gammaHI =
+ * yGrecHII (psystem.c:653). */
 int psg_write_output(psg_context *ctx, const char *filename, const psg_snapshot *meta);
 /* Per-particle deposit counters (psys.hits), caller order; for a resumed run. */
 int psg_set_hits(psg_context *ctx, const int32_t *hits);

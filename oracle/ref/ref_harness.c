@@ -49,9 +49,7 @@ double C_H = 0.72;
 double C_HMF = 0.76;
 double C_HEMF = 0.24;
 Epoch *EPOCHS = NULL;
-/* Table column ids owned by secion.c, which is not linked (its callers are
- * on bypassed paths). lte.c is built in ref_lte.c. */
-int SECION_PHI_HI = -1, SECION_PHI_HEI = -1, SECION_EH = -1;
+/* lte.c is built in ref_lte.c; secion.c is linked from the reference. */
 int N_EPOCHS = 0;
 PSystem psys = {0};
 stat_t stat = {0};
@@ -77,7 +75,6 @@ void stat_stop() { bypassed("stat_stop"); }
 void psystem_write_output(int n) { (void)n; bypassed("psystem_write_output"); }
 void psystem_weight_srcs(double w[]) { (void)w; bypassed("psystem_weight_srcs"); }
 double spec_gen_freq(const int id) { (void)id; bypassed("spec_gen_freq"); return 0; }
-double secion_get(int id, double E, double x) { (void)id; (void)E; (void)x; bypassed("secion_get"); return 0; }
 double eos_get_cloud_fraction(const double d) { (void)d; bypassed("eos_get_cloud_fraction"); return 0; }
 double eos_get_egyhot(const double d) { (void)d; bypassed("eos_get_egyhot"); return 0; }
 
@@ -171,6 +168,14 @@ int ref_load_particles(size_t n, const float *pos, const float *mass,
 		const double xHII = 1.0 - xHI[i];
 		psys_set_lambdaH(i, xHI[i], xHII);
 		double yeMET = fdim(psys.yeMET[i], xHII);
+		if (!CFG_H_ONLY) {      /* psystem.c:350-357 */
+			double xHeII = yeMET * C_HMF / (1 - C_HMF) * 4;
+			double xHeIII = fdim(xHeII, 1.0);
+			xHeII = fmin(1.0, xHeII);
+			xHeIII = fmin(1.0 - xHeII, xHeIII);
+			psys_set_lambdaHe(i, 1.0 - xHeII - xHeIII, xHeII, xHeIII);
+			yeMET = fdim(yeMET, (xHeII + 2 * xHeIII) * (1 - C_HMF) / C_HMF * 0.25);
+		}
 		psys.yeMET[i] = yeMET;
 		psys.id[i] = i;
 	}
@@ -236,6 +241,40 @@ size_t ref_ray_hits(size_t i, int64_t *ipar, double *d, double *b) {
 size_t ref_active_count(void) { return active_set_length; }
 void ref_active(int64_t *out) {
 	for (size_t i = 0; i < active_set_length; i++) out[i] = active_set[i];
+}
+
+/* Secondary ionisation (psphray.secondaryIonization, secion.c): on/off and
+ * its table (secion_init() builds it once). */
+extern void secion_init(void);
+void ref_set_secondary(int on) {
+	static int built = 0;
+	CFG_SECONDARY_IONIZATION = on;
+	if (on && !built) {
+		secion_init();
+		built = 1;
+	}
+}
+/* secion_get() for column 0 PhiHI, 1 PhiHeI, 2 Eh. */
+double ref_secion_get(int col, double E, double log10x) {
+	const int ids[3] = {SECION_PHI_HI, SECION_PHI_HEI, SECION_EH};
+	return secion_get(ids[col], E, log10x);
+}
+
+/* Helium state (psystem.h:35-36, 49-50) and yeMET. */
+void ref_get_he(double *lambdaHeI, double *lambdaHeII, float *yGdepHeI, float *yGdepHeII, float *yeMET) {
+	for (size_t i = 0; i < psys.npar; i++) {
+		if (lambdaHeI) lambdaHeI[i] = psys.lambdaHeI[i];
+		if (lambdaHeII) lambdaHeII[i] = psys.lambdaHeII[i];
+		if (yGdepHeI) yGdepHeI[i] = psys.yGdepHeI[i];
+		if (yGdepHeII) yGdepHeII[i] = psys.yGdepHeII[i];
+		if (yeMET) yeMET[i] = psys.yeMET[i];
+	}
+}
+void ref_set_he(const double *lambdaHeI, const double *lambdaHeII) {
+	for (size_t i = 0; i < psys.npar; i++) {
+		if (lambdaHeI) psys.lambdaHeI[i] = lambdaHeI[i];
+		if (lambdaHeII) psys.lambdaHeII[i] = lambdaHeII[i];
+	}
 }
 
 /* yGrecHII (psystem.h:56): the recombination photons of runs not on the

@@ -66,6 +66,11 @@ class Reference:
         lib.ref_tree_ncells.restype = C.c_size_t
         lib.ref_step_evolve.argtypes = [C.c_void_p, C.c_size_t]
         lib.ref_sizeof_step.restype = C.c_size_t
+        lib.ref_set_secondary.argtypes = [C.c_int]
+        lib.ref_secion_get.argtypes = [C.c_int, C.c_double, C.c_double]
+        lib.ref_secion_get.restype = C.c_double
+        lib.ref_get_he.argtypes = [C.c_void_p] * 5
+        lib.ref_set_he.argtypes = [C.c_void_p] * 2
         lib.ref_get_ygrec.argtypes = [C.c_void_p]
         lib.ref_set_ygrec.argtypes = [C.c_void_p]
         lib.ref_lte_row.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
@@ -166,6 +171,25 @@ class Reference:
                 np.ascontiguousarray(ie, np.float32) if ie is not None else None,
                 np.ascontiguousarray(lasthit, np.int64) if lasthit is not None else None]
         self.lib.ref_set_state(*[a.ctypes.data_as(C.c_void_p) if a is not None else None for a in keep])
+
+    def set_secondary(self, on: bool) -> None:
+        """psphray.secondaryIonization (builds secion.c's table once)."""
+        self.lib.ref_set_secondary(int(bool(on)))
+
+    def secion_get(self, col: int, E: float, log10x: float) -> float:
+        """secion_get() src/secion.c for column 0 PhiHI, 1 PhiHeI, 2 Eh."""
+        return self.lib.ref_secion_get(int(col), float(E), float(log10x))
+
+    def he_state(self) -> dict:
+        n = self.n
+        a, b = np.zeros(n), np.zeros(n)
+        c, d, e = (np.zeros(n, np.float32) for _ in range(3))
+        self.lib.ref_get_he(*[x.ctypes.data_as(C.c_void_p) for x in (a, b, c, d, e)])
+        return dict(lambdaHeI=a, lambdaHeII=b, yGdepHeI=c, yGdepHeII=d, yeMET=e)
+
+    def set_he(self, lambdaHeI=None, lambdaHeII=None) -> None:
+        keep = [None if v is None else np.ascontiguousarray(v, np.float64) for v in (lambdaHeI, lambdaHeII)]
+        self.lib.ref_set_he(*[None if v is None else v.ctypes.data_as(C.c_void_p) for v in keep])
 
     def ygrec(self) -> np.ndarray:
         """yGrecHII of every particle (runs not on the spot)."""

@@ -67,7 +67,7 @@ class XsTable(C.Structure):
 
 class Flags(C.Structure):
     _fields_ = [("isothermal", C.c_int), ("on_the_spot", C.c_int), ("h_only", C.c_int),
-                ("adiabatic", C.c_int), ("euler", C.c_int)]
+                ("adiabatic", C.c_int), ("euler", C.c_int), ("secondary_ionization", C.c_int)]
 
 
 class Particles(C.Structure):
@@ -231,6 +231,9 @@ def lib() -> C.CDLL:
         "psg_write_output": ([vp, C.c_char_p, C.POINTER(CSnapshot)], C.c_int),
         "psg_set_hits": ([vp, vp], C.c_int),
         "psg_set_recombination": ([vp, C.c_int, dbl, C.c_int, C.c_uint64], C.c_int),
+        "psg_get_he_state": ([vp, vp, vp, vp], C.c_int),
+        "psg_set_he_state": ([vp, vp, vp], C.c_int),
+        "psg_secion_table_build": ([C.POINTER(CUnits), vp], C.c_int),
         "psg_get_rec_rays": ([vp, vp, vp, sz, C.POINTER(sz)], C.c_int),
         "psg_get_rec_state": ([vp, vp, vp], C.c_int),
         "psg_set_rec_state": ([vp, vp, vp], C.c_int),
@@ -252,7 +255,8 @@ class Physics:
     file formats (units_init, ar_init, xs_init, kernel.akline)."""
 
     def __init__(self, units, rates_path: str = RATES_HUI, kernel_path: str = KERNEL_AKLINE,
-                 isothermal=True, on_the_spot=True, h_only=True, adiabatic=False, euler=False):
+                 isothermal=True, on_the_spot=True, h_only=True, adiabatic=False, euler=False,
+                 secondary_ionization=False):
         L = lib()
         self.units = units
         p = UnitParams(units.h, units.hmf, units.length_cmh, units.mass_gramh, units.time_sh)
@@ -268,7 +272,8 @@ class Physics:
         self._check(L.psg_kernel_table_load(kernel_path.encode(), self.kernel.ctypes.data, 65536, C.byref(n)),
                     f"psg_kernel_table_load({kernel_path})")
         self.kernel = self.kernel[: n.value].copy()
-        self.flags = Flags(int(isothermal), int(on_the_spot), int(h_only), int(adiabatic), int(euler))
+        self.flags = Flags(int(isothermal), int(on_the_spot), int(h_only), int(adiabatic), int(euler),
+                           int(secondary_ionization))
 
     @staticmethod
     def _check(rc, what):
@@ -524,6 +529,16 @@ class Context:
             self._check(lib().psg_get_rec_rays(self.h, rays.ctypes.data, ipar.ctypes.data, n.value, C.byref(n)),
                         "psg_get_rec_rays")
         return rays, ipar
+
+    def he_state(self) -> dict:
+        """Helium fractions (lambdaHeI = x_HeI, lambdaHeII = x_HeII) and yeMET."""
+        a, b, c = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n, np.float32)
+        self._check(lib().psg_get_he_state(self.h, a.ctypes.data, b.ctypes.data, c.ctypes.data), "psg_get_he_state")
+        return dict(lambdaHeI=a, lambdaHeII=b, yeMET=c)
+
+    def set_he_state(self, lambdaHeI=None, lambdaHeII=None):
+        keep = [None if v is None else np.ascontiguousarray(v, np.float64) for v in (lambdaHeI, lambdaHeII)]
+        self._check(lib().psg_set_he_state(self.h, *[_ptr(a) for a in keep]), "psg_set_he_state")
 
     def rec_state(self):
         """yGrecHII and the tick each particle was last hit by a source ray."""

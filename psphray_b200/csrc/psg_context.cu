@@ -71,12 +71,12 @@ extern "C" int psg_create(psg_context **out, int device) {
 static void free_particles(psg_context *ctx) {
 	void *ptrs[] = {ctx->d_psml, ctx->d_mass, ctx->d_rho, ctx->d_yeMET, ctx->d_ie, ctx->d_flag,
 		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep, ctx->d_order, ctx->d_gcarry, ctx->d_ygrec,
-		ctx->d_srcmark};
+		ctx->d_srcmark, ctx->d_lamHeI, ctx->d_lamHeII};
 	for (void *p : ptrs) if (p) cudaFree(p);
 	ctx->d_psml = nullptr; ctx->d_mass = ctx->d_rho = ctx->d_yeMET = ctx->d_ie = nullptr;
 	ctx->d_flag = nullptr; ctx->d_lambdaH = nullptr; ctx->d_hits = nullptr; ctx->d_lasthit = nullptr;
 	ctx->d_hstep = nullptr; ctx->d_order = nullptr; ctx->d_gcarry = nullptr; ctx->d_ygrec = nullptr;
-	ctx->d_srcmark = nullptr;
+	ctx->d_srcmark = nullptr; ctx->d_lamHeI = ctx->d_lamHeII = nullptr;
 	ctx->rec_last = ctx->rec_last_R = 0;
 	ctx->n = 0;
 }
@@ -104,6 +104,7 @@ extern "C" void psg_destroy(psg_context *ctx) {
 	if (ctx->d_emit) cudaFree(ctx->d_emit);
 	if (ctx->d_surr) cudaFree(ctx->d_surr);
 	if (ctx->d_lte) cudaFree(ctx->d_lte);
+	if (ctx->d_si) cudaFree(ctx->d_si);
 	for (auto &b : ctx->scratch) if (b.p) cudaFree(b.p);
 	for (auto &ev : ctx->ev) if (ev) cudaEventDestroy(ev);
 	for (auto &ev : ctx->kev) if (ev) cudaEventDestroy(ev);
@@ -137,8 +138,11 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 	if (!ctx) return PSG_E_INVAL;
 	if (!u || !ar || !xs || !kernel || kernel_n <= 0 || !flags || ar->nrows < 2 || xs->nrows < 2)
 		return psg_fail(ctx, PSG_E_INVAL, "psg_set_physics: missing or empty table");
-	if (!flags->h_only)
-		return psg_fail(ctx, PSG_E_INVAL, "psg_set_physics: only hydrogen-only runs (HOnly) are supported");
+	if (!flags->h_only && !flags->on_the_spot)
+		return psg_fail(ctx, PSG_E_INVAL,
+				"psg_set_physics: helium runs are supported on the spot only (no helium recombination rays)");
+	if (ctx->n && ctx->have_physics && !flags->h_only != !ctx->flags.h_only)
+		return psg_fail(ctx, PSG_E_INVAL, "psg_set_physics: HOnly cannot change after psg_load_particles");
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	if (ctx->d_ar) cudaFree(ctx->d_ar);
 	if (ctx->d_ar_ni) cudaFree(ctx->d_ar_ni);
@@ -194,10 +198,21 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 		PSG_CUDA(e2);
 	}
 	const size_t nx = (size_t)xs->nrows;
-	PSG_CUDA(cudaMalloc(&ctx->d_xs, sizeof(double) * nx * 2));
+	PSG_CUDA(cudaMalloc(&ctx->d_xs, sizeof(double) * nx * 4));
 	PSG_CUDA(cudaMemcpy(ctx->d_xs, xs->eng, sizeof(double) * nx, cudaMemcpyHostToDevice));
-	PSG_CUDA(cudaMemcpy(ctx->d_xs + nx, xs->sigma[PSG_XS_HI], sizeof(double) * nx,
-			cudaMemcpyHostToDevice));
+	for (int s = 0; s < 3; s++)
+		PSG_CUDA(cudaMemcpy(ctx->d_xs + (1 + s) * nx, xs->sigma[PSG_XS_HI + s], sizeof(double) * nx,
+				cudaMemcpyHostToDevice));
+	if (flags->secondary_ionization && !ctx->d_si) {
+		const size_t ns = (size_t)3 * PSG_SECION_NE * PSG_SECION_NX;
+		double *h = (double *)malloc(sizeof(double) * ns);
+		if (!h) return psg_fail(ctx, PSG_E_NOMEM, "psg_set_physics: host allocation failed");
+		psg_secion_table_build(u, h);
+		cudaError_t e3 = cudaMalloc(&ctx->d_si, sizeof(double) * ns);
+		if (e3 == cudaSuccess) e3 = cudaMemcpy(ctx->d_si, h, sizeof(double) * ns, cudaMemcpyHostToDevice);
+		free(h);
+		PSG_CUDA(e3);
+	}
 	PSG_CUDA(cudaMalloc(&ctx->d_kernel, sizeof(double) * kernel_n));
 	PSG_CUDA(cudaMemcpy(ctx->d_kernel, kernel, sizeof(double) * kernel_n, cudaMemcpyHostToDevice));
 	ctx->u = *u;
@@ -210,6 +225,8 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 	ctx->xs_min = xs->min;
 	ctx->xs_step_inv = xs->step_inv;
 	ctx->xs_cut_HI = xs->cut[PSG_XS_HI];
+	ctx->xs_cut_HeI = xs->cut[PSG_XS_HEI];
+	ctx->xs_cut_HeII = xs->cut[PSG_XS_HEII];
 	ctx->kernel_n = kernel_n;
 	if (!flags->on_the_spot) {
 		const int rc = psg_build_lte(ctx, xs);
@@ -221,8 +238,12 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 
 // lambdaH and yeMET from the snapshot's xHI and ye, psystem.c:340-356 with
 // psys_set_lambdaH() psystem.h:156-160 (hydrogen-only branch).
+// With helium the rest of the ye block beyond x_HII is helium's electrons
+// first (psystem.c:350-357, psys_set_lambdaHe() psystem.h:161-170); with
+// HOnly the helium fractions stay 0.
 __global__ void k_init_particles(size_t n, const float *pos, const float *sml, const float *xHI,
-		const float *ye, float4 *psml, double *lambdaH, float *yeMET) {
+		const float *ye, int helium, double hmf, float4 *psml, double *lambdaH, float *yeMET,
+		double *lamHeI, double *lamHeII) {
 	const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	psml[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], sml[i]);
@@ -233,7 +254,25 @@ __global__ void k_init_particles(size_t n, const float *pos, const float *sml, c
 	else if (xhi <= 0.0 || xhii >= 1.0) lam = 0.0;
 	else lam = xhi;
 	lambdaH[i] = lam;
-	yeMET[i] = (float)fdim((double)ye[i], xhii);
+	double yem = fdim((double)ye[i], xhii);
+	double l1 = 0.0, l2 = 0.0;
+	if (helium) {
+		double x2 = yem * hmf / (1 - hmf) * 4;
+		double x3 = fdim(x2, 1.0);
+		x2 = fmin(1.0, x2);
+		x3 = fmin(1.0 - x2, x3);
+		const double x1 = 1.0 - x2 - x3;
+		if (x1 >= 1.0 || (x2 + x3) <= 0.0) l1 = 1.0;
+		else if (x1 <= 0.0 || (x2 + x3) >= 1.0) l1 = 0.0;
+		else l1 = x1;
+		if (x2 >= 1.0 || (x1 + x3) <= 0.0) l2 = 1.0;
+		else if (x2 <= 0.0 || (x3 + x1) >= 1.0) l2 = 0.0;
+		else l2 = x2;
+		yem = fdim(yem, (x2 + 2 * x3) * (1 - hmf) / hmf * 0.25);
+	}
+	lamHeI[i] = l1;
+	lamHeII[i] = l2;
+	yeMET[i] = (float)yem;
 }
 
 extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
@@ -263,6 +302,8 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMalloc(&ctx->d_gcarry, sizeof(double) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_ygrec, sizeof(float) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_srcmark, sizeof(int32_t) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_lamHeI, sizeof(double) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_lamHeII, sizeof(double) * n));
 	float *d_pos = (float *)psg_scratch(ctx, S_MISC, sizeof(float) * n * 7);
 	if (!d_pos) return PSG_E_NOMEM;
 	float *d_sml = d_pos + 3 * n, *d_xHI = d_pos + 4 * n, *d_ye = d_pos + 5 * n;
@@ -284,7 +325,8 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMemsetAsync(ctx->d_srcmark, 0xff, sizeof(int32_t) * n, s));
 	const int bs = 256;
 	k_init_particles<<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(n, d_pos, d_sml, d_xHI, d_ye,
-			ctx->d_psml, ctx->d_lambdaH, ctx->d_yeMET);
+			ctx->have_physics && !ctx->flags.h_only, ctx->u.hmf, ctx->d_psml, ctx->d_lambdaH, ctx->d_yeMET,
+			ctx->d_lamHeI, ctx->d_lamHeII);
 	PSG_CHECK_LAUNCH();
 	PSG_CUDA(cudaStreamSynchronize(s));
 	return PSG_OK;
@@ -332,7 +374,8 @@ int psg_permute_particles(psg_context *ctx, const uint32_t *g) {
 			(rc = permute_array(ctx, ctx->d_lambdaH, g)) || (rc = permute_array(ctx, ctx->d_hits, g)) ||
 			(rc = permute_array(ctx, ctx->d_lasthit, g)) || (rc = permute_array(ctx, ctx->d_hstep, g)) ||
 			(rc = permute_array(ctx, ctx->d_gcarry, g)) || (rc = permute_array(ctx, ctx->d_ygrec, g)) ||
-			(rc = permute_array(ctx, ctx->d_srcmark, g)))
+			(rc = permute_array(ctx, ctx->d_srcmark, g)) || (rc = permute_array(ctx, ctx->d_lamHeI, g)) ||
+			(rc = permute_array(ctx, ctx->d_lamHeII, g)))
 		return rc;
 	// the caller index of every new position: through the previous order
 	const size_t n = ctx->n;
@@ -424,6 +467,29 @@ extern "C" int psg_set_hits(psg_context *ctx, const int32_t *hits) {
 	return PSG_OK;
 }
 
+extern "C" int psg_get_he_state(psg_context *ctx, double *lambdaHeI, double *lambdaHeII, float *yeMET) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_get_he_state: no particles loaded");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	int rc = 0;
+	if (lambdaHeI && (rc = to_caller(ctx, lambdaHeI, ctx->d_lamHeI))) return rc;
+	if (lambdaHeII && (rc = to_caller(ctx, lambdaHeII, ctx->d_lamHeII))) return rc;
+	if (yeMET && (rc = to_caller(ctx, yeMET, ctx->d_yeMET))) return rc;
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	return PSG_OK;
+}
+
+extern "C" int psg_set_he_state(psg_context *ctx, const double *lambdaHeI, const double *lambdaHeII) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_set_he_state: no particles loaded");
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	int rc = 0;
+	if (lambdaHeI && (rc = from_caller(ctx, ctx->d_lamHeI, lambdaHeI))) return rc;
+	if (lambdaHeII && (rc = from_caller(ctx, ctx->d_lamHeII, lambdaHeII))) return rc;
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	return PSG_OK;
+}
+
 extern "C" int psg_get_rec_state(psg_context *ctx, float *yGrecHII, int32_t *srcmark) {
 	if (!ctx) return PSG_E_INVAL;
 	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_get_rec_state: no particles loaded");
@@ -454,26 +520,29 @@ extern "C" int psg_write_output(psg_context *ctx, const char *filename, const ps
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	const size_t n = ctx->n;
 	std::vector<float4> psml(n);
-	std::vector<float> pos(3 * n), sml(n), mass(n), rho(n), ie(n), xHI(n), ye(n), zero(n, 0.0f);
-	std::vector<double> lam(n);
+	std::vector<float> pos(3 * n), sml(n), mass(n), rho(n), ie(n), xHI(n), ye(n), xHeI(n), xHeII(n), ygrec(n);
+	std::vector<double> lam(n), l1(n), l2(n);
 	std::vector<int32_t> hits(n);
 	std::vector<int64_t> lasthit(n), ids;
 	int rc = 0;
 	if ((rc = to_caller(ctx, psml.data(), ctx->d_psml)) || (rc = to_caller(ctx, mass.data(), ctx->d_mass)) ||
 			(rc = to_caller(ctx, rho.data(), ctx->d_rho)) || (rc = to_caller(ctx, ie.data(), ctx->d_ie)) ||
 			(rc = to_caller(ctx, lam.data(), ctx->d_lambdaH)) || (rc = to_caller(ctx, hits.data(), ctx->d_hits)) ||
-			(rc = to_caller(ctx, lasthit.data(), ctx->d_lasthit)))
+			(rc = to_caller(ctx, lasthit.data(), ctx->d_lasthit)) || (rc = to_caller(ctx, l1.data(), ctx->d_lamHeI)) ||
+			(rc = to_caller(ctx, l2.data(), ctx->d_lamHeII)) || (rc = to_caller(ctx, ygrec.data(), ctx->d_ygrec)))
 		return rc;
 	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
-	// helium frozen fully ionised in hydrogen-only runs (lambdaHeI = lambdaHeII = 0)
-	const double he_e = ctx->u.hemf / ctx->u.hmf * 0.25 * 2.0;
+	// psys_ye() psystem.h:177 (lambda_to_ye() psystem.h:134-138): with
+	// HOnly both helium fractions are 0, i.e. helium frozen fully ionised
 	for (size_t i = 0; i < n; i++) {
 		pos[3 * i] = psml[i].x;
 		pos[3 * i + 1] = psml[i].y;
 		pos[3 * i + 2] = psml[i].z;
 		sml[i] = psml[i].w;
 		xHI[i] = (float)lam[i];
-		ye[i] = (float)((1.0 - lam[i]) + he_e);
+		xHeI[i] = (float)l1[i];
+		xHeII[i] = (float)l2[i];
+		ye[i] = (float)((1.0 - lam[i]) + ctx->u.hemf / ctx->u.hmf * 0.25 * (l2[i] + 2 * (1.0 - l2[i] - l1[i])));
 	}
 	psg_snapshot s = *meta;
 	if (!s.id) {
@@ -488,9 +557,9 @@ extern "C" int psg_write_output(psg_context *ctx, const char *filename, const ps
 	s.ie = ie.data();
 	s.xHI = xHI.data();
 	s.ye = ye.data();
-	s.xHeI = zero.data();
-	s.xHeII = zero.data();
-	s.gammaHI = zero.data();
+	s.xHeI = xHeI.data();
+	s.xHeII = xHeII.data();
+	s.gammaHI = ygrec.data();      // the block holds yGrecHII (psystem.c:653)
 	s.lasthit = lasthit.data();
 	s.hits = hits.data();
 	if (s.boxsize == 0.0) s.boxsize = ctx->boxsize;

@@ -264,6 +264,55 @@ double psg_xs_get(const psg_xs_table *t, int species, double freq) {
 	return tab_get(t->nrows, t->min, t->step_inv, t->eng, t->sigma[species], freq);
 }
 
+/* ---- secondary ionisation: secion.c -------------------------------------- */
+/* The fits of Ricotti, Gnedin & Shull (2002, ApJ 575, 33) as secion.c
+ * writes them: for the ionisation fractions (k = 0 HI, 1 HeI)
+ *     Phi = A_k (1 - x^b_k)^c_k [E >= E_0 - 0.1]
+ *         - A'_k x^0.2 (1 - x^0.38)^2 [E >= E_0 - 0.1] (E_0/E)^0.4,  E_0 = 28 eV,
+ * and for the heating fraction
+ *     Eh = 1 - (1 - x^0.2663)^1.3163 [E >= E_1 - 0.1]
+ *        + 3.9811 x^0.4 (1 - x^0.34)^2 [E >= E_1 - 0.1] (E_1/E)^0.7,  E_1 = 11 eV
+ * (the 0.1 is subtracted in internal energy units, as there). */
+static const double RGS_A[2] = {0.3908, 0.0554}, RGS_B[2] = {0.4092, 0.4614}, RGS_C[2] = {1.7592, 1.6660};
+static const double RGS_A2[2] = {0.6941, 0.0984};
+
+static double rgs_phi(int k, double E, double x, double ev) {
+	const double gate = 28 * ev;
+	const int f1 = (E >= (gate - 0.1));
+	const double f2 = f1 * pow(gate / E, 0.4);
+	const double y1 = RGS_A[k] * pow(1. - pow(x, RGS_B[k]), RGS_C[k]);
+	const double y2 = RGS_A2[k] * pow(x, 0.2) * pow(1 - pow(x, 0.38), 2.0);
+	return (y1 * f1 - y2 * f2);
+}
+
+static double rgs_heat(double E, double x, double ev) {
+	const double gate = 11 * ev;
+	const int f1 = (E >= gate - 0.1);
+	const double f2 = f1 * pow(gate / E, 0.7);
+	const double y1 = 1.0 * pow(1 - pow(x, 0.2663), 1.3163);
+	const double y2 = 3.9811 * pow(x, 0.4) * pow(1 - pow(x, 0.34), 2.0);
+	return (1. - y1 * f1 + y2 * f2);
+}
+
+/* secion_init() secion.c:74-98 with tabfun2_ensure_col() tabfun.c:151-171 */
+int psg_secion_table_build(const psg_units *u, double *out) {
+	if (!u || !out) return PSG_E_INVAL;
+	const double min1 = 10 * u->EV, max1 = 200 * u->EV, min2 = -8, max2 = 0;
+	const double step1 = (max1 - min1) / PSG_SECION_NE, step2 = (max2 - min2) / PSG_SECION_NX;
+	const size_t plane = (size_t)PSG_SECION_NE * PSG_SECION_NX;
+	for (int i = 0; i < PSG_SECION_NE; i++) {
+		const double E = min1 + i * step1;
+		for (int j = 0; j < PSG_SECION_NX; j++) {
+			const double x = pow(10, min2 + j * step2);
+			const size_t o = (size_t)i * PSG_SECION_NX + j;
+			out[o] = rgs_phi(0, E, x, u->EV);
+			out[plane + o] = rgs_phi(1, E, x, u->EV);
+			out[2 * plane + o] = rgs_heat(E, x, u->EV);
+		}
+	}
+	return PSG_OK;
+}
+
 /* ---- kernel.akline reader and sph_depth() sph-depth.c:26-33 ------------- */
 int psg_kernel_table_load(const char *path, double *out, int cap, int *n) {
 	if (!path || !out || !n || cap <= 0) return PSG_E_INVAL;

@@ -55,9 +55,10 @@ struct psg_context {
 	double ar_ni_scale[8] = {};  // each d_ar_ni column is stored divided by this
 	int ar_nrows = 0;
 	double ar_min = 0, ar_step_inv = 0;
-	double *d_xs = nullptr;      // [2][xs_nrows]: energy, sigma_HI
+	double *d_xs = nullptr;      // [4][xs_nrows]: energy, sigma_HI, sigma_HeI, sigma_HeII
 	int xs_nrows = 0;
-	double xs_min = 0, xs_step_inv = 0, xs_cut_HI = 0;
+	double xs_min = 0, xs_step_inv = 0, xs_cut_HI = 0, xs_cut_HeI = 0, xs_cut_HeII = 0;
+	double *d_si = nullptr;      // secondary ionisation: [3][PSG_SECION_NE][PSG_SECION_NX]
 	double *d_kernel = nullptr;
 	int kernel_n = 0;
 
@@ -73,6 +74,8 @@ struct psg_context {
 	float *d_hstep = nullptr;    // last integrator step proposal, seconds (0: none yet)
 	double *d_gcarry = nullptr;  // absorbed photons per H left over by an explicit step
 	float *d_ygrec = nullptr;    // yGrecHII: recombination photons per H not yet emitted
+	double *d_lamHeI = nullptr, *d_lamHeII = nullptr;  // x_HeI, x_HeII (with helium or
+	                             // secondary ionisation; 0 with HOnly)
 	int32_t *d_srcmark = nullptr; // last tick a source ray (or the tick's first recombination
 	                             // ray) hit the particle, -1 never: the emitters of the next tick
 	uint32_t *d_order = nullptr; // after a tree build the arrays above are in leaf order:

@@ -37,15 +37,21 @@ struct PhysParams {
 	double ar_ni_scale[8]; // ... each column divided by its largest magnitude
 	int ar_nrows;
 	double ar_min, ar_step_inv, ar_step;
-	const double *xs;      // [2][xs_nrows]: energy, sigma_HI
+	const double *xs;      // [4][xs_nrows]: energy, sigma_HI, sigma_HeI, sigma_HeII
 	int xs_nrows;
-	double xs_min, xs_step_inv, xs_cut_HI;
+	double xs_min, xs_step_inv, xs_cut_HI, xs_cut_HeI, xs_cut_HeII;
 	const double *kernel;
 	int kernel_n;
 	double H_PER_MASS, HI_ENERGY, MPROTON_OVER_BOLTZMANN, BOLTZMANN_OVER_MPROTON, hmf, hemf;
 	double he_e;           // helium electrons per H, helium frozen (psystem.h:134-137)
 	int isothermal, on_the_spot, adiabatic, euler;
 	float *ygrec;          // yGrecHII per particle (leaf order), when not on the spot
+	// helium (h_only = 0) and secondary ionisation
+	int h_only, secondary;
+	double HE_PER_MASS, HEI_ENERGY, HEII_ENERGY;
+	double *lamHeI, *lamHeII;
+	const double *si;      // [3][PSG_SECION_NE][PSG_SECION_NX]: PhiHI, PhiHeI, Eh
+	double si_min1, si_step1, si_step1_inv, si_min2, si_step2, si_step2_inv;
 };
 
 PhysParams psg_phys_params(const psg_context *ctx);

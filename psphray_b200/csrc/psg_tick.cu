@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "psg_internal.cuh"
+#include "psg_helium.cuh"
 #include "psg_solve.cuh"
 #include "psg_surrogate.cuh"
 
@@ -54,6 +55,23 @@ PhysParams psg_phys_params(const psg_context *ctx) {
 	P.adiabatic = ctx->flags.adiabatic;
 	P.euler = ctx->flags.euler;
 	P.ygrec = ctx->flags.on_the_spot ? nullptr : ctx->d_ygrec;
+	P.xs_cut_HeI = ctx->xs_cut_HeI;
+	P.xs_cut_HeII = ctx->xs_cut_HeII;
+	P.h_only = ctx->flags.h_only;
+	P.secondary = ctx->flags.secondary_ionization;
+	P.HE_PER_MASS = ctx->u.HE_PER_MASS;
+	P.HEI_ENERGY = ctx->u.HEI_ENERGY;
+	P.HEII_ENERGY = ctx->u.HEII_ENERGY;
+	P.lamHeI = ctx->d_lamHeI;
+	P.lamHeII = ctx->d_lamHeII;
+	// secion_init() secion.c:75-86
+	P.si = ctx->d_si;
+	P.si_min1 = 10 * ctx->u.EV;
+	P.si_step1 = (200 * ctx->u.EV - P.si_min1) / PSG_SECION_NE;
+	P.si_step1_inv = 1.0 / P.si_step1;
+	P.si_min2 = -8;
+	P.si_step2 = (0.0 - P.si_min2) / PSG_SECION_NX;
+	P.si_step2_inv = 1.0 / P.si_step2;
 	return P;
 }
 
@@ -275,6 +293,208 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 	if (t == 0 && !skip_ray) lost += TM;
 }
 
+// The same with helium and/or secondary ionisation (loop.c:409-567): the
+// scan runs over the sum of the three species' optical depths; a hit
+// absorbs tau_s/tausum of the photons per species, each capped at its
+// atoms (loop.c:476-505); it writes yGdepHI (acc), heat, yGdepHeI and
+// yGdepHeII (acc_he, acc_he + hb) increments, with the secondary
+// ionisation and heating of loop.c:513-552 (whose HeII terms the
+// reference's statements drop, loop.c:523,542).
+template <int NT>
+__device__ void deposit_ray_gen(const psg_ray &ray, int64_t h0, int64_t h1, int t,
+		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern, const uint32_t *__restrict__ slot,
+		const double *__restrict__ lambdaH, const float *__restrict__ mass, const PhysParams &P, int want_heat,
+		double *__restrict__ acc, double *__restrict__ acc_heat, double *__restrict__ acc_he, size_t hb,
+		DepShared &sh, unsigned &nsat, double &lost, int bar) {
+	const int lane = t & 31, wid = t >> 5;
+	constexpr int NW = NT / 32;
+	const double Nph = ray.Nph;
+	const double freq = ray.freq;
+	const bool skip_ray = (Nph == 0.0);
+	const double sigma = xs_get_HI(P, freq);
+	const double sHeI = xs_get_s(P, 1, freq), sHeII = xs_get_s(P, 2, freq);
+	const double dE0 = fdim(freq, P.HI_ENERGY), dE1 = fdim(freq, P.HEI_ENERGY), dE2 = fdim(freq, P.HEII_ENERGY);
+	const double hf0 = P.H_PER_MASS * dE0, hf1 = P.HE_PER_MASS * dE1, hf2 = P.HE_PER_MASS * dE2;
+	double TM = Nph;
+	bool done = skip_ray;
+	// the next step's loads are issued one step ahead
+	uint32_t np_slot = 0;
+	double np_kern = 0.0, np_lam = 0.0, np_l1 = 0.0, np_l2 = 0.0;
+	float np_mass = 1.0f;
+	{
+		const int64_t h = h0 + t;
+		if (h < h1) {
+			const uint32_t p = hipar[h];
+			np_kern = hkern[h];
+			np_slot = slot[h];
+			if (!done) { np_lam = lambdaH[p]; np_mass = mass[p]; np_l1 = P.lamHeI[p]; np_l2 = P.lamHeII[p]; }
+		}
+	}
+	for (int64_t base = h0; base < h1; base += NT) {
+		const int64_t h = base + t;
+		const bool valid = h < h1;
+		const double kern_c = np_kern, lam_c = np_lam, l1_c = np_l1, l2_c = np_l2;
+		const float mass_c = np_mass;
+		const uint32_t slot_c = np_slot;
+		{
+			const int64_t hn = h + NT;
+			if (hn < h1) {
+				const uint32_t p = hipar[hn];
+				np_kern = hkern[hn];
+				np_slot = slot[hn];
+				if (!done) { np_lam = lambdaH[p]; np_mass = mass[p]; np_l1 = P.lamHeI[p]; np_l2 = P.lamHeII[p]; }
+			}
+		}
+		// species s = 0 HI, 1 HeI, 2 HeII: atoms N_s, optical depth t_s
+		double tau = 0.0, NHI = 0.0, NH_inv = 0.0, delta = -1.0;
+		double N1 = 0.0, N2 = 0.0, t0 = 0.0, t1 = 0.0, t2 = 0.0, NHe_inv = 0.0, xe = 0.0;
+		double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+		bool he = false;
+		if (valid && !done) {
+			const double NH = (double)mass_c * P.H_PER_MASS;
+			const double NHe = (double)mass_c * P.HE_PER_MASS;
+			NHI = lam_c * NH;
+			t0 = sigma * (kern_c * NHI);
+			tau = 0.0 + t0;
+			he = !P.h_only && NHe != 0.0;
+			if (he) {
+				N1 = l1_c * NHe;
+				t1 = sHeI * (kern_c * N1);
+				tau += t1;
+				N2 = l2_c * NHe;
+				t2 = sHeII * (kern_c * N2);
+				tau += t2;
+			}
+			NH_inv = 1.0 / NH;
+			NHe_inv = 1.0 / NHe;
+			xe = ye_he(P, lam_c, l1_c, l2_c) * NH / (NH + NHe);     // loop.c:512-513
+			if (xe > 1.0) xe = 1.0;
+		}
+		int start = 0;
+		while (!done && start < NT) {
+			const bool part = valid && t >= start && tau != 0.0;
+			const double my_tau = part ? tau : 0.0;
+			double wi = my_tau;
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				const double v = __shfl_up_sync(0xffffffffu, wi, o);
+				if (lane >= o) wi += v;
+			}
+			double woff = 0.0, total;
+			if (NW == 1) {
+				total = __shfl_sync(0xffffffffu, wi, 31);
+			} else {
+				if (lane == 31) sh.wsum[wid] = wi;
+				if (t == 0) sh.first = NT;
+				group_sync<NT>(bar);
+				total = 0.0;
+#pragma unroll
+				for (int k = 0; k < NW; k++) {
+					const double v = sh.wsum[k];
+					if (k < wid) woff += v;
+					total += v;
+				}
+			}
+			double TMj = 0.0, absorb = 0.0, TMafter = 0.0;
+			bool capped = false, cut = false;
+			double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+			if (part) {
+				const double excl = (woff + wi) - my_tau;
+				TMj = TM * exp(-excl);
+				absorb = TMj * -expm1(-my_tau);
+				TMafter = TMj - absorb;
+				a0 = t0 / my_tau * absorb;
+				capped = a0 > NHI;
+				if (he) {
+					a1 = t1 / my_tau * absorb;
+					a2 = t2 / my_tau * absorb;
+					capped = capped || a1 > N1 || a2 > N2;
+				}
+				cut = below_cutoff(TMafter, Nph);
+			}
+			int f;
+			if (NW == 1) {
+				const unsigned ev = __ballot_sync(0xffffffffu, capped || cut);
+				f = ev ? __ffs(ev) - 1 : NT;
+			} else {
+				if (capped || cut) atomicMin(&sh.first, t);
+				group_sync<NT>(bar);
+				f = sh.first;
+			}
+			if (part && t < f) {
+				d0 = a0 * NH_inv;
+				if (he) { d1 = a1 * NHe_inv; d2 = a2 * NHe_inv; }
+				delta = d0;
+			}
+			if (f == NT) {
+				TM = TM * exp(-total);
+				group_sync<NT>(bar);       // shared words are rewritten by the next step
+				break;
+			}
+			double TMnew = 0.0;
+			if (t == f) {
+				TMnew = TMafter;
+				if (capped) {
+					if (a0 > NHI) { a0 = NHI; nsat++; }
+					double ab = a0;
+					if (he) {
+						if (a1 > N1) { a1 = N1; nsat++; }
+						if (a2 > N2) { a2 = N2; nsat++; }
+						ab += (a1 + a2);
+					}
+					TMnew = TMj - ab;
+				}
+				d0 = a0 * NH_inv;
+				if (he) { d1 = a1 * NHe_inv; d2 = a2 * NHe_inv; }
+				delta = d0;
+				if (NW > 1) sh.tm = TMnew;
+			}
+			if (NW == 1) {
+				TM = __shfl_sync(0xffffffffu, TMnew, f);
+			} else {
+				group_sync<NT>(bar);
+				TM = sh.tm;
+			}
+			if (below_cutoff(TM, Nph)) done = true;
+			start = f + 1;
+			group_sync<NT>(bar);
+		}
+		if (valid) {
+			// loop.c:512-552: yGdep increments and heat of the hit
+			double y0 = delta, y1 = 0.0, y2 = 0.0, heat = 0.0;
+			if (delta >= 0.0) {
+				if (P.secondary && xe > 0.0) {
+					const double lx = log10(xe);
+					y0 = d0 + (d0 * dE0 / P.HI_ENERGY * secion_get(P, 0, dE0, lx) +
+							d1 * dE1 / P.HI_ENERGY * secion_get(P, 0, dE1, lx));
+					heat = hf0 * d0 * secion_get(P, 2, dE0, lx);
+					if (he) {
+						y1 = d1 + (d0 * dE0 / P.HEI_ENERGY * secion_get(P, 1, dE0, lx) +
+								d1 * dE1 / P.HEI_ENERGY * secion_get(P, 1, dE1, lx));
+						heat += hf1 * d1 * secion_get(P, 2, dE1, lx);
+						y2 = d2;
+					}
+				} else {
+					heat = hf0 * d0;
+					if (he) {
+						y1 = d1;
+						y2 = d2;
+						heat += d1 * hf1;
+						heat += d2 * hf2;
+					}
+				}
+			}
+			acc[slot_c] = y0;
+			if (want_heat) acc_heat[slot_c] = heat;
+			if (acc_he) {
+				acc_he[slot_c] = y1;
+				acc_he[hb + slot_c] = y2;
+			}
+		}
+	}
+	if (t == 0 && !skip_ray) lost += TM;
+}
+
 // Blocks [0, nlong) take one long ray each with all DEP_THREADS threads;
 // the next nmid_blocks take four middle rays each, 128 threads per ray; the
 // remaining blocks take DEP_THREADS/32 short rays, one per warp.
@@ -282,13 +502,14 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 #define DEP_LONG 96       // more hits than this: a group of threads, else a warp
 #define DEP_MID 384       // more hits than this: the whole block, else a 128-thread quarter
 
+template <bool GEN>
 __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__restrict__ rays,
 		const uint32_t *__restrict__ long_rays, int nlong, const uint32_t *__restrict__ mid_rays, int nmid,
 		const uint32_t *__restrict__ short_rays, int nshort,
 		const int64_t *__restrict__ off, const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
 		const uint32_t *__restrict__ slot, const double *__restrict__ lambdaH, const float *__restrict__ mass,
 		PhysParams P, int want_heat, double *__restrict__ acc, double *__restrict__ acc_heat,
-		unsigned long long *__restrict__ n_sat, double *__restrict__ lost) {
+		double *__restrict__ acc_he, size_t hb, unsigned long long *__restrict__ n_sat, double *__restrict__ lost) {
 	__shared__ DepShared sh_block;
 	__shared__ DepShared sh_quarter[4];
 	__shared__ DepShared sh_warp[DEP_THREADS / 32];
@@ -298,23 +519,36 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 	const int nmid_blocks = (nmid + 3) / 4;
 	if ((int)blockIdx.x < nlong) {
 		const uint32_t r = long_rays[blockIdx.x];
-		deposit_ray<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P, want_heat,
-				acc, acc_heat, sh_block, nsat, tm_lost, 0);
+		if (GEN)
+			deposit_ray_gen<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
+					want_heat, acc, acc_heat, acc_he, hb, sh_block, nsat, tm_lost, 0);
+		else
+			deposit_ray<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
+					want_heat, acc, acc_heat, sh_block, nsat, tm_lost, 0);
 	} else if ((int)blockIdx.x < nlong + nmid_blocks) {
 		const int q = tid >> 7;
 		const int m = ((int)blockIdx.x - nlong) * 4 + q;
 		if (m < nmid) {
 			const uint32_t r = mid_rays[m];
-			deposit_ray<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
-					want_heat, acc, acc_heat, sh_quarter[q], nsat, tm_lost, 1 + q);
+			if (GEN)
+				deposit_ray_gen<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
+						want_heat, acc, acc_heat, acc_he, hb, sh_quarter[q], nsat, tm_lost, 1 + q);
+			else
+				deposit_ray<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
+						want_heat, acc, acc_heat, sh_quarter[q], nsat, tm_lost, 1 + q);
 		}
 	} else {
 		const int w = ((int)blockIdx.x - nlong - nmid_blocks) * (DEP_THREADS / 32) + wid;
 		if (w < nshort) {
 			const uint32_t r = short_rays[w];
-			if (off[r + 1] > off[r])
-				deposit_ray<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P, want_heat,
-						acc, acc_heat, sh_warp[wid], nsat, tm_lost, 0);
+			if (off[r + 1] > off[r]) {
+				if (GEN)
+					deposit_ray_gen<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
+							want_heat, acc, acc_heat, acc_he, hb, sh_warp[wid], nsat, tm_lost, 0);
+				else
+					deposit_ray<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
+							want_heat, acc, acc_heat, sh_warp[wid], nsat, tm_lost, 0);
+			}
 		}
 	}
 	for (int o = 16; o > 0; o >>= 1) nsat += __shfl_down_sync(0xffffffffu, nsat, o);
@@ -676,6 +910,54 @@ __global__ void __launch_bounds__(128) k_update_euler(int t, const int32_t *__re
 	if (st) atomicOr(status, st);
 }
 
+// update_pars() loop.c:647-776 with helium: one thread per active particle
+// of the tick sums its deposits (yGdepHI, heat, yGdepHeI, yGdepHeII, in slot
+// order) and integrates the four variables; isothermal, ie follows T at the
+// new ye (loop.c:764-766).
+__global__ void __launch_bounds__(128) k_update_he(int t, const int32_t *__restrict__ tick_act,
+		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg, const double *__restrict__ acc,
+		const double *__restrict__ acc_heat, const double *__restrict__ acc_he, size_t hb, int want_heat,
+		int32_t *__restrict__ hits, double *__restrict__ lambdaH, float *__restrict__ ie,
+		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P,
+		int64_t tick, double tick_time, uint32_t *__restrict__ status) {
+	const int a = tick_act[t] + blockIdx.x * blockDim.x + threadIdx.x;
+	if (a >= tick_act[t + 1]) return;
+	const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
+	double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
+	int nh = 0;
+	for (uint32_t k = s0; k < s1; k++) {
+		const double d = acc[k];
+		if (d >= 0.0) {
+			g0 += d;
+			g1 += acc_he[k];
+			g2 += acc_he[hb + k];
+			if (want_heat) heat += acc_heat[k];
+			nh++;
+		}
+	}
+	const uint32_t p = act_ipar[a];
+	hits[p] += nh;
+	HeStep s;
+	s.yeMET = (double)yeMET[p];
+	s.gHI = g0;
+	s.gHeI = g1;
+	s.gHeII = g2;
+	s.heat = heat;
+	s.time = (double)(tick - lasthit[p]) * tick_time;
+	s.nH = P.H_PER_MASS * (double)rho[p];
+	const double ie0 = (double)ie[p];
+	s.T = ieye2T(P, ie0, ye_he(P, lambdaH[p], P.lamHeI[p], P.lamHeII[p]));     // psys_T()
+	double x[4] = {lambdaH[p], P.lamHeI[p], P.lamHeII[p], ie0};
+	const uint32_t st = solve_step_he(P, s, x);
+	lambdaH[p] = x[0];
+	P.lamHeI[p] = x[1];
+	P.lamHeII[p] = x[2];
+	if (P.isothermal) ie[p] = (float)Tye2ie(P, s.T, ye_he(P, x[0], x[1], x[2]));
+	else if (!P.adiabatic) ie[p] = (float)x[3];
+	lasthit[p] = tick;
+	if (st) atomicOr(status, st);
+}
+
 // Update log (training data of the surrogate): the inputs of every active
 // particle's step before the update, the outputs after it.
 __global__ void k_log_pre(int t, const int32_t *__restrict__ tick_act, const uint32_t *__restrict__ act_ipar,
@@ -723,6 +1005,31 @@ __global__ void k_step_evolve(psg_step *steps, size_t n, PhysParams P, uint32_t 
 	const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	psg_step s = steps[i];
+	if (!P.h_only) {
+		// step_evolve() with helium (solve.c:170-316)
+		HeStep hs;
+		hs.yeMET = s.yeMET; hs.gHI = s.yGdepHI; hs.gHeI = s.yGdepHeI; hs.gHeII = s.yGdepHeII;
+		hs.heat = s.heat; hs.time = s.time; hs.nH = s.nH; hs.T = s.T;
+		double x[4] = {s.lambdaH, s.lambdaHeI, s.lambdaHeII, s.ie};
+		uint32_t st;
+		if (P.euler) {
+			double remain = 0.0;
+			int refined = 0;
+			st = euler_he(P, hs, x, remain, refined);
+			s.step_remain = remain;
+			s.refined = refined;
+		} else {
+			st = solve_step_he(P, hs, x);
+			s.step_remain = 0.0;
+		}
+		s.lambdaH = x[0];
+		s.lambdaHeI = x[1];
+		s.lambdaHeII = x[2];
+		s.ie = x[3];
+		steps[i] = s;
+		if (st) atomicOr(status, st);
+		return;
+	}
 	if (P.euler) {
 		// step_evolve_euler(): no clamping here (update_pars clamps), the
 		// unused fraction of the step and whether it was subdivided
@@ -774,13 +1081,13 @@ static int check_status(psg_context *ctx) {
 // act_key (hb+1, 16-aligned).
 template <typename KT>
 static int build_slots(psg_context *ctx, size_t nray, size_t R, size_t K, size_t nhit, int shift, int tbits,
-		const int64_t *off64, const uint32_t *hit_ipar, int want_heat, int *nact_out) {
+		const int64_t *off64, const uint32_t *hit_ipar, int nacc, int *nact_out) {
 	cudaStream_t st = ctx->stream;
 	const size_t hb = nhit ? nhit : 1;
 	KT *keys = (KT *)psg_scratch(ctx, S_KEYS, sizeof(KT) * 2 * hb);
 	uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
 	uint32_t *slot = (uint32_t *)psg_scratch(ctx, S_SLOT, sizeof(uint32_t) * hb);
-	double *acc = (double *)psg_scratch(ctx, S_ACC, sizeof(double) * hb * (want_heat ? 2 : 1));
+	double *acc = (double *)psg_scratch(ctx, S_ACC, sizeof(double) * hb * nacc);
 	char *actm = (char *)psg_scratch(ctx, S_ACT, sizeof(int32_t) * 4 * (hb + 1) + sizeof(int32_t) * (K + 2)
 			+ sizeof(KT) * (hb + 1) + 1024);
 	if (!keys || !vals || !slot || !acc || !actm) return PSG_E_NOMEM;
@@ -838,6 +1145,13 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 	const size_t nray = R * K;
 	const PhysParams P = psg_phys_params(ctx);
 	const int want_heat = !ctx->flags.isothermal;
+	// helium and/or secondary ionisation take the general deposit; helium
+	// its own update
+	const bool gen = !ctx->flags.h_only || ctx->flags.secondary_ionization;
+	const bool helium = !ctx->flags.h_only;
+	const int nacc = helium ? 4 : (want_heat ? 2 : 1);
+	if (helium && ctx->flags.euler)
+		return psg_fail(ctx, PSG_E_INVAL, "psg_run_ticks: helium ticks with the explicit solver are not supported");
 
 	ctx->nkev = 0;
 	ctx->launches = 0;
@@ -860,11 +1174,12 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 	while ((1ull << tbits) < (unsigned long long)K) tbits++;
 	int nact = 0;
 	int rc2 = (shift + tbits <= 32) ? build_slots<uint32_t>(ctx, nray, R, K, nhit, shift, tbits, off64, hit_ipar,
-			want_heat, &nact)
-		: build_slots<unsigned long long>(ctx, nray, R, K, nhit, shift, tbits, off64, hit_ipar, want_heat, &nact);
+			nacc, &nact)
+		: build_slots<unsigned long long>(ctx, nray, R, K, nhit, shift, tbits, off64, hit_ipar, nacc, &nact);
 	if (rc2) return rc2;
 	double *acc = (double *)ctx->scratch[S_ACC].p;
-	double *acc_heat = want_heat ? acc + hb : nullptr;
+	double *acc_heat = (want_heat || helium) ? acc + hb : nullptr;
+	double *acc_he = helium ? acc + 2 * hb : nullptr;
 	uint32_t *slot = (uint32_t *)ctx->scratch[S_SLOT].p;
 	char *actm = (char *)ctx->scratch[S_ACT].p;
 	int32_t *head = (int32_t *)actm;
@@ -917,7 +1232,8 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 	for (size_t t = 0; t < K; t++) maxt = std::max<size_t>(maxt, (size_t)(h_tick_act[t + 1] - h_tick_act[t]));
 	const bool euler = ctx->flags.euler != 0;
 	// (the network does not model the recombination photons: on the spot only)
-	const bool surr = !iso && !euler && ctx->surr_on && !ctx->flags.adiabatic && ctx->flags.on_the_spot;
+	const bool surr = !iso && !euler && ctx->surr_on && !ctx->flags.adiabatic && ctx->flags.on_the_spot &&
+			ctx->flags.h_only;
 	char *um = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * 3 * (K + 1)
 			+ (iso ? 0 : sizeof(StiffItem) * maxt) + (surr ? sizeof(uint32_t) * maxt : 0) + 512);
 	int32_t *aflag = (int32_t *)psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (3 * (na + 1) + K + 1) + 512);
@@ -937,7 +1253,7 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 		if (!urec) return PSG_E_NOMEM;
 	}
 	float *feat = nullptr;
-	if (ctx->log_buf && !iso) {
+	if (ctx->log_buf && !iso && !helium) {
 		feat = (float *)psg_scratch(ctx, S_LOG, sizeof(float) * 8 * maxt);
 		if (!feat) return PSG_E_NOMEM;
 	}
@@ -970,15 +1286,25 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 		const int nshort = (int)R - nlong - nmid;
 		const unsigned grid = (unsigned)(nlong + (nmid + 3) / 4 + (nshort + DEP_THREADS / 32 - 1) / (DEP_THREADS / 32));
 		psg_mark_begin(ctx, PSG_K_DEPOSIT);
-		if (grid)
-			k_deposit<<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0, nmid,
+		if (grid && gen)
+			k_deposit<true><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0, nmid,
 					short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
-					want_heat, acc, acc_heat, d_nsat, d_lost);
+					want_heat, acc, acc_heat, acc_he, hb, d_nsat, d_lost);
+		else if (grid)
+			k_deposit<false><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0, nmid,
+					short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+					want_heat, acc, acc_heat, nullptr, hb, d_nsat, d_lost);
 		PSG_CHECK_LAUNCH();
 		psg_mark_end(ctx);
 		const int nact_t = h_tick_act[t + 1] - h_tick_act[t];
 		psg_mark_begin(ctx, PSG_K_UPDATE);
-		if (nact_t > 0) {
+		if (nact_t > 0 && helium) {
+			k_update_he<<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat,
+					acc_he, hb, want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
+					ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, ctx->d_status);
+			PSG_CHECK_LAUNCH();
+			ctx->launches++;
+		} else if (nact_t > 0) {
 			const int64_t tick = first_tick + (int64_t)t;
 			const int nl = h_tick_long[t + 1] - h_tick_long[t];
 			const int lb = (nl + 7) / 8;
