@@ -129,10 +129,10 @@ typedef struct {
 #define PSG_SECION_NX 1024
 int psg_secion_table_build(const psg_units *u, double *out);
 
-/* Upload units, tables and flags. Must precede psg_load_particles().
- * Helium (h_only = 0) runs on the spot only (recombination rays of helium
- * are not emitted), and its ticks use the adaptive integrator (euler = 1
- * is accepted by psg_step_evolve only). */
+/* Upload units, tables and flags. Must precede psg_load_particles() (the
+ * ye block is split into hydrogen, helium and metal electrons at load with
+ * the HOnly flag set then). Helium (h_only = 0) ticks use the adaptive
+ * integrator (euler = 1 is accepted by psg_step_evolve only). */
 int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_rate_table *ar,
 		const psg_xs_table *xs, const double *kernel, int kernel_n, const psg_flags *flags);
 
@@ -227,12 +227,13 @@ int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, size_t nray_pe
 /* The recombination half of emit_rays() loop.c:197-232, 273-300, 322-368:
  * from the second tick on, the particles hit in the previous tick by its
  * source rays (and by its first recombination ray, merge_pars()
- * loop.c:628-630) emit nrec rays per tick, each drawing its particle with
- * weight yGrecHII/xHI; a ray starts at the particle, goes in an isotropic
- * direction for 0.2 box sides, carries the particle's yGrecHII*NH split
- * evenly over the rays that drew it, and has an energy drawn from
- * lte_gen_freq() lte.c:36-44 at the particle's temperature (or the HI edge
- * with disable_lte, psphray.disableLTE). The photons leave yGrecHII. With
+ * loop.c:628-630) emit nrec rays per tick and species (HII; with helium also
+ * HeII and HeIII), each drawing its particle with weight yGrec/xHI; a ray
+ * starts at the particle, goes in an isotropic direction for 0.2 box
+ * sides, carries the particle's yGrec times NH (HII) or NHe split evenly
+ * over the rays that drew it, and has an energy drawn from lte_gen_freq()
+ * lte.c:36-44 at the particle's temperature (or the species' edge with
+ * disable_lte, psphray.disableLTE). The photons leave yGrec. With
  * nrec < 0 every such particle with yGrecHII > threshold
  * (psphray.recombineThreshold) emits one ray; with nrec = 0 none is emitted
  * and the photons stay in yGrecHII. Defaults: nrec 100 (epoch
@@ -240,9 +241,11 @@ int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, size_t nray_pe
  * library's own stream (Philox4x32-10, streams 4-6). */
 int psg_set_recombination(psg_context *ctx, int nrec, double threshold, int disable_lte, uint64_t seed);
 /* The recombination rays of the last tick run, in the order they were
- * traced (by emitting particle), with each emitter's caller index; *n
- * receives their number (rays and ipar may be NULL). */
-int psg_get_rec_rays(psg_context *ctx, psg_ray *rays, int64_t *ipar, size_t cap, size_t *n);
+ * traced (by species, then emitting particle), with each emitter's caller
+ * index and the ray's type (0 HII, 1 HeII, 2 HeIII recombination, as r_t's
+ * type, loop.c:264-266); *n receives their number (rays, ipar and type may
+ * be NULL). */
+int psg_get_rec_rays(psg_context *ctx, psg_ray *rays, int64_t *ipar, int32_t *type, size_t cap, size_t *n);
 /* yGrecHII (psystem.h:56) and the tick each particle was last hit by a
  * source ray (-1: never; the next tick's emitters are those of the
  * previous tick), caller order. Any pointer may be NULL. */
@@ -301,12 +304,16 @@ int psg_run_ticks_emit(psg_context *ctx, size_t nray_per_tick, size_t nticks, in
 int psg_get_state(psg_context *ctx, double *lambdaH, float *ie, int32_t *hits, int64_t *lasthit);
 int psg_set_state(psg_context *ctx, const double *lambdaH, const float *ie, const int64_t *lasthit);
 /* Helium state, caller order: lambdaHeI = x_HeI, lambdaHeII = x_HeII
- * (psystem.h:35-36) and yeMET (the electrons from metals, after the
- * hydrogen and helium ones are taken out of the ye block at load,
- * psystem.c:340-358). With HOnly both fractions stay 0 (x_HeIII = 1), as
- * in the reference. Any pointer may be NULL. */
-int psg_get_he_state(psg_context *ctx, double *lambdaHeI, double *lambdaHeII, float *yeMET);
-int psg_set_he_state(psg_context *ctx, const double *lambdaHeI, const double *lambdaHeII);
+ * (psystem.h:35-36), yeMET (the electrons from metals, after the hydrogen
+ * and helium ones are taken out of the ye block at load,
+ * psystem.c:340-358) and, not on the spot, the recombination photons per
+ * helium atom yGrecHeII, yGrecHeIII (psystem.h:57-58). With HOnly both
+ * fractions stay 0 (x_HeIII = 1), as in the reference. Any pointer may be
+ * NULL. */
+int psg_get_he_state(psg_context *ctx, double *lambdaHeI, double *lambdaHeII, float *yeMET, float *yGrecHeII,
+		float *yGrecHeIII);
+int psg_set_he_state(psg_context *ctx, const double *lambdaHeI, const double *lambdaHeII, const float *yGrecHeII,
+		const float *yGrecHeIII);
 
 /* ---- solver ---------------------------------------------------------------- */
 typedef struct {

@@ -5,9 +5,10 @@ never on the product path).
   psg_secion_table_build() (secion_init() src/secion.c:74-98), restated in
   Python: clamped rows or columns interpolate along the other axis, inside
   the table bilinear;
-- he_step(): one step of function() src/solve.c:76-141 with helium, on the
-  spot, integrated tightly (Radau) over (lambdaH, lambdaHeI, lambdaHeII,
-  ie), with LSODA's exit clamps (src/solve.c:208-210);
+- he_step(): one step of function() src/solve.c:76-141 with helium, on
+  the spot or not (then with the three recombination-photon counts),
+  integrated tightly (Radau) over (lambdaH, lambdaHeI, lambdaHeII, ie),
+  with LSODA's exit clamps (src/solve.c:208-213);
 - load_split(): the helium fractions and yeMET that psystem_read_epoch()
   src/psystem.c:340-358 takes out of the ye block.
 """
@@ -74,9 +75,13 @@ def load_split(xHI: np.ndarray, ye: np.ndarray, hmf: float):
     return l1, l2, ym
 
 
-def he_step(x0, yeMET, gHI, gHeI, gHeII, heat, time, nH, T, consts, ar_get, isothermal: bool, rtol=1e-10):
+def he_step(x0, yeMET, gHI, gHeI, gHeII, heat, time, nH, T, consts, ar_get, isothermal: bool, rtol=1e-10,
+            on_the_spot: bool = True, rec0=(0.0, 0.0, 0.0), h_only: bool = False):
     """x0 = (lambdaH, lambdaHeI, lambdaHeII, ie); returns the four after one
-    step, clamped as solve.c:208-210 does."""
+    step, clamped as solve.c:208-210 does; not on the spot (case A) also
+    the three recombination-photon counts from rec0 (clamped at 0,
+    solve.c:211-213). With h_only the helium fractions stay put
+    (solve.c:88-90, 96-98)."""
     from scipy.integrate import solve_ivp
     hmf, hemf = consts["hmf"], consts["hemf"]
     hpm, mob = consts["H_PER_MASS"], consts["MPROTON_OVER_BOLTZMANN"]
@@ -87,22 +92,38 @@ def he_step(x0, yeMET, gHI, gHeI, gHeII, heat, time, nH, T, consts, ar_get, isot
         ye = (xHII + hemf / hmf * 0.25 * (xHeII + 2 * xHeIII)) + yeMET
         Tk = T if isothermal else mob * x[3] / (hemf * 0.25 + hmf + hmf * ye) * 2.0 / 3.0
         lt = math.log10(Tk)
-        r = {k: ar_get(k, lt) * nH for k in ("HIci", "HIIrcB", "HeIci", "HeIIci", "HeIIrcB", "HeIIIrcB", "HIIrccB",
-                                              "HIcec", "HIcic", "Brem")}
-        d0 = -gHI + time * (-r["HIci"] * ye * xHI + r["HIIrcB"] * ye * xHII)
-        d1 = -gHeI + time * (-r["HeIci"] * ye * xHI + r["HeIIrcB"] * ye * xHeII)
-        d2 = -gHeII + time * (-r["HeIIci"] * ye * xHI - r["HeIIrcB"] * ye * xHeII + r["HeIIIrcB"] * ye * xHeIII)
+        r = {k: ar_get(k, lt) * nH for k in ("HIci", "HIIrcA", "HIIrcB", "HeIci", "HeIIci", "HeIIrcA", "HeIIrcB",
+                                              "HeIIIrcA", "HeIIIrcB", "HIIrccA", "HIIrccB", "HIcec", "HIcic", "Brem")}
+        if on_the_spot:
+            d0 = -gHI + time * (-r["HIci"] * ye * xHI + r["HIIrcB"] * ye * xHII)
+            d1 = -gHeI + time * (-r["HeIci"] * ye * xHI + r["HeIIrcB"] * ye * xHeII)
+            d2 = -gHeII + time * (-r["HeIIci"] * ye * xHI - r["HeIIrcB"] * ye * xHeII + r["HeIIIrcB"] * ye * xHeIII)
+            dr = [0.0, 0.0, 0.0]
+        else:
+            xHeI = x[1]
+            d0 = -gHI + time * (-r["HIci"] * ye * xHI + r["HIIrcA"] * ye * xHII)
+            d1 = -gHeI + time * (-r["HeIci"] * ye * xHeI + r["HeIIrcA"] * ye * xHeII)
+            d2 = -gHeII + time * (-r["HeIIci"] * ye * xHeII - r["HeIIrcA"] * ye * xHeII + r["HeIIIrcA"] * ye * xHeIII)
+            dr = [time * max(r["HIIrcA"] - r["HIIrcB"], 0.0) * ye * xHII,
+                  time * max(r["HeIIrcA"] - r["HeIIrcB"], 0.0) * ye * xHeII,
+                  time * max(r["HeIIIrcA"] - r["HeIIIrcB"], 0.0) * ye * xHeIII]
         if isothermal:
             d3 = 0.0
         else:
-            L = hpm * ((r["HIcic"] + r["HIcec"]) * ye * xHI + r["HIIrccB"] * ye * xHII + r["Brem"] * ye * xHII
+            eta = r["HIIrccB"] if on_the_spot else r["HIIrccA"]
+            L = hpm * ((r["HIcic"] + r["HIcec"]) * ye * xHI + eta * ye * xHII + r["Brem"] * ye * xHII
                        + ar_get("Compton", lt) * ye)
             d3 = heat - time * L
-        return [d0, d1, d2, d3]
-    sol = solve_ivp(f, (0.0, 1.0), list(x0), method="Radau", rtol=rtol,
-                    atol=[1e-13, 1e-13, 1e-13, 1e-13 * abs(x0[3])])
+        if h_only:
+            d1 = d2 = 0.0
+            dr[1] = dr[2] = 0.0
+        return [d0, d1, d2, d3] + dr
+    sol = solve_ivp(f, (0.0, 1.0), list(x0) + list(rec0), method="Radau", rtol=rtol,
+                    atol=[1e-13, 1e-13, 1e-13, 1e-13 * abs(x0[3]), 1e-15, 1e-15, 1e-15])
     x = sol.y[:, -1]
     l0 = min(1.0, max(0.0, x[0]))
     l1 = min(1.0, max(0.0, x[1]))
     l2 = min(1.0 - l1, max(0.0, x[2]))
-    return l0, l1, l2, x[3]
+    if on_the_spot:
+        return l0, l1, l2, x[3]
+    return l0, l1, l2, x[3], max(x[4], 0.0), max(x[5], 0.0), max(x[6], 0.0)

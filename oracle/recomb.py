@@ -63,71 +63,90 @@ def lte_index(cdf_row: np.ndarray, u: float) -> int:
     return j
 
 
-def temperature(ie, lam, c) -> np.ndarray:
-    """ieye2T() src/config.h:106-110 with psys_ye() (no yeMET), the
-    product's rounding order."""
-    he_e = c["hemf"] / c["hmf"] * 0.25 * 2.0
-    ye = (1.0 - lam) + he_e
+def temperature(ie, lam, c, l1=None, l2=None) -> np.ndarray:
+    """ieye2T() src/config.h:106-110 with psys_ye() (no yeMET; helium
+    fractions l1 = x_HeI, l2 = x_HeII, 0 with HOnly), the product's
+    rounding order."""
+    l1 = np.zeros_like(lam) if l1 is None else l1
+    l2 = np.zeros_like(lam) if l2 is None else l2
+    ye = (1.0 - lam) + c["hemf"] / c["hmf"] * 0.25 * (l2 + 2 * (1.0 - l2 - l1))
     den = (c["hemf"] * 0.25 + c["hmf"]) + c["hmf"] * ye
     return ((c["MPROTON_OVER_BOLTZMANN"] * ie.astype(np.float64)) / den * 2.0) / 3.0
 
 
+THRESHOLDS = ("HI_ENERGY", "HEI_ENERGY", "HEII_ENERGY")
+PICK_STREAMS = (4, 7, 8)        # the emitter draws of HII, HeII, HeIII recombinations
+
+
 def emit(yg, lam, mark, pos, mass, ie, tick: int, nrec: int, seed: int, boxsize: float, consts: dict,
-         lte=None, threshold: float = 0.1):
-    """State arrays in caller order. Returns (rays, emitter index, yGrecHII
-    after the emission). lte = (freq, cdf) or None (disableLTE)."""
+         lte=None, threshold: float = 0.1, l1=None, l2=None, types: bool = False):
+    """State arrays in caller order. yg: yGrecHII, or the list [yGrecHII,
+    yGrecHeII, yGrecHeIII] (helium); lte: (freq, cdf) or a list of them per
+    species, None for disableLTE. Returns (rays, emitter index[, type],
+    yGrec after the emission, in the form given)."""
     from psphray_b200.fields import RAY_DTYPE
+    single = not isinstance(yg, (list, tuple))
+    ygs = [yg] if single else list(yg)
+    ltes = [lte] if (single or lte is None or not isinstance(lte, list)) else lte
     n = len(lam)
     marked = mark == tick - 1
-    yg64 = yg.astype(np.float64)
-    if nrec == 0:
-        return np.zeros(0, RAY_DTYPE), np.zeros(0, np.int64), yg.copy()
-    if nrec > 0:
-        x = np.where(lam == 0.0, 1e-10, lam)
-        w = np.where(marked, yg64 / x, 0.0)
-        cdf = np.cumsum(w)
-        total = cdf[-1]
-        if not total > 0.0:
-            return np.zeros(0, RAY_DTYPE), np.zeros(0, np.int64), yg.copy()
-        d = _draw(nrec, tick, 4, seed)
-        c = np.searchsorted(cdf, _u01(d[:, 0], d[:, 1]) * total, side="right")
-        c[c >= n] = np.searchsorted(cdf, total, side="left")
-        keys = (c.astype(np.int64) << 24) | np.arange(nrec, dtype=np.int64)
-        em = c[np.argsort(keys, kind="stable")].astype(np.int64)
-    else:
-        em = np.nonzero(marked & (yg64 > threshold))[0].astype(np.int64)
-    M = len(em)
+    keys = []
+    if nrec != 0:
+        for s, y in enumerate(ygs):
+            y64 = y.astype(np.float64)
+            if nrec > 0:
+                x = np.where(lam == 0.0, 1e-10, lam)
+                w = np.where(marked, y64 / x, 0.0)
+                cdf = np.cumsum(w)
+                total = cdf[-1]
+                if not total > 0.0:
+                    continue
+                d = _draw(nrec, tick, PICK_STREAMS[s], seed)
+                c = np.searchsorted(cdf, _u01(d[:, 0], d[:, 1]) * total, side="right")
+                c[c >= n] = np.searchsorted(cdf, total, side="left")
+                keys.append((np.int64(s) << 56) | (c.astype(np.int64) << 24) | np.arange(nrec, dtype=np.int64))
+            else:
+                c = np.nonzero(marked & (y64 > threshold))[0].astype(np.int64)
+                keys.append((np.int64(s) << 56) | (c << 24))
+    keys = np.sort(np.concatenate(keys)) if keys else np.zeros(0, np.int64)
+    em = (keys >> 24) & 0xFFFFFFFF
+    typ = (keys >> 56).astype(np.int32)
+    M = len(keys)
     rays = np.zeros(M, RAY_DTYPE)
-    if M == 0:
-        return rays, em, yg.copy()
-    _, inv, cnt = np.unique(em, return_inverse=True, return_counts=True)
-    c_of = cnt[inv].astype(np.float64)
-    NH = mass[em].astype(np.float64) * consts["H_PER_MASS"]
-    rays["Nph"] = (yg64[em] * NH) * (1.0 / c_of)
-    rays["s"] = pos[em].astype(np.float32)
-    rays["length"] = boxsize * 2.0 * 0.1
-    d5 = _draw(M, tick, 5, seed)
-    cz = 2.0 * _u01(d5[:, 0], d5[:, 1]) - 1.0
-    phi = (2.0 * 3.141592653589793) * _u01(d5[:, 2], d5[:, 3])
-    st = np.sqrt(np.maximum(0.0, 1.0 - cz * cz))
-    rays["dir"] = np.stack([st * np.cos(phi), st * np.sin(phi), cz], axis=1).astype(np.float32)
-    if lte is None:
-        rays["freq"] = consts["HI_ENERGY"]
-    else:
-        freq, table = lte
-        T = temperature(ie[em], lam[em], consts)
-        rows = np.clip(np.trunc((np.log10(T) - 3.0) / (7.0 / NLOGT)).astype(np.int64), 0, NLOGT - 1)
-        d6 = _draw(M, tick, 6, seed)
-        u = _u01(d6[:, 0], d6[:, 1])
-        fstep = (16.0 * consts["HI_ENERGY"] - consts["HI_ENERGY"]) / NFREQ
-        rays["freq"] = [consts["HI_ENERGY"] + fstep * lte_index(table[r], uu) for r, uu in zip(rows, u)]
-    out = yg.copy()
-    for i in range(M):
-        p = em[i]
-        y = np.float32(out[p])
-        y = np.float32(np.float64(y) - rays["Nph"][i] / NH[i])
-        out[p] = max(y, np.float32(0.0))
-    return rays, em, out
+    outs = [y.copy() for y in ygs]
+    if M:
+        run = keys >> 24
+        _, inv, cnt = np.unique(run, return_inverse=True, return_counts=True)
+        c_of = cnt[inv].astype(np.float64)
+        per = np.where(typ == 0, consts["H_PER_MASS"], consts.get("HE_PER_MASS", 0.0))
+        N = mass[em].astype(np.float64) * per
+        ygv = np.array([float(ygs[s][p]) for s, p in zip(typ, em)])
+        rays["Nph"] = (ygv * N) * (1.0 / c_of)
+        rays["s"] = pos[em].astype(np.float32)
+        rays["length"] = boxsize * 2.0 * 0.1
+        d5 = _draw(M, tick, 5, seed)
+        cz = 2.0 * _u01(d5[:, 0], d5[:, 1]) - 1.0
+        phi = (2.0 * 3.141592653589793) * _u01(d5[:, 2], d5[:, 3])
+        st = np.sqrt(np.maximum(0.0, 1.0 - cz * cz))
+        rays["dir"] = np.stack([st * np.cos(phi), st * np.sin(phi), cz], axis=1).astype(np.float32)
+        if lte is None:
+            rays["freq"] = [consts[THRESHOLDS[s]] for s in typ]
+        else:
+            T = temperature(ie[em], lam[em], consts, None if l1 is None else l1[em], None if l2 is None else l2[em])
+            rows = np.clip(np.trunc((np.log10(T) - 3.0) / (7.0 / NLOGT)).astype(np.int64), 0, NLOGT - 1)
+            d6 = _draw(M, tick, 6, seed)
+            u = _u01(d6[:, 0], d6[:, 1])
+            fr = []
+            for s, r, uu in zip(typ, rows, u):
+                th = consts[THRESHOLDS[s]]
+                fr.append(th + (16.0 * th - th) / NFREQ * lte_index(ltes[s][1][r], uu))
+            rays["freq"] = fr
+        for i in range(M):
+            s, p = typ[i], em[i]
+            y = np.float32(np.float64(np.float32(outs[s][p])) - rays["Nph"][i] / N[i])
+            outs[s][p] = max(y, np.float32(0.0))
+    after = outs[0] if single else outs
+    return (rays, em, typ, after) if types else (rays, em, after)
 
 
 def iso_step(lam0, gdep, time, nH, T, yeMET, he_e, ar_get):

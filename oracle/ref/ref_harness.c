@@ -285,6 +285,21 @@ void ref_get_ygrec(float *out) {
 void ref_set_ygrec(const float *in) {
 	for (size_t i = 0; i < psys.npar; i++) psys.yGrecHII[i] = in[i];
 }
+/* all three species' recombination photons (psystem.h:56-58) */
+void ref_get_ygrec3(float *a, float *b, float *c) {
+	for (size_t i = 0; i < psys.npar; i++) {
+		a[i] = psys.yGrec[0][i];
+		b[i] = psys.yGrec[1][i];
+		c[i] = psys.yGrec[2][i];
+	}
+}
+void ref_set_ygrec3(const float *a, const float *b, const float *c) {
+	for (size_t i = 0; i < psys.npar; i++) {
+		psys.yGrec[0][i] = a[i];
+		psys.yGrec[1][i] = b[i];
+		psys.yGrec[2][i] = c[i];
+	}
+}
 
 void ref_get_state(double *lambdaH, float *ie, float *yGdepHI, float *heat,
 		int32_t *hits, int64_t *lasthit) {

@@ -72,10 +72,12 @@ class Reference:
         lib.ref_get_he.argtypes = [C.c_void_p] * 5
         lib.ref_set_he.argtypes = [C.c_void_p] * 2
         lib.ref_get_ygrec.argtypes = [C.c_void_p]
+        lib.ref_get_ygrec3.argtypes = [C.c_void_p] * 3
+        lib.ref_set_ygrec3.argtypes = [C.c_void_p] * 3
         lib.ref_set_ygrec.argtypes = [C.c_void_p]
-        lib.ref_lte_row.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        lib.ref_lte_row.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         lib.ref_lte_row.restype = C.c_int
-        lib.ref_lte_gen_freq.argtypes = [C.c_double, C.c_double]
+        lib.ref_lte_gen_freq.argtypes = [C.c_int, C.c_double, C.c_double]
         lib.ref_lte_gen_freq.restype = C.c_double
         assert lib.ref_sizeof_step() == C.sizeof(Step)
         self.units = units
@@ -201,19 +203,30 @@ class Reference:
         a = np.ascontiguousarray(yg, np.float32)
         self.lib.ref_set_ygrec(a.ctypes.data_as(C.c_void_p))
 
+    def ygrec3(self):
+        """[yGrecHII, yGrecHeII, yGrecHeIII] of every particle."""
+        out = [np.zeros(self.n, np.float32) for _ in range(3)]
+        self.lib.ref_get_ygrec3(*[a.ctypes.data_as(C.c_void_p) for a in out])
+        return out
+
+    def set_ygrec3(self, ygs) -> None:
+        keep = [np.ascontiguousarray(a, np.float32) for a in ygs]
+        self.lib.ref_set_ygrec3(*[a.ctypes.data_as(C.c_void_p) for a in keep])
+
     def lte_init(self) -> None:
         """lte_init() src/lte.c:30-34: the LTE recombination spectra."""
         self.lib.ref_lte_init()
 
-    def lte_row(self, row: int):
-        """(energies, weights) of the HI table's row (lte_fill() src/lte.c:46-72)."""
+    def lte_row(self, row: int, species: int = 0):
+        """(energies, weights) of a row of the species' table (0 HI, 1 HeI,
+        2 HeII; lte_fill() src/lte.c:46-72)."""
         f = np.zeros(1024); w = np.zeros(1024)
-        n = self.lib.ref_lte_row(int(row), f.ctypes.data_as(C.c_void_p), w.ctypes.data_as(C.c_void_p))
+        n = self.lib.ref_lte_row(int(species), int(row), f.ctypes.data_as(C.c_void_p), w.ctypes.data_as(C.c_void_p))
         return f[:n], w[:n]
 
-    def lte_gen_freq(self, logT: float, u: float) -> float:
-        """lte_gen_freq(LTE_FREQ_HI, logT) src/lte.c:36-44 drawing at uniform u."""
-        return self.lib.ref_lte_gen_freq(float(logT), float(u))
+    def lte_gen_freq(self, logT: float, u: float, species: int = 0) -> float:
+        """lte_gen_freq() src/lte.c:36-44 of the species' table drawing at uniform u."""
+        return self.lib.ref_lte_gen_freq(int(species), float(logT), float(u))
 
     def stats(self) -> dict:
         out = np.zeros(8)

@@ -231,10 +231,10 @@ def lib() -> C.CDLL:
         "psg_write_output": ([vp, C.c_char_p, C.POINTER(CSnapshot)], C.c_int),
         "psg_set_hits": ([vp, vp], C.c_int),
         "psg_set_recombination": ([vp, C.c_int, dbl, C.c_int, C.c_uint64], C.c_int),
-        "psg_get_he_state": ([vp, vp, vp, vp], C.c_int),
-        "psg_set_he_state": ([vp, vp, vp], C.c_int),
+        "psg_get_he_state": ([vp, vp, vp, vp, vp, vp], C.c_int),
+        "psg_set_he_state": ([vp, vp, vp, vp, vp], C.c_int),
         "psg_secion_table_build": ([C.POINTER(CUnits), vp], C.c_int),
-        "psg_get_rec_rays": ([vp, vp, vp, sz, C.POINTER(sz)], C.c_int),
+        "psg_get_rec_rays": ([vp, vp, vp, vp, sz, C.POINTER(sz)], C.c_int),
         "psg_get_rec_state": ([vp, vp, vp], C.c_int),
         "psg_set_rec_state": ([vp, vp, vp], C.c_int),
     }
@@ -520,24 +520,28 @@ class Context:
         self._check(lib().psg_set_recombination(self.h, int(nrec), float(threshold), int(bool(disable_lte)),
                                                 C.c_uint64(seed)), "psg_set_recombination")
 
-    def rec_rays(self):
-        """The last tick's recombination rays and their emitters (caller index)."""
+    def rec_rays(self, types: bool = False):
+        """The last tick's recombination rays and their emitters (caller
+        index); with types=True also each ray's type (0 HII, 1 HeII, 2 HeIII)."""
         n = C.c_size_t(0)
-        self._check(lib().psg_get_rec_rays(self.h, None, None, 0, C.byref(n)), "psg_get_rec_rays")
-        rays = np.zeros(n.value, RAY_DTYPE); ipar = np.zeros(n.value, np.int64)
+        self._check(lib().psg_get_rec_rays(self.h, None, None, None, 0, C.byref(n)), "psg_get_rec_rays")
+        rays = np.zeros(n.value, RAY_DTYPE); ipar = np.zeros(n.value, np.int64); typ = np.zeros(n.value, np.int32)
         if n.value:
-            self._check(lib().psg_get_rec_rays(self.h, rays.ctypes.data, ipar.ctypes.data, n.value, C.byref(n)),
-                        "psg_get_rec_rays")
-        return rays, ipar
+            self._check(lib().psg_get_rec_rays(self.h, rays.ctypes.data, ipar.ctypes.data, typ.ctypes.data, n.value,
+                                               C.byref(n)), "psg_get_rec_rays")
+        return (rays, ipar, typ) if types else (rays, ipar)
 
     def he_state(self) -> dict:
-        """Helium fractions (lambdaHeI = x_HeI, lambdaHeII = x_HeII) and yeMET."""
-        a, b, c = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n, np.float32)
-        self._check(lib().psg_get_he_state(self.h, a.ctypes.data, b.ctypes.data, c.ctypes.data), "psg_get_he_state")
-        return dict(lambdaHeI=a, lambdaHeII=b, yeMET=c)
+        """Helium fractions (lambdaHeI = x_HeI, lambdaHeII = x_HeII), yeMET and
+        the helium recombination photons yGrecHeII, yGrecHeIII."""
+        a, b = np.zeros(self.n), np.zeros(self.n)
+        c, d, e = (np.zeros(self.n, np.float32) for _ in range(3))
+        self._check(lib().psg_get_he_state(self.h, *[x.ctypes.data for x in (a, b, c, d, e)]), "psg_get_he_state")
+        return dict(lambdaHeI=a, lambdaHeII=b, yeMET=c, yGrecHeII=d, yGrecHeIII=e)
 
-    def set_he_state(self, lambdaHeI=None, lambdaHeII=None):
+    def set_he_state(self, lambdaHeI=None, lambdaHeII=None, yGrecHeII=None, yGrecHeIII=None):
         keep = [None if v is None else np.ascontiguousarray(v, np.float64) for v in (lambdaHeI, lambdaHeII)]
+        keep += [None if v is None else np.ascontiguousarray(v, np.float32) for v in (yGrecHeII, yGrecHeIII)]
         self._check(lib().psg_set_he_state(self.h, *[_ptr(a) for a in keep]), "psg_set_he_state")
 
     def rec_state(self):

@@ -71,12 +71,13 @@ extern "C" int psg_create(psg_context **out, int device) {
 static void free_particles(psg_context *ctx) {
 	void *ptrs[] = {ctx->d_psml, ctx->d_mass, ctx->d_rho, ctx->d_yeMET, ctx->d_ie, ctx->d_flag,
 		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep, ctx->d_order, ctx->d_gcarry, ctx->d_ygrec,
-		ctx->d_srcmark, ctx->d_lamHeI, ctx->d_lamHeII};
+		ctx->d_srcmark, ctx->d_lamHeI, ctx->d_lamHeII, ctx->d_ygrecHe1, ctx->d_ygrecHe2};
 	for (void *p : ptrs) if (p) cudaFree(p);
 	ctx->d_psml = nullptr; ctx->d_mass = ctx->d_rho = ctx->d_yeMET = ctx->d_ie = nullptr;
 	ctx->d_flag = nullptr; ctx->d_lambdaH = nullptr; ctx->d_hits = nullptr; ctx->d_lasthit = nullptr;
 	ctx->d_hstep = nullptr; ctx->d_order = nullptr; ctx->d_gcarry = nullptr; ctx->d_ygrec = nullptr;
 	ctx->d_srcmark = nullptr; ctx->d_lamHeI = ctx->d_lamHeII = nullptr;
+	ctx->d_ygrecHe1 = ctx->d_ygrecHe2 = nullptr;
 	ctx->rec_last = ctx->rec_last_R = 0;
 	ctx->n = 0;
 }
@@ -138,11 +139,6 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 	if (!ctx) return PSG_E_INVAL;
 	if (!u || !ar || !xs || !kernel || kernel_n <= 0 || !flags || ar->nrows < 2 || xs->nrows < 2)
 		return psg_fail(ctx, PSG_E_INVAL, "psg_set_physics: missing or empty table");
-	if (!flags->h_only && !flags->on_the_spot)
-		return psg_fail(ctx, PSG_E_INVAL,
-				"psg_set_physics: helium runs are supported on the spot only (no helium recombination rays)");
-	if (ctx->n && ctx->have_physics && !flags->h_only != !ctx->flags.h_only)
-		return psg_fail(ctx, PSG_E_INVAL, "psg_set_physics: HOnly cannot change after psg_load_particles");
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	if (ctx->d_ar) cudaFree(ctx->d_ar);
 	if (ctx->d_ar_ni) cudaFree(ctx->d_ar_ni);
@@ -304,6 +300,8 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMalloc(&ctx->d_srcmark, sizeof(int32_t) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_lamHeI, sizeof(double) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_lamHeII, sizeof(double) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_ygrecHe1, sizeof(float) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_ygrecHe2, sizeof(float) * n));
 	float *d_pos = (float *)psg_scratch(ctx, S_MISC, sizeof(float) * n * 7);
 	if (!d_pos) return PSG_E_NOMEM;
 	float *d_sml = d_pos + 3 * n, *d_xHI = d_pos + 4 * n, *d_ye = d_pos + 5 * n;
@@ -322,6 +320,8 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMemsetAsync(ctx->d_hstep, 0, sizeof(float) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_gcarry, 0, sizeof(double) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_ygrec, 0, sizeof(float) * n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_ygrecHe1, 0, sizeof(float) * n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_ygrecHe2, 0, sizeof(float) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_srcmark, 0xff, sizeof(int32_t) * n, s));
 	const int bs = 256;
 	k_init_particles<<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(n, d_pos, d_sml, d_xHI, d_ye,
@@ -375,7 +375,8 @@ int psg_permute_particles(psg_context *ctx, const uint32_t *g) {
 			(rc = permute_array(ctx, ctx->d_lasthit, g)) || (rc = permute_array(ctx, ctx->d_hstep, g)) ||
 			(rc = permute_array(ctx, ctx->d_gcarry, g)) || (rc = permute_array(ctx, ctx->d_ygrec, g)) ||
 			(rc = permute_array(ctx, ctx->d_srcmark, g)) || (rc = permute_array(ctx, ctx->d_lamHeI, g)) ||
-			(rc = permute_array(ctx, ctx->d_lamHeII, g)))
+			(rc = permute_array(ctx, ctx->d_lamHeII, g)) || (rc = permute_array(ctx, ctx->d_ygrecHe1, g)) ||
+			(rc = permute_array(ctx, ctx->d_ygrecHe2, g)))
 		return rc;
 	// the caller index of every new position: through the previous order
 	const size_t n = ctx->n;
@@ -467,7 +468,8 @@ extern "C" int psg_set_hits(psg_context *ctx, const int32_t *hits) {
 	return PSG_OK;
 }
 
-extern "C" int psg_get_he_state(psg_context *ctx, double *lambdaHeI, double *lambdaHeII, float *yeMET) {
+extern "C" int psg_get_he_state(psg_context *ctx, double *lambdaHeI, double *lambdaHeII, float *yeMET,
+		float *yGrecHeII, float *yGrecHeIII) {
 	if (!ctx) return PSG_E_INVAL;
 	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_get_he_state: no particles loaded");
 	PSG_CUDA(cudaSetDevice(ctx->device));
@@ -475,17 +477,22 @@ extern "C" int psg_get_he_state(psg_context *ctx, double *lambdaHeI, double *lam
 	if (lambdaHeI && (rc = to_caller(ctx, lambdaHeI, ctx->d_lamHeI))) return rc;
 	if (lambdaHeII && (rc = to_caller(ctx, lambdaHeII, ctx->d_lamHeII))) return rc;
 	if (yeMET && (rc = to_caller(ctx, yeMET, ctx->d_yeMET))) return rc;
+	if (yGrecHeII && (rc = to_caller(ctx, yGrecHeII, ctx->d_ygrecHe1))) return rc;
+	if (yGrecHeIII && (rc = to_caller(ctx, yGrecHeIII, ctx->d_ygrecHe2))) return rc;
 	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
 	return PSG_OK;
 }
 
-extern "C" int psg_set_he_state(psg_context *ctx, const double *lambdaHeI, const double *lambdaHeII) {
+extern "C" int psg_set_he_state(psg_context *ctx, const double *lambdaHeI, const double *lambdaHeII,
+		const float *yGrecHeII, const float *yGrecHeIII) {
 	if (!ctx) return PSG_E_INVAL;
 	if (!ctx->n) return psg_fail(ctx, PSG_E_INVAL, "psg_set_he_state: no particles loaded");
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	int rc = 0;
 	if (lambdaHeI && (rc = from_caller(ctx, ctx->d_lamHeI, lambdaHeI))) return rc;
 	if (lambdaHeII && (rc = from_caller(ctx, ctx->d_lamHeII, lambdaHeII))) return rc;
+	if (yGrecHeII && (rc = from_caller(ctx, ctx->d_ygrecHe1, yGrecHeII))) return rc;
+	if (yGrecHeIII && (rc = from_caller(ctx, ctx->d_ygrecHe2, yGrecHeIII))) return rc;
 	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
 	return PSG_OK;
 }

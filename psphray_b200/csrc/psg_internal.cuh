@@ -74,6 +74,7 @@ struct psg_context {
 	float *d_hstep = nullptr;    // last integrator step proposal, seconds (0: none yet)
 	double *d_gcarry = nullptr;  // absorbed photons per H left over by an explicit step
 	float *d_ygrec = nullptr;    // yGrecHII: recombination photons per H not yet emitted
+	float *d_ygrecHe1 = nullptr, *d_ygrecHe2 = nullptr;  // yGrecHeII, yGrecHeIII (per He)
 	double *d_lamHeI = nullptr, *d_lamHeII = nullptr;  // x_HeI, x_HeII (with helium or
 	                             // secondary ionisation; 0 with HOnly)
 	int32_t *d_srcmark = nullptr; // last tick a source ray (or the tick's first recombination
@@ -102,8 +103,8 @@ struct psg_context {
 	double rec_threshold = 0.1;  // psphray.recombineThreshold (config.c:37)
 	int rec_disable_lte = 0;     // psphray.disableLTE (config.c:33)
 	uint64_t rec_seed = 0;
-	double *d_lte = nullptr;     // [PSG_LTE_NLOGT][PSG_LTE_NFREQ] cumulative weights
-	double lte_freq_min = 0, lte_freq_step = 0;
+	double *d_lte = nullptr;     // [3][PSG_LTE_NLOGT][PSG_LTE_NFREQ] cumulative weights
+	double lte_freq_min[3] = {}, lte_freq_step[3] = {};
 	size_t rec_last = 0;         // recombination rays of the last tick (after the source rays in S_RECRAYS)
 	size_t rec_last_R = 0;       // source rays of that tick
 	size_t rec_last_kmax = 0;    // capacity of that tick's key arrays (S_RECK)

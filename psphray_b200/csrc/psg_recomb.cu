@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "psg_internal.cuh"
+#include "psg_helium.cuh"
 #include "psg_philox.cuh"
 #include "psg_solve.cuh"
 
@@ -73,22 +74,22 @@ __global__ void k_rec_weight(size_t n, int32_t prev, const int32_t *__restrict__
 	leaf_of[c] = (uint32_t)p;
 }
 
-// nrec draws from the cumulative weights (caller order): key = caller index
-// << 24 | draw, value = the particle (leaf order); *count = nrec, or 0 when
-// no weight is positive.
-__global__ void k_rec_draw(size_t n, int nrec, const double *__restrict__ cdf, int64_t tick, uint64_t seed,
-		const uint32_t *__restrict__ leaf_of, unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals,
-		unsigned *__restrict__ count) {
+// nrec draws of species s from the cumulative weights (caller order):
+// key = s << 56 | caller index << 24 | draw, value = the particle (leaf
+// order); count[s] = nrec, or 0 when no weight is positive.
+__global__ void k_rec_draw(size_t n, int nrec, int s, uint32_t stream, const double *__restrict__ cdf, int64_t tick,
+		uint64_t seed, const uint32_t *__restrict__ leaf_of, unsigned long long *__restrict__ keys,
+		uint32_t *__restrict__ vals, unsigned *__restrict__ count) {
 	const double total = cdf[n - 1];
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k == 0) *count = total > 0.0 ? (unsigned)nrec : 0u;
+	if (k == 0) count[s] = total > 0.0 ? (unsigned)nrec : 0u;
 	if (k >= nrec || !(total > 0.0)) return;
 	uint32_t x[4];
-	draw(x, (uint32_t)k, tick, 4u, seed);
+	draw(x, (uint32_t)k, tick, stream, seed);
 	const double target = rn_dmul(u01(x[0], x[1]), total);
 	int c = upper_index(cdf, 0, (int)n, target);
 	if (c >= (int)n) c = lower_index(cdf, 0, (int)n, total);   // the last particle with weight
-	keys[k] = ((unsigned long long)c << 24) | (unsigned long long)k;
+	keys[k] = ((unsigned long long)s << 56) | ((unsigned long long)c << 24) | (unsigned long long)k;
 	vals[k] = leaf_of[c];
 }
 
@@ -100,39 +101,50 @@ __global__ void k_rec_flag(size_t n, int32_t prev, const int32_t *__restrict__ m
 	flag[p] = (mark[p] == prev && (double)ygrec[p] > threshold) ? 1u : 0u;
 }
 
-__global__ void k_rec_compact(size_t n, const uint32_t *__restrict__ flag, const uint32_t *__restrict__ pos,
+__global__ void k_rec_compact(size_t n, int s, const uint32_t *__restrict__ flag, const uint32_t *__restrict__ pos,
 		const uint32_t *__restrict__ order, unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals,
 		unsigned *__restrict__ count) {
 	const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (p >= n) return;
-	if (p == n - 1) *count = pos[p] + flag[p];
+	if (p == n - 1) count[s] = pos[p] + flag[p];
 	if (!flag[p]) return;
-	keys[pos[p]] = (unsigned long long)caller_of(order, (uint32_t)p) << 24;
+	keys[pos[p]] = ((unsigned long long)s << 56) | ((unsigned long long)caller_of(order, (uint32_t)p) << 24);
 	vals[pos[p]] = (uint32_t)p;
 }
 
+// The LTE tables of the three species (HI, HeI, HeII recombinations).
 struct LteView {
-	const double *cdf;        // [PSG_LTE_NLOGT][PSG_LTE_NFREQ], cumulative weights per row
-	double freq_min, freq_step;
+	const double *cdf;        // [3][PSG_LTE_NLOGT][PSG_LTE_NFREQ], cumulative weights per row
+	double freq_min[3], freq_step[3];
 	int disabled;
 };
 
-// The rays, in (caller index, draw) order -- the reference sorts its rays
-// by (type, ipar), loop.c:236. Each ray's photons: yGrecHII*NH of its
-// particle, split over the run of rays that drew it (loop.c:305-320).
-__global__ void k_rec_rays(int M, const uint32_t *__restrict__ vals, int64_t tick, uint64_t seed,
-		const float4 *__restrict__ psml, const float *__restrict__ mass, const float *__restrict__ ygrec,
+struct RecState {
+	float *yg[3];             // yGrecHII, yGrecHeII, yGrecHeIII
+};
+
+// Emitter and species of a sorted key; rays of one run share them.
+__device__ __forceinline__ unsigned long long run_of(unsigned long long key) { return key >> 24; }
+
+// The rays, in (species, caller index, draw) order -- the reference sorts
+// its rays by (type, ipar), loop.c:236. Each ray's photons: the emitter's
+// yGrec of the species times NH (HII) or NHe (HeII, HeIII), split over the
+// run of rays that drew it (loop.c:277-290, 305-320).
+__global__ void k_rec_rays(int M, const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ vals,
+		int64_t tick, uint64_t seed, const float4 *__restrict__ psml, const float *__restrict__ mass, RecState Y,
 		const double *__restrict__ lambdaH, const float *__restrict__ ie, PhysParams P, LteView L, double length,
 		psg_ray *__restrict__ out, double *__restrict__ nph_sum) {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= M) return;
 	const uint32_t p = vals[i];
+	const unsigned long long run = run_of(keys[i]);
+	const int s = (int)(keys[i] >> 56);
 	int c = 1;
-	for (int j = i - 1; j >= 0 && vals[j] == p; j--) c++;
-	for (int j = i + 1; j < M && vals[j] == p; j++) c++;
-	const double NH = rn_dmul((double)mass[p], P.H_PER_MASS);
+	for (int j = i - 1; j >= 0 && run_of(keys[j]) == run; j--) c++;
+	for (int j = i + 1; j < M && run_of(keys[j]) == run; j++) c++;
+	const double N = rn_dmul((double)mass[p], s == 0 ? P.H_PER_MASS : P.HE_PER_MASS);
 	psg_ray r;
-	r.Nph = rn_dmul(rn_dmul((double)ygrec[p], NH), __ddiv_rn(1.0, (double)c));
+	r.Nph = rn_dmul(rn_dmul((double)Y.yg[s][p], N), __ddiv_rn(1.0, (double)c));
 	const float4 q = psml[p];
 	r.s[0] = q.x;
 	r.s[1] = q.y;
@@ -149,40 +161,42 @@ __global__ void k_rec_rays(int M, const uint32_t *__restrict__ vals, int64_t tic
 	r.dir[1] = (float)rn_dmul(st, sp);
 	r.dir[2] = (float)cz;
 	if (L.disabled) {
-		r.freq = L.freq_min;
+		r.freq = L.freq_min[s];
 	} else {
-		// psys_T() psystem.h:180-182: T from ie and ye without yeMET
-		const double T = ieye2T(P, (double)ie[p], rn_dadd(rn_dsub(1.0, lambdaH[p]), P.he_e));
+		// psys_T() psystem.h:180-182: T from ie and ye (without yeMET)
+		const double T = ieye2T(P, (double)ie[p], ye_he(P, lambdaH[p], P.lamHeI[p], P.lamHeII[p]));
 		const double logT = log10(T);
 		int row = (int)__ddiv_rn(rn_dsub(logT, 3.0), 7.0 / PSG_LTE_NLOGT);
 		if (row < 0) row = 0;
 		if (row >= PSG_LTE_NLOGT) row = PSG_LTE_NLOGT - 1;
-		const double *cdf = L.cdf + (size_t)row * PSG_LTE_NFREQ;
+		const double *cdf = L.cdf + ((size_t)s * PSG_LTE_NLOGT + row) * PSG_LTE_NFREQ;
 		draw(x, (uint32_t)i, tick, 6u, seed);
 		const double total = cdf[PSG_LTE_NFREQ - 1];
 		int j = upper_index(cdf, 0, PSG_LTE_NFREQ, rn_dmul(u01(x[0], x[1]), total));
 		if (j >= PSG_LTE_NFREQ) j = lower_index(cdf, 0, PSG_LTE_NFREQ, total);
-		r.freq = rn_dadd(L.freq_min, rn_dmul(L.freq_step, (double)j));
+		r.freq = rn_dadd(L.freq_min[s], rn_dmul(L.freq_step[s], (double)j));
 	}
 	out[i] = r;
 	atomicAdd(nph_sum, r.Nph);
 }
 
-// The photons leave the emitter (loop.c:345-356): once per run, ray by ray
+// The photons leave the emitter (loop.c:345-368): once per run, ray by ray
 // in float as the reference's compound assignment rounds, never below 0.
-__global__ void k_rec_purge(int M, const uint32_t *__restrict__ vals, const psg_ray *__restrict__ rays,
-		const float *__restrict__ mass, float *__restrict__ ygrec, PhysParams P) {
+__global__ void k_rec_purge(int M, const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ vals,
+		const psg_ray *__restrict__ rays, const float *__restrict__ mass, RecState Y, PhysParams P) {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= M) return;
+	const unsigned long long run = run_of(keys[i]);
+	if (i > 0 && run_of(keys[i - 1]) == run) return;
 	const uint32_t p = vals[i];
-	if (i > 0 && vals[i - 1] == p) return;
-	const double NH = rn_dmul((double)mass[p], P.H_PER_MASS);
-	float y = ygrec[p];
-	for (int j = i; j < M && vals[j] == p; j++) {
-		y = (float)rn_dsub((double)y, __ddiv_rn(rays[j].Nph, NH));
+	const int s = (int)(keys[i] >> 56);
+	const double N = rn_dmul((double)mass[p], s == 0 ? P.H_PER_MASS : P.HE_PER_MASS);
+	float y = Y.yg[s][p];
+	for (int j = i; j < M && run_of(keys[j]) == run; j++) {
+		y = (float)rn_dsub((double)y, __ddiv_rn(rays[j].Nph, N));
 		if (y < 0.0f) y = 0.0f;
 	}
-	ygrec[p] = y;
+	Y.yg[s][p] = y;
 }
 
 // The emitters of the next tick: every particle on the hit lists of the
@@ -196,66 +210,84 @@ __global__ void k_rec_mark(int nmark, const int64_t *__restrict__ off, const uin
 }
 
 // The tick's recombination rays into out (at most cap); *M_out their number.
+// One pass per species (HII; with helium also HeII and HeIII, loop.c:199):
+// weights or threshold flags, draws into the species' part of the key
+// array (unused entries stay all ones and sort last), then one sort.
 int emit_rec(psg_context *ctx, int64_t tick, size_t cap, psg_ray *out, size_t *M_out) {
 	cudaStream_t st = ctx->stream;
 	const size_t n = ctx->n;
 	const PhysParams P = psg_phys_params(ctx);
 	const int threshold_mode = ctx->rec_nrec < 0;
-	const size_t kmax = threshold_mode ? n : (size_t)ctx->rec_nrec;
+	const int nspec = ctx->flags.h_only ? 1 : 3;
+	const size_t kmax = threshold_mode ? n : (size_t)ctx->rec_nrec;     // per species
+	const size_t ktot = kmax * nspec;
 	char *wm = (char *)psg_scratch(ctx, S_RECW, sizeof(double) * 2 * n + sizeof(uint32_t) * n + 512);
-	char *km = (char *)psg_scratch(ctx, S_RECK, (sizeof(unsigned long long) + sizeof(uint32_t)) * 2 * kmax + 1024);
+	char *km = (char *)psg_scratch(ctx, S_RECK, (sizeof(unsigned long long) + sizeof(uint32_t)) * 2 * ktot + 1024);
 	if (!wm || !km) return PSG_E_NOMEM;
 	unsigned long long *keys = (unsigned long long *)km;
-	uint32_t *vals = (uint32_t *)(keys + 2 * kmax);
-	unsigned *d_count = (unsigned *)(ctx->d_counters + 11);
+	uint32_t *vals = (uint32_t *)(keys + 2 * ktot);
+	unsigned *d_count = (unsigned *)(ctx->d_counters + 11);      // [3]
 	double *d_nph = (double *)(ctx->d_counters + 10);
 	const int32_t prev = (int32_t)(tick - 1);
-	if (!threshold_mode) {
-		double *w = (double *)wm, *cdf = w + n;
-		uint32_t *leaf_of = (uint32_t *)(cdf + n);
-		k_rec_weight<<<nblocks(n, 256), 256, 0, st>>>(n, prev, ctx->d_srcmark, ctx->d_ygrec, ctx->d_lambdaH,
-				ctx->d_order, w, leaf_of);
-		PSG_CHECK_LAUNCH();
-		size_t tmp = 0;
-		PSG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, w, cdf, (int64_t)n, st));
-		void *dt = psg_scratch(ctx, S_CUB, tmp);
-		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceScan::InclusiveSum(dt, tmp, w, cdf, (int64_t)n, st));
-		k_rec_draw<<<nblocks(kmax, 128), 128, 0, st>>>(n, (int)kmax, cdf, tick, ctx->rec_seed, leaf_of,
-				keys, vals, d_count);
-		PSG_CHECK_LAUNCH();
-	} else {
-		uint32_t *flag = (uint32_t *)wm, *pos = flag + n;
-		k_rec_flag<<<nblocks(n, 256), 256, 0, st>>>(n, prev, ctx->d_srcmark, ctx->d_ygrec, ctx->rec_threshold, flag);
-		PSG_CHECK_LAUNCH();
-		size_t tmp = 0;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag, pos, (int64_t)n, st));
-		void *dt = psg_scratch(ctx, S_CUB, tmp);
-		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, flag, pos, (int64_t)n, st));
-		k_rec_compact<<<nblocks(n, 256), 256, 0, st>>>(n, flag, pos, ctx->d_order, keys, vals, d_count);
-		PSG_CHECK_LAUNCH();
+	const RecState Y{{ctx->d_ygrec, ctx->d_ygrecHe1, ctx->d_ygrecHe2}};
+	PSG_CUDA(cudaMemsetAsync(keys, 0xff, sizeof(unsigned long long) * ktot, st));
+	PSG_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned) * 4, st));
+	for (int s = 0; s < nspec; s++) {
+		if (!threshold_mode) {
+			double *w = (double *)wm, *cdf = w + n;
+			uint32_t *leaf_of = (uint32_t *)(cdf + n);
+			k_rec_weight<<<nblocks(n, 256), 256, 0, st>>>(n, prev, ctx->d_srcmark, Y.yg[s], ctx->d_lambdaH,
+					ctx->d_order, w, leaf_of);
+			PSG_CHECK_LAUNCH();
+			size_t tmp = 0;
+			PSG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, w, cdf, (int64_t)n, st));
+			void *dt = psg_scratch(ctx, S_CUB, tmp);
+			if (!dt) return PSG_E_NOMEM;
+			PSG_CUDA(cub::DeviceScan::InclusiveSum(dt, tmp, w, cdf, (int64_t)n, st));
+			// streams: 4 the HII emitters, 7 and 8 those of HeII and HeIII
+			k_rec_draw<<<nblocks(kmax, 128), 128, 0, st>>>(n, (int)kmax, s, s == 0 ? 4u : 6u + (uint32_t)s, cdf,
+					tick, ctx->rec_seed, leaf_of, keys + s * kmax, vals + s * kmax, d_count);
+			PSG_CHECK_LAUNCH();
+		} else {
+			uint32_t *flag = (uint32_t *)wm, *pos = flag + n;
+			k_rec_flag<<<nblocks(n, 256), 256, 0, st>>>(n, prev, ctx->d_srcmark, Y.yg[s], ctx->rec_threshold, flag);
+			PSG_CHECK_LAUNCH();
+			size_t tmp = 0;
+			PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag, pos, (int64_t)n, st));
+			void *dt = psg_scratch(ctx, S_CUB, tmp);
+			if (!dt) return PSG_E_NOMEM;
+			PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, flag, pos, (int64_t)n, st));
+			k_rec_compact<<<nblocks(n, 256), 256, 0, st>>>(n, s, flag, pos, ctx->d_order, keys + s * kmax,
+					vals + s * kmax, d_count);
+			PSG_CHECK_LAUNCH();
+		}
+		ctx->launches += 3;
 	}
-	ctx->launches += 3;
-	unsigned M = 0;
-	PSG_CUDA(cudaMemcpyAsync(&M, d_count, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+	unsigned cnt[3] = {0, 0, 0};
+	PSG_CUDA(cudaMemcpyAsync(cnt, d_count, sizeof(unsigned) * 3, cudaMemcpyDeviceToHost, st));
 	PSG_CUDA(cudaStreamSynchronize(st));
-	if (M > cap) return psg_fail(ctx, PSG_E_OVERFLOW, "recombination rays: %u > capacity %zu", M, cap);
+	const size_t M = (size_t)cnt[0] + cnt[1] + cnt[2];
+	if (M > cap) return psg_fail(ctx, PSG_E_OVERFLOW, "recombination rays: %zu > capacity %zu", M, cap);
 	*M_out = M;
 	if (M == 0) return PSG_OK;
-	int nbits = 24;
-	while (nbits < 64 && (1ull << (nbits - 24)) < (unsigned long long)n) nbits++;
 	size_t tmp = 0;
-	PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, keys + kmax, vals, vals + kmax, (int64_t)M, 0, nbits, st));
+	PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, keys + ktot, vals, vals + ktot, (int64_t)ktot, 0, 64,
+			st));
 	void *dt = psg_scratch(ctx, S_CUB, tmp);
 	if (!dt) return PSG_E_NOMEM;
-	PSG_CUDA(cub::DeviceRadixSort::SortPairs(dt, tmp, keys, keys + kmax, vals, vals + kmax, (int64_t)M, 0, nbits, st));
-	const LteView L{ctx->d_lte, ctx->lte_freq_min, ctx->lte_freq_step, ctx->rec_disable_lte};
+	PSG_CUDA(cub::DeviceRadixSort::SortPairs(dt, tmp, keys, keys + ktot, vals, vals + ktot, (int64_t)ktot, 0, 64, st));
+	LteView L;
+	L.cdf = ctx->d_lte;
+	for (int s = 0; s < 3; s++) {
+		L.freq_min[s] = ctx->lte_freq_min[s];
+		L.freq_step[s] = ctx->lte_freq_step[s];
+	}
+	L.disabled = ctx->rec_disable_lte;
 	const double length = ctx->boxsize * 2.0 * 0.1;     // MAX_REC_RAY_LENGTH, loop.c:169
-	k_rec_rays<<<nblocks(M, 128), 128, 0, st>>>((int)M, vals + kmax, tick, ctx->rec_seed, ctx->d_psml, ctx->d_mass,
-			ctx->d_ygrec, ctx->d_lambdaH, ctx->d_ie, P, L, length, out, d_nph);
+	k_rec_rays<<<nblocks(M, 128), 128, 0, st>>>((int)M, keys + ktot, vals + ktot, tick, ctx->rec_seed, ctx->d_psml,
+			ctx->d_mass, Y, ctx->d_lambdaH, ctx->d_ie, P, L, length, out, d_nph);
 	PSG_CHECK_LAUNCH();
-	k_rec_purge<<<nblocks(M, 128), 128, 0, st>>>((int)M, vals + kmax, out, ctx->d_mass, ctx->d_ygrec, P);
+	k_rec_purge<<<nblocks(M, 128), 128, 0, st>>>((int)M, keys + ktot, vals + ktot, out, ctx->d_mass, Y, P);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 2;
 	return PSG_OK;
@@ -263,35 +295,43 @@ int emit_rec(psg_context *ctx, int64_t tick, size_t cap, psg_ray *out, size_t *M
 
 }  // namespace
 
-// lte_fill() lte.c:46-72 for hydrogen: 128 rows of log T from 3 to 10, 1024
-// energies from E_HI up to 16 E_HI; the weights summed in order per row.
+// lte_init() / lte_fill() lte.c:30-72 for the three species (HI, HeI,
+// HeII): 128 rows of log T from 3 to 10, 1024 energies from the threshold
+// E_s up to 16 E_s; the weights sigma_s(E) E^3 exp(-(E - E_s)/kT) summed in
+// order per row.
 int psg_build_lte(psg_context *ctx, const psg_xs_table *xs) {
-	const double fmin_ = ctx->u.HI_ENERGY, fmax_ = 16.0 * ctx->u.HI_ENERGY;
-	const double fstep = (fmax_ - fmin_) / PSG_LTE_NFREQ;
+	const double th[3] = {ctx->u.HI_ENERGY, ctx->u.HEI_ENERGY, ctx->u.HEII_ENERGY};
+	const int xsid[3] = {PSG_XS_HI, PSG_XS_HEI, PSG_XS_HEII};
 	const double tstep = (10.0 - 3.0) / PSG_LTE_NLOGT;
-	std::vector<double> cdf((size_t)PSG_LTE_NLOGT * PSG_LTE_NFREQ), freq(PSG_LTE_NFREQ);
-	for (int j = 0; j < PSG_LTE_NFREQ; j++) freq[j] = fmin_ + fstep * j;
-	for (int i = 0; i < PSG_LTE_NLOGT; i++) {
-		const double logT = 3.0 + tstep * i;
-		const double kT = ctx->u.BOLTZMANN * exp10(logT);
-		double acc = 0.0;
-		for (int j = 0; j < PSG_LTE_NFREQ; j++) {
-			const double f = freq[j];
-			acc += psg_xs_get(xs, PSG_XS_HI, f) * f * f * f * exp(-(f - fmin_) / kT);
-			cdf[(size_t)i * PSG_LTE_NFREQ + j] = acc;
+	const size_t plane = (size_t)PSG_LTE_NLOGT * PSG_LTE_NFREQ;
+	std::vector<double> cdf(3 * plane), freq(PSG_LTE_NFREQ);
+	for (int s = 0; s < 3; s++) {
+		const double fmin_ = th[s], fmax_ = 16.0 * th[s];
+		const double fstep = (fmax_ - fmin_) / PSG_LTE_NFREQ;
+		for (int j = 0; j < PSG_LTE_NFREQ; j++) freq[j] = fmin_ + fstep * j;
+		for (int i = 0; i < PSG_LTE_NLOGT; i++) {
+			const double logT = 3.0 + tstep * i;
+			const double kT = ctx->u.BOLTZMANN * exp10(logT);
+			double acc = 0.0;
+			for (int j = 0; j < PSG_LTE_NFREQ; j++) {
+				const double f = freq[j];
+				acc += psg_xs_get(xs, xsid[s], f) * f * f * f * exp(-(f - fmin_) / kT);
+				cdf[s * plane + (size_t)i * PSG_LTE_NFREQ + j] = acc;
+			}
 		}
+		ctx->lte_freq_min[s] = fmin_;
+		ctx->lte_freq_step[s] = fstep;
 	}
 	if (!ctx->d_lte) PSG_CUDA(cudaMalloc(&ctx->d_lte, sizeof(double) * cdf.size()));
 	PSG_CUDA(cudaMemcpy(ctx->d_lte, cdf.data(), sizeof(double) * cdf.size(), cudaMemcpyHostToDevice));
-	ctx->lte_freq_min = fmin_;
-	ctx->lte_freq_step = fstep;
 	return PSG_OK;
 }
 
 int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K, int64_t first_tick,
 		double tick_time, psg_tick_stats *stats) {
 	cudaStream_t st = ctx->stream;
-	const size_t cap = ctx->rec_nrec > 0 ? (size_t)ctx->rec_nrec : ctx->rec_nrec < 0 ? ctx->n : 0;
+	const size_t cap = (ctx->rec_nrec > 0 ? (size_t)ctx->rec_nrec : ctx->rec_nrec < 0 ? ctx->n : 0) *
+			(ctx->flags.h_only ? 1 : 3);
 	if (R + cap >= (size_t)INT32_MAX) return psg_fail(ctx, PSG_E_OVERFLOW, "psg_run_ticks: batch too large");
 	psg_ray *buf = (psg_ray *)psg_scratch(ctx, S_RECRAYS, sizeof(psg_ray) * (R + cap));
 	if (!buf) return PSG_E_NOMEM;
@@ -357,11 +397,12 @@ extern "C" int psg_set_recombination(psg_context *ctx, int nrec, double threshol
 	return PSG_OK;
 }
 
-extern "C" int psg_get_rec_rays(psg_context *ctx, psg_ray *rays, int64_t *ipar, size_t cap, size_t *n) {
+extern "C" int psg_get_rec_rays(psg_context *ctx, psg_ray *rays, int64_t *ipar, int32_t *type, size_t cap,
+		size_t *n) {
 	if (!ctx) return PSG_E_INVAL;
 	if (!n) return psg_fail(ctx, PSG_E_INVAL, "psg_get_rec_rays: null count");
 	*n = ctx->rec_last;
-	if (ctx->rec_last == 0 || (!rays && !ipar)) return PSG_OK;
+	if (ctx->rec_last == 0 || (!rays && !ipar && !type)) return PSG_OK;
 	if (cap < ctx->rec_last) return psg_fail(ctx, PSG_E_INVAL, "psg_get_rec_rays: %zu rays, capacity %zu", ctx->rec_last, cap);
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	const size_t M = ctx->rec_last;
@@ -370,11 +411,13 @@ extern "C" int psg_get_rec_rays(psg_context *ctx, psg_ray *rays, int64_t *ipar, 
 		PSG_CUDA(cudaMemcpyAsync(rays, (psg_ray *)ctx->scratch[S_RECRAYS].p + ctx->rec_last_R, sizeof(psg_ray) * M,
 				cudaMemcpyDeviceToHost, ctx->stream));
 	std::vector<unsigned long long> keys(M);
-	if (ipar)
+	if (ipar || type)
 		PSG_CUDA(cudaMemcpyAsync(keys.data(), (unsigned long long *)ctx->scratch[S_RECK].p + kmax,
 				sizeof(unsigned long long) * M, cudaMemcpyDeviceToHost, ctx->stream));
 	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
-	if (ipar)
-		for (size_t i = 0; i < M; i++) ipar[i] = (int64_t)(keys[i] >> 24);
+	for (size_t i = 0; i < M; i++) {
+		if (ipar) ipar[i] = (int64_t)((keys[i] >> 24) & 0xFFFFFFFFull);
+		if (type) type[i] = (int32_t)(keys[i] >> 56);
+	}
 	return PSG_OK;
 }

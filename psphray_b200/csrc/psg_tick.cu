@@ -64,6 +64,8 @@ PhysParams psg_phys_params(const psg_context *ctx) {
 	P.HEII_ENERGY = ctx->u.HEII_ENERGY;
 	P.lamHeI = ctx->d_lamHeI;
 	P.lamHeII = ctx->d_lamHeII;
+	P.ygrecHe1 = ctx->flags.on_the_spot ? nullptr : ctx->d_ygrecHe1;
+	P.ygrecHe2 = ctx->flags.on_the_spot ? nullptr : ctx->d_ygrecHe2;
 	// secion_init() secion.c:75-86
 	P.si = ctx->d_si;
 	P.si_min1 = 10 * ctx->u.EV;
@@ -655,7 +657,7 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 	double lam = lam0, grec = 0.0;
 	const uint32_t st = solve_step_iso(P, lam, (double)yeMET[p], g, time, nH, T, REC ? &grec : nullptr);
 	lambdaH[p] = lam;
-	if (REC) P.ygrec[p] = (float)((double)P.ygrec[p] + grec);     // x[3], solve.c:183,218
+	if (REC) P.ygrec[p] = (float)fmax(0.0, (double)P.ygrec[p] + grec);     // x[3], solve.c:183,211,218
 	ie[p] = (float)Tye2ie(P, T, rn_dadd(rn_dsub(1.0, lam), P.he_e));
 	lasthit[p] = tick;
 	if (st) atomicOr(status, st);
@@ -847,7 +849,7 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 				if (!isfinite(lam) || !isfinite(e)) st |= PSG_ST_NAN;
 				lambdaH[p] = fmin(1.0, fmax(0.0, lam));
 				if (!P.adiabatic) ie[p] = (float)e;
-				if (REC) P.ygrec[p] = (float)((double)P.ygrec[p] + S.rec);
+				if (REC) P.ygrec[p] = (float)fmax(0.0, (double)P.ygrec[p] + S.rec);
 				lasthit[p] = tick;
 				hstep[p] = (float)((double)S.hnext * cx.time);
 				have = false;
@@ -872,7 +874,7 @@ __global__ void __launch_bounds__(64) k_update_stiff(const StiffItem *__restrict
 		double x[2] = {it.x0, it.x1};
 		double rec = it.rec;
 		if (!rosenbrock<REC>(P, cx, x, it.t, it.h, UPD_MAX_STEPS, &rec)) st |= PSG_ST_SOLVER;
-		if (REC) P.ygrec[it.p] = (float)((double)P.ygrec[it.p] + rec);
+		if (REC) P.ygrec[it.p] = (float)fmax(0.0, (double)P.ygrec[it.p] + rec);
 		if (!(x[1] >= 0.0)) st |= PSG_ST_IE_NEG;
 		if (!isfinite(x[0]) || !isfinite(x[1])) st |= PSG_ST_NAN;
 		lambdaH[it.p] = fmin(1.0, fmax(0.0, x[0]));
@@ -948,10 +950,21 @@ __global__ void __launch_bounds__(128) k_update_he(int t, const int32_t *__restr
 	const double ie0 = (double)ie[p];
 	s.T = ieye2T(P, ie0, ye_he(P, lambdaH[p], P.lamHeI[p], P.lamHeII[p]));     // psys_T()
 	double x[4] = {lambdaH[p], P.lamHeI[p], P.lamHeII[p], ie0};
-	const uint32_t st = solve_step_he(P, s, x);
+	double rec[3];
+	if (P.ygrec) {
+		rec[0] = (double)P.ygrec[p];
+		rec[1] = (double)P.ygrecHe1[p];
+		rec[2] = (double)P.ygrecHe2[p];
+	}
+	const uint32_t st = solve_step_he(P, s, x, P.ygrec ? rec : nullptr);
 	lambdaH[p] = x[0];
 	P.lamHeI[p] = x[1];
 	P.lamHeII[p] = x[2];
+	if (P.ygrec) {
+		P.ygrec[p] = (float)rec[0];
+		P.ygrecHe1[p] = (float)rec[1];
+		P.ygrecHe2[p] = (float)rec[2];
+	}
 	if (P.isothermal) ie[p] = (float)Tye2ie(P, s.T, ye_he(P, x[0], x[1], x[2]));
 	else if (!P.adiabatic) ie[p] = (float)x[3];
 	lasthit[p] = tick;
@@ -1011,17 +1024,22 @@ __global__ void k_step_evolve(psg_step *steps, size_t n, PhysParams P, uint32_t 
 		hs.yeMET = s.yeMET; hs.gHI = s.yGdepHI; hs.gHeI = s.yGdepHeI; hs.gHeII = s.yGdepHeII;
 		hs.heat = s.heat; hs.time = s.time; hs.nH = s.nH; hs.T = s.T;
 		double x[4] = {s.lambdaH, s.lambdaHeI, s.lambdaHeII, s.ie};
+		double rec[3] = {s.yGrecHII, s.yGrecHeII, s.yGrecHeIII};
 		uint32_t st;
 		if (P.euler) {
-			double remain = 0.0;
+			double remain = 0.0, gain[3] = {0.0, 0.0, 0.0};
 			int refined = 0;
-			st = euler_he(P, hs, x, remain, refined);
+			st = euler_he(P, hs, x, remain, refined, P.on_the_spot ? nullptr : gain);
+			for (int k = 0; k < 3; k++) rec[k] += gain[k];
 			s.step_remain = remain;
 			s.refined = refined;
 		} else {
-			st = solve_step_he(P, hs, x);
+			st = solve_step_he(P, hs, x, P.on_the_spot ? nullptr : rec);
 			s.step_remain = 0.0;
 		}
+		s.yGrecHII = rec[0];
+		s.yGrecHeII = rec[1];
+		s.yGrecHeIII = rec[2];
 		s.lambdaH = x[0];
 		s.lambdaHeI = x[1];
 		s.lambdaHeII = x[2];
@@ -1052,7 +1070,7 @@ __global__ void k_step_evolve(psg_step *steps, size_t n, PhysParams P, uint32_t 
 	const uint32_t st = solve_step(P, lam, e, s.yeMET, s.yGdepHI, s.heat, s.time, s.nH, s.T, &grec);
 	s.lambdaH = lam;
 	s.ie = e;
-	s.yGrecHII += grec;      // x[3] of solve.c:183,218; unchanged on the spot
+	if (!P.on_the_spot) s.yGrecHII = fmax(0.0, s.yGrecHII + grec);      // x[3] of solve.c:183,211,218
 	s.step_remain = 0.0;
 	steps[i] = s;
 	if (st) atomicOr(status, st);

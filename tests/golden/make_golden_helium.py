@@ -16,10 +16,14 @@ writes tests/golden/helium16.npz:
   (1 to 10 Ry): per tick the state before (lambdaH, lambdaHeI, lambdaHeII,
   ie, lasthit, hits), the tick's rays, the deposits after its deposit()
   (yGdepHI, heat, yGdepHeI, yGdepHeII) and the state after its
-  merge_pars() and update_pars(). Three runs: helium
-  isothermal; helium with secondary ionisation, not isothermal; hydrogen
-  only (hydrogen mass fraction 1) with secondary ionisation, not
-  isothermal.
+  merge_pars() and update_pars(). Three runs: helium isothermal; helium
+  with secondary ionisation, not isothermal; hydrogen only (hydrogen mass
+  fraction 1) with secondary ionisation, not isothermal;
+- not on the spot (case-A recombination): Step records with the three
+  species' recombination photons, and ticks of helium, isothermal, with the
+  recombination rays of all three species (made by the oracle's
+  restatement of the device's emission, oracle/recomb.py, from each tick's
+  state) run by the reference's tick phases.
 
 The reference keeps its state in globals, so each case runs in a process of
 its own.
@@ -73,12 +77,16 @@ def _steps(f, tick_time, seed, n, iso, units):
         s.time = tick_time * int(rng.integers(1, 200 if iso else 40))
         s.nH = nH
         s.T = 1e4
+        s.yGrecHII, s.yGrecHeII, s.yGrecHeIII = rng.uniform(0.0, 0.3, 3)
     return steps
 
 
 STEP_IN = ["lambdaH", "lambdaHeI", "lambdaHeII", "ie", "yGdepHI", "yGdepHeI", "yGdepHeII", "heat", "time", "nH",
-           "T", "yeMET"]
-STEP_OUT = ["lambdaH", "lambdaHeI", "lambdaHeII", "ie", "step_remain", "refined"]
+           "T", "yeMET", "yGrecHII", "yGrecHeII", "yGrecHeIII"]
+STEP_OUT = ["lambdaH", "lambdaHeI", "lambdaHeII", "ie", "step_remain", "refined", "yGrecHII", "yGrecHeII",
+            "yGrecHeIII"]
+NREC = 6
+REC_SEED = 11
 
 
 def _case(kind, q):
@@ -92,17 +100,20 @@ def _case(kind, q):
     f = _field(units)
     sch, tick_time = _schedule(units, f)
     out = {}
-    if kind in ("iso", "noniso", "euler_iso", "euler_noniso"):
-        iso = kind in ("iso", "euler_iso")
+    if kind in ("iso", "noniso", "euler_iso", "euler_noniso", "rec_iso", "rec_noniso"):
+        iso = kind in ("iso", "euler_iso", "rec_iso")
         lib = EULER_LIB_PATH if kind.startswith("euler") else LIB_PATH
-        ref = Reference(api.RATES_HUI, units, isothermal=iso, h_only=False, threads=1, lib_path=lib)
-        seed = {"iso": 41, "noniso": 42, "euler_iso": 43, "euler_noniso": 44}[kind]
+        ref = Reference(api.RATES_HUI, units, isothermal=iso, h_only=False, on_the_spot=not kind.startswith("rec"),
+                        threads=1, lib_path=lib)
+        seed = {"iso": 41, "noniso": 42, "euler_iso": 43, "euler_noniso": 44, "rec_iso": 45, "rec_noniso": 46}[kind]
         steps = _steps(f, tick_time, seed, 192, iso, units)
         for k in STEP_IN:
             out[f"{kind}_in_{k}"] = np.array([getattr(s, k) for s in steps])
         ref.step_evolve(steps)
         for k in STEP_OUT:
             out[f"{kind}_out_{k}"] = np.array([getattr(s, k) for s in steps])
+    elif kind == "he_rec":
+        _rec_ticks(units, f, sch, tick_time, out)
     else:
         iso = kind == "he_iso"
         h_only = kind == "h_si"
@@ -143,10 +154,68 @@ def _case(kind, q):
     q.put(out)
 
 
+def _rec_ticks(units, f, sch, tick_time, out):
+    """Helium, isothermal, not on the spot: the ticks with the recombination
+    rays of all three species (oracle/recomb.py) from each tick's state."""
+    import recomb
+    from psphray_b200 import api
+    from refpy import Reference
+    phys = api.Physics(units, isothermal=True, on_the_spot=False, h_only=False)
+    c = {k: phys.unit(k) for k in ("HI_ENERGY", "HEI_ENERGY", "HEII_ENERGY", "BOLTZMANN", "H_PER_MASS",
+                                   "HE_PER_MASS", "MPROTON_OVER_BOLTZMANN", "hmf", "hemf")}
+    ltes = [recomb.lte_table(c[th], c["BOLTZMANN"], (lambda sp: (lambda e: phys.xs_get(sp, e)))(sp))
+            for th, sp in zip(recomb.THRESHOLDS, ("HI", "HeI", "HeII"))]
+    ref = Reference(api.RATES_HUI, units, isothermal=True, h_only=False, on_the_spot=False, threads=1)
+    ref.load(f)
+    ref.build_tree(8)
+    pos = np.asarray(f.pos, np.float32).reshape(-1, 3)
+    mass = np.asarray(f.mass, np.float32)
+    mark = np.full(f.n, -1, np.int32)
+    keys = ("lambdaH", "lambdaHeI", "lambdaHeII", "ie", "lasthit", "hits", "yg0", "yg1", "yg2", "mark")
+    b, a = {k: [] for k in keys}, {k: [] for k in keys}
+    rays_src, rays_rec, rec_ipar, rec_type = [], [], [], []
+
+    def snap(dst):
+        s, he, yg = ref.state(), ref.he_state(), ref.ygrec3()
+        vals = dict(lambdaH=s["lambdaH"], lambdaHeI=he["lambdaHeI"], lambdaHeII=he["lambdaHeII"], ie=s["ie"],
+                    lasthit=s["lasthit"], hits=s["hits"], yg0=yg[0], yg1=yg[1], yg2=yg[2], mark=mark.copy())
+        for k in keys:
+            dst[k].append(vals[k])
+        return vals
+    R = sch.nray
+    for t in range(1, NTICK + 1):
+        v = snap(b)
+        src = sch.rays_for_tick(t)
+        if t > 1:
+            rr, em, ty, ygs = recomb.emit([v["yg0"], v["yg1"], v["yg2"]], v["lambdaH"], mark, pos, mass, v["ie"], t,
+                                          NREC, REC_SEED, f.boxsize, c, lte=ltes, l1=v["lambdaHeI"],
+                                          l2=v["lambdaHeII"], types=True)
+            ref.set_ygrec3(ygs)
+        else:
+            rr, em, ty = np.zeros(0, src.dtype), np.zeros(0, np.int64), np.zeros(0, np.int32)
+        ref.set_rays(np.concatenate([src, rr]), t, tick_time)
+        ref.trace(); ref.deposit(); ref.merge(); ref.update()
+        for i in range(R + (1 if len(rr) else 0)):
+            mark[ref.ray_hits(i)[0]] = t
+        snap(a)
+        rays_src.append(src); rays_rec.append(rr); rec_ipar.append(em); rec_type.append(ty)
+    for k in keys:
+        out["he_rec_b_" + k] = np.stack(b[k])
+        out["he_rec_a_" + k] = np.stack(a[k])
+    out["he_rec_rays"] = np.stack(rays_src)
+    out["he_rec_rec_rays"] = np.concatenate(rays_rec)
+    out["he_rec_rec_ipar"] = np.concatenate(rec_ipar)
+    out["he_rec_rec_type"] = np.concatenate(rec_type)
+    out["he_rec_rec_n"] = np.array([len(x) for x in rays_rec], np.int64)
+    out["he_rec_nrec"] = np.int64(NREC)
+    out["he_rec_seed"] = np.int64(REC_SEED)
+
+
 def main():
     ctx = mp.get_context("spawn")
     out = {"hmf": np.float64(HMF)}
-    for kind in ("iso", "noniso", "euler_iso", "euler_noniso", "he_iso", "he_si", "h_si"):
+    for kind in ("iso", "noniso", "euler_iso", "euler_noniso", "rec_iso", "rec_noniso", "he_iso", "he_si", "h_si",
+                 "he_rec"):
         q = ctx.Queue()
         p = ctx.Process(target=_case, args=(kind, q))
         p.start()

@@ -67,3 +67,53 @@ def test_helium_step_vs_lsoda(kind, units):
         for j, k in enumerate(("lambdaH", "lambdaHeI", "lambdaHeII")):
             assert abs(x[j] - g[f"{kind}_out_{k}"][i]) < 1e-4, (i, k)
         assert abs(x[3] / g[f"{kind}_out_ie"][i] - 1) < 3e-3
+
+
+@pytest.mark.parametrize("kind", ["rec_iso", "rec_noniso"])
+def test_helium_step_not_on_the_spot_vs_lsoda(kind):
+    """Case-A helium with the three species' recombination photons."""
+    import helium
+    from psphray_b200 import api
+    from psphray_b200.units import Units
+    g = load_golden("helium16.npz")
+    iso = kind == "rec_iso"
+    phys = api.Physics(Units(hmf=HMF), isothermal=iso, h_only=False, on_the_spot=False)
+    c = {k: phys.unit(k) for k in ("H_PER_MASS", "MPROTON_OVER_BOLTZMANN", "hmf", "hemf")}
+    for i in range(0, len(g[kind + "_in_lambdaH"]), 6):
+        s = {k: float(g[f"{kind}_in_{k}"][i]) for k in ("lambdaH", "lambdaHeI", "lambdaHeII", "ie", "yGdepHI",
+                                                         "yGdepHeI", "yGdepHeII", "heat", "time", "nH", "T", "yeMET",
+                                                         "yGrecHII", "yGrecHeII", "yGrecHeIII")}
+        x = helium.he_step((s["lambdaH"], s["lambdaHeI"], s["lambdaHeII"], s["ie"]), s["yeMET"], s["yGdepHI"],
+                           s["yGdepHeI"], s["yGdepHeII"], s["heat"], s["time"], s["nH"], s["T"], c, phys.ar_get, iso,
+                           on_the_spot=False, rec0=(s["yGrecHII"], s["yGrecHeII"], s["yGrecHeIII"]))
+        for j, k in enumerate(("lambdaH", "lambdaHeI", "lambdaHeII")):
+            assert abs(x[j] - g[f"{kind}_out_{k}"][i]) < 1e-4, (i, k)
+        assert abs(x[3] / g[f"{kind}_out_ie"][i] - 1) < 3e-3
+        for j, k in enumerate(("yGrecHII", "yGrecHeII", "yGrecHeIII")):
+            assert abs(x[4 + j] - g[f"{kind}_out_{k}"][i]) < 3e-5, (i, k)
+
+
+def test_fixture_helium_recombination_rays_are_the_oracle_emission():
+    import recomb
+    from psphray_b200 import api, fields
+    from psphray_b200.units import Units
+    g = load_golden("helium16.npz")
+    units = Units(hmf=HMF)
+    f = fields.uniform_field(16, 31, units=units)
+    phys = api.Physics(units, isothermal=True, on_the_spot=False, h_only=False)
+    c = {k: phys.unit(k) for k in ("HI_ENERGY", "HEI_ENERGY", "HEII_ENERGY", "BOLTZMANN", "H_PER_MASS",
+                                   "HE_PER_MASS", "MPROTON_OVER_BOLTZMANN", "hmf", "hemf")}
+    ltes = [recomb.lte_table(c[th], c["BOLTZMANN"], (lambda sp: (lambda e: phys.xs_get(sp, e)))(sp))
+            for th, sp in zip(recomb.THRESHOLDS, ("HI", "HeI", "HeII"))]
+    pos = np.asarray(f.pos, np.float32).reshape(-1, 3)
+    off = np.concatenate([[0], np.cumsum(g["he_rec_rec_n"])])
+    for t in range(2, len(off)):
+        b = {k: g["he_rec_b_" + k][t - 1] for k in ("lambdaH", "lambdaHeI", "lambdaHeII", "ie", "yg0", "yg1", "yg2",
+                                                     "mark")}
+        rays, em, ty, ygs = recomb.emit([b["yg0"], b["yg1"], b["yg2"]], b["lambdaH"], b["mark"], pos, f.mass, b["ie"],
+                                        t, int(g["he_rec_nrec"]), int(g["he_rec_seed"]), f.boxsize, c, lte=ltes,
+                                        l1=b["lambdaHeI"], l2=b["lambdaHeII"], types=True)
+        sl = slice(off[t - 1], off[t])
+        assert np.array_equal(rays, g["he_rec_rec_rays"][sl])
+        assert np.array_equal(em, g["he_rec_rec_ipar"][sl]) and np.array_equal(ty, g["he_rec_rec_type"][sl])
+        assert np.all(b["mark"][em] == t - 1)

@@ -38,24 +38,28 @@ def lte(phys_rec):
     return recomb.lte_table(c["HI_ENERGY"], c["BOLTZMANN"], lambda e: phys_rec.xs_get("HI", e), weights=True)
 
 
-def test_lte_tables_vs_reference(reference, phys_rec, lte):
+@pytest.mark.parametrize("species", [0, 1, 2])
+def test_lte_tables_vs_reference(reference, phys_rec, species):
+    """lte_fill() of the three species (HI, HeI, HeII recombinations)."""
     import recomb
     reference.lte_init()
-    freq, cdf, wt = lte
+    c = _consts(phys_rec)
+    th = [c["HI_ENERGY"], phys_rec.unit("HEI_ENERGY"), phys_rec.unit("HEII_ENERGY")][species]
+    sp = ("HI", "HeI", "HeII")[species]
+    freq, cdf, wt = recomb.lte_table(th, c["BOLTZMANN"], lambda e: phys_rec.xs_get(sp, e), weights=True)
     for row in range(recomb.NLOGT):
-        f, w = reference.lte_row(row)
+        f, w = reference.lte_row(row, species)
         assert np.max(np.abs(f - freq) / freq) < 1e-15
         assert np.array_equal(w > 0, wt[row] > 0)
         big = w > 1e-290
         assert np.max(np.abs(wt[row][big] - w[big]) / w[big]) < 1e-11
-    c = _consts(phys_rec)
-    fstep = (16.0 * c["HI_ENERGY"] - c["HI_ENERGY"]) / recomb.NFREQ
-    rng = np.random.default_rng(2)
-    for _ in range(2000):
+    fstep = (16.0 * th - th) / recomb.NFREQ
+    rng = np.random.default_rng(2 + species)
+    for _ in range(1000):
         logT, u = rng.uniform(2.5, 10.5), rng.uniform()
         row = min(max(int((logT - 3.0) / (7.0 / recomb.NLOGT)), 0), recomb.NLOGT - 1)
-        mine = c["HI_ENERGY"] + fstep * recomb.lte_index(cdf[row], u)
-        assert abs(mine - reference.lte_gen_freq(logT, u)) <= 1e-12 * mine
+        mine = th + fstep * recomb.lte_index(cdf[row], u)
+        assert abs(mine - reference.lte_gen_freq(logT, u, species)) <= 1e-12 * mine
 
 
 def test_iso_closed_form_vs_implicit(phys_rec):
