@@ -131,8 +131,7 @@ int psg_secion_table_build(const psg_units *u, double *out);
 
 /* Upload units, tables and flags. Must precede psg_load_particles() (the
  * ye block is split into hydrogen, helium and metal electrons at load with
- * the HOnly flag set then). Helium (h_only = 0) ticks use the adaptive
- * integrator (euler = 1 is accepted by psg_step_evolve only). */
+ * the HOnly flag set then). */
 int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_rate_table *ar,
 		const psg_xs_table *xs, const double *kernel, int kernel_n, const psg_flags *flags);
 

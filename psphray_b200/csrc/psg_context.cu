@@ -71,13 +71,15 @@ extern "C" int psg_create(psg_context **out, int device) {
 static void free_particles(psg_context *ctx) {
 	void *ptrs[] = {ctx->d_psml, ctx->d_mass, ctx->d_rho, ctx->d_yeMET, ctx->d_ie, ctx->d_flag,
 		ctx->d_lambdaH, ctx->d_hits, ctx->d_lasthit, ctx->d_hstep, ctx->d_order, ctx->d_gcarry, ctx->d_ygrec,
-		ctx->d_srcmark, ctx->d_lamHeI, ctx->d_lamHeII, ctx->d_ygrecHe1, ctx->d_ygrecHe2};
+		ctx->d_srcmark, ctx->d_lamHeI, ctx->d_lamHeII, ctx->d_ygrecHe1, ctx->d_ygrecHe2, ctx->d_gcarryHe1,
+		ctx->d_gcarryHe2};
 	for (void *p : ptrs) if (p) cudaFree(p);
 	ctx->d_psml = nullptr; ctx->d_mass = ctx->d_rho = ctx->d_yeMET = ctx->d_ie = nullptr;
 	ctx->d_flag = nullptr; ctx->d_lambdaH = nullptr; ctx->d_hits = nullptr; ctx->d_lasthit = nullptr;
 	ctx->d_hstep = nullptr; ctx->d_order = nullptr; ctx->d_gcarry = nullptr; ctx->d_ygrec = nullptr;
 	ctx->d_srcmark = nullptr; ctx->d_lamHeI = ctx->d_lamHeII = nullptr;
 	ctx->d_ygrecHe1 = ctx->d_ygrecHe2 = nullptr;
+	ctx->d_gcarryHe1 = ctx->d_gcarryHe2 = nullptr;
 	ctx->rec_last = ctx->rec_last_R = 0;
 	ctx->n = 0;
 }
@@ -302,6 +304,8 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMalloc(&ctx->d_lamHeII, sizeof(double) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_ygrecHe1, sizeof(float) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_ygrecHe2, sizeof(float) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_gcarryHe1, sizeof(double) * n));
+	PSG_CUDA(cudaMalloc(&ctx->d_gcarryHe2, sizeof(double) * n));
 	float *d_pos = (float *)psg_scratch(ctx, S_MISC, sizeof(float) * n * 7);
 	if (!d_pos) return PSG_E_NOMEM;
 	float *d_sml = d_pos + 3 * n, *d_xHI = d_pos + 4 * n, *d_ye = d_pos + 5 * n;
@@ -322,6 +326,8 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	PSG_CUDA(cudaMemsetAsync(ctx->d_ygrec, 0, sizeof(float) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_ygrecHe1, 0, sizeof(float) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_ygrecHe2, 0, sizeof(float) * n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_gcarryHe1, 0, sizeof(double) * n, s));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_gcarryHe2, 0, sizeof(double) * n, s));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_srcmark, 0xff, sizeof(int32_t) * n, s));
 	const int bs = 256;
 	k_init_particles<<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(n, d_pos, d_sml, d_xHI, d_ye,
@@ -376,7 +382,8 @@ int psg_permute_particles(psg_context *ctx, const uint32_t *g) {
 			(rc = permute_array(ctx, ctx->d_gcarry, g)) || (rc = permute_array(ctx, ctx->d_ygrec, g)) ||
 			(rc = permute_array(ctx, ctx->d_srcmark, g)) || (rc = permute_array(ctx, ctx->d_lamHeI, g)) ||
 			(rc = permute_array(ctx, ctx->d_lamHeII, g)) || (rc = permute_array(ctx, ctx->d_ygrecHe1, g)) ||
-			(rc = permute_array(ctx, ctx->d_ygrecHe2, g)))
+			(rc = permute_array(ctx, ctx->d_ygrecHe2, g)) || (rc = permute_array(ctx, ctx->d_gcarryHe1, g)) ||
+			(rc = permute_array(ctx, ctx->d_gcarryHe2, g)))
 		return rc;
 	// the caller index of every new position: through the previous order
 	const size_t n = ctx->n;

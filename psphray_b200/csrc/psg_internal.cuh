@@ -75,6 +75,7 @@ struct psg_context {
 	double *d_gcarry = nullptr;  // absorbed photons per H left over by an explicit step
 	float *d_ygrec = nullptr;    // yGrecHII: recombination photons per H not yet emitted
 	float *d_ygrecHe1 = nullptr, *d_ygrecHe2 = nullptr;  // yGrecHeII, yGrecHeIII (per He)
+	double *d_gcarryHe1 = nullptr, *d_gcarryHe2 = nullptr;  // helium photons left by an explicit step
 	double *d_lamHeI = nullptr, *d_lamHeII = nullptr;  // x_HeI, x_HeII (with helium or
 	                             // secondary ionisation; 0 with HOnly)
 	int32_t *d_srcmark = nullptr; // last tick a source ray (or the tick's first recombination

@@ -51,6 +51,7 @@ struct PhysParams {
 	double HE_PER_MASS, HEI_ENERGY, HEII_ENERGY;
 	double *lamHeI, *lamHeII;
 	float *ygrecHe1, *ygrecHe2;   // yGrecHeII, yGrecHeIII, when not on the spot
+	double *gcarry, *gcarryHe1, *gcarryHe2;   // photons an explicit step left (helium ticks)
 	const double *si;      // [3][PSG_SECION_NE][PSG_SECION_NX]: PhiHI, PhiHeI, Eh
 	double si_min1, si_step1, si_step1_inv, si_min2, si_step2, si_step2_inv;
 };

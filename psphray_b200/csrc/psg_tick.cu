@@ -66,6 +66,9 @@ PhysParams psg_phys_params(const psg_context *ctx) {
 	P.lamHeII = ctx->d_lamHeII;
 	P.ygrecHe1 = ctx->flags.on_the_spot ? nullptr : ctx->d_ygrecHe1;
 	P.ygrecHe2 = ctx->flags.on_the_spot ? nullptr : ctx->d_ygrecHe2;
+	P.gcarry = ctx->d_gcarry;
+	P.gcarryHe1 = ctx->d_gcarryHe1;
+	P.gcarryHe2 = ctx->d_gcarryHe2;
 	// secion_init() secion.c:75-86
 	P.si = ctx->d_si;
 	P.si_min1 = 10 * ctx->u.EV;
@@ -939,6 +942,11 @@ __global__ void __launch_bounds__(128) k_update_he(int t, const int32_t *__restr
 	}
 	const uint32_t p = act_ipar[a];
 	hits[p] += nh;
+	if (P.euler) {      // photons left over by an earlier explicit step (loop.c:745-747)
+		g0 += P.gcarry[p];
+		g1 += P.gcarryHe1[p];
+		g2 += P.gcarryHe2[p];
+	}
 	HeStep s;
 	s.yeMET = (double)yeMET[p];
 	s.gHI = g0;
@@ -956,7 +964,24 @@ __global__ void __launch_bounds__(128) k_update_he(int t, const int32_t *__restr
 		rec[1] = (double)P.ygrecHe1[p];
 		rec[2] = (double)P.ygrecHe2[p];
 	}
-	const uint32_t st = solve_step_he(P, s, x, P.ygrec ? rec : nullptr);
+	uint32_t st;
+	if (P.euler) {
+		// step_evolve_euler(): no clamps there; update_pars() clamps
+		// (loop.c:759-761) and keeps the unused photons (loop.c:745-747)
+		double remain = 0.0, gain[3] = {0.0, 0.0, 0.0};
+		int refined = 0;
+		st = euler_he(P, s, x, remain, refined, P.ygrec ? gain : nullptr);
+		if (P.ygrec)
+			for (int k = 0; k < 3; k++) rec[k] += gain[k];
+		x[0] = fmax(0.0, fmin(1.0, x[0]));
+		x[1] = fmax(0.0, fmin(1.0, x[1]));
+		x[2] = fmax(0.0, fmin(1.0 - x[1], x[2]));
+		P.gcarry[p] = g0 * remain;
+		P.gcarryHe1[p] = g1 * remain;
+		P.gcarryHe2[p] = g2 * remain;
+	} else {
+		st = solve_step_he(P, s, x, P.ygrec ? rec : nullptr);
+	}
 	lambdaH[p] = x[0];
 	P.lamHeI[p] = x[1];
 	P.lamHeII[p] = x[2];
@@ -1168,8 +1193,6 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 	const bool gen = !ctx->flags.h_only || ctx->flags.secondary_ionization;
 	const bool helium = !ctx->flags.h_only;
 	const int nacc = helium ? 4 : (want_heat ? 2 : 1);
-	if (helium && ctx->flags.euler)
-		return psg_fail(ctx, PSG_E_INVAL, "psg_run_ticks: helium ticks with the explicit solver are not supported");
 
 	ctx->nkev = 0;
 	ctx->launches = 0;

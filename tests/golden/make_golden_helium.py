@@ -23,7 +23,9 @@ writes tests/golden/helium16.npz:
   species' recombination photons, and ticks of helium, isothermal, with the
   recombination rays of all three species (made by the oracle's
   restatement of the device's emission, oracle/recomb.py, from each tick's
-  state) run by the reference's tick phases.
+  state) run by the reference's tick phases;
+- the explicit build (step_evolve_euler()) with helium, isothermal: ticks
+  from the load, the state after each.
 
 The reference keeps its state in globals, so each case runs in a process of
 its own.
@@ -114,6 +116,26 @@ def _case(kind, q):
             out[f"{kind}_out_{k}"] = np.array([getattr(s, k) for s in steps])
     elif kind == "he_rec":
         _rec_ticks(units, f, sch, tick_time, out)
+    elif kind == "he_euler":
+        # the explicit build, helium, isothermal: ticks run freely from the
+        # load (the photons an early-terminated step leaves stay in yGdep*,
+        # loop.c:745-747)
+        ref = Reference(api.RATES_HUI, units, isothermal=True, h_only=False, threads=1, lib_path=EULER_LIB_PATH)
+        ref.load(f)
+        ref.build_tree(8)
+        rec = {k: [] for k in ("lambdaH", "lambdaHeI", "lambdaHeII", "ie", "lasthit", "hits")}
+        rays_all = []
+        for t in range(1, NTICK + 1):
+            rays = sch.rays_for_tick(t)
+            rays_all.append(rays)
+            ref.set_rays(rays, t, tick_time)
+            ref.trace(); ref.deposit(); ref.merge(); ref.update()
+            s, he = ref.state(), ref.he_state()
+            for k in rec:
+                rec[k].append(he[k] if k.startswith("lambdaHe") else s[k])
+        for k in rec:
+            out["he_euler_a_" + k] = np.stack(rec[k])
+        out["he_euler_rays"] = np.stack(rays_all)
     else:
         iso = kind == "he_iso"
         h_only = kind == "h_si"
@@ -215,7 +237,7 @@ def main():
     ctx = mp.get_context("spawn")
     out = {"hmf": np.float64(HMF)}
     for kind in ("iso", "noniso", "euler_iso", "euler_noniso", "rec_iso", "rec_noniso", "he_iso", "he_si", "h_si",
-                 "he_rec"):
+                 "he_rec", "he_euler"):
         q = ctx.Queue()
         p = ctx.Process(target=_case, args=(kind, q))
         p.start()

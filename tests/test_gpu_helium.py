@@ -212,3 +212,34 @@ def test_ticks_helium_recombination_rays():
                 assert np.max(np.abs(mine - g["he_rec_a_" + k][t - 1])) < 3e-5, (t, k)
     finally:
         ctx.close()
+
+
+def test_ticks_helium_euler():
+    """The explicit solver with helium over six ticks from the load: the
+    photons an early-terminated step leaves carried to the next update for
+    each species (loop.c:745-747); hits and lasthit exact, the fractions
+    within 2e-5 of the reference's explicit build."""
+    from psphray_b200 import api, fields
+    from psphray_b200.units import Units
+    g = load_golden("helium16.npz")
+    units = Units(hmf=HMF)
+    f = fields.uniform_field(16, 31, units=units)
+    phys = api.Physics(units, isothermal=True, h_only=False, euler=True)
+    ctx = api.Context(0)
+    try:
+        ctx.set_physics(phys)
+        ctx.load(f)
+        ctx.build_tree(8)
+        rays = g["he_euler_rays"]
+        tt = float(g["tick_time"])
+        for t in range(1, rays.shape[0] + 1):
+            ctx.run_ticks(rays[t - 1], rays.shape[1], 1, t, tt)
+            a, he = ctx.state(), ctx.he_state()
+            assert np.array_equal(a["hits"], g["he_euler_a_hits"][t - 1]), t
+            assert np.array_equal(a["lasthit"], g["he_euler_a_lasthit"][t - 1]), t
+            assert np.max(np.abs(a["lambdaH"] - g["he_euler_a_lambdaH"][t - 1])) < 2e-5, t
+            for k in ("lambdaHeI", "lambdaHeII"):
+                assert np.max(np.abs(he[k] - g["he_euler_a_" + k][t - 1])) < 2e-5, (t, k)
+            assert np.max(np.abs(a["ie"] / g["he_euler_a_ie"][t - 1] - 1)) < 1e-4, t
+    finally:
+        ctx.close()
