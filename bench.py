@@ -436,6 +436,31 @@ def main():
     recombination = {"value": r_hits / (r_ms / 1e3), "unit": "hits/s", "ms_per_tick": r_ms / (nrs * T),
                      "rec_rays_per_tick": r_rays / (nrs * T), "steps": nrs, "ticks_per_step": T}
 
+    # helium and secondary ionisation (HOnly = false, hydrogen mass fraction
+    # 0.76): the same particles and rays, three-species deposit with the
+    # secondary-ionisation table and the helium update, on the spot
+    from psphray_b200.units import Units
+    hu = Units(hmf=0.76)
+    hf = dataclasses.replace(w.field, units=hu)
+    hctx = api.Context(dev)
+    hctx.set_stream(stream.cuda_stream)
+    hctx.set_physics(api.Physics(hu, isothermal=w.isothermal, h_only=False, secondary_ionization=True))
+    hctx.load(hf)
+    hctx.build_tree(8)
+    hctx.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
+    h_ms, h_hits = 0.0, 0.0
+    for s in range(1, 1 + nrs):
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = hctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
+        e1.record(stream)
+        e1.synchronize()
+        h_ms += e0.elapsed_time(e1)
+        h_hits += st["hits"]
+    hctx.close()
+    helium = {"value": h_hits / (h_ms / 1e3), "unit": "hits/s", "ms_per_tick": h_ms / (nrs * T),
+              "hmf": 0.76, "secondary_ionization": True, "steps": nrs, "ticks_per_step": T}
+
     # roofline of the dominant kernel group
     peak, peak_kind = peaks()
     dom = max(api.KERNELS, key=lambda k: kms[k])
@@ -477,6 +502,7 @@ def main():
             "clocks": clk,
             "surrogate": surrogate,
             "recombination": recombination,
+            "helium": helium,
             "e2e_device_emission": {"value": em_hits / em_t, "unit": "hits/s", "h2d_bytes_per_step": 0,
                                     "d2h_bytes_per_step": int(lam.nbytes)},
             "e2e": {"value": e2e_hits / e2e_t, "unit": "hits/s",
