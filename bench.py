@@ -289,7 +289,6 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")   # > 126 MB L2
     torch.cuda.synchronize(dev)
 
-    ctx.set_timing(True)
     for s in range(args.warmup):
         ctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
     torch.cuda.synchronize(dev)
@@ -317,16 +316,12 @@ def main():
         active += st["active"]
         per_step.append(round(e0.elapsed_time(e1), 3))
         launches += st["launches"]
-        for k in api.KERNELS:
-            kms[k] += st["kernel_ms"][k]
-            kn[k] += st["kernel_launches"][k]
     torch.cuda.synchronize(dev)
     torch.cuda.nvtx.range_pop()
     clk = clocks.stop()
     t_max, hits_all = reduce_over_ranks(total_ms / 1e3, hits, dist, torch.device("cuda", dev))
     value = hits_all / t_max
     sim_myr = args.steps * T * w.tick_time / w.field.units.MYR
-    ctx.set_timing(False)
 
     # e2e: the public host-buffer call, pinned host rays, result read back;
     # one untimed step first (it sizes the library's host-call buffers)
@@ -460,6 +455,20 @@ def main():
     hctx.close()
     helium = {"value": h_hits / (h_ms / 1e3), "unit": "hits/s", "ms_per_tick": h_ms / (nrs * T),
               "hmf": 0.76, "secondary_ionization": True, "steps": nrs, "ticks_per_step": T}
+
+    # the per-kernel-group breakdown: the same steps again (later ticks) with
+    # the library's per-launch events on -- kept out of the timed steps,
+    # whose launches they would slow
+    ctx.set_timing(True)
+    tp = t1 + (args.steps + 8) * T
+    for i, s in enumerate(range(args.warmup, nsteps)):
+        flush.zero_()
+        st = ctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, tp + i * T, w.tick_time)
+        for k in api.KERNELS:
+            kms[k] += st["kernel_ms"][k]
+            kn[k] += st["kernel_launches"][k]
+    torch.cuda.synchronize(dev)
+    ctx.set_timing(False)
 
     # roofline of the dominant kernel group
     peak, peak_kind = peaks()
