@@ -3,8 +3,9 @@
 // Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
 // SC'11), counter = (draw index within the tick, tick low word, tick high
 // word, stream), key = the 64-bit seed. Streams: 0 source choice, 1 point
-// source direction, 2 spectrum energy, 3 plane source position, 4
-// recombination emitter, 5 recombination direction, 6 recombination energy.
+// source direction, 2 spectrum energy, 3 plane source position, 4 HII
+// recombination emitter, 5 recombination direction, 6 recombination
+// energy, 7 and 8 HeII and HeIII recombination emitters.
 #pragma once
 
 #include <stdint.h>

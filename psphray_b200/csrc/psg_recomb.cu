@@ -6,14 +6,15 @@
 // From the second tick on (loop.c:197), the particles that the previous
 // tick's source rays hit -- and those of that tick's first recombination
 // ray, which merge_pars() loop.c:628-630 counts in as well -- emit nrec
-// rays: each ray draws its particle with weight yGrecHII/xHI (xHI = 0
-// counts as 1e-10, loop.c:207-211), starts at the particle, goes in an
-// isotropic direction for a tenth of twice the box (loop.c:169), carries
-// the particle's recombination photons yGrecHII*NH split evenly over the
+// rays per species (HII; with helium also HeII and HeIII): each ray draws
+// its particle with weight yGrec/xHI (xHI = 0 counts as 1e-10,
+// loop.c:207-211), starts at the particle, goes in an isotropic direction
+// for a tenth of twice the box (loop.c:169), carries the particle's
+// recombination photons yGrec*NH (NHe for helium) split evenly over the
 // rays that drew it (loop.c:305-320), and has an energy drawn from the
-// Lyman-continuum spectrum sigma(E) E^3 exp(-(E - E_HI)/kT) at the
+// species' recombination spectrum sigma(E) E^3 exp(-(E - E_th)/kT) at the
 // particle's temperature (lte.c:60-70). The emitted photons leave the
-// particle's yGrecHII (loop.c:345-356). With nrec < 0 every such particle
+// particle's yGrec (loop.c:345-368). With nrec < 0 every such particle
 // above the recombine threshold emits one ray instead (loop.c:221-230; the
 // reference reaches that branch through a negative epoch nrec); with nrec
 // = 0 none is emitted and the photons stay in yGrecHII (loop.c:180,197).
@@ -22,7 +23,7 @@
 // rays the ticks of a batch run one at a time: emit, then trace, deposit,
 // merge and update the tick's source rays and recombination rays together.
 //
-// Random numbers: psg_philox.cuh, streams 4-6, keyed by the seed of
+// Random numbers: psg_philox.cuh, streams 4-8, keyed by the seed of
 // psg_set_recombination. The reference draws from GSL's MT19937 and its
 // Walker tables (gsl_ran_discrete); the draws here are inverse-CDF draws
 // of the same distributions.
@@ -338,6 +339,8 @@ int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t 
 	double *d_nph = (double *)(ctx->d_counters + 10);
 	PSG_CUDA(cudaMemsetAsync(d_nph, 0, sizeof(double), st));
 	psg_tick_stats acc{}, one{};
+	int sms = 148;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
 	double rec_rays = 0.0;
 	long launches = 0;
 	for (size_t k = 0; k < K; k++) {
@@ -357,7 +360,7 @@ int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t 
 		int rc = psg_run_ticks_core(ctx, buf, R + M, 1, tick, tick_time, &one);
 		if (rc) return rc;
 		const int nmark = (int)(R + (M > 0 ? 1 : 0));
-		k_rec_mark<<<4 * 148, 256, 0, st>>>(nmark, (const int64_t *)ctx->scratch[S_OFFSETS].p,
+		k_rec_mark<<<4 * sms, 256, 0, st>>>(nmark, (const int64_t *)ctx->scratch[S_OFFSETS].p,
 				(const uint32_t *)ctx->scratch[S_HIT_IPAR].p, (int32_t)tick, ctx->d_srcmark);
 		PSG_CHECK_LAUNCH();
 		launches += emit_launches + (long)one.launches + 1;
