@@ -418,6 +418,7 @@ def main():
     nrs = min(3, nsteps - 1)
     rctx.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
     r_ms, r_hits, r_rays = 0.0, 0.0, 0.0
+    torch.cuda.nvtx.range_push("recombination_steps")
     for s in range(1, 1 + nrs):
         e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -427,6 +428,7 @@ def main():
         r_ms += e0.elapsed_time(e1)
         r_hits += st["hits"]
         r_rays += st["rec_rays"]
+    torch.cuda.nvtx.range_pop()
     rctx.close()
     recombination = {"value": r_hits / (r_ms / 1e3), "unit": "hits/s", "ms_per_tick": r_ms / (nrs * T),
                      "rec_rays_per_tick": r_rays / (nrs * T), "steps": nrs, "ticks_per_step": T}
@@ -444,6 +446,7 @@ def main():
     hctx.build_tree(8)
     hctx.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
     h_ms, h_hits = 0.0, 0.0
+    torch.cuda.nvtx.range_push("helium_steps")
     for s in range(1, 1 + nrs):
         e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -452,6 +455,7 @@ def main():
         e1.synchronize()
         h_ms += e0.elapsed_time(e1)
         h_hits += st["hits"]
+    torch.cuda.nvtx.range_pop()
     hctx.close()
     helium = {"value": h_hits / (h_ms / 1e3), "unit": "hits/s", "ms_per_tick": h_ms / (nrs * T),
               "hmf": 0.76, "secondary_ionization": True, "steps": nrs, "ticks_per_step": T}

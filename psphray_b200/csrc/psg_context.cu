@@ -144,10 +144,12 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	if (ctx->d_ar) cudaFree(ctx->d_ar);
 	if (ctx->d_ar_ni) cudaFree(ctx->d_ar_ni);
+	if (ctx->d_ar_all) cudaFree(ctx->d_ar_all);
 	if (ctx->d_xs) cudaFree(ctx->d_xs);
 	if (ctx->d_kernel) cudaFree(ctx->d_kernel);
 	ctx->d_ar = ctx->d_xs = ctx->d_kernel = nullptr;
 	ctx->d_ar_ni = nullptr;
+	ctx->d_ar_all = nullptr;
 	// rows of 16 doubles (one 128-byte line): log T, then the 15 rate columns
 	const size_t nr = (size_t)ar->nrows;
 	static_assert(PSG_AR_NCOLS + 1 == 16, "one rate row is one 128-byte line");
@@ -194,6 +196,27 @@ extern "C" int psg_set_physics(psg_context *ctx, const psg_units *u, const psg_r
 		if (e2 == cudaSuccess) e2 = cudaMemcpy(ctx->d_ar_ni, ni, sizeof(float) * nr * 16, cudaMemcpyHostToDevice);
 		free(ni);
 		PSG_CUDA(e2);
+	}
+	// The helium right-hand side reads up to 15 columns: the same FP32 value
+	// and slope form, a (value, slope) pair per column, one 128-byte row.
+	{
+		float *all = (float *)calloc(nr * 32, sizeof(float));
+		if (!all) return psg_fail(ctx, PSG_E_NOMEM, "psg_set_physics: host allocation failed");
+		for (int c = 0; c < PSG_AR_NCOLS; c++) {
+			double m = 0.0;
+			for (size_t j = 0; j < nr; j++) m = fmax(m, fabs(ar->col[c][j]));
+			ctx->ar_all_scale[c] = m > 0.0 ? m : 1.0;
+			for (size_t j = 0; j < nr; j++) {
+				const double v = ar->col[c][j] / ctx->ar_all_scale[c];
+				const double s = j + 1 < nr ? (ar->col[c][j + 1] / ctx->ar_all_scale[c] - v) * ar->step_inv : 0.0;
+				all[32 * j + 2 * c] = (float)v;
+				all[32 * j + 2 * c + 1] = (float)s;
+			}
+		}
+		cudaError_t e4 = cudaMalloc(&ctx->d_ar_all, sizeof(float) * nr * 32);
+		if (e4 == cudaSuccess) e4 = cudaMemcpy(ctx->d_ar_all, all, sizeof(float) * nr * 32, cudaMemcpyHostToDevice);
+		free(all);
+		PSG_CUDA(e4);
 	}
 	const size_t nx = (size_t)xs->nrows;
 	PSG_CUDA(cudaMalloc(&ctx->d_xs, sizeof(double) * nx * 4));

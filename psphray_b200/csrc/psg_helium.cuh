@@ -60,6 +60,37 @@ __device__ __forceinline__ double ye_he(const PhysParams &P, double lamH, double
 	return (1.0 - lamH) + P.hemf / P.hmf * 0.25 * (l2 + 2 * (1.0 - l2 - l1));
 }
 
+// The rate columns at one log T from the FP32 (value, slope) rows (each
+// column scaled by its largest magnitude): the two-point line of
+// tabfun_get() tabfun.c:38-58 written as value + slope * offset; a column
+// is one 8-byte load.
+struct RateRow {
+	const float2 *row;
+	double du;
+	const double *scale;
+	__device__ __forceinline__ double operator()(int c) const {
+		const float2 vs = row[c];
+		return __fma_rn((double)vs.y, du, (double)vs.x) * scale[c];
+	}
+};
+
+__device__ __forceinline__ RateRow rate_row(const PhysParams &P, double logT) {
+	long long idx = (long long)((logT - P.ar_min) * P.ar_step_inv);
+	RateRow R;
+	if (idx < 0) {
+		idx = 0;
+		R.du = 0.0;
+	} else if (idx >= P.ar_nrows - 1) {
+		idx = P.ar_nrows - 1;
+		R.du = 0.0;
+	} else {
+		R.du = logT - __fma_rn((double)idx, P.ar_step, P.ar_min);
+	}
+	R.row = P.ar_all + 16 * idx;
+	R.scale = P.ar_all_scale;
+	return R;
+}
+
 // One helium step: the Step fields the right-hand side reads.
 struct HeStep {
 	double yeMET, gHI, gHeI, gHeII, heat, time, nH, T;
@@ -77,7 +108,7 @@ __device__ inline void rhs_he(const PhysParams &P, const HeStep &s, const double
 	const double xHeIII = 1.0 - x[2] - x[1];
 	const double ye = (xHII + P.hemf / P.hmf * 0.25 * (xHeII + 2 * xHeIII)) + s.yeMET;
 	const double T = P.isothermal ? s.T : ieye2T(P, x[3], ye);
-	const RateAt R = rates_at(P, log10(T));
+	const RateRow R = rate_row(P, log10(T));
 	const double nH = s.nH, t = s.time;
 	const double gamma_HI = R(PSG_AR_HI_CI) * nH;
 	const double gamma_HeI = R(PSG_AR_HEI_CI) * nH;
@@ -226,11 +257,14 @@ __device__ inline bool rosenbrock_he(const PhysParams &P, const HeStep &s, doubl
 	return t >= 1.0;
 }
 
-// Dormand-Prince 5(4) over the four variables, then the Rosenbrock finish.
-// With rec (not on the spot), rec[3] accumulates the recombination photons
-// as a quadrature over the same stages.
-__device__ inline bool dopri_he(const PhysParams &P, const HeStep &s, double x[4], int max_steps,
-		double *rec = nullptr) {
+// Up to HE_SWITCH Dormand-Prince 5(4) steps over the four variables from
+// s = 0; returns true once s = 1 is reached, else leaves the time reached
+// and the next step size in *t_out, *h_out. With rec (not on the spot),
+// rec[3] accumulates the recombination photons as a quadrature over the
+// same stages.
+template <bool REC>
+__device__ inline bool dopri_he_explicit(const PhysParams &P, const HeStep &s, double x[4], double *rec,
+		double *t_out, double *h_out) {
 	const double a21 = 1. / 5, a31 = 3. / 40, a32 = 9. / 40, a41 = 44. / 45, a42 = -56. / 15, a43 = 32. / 9;
 	const double a51 = 19372. / 6561, a52 = -25360. / 2187, a53 = 64448. / 6561, a54 = -212. / 729;
 	const double a61 = 9017. / 3168, a62 = -355. / 33, a63 = 46732. / 5247, a64 = 49. / 176, a65 = -5103. / 18656;
@@ -239,7 +273,7 @@ __device__ inline bool dopri_he(const PhysParams &P, const HeStep &s, double x[4
 			e7 = -1. / 40;
 	const double atol3 = DP_ATOL1_REL * fabs(x[3]) + 1e-300;
 	double k1[4], r1[3] = {0.0, 0.0, 0.0};
-	rhs_he(P, s, x, k1, rec ? r1 : nullptr);
+	rhs_he(P, s, x, k1, REC ? r1 : nullptr);
 	double h = 1.0;
 	for (int i = 0; i < 4; i++) {
 		const double scale = fabs(x[i]) + (i < 3 ? DP_ATOL0 : atol3) / DP_RTOL;
@@ -252,8 +286,8 @@ __device__ inline bool dopri_he(const PhysParams &P, const HeStep &s, double x[4
 		if (t + h > 1.0) h = 1.0 - t;
 		double k2[4], k3[4], k4[4], k5[4], k6[4], k7[4], y[4], yn[4], e[4];
 		double r2[3], r3[3], r4[3], r5[3], r6[3], r7[3];
-		double *q2 = rec ? r2 : nullptr, *q3 = rec ? r3 : nullptr, *q4 = rec ? r4 : nullptr;
-		double *q5 = rec ? r5 : nullptr, *q6 = rec ? r6 : nullptr, *q7 = rec ? r7 : nullptr;
+		double *q2 = REC ? r2 : nullptr, *q3 = REC ? r3 : nullptr, *q4 = REC ? r4 : nullptr;
+		double *q5 = REC ? r5 : nullptr, *q6 = REC ? r6 : nullptr, *q7 = REC ? r7 : nullptr;
 		for (int i = 0; i < 4; i++) y[i] = x[i] + h * (a21 * k1[i]);
 		rhs_he(P, s, y, k2, q2);
 		for (int i = 0; i < 4; i++) y[i] = x[i] + h * (a31 * k1[i] + a32 * k2[i]);
@@ -276,7 +310,7 @@ __device__ inline bool dopri_he(const PhysParams &P, const HeStep &s, double x[4
 				x[i] = yn[i];
 				k1[i] = k7[i];
 			}
-			if (rec)
+			if (REC)
 				for (int i = 0; i < 3; i++) {
 					rec[i] += h * (b1 * r1[i] + b3 * r3[i] + b4 * r4[i] + b5 * r5[i] + b6 * r6[i]);
 					r1[i] = r7[i];
@@ -285,7 +319,17 @@ __device__ inline bool dopri_he(const PhysParams &P, const HeStep &s, double x[4
 		const double fac = err > 0.0 ? fmin(5.0, fmax(0.2, 0.9 * pow(err, -0.2))) : 5.0;
 		h = fmax(h * fac, 1e-14);
 	}
-	if (t >= 1.0) return true;
+	*t_out = t;
+	*h_out = h;
+	return t >= 1.0;
+}
+
+// Dormand-Prince 5(4) over the four variables, then the Rosenbrock finish.
+__device__ inline bool dopri_he(const PhysParams &P, const HeStep &s, double x[4], int max_steps,
+		double *rec = nullptr) {
+	double t = 0.0, h = 0.0;
+	const bool done = rec ? dopri_he_explicit<true>(P, s, x, rec, &t, &h) : dopri_he_explicit<false>(P, s, x, rec, &t, &h);
+	if (done) return true;
 	return rosenbrock_he(P, s, x, t, h, max_steps, rec);
 }
 
@@ -334,6 +378,13 @@ __device__ inline uint32_t euler_he(const PhysParams &P, const HeStep &s, double
 	}
 	step_remain = 1.0 - (double)((float)k / (float)nsteps);
 	return st;
+}
+
+// LSODA's exit clamps of the fractions (solve.c:208-210).
+__device__ __forceinline__ void clamp_he(double x[4]) {
+	x[0] = fmin(1., fmax(0., x[0]));
+	x[1] = fmin(1., fmax(0., x[1]));
+	x[2] = fmin(1. - x[1], fmax(0., x[2]));
 }
 
 // One helium step of step_evolve() (LSODA's exit clamps, solve.c:208-213):

@@ -53,6 +53,8 @@ struct psg_context {
 	                             // right-hand side, values then slopes per log T
 	double ar_step = 0;
 	double ar_ni_scale[8] = {};  // each d_ar_ni column is stored divided by this
+	float2 *d_ar_all = nullptr;  // [ar_nrows][16]: (value, slope) of all 15 rate columns (helium)
+	double ar_all_scale[PSG_AR_NCOLS] = {};
 	int ar_nrows = 0;
 	double ar_min = 0, ar_step_inv = 0;
 	double *d_xs = nullptr;      // [4][xs_nrows]: energy, sigma_HI, sigma_HeI, sigma_HeII

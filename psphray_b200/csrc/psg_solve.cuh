@@ -35,6 +35,8 @@ struct PhysParams {
 	const float4 *ar_ni;   // [ar_nrows][4]: the right-hand side's 7 rates (+ alpha_B when not
 	                       // on the spot), values and slopes
 	double ar_ni_scale[8]; // ... each column divided by its largest magnitude
+	const float2 *ar_all;  // [ar_nrows][16]: (value, slope) of all 15 columns (helium)
+	double ar_all_scale[PSG_AR_NCOLS];
 	int ar_nrows;
 	double ar_min, ar_step_inv, ar_step;
 	const double *xs;      // [4][xs_nrows]: energy, sigma_HI, sigma_HeI, sigma_HeII

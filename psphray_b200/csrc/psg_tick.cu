@@ -31,6 +31,8 @@ PhysParams psg_phys_params(const psg_context *ctx) {
 	P.ar = ctx->d_ar;
 	P.ar_ni = ctx->d_ar_ni;
 	for (int c = 0; c < 8; c++) P.ar_ni_scale[c] = ctx->ar_ni_scale[c];
+	P.ar_all = ctx->d_ar_all;
+	for (int c = 0; c < PSG_AR_NCOLS; c++) P.ar_all_scale[c] = ctx->ar_all_scale[c];
 	P.ar_step = ctx->ar_step;
 	P.ar_nrows = ctx->ar_nrows;
 	P.ar_min = ctx->ar_min;
@@ -918,13 +920,39 @@ __global__ void __launch_bounds__(128) k_update_euler(int t, const int32_t *__re
 // update_pars() loop.c:647-776 with helium: one thread per active particle
 // of the tick sums its deposits (yGdepHI, heat, yGdepHeI, yGdepHeII, in slot
 // order) and integrates the four variables; isothermal, ie follows T at the
-// new ye (loop.c:764-766).
-__global__ void __launch_bounds__(128) k_update_he(int t, const int32_t *__restrict__ tick_act,
+// new ye (loop.c:764-766). A particle still unfinished after the explicit
+// steps goes to k_update_he_stiff (the Rosenbrock finish), which keeps the
+// W-method's registers out of this kernel.
+struct HeStiffItem {
+	HeStep s;
+	double x[4], rec[3], t, h;
+	uint32_t p;
+};
+
+// The step's results into the particle (update_pars() loop.c:756-768).
+__device__ __forceinline__ void he_write(const PhysParams &P, uint32_t p, const double x[4], const double rec[3],
+		double T, int64_t tick, double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit) {
+	lambdaH[p] = x[0];
+	P.lamHeI[p] = x[1];
+	P.lamHeII[p] = x[2];
+	if (P.ygrec) {
+		P.ygrec[p] = (float)rec[0];
+		P.ygrecHe1[p] = (float)rec[1];
+		P.ygrecHe2[p] = (float)rec[2];
+	}
+	if (P.isothermal) ie[p] = (float)Tye2ie(P, T, ye_he(P, x[0], x[1], x[2]));
+	else if (!P.adiabatic) ie[p] = (float)x[3];
+	lasthit[p] = tick;
+}
+
+template <bool REC>
+__global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg, const double *__restrict__ acc,
 		const double *__restrict__ acc_heat, const double *__restrict__ acc_he, size_t hb, int want_heat,
 		int32_t *__restrict__ hits, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P,
-		int64_t tick, double tick_time, uint32_t *__restrict__ status) {
+		int64_t tick, double tick_time, HeStiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff,
+		uint32_t *__restrict__ status) {
 	const int a = tick_act[t] + blockIdx.x * blockDim.x + threadIdx.x;
 	if (a >= tick_act[t + 1]) return;
 	const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
@@ -958,13 +986,13 @@ __global__ void __launch_bounds__(128) k_update_he(int t, const int32_t *__restr
 	const double ie0 = (double)ie[p];
 	s.T = ieye2T(P, ie0, ye_he(P, lambdaH[p], P.lamHeI[p], P.lamHeII[p]));     // psys_T()
 	double x[4] = {lambdaH[p], P.lamHeI[p], P.lamHeII[p], ie0};
-	double rec[3];
+	double rec[3] = {0.0, 0.0, 0.0};
 	if (P.ygrec) {
 		rec[0] = (double)P.ygrec[p];
 		rec[1] = (double)P.ygrecHe1[p];
 		rec[2] = (double)P.ygrecHe2[p];
 	}
-	uint32_t st;
+	uint32_t st = 0;
 	if (P.euler) {
 		// step_evolve_euler(): no clamps there; update_pars() clamps
 		// (loop.c:759-761) and keeps the unused photons (loop.c:745-747)
@@ -980,19 +1008,49 @@ __global__ void __launch_bounds__(128) k_update_he(int t, const int32_t *__restr
 		P.gcarryHe1[p] = g1 * remain;
 		P.gcarryHe2[p] = g2 * remain;
 	} else {
-		st = solve_step_he(P, s, x, P.ygrec ? rec : nullptr);
+		double gain[3] = {0.0, 0.0, 0.0}, tt = 0.0, hh = 0.0;
+		if (!dopri_he_explicit<REC>(P, s, x, gain, &tt, &hh)) {
+			HeStiffItem it;
+			it.s = s;
+			for (int k = 0; k < 4; k++) it.x[k] = x[k];
+			for (int k = 0; k < 3; k++) it.rec[k] = rec[k] + gain[k];
+			it.t = tt;
+			it.h = hh;
+			it.p = p;
+			stiff[atomicAdd(nstiff, 1u)] = it;
+			return;
+		}
+		if (!(x[3] >= 0.0)) st |= PSG_ST_IE_NEG;
+		for (int k = 0; k < 4; k++)
+			if (!isfinite(x[k])) st |= PSG_ST_NAN;
+		clamp_he(x);
+		if (P.ygrec)
+			for (int k = 0; k < 3; k++) rec[k] = fmax(0.0, rec[k] + gain[k]);
 	}
-	lambdaH[p] = x[0];
-	P.lamHeI[p] = x[1];
-	P.lamHeII[p] = x[2];
-	if (P.ygrec) {
-		P.ygrec[p] = (float)rec[0];
-		P.ygrecHe1[p] = (float)rec[1];
-		P.ygrecHe2[p] = (float)rec[2];
+	he_write(P, p, x, rec, s.T, tick, lambdaH, ie, lasthit);
+	if (st) atomicOr(status, st);
+}
+
+// The stiff helium particles of a tick, one thread each (their number is
+// read on the device): the Rosenbrock finish from where the explicit steps
+// stopped.
+__global__ void __launch_bounds__(64) k_update_he_stiff(const HeStiffItem *__restrict__ stiff,
+		const unsigned *__restrict__ nstiff, double *__restrict__ lambdaH, float *__restrict__ ie,
+		int64_t *__restrict__ lasthit, PhysParams P, int64_t tick, uint32_t *__restrict__ status) {
+	const unsigned n = *nstiff;
+	uint32_t st = 0;
+	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		const HeStiffItem &it = stiff[i];
+		double x[4] = {it.x[0], it.x[1], it.x[2], it.x[3]};
+		double gain[3] = {0.0, 0.0, 0.0}, rec[3];
+		if (!rosenbrock_he(P, it.s, x, it.t, it.h, UPD_MAX_STEPS, P.ygrec ? gain : nullptr)) st |= PSG_ST_SOLVER;
+		if (!(x[3] >= 0.0)) st |= PSG_ST_IE_NEG;
+		for (int k = 0; k < 4; k++)
+			if (!isfinite(x[k])) st |= PSG_ST_NAN;
+		clamp_he(x);
+		for (int k = 0; k < 3; k++) rec[k] = fmax(0.0, it.rec[k] + gain[k]);
+		he_write(P, it.p, x, rec, it.s.T, tick, lambdaH, ie, lasthit);
 	}
-	if (P.isothermal) ie[p] = (float)Tye2ie(P, s.T, ye_he(P, x[0], x[1], x[2]));
-	else if (!P.adiabatic) ie[p] = (float)x[3];
-	lasthit[p] = tick;
 	if (st) atomicOr(status, st);
 }
 
@@ -1289,7 +1347,11 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 	PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * 3 * (K + 1), st));
 	if (surr) PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 8, 0, sizeof(unsigned long long), st));
 	UpdRec *urec = nullptr;
-	if (!iso || euler) {
+	HeStiffItem *hstiff = nullptr;      // helium: the stiff particles of a tick
+	if (helium) {
+		hstiff = (HeStiffItem *)psg_scratch(ctx, S_REC, sizeof(HeStiffItem) * maxt);
+		if (!hstiff) return PSG_E_NOMEM;
+	} else if (!iso || euler) {
 		urec = (UpdRec *)psg_scratch(ctx, S_REC, sizeof(UpdRec) * maxt);
 		if (!urec) return PSG_E_NOMEM;
 	}
@@ -1340,11 +1402,21 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 		const int nact_t = h_tick_act[t + 1] - h_tick_act[t];
 		psg_mark_begin(ctx, PSG_K_UPDATE);
 		if (nact_t > 0 && helium) {
-			k_update_he<<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat,
-					acc_he, hb, want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
-					ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, ctx->d_status);
+			if (P.ygrec)
+				k_update_he<true><<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
+						acc_heat, acc_he, hb, want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
+						ctx->d_rho, ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, hstiff, nstiff + t,
+						ctx->d_status);
+			else
+				k_update_he<false><<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
+						acc_heat, acc_he, hb, want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
+						ctx->d_rho, ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, hstiff, nstiff + t,
+						ctx->d_status);
 			PSG_CHECK_LAUNCH();
-			ctx->launches++;
+			k_update_he_stiff<<<dev_sms, 64, 0, st>>>(hstiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
+					P, first_tick + (int64_t)t, ctx->d_status);
+			PSG_CHECK_LAUNCH();
+			ctx->launches += 2;
 		} else if (nact_t > 0) {
 			const int64_t tick = first_tick + (int64_t)t;
 			const int nl = h_tick_long[t + 1] - h_tick_long[t];
