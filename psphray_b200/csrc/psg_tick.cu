@@ -171,12 +171,28 @@ __device__ __forceinline__ void group_sync(int bar) {
 	else asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(NT) : "memory");
 }
 
+// One hit's deposits sit together, nacc doubles per slot (photons/NH; with
+// heat the heat; with helium yGdepHeI and yGdepHeII), so that the scattered
+// store of a hit touches one 32-byte sector and the by-particle sums read
+// one contiguous run.
+__device__ __forceinline__ void acc_store(double *__restrict__ acc, int nacc, uint32_t s, double y, double heat,
+		double y1, double y2) {
+	if (nacc == 4) {
+		double2 *a = reinterpret_cast<double2 *>(acc) + 2 * (size_t)s;
+		a[0] = make_double2(y, heat);
+		a[1] = make_double2(y1, y2);
+	} else if (nacc == 2) {
+		reinterpret_cast<double2 *>(acc)[s] = make_double2(y, heat);
+	} else {
+		acc[s] = y;
+	}
+}
+
 template <int NT>
 __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern, const uint32_t *__restrict__ slot,
 		const double *__restrict__ lambdaH, const float *__restrict__ mass, const PhysParams &P, int want_heat,
-		double *__restrict__ acc, double *__restrict__ acc_heat, DepShared &sh, unsigned &nsat, double &lost,
-		int bar) {
+		double *__restrict__ acc, DepShared &sh, unsigned &nsat, double &lost, int bar) {
 	const int lane = t & 31, wid = t >> 5;
 	constexpr int NW = NT / 32;
 	const double Nph = ray.Nph;
@@ -293,8 +309,8 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 			group_sync<NT>(bar);
 		}
 		if (valid) {
-			acc[slot_c] = delta;
-			if (want_heat) acc_heat[slot_c] = delta >= 0.0 ? rn_dmul(heat_factor, delta) : 0.0;
+			acc_store(acc, want_heat ? 2 : 1, slot_c, delta,
+					want_heat && delta >= 0.0 ? rn_dmul(heat_factor, delta) : 0.0, 0.0, 0.0);
 		}
 	}
 	if (t == 0 && !skip_ray) lost += TM;
@@ -303,16 +319,15 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 // The same with helium and/or secondary ionisation (loop.c:409-567): the
 // scan runs over the sum of the three species' optical depths; a hit
 // absorbs tau_s/tausum of the photons per species, each capped at its
-// atoms (loop.c:476-505); it writes yGdepHI (acc), heat, yGdepHeI and
-// yGdepHeII (acc_he, acc_he + hb) increments, with the secondary
+// atoms (loop.c:476-505); it writes yGdepHI, heat, yGdepHeI and yGdepHeII
+// increments (nacc of them per slot), with the secondary
 // ionisation and heating of loop.c:513-552 (whose HeII terms the
 // reference's statements drop, loop.c:523,542).
 template <int NT>
 __device__ void deposit_ray_gen(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern, const uint32_t *__restrict__ slot,
 		const double *__restrict__ lambdaH, const float *__restrict__ mass, const PhysParams &P, int want_heat,
-		double *__restrict__ acc, double *__restrict__ acc_heat, double *__restrict__ acc_he, size_t hb,
-		DepShared &sh, unsigned &nsat, double &lost, int bar) {
+		double *__restrict__ acc, int nacc, DepShared &sh, unsigned &nsat, double &lost, int bar) {
 	const int lane = t & 31, wid = t >> 5;
 	constexpr int NW = NT / 32;
 	const double Nph = ray.Nph;
@@ -491,12 +506,7 @@ __device__ void deposit_ray_gen(const psg_ray &ray, int64_t h0, int64_t h1, int 
 					}
 				}
 			}
-			acc[slot_c] = y0;
-			if (want_heat) acc_heat[slot_c] = heat;
-			if (acc_he) {
-				acc_he[slot_c] = y1;
-				acc_he[hb + slot_c] = y2;
-			}
+			acc_store(acc, nacc, slot_c, y0, heat, y1, y2);
 		}
 	}
 	if (t == 0 && !skip_ray) lost += TM;
@@ -515,8 +525,8 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 		const uint32_t *__restrict__ short_rays, int nshort,
 		const int64_t *__restrict__ off, const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
 		const uint32_t *__restrict__ slot, const double *__restrict__ lambdaH, const float *__restrict__ mass,
-		PhysParams P, int want_heat, double *__restrict__ acc, double *__restrict__ acc_heat,
-		double *__restrict__ acc_he, size_t hb, unsigned long long *__restrict__ n_sat, double *__restrict__ lost) {
+		PhysParams P, int want_heat, double *__restrict__ acc, int nacc, unsigned long long *__restrict__ n_sat,
+		double *__restrict__ lost) {
 	__shared__ DepShared sh_block;
 	__shared__ DepShared sh_quarter[4];
 	__shared__ DepShared sh_warp[DEP_THREADS / 32];
@@ -528,10 +538,10 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 		const uint32_t r = long_rays[blockIdx.x];
 		if (GEN)
 			deposit_ray_gen<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
-					want_heat, acc, acc_heat, acc_he, hb, sh_block, nsat, tm_lost, 0);
+					want_heat, acc, nacc, sh_block, nsat, tm_lost, 0);
 		else
 			deposit_ray<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
-					want_heat, acc, acc_heat, sh_block, nsat, tm_lost, 0);
+					want_heat, acc, sh_block, nsat, tm_lost, 0);
 	} else if ((int)blockIdx.x < nlong + nmid_blocks) {
 		const int q = tid >> 7;
 		const int m = ((int)blockIdx.x - nlong) * 4 + q;
@@ -539,10 +549,10 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 			const uint32_t r = mid_rays[m];
 			if (GEN)
 				deposit_ray_gen<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
-						want_heat, acc, acc_heat, acc_he, hb, sh_quarter[q], nsat, tm_lost, 1 + q);
+						want_heat, acc, nacc, sh_quarter[q], nsat, tm_lost, 1 + q);
 			else
 				deposit_ray<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
-						want_heat, acc, acc_heat, sh_quarter[q], nsat, tm_lost, 1 + q);
+						want_heat, acc, sh_quarter[q], nsat, tm_lost, 1 + q);
 		}
 	} else {
 		const int w = ((int)blockIdx.x - nlong - nmid_blocks) * (DEP_THREADS / 32) + wid;
@@ -551,10 +561,10 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 			if (off[r + 1] > off[r]) {
 				if (GEN)
 					deposit_ray_gen<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
-							want_heat, acc, acc_heat, acc_he, hb, sh_warp[wid], nsat, tm_lost, 0);
+							want_heat, acc, nacc, sh_warp[wid], nsat, tm_lost, 0);
 				else
 					deposit_ray<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
-							want_heat, acc, acc_heat, sh_warp[wid], nsat, tm_lost, 0);
+							want_heat, acc, sh_warp[wid], nsat, tm_lost, 0);
 			}
 		}
 	}
@@ -677,7 +687,7 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 template <bool ISO, bool REC>
 __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
-		const double *__restrict__ acc, const double *__restrict__ acc_heat, int want_heat,
+		const double *__restrict__ acc, int want_heat,
 		const uint32_t *__restrict__ long_act, int nlong, int long_blocks,
 		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat,
 		double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit,
@@ -693,17 +703,33 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		double sg = 0.0, sh = 0.0;
 		int sn = 0;
 		uint32_t k = b0 + lane;
-		for (; k + 7 * 32 < b1; k += 8 * 32) {
-			double v[8];
+		if (want_heat) {
+			const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
+			for (; k + 7 * 32 < b1; k += 8 * 32) {
+				double2 v[8];
 #pragma unroll
-			for (int u = 0; u < 8; u++) v[u] = acc[k + 32 * u];
+				for (int u = 0; u < 8; u++) v[u] = acc2[k + 32 * u];
 #pragma unroll
-			for (int u = 0; u < 8; u++)
-				if (v[u] >= 0.0) { sg += v[u]; if (want_heat) sh += acc_heat[k + 32 * u]; sn++; }
-		}
-		for (; k < b1; k += 32) {
-			const double d = acc[k];
-			if (d >= 0.0) { sg += d; if (want_heat) sh += acc_heat[k]; sn++; }
+				for (int u = 0; u < 8; u++)
+					if (v[u].x >= 0.0) { sg += v[u].x; sh += v[u].y; sn++; }
+			}
+			for (; k < b1; k += 32) {
+				const double2 d = acc2[k];
+				if (d.x >= 0.0) { sg += d.x; sh += d.y; sn++; }
+			}
+		} else {
+			for (; k + 7 * 32 < b1; k += 8 * 32) {
+				double v[8];
+#pragma unroll
+				for (int u = 0; u < 8; u++) v[u] = acc[k + 32 * u];
+#pragma unroll
+				for (int u = 0; u < 8; u++)
+					if (v[u] >= 0.0) { sg += v[u]; sn++; }
+			}
+			for (; k < b1; k += 32) {
+				const double d = acc[k];
+				if (d >= 0.0) { sg += d; sn++; }
+			}
 		}
 #pragma unroll
 		for (int o = 16; o > 0; o >>= 1) {
@@ -723,8 +749,13 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 	double g = 0.0, heat = 0.0;
 	int nh = 0;
 	for (uint32_t k = s0; k < s1; k++) {
-		const double d = acc[k];
-		if (d >= 0.0) { g += d; if (want_heat) heat += acc_heat[k]; nh++; }
+		if (want_heat) {
+			const double2 d = reinterpret_cast<const double2 *>(acc)[k];
+			if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
+		} else {
+			const double d = acc[k];
+			if (d >= 0.0) { g += d; nh++; }
+		}
 	}
 	finish_particle<ISO, REC>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET, hstep,
 			rec, tick_act[t], gcarry, P, tick, tick_time, status);
@@ -948,7 +979,7 @@ __device__ __forceinline__ void he_write(const PhysParams &P, uint32_t p, const 
 template <bool REC>
 __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg, const double *__restrict__ acc,
-		const double *__restrict__ acc_heat, const double *__restrict__ acc_he, size_t hb, int want_heat,
+		int want_heat,
 		int32_t *__restrict__ hits, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P,
 		int64_t tick, double tick_time, HeStiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff,
@@ -958,13 +989,15 @@ __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__re
 	const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
 	double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
 	int nh = 0;
+	const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
 	for (uint32_t k = s0; k < s1; k++) {
-		const double d = acc[k];
-		if (d >= 0.0) {
-			g0 += d;
-			g1 += acc_he[k];
-			g2 += acc_he[hb + k];
-			if (want_heat) heat += acc_heat[k];
+		const double2 a = acc2[2 * (size_t)k];
+		if (a.x >= 0.0) {
+			const double2 b = acc2[2 * (size_t)k + 1];
+			g0 += a.x;
+			g1 += b.x;
+			g2 += b.y;
+			if (want_heat) heat += a.y;
 			nh++;
 		}
 	}
@@ -1277,8 +1310,6 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 		: build_slots<unsigned long long>(ctx, nray, R, K, nhit, shift, tbits, off64, hit_ipar, nacc, &nact);
 	if (rc2) return rc2;
 	double *acc = (double *)ctx->scratch[S_ACC].p;
-	double *acc_heat = (want_heat || helium) ? acc + hb : nullptr;
-	double *acc_he = helium ? acc + 2 * hb : nullptr;
 	uint32_t *slot = (uint32_t *)ctx->scratch[S_SLOT].p;
 	char *actm = (char *)ctx->scratch[S_ACT].p;
 	int32_t *head = (int32_t *)actm;
@@ -1392,11 +1423,11 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 		if (grid && gen)
 			k_deposit<true><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0, nmid,
 					short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
-					want_heat, acc, acc_heat, acc_he, hb, d_nsat, d_lost);
+					want_heat, acc, nacc, d_nsat, d_lost);
 		else if (grid)
 			k_deposit<false><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0, nmid,
 					short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
-					want_heat, acc, acc_heat, nullptr, hb, d_nsat, d_lost);
+					want_heat, acc, nacc, d_nsat, d_lost);
 		PSG_CHECK_LAUNCH();
 		psg_mark_end(ctx);
 		const int nact_t = h_tick_act[t + 1] - h_tick_act[t];
@@ -1404,12 +1435,12 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 		if (nact_t > 0 && helium) {
 			if (P.ygrec)
 				k_update_he<true><<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
-						acc_heat, acc_he, hb, want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
+						want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
 						ctx->d_rho, ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, hstiff, nstiff + t,
 						ctx->d_status);
 			else
 				k_update_he<false><<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
-						acc_heat, acc_he, hb, want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
+						want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
 						ctx->d_rho, ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, hstiff, nstiff + t,
 						ctx->d_status);
 			PSG_CHECK_LAUNCH();
@@ -1424,7 +1455,7 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 			const unsigned rgrid = (unsigned)(lb + (int)blocks(nact_t, 256));
 			const double *gcarry = euler ? ctx->d_gcarry : nullptr;
 #define PSG_REDUCE(ISO_, REC_)                                                                              \
-	k_reduce<ISO_, REC_><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, acc_heat, want_heat, \
+	k_reduce<ISO_, REC_><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, want_heat, \
 			long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,        \
 			ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, tick, tick_time,          \
 			ctx->d_status)
