@@ -43,12 +43,15 @@ REF_TICKS = {"iliev32": 40, "iliev64": 4, "lognormal128": 1}   # per step of --i
 # mass 4 + FP64 absorbed photons 8. Per kernel group, per unit it processes:
 # trace fill reads pos+sml (16) and writes (ipar 4, d 8, b 8) per hit; the
 # sort reads and writes (ipar, d, b) and writes the kernel value; slots read
-# ipar and write a slot per hit; deposit reads the slot's particle state and
-# writes an FP64 sum per hit; the update reads ~60 B and writes ~40 B of
-# particle state per active (tick, particle) pair.
+# ipar and write a slot per hit; deposit reads (ipar 4, kern 8, slot 4) and
+# the hit particle's lambdaH 8 and mass 4 and writes an FP64 deposit per hit
+# (36 B), plus an FP64 heat when not isothermal (DEPOSIT_HEAT_BYTES); the
+# update reads ~60 B and writes ~40 B of particle state per active (tick,
+# particle) pair.
 BYTES_PER_HIT = 36
 GROUP_BYTES = {"trace_count": (16, "hit"), "trace_fill": (36, "hit"), "sort": (60, "hit"),
-               "slots": (48, "hit"), "deposit": (32, "hit"), "update": (100, "active particle")}
+               "slots": (48, "hit"), "deposit": (36, "hit"), "update": (100, "active particle")}
+DEPOSIT_HEAT_BYTES = 8
 
 
 def peaks():
@@ -478,6 +481,8 @@ def main():
     peak, peak_kind = peaks()
     dom = max(api.KERNELS, key=lambda k: kms[k])
     unit_bytes, unit_name = GROUP_BYTES[dom]
+    if dom == "deposit" and not w.isothermal:
+        unit_bytes += DEPOSIT_HEAT_BYTES
     units = active if unit_name == "active particle" else hits
     achieved = units * unit_bytes / (kms[dom] / 1e3) / 1e9 if kms[dom] > 0 else None
     path_gbs = value / world * BYTES_PER_HIT / 1e9    # per GPU, over the whole step
