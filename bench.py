@@ -37,8 +37,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-DEFAULT_TICKS = {"iliev32": 400, "iliev64": 100, "lognormal128": 8}
-REF_TICKS = {"iliev32": 40, "iliev64": 4, "lognormal128": 1}   # per step of --impl reference
+DEFAULT_TICKS = {"iliev32": 400, "iliev64": 100, "lognormal128": 8, "lognormal256": 1}
+REF_TICKS = {"iliev32": 40, "iliev64": 4, "lognormal128": 1, "lognormal256": 1}   # per step of --impl reference
+SIDE_LEGS = ("iliev32", "iliev64", "lognormal128")
 # Algorithmic bytes. Per hit (the whole path): pos 12 + sml 4 + lambdaH 8 +
 # mass 4 + FP64 absorbed photons 8. Per kernel group, per unit it processes:
 # trace fill reads pos+sml (16) and writes (ipar 4, d 8, b 8) per hit; the
@@ -409,59 +410,63 @@ def main():
                      "x_HII_rel_diff": {"p50": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),
                                         "max": float(rel.max())}}
 
-    # recombination rays (onTheSpot = false): the same rays on a context
-    # with case-A recombination, nrec = 100 recombination rays per tick
-    # emitted on the device; the ticks then run one at a time
-    rctx = api.Context(dev)
-    rctx.set_stream(stream.cuda_stream)
-    rctx.set_physics(api.Physics(w.field.units, isothermal=w.isothermal, on_the_spot=False))
-    rctx.load(w.field)
-    rctx.build_tree(8)
-    rctx.set_recombination(nrec=100)
-    nrs = min(3, nsteps - 1)
-    rctx.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
-    r_ms, r_hits, r_rays = 0.0, 0.0, 0.0
-    torch.cuda.nvtx.range_push("recombination_steps")
-    for s in range(1, 1 + nrs):
-        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        st = rctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
-        e1.record(stream)
-        e1.synchronize()
-        r_ms += e0.elapsed_time(e1)
-        r_hits += st["hits"]
-        r_rays += st["rec_rays"]
-    torch.cuda.nvtx.range_pop()
-    rctx.close()
-    recombination = {"value": r_hits / (r_ms / 1e3), "unit": "hits/s", "ms_per_tick": r_ms / (nrs * T),
-                     "rec_rays_per_tick": r_rays / (nrs * T), "steps": nrs, "ticks_per_step": T}
+    # the side legs (recombination rays, helium) load further contexts of the
+    # same field; the 16.8 M-particle field is measured without them
+    recombination = helium = None
+    if args.workload in SIDE_LEGS:
+        # recombination rays (onTheSpot = false): the same rays on a context
+        # with case-A recombination, nrec = 100 recombination rays per tick
+        # emitted on the device; the ticks then run one at a time
+        rctx = api.Context(dev)
+        rctx.set_stream(stream.cuda_stream)
+        rctx.set_physics(api.Physics(w.field.units, isothermal=w.isothermal, on_the_spot=False))
+        rctx.load(w.field)
+        rctx.build_tree(8)
+        rctx.set_recombination(nrec=100)
+        nrs = min(3, nsteps - 1)
+        rctx.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
+        r_ms, r_hits, r_rays = 0.0, 0.0, 0.0
+        torch.cuda.nvtx.range_push("recombination_steps")
+        for s in range(1, 1 + nrs):
+            e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = rctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
+            e1.record(stream)
+            e1.synchronize()
+            r_ms += e0.elapsed_time(e1)
+            r_hits += st["hits"]
+            r_rays += st["rec_rays"]
+        torch.cuda.nvtx.range_pop()
+        rctx.close()
+        recombination = {"value": r_hits / (r_ms / 1e3), "unit": "hits/s", "ms_per_tick": r_ms / (nrs * T),
+                         "rec_rays_per_tick": r_rays / (nrs * T), "steps": nrs, "ticks_per_step": T}
 
-    # helium and secondary ionisation (HOnly = false, hydrogen mass fraction
-    # 0.76): the same particles and rays, three-species deposit with the
-    # secondary-ionisation table and the helium update, on the spot
-    from psphray_b200.units import Units
-    hu = Units(hmf=0.76)
-    hf = dataclasses.replace(w.field, units=hu)
-    hctx = api.Context(dev)
-    hctx.set_stream(stream.cuda_stream)
-    hctx.set_physics(api.Physics(hu, isothermal=w.isothermal, h_only=False, secondary_ionization=True))
-    hctx.load(hf)
-    hctx.build_tree(8)
-    hctx.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
-    h_ms, h_hits = 0.0, 0.0
-    torch.cuda.nvtx.range_push("helium_steps")
-    for s in range(1, 1 + nrs):
-        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        st = hctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
-        e1.record(stream)
-        e1.synchronize()
-        h_ms += e0.elapsed_time(e1)
-        h_hits += st["hits"]
-    torch.cuda.nvtx.range_pop()
-    hctx.close()
-    helium = {"value": h_hits / (h_ms / 1e3), "unit": "hits/s", "ms_per_tick": h_ms / (nrs * T),
-              "hmf": 0.76, "secondary_ionization": True, "steps": nrs, "ticks_per_step": T}
+        # helium and secondary ionisation (HOnly = false, hydrogen mass fraction
+        # 0.76): the same particles and rays, three-species deposit with the
+        # secondary-ionisation table and the helium update, on the spot
+        from psphray_b200.units import Units
+        hu = Units(hmf=0.76)
+        hf = dataclasses.replace(w.field, units=hu)
+        hctx = api.Context(dev)
+        hctx.set_stream(stream.cuda_stream)
+        hctx.set_physics(api.Physics(hu, isothermal=w.isothermal, h_only=False, secondary_ionization=True))
+        hctx.load(hf)
+        hctx.build_tree(8)
+        hctx.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
+        h_ms, h_hits = 0.0, 0.0
+        torch.cuda.nvtx.range_push("helium_steps")
+        for s in range(1, 1 + nrs):
+            e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = hctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
+            e1.record(stream)
+            e1.synchronize()
+            h_ms += e0.elapsed_time(e1)
+            h_hits += st["hits"]
+        torch.cuda.nvtx.range_pop()
+        hctx.close()
+        helium = {"value": h_hits / (h_ms / 1e3), "unit": "hits/s", "ms_per_tick": h_ms / (nrs * T),
+                  "hmf": 0.76, "secondary_ionization": True, "steps": nrs, "ticks_per_step": T}
 
     # the per-kernel-group breakdown: the same steps again (later ticks) with
     # the library's per-launch events on -- kept out of the timed steps,

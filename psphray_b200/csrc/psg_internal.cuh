@@ -129,6 +129,7 @@ struct psg_context {
 
 	// scratch, grown on demand
 	psg_buf scratch[S_NSLOTS];
+	double sat_frac = 0.0;  // capped share of the last batch's hits (picks the deposit's settle form)
 	size_t slab_cap = 0;  // hits each ray can hold in the traversal's output slabs
 	int ppc = 8;          // leaf capacity of the current tree
 	cudaEvent_t ev[8] = {};

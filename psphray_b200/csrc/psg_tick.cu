@@ -158,6 +158,7 @@ __device__ __forceinline__ bool below_cutoff(double TM, double Nph) {
 // writes photons/NH to its slot, or -1 where the reference deposits nothing.
 struct DepShared {
 	double wsum[32];
+	double wb[32];
 	double tm;
 	int first;
 };
@@ -188,7 +189,114 @@ __device__ __forceinline__ void acc_store(double *__restrict__ acc, int nacc, ui
 	}
 }
 
+// Past a capped hit f the step mixes capped hits, which take TM to
+// TM - NHI (loop.c:482-485, 580), and uncapped ones, TM to TM*exp(-tau):
+// affine maps, whose composition is associative. A group scan of the maps
+// gives TM before every hit for a guessed capped/uncapped pattern; the hits
+// before the first whose decision (or the 1e-10 cut) disagrees with the
+// guess are settled, that one is settled from its exact TM, and the next
+// pass guesses from this pass's decisions. TM changes slowly along a capped
+// run, so a step settles in a few passes instead of one per capped hit.
+// Called by every thread of the group with start = f + 1 and TM after f;
+// returns with the step settled (or the ray done). The deposit takes this
+// form (AFF) when the previous batch capped more than 1e-3 of its hits: on
+// a ray with few capped hits, its registers slow the common path.
 template <int NT>
+__device__ __forceinline__ void settle_capped(int t, bool valid, double tau, double NHI, double NH_inv, double Nph,
+		int start, double &TM, bool &done, double &delta, unsigned &nsat, DepShared &sh, int bar) {
+	const int lane = t & 31, wid = t >> 5;
+	constexpr int NW = NT / 32;
+	const double m1 = (valid && tau != 0.0) ? -expm1(-tau) : 0.0;
+	bool pcap = valid && t >= start && tau != 0.0 && TM * m1 > NHI;
+	while (start < NT) {
+		const bool pb = valid && t >= start && tau != 0.0;
+		double A = 1.0, B = 0.0;            // this hit's map, TM -> A*TM + B
+		if (pb) {
+			if (pcap) B = -NHI;
+			else A = 1.0 - m1;
+		}
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const double pa = __shfl_up_sync(0xffffffffu, A, o);
+			const double pv = __shfl_up_sync(0xffffffffu, B, o);
+			if (lane >= o) {
+				B = A * pv + B;
+				A = A * pa;
+			}
+		}
+		// the maps of the hits before this one: the lower lanes', after
+		// the earlier warps'
+		double xa = __shfl_up_sync(0xffffffffu, A, 1), xb = __shfl_up_sync(0xffffffffu, B, 1);
+		if (lane == 0) { xa = 1.0; xb = 0.0; }
+		double ta = A, tb = B;               // the whole step's map
+		if (NW > 1) {
+			if (lane == 31) { sh.wsum[wid] = A; sh.wb[wid] = B; }
+			if (t == 0) sh.first = NT;
+			group_sync<NT>(bar);
+			double ea = 1.0, eb = 0.0;
+			ta = 1.0;
+			tb = 0.0;
+#pragma unroll
+			for (int k = 0; k < NW; k++) {
+				const double wa = sh.wsum[k], wb = sh.wb[k];
+				if (k < wid) {
+					eb = wa * eb + wb;
+					ea = wa * ea;
+				}
+				tb = wa * tb + wb;
+				ta = wa * ta;
+			}
+			xb = xa * eb + xb;
+			xa = xa * ea;
+		} else {
+			ta = __shfl_sync(0xffffffffu, A, 31);
+			tb = __shfl_sync(0xffffffffu, B, 31);
+		}
+		double TMj = 0.0, absorb = 0.0, after = 0.0;
+		bool cap = false, bad = false;
+		if (pb) {
+			TMj = xa * TM + xb;
+			absorb = TMj * m1;
+			cap = absorb > NHI;
+			after = cap ? TMj - NHI : TMj - absorb;
+			bad = (cap != pcap) || below_cutoff(after, Nph);
+		}
+		int m;
+		if (NW == 1) {
+			const unsigned ev = __ballot_sync(0xffffffffu, bad);
+			m = ev ? __ffs(ev) - 1 : NT;
+		} else {
+			if (bad) atomicMin(&sh.first, t);
+			group_sync<NT>(bar);
+			m = sh.first;
+		}
+		if (pb && t <= m) {        // the settled hits, and hit m from its exact TM
+			delta = rn_dmul(cap ? NHI : absorb, NH_inv);
+			if (cap) nsat++;
+		}
+		if (m == NT) {
+			TM = ta * TM + tb;
+			group_sync<NT>(bar);       // shared words are rewritten by the next scan
+			break;
+		}
+		if (NW == 1) {
+			TM = __shfl_sync(0xffffffffu, after, m);
+		} else {
+			if (t == m) sh.tm = after;
+			group_sync<NT>(bar);
+			TM = sh.tm;
+		}
+		start = m + 1;
+		pcap = cap;
+		group_sync<NT>(bar);
+		if (below_cutoff(TM, Nph)) {
+			done = true;
+			break;
+		}
+	}
+}
+
+template <int NT, bool AFF>
 __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern, const uint32_t *__restrict__ slot,
 		const double *__restrict__ lambdaH, const float *__restrict__ mass, const PhysParams &P, int want_heat,
@@ -307,6 +415,11 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 			if (below_cutoff(TM, Nph)) done = true;
 			start = f + 1;
 			group_sync<NT>(bar);
+			if (AFF && !done) {
+				// f was capped: the rest of the step through the affine-map scan
+				settle_capped<NT>(t, valid, tau, NHI, NH_inv, Nph, start, TM, done, delta, nsat, sh, bar);
+				break;
+			}
 		}
 		if (valid) {
 			acc_store(acc, want_heat ? 2 : 1, slot_c, delta,
@@ -519,7 +632,7 @@ __device__ void deposit_ray_gen(const psg_ray &ray, int64_t h0, int64_t h1, int 
 #define DEP_LONG 96       // more hits than this: a group of threads, else a warp
 #define DEP_MID 384       // more hits than this: the whole block, else a 128-thread quarter
 
-template <bool GEN>
+template <bool GEN, bool AFF>
 __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__restrict__ rays,
 		const uint32_t *__restrict__ long_rays, int nlong, const uint32_t *__restrict__ mid_rays, int nmid,
 		const uint32_t *__restrict__ short_rays, int nshort,
@@ -540,7 +653,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 			deposit_ray_gen<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
 					want_heat, acc, nacc, sh_block, nsat, tm_lost, 0);
 		else
-			deposit_ray<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
+			deposit_ray<DEP_THREADS, AFF>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
 					want_heat, acc, sh_block, nsat, tm_lost, 0);
 	} else if ((int)blockIdx.x < nlong + nmid_blocks) {
 		const int q = tid >> 7;
@@ -551,7 +664,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 				deposit_ray_gen<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
 						want_heat, acc, nacc, sh_quarter[q], nsat, tm_lost, 1 + q);
 			else
-				deposit_ray<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
+				deposit_ray<128, AFF>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
 						want_heat, acc, sh_quarter[q], nsat, tm_lost, 1 + q);
 		}
 	} else {
@@ -563,7 +676,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 					deposit_ray_gen<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
 							want_heat, acc, nacc, sh_warp[wid], nsat, tm_lost, 0);
 				else
-					deposit_ray<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
+					deposit_ray<32, AFF>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
 							want_heat, acc, sh_warp[wid], nsat, tm_lost, 0);
 			}
 		}
@@ -1412,6 +1525,8 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 	std::vector<int32_t> h_tick_long(K + 1);
 	PSG_CUDA(cudaMemcpyAsync(h_tick_long.data(), tick_long, sizeof(int32_t) * (K + 1), cudaMemcpyDeviceToHost, st));
 	PSG_CUDA(cudaStreamSynchronize(st));
+	// capped hits settled by the affine-map scan when the last batch had many
+	const bool aff = ctx->sat_frac > 1e-3;
 	for (size_t t = 0; t < K; t++) {
 		const unsigned long long c0 = h_scan[t * R], c1 = (t + 1 < K) ? h_scan[(t + 1) * R] : tot;
 		const int l0 = (int)(uint32_t)c0, m0 = (int)(uint32_t)(c0 >> 32);
@@ -1421,12 +1536,16 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 		const unsigned grid = (unsigned)(nlong + (nmid + 3) / 4 + (nshort + DEP_THREADS / 32 - 1) / (DEP_THREADS / 32));
 		psg_mark_begin(ctx, PSG_K_DEPOSIT);
 		if (grid && gen)
-			k_deposit<true><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0, nmid,
-					short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+			k_deposit<true, false><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0,
+					nmid, short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+					want_heat, acc, nacc, d_nsat, d_lost);
+		else if (grid && aff)
+			k_deposit<false, true><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0,
+					nmid, short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
 					want_heat, acc, nacc, d_nsat, d_lost);
 		else if (grid)
-			k_deposit<false><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0, nmid,
-					short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+			k_deposit<false, false><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0,
+					nmid, short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
 					want_heat, acc, nacc, d_nsat, d_lost);
 		PSG_CHECK_LAUNCH();
 		psg_mark_end(ctx);
@@ -1516,12 +1635,13 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 		ctx->launches++;
 	}
 	PSG_CUDA(cudaEventRecord(ctx->ev[2], st));
-	rc = check_status(ctx);
+	unsigned long long nsat = 0;
+	PSG_CUDA(cudaMemcpyAsync(&nsat, d_nsat, sizeof(nsat), cudaMemcpyDeviceToHost, st));
+	rc = check_status(ctx);      // (synchronises the stream)
 	if (rc) return rc;
+	ctx->sat_frac = nhit ? (double)nsat / (double)nhit : 0.0;
 	if (stats) {
-		unsigned long long nsat = 0;
 		double lost = 0;
-		PSG_CUDA(cudaMemcpyAsync(&nsat, d_nsat, sizeof(nsat), cudaMemcpyDeviceToHost, st));
 		PSG_CUDA(cudaMemcpyAsync(&lost, d_lost, sizeof(lost), cudaMemcpyDeviceToHost, st));
 		PSG_CUDA(cudaStreamSynchronize(st));
 		float trace_ms = 0.f, tick_ms = 0.f;

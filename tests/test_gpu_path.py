@@ -229,6 +229,38 @@ def test_capped_deposits_vs_oracle(gpu_ctx, phys):
     assert np.max(np.abs(gs["lambdaH"] - orc.lambdaH)) < 1e-9
 
 
+@pytest.mark.parametrize("boost", [1e6, 1e9])
+def test_capped_runs_vs_oracle(gpu_ctx, phys, boost):
+    """Rays from the corner source of the 32^3 uniform field (in-box rays of
+    ~480 hits: the whole-block and quarter-block deposit groups) carrying
+    1e6x and 1e9x the photons: runs of capped hits mixed with uncapped ones,
+    against the sequential restatement: saturation count, per-particle
+    deposit counters exact, lambda to 1e-9. The ticks run as two batches:
+    the first batch caps most of its hits, so the second settles them with
+    the affine-map scan (the first takes either form)."""
+    from psphray_b200 import fields
+    w = fields.make_workload("iliev32", nray=128, seed=5)
+    f = w.field
+    _gpu(gpu_ctx, f, phys)
+    orc = Oracle(f, phys)
+    orc.build_tree(8)
+    R = 128
+    rays = w.schedule.rays_for_ticks(1, 2)
+    rays["Nph"] *= boost
+    st = gpu_ctx.run_ticks(rays[:R], R, 1, 1, w.tick_time)
+    st2 = gpu_ctx.run_ticks(rays[R:], R, 1, 2, w.tick_time)
+    assert st["saturated"] > 1e-3 * st["hits"]
+    st["saturated"] += st2["saturated"]
+    sat = 0
+    for k in range(2):
+        sat += orc.tick(rays[k * R:(k + 1) * R], k + 1, w.tick_time)["saturated"]
+    assert sat > 1000 and st["saturated"] == sat
+    gs = gpu_ctx.state()
+    assert np.array_equal(gs["hits"], orc.hits)
+    assert np.array_equal(gs["lasthit"], orc.lasthit)
+    assert np.max(np.abs(gs["lambdaH"] - orc.lambdaH)) < 1e-9
+
+
 def test_ticks_noniso_vs_oracle(gpu_ctx, phys_noniso):
     """Not isothermal, 8-bin blackbody rays (photo-heating on): 6 ticks on
     the log-normal field through the work-queue integrator against the
