@@ -310,6 +310,7 @@ extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {
 	const size_t n = p->n;
 	ctx->n = n;
 	ctx->boxsize = p->boxsize;
+	ctx->sat_frac = 0.0;       // a new field starts on the deposit's common form
 	PSG_CUDA(cudaMalloc(&ctx->d_psml, sizeof(float4) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_mass, sizeof(float) * n));
 	PSG_CUDA(cudaMalloc(&ctx->d_rho, sizeof(float) * n));

@@ -236,8 +236,9 @@ def test_capped_runs_vs_oracle(gpu_ctx, phys, boost):
     1e6x and 1e9x the photons: runs of capped hits mixed with uncapped ones,
     against the sequential restatement: saturation count, per-particle
     deposit counters exact, lambda to 1e-9. The ticks run as two batches:
-    the first batch caps most of its hits, so the second settles them with
-    the affine-map scan (the first takes either form)."""
+    the first (just after the load) settles capped hits one at a time and
+    caps most of its hits, so the second settles them with the affine-map
+    scan -- both forms of the deposit against the same restatement."""
     from psphray_b200 import fields
     w = fields.make_workload("iliev32", nray=128, seed=5)
     f = w.field
