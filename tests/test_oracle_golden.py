@@ -75,6 +75,38 @@ def test_deposit_matches_reference(phys):
         assert rel.max() < 1e-6, rel.max()
 
 
+@pytest.mark.parametrize("boost", [1e6, 1e9])
+def test_capped_runs_match_reference(reference, phys, boost):
+    """Corner-source rays through the 32^3 uniform field carrying 1e6x and
+    1e9x the photons, so that most hits cap (loop.c:482-485): one tick's
+    deposit through the reference build and through the restatement -- the
+    same saturation count and per-particle hit counters, absorbed photons
+    per particle to 1e-6 (the reference sums them into float). The GPU's
+    capped-run settling is checked against the restatement on the same
+    rays."""
+    from psphray_b200 import fields
+    w = fields.make_workload("iliev32", nray=128, seed=5)
+    rays = w.schedule.rays_for_ticks(1, 1).copy()
+    rays["Nph"] *= boost
+    reference.load(w.field)
+    reference.build_tree(8)
+    reference.reset_stats()
+    reference.set_rays(rays, 1, w.tick_time)
+    reference.trace()
+    reference.deposit()
+    rs, rst = reference.stats(), reference.state()
+    orc = Oracle(w.field, phys)
+    orc.build_tree(8)
+    off, hits = orc.trace_all(rays)
+    st = orc.deposit(rays, off, hits)
+    assert rs["saturated"] > 1000 and st["saturated"] == rs["saturated"]
+    assert np.array_equal(orc.hits, rst["hits"])
+    ref = rst["yGdepHI"].astype(np.float64)
+    m = (ref > 0) | (orc.yGdepHI > 0)
+    rel = np.abs(orc.yGdepHI[m] - ref[m]) / np.maximum(ref[m], 1e-30)
+    assert rel.max() < 1e-6, rel.max()
+
+
 def test_ticks_track_reference(phys):
     """40 ticks of trace/deposit/merge/update against the reference's LSODA
     run: lasthit exact, x_HII within 1e-3 (LSODA's rtol=1e-4 per step is the
