@@ -753,8 +753,10 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 	hits[p] += nh;
 	if (gcarry) g += gcarry[p];      // photons left over by an earlier explicit step (loop.c:745)
 	if (!ISO) {
-		act_g[a] = g;
-		act_heat[a] = heat;
+		if (act_g) {        // read by the surrogate and the update log only
+			act_g[a] = g;
+			act_heat[a] = heat;
+		}
 		UpdRec r;
 		r.time = rn_dmul((double)(tick - lasthit[p]), tick_time);
 		r.lam0 = lambdaH[p];
@@ -1573,9 +1575,10 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 			const int lb = (nl + 7) / 8;
 			const unsigned rgrid = (unsigned)(lb + (int)blocks(nact_t, 256));
 			const double *gcarry = euler ? ctx->d_gcarry : nullptr;
+			double *keep_g = (surr || feat) ? act_g : nullptr, *keep_heat = (surr || feat) ? act_heat : nullptr;
 #define PSG_REDUCE(ISO_, REC_)                                                                              \
 	k_reduce<ISO_, REC_><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, want_heat, \
-			long_act + h_tick_long[t], nl, lb, ctx->d_hits, act_g, act_heat, ctx->d_lambdaH, ctx->d_ie,        \
+			long_act + h_tick_long[t], nl, lb, ctx->d_hits, keep_g, keep_heat, ctx->d_lambdaH, ctx->d_ie,      \
 			ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, tick, tick_time,          \
 			ctx->d_status)
 			if (iso && !euler) {
