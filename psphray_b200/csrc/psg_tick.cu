@@ -148,14 +148,17 @@ __device__ __forceinline__ bool below_cutoff(double TM, double Nph) {
 	return TM < 0.0 || __ddiv_rn(TM, Nph) < 1e-10;
 }
 
-// Deposit of one ray by a group of NT threads (a warp, or a whole block):
-// hits are taken NT at a time; optical depths are summed with an FP64 scan
-// over the group; the first hit whose absorption exceeds its neutral atoms
-// (loop.c:482-485) or after which TM/Nph < 1e-10 (loop.c:585) is found with
-// a group min, settled by its own thread, and the scan restarts after it.
-// Transmitted photons before hit j are TM*exp(-(sum of earlier tau)); after
-// it, TM_j minus the absorbed photons, as loop.c:580 updates TM. Each hit
-// writes photons/NH to its slot, or -1 where the reference deposits nothing.
+// Deposit of one ray by a group of NT threads (a warp, a 128-thread quarter
+// or a whole block): hits are taken NT at a time; optical depths are summed
+// with an FP64 scan over the group; the first hit whose absorption exceeds
+// its neutral atoms (loop.c:482-485) or after which TM/Nph < 1e-10
+// (loop.c:585) is found with a group min, settled by its own thread, and the
+// scan restarts after it (or, in the AFF form, the rest of the step goes to
+// settle_capped()). Transmitted photons before hit j are
+// TM*exp(-(sum of earlier tau)); after it, TM_j minus the absorbed photons,
+// as loop.c:580 updates TM. Each hit writes photons/NH to its slot, or -1
+// where the reference deposits nothing. wsum and wb carry the per-warp scan
+// totals (wb: the affine maps' offsets).
 struct DepShared {
 	double wsum[32];
 	double wb[32];
