@@ -531,7 +531,9 @@ def main():
             "e2e": {"value": e2e_hits / e2e_t, "unit": "hits/s",
                     "h2d_bytes_per_step": int(host_rays[0].nbytes),
                     "d2h_bytes_per_step": int(lam.nbytes)}}
-    if rank == 0 and not args.no_cpu_baseline:
+    # the host-core baseline: rank 0 of a one-GPU run only (with more ranks,
+    # their host threads would share the cores it is timed on)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_reference(make(args.workload), seconds=args.cpu_seconds)
     if rank == 0:
         print(json.dumps(line), flush=True)
