@@ -17,9 +17,14 @@ lognormal128, the 2M-particle case the hits/s target is stated at):
   iliev32       32^3, 32 rays/tick (the reference's CPU-sized case)
   lognormal128  128^3 particles on a log-normal field (sigma 1), 16 sources,
                 8192 rays/tick, 8-bin 1e5 K blackbody, non-isothermal
+  lognormal256  256^3 particles on a log-normal field (sigma 1.5), 256
+                sources of 1e46-1e49 photons/s, 65536 rays/tick, one tick
+                per step, non-isothermal; without the recombination and
+                helium legs
 
 --gpus N under torchrun runs N independent replicas, one per GPU (the path
 is single-GPU; no data crosses GPUs), barrier + max over ranks for time.
+The host-core baseline (cpu_baseline) is timed in one-GPU runs only.
 """
 from __future__ import annotations
 
