@@ -19,6 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpsg.so")
+RUN = os.path.join(HERE, "psg_run")
 
 CU_SOURCES = ["psg_context.cu", "psg_tree.cu", "psg_trace.cu", "psg_tick.cu", "psg_emit.cu", "psg_mlp.cu", "psg_surrogate.cu",
               "psg_recomb.cu"]
@@ -67,6 +68,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(o)
     if force or _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+    # the C host driver over the library's C ABI
+    src = os.path.join(CSRC, "psg_run.c")
+    if force or _stale(RUN, [src, LIB, os.path.join(INCLUDE, "psg.h")]):
+        _run(["gcc", "-std=c11", "-O2", "-Wall", "-Wextra", "-I", INCLUDE, src, "-L", HERE, "-lpsg",
+              "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,$ORIGIN", "-o", RUN])
     return LIB
 
 
