@@ -17,9 +17,9 @@ def _run(*args):
     return subprocess.run([RUN, *map(str, args)], capture_output=True, text=True, timeout=120)
 
 
-def _snapshot(tmp_path):
+def _snapshot(tmp_path, n_side=8):
     from psphray_b200 import api, fields
-    w = fields.make_workload("iliev32", n_side=8, nray=16, seed=4)
+    w = fields.make_workload("iliev32", n_side=n_side, nray=16, seed=4)
     f = w.field
     path = str(tmp_path / "in.psphray")
     api.write_snapshot(path, f.n, {"pos": f.pos, "mass": f.mass, "sml": f.sml, "rho": f.rho, "ie": f.ie,
@@ -53,3 +53,41 @@ def test_driver_host_side_without_gpu(built, tmp_path):
     assert r.returncode == 3, r.stderr
     assert "psg_create" in r.stderr
     assert not os.path.exists(tmp_path / "out")
+
+
+@pytest.mark.gpu
+def test_driver_epoch_matches_binding(built, tmp_path):
+    """16 ticks of 64 device-emitted rays on a 16^3 field, once through the
+    driver and once through the Python binding with the same source, seed
+    and tick time: hit counters and lasthit equal, the output's xHI the
+    float of lambdaH (to 1e-6: the C and Python unit constants may differ
+    in the last bit)."""
+    from types import SimpleNamespace
+    from psphray_b200 import api, fields
+    from psphray_b200.api import KERNEL_AKLINE, RATES_HUI
+    snap = _snapshot(tmp_path, n_side=16)
+    out = tmp_path / "out.psphray"
+    seed = 77
+    r = _run(snap, RATES_HUI, KERNEL_AKLINE, 16, 64, 0.8, out, "--isothermal", "--batch", "8", "--seed", seed)
+    assert r.returncode == 0, r.stderr
+    assert "16 ticks of 64 rays" in r.stdout
+    w = fields.make_workload("iliev32", n_side=16, nray=16, seed=4)
+    f = w.field
+    ctx = api.Context(0)
+    try:
+        ctx.set_physics(api.Physics(f.units, isothermal=True))
+        ctx.load(f)
+        ctx.build_tree(8)
+        src = SimpleNamespace(pos=(0.0, 0.0, 0.0), ngamma_dot=w.schedule.sources[0].ngamma_dot, lastemit=0)
+        ctx.set_sources([src], [(np.array([13.6 * f.units.EV]), np.array([1.0]))], seed=seed)
+        tick_time = 0.8 * f.units.MYR / 16
+        ctx.run_ticks_emit(64, 8, 1, tick_time)
+        ctx.run_ticks_emit(64, 8, 9, tick_time)
+        st = ctx.state()
+    finally:
+        ctx.close()
+    o = api.read_snapshot(str(out))
+    assert (st["lasthit"] > 0).sum() > 1000
+    assert np.array_equal(o["lasthit"], st["lasthit"])
+    assert np.array_equal(o["hits"], st["hits"])
+    assert np.max(np.abs(o["xHI"].astype(np.float64) - st["lambdaH"].astype(np.float32))) <= 1e-6
