@@ -72,7 +72,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     src = os.path.join(CSRC, "psg_run.c")
     if force or _stale(RUN, [src, LIB, os.path.join(INCLUDE, "psg.h")]):
         _run(["gcc", "-std=c11", "-O2", "-Wall", "-Wextra", "-I", INCLUDE, src, "-L", HERE, "-lpsg",
-              "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,$ORIGIN", "-o", RUN])
+              "-L", "/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,$ORIGIN", "-lm", "-o", RUN])
     return LIB
 
 

@@ -22,8 +22,10 @@
  *     MYR       the epoch's duration in Myr (tick_time = MYR / NTICKS)
  *     OUTPUT    psphray-format output written at the end
  *   options: --batch K (ticks per library call, default 8), --energy EV
- *     (monochromatic photons, default 13.6), --isothermal, --hmf X (default
- *     1: hydrogen only), --ppc P (default 8), --seed S, --device D
+ *     (monochromatic photons, default 13.6), --blackbody T (instead: an
+ *     8-line blackbody spectrum of temperature T over 1-10 Ry, log-spaced
+ *     bins, photon-number weights), --isothermal, --hmf X (default 1:
+ *     hydrogen only), --ppc P (default 8), --seed S, --device D
  *
  * Exit status: 0 done; 1 usage; 2 input files; 3 library or device error
  * (the library's message is printed). */
@@ -31,6 +33,7 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <math.h>
 #include <string.h>
 #include <time.h>
 
@@ -39,7 +42,7 @@
 static int usage(void) {
 	fprintf(stderr,
 			"usage: psg_run SNAPSHOT RATES KERNEL NTICKS NRAY MYR OUTPUT [--batch K] [--energy EV]\n"
-			"               [--isothermal] [--hmf X] [--ppc P] [--seed S] [--device D]\n");
+			"               [--blackbody T] [--isothermal] [--hmf X] [--ppc P] [--seed S] [--device D]\n");
 	return 1;
 }
 
@@ -61,7 +64,7 @@ int main(int argc, char **argv) {
 	const double myr = atof(argv[6]);
 	long long batch = 8, ppc = 8, device = 0;
 	unsigned long long seed = 20261203ull;
-	double energy_ev = 13.6, hmf = 1.0;
+	double energy_ev = 13.6, hmf = 1.0, bb_T = 0.0;
 	int isothermal = 0;
 	for (int i = 8; i < argc; i++) {
 		const char *a = argv[i];
@@ -69,6 +72,7 @@ int main(int argc, char **argv) {
 		if (!strcmp(a, "--isothermal")) isothermal = 1;
 		else if (!strcmp(a, "--batch") && more) batch = atoll(argv[++i]);
 		else if (!strcmp(a, "--energy") && more) energy_ev = atof(argv[++i]);
+		else if (!strcmp(a, "--blackbody") && more) bb_T = atof(argv[++i]);
 		else if (!strcmp(a, "--hmf") && more) hmf = atof(argv[++i]);
 		else if (!strcmp(a, "--ppc") && more) ppc = atoll(argv[++i]);
 		else if (!strcmp(a, "--seed") && more) seed = strtoull(argv[++i], NULL, 10);
@@ -76,7 +80,7 @@ int main(int argc, char **argv) {
 		else return usage();
 	}
 	if (nticks <= 0 || nray <= 0 || !(myr > 0) || batch <= 0 || ppc <= 0 || !(hmf > 0 && hmf <= 1) ||
-			!(energy_ev > 0))
+			!(energy_ev > 0) || bb_T < 0)
 		return usage();
 
 	/* the epoch's particles and sources */
@@ -131,7 +135,7 @@ int main(int argc, char **argv) {
 	if ((rc = psg_load_particles(ctx, &p)) != PSG_OK) return lib_fail(ctx, rc, "psg_load_particles");
 	if ((rc = psg_build_tree(ctx, (int)ppc)) != PSG_OK) return lib_fail(ctx, rc, "psg_build_tree");
 
-	/* point sources of one monochromatic spectrum, constant luminosity */
+	/* point sources of one spectrum, constant luminosity */
 	psg_source *srcs = calloc(nsrc, sizeof(psg_source));
 	const int64_t hist_tick = 0;
 	if (!srcs) return 2;
@@ -144,8 +148,20 @@ int main(int argc, char **argv) {
 		srcs[i].nhist = 1;
 		srcs[i].lastemit = 0;
 	}
-	const double eng = energy_ev * u.EV, weight = 1.0;
-	const psg_spectrum spec = {&eng, &weight, 1};
+	double eng[8] = {energy_ev * u.EV}, weight[8] = {1.0};
+	int nline = 1;
+	if (bb_T > 0) {
+		/* photon numbers of B_nu / (h nu) over log-spaced bins of 1-10 Ry,
+		 * each line at the bin's geometric centre */
+		const double kT = u.BOLTZMANN * bb_T;
+		nline = 8;
+		for (int k = 0; k < nline; k++) {
+			const double e0 = u.RY_ENG * pow(10.0, (double)k / nline), e1 = u.RY_ENG * pow(10.0, (double)(k + 1) / nline);
+			eng[k] = sqrt(e0 * e1);
+			weight[k] = eng[k] * eng[k] / expm1(eng[k] / kT) * (e1 - e0);
+		}
+	}
+	const psg_spectrum spec = {eng, weight, nline};
 	if ((rc = psg_set_sources(ctx, srcs, (int)nsrc, &spec, 1, seed)) != PSG_OK) return lib_fail(ctx, rc, "psg_set_sources");
 
 	/* the ticks */

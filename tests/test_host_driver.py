@@ -39,6 +39,8 @@ def test_driver_builds_and_checks_arguments(built, tmp_path):
     snap = _snapshot(tmp_path)
     r = _run(snap, RATES_HUI, KERNEL_AKLINE, 0, 16, 1.0, tmp_path / "out")
     assert r.returncode == 1
+    r = _run(snap, RATES_HUI, KERNEL_AKLINE, 4, 16, 1.0, tmp_path / "out", "--blackbody", "-1")
+    assert r.returncode == 1
     r = _run(snap, tmp_path / "no-rates", KERNEL_AKLINE, 4, 16, 1.0, tmp_path / "out")
     assert r.returncode == 2 and "cannot build the tables" in r.stderr
 
