@@ -104,6 +104,10 @@ int psg_set_timing(psg_context *ctx, int on);
  * as void*; NULL restores the context's own stream). No reference
  * counterpart: the reference has no device. */
 int psg_set_stream(psg_context *ctx, void *stream);
+/* The SASS and PTX architecture versions (major*10 + minor, 100 for
+ * sm_100a) of the library's device code as loaded on the context's device
+ * (cudaFuncGetAttributes). No reference counterpart: a build check. */
+int psg_device_arch(psg_context *ctx, int *binary_version, int *ptx_version);
 
 /* Physics switches, the config.c flags that the path reads. */
 typedef struct {
@@ -329,9 +333,16 @@ int psg_step_evolve(psg_context *ctx, psg_step *steps, size_t n);
 /* psg_step_evolve without any device allocation (no counterpart in the
  * reference): the steps are staged in a fixed buffer inside the library,
  * one per device, of PSG_NOALLOC_MAX_STEPS (16384) steps; larger n is
- * rejected with PSG_E_INVAL. The first call on each device looks the buffer
- * up (cudaGetSymbolAddress) and should come before any stream capture on
- * that device. Calls that overlap in time on one device race on the buffer. */
+ * rejected with PSG_E_INVAL. For hosts that cannot allocate device memory
+ * while a step is under way: a code whose pool allocator already holds the
+ * device's free memory, or one that must avoid the device-wide
+ * synchronisation of cudaMalloc/cudaFree. The buffer (2.25 MiB) is reserved
+ * when psg_create() runs on the device (it loads the library's module that
+ * holds it) and stays until the process exits, so create the context
+ * before the host's pool takes the memory. Every call looks the buffer's
+ * address up afresh (cheap); a device reset by the host between calls
+ * reloads the module on the next call. Calls that overlap in time on one
+ * device race on the buffer: serialise them. */
 #define PSG_NOALLOC_MAX_STEPS 16384
 int psg_step_evolve_noalloc(psg_context *ctx, psg_step *steps, size_t n);
 

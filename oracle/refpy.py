@@ -41,7 +41,7 @@ class Reference:
         if lib_path in Reference._libs:
             raise RuntimeError("the reference harness holds global state; one instance per library and process")
         if not os.path.exists(lib_path):
-            raise FileNotFoundError(f"{lib_path} missing: run `make -C oracle ref`")
+            raise FileNotFoundError(f"{lib_path} missing: run `make -C oracle ref REF=<psphray tree>`")
         lib = C.CDLL(lib_path)
         Reference._libs[lib_path] = lib
         self.lib = lib

@@ -64,6 +64,13 @@ extern "C" int psg_create(psg_context **out, int device) {
 	}
 	ctx->stream = ctx->own_stream;
 	for (auto &ev : ctx->ev) cudaEventCreate(&ev);
+	// reserve psg_step_evolve_noalloc's static buffer on this device now (its
+	// module loads on the first lookup), not on its first call
+	unsigned char *nb = nullptr;
+	if (psg_noalloc_lookup(&nb) != 0) {
+		psg_destroy(ctx);
+		return PSG_E_CUDA;
+	}
 	*out = ctx;
 	return PSG_OK;
 }
@@ -294,6 +301,19 @@ __global__ void k_init_particles(size_t n, const float *pos, const float *sml, c
 	lamHeI[i] = l1;
 	lamHeII[i] = l2;
 	yeMET[i] = (float)yem;
+}
+
+// The architecture of the device code the runtime loaded for this library
+// (one kernel stands for all: every .cu file is built with the same
+// -gencode). No reference counterpart: a build check for the host.
+extern "C" int psg_device_arch(psg_context *ctx, int *binary_version, int *ptx_version) {
+	if (!ctx || !binary_version || !ptx_version) return PSG_E_INVAL;
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	cudaFuncAttributes a;
+	PSG_CUDA(cudaFuncGetAttributes(&a, k_init_particles));
+	*binary_version = a.binaryVersion;
+	*ptx_version = a.ptxVersion;
+	return PSG_OK;
 }
 
 extern "C" int psg_load_particles(psg_context *ctx, const psg_particles *p) {

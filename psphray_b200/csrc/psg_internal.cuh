@@ -143,6 +143,9 @@ struct psg_context {
 // error helpers ---------------------------------------------------------------
 int psg_fail(psg_context *ctx, int code, const char *fmt, ...);
 int psg_cuda_fail(psg_context *ctx, cudaError_t e, const char *what, const char *file, int line);
+// Address of psg_step_evolve_noalloc's static buffer on the current device
+// (psg_tick.cu); 0 or the cudaError_t of the lookup.
+int psg_noalloc_lookup(unsigned char **base);
 #define PSG_CUDA(call)                                                               \
 	do {                                                                             \
 		cudaError_t e_ = (call);                                                     \

@@ -25,7 +25,19 @@
  *     (monochromatic photons, default 13.6), --blackbody T (instead: an
  *     8-line blackbody spectrum of temperature T over 1-10 Ry, log-spaced
  *     bins, photon-number weights), --isothermal, --hmf X (default 1:
- *     hydrogen only), --ppc P (default 8), --seed S, --device D
+ *     hydrogen only), --ppc P (default 8), --seed S, --device D, --resume
+ *     (with --hmf below 1: take the helium fractions from the file's xHeI
+ *     and xHeII blocks, as an earlier epoch's output wrote them, instead of
+ *     deriving them from ye)
+ *
+ * Helium at load. The reference's live reader (psystem.c:330-360) reads
+ * only ye and splits its electrons beyond x_HII into helium (HeII first,
+ * then HeIII) and metals; psg_load_particles() does the same. Its resume
+ * from an output (psystem.c:520-597) would read xHeI and xHeII back, but it
+ * is compiled out (#if 0). --resume restores them: after the load, the
+ * file's fractions replace the derived ones (psg_set_he_state). yeMET keeps
+ * the load's value: an output's ye holds the hydrogen and helium electrons
+ * only, so the split leaves the same (zero) metal electrons either way.
  *
  * Exit status: 0 done; 1 usage; 2 input files; 3 library or device error
  * (the library's message is printed). */
@@ -42,7 +54,8 @@
 static int usage(void) {
 	fprintf(stderr,
 			"usage: psg_run SNAPSHOT RATES KERNEL NTICKS NRAY MYR OUTPUT [--batch K] [--energy EV]\n"
-			"               [--blackbody T] [--isothermal] [--hmf X] [--ppc P] [--seed S] [--device D]\n");
+			"               [--blackbody T] [--isothermal] [--hmf X] [--ppc P] [--seed S] [--device D]\n"
+			"               [--resume]\n");
 	return 1;
 }
 
@@ -65,11 +78,12 @@ int main(int argc, char **argv) {
 	long long batch = 8, ppc = 8, device = 0;
 	unsigned long long seed = 20261203ull;
 	double energy_ev = 13.6, hmf = 1.0, bb_T = 0.0;
-	int isothermal = 0;
+	int isothermal = 0, resume = 0;
 	for (int i = 8; i < argc; i++) {
 		const char *a = argv[i];
 		const int more = i + 1 < argc;
 		if (!strcmp(a, "--isothermal")) isothermal = 1;
+		else if (!strcmp(a, "--resume")) resume = 1;
 		else if (!strcmp(a, "--batch") && more) batch = atoll(argv[++i]);
 		else if (!strcmp(a, "--energy") && more) energy_ev = atof(argv[++i]);
 		else if (!strcmp(a, "--blackbody") && more) bb_T = atof(argv[++i]);
@@ -110,6 +124,33 @@ int main(int argc, char **argv) {
 		fprintf(stderr, "psg_run: %s: unreadable blocks\n", snap_path);
 		return 2;
 	}
+	/* the helium fractions of an earlier epoch's output */
+	double *lamHeI = NULL, *lamHeII = NULL;
+	if (resume && hmf < 1.0) {
+		psg_snapshot hs;
+		memset(&hs, 0, sizeof hs);
+		hs.ngas = snap.ngas;
+		hs.nsrc = snap.nsrc;
+		float *xHeI = malloc(sizeof(float) * n), *xHeII = malloc(sizeof(float) * n);
+		lamHeI = malloc(sizeof(double) * n);
+		lamHeII = malloc(sizeof(double) * n);
+		if (!xHeI || !xHeII || !lamHeI || !lamHeII) {
+			fprintf(stderr, "psg_run: out of host memory for %zu particles\n", n);
+			return 2;
+		}
+		hs.xHeI = xHeI;
+		hs.xHeII = xHeII;
+		if (psg_snapshot_read(snap_path, &hs) != PSG_OK) {
+			fprintf(stderr, "psg_run: %s: --resume needs the xHeI and xHeII blocks\n", snap_path);
+			return 2;
+		}
+		for (size_t i = 0; i < n; i++) {
+			lamHeI[i] = (double)xHeI[i];
+			lamHeII[i] = (double)xHeII[i];
+		}
+		free(xHeI);
+		free(xHeII);
+	}
 
 	/* units and tables (config.c defaults, cosmology.h from the file) */
 	psg_unit_params up = {snap.h > 0 ? snap.h : 0.72, hmf, 3.0835455558318480e21, 1.9847005219450705e43,
@@ -133,6 +174,8 @@ int main(int argc, char **argv) {
 	if ((rc = psg_set_physics(ctx, &u, &ar, &xs, kernel, nk, &fl)) != PSG_OK) return lib_fail(ctx, rc, "psg_set_physics");
 	const psg_particles p = {n, pos, mass, sml, rho, ie, xHI, ye, NULL, snap.boxsize};
 	if ((rc = psg_load_particles(ctx, &p)) != PSG_OK) return lib_fail(ctx, rc, "psg_load_particles");
+	if (lamHeI && (rc = psg_set_he_state(ctx, lamHeI, lamHeII, NULL, NULL)) != PSG_OK)
+		return lib_fail(ctx, rc, "psg_set_he_state");
 	if ((rc = psg_build_tree(ctx, (int)ppc)) != PSG_OK) return lib_fail(ctx, rc, "psg_build_tree");
 
 	/* point sources of one spectrum, constant luminosity */
@@ -188,5 +231,6 @@ int main(int argc, char **argv) {
 	psg_xs_table_free(&xs);
 	free(srcs);
 	free(pos); free(mass); free(sml); free(rho); free(ie); free(xHI); free(ye); free(src_pos); free(id); free(ngammas);
+	free(lamHeI); free(lamHeII);
 	return 0;
 }

@@ -18,7 +18,6 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
-#include <mutex>
 #include <vector>
 
 #include "psg_internal.cuh"
@@ -1729,34 +1728,30 @@ extern "C" int psg_step_evolve(psg_context *ctx, psg_step *steps, size_t n) {
 // would fail there), or one that must not pay the device-wide
 // synchronisation that cudaMalloc and cudaFree can imply while its other
 // streams are busy. The buffer holds PSG_NOALLOC_MAX_STEPS steps (2.25 MiB)
-// plus a status word; every device gets its own copy. There is one buffer per
-// device, not per context: calls that overlap in time on the same device
-// (two host threads, two contexts or two streams) race on it, and the caller
-// must serialise them.
-#define PSG_NOALLOC_MAX_DEVICES 64
+// plus a status word; every device gets its own copy, held until the process
+// exits. There is one buffer per device, not per context: calls that overlap
+// in time on the same device (two host threads, two contexts or two streams)
+// race on it, and the caller must serialise them.
 static constexpr size_t kNoallocStatusOffset = (size_t)PSG_NOALLOC_MAX_STEPS * sizeof(psg_step);
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocStatusOffset + 256];
 
-static std::mutex g_noalloc_mutex;
-static unsigned char *g_noalloc_base[PSG_NOALLOC_MAX_DEVICES];
-
-// Device address of the static buffer on ctx->device, looked up on the first
-// call for that device (with the device current) and cached afterwards.
-static int noalloc_buffer(psg_context *ctx, unsigned char **base) {
-	if (ctx->device < 0 || ctx->device >= PSG_NOALLOC_MAX_DEVICES)
-		return psg_fail(ctx, PSG_E_INVAL, "psg_step_evolve_noalloc: device %d beyond the %d supported", ctx->device,
-				PSG_NOALLOC_MAX_DEVICES);
-	std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-	if (!g_noalloc_base[ctx->device]) {
-		void *p = nullptr;
-		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-		if (e != cudaSuccess || !p)
-			return psg_cuda_fail(ctx, e != cudaSuccess ? e : cudaErrorInvalidSymbol,
-					"cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
-		g_noalloc_base[ctx->device] = (unsigned char *)p;
+// Device address of the static buffer on the current device. The lookup
+// loads this file's module on that device if it is not loaded yet (CUDA
+// loads modules lazily), and loading the module is what reserves the
+// buffer: psg_create() calls this once so that the reservation happens when
+// the context is made, before a host's pool allocator takes the device's
+// free memory. Each psg_step_evolve_noalloc() call looks the address up
+// again rather than caching it, so a host that reset the device in between
+// gets the buffer of the new primary context, not a stale address.
+int psg_noalloc_lookup(unsigned char **base) {
+	void *p = nullptr;
+	const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+	if (e != cudaSuccess || !p) {
+		cudaGetLastError();
+		return e != cudaSuccess ? (int)e : (int)cudaErrorInvalidSymbol;
 	}
-	*base = g_noalloc_base[ctx->device];
-	return PSG_OK;
+	*base = (unsigned char *)p;
+	return 0;
 }
 
 extern "C" int psg_step_evolve_noalloc(psg_context *ctx, psg_step *steps, size_t n) {
@@ -1770,8 +1765,8 @@ extern "C" int psg_step_evolve_noalloc(psg_context *ctx, psg_step *steps, size_t
 	if (!steps) return psg_fail(ctx, PSG_E_INVAL, "psg_step_evolve_noalloc: null steps");
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	unsigned char *base = nullptr;
-	const int rc = noalloc_buffer(ctx, &base);
-	if (rc) return rc;
+	const int e = psg_noalloc_lookup(&base);
+	if (e) return psg_cuda_fail(ctx, (cudaError_t)e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
 	psg_step *d = (psg_step *)base;
 	uint32_t *d_status = (uint32_t *)(base + kNoallocStatusOffset);
 	cudaStream_t st = ctx->stream;

@@ -25,4 +25,6 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python -m psphray_b200.data.import_tables /path/to/psphray")
+    main(sys.argv[1])

@@ -26,11 +26,17 @@ def test_every_declared_symbol_is_exported(built):
     assert not missing, missing
 
 
-def test_library_is_sm100a_only(built):
-    from psphray_b200 import api
-    # the device code is compiled for sm_100a alone (no PTX fallback to JIT)
-    data = open(api.LIB_PATH, "rb").read()
-    assert b"sm_100a" in data
+def test_build_targets_sm100a_only():
+    """Every nvcc step of the build (objects and the device link) carries
+    exactly one -gencode, arch=compute_100a,code=sm_100a: SASS for sm_100a
+    and no PTX that a driver could JIT for another architecture. The loaded
+    code's architecture is checked on the GPU (test_gpu_path.py)."""
+    from psphray_b200 import build
+    arch = build.ARCH
+    assert arch == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert build.NVCC_FLAGS.count("-gencode") == 1
+    assert all(not f.startswith("-arch") and "compute_" not in f.split("code=")[-1]
+               for f in build.NVCC_FLAGS if "code=" in f)
 
 
 def test_tables_match_reference(phys):

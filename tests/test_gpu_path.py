@@ -17,6 +17,16 @@ def _gpu(ctx, field, phys, flag=None, ppc=8):
     return ctx
 
 
+def test_loaded_code_is_sm100a(gpu_ctx):
+    """The runtime loaded SASS built for sm_100a (binaryVersion 100), not a
+    JIT translation of PTX for another architecture."""
+    import ctypes as C
+    from psphray_b200 import api
+    b, p = C.c_int(0), C.c_int(0)
+    assert api.lib().psg_device_arch(gpu_ctx.h, C.byref(b), C.byref(p)) == 0
+    assert b.value == 100 and p.value == 100, (b.value, p.value)
+
+
 @pytest.mark.parametrize("name", ["uniform16.npz", "lognormal16.npz", "edges.npz"])
 def test_tree_golden(gpu_ctx, phys, name):
     g = load_golden(name)

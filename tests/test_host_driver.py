@@ -93,3 +93,38 @@ def test_driver_epoch_matches_binding(built, tmp_path):
     assert np.array_equal(o["lasthit"], st["lasthit"])
     assert np.array_equal(o["hits"], st["hits"])
     assert np.max(np.abs(o["xHI"].astype(np.float64) - st["lambdaH"].astype(np.float32))) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_driver_resume_keeps_helium(built, tmp_path):
+    """An epoch with helium (--hmf 0.76, a 1e5 K blackbody reaching past
+    the HeII edge) writes its output; a second epoch starts from that file.
+    With --resume the particles the second epoch does not hit keep the
+    file's xHeI and xHeII exactly; without it the load derives them from ye
+    (psystem.c:340-358), which puts every helium electron on HeII first and
+    so moves the particles that held HeIII."""
+    from psphray_b200 import api
+    from psphray_b200.api import KERNEL_AKLINE, RATES_HUI
+    snap = _snapshot(tmp_path, n_side=16)
+    a = tmp_path / "a.psphray"
+    r = _run(snap, RATES_HUI, KERNEL_AKLINE, 40, 256, 40.0, a, "--hmf", "0.76", "--blackbody", "1e5")
+    assert r.returncode == 0, r.stderr
+    A = api.read_snapshot(str(a))
+    heIII = 1.0 - A["xHeI"].astype(np.float64) - A["xHeII"]
+    assert (heIII > 1e-3).sum() > 10
+    outs = {}
+    for tag, extra in (("resume", ["--resume"]), ("derive", [])):
+        b = tmp_path / f"b_{tag}.psphray"
+        r = _run(a, RATES_HUI, KERNEL_AKLINE, 1, 4, 0.01, b, "--hmf", "0.76", *extra)
+        assert r.returncode == 0, r.stderr
+        outs[tag] = api.read_snapshot(str(b))
+    B = outs["resume"]
+    cold = B["lasthit"] == 0
+    assert cold.sum() > 0.5 * len(cold)
+    assert np.array_equal(B["xHeI"][cold], A["xHeI"][cold])
+    assert np.array_equal(B["xHeII"][cold], A["xHeII"][cold])
+    D = outs["derive"]
+    cold_d = D["lasthit"] == 0
+    moved = cold_d & (heIII > 1e-3)
+    assert moved.sum() > 0
+    assert np.any(D["xHeII"][moved] != A["xHeII"][moved])

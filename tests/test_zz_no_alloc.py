@@ -1,8 +1,14 @@
 """psg_step_evolve_noalloc (a fixed in-library device buffer instead of the
 context's growable scratch) against psg_step_evolve, both through the C ABI,
-on two calls in a row; and its size limit. Both run the same kernel, so the
-results must agree to the tolerance of the step_evolve parity tests (they are
-in fact identical)."""
+on two calls in a row; against the oracle's solver directly; that repeated
+calls leave the device's free memory unchanged; and its size limit. Both
+entry points run the same kernel, so their results must agree to the
+tolerance of the step_evolve parity tests (they are in fact identical).
+
+It is for hosts that cannot allocate device memory while a step is under
+way (their pool allocator already holds the free memory, or they cannot
+afford the synchronisation of cudaMalloc), so the property that matters is
+that a call takes no memory at all."""
 import ctypes as C
 
 import numpy as np
@@ -53,6 +59,36 @@ def test_noalloc_matches_step_evolve(gpu_ctx, phys, phys_noniso, iso):
         assert np.max(np.abs(out["lambdaH"] - exp["lambdaH"])) < 1e-12
         assert np.max(np.abs(out["ie"] - exp["ie"]) / exp["ie"]) < 1e-12
         assert np.all(out["step_remain"] == exp["step_remain"])
+
+
+def test_noalloc_vs_oracle_and_no_memory_taken(gpu_ctx, phys):
+    """Isothermal steps against the restatement's closed form (1e-12, the
+    bar of psg_step_evolve's own oracle test); then ten calls up to the
+    buffer's size, with the device's free bytes read before and after."""
+    import torch
+    from oracle import Oracle
+    g = load_golden("uniform16.npz")
+    f = golden_field(g)
+    gpu_ctx.set_physics(phys)
+    orc = Oracle(f, phys)
+    steps = _steps(f, phys, float(g["tick_time"]), 31, 512)
+    steps["heat"] = 0.0
+    rc, out = _noalloc(gpu_ctx, steps)
+    assert rc == 0
+    exp = np.array([orc.solve(s["lambdaH"], s["ie"], 0.0, s["yGdepHI"], 0.0, s["time"], s["nH"], 1e4)[0]
+                    for s in steps])
+    assert np.max(np.abs(out["lambdaH"] - exp)) < 1e-12
+    big = _steps(f, phys, float(g["tick_time"]), 32, MAX_STEPS)
+    rc, _ = _noalloc(gpu_ctx, big)                 # warm-up at the full size
+    assert rc == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for i in range(10):
+        rc, _ = _noalloc(gpu_ctx, big[: MAX_STEPS - 997 * i])
+        assert rc == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, (free0, free1)
 
 
 def test_noalloc_rejects_oversize(gpu_ctx, phys):
