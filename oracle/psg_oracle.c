@@ -228,14 +228,18 @@ size_t po_trace(const po_tree *t, const float *pos, const float *sml, const int8
 			if (t->first_child[c] != -1) { c = t->first_child[c]; continue; }
 			for (int64_t p = t->head[c]; p != -1; p = t->next[p]) {
 				if (flag && (flag[p] & 1)) continue;
-				double dd2 = 0.0, proj = 0.0;
+				/* raytrace.c:176-183 as the reference's build runs it: float
+				 * differences and products; the double sums reassociated
+				 * by its -O3 -ffast-math into (y + z) + x (the order of
+				 * its compiled x86 code), not the source's x, y, z */
+				float pr[3], sq[3];
 				for (int d = 0; d < 3; d++) {
 					const float dd = pos[3 * p + d] - s[d];
-					const float pr = dd * dir[d];
-					const float sq = dd * dd;
-					proj += pr;
-					dd2 += sq;
+					pr[d] = dd * dir[d];
+					sq[d] = dd * dd;
 				}
+				const double proj = ((double)pr[1] + (double)pr[2]) + (double)pr[0];
+				const double dd2 = ((double)sq[1] + (double)sq[2]) + (double)sq[0];
 				const double dc = sqrt(dd2);
 				const double r2 = (dc - proj) * (dc + proj);
 				const float h2 = sml[p] * sml[p];

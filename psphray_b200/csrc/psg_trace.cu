@@ -60,7 +60,8 @@ __device__ __forceinline__ RayGeom load_ray(const psg_ray *__restrict__ rays, si
 }
 
 // The line test of raytrace.c:168-195: float differences and products,
-// double sums; accepted iff sml^2 >= (dc - proj)(dc + proj).
+// double sums (in the order the reference's build adds them: y and z
+// first, then x); accepted iff sml^2 >= (dc - proj)(dc + proj).
 // Candidates that miss by a wide margin are rejected in float first: the
 // float estimate r2f = d2f - projf^2 carries at most ~12 roundings of
 // relative size 2^-24 of d2 (about 7.2e-7 d2), so r2f - sml^2 > 1e-5 d2f
@@ -74,12 +75,12 @@ __device__ __forceinline__ bool line_hits_particle(const RayGeom &g, float4 q, d
 		const float r2f = __fsub_rn(d2f, rn_fmul(pf, pf));
 		if (__fsub_rn(r2f, rn_fmul(q.w, q.w)) > 1e-5f * d2f) return false;
 	}
-	double proj = (double)rn_fmul(dx, g.dir[0]);
-	proj = rn_dadd(proj, (double)rn_fmul(dy, g.dir[1]));
-	proj = rn_dadd(proj, (double)rn_fmul(dz, g.dir[2]));
-	double d2 = (double)rn_fmul(dx, dx);
-	d2 = rn_dadd(d2, (double)rn_fmul(dy, dy));
-	d2 = rn_dadd(d2, (double)rn_fmul(dz, dz));
+	// the three-term sums as the reference's build evaluates them: its
+	// -ffast-math lets the compiler reassociate the loop into (y + z) + x,
+	// which rounds differently from (x + y) + z in rare cases (1 ulp of d)
+	const double proj = rn_dadd((double)rn_fmul(dx, g.dir[0]),
+			rn_dadd((double)rn_fmul(dy, g.dir[1]), (double)rn_fmul(dz, g.dir[2])));
+	const double d2 = rn_dadd((double)rn_fmul(dx, dx), rn_dadd((double)rn_fmul(dy, dy), (double)rn_fmul(dz, dz)));
 	dc = __dsqrt_rn(d2);
 	r2 = rn_dmul(rn_dsub(dc, proj), rn_dadd(dc, proj));
 	return !((double)rn_fmul(q.w, q.w) < r2);
