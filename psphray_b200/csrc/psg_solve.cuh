@@ -196,15 +196,26 @@ __device__ __forceinline__ RhsCtx make_rhs_ctx(const PhysParams &P, double yeMET
 // isothermal): the same equations with the step length folded into the
 // rates, and fused multiply-adds (the last bits of an integrator's stage do
 // not matter; the isothermal closed form keeps the reference's roundings).
-// With REC, *rec receives d(yGrecHII)/ds.
-template <bool REC = false>
+// With REC, *rec receives d(yGrecHII)/ds. With T32 (the explicit
+// integrator's stages) the temperature and its logarithm, which only pick
+// the rate table's row and the interpolation weight, are computed in FP32:
+// the rates are FP32 table values anyway, and a 1e-7 relative error in log T
+// moves a rate by well under 1e-6 of itself (the integrator's rtol); the
+// state and its derivatives stay FP64. Without it (finite-difference
+// Jacobians, residual checks, the explicit build's steps) everything is FP64.
+template <bool REC = false, bool T32 = false>
 __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const double x[2], double dx[2],
 		double *rec = nullptr) {
 	const double xHI = x[0], xHII = 1.0 - x[0];
 	const double ye = xHII + P.he_e + cx.yeMET;
-	const double T = P.isothermal ? cx.T : cx.T_num * x[1] / __fma_rn(P.hmf, ye, cx.T_den0);
 	// the row of tabfun_get() and the offset into it (clamped rows: offset 0)
-	const double logT = log10(T);
+	double logT;
+	if (T32 && !P.isothermal) {
+		const float Tf = (float)cx.T_num * (float)x[1] / (float)__fma_rn(P.hmf, ye, cx.T_den0);
+		logT = (double)log10f(Tf);
+	} else {
+		logT = log10(P.isothermal ? cx.T : cx.T_num * x[1] / __fma_rn(P.hmf, ye, cx.T_den0));
+	}
 	long long idx = (long long)((logT - P.ar_min) * P.ar_step_inv);
 	double du;
 	if (idx < 0) {
@@ -273,7 +284,7 @@ __device__ __forceinline__ void dp_init_k1(DPState &S) {
 template <bool REC = false>
 __device__ __forceinline__ void dp_init(const PhysParams &P, const RhsCtx &cx, DPState &S) {
 	S.rec = 0.0;
-	rhs<REC>(P, cx, S.x, S.k1, &S.krec);
+	rhs<REC, true>(P, cx, S.x, S.k1, &S.krec);
 	S.t = 0.0;
 	S.steps = 0;
 	double h = 1.0;
@@ -303,18 +314,18 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 	const double *x = S.x, *k1 = S.k1;
 #define F __fma_rn
 	for (int i = 0; i < 2; i++) y[i] = F(h, a21 * k1[i], x[i]);
-	rhs<REC>(P, cx, y, k2, &r2);
+	rhs<REC, true>(P, cx, y, k2, &r2);
 	for (int i = 0; i < 2; i++) y[i] = F(h, F(a32, k2[i], a31 * k1[i]), x[i]);
-	rhs<REC>(P, cx, y, k3, &r3);
+	rhs<REC, true>(P, cx, y, k3, &r3);
 	for (int i = 0; i < 2; i++) y[i] = F(h, F(a43, k3[i], F(a42, k2[i], a41 * k1[i])), x[i]);
-	rhs<REC>(P, cx, y, k4, &r4);
+	rhs<REC, true>(P, cx, y, k4, &r4);
 	for (int i = 0; i < 2; i++) y[i] = F(h, F(a54, k4[i], F(a53, k3[i], F(a52, k2[i], a51 * k1[i]))), x[i]);
-	rhs<REC>(P, cx, y, k5, &r5);
+	rhs<REC, true>(P, cx, y, k5, &r5);
 	for (int i = 0; i < 2; i++)
 		y[i] = F(h, F(a65, k5[i], F(a64, k4[i], F(a63, k3[i], F(a62, k2[i], a61 * k1[i])))), x[i]);
-	rhs<REC>(P, cx, y, k6, &r6);
+	rhs<REC, true>(P, cx, y, k6, &r6);
 	for (int i = 0; i < 2; i++) yn[i] = F(h, F(b6, k6[i], F(b5, k5[i], F(b4, k4[i], F(b3, k3[i], b1 * k1[i])))), x[i]);
-	rhs<REC>(P, cx, yn, k7, &r7);
+	rhs<REC, true>(P, cx, yn, k7, &r7);
 	double err = 0.0;
 	for (int i = 0; i < 2; i++) {
 		const double e = h * F(e7, k7[i], F(e6, k6[i], F(e5, k5[i], F(e4, k4[i], F(e3, k3[i], e1 * k1[i])))));

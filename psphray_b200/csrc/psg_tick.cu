@@ -776,7 +776,7 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 		const RhsCtx cx = make_rhs_ctx(P, (double)r.yeMET, g, heat, r.time, rn_dmul(P.H_PER_MASS, (double)r.rho), T);
 		const double x0[2] = {r.lam0, ie0};
 		double f0[2];
-		rhs<REC>(P, cx, x0, f0, &r.krec);
+		rhs<REC, true>(P, cx, x0, f0, &r.krec);
 		r.k0 = f0[0];
 		r.k1 = f0[1];
 		rec[a - lo] = r;    // records of one tick, from its first active particle
