@@ -268,6 +268,7 @@ def main():
     ap.add_argument("--ref-ticks", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch shapes")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -298,6 +299,10 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")   # > 126 MB L2
     torch.cuda.synchronize(dev)
 
+    # launch shapes chosen by the library's autotuner on the first step's
+    # rays (every trial restores the particle state), before the warm-up
+    tune, tune_ms = (ctx.autotune(dev_rays[0].data_ptr(), R, T, 1, w.tick_time, reps=2)
+                     if not args.no_autotune else (ctx.tune(), None))
     for s in range(args.warmup):
         ctx.run_ticks_device(dev_rays[s].data_ptr(), R, T, 1 + s * T, w.tick_time)
     torch.cuda.synchronize(dev)
@@ -308,7 +313,7 @@ def main():
     torch.cuda.synchronize(dev)
     clocks.start()
     torch.cuda.nvtx.range_push("timed_steps")      # lets a profiler capture exactly these launches
-    total_ms, hits, launches, sat, active = 0.0, 0.0, 0.0, 0.0, 0.0
+    total_ms, hits, launches, sat, active, syncs = 0.0, 0.0, 0.0, 0.0, 0.0, 0.0
     per_step = []
     kms = {k: 0.0 for k in api.KERNELS}
     kn = {k: 0.0 for k in api.KERNELS}
@@ -325,6 +330,7 @@ def main():
         active += st["active"]
         per_step.append(round(e0.elapsed_time(e1), 3))
         launches += st["launches"]
+        syncs += st["host_syncs"]
     torch.cuda.synchronize(dev)
     torch.cuda.nvtx.range_pop()
     clk = clocks.stop()
@@ -430,7 +436,7 @@ def main():
         rctx.set_recombination(nrec=100)
         nrs = min(3, nsteps - 1)
         rctx.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
-        r_ms, r_hits, r_rays = 0.0, 0.0, 0.0
+        r_ms, r_hits, r_rays, r_syncs = 0.0, 0.0, 0.0, 0.0
         torch.cuda.nvtx.range_push("recombination_steps")
         for s in range(1, 1 + nrs):
             e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
@@ -441,10 +447,12 @@ def main():
             r_ms += e0.elapsed_time(e1)
             r_hits += st["hits"]
             r_rays += st["rec_rays"]
+            r_syncs += st["host_syncs"]
         torch.cuda.nvtx.range_pop()
         rctx.close()
         recombination = {"value": r_hits / (r_ms / 1e3), "unit": "hits/s", "ms_per_tick": r_ms / (nrs * T),
-                         "rec_rays_per_tick": r_rays / (nrs * T), "steps": nrs, "ticks_per_step": T}
+                         "rec_rays_per_tick": r_rays / (nrs * T), "steps": nrs, "ticks_per_step": T,
+                         "host_syncs_per_step": r_syncs / nrs}
 
         # helium and secondary ionisation (HOnly = false, hydrogen mass fraction
         # 0.76): the same particles and rays, three-species deposit with the
@@ -515,6 +523,8 @@ def main():
                        "parallelism": f"replicas{world}"},
             "gpu_s_per_sim_myr": t_max / sim_myr,
             "gpu_launches": launches,
+            "host_syncs_per_step": syncs / args.steps,
+            "tune": dict(tune, batch_ms=tune_ms),
             "saturated_deposits_per_step": sat / args.steps,
             "step_ms": per_step,
             "kernel_ms_per_step": {k: kms[k] / args.steps for k in api.KERNELS},

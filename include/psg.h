@@ -211,6 +211,7 @@ typedef struct {
 	double surrogate_accepted;  /* particle updates taken from the surrogate (psg_set_surrogate) */
 	double rec_rays;        /* recombination rays emitted (stat.rec_ray_count) */
 	double rec_photons;     /* photons they carried (stat.rec_photon_count) */
+	double host_syncs;      /* times the call waited for the device (host reads of device counts) */
 } psg_tick_stats;
 
 /* Runs nticks ticks; rays holds nray_per_tick rays for each tick, tick by
@@ -225,6 +226,32 @@ int psg_run_ticks(psg_context *ctx, const psg_ray *rays, size_t nray_per_tick, s
 /* Same with rays already in device memory. */
 int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, size_t nray_per_tick,
 		size_t nticks, int64_t first_tick, double tick_time, psg_tick_stats *stats);
+
+/* ---- launch shapes and their autotuner ------------------------------------ */
+/* No reference counterpart (the reference has one CPU code path): the shapes
+ * of the device path that do not change its results beyond FP64 rounding,
+ * chosen per device by timing. */
+typedef struct {
+	int trace_warps;        /* warps per traversal block, 1-16 (default 4) */
+	int deposit_long;       /* rays with more hits than this take a 128-thread group (default 96) ... */
+	int deposit_mid;        /* ... more than this a 512-thread block (default 384); fewer take a warp */
+	int update_minblocks;   /* 3: the integrator's registers capped for 3 resident blocks per
+	                         * multiprocessor (spilling the rest); 1: uncapped (default) */
+	int leaf_size;          /* particles per octree leaf: the reference's CFG_OCTTREE_PPC, 8; the hit
+	                         * lists are bit-exact only with the reference's leaves, so it is reported,
+	                         * never searched */
+} psg_tune;
+int psg_set_tune(psg_context *ctx, const psg_tune *tune);
+int psg_get_tune(psg_context *ctx, psg_tune *tune);
+/* Times candidate shapes on one batch of the caller's device rays (R rays
+ * per tick, K ticks, as psg_run_ticks_device), each `reps` times, one
+ * dimension after another (traversal warps, deposit thresholds, integrator
+ * registers), and keeps the fastest. The particle state is restored after
+ * every trial, so the call does not advance the run. The result becomes the
+ * context's shapes and the device's cached shapes, which contexts created
+ * later on that device start from. *best_ms: the kept shape's batch time. */
+int psg_autotune(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K, int64_t first_tick,
+		double tick_time, int reps, psg_tune *out, double *best_ms);
 
 /* ---- recombination rays (psphray.onTheSpot = false) ---------------------- */
 /* The recombination half of emit_rays() loop.c:197-232, 273-300, 322-368:

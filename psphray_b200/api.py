@@ -148,6 +148,15 @@ def read_snapshot(path: str) -> dict:
     return out
 
 
+class Tune(C.Structure):
+    """psg_tune: launch shapes that do not change results."""
+    _fields_ = [("trace_warps", C.c_int), ("deposit_long", C.c_int), ("deposit_mid", C.c_int),
+                ("update_minblocks", C.c_int), ("leaf_size", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class CSpectrum(C.Structure):
     _fields_ = [("eng", C.c_void_p), ("weight", C.c_void_p), ("n", C.c_int)]
 
@@ -156,7 +165,8 @@ class TickStats(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("hits", "saturated", "active", "lost_photons",
                                           "trace_ms", "tick_ms", "launches")] + [
         ("kernel_ms", C.c_double * len(KERNELS)), ("kernel_launches", C.c_double * len(KERNELS)),
-        ("surrogate_accepted", C.c_double), ("rec_rays", C.c_double), ("rec_photons", C.c_double)]
+        ("surrogate_accepted", C.c_double), ("rec_rays", C.c_double), ("rec_photons", C.c_double),
+        ("host_syncs", C.c_double)]
 
 
 def _stats(st: TickStats) -> dict:
@@ -166,6 +176,7 @@ def _stats(st: TickStats) -> dict:
     d["surrogate_accepted"] = st.surrogate_accepted
     d["rec_rays"] = st.rec_rays
     d["rec_photons"] = st.rec_photons
+    d["host_syncs"] = st.host_syncs
     return d
 
 
@@ -237,6 +248,10 @@ def lib() -> C.CDLL:
         "psg_get_rec_rays": ([vp, vp, vp, vp, sz, C.POINTER(sz)], C.c_int),
         "psg_get_rec_state": ([vp, vp, vp], C.c_int),
         "psg_set_rec_state": ([vp, vp, vp], C.c_int),
+        "psg_set_tune": ([vp, C.POINTER(Tune)], C.c_int),
+        "psg_get_tune": ([vp, C.POINTER(Tune)], C.c_int),
+        "psg_autotune": ([vp, vp, sz, sz, i64, dbl, C.c_int, C.POINTER(Tune), C.POINTER(dbl)], C.c_int),
+        "psg_device_arch": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -554,6 +569,27 @@ class Context:
         keep = [None if yGrecHII is None else np.ascontiguousarray(yGrecHII, np.float32),
                 None if srcmark is None else np.ascontiguousarray(srcmark, np.int32)]
         self._check(lib().psg_set_rec_state(self.h, *[_ptr(a) for a in keep]), "psg_set_rec_state")
+
+    def tune(self) -> dict:
+        t = Tune()
+        self._check(lib().psg_get_tune(self.h, C.byref(t)), "psg_get_tune")
+        return t.as_dict()
+
+    def set_tune(self, **kw):
+        t = Tune()
+        self._check(lib().psg_get_tune(self.h, C.byref(t)), "psg_get_tune")
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        self._check(lib().psg_set_tune(self.h, C.byref(t)), "psg_set_tune")
+
+    def autotune(self, d_rays_ptr: int, nray_per_tick: int, nticks: int, first_tick: int, tick_time: float,
+                 reps: int = 2) -> tuple[dict, float]:
+        """psg_autotune on device rays: the kept shapes and their batch time (ms)."""
+        t = Tune()
+        ms = C.c_double(0.0)
+        self._check(lib().psg_autotune(self.h, C.c_void_p(d_rays_ptr), nray_per_tick, nticks, first_tick, tick_time,
+                                       int(reps), C.byref(t), C.byref(ms)), "psg_autotune")
+        return t.as_dict(), ms.value
 
     def step_evolve(self, steps: np.ndarray) -> np.ndarray:
         steps = np.ascontiguousarray(steps, STEP_DTYPE)

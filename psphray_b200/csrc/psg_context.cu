@@ -6,6 +6,8 @@
 
 #include <vector>
 
+#include <mutex>
+
 #include "psg_internal.cuh"
 
 int psg_fail(psg_context *ctx, int code, const char *fmt, ...) {
@@ -57,13 +59,17 @@ extern "C" int psg_create(psg_context **out, int device) {
 			cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
 			cudaMalloc(&ctx->d_status, sizeof(uint32_t)) != cudaSuccess ||
 			cudaMemset(ctx->d_status, 0, sizeof(uint32_t)) != cudaSuccess ||
-			cudaMalloc(&ctx->d_counters, 32 * sizeof(unsigned long long)) != cudaSuccess) {
+			cudaMalloc(&ctx->d_counters, 32 * sizeof(unsigned long long)) != cudaSuccess ||
+			cudaMemset(ctx->d_counters, 0, 32 * sizeof(unsigned long long)) != cudaSuccess ||
+			cudaMalloc(&ctx->d_batch, sizeof(PsgBatchDev)) != cudaSuccess ||
+			cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
 		cudaGetLastError();
 		delete ctx;
 		return PSG_E_CUDA;
 	}
 	ctx->stream = ctx->own_stream;
 	for (auto &ev : ctx->ev) cudaEventCreate(&ev);
+	psg_tune_cached(device, &ctx->tune);     // the device's tuned shapes, if any
 	// reserve psg_step_evolve_noalloc's static buffer on this device now (its
 	// module loads on the first lookup), not on its first call
 	unsigned char *nb = nullptr;
@@ -111,6 +117,8 @@ extern "C" void psg_destroy(psg_context *ctx) {
 	if (ctx->d_kernel) cudaFree(ctx->d_kernel);
 	if (ctx->d_status) cudaFree(ctx->d_status);
 	if (ctx->d_counters) cudaFree(ctx->d_counters);
+	if (ctx->d_batch) cudaFree(ctx->d_batch);
+	psg_graphs_free(ctx);
 	if (ctx->d_emit) cudaFree(ctx->d_emit);
 	if (ctx->d_surr) cudaFree(ctx->d_surr);
 	if (ctx->d_lte) cudaFree(ctx->d_lte);
@@ -120,6 +128,103 @@ extern "C" void psg_destroy(psg_context *ctx) {
 	for (auto &ev : ctx->kev) if (ev) cudaEventDestroy(ev);
 	cudaStreamDestroy(ctx->own_stream);
 	delete ctx;
+}
+
+// ---- particle-state snapshot (autotuner trials, a recombination batch's undo) --
+namespace {
+struct StateArray {
+	void *p;
+	size_t item;
+};
+int state_arrays(psg_context *ctx, StateArray *out) {
+	int k = 0;
+	out[k++] = {ctx->d_lambdaH, sizeof(double)};
+	out[k++] = {ctx->d_ie, sizeof(float)};
+	out[k++] = {ctx->d_hits, sizeof(int32_t)};
+	out[k++] = {ctx->d_lasthit, sizeof(int64_t)};
+	out[k++] = {ctx->d_hstep, sizeof(float)};
+	out[k++] = {ctx->d_gcarry, sizeof(double)};
+	out[k++] = {ctx->d_ygrec, sizeof(float)};
+	out[k++] = {ctx->d_srcmark, sizeof(int32_t)};
+	out[k++] = {ctx->d_lamHeI, sizeof(double)};
+	out[k++] = {ctx->d_lamHeII, sizeof(double)};
+	out[k++] = {ctx->d_ygrecHe1, sizeof(float)};
+	out[k++] = {ctx->d_ygrecHe2, sizeof(float)};
+	out[k++] = {ctx->d_gcarryHe1, sizeof(double)};
+	out[k++] = {ctx->d_gcarryHe2, sizeof(double)};
+	return k;
+}
+}  // namespace
+
+int psg_state_save(psg_context *ctx) {
+	StateArray a[16];
+	const int na = state_arrays(ctx, a);
+	size_t total = 0;
+	for (int i = 0; i < na; i++) total += (a[i].item * ctx->n + 255) & ~(size_t)255;
+	char *snap = (char *)psg_scratch(ctx, S_SNAP, total);
+	if (!snap) return PSG_E_NOMEM;
+	for (int i = 0; i < na; i++) {
+		const size_t b = a[i].item * ctx->n;
+		if (a[i].p) PSG_CUDA(cudaMemcpyAsync(snap, a[i].p, b, cudaMemcpyDeviceToDevice, ctx->stream));
+		snap += (b + 255) & ~(size_t)255;
+	}
+	return PSG_OK;
+}
+
+int psg_state_restore(psg_context *ctx) {
+	StateArray a[16];
+	const int na = state_arrays(ctx, a);
+	char *snap = (char *)ctx->scratch[S_SNAP].p;
+	if (!snap) return psg_fail(ctx, PSG_E_INVAL, "no saved state");
+	for (int i = 0; i < na; i++) {
+		const size_t b = a[i].item * ctx->n;
+		if (a[i].p) PSG_CUDA(cudaMemcpyAsync(a[i].p, snap, b, cudaMemcpyDeviceToDevice, ctx->stream));
+		snap += (b + 255) & ~(size_t)255;
+	}
+	return PSG_OK;
+}
+
+// ---- launch shapes ----------------------------------------------------------
+namespace {
+std::mutex g_tune_mutex;
+psg_tune g_tune_cache[64];
+bool g_tune_have[64];
+int check_tune(const psg_tune *t) {
+	if (t->trace_warps < 1 || t->trace_warps > 16) return 0;
+	if (t->deposit_long < 32 || t->deposit_mid < t->deposit_long || t->deposit_mid > 1 << 20) return 0;
+	if (t->update_minblocks != 1 && t->update_minblocks != 3) return 0;
+	return t->leaf_size == 8;
+}
+}  // namespace
+
+bool psg_tune_cached(int device, psg_tune *t) {
+	if (device < 0 || device >= 64) return false;
+	std::lock_guard<std::mutex> lock(g_tune_mutex);
+	if (!g_tune_have[device]) return false;
+	*t = g_tune_cache[device];
+	return true;
+}
+
+void psg_tune_store(int device, const psg_tune *t) {
+	if (device < 0 || device >= 64) return;
+	std::lock_guard<std::mutex> lock(g_tune_mutex);
+	g_tune_cache[device] = *t;
+	g_tune_have[device] = true;
+}
+
+extern "C" int psg_set_tune(psg_context *ctx, const psg_tune *tune) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!tune || !check_tune(tune))
+		return psg_fail(ctx, PSG_E_INVAL, "psg_set_tune: trace_warps 1-16, 32 <= deposit_long <= deposit_mid, "
+				"update_minblocks 1 or 3, leaf_size 8");
+	ctx->tune = *tune;
+	return PSG_OK;
+}
+
+extern "C" int psg_get_tune(psg_context *ctx, psg_tune *tune) {
+	if (!ctx || !tune) return PSG_E_INVAL;
+	*tune = ctx->tune;
+	return PSG_OK;
 }
 
 extern "C" const char *psg_last_error(const psg_context *ctx) {

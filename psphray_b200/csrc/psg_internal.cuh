@@ -29,8 +29,18 @@
 enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
 	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
-	S_EMIT, S_MAP, S_ALONG, S_MLP, S_LOG, S_SURR, S_REC, S_RECW, S_RECK, S_RECRAYS,
+	S_EMIT, S_MAP, S_ALONG, S_MLP, S_LOG, S_SURR, S_REC, S_RECW, S_RECK, S_RECRAYS, S_SNAP,
 	S_NSLOTS
+};
+
+// Per-call values the tick kernels read on the device, so that a captured
+// batch replays unchanged for any first tick and any rays.
+struct PsgBatchDev {
+	int64_t tick0;          // the batch's first tick (the recombination path advances it per tick)
+	double tick_time;       // internal time per tick
+	const psg_ray *rays;    // the rays the ticks deposit (the traced ones)
+	const psg_ray *src;     // the caller's source rays (recombination path: copied tick by tick)
+	int64_t k;              // recombination path: the tick's index within the call
 };
 
 struct psg_buf {
@@ -124,8 +134,19 @@ struct psg_context {
 
 	uint32_t *d_status = nullptr;
 	unsigned long long *d_counters = nullptr;   // 32 device counters: 1 capped deposits, 2 lost photons,
-	                                            // 4 longest hit list, 8 surrogate accepts, 9 trace ray
-	                                            // cursor, 16-23 sort size classes
+	                                            // 3 longest list of a call, 4 longest hit list, 5 hit total,
+	                                            // 6 active particles, 7 hits of a call, 8 surrogate accepts,
+	                                            // 9 trace ray cursor, 10-13 recombination emission,
+	                                            // 14 recombination rays of a call, 16-23 sort size classes
+	PsgBatchDev *d_batch = nullptr;             // per-call values read by the tick kernels (device)
+	int sms = 148;                              // multiprocessors of the device
+	size_t hit_cap = 0;                         // hits the sorted-list buffers hold
+	size_t batch_cap = 0;                       // hits the tick batches' per-hit buffers hold
+	unsigned sort_grid[8] = {};                 // persistent grids of the per-ray sort's classes
+	psg_tune tune{4, 96, 384, 1, 8};            // launch shapes (psg_set_tune, psg_autotune)
+	long host_syncs = 0;                        // host synchronisations of the current call
+	void *graphs = nullptr;                     // captured tick batches (psg_tick.cu)
+	int use_graphs = 1;                         // replay captured batches (0: issue launches one by one)
 
 	// scratch, grown on demand
 	psg_buf scratch[S_NSLOTS];
@@ -155,6 +176,15 @@ int psg_noalloc_lookup(unsigned char **base);
 
 // scratch buffer slot `slot` with at least `bytes`; returns nullptr on failure
 void *psg_scratch(psg_context *ctx, int slot, size_t bytes);
+// releases the captured tick batches of a context (psg_tick.cu)
+void psg_graphs_free(psg_context *ctx);
+// copies every per-particle array a tick changes into S_SNAP / back
+// (psg_context.cu)
+int psg_state_save(psg_context *ctx);
+int psg_state_restore(psg_context *ctx);
+// the device's cached launch shapes, if psg_autotune ran on it in this process
+bool psg_tune_cached(int device, psg_tune *t);
+void psg_tune_store(int device, const psg_tune *t);
 
 
 // Per-launch timing: mark_begin/mark_end bracket a group of launches of one
@@ -177,9 +207,10 @@ int psg_permute_particles(psg_context *ctx, const uint32_t *g);
 
 // the surrogate's tick (psg_surrogate.cu)
 struct PhysParams;
-int psg_surrogate_tick(psg_context *ctx, int t, int nact_t, const int32_t *tick_act, const uint32_t *act_ipar,
-		const double *act_g, const double *act_heat, const PhysParams &P, int64_t tick, double tick_time,
-		uint32_t *rej, unsigned *nrej, int sms);
+int psg_surrogate_prepare(psg_context *ctx);
+int psg_surrogate_tick(psg_context *ctx, int t, const int32_t *tick_act, const uint32_t *act_ipar,
+		const double *act_g, const double *act_heat, const PhysParams &P, const PsgBatchDev *B, uint32_t *rej,
+		unsigned *nrej);
 
 // recombination rays (psg_recomb.cu): the tick-by-tick loop used by
 // psg_run_ticks_device when not on the spot, and the LTE table build
@@ -189,8 +220,16 @@ int psg_build_lte(psg_context *ctx, const psg_xs_table *xs);
 #define PSG_LTE_NLOGT 128
 #define PSG_LTE_NFREQ 1024
 
-// tree / trace entry points used across units
-int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_db);
+// tree / trace entry points used across units (psg_trace.cu)
+struct PsgTraceFill {
+	size_t nhit;                    // hits of all rays
+	unsigned long long maxcount;    // longest hit list
+	size_t scap;                    // slab capacity per ray
+};
+int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTraceFill *tf);
+int psg_trace_sort_prepare(psg_context *ctx, size_t nray, size_t cap, unsigned long long maxcount);
+int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned long long maxcount, int want_kern);
+int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_kern);
 
 // ---- device helpers ------------------------------------------------------------
 // Single-rounding float/double ops: the reference is compiled for x86-64 SSE

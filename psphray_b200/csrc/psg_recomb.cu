@@ -267,6 +267,7 @@ int emit_rec(psg_context *ctx, int64_t tick, size_t cap, psg_ray *out, size_t *M
 	unsigned cnt[3] = {0, 0, 0};
 	PSG_CUDA(cudaMemcpyAsync(cnt, d_count, sizeof(unsigned) * 3, cudaMemcpyDeviceToHost, st));
 	PSG_CUDA(cudaStreamSynchronize(st));
+	ctx->host_syncs++;
 	const size_t M = (size_t)cnt[0] + cnt[1] + cnt[2];
 	if (M > cap) return psg_fail(ctx, PSG_E_OVERFLOW, "recombination rays: %zu > capacity %zu", M, cap);
 	*M_out = M;
@@ -339,20 +340,21 @@ int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t 
 	double *d_nph = (double *)(ctx->d_counters + 10);
 	PSG_CUDA(cudaMemsetAsync(d_nph, 0, sizeof(double), st));
 	psg_tick_stats acc{}, one{};
-	int sms = 148;
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-	double rec_rays = 0.0;
+	const int sms = ctx->sms;
+	double rec_rays = 0.0, syncs = 0.0;
 	long launches = 0;
 	for (size_t k = 0; k < K; k++) {
 		const int64_t tick = first_tick + (int64_t)k;
 		PSG_CUDA(cudaMemcpyAsync(buf, d_rays + k * R, sizeof(psg_ray) * R, cudaMemcpyDeviceToDevice, st));
 		ctx->launches = 0;
+		ctx->host_syncs = 0;
 		size_t M = 0;
 		if (tick > 1 && ctx->rec_nrec != 0) {      // loop.c:197
 			const int rc = emit_rec(ctx, tick, cap, buf + R, &M);
 			if (rc) return rc;
 		}
 		const long emit_launches = ctx->launches;
+		syncs += (double)ctx->host_syncs;
 		ctx->rec_last = M;
 		ctx->rec_last_R = R;
 		ctx->rec_last_kmax = cap;
@@ -369,6 +371,7 @@ int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t 
 		acc.active += one.active;
 		acc.lost_photons += one.lost_photons;
 		acc.trace_ms += one.trace_ms;
+		syncs += one.host_syncs;
 		acc.tick_ms += one.tick_ms;
 		for (int g = 0; g < PSG_K_NKERNELS; g++) {
 			acc.kernel_ms[g] += one.kernel_ms[g];
@@ -381,6 +384,7 @@ int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t 
 	ctx->launches = launches;
 	if (stats) {
 		acc.launches = (double)launches;
+		acc.host_syncs = syncs + 1.0;
 		acc.rec_rays = rec_rays;
 		acc.rec_photons = nph;
 		*stats = acc;

@@ -138,8 +138,8 @@ template <bool RAW>
 __global__ void __launch_bounds__(128, 4) k_surrogate(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const double *__restrict__ act_g, const double *__restrict__ act_heat,
 		double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit,
-		const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P, int64_t tick,
-		double tick_time, const char *__restrict__ blob, float tol, uint32_t *__restrict__ rej,
+		const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P,
+		const PsgBatchDev *__restrict__ B, const char *__restrict__ blob, float tol, uint32_t *__restrict__ rej,
 		unsigned *__restrict__ nrej, unsigned long long *__restrict__ nacc, uint32_t *__restrict__ status, RawIO io) {
 	extern __shared__ __align__(1024) char smem[];
 	char *A = smem;
@@ -148,6 +148,8 @@ __global__ void __launch_bounds__(128, 4) k_surrogate(int t, const int32_t *__re
 	uint32_t *tmem_slot = (uint32_t *)(Wsm + BLOB_BYTES + 16);
 	const int tid = threadIdx.x, warp = tid >> 5;
 	const int lo = RAW ? 0 : tick_act[t], hi = RAW ? io.n : tick_act[t + 1];
+	const int64_t tick = RAW ? 0 : B->tick0 + t;
+	const double tick_time = RAW ? 0.0 : B->tick_time;
 	const int ntile = (hi - lo + M - 1) / M;
 	if ((int)blockIdx.x >= ntile) return;
 
@@ -358,16 +360,20 @@ extern "C" int psg_set_surrogate(psg_context *ctx, const float *params, const fl
 
 // Runs the surrogate over tick t's active particles; rejected ones are
 // listed in rej (count in *nrej, on the device).
-int psg_surrogate_tick(psg_context *ctx, int t, int nact_t, const int32_t *tick_act, const uint32_t *act_ipar,
-		const double *act_g, const double *act_heat, const PhysParams &P, int64_t tick, double tick_time,
-		uint32_t *rej, unsigned *nrej, int sms) {
+int psg_surrogate_prepare(psg_context *ctx) {
+	PSG_CUDA(cudaFuncSetAttribute(k_surrogate<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+	return PSG_OK;
+}
+
+int psg_surrogate_tick(psg_context *ctx, int t, const int32_t *tick_act, const uint32_t *act_ipar,
+		const double *act_g, const double *act_heat, const PhysParams &P, const PsgBatchDev *B, uint32_t *rej,
+		unsigned *nrej) {
 	static_assert(SMEM_BYTES < 200 * 1024, "smem");
 	cudaStream_t st = ctx->stream;
-	PSG_CUDA(cudaFuncSetAttribute(k_surrogate<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-	const int ntile = (nact_t + M - 1) / M;
-	const unsigned grid = (unsigned)std::min(ntile, sms * 4);
+	// a persistent grid: the tick's particle count is read on the device
+	const unsigned grid = (unsigned)(ctx->sms * 4);
 	k_surrogate<false><<<grid, 128, SMEM_BYTES, st>>>(t, tick_act, act_ipar, act_g, act_heat, ctx->d_lambdaH,
-			ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, tick, tick_time, (const char *)ctx->d_surr,
+			ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, B, (const char *)ctx->d_surr,
 			ctx->surr_tol, rej, nrej, ctx->d_counters + 8, ctx->d_status, RawIO{nullptr, nullptr, 0});
 	PSG_CHECK_LAUNCH();
 	return PSG_OK;
@@ -387,7 +393,7 @@ extern "C" int psg_surrogate_forward(psg_context *ctx, const float *d_x, size_t 
 	PhysParams P{};
 	PSG_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
 	k_surrogate<true><<<grid, 128, SMEM_BYTES, ctx->stream>>>(0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-			nullptr, nullptr, nullptr, P, 0, 0.0, (const char *)ctx->d_surr, ctx->surr_tol, nullptr, nullptr, nullptr,
+			nullptr, nullptr, nullptr, P, nullptr, (const char *)ctx->d_surr, ctx->surr_tol, nullptr, nullptr, nullptr,
 			ctx->d_status, RawIO{d_x, d_y, (int)n});
 	PSG_CHECK_LAUNCH();
 	uint32_t st = 0;

@@ -101,34 +101,58 @@ __global__ void k_slot_keys(size_t nray, int nray_per_tick, int shift, const int
 	}
 }
 
+// The key sort runs over the buffers' capacity (a size fixed between
+// batches, so a captured batch replays for any hit count): entries past the
+// batch's hits (nhit = off[nray], read here) take the largest key and sort
+// last.
 template <typename KT>
-__global__ void k_slots(size_t nhit, const KT *__restrict__ skeys, const uint32_t *__restrict__ svals,
-		uint32_t *__restrict__ slot, int32_t *__restrict__ head) {
-	const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (k >= nhit) return;
-	slot[svals[k]] = (uint32_t)k;
-	head[k] = (k == 0 || skeys[k] != skeys[k - 1]) ? 1 : 0;
+__global__ void k_pad_keys(size_t cap, const int64_t *__restrict__ off, size_t nray, KT *__restrict__ keys,
+		uint32_t *__restrict__ vals) {
+	const size_t nhit = (size_t)off[nray];
+	for (size_t h = nhit + blockIdx.x * (size_t)blockDim.x + threadIdx.x; h < cap; h += (size_t)gridDim.x * blockDim.x) {
+		keys[h] = ~(KT)0;
+		vals[h] = (uint32_t)h;
+	}
 }
 
 template <typename KT>
-__global__ void k_active(size_t nhit, int shift, const KT *__restrict__ skeys, const int32_t *__restrict__ head,
-		const int32_t *__restrict__ scan, uint32_t *__restrict__ act_ipar, uint32_t *__restrict__ act_seg,
-		KT *__restrict__ act_key) {
-	const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (k >= nhit) return;
-	if (!head[k]) return;
-	const int a = scan[k];
-	act_ipar[a] = (uint32_t)(skeys[k] & (((KT)1 << shift) - 1));
-	act_seg[a] = (uint32_t)k;
-	act_key[a] = skeys[k];
+__global__ void k_slots(size_t cap, const int64_t *__restrict__ off, size_t nray, const KT *__restrict__ skeys,
+		const uint32_t *__restrict__ svals, uint32_t *__restrict__ slot, int32_t *__restrict__ head) {
+	const size_t nhit = (size_t)off[nray];
+	for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < cap; k += (size_t)gridDim.x * blockDim.x) {
+		if (k < nhit) {
+			slot[svals[k]] = (uint32_t)k;
+			head[k] = (k == 0 || skeys[k] != skeys[k - 1]) ? 1 : 0;
+		} else {
+			head[k] = 0;
+		}
+	}
 }
 
-// first active entry of every tick (and the total at index nticks)
 template <typename KT>
-__global__ void k_tick_bounds(int nticks, int shift, const KT *__restrict__ act_key, int nact,
-		uint32_t *__restrict__ act_seg, uint32_t nhit, int32_t *__restrict__ tick_act) {
+__global__ void k_active(const int64_t *__restrict__ off, size_t nray, int shift, const KT *__restrict__ skeys,
+		const int32_t *__restrict__ head, const int32_t *__restrict__ scan, uint32_t *__restrict__ act_ipar,
+		uint32_t *__restrict__ act_seg, KT *__restrict__ act_key) {
+	const size_t nhit = (size_t)off[nray];
+	for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nhit; k += (size_t)gridDim.x * blockDim.x) {
+		if (!head[k]) continue;
+		const int a = scan[k];
+		act_ipar[a] = (uint32_t)(skeys[k] & (((KT)1 << shift) - 1));
+		act_seg[a] = (uint32_t)k;
+		act_key[a] = skeys[k];
+	}
+}
+
+// first active entry of every tick (and the total at index nticks); the
+// active total is the heads' scan at the last hit, read here
+template <typename KT>
+__global__ void k_tick_bounds(int nticks, int shift, const KT *__restrict__ act_key, const int64_t *__restrict__ off,
+		size_t nray, const int32_t *__restrict__ head, const int32_t *__restrict__ scan,
+		uint32_t *__restrict__ act_seg, int32_t *__restrict__ tick_act, unsigned long long *__restrict__ nact_out) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t > nticks) return;
+	const size_t nhit = (size_t)off[nray];
+	const int nact = nhit ? scan[nhit - 1] + head[nhit - 1] : 0;
 	int lo = 0, hi = nact;
 	if (t < nticks) {
 		const KT want = (KT)t << shift;
@@ -140,7 +164,10 @@ __global__ void k_tick_bounds(int nticks, int shift, const KT *__restrict__ act_
 		lo = nact;
 	}
 	tick_act[t] = lo;
-	if (t == nticks) act_seg[nact] = nhit;
+	if (t == nticks) {
+		act_seg[nact] = (uint32_t)nhit;
+		atomicAdd(nact_out, (unsigned long long)nact);     // over the call's batches
+	}
 }
 
 __device__ __forceinline__ bool below_cutoff(double TM, double Nph) {
@@ -627,17 +654,27 @@ __device__ void deposit_ray_gen(const psg_ray &ray, int64_t h0, int64_t h1, int 
 	if (t == 0 && !skip_ray) lost += TM;
 }
 
-// Blocks [0, nlong) take one long ray each with all DEP_THREADS threads;
-// the next nmid_blocks take four middle rays each, 128 threads per ray; the
-// remaining blocks take DEP_THREADS/32 short rays, one per warp.
+// A tick's rays by deposit group: long rays (a whole block each), middle
+// rays (a 128-thread quarter each) and short rays (a warp each), as ranges
+// of the batch's three ray lists. Filled on the device (k_tick_rays).
+struct TickRays {
+	int l0, nlong, m0, nmid, s0, nshort, pad0, pad1;
+};
+
+// Work units of a tick: [0, nlong) take one long ray each with all
+// DEP_THREADS threads; the next ceil(nmid/4) take four middle rays each, 128
+// threads per ray; the rest take DEP_THREADS/32 short rays, one per warp.
+// The grid is persistent: blocks claim units from the tick's counter, so
+// the launch needs no count from the host.
 #define DEP_THREADS 512
 #define DEP_LONG 96       // more hits than this: a group of threads, else a warp
 #define DEP_MID 384       // more hits than this: the whole block, else a 128-thread quarter
 
 template <bool GEN, bool AFF>
-__global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__restrict__ rays,
-		const uint32_t *__restrict__ long_rays, int nlong, const uint32_t *__restrict__ mid_rays, int nmid,
-		const uint32_t *__restrict__ short_rays, int nshort,
+__global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(int t, const TickRays *__restrict__ tick_rays,
+		unsigned *__restrict__ unit_ctr, const PsgBatchDev *__restrict__ B,
+		const uint32_t *__restrict__ long_rays, const uint32_t *__restrict__ mid_rays,
+		const uint32_t *__restrict__ short_rays,
 		const int64_t *__restrict__ off, const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
 		const uint32_t *__restrict__ slot, const double *__restrict__ lambdaH, const float *__restrict__ mass,
 		PhysParams P, int want_heat, double *__restrict__ acc, int nacc, unsigned long long *__restrict__ n_sat,
@@ -645,41 +682,53 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 	__shared__ DepShared sh_block;
 	__shared__ DepShared sh_quarter[4];
 	__shared__ DepShared sh_warp[DEP_THREADS / 32];
+	__shared__ int s_unit;
 	const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 	unsigned nsat = 0;
 	double tm_lost = 0.0;
+	const psg_ray *__restrict__ rays = B->rays;      // read here: a replayed graph serves any call's rays
+	const TickRays T = tick_rays[t];
+	const int nlong = T.nlong, nmid = T.nmid, nshort = T.nshort;
 	const int nmid_blocks = (nmid + 3) / 4;
-	if ((int)blockIdx.x < nlong) {
-		const uint32_t r = long_rays[blockIdx.x];
-		if (GEN)
-			deposit_ray_gen<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
-					want_heat, acc, nacc, sh_block, nsat, tm_lost, 0);
-		else
-			deposit_ray<DEP_THREADS, AFF>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
-					want_heat, acc, sh_block, nsat, tm_lost, 0);
-	} else if ((int)blockIdx.x < nlong + nmid_blocks) {
-		const int q = tid >> 7;
-		const int m = ((int)blockIdx.x - nlong) * 4 + q;
-		if (m < nmid) {
-			const uint32_t r = mid_rays[m];
+	const int nunits = nlong + nmid_blocks + (nshort + DEP_THREADS / 32 - 1) / (DEP_THREADS / 32);
+	for (;;) {
+		if (tid == 0) s_unit = (int)atomicAdd(unit_ctr + t, 1u);
+		__syncthreads();
+		const int u = s_unit;
+		__syncthreads();       // (also: the previous unit's shared state is no longer read)
+		if (u >= nunits) break;
+		if (u < nlong) {
+			const uint32_t r = long_rays[T.l0 + u];
 			if (GEN)
-				deposit_ray_gen<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
-						want_heat, acc, nacc, sh_quarter[q], nsat, tm_lost, 1 + q);
+				deposit_ray_gen<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
+						want_heat, acc, nacc, sh_block, nsat, tm_lost, 0);
 			else
-				deposit_ray<128, AFF>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
-						want_heat, acc, sh_quarter[q], nsat, tm_lost, 1 + q);
-		}
-	} else {
-		const int w = ((int)blockIdx.x - nlong - nmid_blocks) * (DEP_THREADS / 32) + wid;
-		if (w < nshort) {
-			const uint32_t r = short_rays[w];
-			if (off[r + 1] > off[r]) {
+				deposit_ray<DEP_THREADS, AFF>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
+						want_heat, acc, sh_block, nsat, tm_lost, 0);
+		} else if (u < nlong + nmid_blocks) {
+			const int q = tid >> 7;
+			const int m = (u - nlong) * 4 + q;
+			if (m < nmid) {
+				const uint32_t r = mid_rays[T.m0 + m];
 				if (GEN)
-					deposit_ray_gen<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
-							want_heat, acc, nacc, sh_warp[wid], nsat, tm_lost, 0);
+					deposit_ray_gen<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
+							want_heat, acc, nacc, sh_quarter[q], nsat, tm_lost, 1 + q);
 				else
-					deposit_ray<32, AFF>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
-							want_heat, acc, sh_warp[wid], nsat, tm_lost, 0);
+					deposit_ray<128, AFF>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
+							want_heat, acc, sh_quarter[q], nsat, tm_lost, 1 + q);
+			}
+		} else {
+			const int w = (u - nlong - nmid_blocks) * (DEP_THREADS / 32) + wid;
+			if (w < nshort) {
+				const uint32_t r = short_rays[T.s0 + w];
+				if (off[r + 1] > off[r]) {
+					if (GEN)
+						deposit_ray_gen<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
+								want_heat, acc, nacc, sh_warp[wid], nsat, tm_lost, 0);
+					else
+						deposit_ray<32, AFF>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
+								want_heat, acc, sh_warp[wid], nsat, tm_lost, 0);
+				}
 			}
 		}
 	}
@@ -688,15 +737,38 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(const psg_ray *__res
 	if (lane == 0 && tm_lost != 0.0) atomicAdd(lost, tm_lost);
 }
 
+// Per tick, the ranges of its rays in the long / middle / short lists, from
+// the classes' running counts (the lists keep ray order, so each tick's rays
+// are a run of each list).
+__global__ void k_tick_rays(int K, size_t R, size_t nray, const unsigned long long *__restrict__ cls,
+		const unsigned long long *__restrict__ scan, TickRays *__restrict__ out) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= K) return;
+	const unsigned long long tot = scan[nray - 1] + cls[nray - 1];
+	const unsigned long long c0 = scan[(size_t)t * R], c1 = (t + 1 < K) ? scan[(size_t)(t + 1) * R] : tot;
+	TickRays T;
+	T.l0 = (int)(uint32_t)c0;
+	T.m0 = (int)(uint32_t)(c0 >> 32);
+	T.nlong = (int)(uint32_t)c1 - T.l0;
+	T.nmid = (int)(uint32_t)(c1 >> 32) - T.m0;
+	T.s0 = (int)((size_t)t * R) - T.l0 - T.m0;
+	T.nshort = (int)R - T.nlong - T.nmid;
+	T.pad0 = T.pad1 = 0;
+	out[t] = T;
+}
+
 // Rays of the batch split into long, middle and short lists (ray order
 // kept): cls = 1 for long, 1 << 32 for middle, so one scan counts both.
-__global__ void k_ray_class(size_t nray, const int64_t *__restrict__ off, unsigned long long *__restrict__ cls) {
+// (dep_long and dep_mid: the thresholds, DEP_LONG and DEP_MID unless tuned)
+__global__ void k_ray_class(size_t nray, const int64_t *__restrict__ off, int dep_long, int dep_mid,
+		unsigned long long *__restrict__ cls) {
 	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (r >= nray) return;
 	const int64_t n = off[r + 1] - off[r];
-	cls[r] = n > DEP_MID ? 1ull : (n > DEP_LONG ? (1ull << 32) : 0ull);
+	cls[r] = n > dep_mid ? 1ull : (n > dep_long ? (1ull << 32) : 0ull);
 }
 
+// (each list has room for every ray of the batch)
 __global__ void k_ray_lists(size_t nray, const unsigned long long *__restrict__ cls,
 		const unsigned long long *__restrict__ scan, uint32_t *__restrict__ long_rays,
 		uint32_t *__restrict__ mid_rays, uint32_t *__restrict__ short_rays) {
@@ -712,15 +784,20 @@ __global__ void k_ray_lists(size_t nray, const unsigned long long *__restrict__ 
 // Active particles of the batch whose deposit segment is longer than a warp
 // (particles next to a source are hit by nearly every ray); flag[na] = 0 so
 // that the scan's last entry is the total.
-__global__ void k_act_class(size_t na, const uint32_t *__restrict__ act_seg, int32_t *__restrict__ flag) {
-	const size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (a > na) return;
-	flag[a] = (a < na && act_seg[a + 1] - act_seg[a] > 32) ? 1 : 0;
+// The active count of the batch, nact = tick_act[K], is read on the device;
+// flags cover the capacity cap + 1 (zero past nact) so the scan's size is
+// fixed.
+__global__ void k_act_class(size_t cap, const int32_t *__restrict__ tick_act, int K,
+		const uint32_t *__restrict__ act_seg, int32_t *__restrict__ flag) {
+	const size_t na = (size_t)tick_act[K];
+	for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a <= cap; a += (size_t)gridDim.x * blockDim.x)
+		flag[a] = (a < na && act_seg[a + 1] - act_seg[a] > 32) ? 1 : 0;
 }
-__global__ void k_act_lists(size_t na, const int32_t *__restrict__ flag, const int32_t *__restrict__ scan,
-		uint32_t *__restrict__ long_act) {
-	const size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (a < na && flag[a]) long_act[scan[a]] = (uint32_t)a;
+__global__ void k_act_lists(const int32_t *__restrict__ tick_act, int K, const int32_t *__restrict__ flag,
+		const int32_t *__restrict__ scan, uint32_t *__restrict__ long_act) {
+	const size_t na = (size_t)tick_act[K];
+	for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a < na; a += (size_t)gridDim.x * blockDim.x)
+		if (flag[a]) long_act[scan[a]] = (uint32_t)a;
 }
 // first long entry of every tick
 __global__ void k_tick_long(int K, const int32_t *__restrict__ tick_act, const int32_t *__restrict__ scan,
@@ -759,6 +836,7 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 			act_g[a] = g;
 			act_heat[a] = heat;
 		}
+		if (!rec) return;      // sums only: the integrator builds its own records
 		UpdRec r;
 		r.time = rn_dmul((double)(tick - lasthit[p]), tick_time);
 		r.lam0 = lambdaH[p];
@@ -795,87 +873,122 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 	if (st) atomicOr(status, st);
 }
 
+// One long deposit segment [b0, b1) summed by a warp: lanes strided over
+// it (eight loads in flight per lane), then a fixed butterfly; every lane
+// ends with the totals.
+__device__ __forceinline__ void warp_segment_sum(const double *__restrict__ acc, int want_heat, uint32_t b0,
+		uint32_t b1, int lane, double &sg, double &sh, int &sn) {
+	sg = 0.0;
+	sh = 0.0;
+	sn = 0;
+	uint32_t k = b0 + lane;
+	if (want_heat) {
+		const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
+		for (; k + 7 * 32 < b1; k += 8 * 32) {
+			double2 v[8];
+#pragma unroll
+			for (int u = 0; u < 8; u++) v[u] = acc2[k + 32 * u];
+#pragma unroll
+			for (int u = 0; u < 8; u++)
+				if (v[u].x >= 0.0) { sg += v[u].x; sh += v[u].y; sn++; }
+		}
+		for (; k < b1; k += 32) {
+			const double2 d = acc2[k];
+			if (d.x >= 0.0) { sg += d.x; sh += d.y; sn++; }
+		}
+	} else {
+		for (; k + 7 * 32 < b1; k += 8 * 32) {
+			double v[8];
+#pragma unroll
+			for (int u = 0; u < 8; u++) v[u] = acc[k + 32 * u];
+#pragma unroll
+			for (int u = 0; u < 8; u++)
+				if (v[u] >= 0.0) { sg += v[u]; sn++; }
+		}
+		for (; k < b1; k += 32) {
+			const double d = acc[k];
+			if (d >= 0.0) { sg += d; sn++; }
+		}
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		sg += __shfl_xor_sync(0xffffffffu, sg, o);
+		sh += __shfl_xor_sync(0xffffffffu, sh, o);
+		sn += __shfl_xor_sync(0xffffffffu, sn, o);
+	}
+}
+
+// The tick's long segments only (more deposits than a warp), a warp each:
+// their sums for the integrator (act_g, act_heat) and the deposit counters.
+// The integrator sums the short ones itself while it builds its records.
+__global__ void __launch_bounds__(256) k_sum_long(int t, const uint32_t *__restrict__ act_ipar,
+		const uint32_t *__restrict__ act_seg, const double *__restrict__ acc, int want_heat,
+		const uint32_t *__restrict__ long_act, const int32_t *__restrict__ tick_long, int32_t *__restrict__ hits,
+		double *__restrict__ act_g, double *__restrict__ act_heat) {
+	const int lane = threadIdx.x & 31;
+	const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+	for (int e = tick_long[t] + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); e < tick_long[t + 1];
+			e += nwarp) {
+		const int a = (int)long_act[e];
+		double sg, sh;
+		int sn;
+		warp_segment_sum(acc, want_heat, act_seg[a], act_seg[a + 1], lane, sg, sh, sn);
+		if (lane == 0) {
+			act_g[a] = sg;
+			act_heat[a] = sh;
+			hits[act_ipar[a]] += sn;
+		}
+	}
+}
+
 // Per-particle sums of one tick's deposits (photons/NH, heat, deposit count)
-// in slot order. The first long_blocks blocks take the tick's long segments,
-// a warp each: lanes strided over the segment (eight loads in flight per
-// lane), then a fixed butterfly. The other blocks take the short ones, a
-// thread each. Particles are in leaf order, so the long ones are neighbours;
-// giving each its own warp keeps them from piling up on a few warps.
+// in slot order. Warps first take the tick's long segments, a warp each
+// (particles are in leaf order, so the long ones are neighbours; giving each
+// its own warp keeps them from piling up on a few warps), then every thread
+// takes short ones, a thread each. The grid is persistent (both loops stride
+// over the tick's ranges, read on the device).
 template <bool ISO, bool REC>
 __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
 		const double *__restrict__ acc, int want_heat,
-		const uint32_t *__restrict__ long_act, int nlong, int long_blocks,
+		const uint32_t *__restrict__ long_act, const int32_t *__restrict__ tick_long,
 		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat,
 		double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit,
 		const float *__restrict__ rho, const float *__restrict__ yeMET, const float *__restrict__ hstep,
-		UpdRec *__restrict__ rec, const double *__restrict__ gcarry, PhysParams P, int64_t tick, double tick_time,
-		uint32_t *__restrict__ status) {
-	if ((int)blockIdx.x < long_blocks) {
-		const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
-		const int lane = threadIdx.x & 31;
-		if (e >= nlong) return;
+		UpdRec *__restrict__ rec, const double *__restrict__ gcarry, PhysParams P,
+		const PsgBatchDev *__restrict__ B, uint32_t *__restrict__ status) {
+	const int64_t tick = B->tick0 + t;
+	const double tick_time = B->tick_time;
+	const int lo = tick_act[t], hi = tick_act[t + 1];
+	const int lane = threadIdx.x & 31;
+	const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+	for (int e = tick_long[t] + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); e < tick_long[t + 1];
+			e += nwarp) {
 		const int a = (int)long_act[e];
-		const uint32_t b0 = act_seg[a], b1 = act_seg[a + 1];
-		double sg = 0.0, sh = 0.0;
-		int sn = 0;
-		uint32_t k = b0 + lane;
-		if (want_heat) {
-			const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
-			for (; k + 7 * 32 < b1; k += 8 * 32) {
-				double2 v[8];
-#pragma unroll
-				for (int u = 0; u < 8; u++) v[u] = acc2[k + 32 * u];
-#pragma unroll
-				for (int u = 0; u < 8; u++)
-					if (v[u].x >= 0.0) { sg += v[u].x; sh += v[u].y; sn++; }
-			}
-			for (; k < b1; k += 32) {
-				const double2 d = acc2[k];
-				if (d.x >= 0.0) { sg += d.x; sh += d.y; sn++; }
-			}
-		} else {
-			for (; k + 7 * 32 < b1; k += 8 * 32) {
-				double v[8];
-#pragma unroll
-				for (int u = 0; u < 8; u++) v[u] = acc[k + 32 * u];
-#pragma unroll
-				for (int u = 0; u < 8; u++)
-					if (v[u] >= 0.0) { sg += v[u]; sn++; }
-			}
-			for (; k < b1; k += 32) {
-				const double d = acc[k];
-				if (d >= 0.0) { sg += d; sn++; }
-			}
-		}
-#pragma unroll
-		for (int o = 16; o > 0; o >>= 1) {
-			sg += __shfl_xor_sync(0xffffffffu, sg, o);
-			sh += __shfl_xor_sync(0xffffffffu, sh, o);
-			sn += __shfl_xor_sync(0xffffffffu, sn, o);
-		}
+		double sg, sh;
+		int sn;
+		warp_segment_sum(acc, want_heat, act_seg[a], act_seg[a + 1], lane, sg, sh, sn);
 		if (lane == 0)
 			finish_particle<ISO, REC>(a, sg, sh, sn, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
-					hstep, rec, tick_act[t], gcarry, P, tick, tick_time, status);
-		return;
+					hstep, rec, lo, gcarry, P, tick, tick_time, status);
 	}
-	const int a = tick_act[t] + (blockIdx.x - long_blocks) * blockDim.x + threadIdx.x;
-	if (a >= tick_act[t + 1]) return;
-	const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
-	if (s1 - s0 > 32) return;
-	double g = 0.0, heat = 0.0;
-	int nh = 0;
-	for (uint32_t k = s0; k < s1; k++) {
-		if (want_heat) {
-			const double2 d = reinterpret_cast<const double2 *>(acc)[k];
-			if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
-		} else {
-			const double d = acc[k];
-			if (d >= 0.0) { g += d; nh++; }
+	for (int a = lo + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi; a += (int)(gridDim.x * blockDim.x)) {
+		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
+		if (s1 - s0 > 32) continue;
+		double g = 0.0, heat = 0.0;
+		int nh = 0;
+		for (uint32_t k = s0; k < s1; k++) {
+			if (want_heat) {
+				const double2 d = reinterpret_cast<const double2 *>(acc)[k];
+				if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
+			} else {
+				const double d = acc[k];
+				if (d >= 0.0) { g += d; nh++; }
+			}
 		}
+		finish_particle<ISO, REC>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
+				hstep, rec, lo, gcarry, P, tick, tick_time, status);
 	}
-	finish_particle<ISO, REC>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET, hstep,
-			rec, tick_act[t], gcarry, P, tick, tick_time, status);
 }
 
 // update_pars() loop.c:653-770, not isothermal: every lane integrates one
@@ -887,33 +1000,42 @@ struct StiffItem {
 	double t, h, x0, x1, yeMET, g, heat, time, nH, T, rec;
 	uint32_t p;
 };
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
-			"l"(gmem_src)
-			: "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
 #define UPD_WARPS 8
+// Where the integrator's records come from: the tick's active particles,
+// their deposit segments (short ones are summed while the record is built;
+// long ones, or all when `pre_all`, were summed into act_g/act_heat before)
+// and the particle state.
+struct UpdSrc {
+	const uint32_t *act_ipar, *act_seg;
+	const double *acc;
+	const double *act_g, *act_heat;
+	int want_heat, pre_all;
+	int32_t *hits;
+	const float *rho, *yeMET;
+};
+
 // Every warp owns two buffers of 32 records in shared memory: it claims
-// chunks of 32 particles from the tick's cursor and copies their records
-// with cp.async one chunk ahead, so a lane whose particle is done takes the
-// next one from shared memory without waiting on a gather.
-template <bool REC>
-__global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const int32_t *__restrict__ tick_act,
-		const UpdRec *__restrict__ rec, double *__restrict__ lambdaH, float *__restrict__ ie,
-		int64_t *__restrict__ lasthit, float *__restrict__ hstep, PhysParams P, int64_t tick,
+// chunks of 32 particles from the tick's cursor and builds their records
+// (the summed deposits, the state, the step length) one chunk ahead, so a
+// lane whose particle is done takes the next one from shared memory; the
+// gathers of a chunk are paid once per 32 particles, not per integrator
+// step, and no record goes through device memory. MINB caps the registers
+// for that many resident blocks per multiprocessor (psg_tune).
+template <bool REC, int MINB>
+__global__ void __launch_bounds__(32 * UPD_WARPS, MINB) k_update_queue(int t, const int32_t *__restrict__ tick_act,
+		const UpdSrc src, double *__restrict__ lambdaH, float *__restrict__ ie,
+		int64_t *__restrict__ lasthit, float *__restrict__ hstep, PhysParams P, const PsgBatchDev *__restrict__ B,
 		unsigned *__restrict__ cursor, StiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff,
 		const uint32_t *__restrict__ alist, const unsigned *__restrict__ nalist, uint32_t *__restrict__ status) {
 	__shared__ UpdRec buf[UPD_WARPS][2][32];
+	const int64_t tick = B->tick0 + t;
+	const double tick_time = B->tick_time;
 	// the tick's particles, or only those listed in alist (the surrogate's rejects)
 	const int lo = tick_act[t], hi = tick_act[t + 1];
 	const unsigned n = alist ? *nalist : (unsigned)(hi - lo);
 	const int lane = threadIdx.x & 31;
 	const unsigned lt_mask = (1u << lane) - 1u;
-	UpdRec (*B)[32] = buf[threadIdx.x >> 5];
+	UpdRec (*WB)[32] = buf[threadIdx.x >> 5];
 	auto fetch = [&](int b) -> int {
 		unsigned base = 0;
 		if (lane == 0) base = atomicAdd(cursor, 32u);
@@ -922,19 +1044,45 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 		if (lane < cnt) {
 			const unsigned k = base + lane;
 			const int a = alist ? (int)alist[k] : lo + (int)k;
-			const char *src = (const char *)(rec + (a - lo));
-			char *dst = (char *)&B[b][lane];
-#pragma unroll
-			for (int q = 0; q < 5; q++) cp_async16(dst + 16 * q, src + 16 * q);
+			const uint32_t p = src.act_ipar[a];
+			double g = 0.0, heat = 0.0;
+			const uint32_t s0 = src.act_seg[a], s1 = src.act_seg[a + 1];
+			if (src.pre_all || s1 - s0 > 32) {
+				g = src.act_g[a];
+				heat = src.act_heat[a];
+			} else {
+				int nh = 0;
+				for (uint32_t q = s0; q < s1; q++) {
+					if (src.want_heat) {
+						const double2 d = reinterpret_cast<const double2 *>(src.acc)[q];
+						if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
+					} else {
+						const double d = src.acc[q];
+						if (d >= 0.0) { g += d; nh++; }
+					}
+				}
+				src.hits[p] += nh;
+			}
+			UpdRec r;
+			r.time = rn_dmul((double)(tick - lasthit[p]), tick_time);
+			r.lam0 = lambdaH[p];
+			r.g = g;
+			r.heat = heat;
+			r.ie0 = ie[p];
+			r.rho = src.rho[p];
+			r.yeMET = src.yeMET[p];
+			r.hstep = hstep[p];
+			r.p = p;
+			r.pad0 = 0u;
+			r.k0 = r.k1 = r.krec = 0.0;
+			WB[b][lane] = r;
 		}
-		cp_async_commit();
+		__syncwarp();
 		return cnt;
 	};
 	int avail[2];
 	avail[0] = fetch(0);
 	avail[1] = fetch(1);
-	cp_async_wait<1>();
-	__syncwarp();
 	int cur = 0, used = 0;
 	bool exhausted = false;
 	DPState S;
@@ -952,8 +1100,6 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 					exhausted = true;
 					break;
 				}
-				cp_async_wait<0>();
-				__syncwarp();
 				cur ^= 1;
 				used = 0;
 				avail[cur ^ 1] = fetch(cur ^ 1);
@@ -962,17 +1108,15 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 			const int rank = __popc(need & lt_mask);
 			const int take = min(__popc(need), left);
 			if (!have && rank < take) {
-				const UpdRec &r = B[cur][used + rank];
+				const UpdRec &r = WB[cur][used + rank];
 				p = r.p;
 				const double ie0 = (double)r.ie0;
 				const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, r.lam0), P.he_e));
 				cx = make_rhs_ctx(P, (double)r.yeMET, r.g, r.heat, r.time, rn_dmul(P.H_PER_MASS, (double)r.rho), T);
 				S.x[0] = r.lam0;
 				S.x[1] = ie0;
-				S.k1[0] = r.k0;
-				S.k1[1] = r.k1;
 				S.rec = 0.0;
-				S.krec = r.krec;
+				rhs<REC, true>(P, cx, S.x, S.k1, &S.krec);
 				atol1 = DP_ATOL1_REL * fabs(ie0) + 1e-300;
 				dp_init_k1(S);
 				// the particle's last step proposal is a better first
@@ -1009,7 +1153,6 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 			}
 		}
 	}
-	cp_async_wait<0>();
 	if (st) atomicOr(status, st);
 }
 
@@ -1018,7 +1161,9 @@ __global__ void __launch_bounds__(32 * UPD_WARPS) k_update_queue(int t, const in
 template <bool REC>
 __global__ void __launch_bounds__(64) k_update_stiff(const StiffItem *__restrict__ stiff,
 		const unsigned *__restrict__ nstiff, double *__restrict__ lambdaH, float *__restrict__ ie,
-		int64_t *__restrict__ lasthit, PhysParams P, int64_t tick, uint32_t *__restrict__ status) {
+		int64_t *__restrict__ lasthit, PhysParams P, const PsgBatchDev *__restrict__ B, int t,
+		uint32_t *__restrict__ status) {
+	const int64_t tick = B->tick0 + t;
 	const unsigned n = *nstiff;
 	uint32_t st = 0;
 	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1042,11 +1187,11 @@ __global__ void __launch_bounds__(64) k_update_stiff(const StiffItem *__restrict
 // to the particle's next update (loop.c:745), heat is not (loop.c:769).
 __global__ void __launch_bounds__(128) k_update_euler(int t, const int32_t *__restrict__ tick_act,
 		const UpdRec *__restrict__ rec, double *__restrict__ lambdaH, float *__restrict__ ie,
-		int64_t *__restrict__ lasthit, double *__restrict__ gcarry, PhysParams P, int64_t tick,
+		int64_t *__restrict__ lasthit, double *__restrict__ gcarry, PhysParams P, const PsgBatchDev *__restrict__ B,
 		uint32_t *__restrict__ status) {
-	const int lo = tick_act[t];
-	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
-	if (a >= tick_act[t + 1]) return;
+	const int64_t tick = B->tick0 + t;
+	const int lo = tick_act[t], hi = tick_act[t + 1];
+	for (int a = lo + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi; a += (int)(gridDim.x * blockDim.x)) {
 	const UpdRec r = rec[a - lo];
 	const double ie0 = (double)r.ie0;
 	const double T = ieye2T(P, ie0, rn_dadd(rn_dsub(1.0, r.lam0), P.he_e));
@@ -1063,6 +1208,7 @@ __global__ void __launch_bounds__(128) k_update_euler(int t, const int32_t *__re
 	lasthit[r.p] = tick;
 	gcarry[r.p] = r.g * remain;
 	if (st) atomicOr(status, st);
+	}
 }
 
 // update_pars() loop.c:647-776 with helium: one thread per active particle
@@ -1099,10 +1245,13 @@ __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__re
 		int want_heat,
 		int32_t *__restrict__ hits, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P,
-		int64_t tick, double tick_time, HeStiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff,
+		const PsgBatchDev *__restrict__ B, HeStiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff,
 		uint32_t *__restrict__ status) {
-	const int a = tick_act[t] + blockIdx.x * blockDim.x + threadIdx.x;
-	if (a >= tick_act[t + 1]) return;
+	const int64_t tick = B->tick0 + t;
+	const double tick_time = B->tick_time;
+	const int hi = tick_act[t + 1];
+	for (int a = tick_act[t] + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi;
+			a += (int)(gridDim.x * blockDim.x)) {
 	const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
 	double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
 	int nh = 0;
@@ -1168,7 +1317,7 @@ __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__re
 			it.h = hh;
 			it.p = p;
 			stiff[atomicAdd(nstiff, 1u)] = it;
-			return;
+			continue;
 		}
 		if (!(x[3] >= 0.0)) st |= PSG_ST_IE_NEG;
 		for (int k = 0; k < 4; k++)
@@ -1179,6 +1328,7 @@ __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__re
 	}
 	he_write(P, p, x, rec, s.T, tick, lambdaH, ie, lasthit);
 	if (st) atomicOr(status, st);
+	}
 }
 
 // The stiff helium particles of a tick, one thread each (their number is
@@ -1186,7 +1336,9 @@ __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__re
 // stopped.
 __global__ void __launch_bounds__(64) k_update_he_stiff(const HeStiffItem *__restrict__ stiff,
 		const unsigned *__restrict__ nstiff, double *__restrict__ lambdaH, float *__restrict__ ie,
-		int64_t *__restrict__ lasthit, PhysParams P, int64_t tick, uint32_t *__restrict__ status) {
+		int64_t *__restrict__ lasthit, PhysParams P, const PsgBatchDev *__restrict__ B, int t,
+		uint32_t *__restrict__ status) {
+	const int64_t tick = B->tick0 + t;
 	const unsigned n = *nstiff;
 	uint32_t st = 0;
 	for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1209,10 +1361,11 @@ __global__ void __launch_bounds__(64) k_update_he_stiff(const HeStiffItem *__res
 __global__ void k_log_pre(int t, const int32_t *__restrict__ tick_act, const uint32_t *__restrict__ act_ipar,
 		const double *__restrict__ act_g, const double *__restrict__ act_heat, const double *__restrict__ lambdaH,
 		const float *__restrict__ ie, const int64_t *__restrict__ lasthit, const float *__restrict__ rho,
-		const float *__restrict__ yeMET, PhysParams P, int64_t tick, double tick_time, float *__restrict__ feat) {
-	const int lo = tick_act[t];
-	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
-	if (a >= tick_act[t + 1]) return;
+		const float *__restrict__ yeMET, PhysParams P, const PsgBatchDev *__restrict__ B, float *__restrict__ feat) {
+	const int64_t tick = B->tick0 + t;
+	const double tick_time = B->tick_time;
+	const int lo = tick_act[t], hi = tick_act[t + 1];
+	for (int a = lo + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi; a += (int)(gridDim.x * blockDim.x)) {
 	const uint32_t p = act_ipar[a];
 	const double time = rn_dmul((double)(tick - lasthit[p]), tick_time);
 	const double lam0 = lambdaH[p], ie0 = (double)ie[p];
@@ -1222,29 +1375,30 @@ __global__ void k_log_pre(int t, const int32_t *__restrict__ tick_act, const uin
 	float f[PSG_SURR_NFEAT];
 	surr_features(cx, lam0, ie0, f);
 	for (int i = 0; i < PSG_SURR_NFEAT; i++) feat[(size_t)(a - lo) * 8 + i] = f[i];
+	}
 }
 
 __global__ void k_log_post(int t, const int32_t *__restrict__ tick_act, const uint32_t *__restrict__ act_ipar,
 		const double *__restrict__ lambdaH, const float *__restrict__ ie, const float *__restrict__ yeMET,
 		PhysParams P, const float *__restrict__ feat, float *__restrict__ out, size_t cap,
 		unsigned long long *__restrict__ count) {
-	const int lo = tick_act[t];
-	const int a = lo + blockIdx.x * blockDim.x + threadIdx.x;
-	if (a >= tick_act[t + 1]) return;
+	const int lo = tick_act[t], hi = tick_act[t + 1];
+	for (int a = lo + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi; a += (int)(gridDim.x * blockDim.x)) {
 	const uint32_t p = act_ipar[a];
 	const double lam1 = lambdaH[p];
 	const double T1 = ieye2T(P, (double)ie[p], rn_dadd(rn_dsub(1.0, lam1), P.he_e));
 	const float *f = feat + (size_t)(a - lo) * 8;
 	const float y0 = (float)(surr_logit(lam1) - (double)f[2]);
 	const float y1 = (float)(log10(fmax(T1, 1e-300)) - (double)f[1]);
-	if (!isfinite(y0) || !isfinite(y1)) return;
+	if (!isfinite(y0) || !isfinite(y1)) continue;
 	const unsigned long long row = atomicAdd(count, 1ull);
-	if (row >= cap) return;
+	if (row >= cap) continue;
 	float *o = out + row * 8;
 	for (int i = 0; i < PSG_SURR_NFEAT; i++) o[i] = f[i];
 	o[5] = y0;
 	o[6] = y1;
 	o[7] = 0.0f;
+	}
 }
 
 __global__ void k_step_evolve(psg_step *steps, size_t n, PhysParams P, uint32_t *status) {
@@ -1325,60 +1479,519 @@ static int check_status(psg_context *ctx) {
 	return PSG_OK;
 }
 
-// The per-batch by-particle order: sort (tick, ipar) keys of all hits,
-// give every hit its slot, list the distinct (tick, particle) pairs with the
-// first slot of each, and the first pair of every tick. Layout of S_ACT:
-// head, scan, act_ipar, act_seg (hb+1 each), tick_act (K+1, 16-aligned),
-// act_key (hb+1, 16-aligned).
-template <typename KT>
-static int build_slots(psg_context *ctx, size_t nray, size_t R, size_t K, size_t nhit, int shift, int tbits,
-		const int64_t *off64, const uint32_t *hit_ipar, int nacc, int *nact_out) {
-	cudaStream_t st = ctx->stream;
-	const size_t hb = nhit ? nhit : 1;
-	KT *keys = (KT *)psg_scratch(ctx, S_KEYS, sizeof(KT) * 2 * hb);
-	uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
-	uint32_t *slot = (uint32_t *)psg_scratch(ctx, S_SLOT, sizeof(uint32_t) * hb);
-	double *acc = (double *)psg_scratch(ctx, S_ACC, sizeof(double) * hb * nacc);
-	char *actm = (char *)psg_scratch(ctx, S_ACT, sizeof(int32_t) * 4 * (hb + 1) + sizeof(int32_t) * (K + 2)
-			+ sizeof(KT) * (hb + 1) + 1024);
-	if (!keys || !vals || !slot || !acc || !actm) return PSG_E_NOMEM;
-	int32_t *head = (int32_t *)actm;
-	int32_t *hscan = head + (hb + 1);
-	uint32_t *act_ipar = (uint32_t *)(hscan + (hb + 1));
-	uint32_t *act_seg = act_ipar + (hb + 1);
-	int32_t *tick_act = (int32_t *)(((uintptr_t)(act_seg + hb + 1) + 15) & ~(uintptr_t)15);
-	KT *act_key = (KT *)(((uintptr_t)(tick_act + K + 1) + 15) & ~(uintptr_t)15);
-	int nact = 0;
-	if (nhit) {
-		k_slot_keys<KT><<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, shift, off64, hit_ipar, keys, vals);
-		PSG_CHECK_LAUNCH();
-		const int endbit = shift + tbits;
-		size_t tmp = 0;
-		PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, keys + hb, vals, vals + hb, (int64_t)nhit, 0, endbit, st));
-		void *dt = psg_scratch(ctx, S_CUB, tmp);
-		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceRadixSort::SortPairs(dt, tmp, keys, keys + hb, vals, vals + hb, (int64_t)nhit, 0, endbit, st));
-		k_slots<KT><<<blocks(nhit, 256), 256, 0, st>>>(nhit, keys + hb, vals + hb, slot, head);
-		PSG_CHECK_LAUNCH();
-		tmp = 0;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, head, hscan, (int)nhit, st));
-		dt = psg_scratch(ctx, S_CUB, tmp);
-		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, head, hscan, (int)nhit, st));
-		k_active<KT><<<blocks(nhit, 256), 256, 0, st>>>(nhit, shift, keys + hb, head, hscan, act_ipar, act_seg, act_key);
-		PSG_CHECK_LAUNCH();
-		ctx->launches += 3;
-		int last_scan = 0, last_head = 0;
-		PSG_CUDA(cudaMemcpyAsync(&last_scan, hscan + nhit - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-		PSG_CUDA(cudaMemcpyAsync(&last_head, head + nhit - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-		PSG_CUDA(cudaStreamSynchronize(st));
-		nact = last_scan + last_head;
+// ---- one batch of ticks on the host side -------------------------------------
+//
+// A batch is: the traversal of all its rays (psg_trace_fill), then one host
+// synchronisation that reads the hit total; everything after it -- the
+// per-ray sort, the by-particle order, the ray and particle classes and the
+// K ticks of deposit and update -- is issued by enqueue_batch() with sizes
+// fixed by the batch's shape and buffer capacities, counts read on the
+// device, and no allocation. That part is captured once as a CUDA graph and
+// replayed for every later batch of the same shape (first tick, tick length
+// and rays are read from ctx->d_batch). A last synchronisation reads the
+// counters and the status word: two per batch.
+
+__global__ void k_set_batch(PsgBatchDev *b, int64_t tick0, double tick_time, const psg_ray *rays,
+		const psg_ray *src) {
+	b->tick0 = tick0;
+	b->tick_time = tick_time;
+	b->rays = rays;
+	b->src = src;
+	b->k = 0;
+}
+
+namespace {
+
+// Buffers and sizes of one batch, all fixed before anything is issued.
+struct BatchPlan {
+	size_t R = 0, K = 0, nray = 0;
+	size_t nhit = 0;            // the batch's hits (used only by the long-list sort, which is never captured)
+	size_t cap = 0;             // hits the per-hit buffers hold (>= the batch's hits)
+	size_t pcap = 0;            // particles one tick can update (min(n, cap))
+	unsigned long long maxcount = 0;
+	int shift = 1, tbits = 0, key64 = 0, nacc = 1, want_heat = 0;
+	bool gen = false, helium = false, iso = false, euler = false, surr = false, aff = false, feat_on = false;
+	// CUB temporary sizes
+	size_t sort_tmp = 0, head_tmp = 0, cls_tmp = 0, act_tmp = 0;
+	// grids
+	unsigned dep_grid = 0, red_grid = 0, queue_grid = 0, he_grid = 0, euler_grid = 0, log_grid = 0;
+	int queue_minb = 1;         // the integrator's register limit: resident blocks per SM
+};
+
+struct GraphEntry {
+	std::vector<unsigned long long> key;
+	cudaGraphExec_t exec = nullptr;
+	long launches = 0;
+};
+struct GraphCache {
+	std::vector<GraphEntry> e;
+};
+
+template <typename KF>
+unsigned occ_grid(const psg_context *ctx, KF kern, int threads, size_t smem = 0) {
+	int per_sm = 1;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess) {
+		cudaGetLastError();
+		per_sm = 1;
 	}
-	k_tick_bounds<KT><<<blocks(K + 1, 128), 128, 0, st>>>((int)K, shift, act_key, nact, act_seg, (uint32_t)nhit, tick_act);
-	PSG_CHECK_LAUNCH();
-	ctx->launches++;
-	*nact_out = nact;
+	return (unsigned)(std::max(per_sm, 1) * ctx->sms);
+}
+
+// Layout of the per-batch scratch slots.
+struct ActView {
+	int32_t *head, *hscan;
+	uint32_t *act_ipar, *act_seg;
+	int32_t *tick_act;
+	void *act_key;
+};
+ActView act_view(psg_context *ctx, const BatchPlan &pl) {
+	ActView v;
+	const size_t hb = pl.cap;
+	char *actm = (char *)ctx->scratch[S_ACT].p;
+	v.head = (int32_t *)actm;
+	v.hscan = v.head + (hb + 1);
+	v.act_ipar = (uint32_t *)(v.hscan + (hb + 1));
+	v.act_seg = v.act_ipar + (hb + 1);
+	v.tick_act = (int32_t *)(((uintptr_t)(v.act_seg + hb + 1) + 15) & ~(uintptr_t)15);
+	v.act_key = (void *)(((uintptr_t)(v.tick_act + pl.K + 1) + 15) & ~(uintptr_t)15);
+	return v;
+}
+size_t act_bytes(const BatchPlan &pl) {
+	return sizeof(int32_t) * 4 * (pl.cap + 1) + sizeof(int32_t) * (pl.K + 2) +
+			(pl.key64 ? 8 : 4) * (pl.cap + 1) + 1024;
+}
+struct UpdView {
+	double *act_g, *act_heat;
+	unsigned *cursors, *nstiff, *nrej, *dep_ctr;
+	TickRays *tick_rays;
+	StiffItem *stiff;
+	uint32_t *rej;
+};
+UpdView upd_view(psg_context *ctx, const BatchPlan &pl) {
+	UpdView v;
+	char *um = (char *)ctx->scratch[S_UPD].p;
+	v.act_g = (double *)um;
+	v.act_heat = v.act_g + pl.cap;
+	v.cursors = (unsigned *)(v.act_heat + pl.cap);
+	v.nstiff = v.cursors + (pl.K + 1);
+	v.nrej = v.nstiff + (pl.K + 1);
+	v.dep_ctr = v.nrej + (pl.K + 1);
+	v.tick_rays = (TickRays *)(((uintptr_t)(v.dep_ctr + pl.K + 1) + 31) & ~(uintptr_t)31);
+	v.stiff = (StiffItem *)(((uintptr_t)(v.tick_rays + pl.K) + 15) & ~(uintptr_t)15);
+	v.rej = (uint32_t *)(v.stiff + (pl.iso ? 0 : pl.pcap));
+	return v;
+}
+size_t upd_bytes(const BatchPlan &pl) {
+	return sizeof(double) * 2 * pl.cap + sizeof(unsigned) * 4 * (pl.K + 1) + sizeof(TickRays) * pl.K +
+			(pl.iso ? 0 : sizeof(StiffItem) * pl.pcap) + (pl.surr ? sizeof(uint32_t) * pl.pcap : 0) + 512;
+}
+
+// Sizes, capacities and every buffer of the batch (allocates; before any
+// capture). tf: the traversal's totals.
+int plan_batch(psg_context *ctx, size_t R, size_t K, const PsgTraceFill &tf, BatchPlan &pl) {
+	pl.R = R;
+	pl.K = K;
+	pl.nray = R * K;
+	pl.maxcount = tf.maxcount;
+	pl.nhit = tf.nhit;
+	// grow-only capacity with an eighth of headroom, so batches of similar
+	// hit counts share one captured graph
+	if (tf.nhit > ctx->batch_cap) {
+		size_t c = tf.nhit + tf.nhit / 8;
+		c = (c + 65535) & ~(size_t)65535;
+		ctx->batch_cap = c;
+	}
+	pl.cap = std::max<size_t>(ctx->batch_cap, 1);
+	pl.pcap = std::max<size_t>(std::min(ctx->n, pl.cap), 1);
+	while (pl.shift < 32 && (1ull << pl.shift) < (unsigned long long)ctx->n) pl.shift++;
+	while ((1ull << pl.tbits) < (unsigned long long)K) pl.tbits++;
+	pl.key64 = pl.shift + pl.tbits > 32;
+	pl.want_heat = !ctx->flags.isothermal;
+	pl.gen = !ctx->flags.h_only || ctx->flags.secondary_ionization;
+	pl.helium = !ctx->flags.h_only;
+	pl.nacc = pl.helium ? 4 : (pl.want_heat ? 2 : 1);
+	pl.iso = ctx->flags.isothermal != 0;
+	pl.euler = ctx->flags.euler != 0;
+	// (the network does not model the recombination photons: on the spot only)
+	pl.surr = !pl.iso && !pl.euler && ctx->surr_on && !ctx->flags.adiabatic && ctx->flags.on_the_spot &&
+			ctx->flags.h_only;
+	pl.feat_on = ctx->log_buf && !pl.iso && !pl.helium;
+	// capped hits settled by the affine-map scan when the last batch had many
+	pl.aff = ctx->sat_frac > 1e-3;
+	const size_t cap = pl.cap, nray = pl.nray;
+
+	int rc = psg_trace_sort_prepare(ctx, nray, cap, pl.maxcount);
+	if (rc) return rc;
+	// slots and the active lists
+	const size_t ksz = pl.key64 ? 8 : 4;
+	const size_t key_bytes = std::max(ksz * 2 * cap, pl.maxcount > PSG_SORT_MAX ? 16 * cap : (size_t)0);
+	if (!psg_scratch(ctx, S_KEYS, key_bytes) || !psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * cap) ||
+			!psg_scratch(ctx, S_SLOT, sizeof(uint32_t) * cap) ||
+			!psg_scratch(ctx, S_ACC, sizeof(double) * cap * pl.nacc) || !psg_scratch(ctx, S_ACT, act_bytes(pl)))
+		return PSG_E_NOMEM;
+	// ray classes (S_COUNT: class flags and scan; S_RAYLIST: the three lists,
+	// a room of nray each, inside the sort's class lists)
+	if (!psg_scratch(ctx, S_COUNT, sizeof(unsigned long long) * 2 * (nray + 1))) return PSG_E_NOMEM;
+	if (ctx->scratch[S_RAYLIST].bytes < sizeof(uint32_t) * 3 * (nray + 1)) return PSG_E_NOMEM;
+	// updates
+	if (!psg_scratch(ctx, S_UPD, upd_bytes(pl)) ||
+			!psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (3 * (cap + 1) + K + 1) + 512))
+		return PSG_E_NOMEM;
+	if (pl.helium) {
+		if (!psg_scratch(ctx, S_REC, sizeof(HeStiffItem) * pl.pcap)) return PSG_E_NOMEM;
+	} else if (pl.euler) {
+		if (!psg_scratch(ctx, S_REC, sizeof(UpdRec) * pl.pcap)) return PSG_E_NOMEM;
+	}
+	if (pl.feat_on && !psg_scratch(ctx, S_LOG, sizeof(float) * 8 * pl.pcap)) return PSG_E_NOMEM;
+	// library temporaries (one buffer, used one after another in stream order)
+	{
+		ActView av = act_view(ctx, pl);
+		size_t t1 = 0, t2 = 0, t3 = 0, t4 = 0;
+		const int endbit = pl.shift + pl.tbits;
+		if (pl.key64) {
+			unsigned long long *keys = (unsigned long long *)ctx->scratch[S_KEYS].p;
+			PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t1, keys, keys + cap, (uint32_t *)nullptr,
+					(uint32_t *)nullptr, (int64_t)cap, 0, endbit, ctx->stream));
+		} else {
+			uint32_t *keys = (uint32_t *)ctx->scratch[S_KEYS].p;
+			PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t1, keys, keys + cap, (uint32_t *)nullptr,
+					(uint32_t *)nullptr, (int64_t)cap, 0, endbit, ctx->stream));
+		}
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t2, av.head, av.hscan, (int)cap, ctx->stream));
+		unsigned long long *cls = (unsigned long long *)ctx->scratch[S_COUNT].p;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t3, cls, cls + (nray + 1), (int)nray, ctx->stream));
+		int32_t *aflag = (int32_t *)ctx->scratch[S_ALONG].p;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t4, aflag, aflag + (cap + 1), (int)(cap + 1), ctx->stream));
+		pl.sort_tmp = t1; pl.head_tmp = t2; pl.cls_tmp = t3; pl.act_tmp = t4;
+		if (!psg_scratch(ctx, S_CUB, std::max(std::max(t1, t2), std::max(t3, t4)))) return PSG_E_NOMEM;
+	}
+	// grids of the persistent kernels
+	pl.dep_grid = pl.gen ? occ_grid(ctx, k_deposit<true, false>, DEP_THREADS)
+			: (pl.aff ? occ_grid(ctx, k_deposit<false, true>, DEP_THREADS) : occ_grid(ctx, k_deposit<false, false>,
+					DEP_THREADS));
+	pl.red_grid = occ_grid(ctx, k_reduce<false, false>, 256);
+	pl.queue_minb = ctx->tune.update_minblocks >= 3 ? 3 : 1;
+	pl.queue_grid = pl.queue_minb == 3 ? occ_grid(ctx, k_update_queue<false, 3>, 32 * UPD_WARPS)
+			: occ_grid(ctx, k_update_queue<false, 1>, 32 * UPD_WARPS);
+	pl.he_grid = occ_grid(ctx, k_update_he<false>, 128);
+	pl.euler_grid = occ_grid(ctx, k_update_euler, 128);
+	pl.log_grid = (unsigned)(ctx->sms * 8);
+	if (pl.surr) {
+		rc = psg_surrogate_prepare(ctx);
+		if (rc) return rc;
+	}
 	return PSG_OK;
+}
+
+// Everything of the batch after the traversal. No host reads, no
+// allocation: the launch shapes depend on the plan alone; per-call values
+// come from B.
+template <typename KT>
+int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
+	cudaStream_t st = ctx->stream;
+	const size_t R = pl.R, K = pl.K, nray = pl.nray, cap = pl.cap;
+	const PhysParams P = psg_phys_params(ctx);
+	const int sms = ctx->sms;
+	int rc = psg_trace_sort_enqueue(ctx, nray, pl.nhit, pl.maxcount, 1);
+	if (rc) return rc;
+	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
+	uint32_t *hit_ipar = (uint32_t *)ctx->scratch[S_HIT_IPAR].p;
+	double *hit_kern = (double *)ctx->scratch[S_HIT_KERN].p;
+	void *cubtmp = ctx->scratch[S_CUB].p;
+
+	// by-particle order of all hits: (tick, ipar) keys over the capacity
+	psg_mark_begin(ctx, PSG_K_SLOTS);
+	KT *keys = (KT *)ctx->scratch[S_KEYS].p;
+	uint32_t *vals = (uint32_t *)ctx->scratch[S_VALS].p;
+	uint32_t *slot = (uint32_t *)ctx->scratch[S_SLOT].p;
+	double *acc = (double *)ctx->scratch[S_ACC].p;
+	ActView av = act_view(ctx, pl);
+	KT *act_key = (KT *)av.act_key;
+	const unsigned cgrid = (unsigned)std::min<size_t>(blocks(cap, 256), (size_t)sms * 16);
+	k_slot_keys<KT><<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, pl.shift, off64, hit_ipar, keys, vals);
+	PSG_CHECK_LAUNCH();
+	k_pad_keys<KT><<<cgrid, 256, 0, st>>>(cap, off64, nray, keys, vals);
+	PSG_CHECK_LAUNCH();
+	{
+		size_t tmp = pl.sort_tmp;
+		PSG_CUDA(cub::DeviceRadixSort::SortPairs(cubtmp, tmp, keys, keys + cap, vals, vals + cap, (int64_t)cap, 0,
+				pl.shift + pl.tbits, st));
+	}
+	k_slots<KT><<<cgrid, 256, 0, st>>>(cap, off64, nray, keys + cap, vals + cap, slot, av.head);
+	PSG_CHECK_LAUNCH();
+	{
+		size_t tmp = pl.head_tmp;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, tmp, av.head, av.hscan, (int)cap, st));
+	}
+	k_active<KT><<<cgrid, 256, 0, st>>>(off64, nray, pl.shift, keys + cap, av.head, av.hscan, av.act_ipar,
+			av.act_seg, act_key);
+	PSG_CHECK_LAUNCH();
+	unsigned long long *d_nact = ctx->d_counters + 6;
+	k_tick_bounds<KT><<<blocks(K + 1, 128), 128, 0, st>>>((int)K, pl.shift, act_key, off64, nray, av.head, av.hscan,
+			av.act_seg, av.tick_act, d_nact);
+	PSG_CHECK_LAUNCH();
+	ctx->launches += 6;
+	unsigned long long *d_nsat = ctx->d_counters + 1;      // (zeroed by the caller, per call)
+	psg_mark_end(ctx);
+
+	// long / middle / short ray lists of the batch (ray order, so each
+	// tick's rays are a run of each), and each tick's ranges in them
+	unsigned long long *cls = (unsigned long long *)ctx->scratch[S_COUNT].p;
+	unsigned long long *cls_scan = cls + (nray + 1);
+	uint32_t *ray_lists = (uint32_t *)ctx->scratch[S_RAYLIST].p;
+	uint32_t *long_rays = ray_lists, *mid_rays = ray_lists + nray, *short_rays = ray_lists + 2 * nray;
+	UpdView uv = upd_view(ctx, pl);
+	k_ray_class<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, ctx->tune.deposit_long, ctx->tune.deposit_mid, cls);
+	PSG_CHECK_LAUNCH();
+	{
+		size_t tmp = pl.cls_tmp;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, tmp, cls, cls_scan, (int)nray, st));
+	}
+	k_ray_lists<<<blocks(nray, 256), 256, 0, st>>>(nray, cls, cls_scan, long_rays, mid_rays, short_rays);
+	PSG_CHECK_LAUNCH();
+	k_tick_rays<<<blocks(K, 128), 128, 0, st>>>((int)K, R, nray, cls, cls_scan, uv.tick_rays);
+	PSG_CHECK_LAUNCH();
+	ctx->launches += 3;
+
+	// the long-segment lists and (not isothermal) the integrator's work
+	// cursors, stiff lists and the deposit's unit counters
+	PSG_CUDA(cudaMemsetAsync(uv.cursors, 0, sizeof(unsigned) * 4 * (K + 1), st));
+	if (pl.surr) PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 8, 0, sizeof(unsigned long long), st));
+	UpdRec *urec = (!pl.helium && pl.euler) ? (UpdRec *)ctx->scratch[S_REC].p : nullptr;
+	HeStiffItem *hstiff = pl.helium ? (HeStiffItem *)ctx->scratch[S_REC].p : nullptr;
+	float *feat = pl.feat_on ? (float *)ctx->scratch[S_LOG].p : nullptr;
+	int32_t *aflag = (int32_t *)ctx->scratch[S_ALONG].p;
+	int32_t *ascan = aflag + (cap + 1);
+	uint32_t *long_act = (uint32_t *)(ascan + (cap + 1));
+	int32_t *tick_long = (int32_t *)(long_act + (cap + 1));
+	k_act_class<<<cgrid, 256, 0, st>>>(cap, av.tick_act, (int)K, av.act_seg, aflag);
+	PSG_CHECK_LAUNCH();
+	{
+		size_t tmp = pl.act_tmp;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, tmp, aflag, ascan, (int)(cap + 1), st));
+	}
+	k_act_lists<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, aflag, ascan, long_act);
+	PSG_CHECK_LAUNCH();
+	k_tick_long<<<blocks(K + 1, 256), 256, 0, st>>>((int)K, av.tick_act, ascan, tick_long);
+	PSG_CHECK_LAUNCH();
+	ctx->launches += 3;
+
+	// the tick loop
+	double *d_lost = (double *)(ctx->d_counters + 2);
+	for (size_t t = 0; t < K; t++) {
+		psg_mark_begin(ctx, PSG_K_DEPOSIT);
+		if (pl.gen)
+			k_deposit<true, false><<<pl.dep_grid, DEP_THREADS, 0, st>>>((int)t, uv.tick_rays, uv.dep_ctr, B,
+					long_rays, mid_rays, short_rays, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+					pl.want_heat, acc, pl.nacc, d_nsat, d_lost);
+		else if (pl.aff)
+			k_deposit<false, true><<<pl.dep_grid, DEP_THREADS, 0, st>>>((int)t, uv.tick_rays, uv.dep_ctr, B,
+					long_rays, mid_rays, short_rays, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+					pl.want_heat, acc, pl.nacc, d_nsat, d_lost);
+		else
+			k_deposit<false, false><<<pl.dep_grid, DEP_THREADS, 0, st>>>((int)t, uv.tick_rays, uv.dep_ctr, B,
+					long_rays, mid_rays, short_rays, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+					pl.want_heat, acc, pl.nacc, d_nsat, d_lost);
+		PSG_CHECK_LAUNCH();
+		ctx->launches++;
+		psg_mark_end(ctx);
+		psg_mark_begin(ctx, PSG_K_UPDATE);
+		if (pl.helium) {
+			if (P.ygrec)
+				k_update_he<true><<<pl.he_grid, 128, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc,
+						pl.want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
+						ctx->d_yeMET, P, B, hstiff, uv.nstiff + t, ctx->d_status);
+			else
+				k_update_he<false><<<pl.he_grid, 128, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc,
+						pl.want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
+						ctx->d_yeMET, P, B, hstiff, uv.nstiff + t, ctx->d_status);
+			PSG_CHECK_LAUNCH();
+			k_update_he_stiff<<<sms, 64, 0, st>>>(hstiff, uv.nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
+					P, B, (int)t, ctx->d_status);
+			PSG_CHECK_LAUNCH();
+			ctx->launches += 2;
+		} else {
+			const double *gcarry = pl.euler ? ctx->d_gcarry : nullptr;
+			// the integrator sums the short segments itself unless every sum
+			// is wanted first (the surrogate, the update log)
+			const bool pre_all = pl.surr || feat;
+			double *keep_g = pre_all ? uv.act_g : nullptr;
+			double *keep_heat = pre_all ? uv.act_heat : nullptr;
+#define PSG_REDUCE(ISO_, REC_)                                                                                 \
+	k_reduce<ISO_, REC_><<<pl.red_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc,      \
+			pl.want_heat, long_act, tick_long, ctx->d_hits, keep_g, keep_heat, ctx->d_lambdaH, ctx->d_ie,       \
+			ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, B, ctx->d_status)
+			if (pl.iso && !pl.euler) {
+				if (P.ygrec) PSG_REDUCE(true, true);
+				else PSG_REDUCE(true, false);
+			} else if (pl.euler || pre_all) {
+				if (P.ygrec) PSG_REDUCE(false, true);
+				else PSG_REDUCE(false, false);
+			} else {
+				k_sum_long<<<pl.red_grid, 256, 0, st>>>((int)t, av.act_ipar, av.act_seg, acc, pl.want_heat, long_act,
+						tick_long, ctx->d_hits, uv.act_g, uv.act_heat);
+			}
+#undef PSG_REDUCE
+			PSG_CHECK_LAUNCH();
+			ctx->launches++;
+			if (pl.euler) {
+				k_update_euler<<<pl.euler_grid, 128, 0, st>>>((int)t, av.tick_act, urec, ctx->d_lambdaH, ctx->d_ie,
+						ctx->d_lasthit, ctx->d_gcarry, P, B, ctx->d_status);
+				PSG_CHECK_LAUNCH();
+				ctx->launches++;
+			} else if (!pl.iso) {
+				UpdSrc us;
+				us.act_ipar = av.act_ipar;
+				us.act_seg = av.act_seg;
+				us.acc = acc;
+				us.act_g = uv.act_g;
+				us.act_heat = uv.act_heat;
+				us.want_heat = pl.want_heat;
+				us.pre_all = pre_all;
+				us.hits = ctx->d_hits;
+				us.rho = ctx->d_rho;
+				us.yeMET = ctx->d_yeMET;
+				if (feat) {
+					k_log_pre<<<pl.log_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, uv.act_g, uv.act_heat,
+							ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, B, feat);
+					PSG_CHECK_LAUNCH();
+				}
+				if (pl.surr) {
+					// the network first; the integrator takes its rejects
+					rc = psg_surrogate_tick(ctx, (int)t, av.tick_act, av.act_ipar, uv.act_g, uv.act_heat, P, B, uv.rej,
+							uv.nrej + t);
+					if (rc) return rc;
+					ctx->launches++;
+				}
+				if (P.ygrec) {
+					k_update_queue<true, 1><<<pl.queue_grid, 32 * UPD_WARPS, 0, st>>>((int)t, av.tick_act, us,
+							ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, B, uv.cursors + t, uv.stiff,
+							uv.nstiff + t, nullptr, nullptr, ctx->d_status);
+					PSG_CHECK_LAUNCH();
+					k_update_stiff<true><<<sms, 64, 0, st>>>(uv.stiff, uv.nstiff + t, ctx->d_lambdaH, ctx->d_ie,
+							ctx->d_lasthit, P, B, (int)t, ctx->d_status);
+				} else {
+#define PSG_QUEUE(MINB_)                                                                                       \
+	k_update_queue<false, MINB_><<<pl.queue_grid, 32 * UPD_WARPS, 0, st>>>((int)t, av.tick_act, us,          \
+			ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, B, uv.cursors + t, uv.stiff,           \
+			uv.nstiff + t, pl.surr ? uv.rej : nullptr, pl.surr ? uv.nrej + t : nullptr, ctx->d_status)
+					if (pl.queue_minb == 3) PSG_QUEUE(3);
+					else PSG_QUEUE(1);
+#undef PSG_QUEUE
+					PSG_CHECK_LAUNCH();
+					k_update_stiff<false><<<sms, 64, 0, st>>>(uv.stiff, uv.nstiff + t, ctx->d_lambdaH, ctx->d_ie,
+							ctx->d_lasthit, P, B, (int)t, ctx->d_status);
+				}
+				PSG_CHECK_LAUNCH();
+				ctx->launches += 2;
+				if (feat) {
+					k_log_post<<<pl.log_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, ctx->d_lambdaH,
+							ctx->d_ie, ctx->d_yeMET, P, feat, ctx->log_buf, ctx->log_cap, ctx->log_count);
+					PSG_CHECK_LAUNCH();
+				}
+			}
+		}
+		psg_mark_end(ctx);
+	}
+	return PSG_OK;
+}
+
+// What a captured batch depends on: the plan, every buffer address, the
+// physics (PhysParams by value), the launch shapes and the surrogate and log
+// settings.
+std::vector<unsigned long long> batch_key(const psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
+	std::vector<unsigned long long> k;
+	k.push_back(pl.R); k.push_back(pl.K); k.push_back(pl.cap); k.push_back(pl.pcap);
+	k.push_back(pl.maxcount > PSG_SORT_MAX); k.push_back(pl.shift); k.push_back(pl.tbits);
+	k.push_back((unsigned long long)pl.nacc | (pl.want_heat << 4) | (pl.gen << 5) | (pl.helium << 6) | (pl.iso << 7) |
+			(pl.euler << 8) | (pl.surr << 9) | (pl.aff << 10) | (pl.feat_on << 11));
+	k.push_back((unsigned long long)(uintptr_t)ctx->stream);
+	k.push_back((unsigned long long)(uintptr_t)B);
+	for (int sl = 0; sl < S_NSLOTS; sl++) {
+		k.push_back((unsigned long long)(uintptr_t)ctx->scratch[sl].p);
+		k.push_back(ctx->scratch[sl].bytes);
+	}
+	k.push_back(ctx->slab_cap);
+	const PhysParams P = psg_phys_params(ctx);
+	const unsigned char *pb = (const unsigned char *)&P;
+	for (size_t i = 0; i < sizeof(P); i += 8) {
+		unsigned long long v = 0;
+		memcpy(&v, pb + i, std::min<size_t>(8, sizeof(P) - i));
+		k.push_back(v);
+	}
+	k.push_back((unsigned long long)(uintptr_t)ctx->d_surr);
+	unsigned tolbits = 0;
+	memcpy(&tolbits, &ctx->surr_tol, 4);
+	k.push_back(tolbits);
+	k.push_back((unsigned long long)(uintptr_t)ctx->log_buf);
+	k.push_back(ctx->log_cap);
+	k.push_back((unsigned long long)(uintptr_t)ctx->log_count);
+	const void *dev[] = {ctx->d_psml, ctx->d_order, ctx->d_mass, ctx->d_rho, ctx->d_yeMET, ctx->d_ie, ctx->d_lambdaH,
+		ctx->d_hits, ctx->d_lasthit, ctx->d_hstep, ctx->d_gcarry, ctx->d_status, ctx->d_counters};
+	for (const void *q : dev) k.push_back((unsigned long long)(uintptr_t)q);
+	k.push_back(ctx->n);
+	k.push_back(ctx->hit_cap);
+	k.push_back((unsigned long long)ctx->tune.deposit_long << 32 | (unsigned)ctx->tune.deposit_mid);
+	k.push_back((unsigned long long)pl.queue_minb);
+	return k;
+}
+
+int enqueue_any(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
+	return pl.key64 ? enqueue_batch<unsigned long long>(ctx, pl, B) : enqueue_batch<uint32_t>(ctx, pl, B);
+}
+
+// Replays the batch's graph, capturing it first if no graph of this key
+// exists. A failed capture is discarded before anything of it runs.
+int launch_batch_graph(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
+	GraphCache *gc = (GraphCache *)ctx->graphs;
+	if (!gc) {
+		gc = new GraphCache();
+		ctx->graphs = gc;
+	}
+	std::vector<unsigned long long> key = batch_key(ctx, pl, B);
+	for (auto &e : gc->e) {
+		if (e.key == key) {
+			PSG_CUDA(cudaGraphLaunch(e.exec, ctx->stream));
+			ctx->launches += e.launches;
+			return PSG_OK;
+		}
+	}
+	cudaStream_t st = ctx->stream;
+	PSG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+	const long l0 = ctx->launches;
+	int rc = enqueue_any(ctx, pl, B);
+	cudaGraph_t g = nullptr;
+	const cudaError_t ec = cudaStreamEndCapture(st, &g);
+	if (rc || ec != cudaSuccess) {
+		if (g) cudaGraphDestroy(g);
+		cudaGetLastError();
+		ctx->launches = l0;
+		return rc ? rc : psg_cuda_fail(ctx, ec, "cudaStreamEndCapture", __FILE__, __LINE__);
+	}
+	GraphEntry e;
+	e.key = std::move(key);
+	e.launches = ctx->launches - l0;
+	const cudaError_t ei = cudaGraphInstantiate(&e.exec, g, 0);
+	cudaGraphDestroy(g);
+	if (ei != cudaSuccess) return psg_cuda_fail(ctx, ei, "cudaGraphInstantiate", __FILE__, __LINE__);
+	if (gc->e.size() >= 6) {
+		cudaGraphExecDestroy(gc->e.front().exec);
+		gc->e.erase(gc->e.begin());
+	}
+	gc->e.push_back(std::move(e));
+	PSG_CUDA(cudaGraphLaunch(gc->e.back().exec, st));
+	return PSG_OK;
+}
+
+}  // namespace
+
+void psg_graphs_free(psg_context *ctx) {
+	GraphCache *gc = (GraphCache *)ctx->graphs;
+	if (!gc) return;
+	for (auto &e : gc->e)
+		if (e.exec) cudaGraphExecDestroy(e.exec);
+	delete gc;
+	ctx->graphs = nullptr;
 }
 
 // One batch of K ticks of R rays each, rays already traced together: the
@@ -1394,279 +2007,60 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 	PSG_CUDA(cudaSetDevice(ctx->device));
 	cudaStream_t st = ctx->stream;
 	const size_t nray = R * K;
-	const PhysParams P = psg_phys_params(ctx);
-	const int want_heat = !ctx->flags.isothermal;
-	// helium and/or secondary ionisation take the general deposit; helium
-	// its own update
-	const bool gen = !ctx->flags.h_only || ctx->flags.secondary_ionization;
-	const bool helium = !ctx->flags.h_only;
-	const int nacc = helium ? 4 : (want_heat ? 2 : 1);
-
 	ctx->nkev = 0;
 	ctx->launches = 0;
+	ctx->host_syncs = 0;
 	PSG_CUDA(cudaEventRecord(ctx->ev[0], st));
-	int rc = psg_trace_internal(ctx, d_rays, nray, 1);
+	PsgTraceFill tf;
+	int rc = psg_trace_fill(ctx, d_rays, nray, &tf);
 	if (rc) return rc;
-	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
-	int64_t nhit64 = 0;
-	PSG_CUDA(cudaMemcpyAsync(&nhit64, off64 + nray, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-	PSG_CUDA(cudaStreamSynchronize(st));
-	const size_t nhit = (size_t)nhit64;
-	const size_t hb = nhit ? nhit : 1;
-	uint32_t *hit_ipar = (uint32_t *)ctx->scratch[S_HIT_IPAR].p;
-	double *hit_kern = (double *)ctx->scratch[S_HIT_KERN].p;
-	psg_mark_begin(ctx, PSG_K_SLOTS);
-	// by-particle order of all hits
-	int shift = 1;
-	while (shift < 32 && (1ull << shift) < (unsigned long long)ctx->n) shift++;
-	int tbits = 0;
-	while ((1ull << tbits) < (unsigned long long)K) tbits++;
-	int nact = 0;
-	int rc2 = (shift + tbits <= 32) ? build_slots<uint32_t>(ctx, nray, R, K, nhit, shift, tbits, off64, hit_ipar,
-			nacc, &nact)
-		: build_slots<unsigned long long>(ctx, nray, R, K, nhit, shift, tbits, off64, hit_ipar, nacc, &nact);
-	if (rc2) return rc2;
-	double *acc = (double *)ctx->scratch[S_ACC].p;
-	uint32_t *slot = (uint32_t *)ctx->scratch[S_SLOT].p;
-	char *actm = (char *)ctx->scratch[S_ACT].p;
-	int32_t *head = (int32_t *)actm;
-	int32_t *hscan = head + (hb + 1);
-	uint32_t *act_ipar = (uint32_t *)(hscan + (hb + 1));
-	uint32_t *act_seg = act_ipar + (hb + 1);
-	int32_t *tick_act = (int32_t *)(((uintptr_t)(act_seg + hb + 1) + 15) & ~(uintptr_t)15);
-	(void)head;
-	unsigned long long *d_nsat = ctx->d_counters + 1;
-	double *d_lost = (double *)(ctx->d_counters + 2);
-	PSG_CUDA(cudaMemsetAsync(d_nsat, 0, 16, st));
-	psg_mark_end(ctx);
+	BatchPlan pl;
+	rc = plan_batch(ctx, R, K, tf, pl);
+	if (rc) return rc;
 	PSG_CUDA(cudaEventRecord(ctx->ev[1], st));
-
-	// the tick loop
-	std::vector<int32_t> h_tick_act(K + 1);
-	PSG_CUDA(cudaMemcpyAsync(h_tick_act.data(), tick_act, sizeof(int32_t) * (K + 1), cudaMemcpyDeviceToHost, st));
-	// long / middle / short ray lists of the batch (ray order, so each tick's
-	// rays are a run)
-	unsigned long long *cls = (unsigned long long *)psg_scratch(ctx, S_COUNT, sizeof(unsigned long long) * 2 * (nray + 1));
-	uint32_t *ray_lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * (nray + 1));
-	if (!cls || !ray_lists) return PSG_E_NOMEM;
-	unsigned long long *cls_scan = cls + (nray + 1);
-	k_ray_class<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, cls);
+	k_set_batch<<<1, 1, 0, st>>>(ctx->d_batch, first_tick, tick_time, d_rays, d_rays);
 	PSG_CHECK_LAUNCH();
-	{
-		size_t tmp = 0;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cls, cls_scan, (int)nray, st));
-		void *dt = psg_scratch(ctx, S_CUB, tmp);
-		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, cls, cls_scan, (int)nray, st));
-	}
-	std::vector<unsigned long long> h_scan(nray), h_last(1);
-	PSG_CUDA(cudaMemcpyAsync(h_scan.data(), cls_scan, sizeof(unsigned long long) * nray, cudaMemcpyDeviceToHost, st));
-	PSG_CUDA(cudaMemcpyAsync(h_last.data(), cls + nray - 1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-	PSG_CUDA(cudaStreamSynchronize(st));
-	const unsigned long long tot = h_scan[nray - 1] + h_last[0];
-	const int nlong_all = (int)(uint32_t)tot, nmid_all = (int)(uint32_t)(tot >> 32);
-	uint32_t *long_rays = ray_lists, *mid_rays = ray_lists + nlong_all, *short_rays = mid_rays + nmid_all;
-	k_ray_lists<<<blocks(nray, 256), 256, 0, st>>>(nray, cls, cls_scan, long_rays, mid_rays, short_rays);
-	PSG_CHECK_LAUNCH();
-	ctx->launches += 2;
-	// per-particle sums, the long-segment lists and (not isothermal) the
-	// integrator's work cursors and stiff lists
-	int dev_sms = 148;
-	cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
-	const bool iso = ctx->flags.isothermal != 0;
-	const size_t na = (size_t)(h_tick_act[K] > 0 ? h_tick_act[K] : 1);
-	size_t maxt = 1;
-	for (size_t t = 0; t < K; t++) maxt = std::max<size_t>(maxt, (size_t)(h_tick_act[t + 1] - h_tick_act[t]));
-	const bool euler = ctx->flags.euler != 0;
-	// (the network does not model the recombination photons: on the spot only)
-	const bool surr = !iso && !euler && ctx->surr_on && !ctx->flags.adiabatic && ctx->flags.on_the_spot &&
-			ctx->flags.h_only;
-	char *um = (char *)psg_scratch(ctx, S_UPD, sizeof(double) * 2 * na + sizeof(unsigned) * 3 * (K + 1)
-			+ (iso ? 0 : sizeof(StiffItem) * maxt) + (surr ? sizeof(uint32_t) * maxt : 0) + 512);
-	int32_t *aflag = (int32_t *)psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (3 * (na + 1) + K + 1) + 512);
-	if (!um || !aflag) return PSG_E_NOMEM;
-	double *act_g = (double *)um;
-	double *act_heat = act_g + na;
-	unsigned *cursors = (unsigned *)(act_heat + na);
-	unsigned *nstiff = cursors + (K + 1);
-	unsigned *nrej = nstiff + (K + 1);
-	StiffItem *stiff = (StiffItem *)(((uintptr_t)(nrej + K + 1) + 15) & ~(uintptr_t)15);
-	uint32_t *rej = (uint32_t *)(stiff + (iso ? 0 : maxt));
-	PSG_CUDA(cudaMemsetAsync(cursors, 0, sizeof(unsigned) * 3 * (K + 1), st));
-	if (surr) PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 8, 0, sizeof(unsigned long long), st));
-	UpdRec *urec = nullptr;
-	HeStiffItem *hstiff = nullptr;      // helium: the stiff particles of a tick
-	if (helium) {
-		hstiff = (HeStiffItem *)psg_scratch(ctx, S_REC, sizeof(HeStiffItem) * maxt);
-		if (!hstiff) return PSG_E_NOMEM;
-	} else if (!iso || euler) {
-		urec = (UpdRec *)psg_scratch(ctx, S_REC, sizeof(UpdRec) * maxt);
-		if (!urec) return PSG_E_NOMEM;
-	}
-	float *feat = nullptr;
-	if (ctx->log_buf && !iso && !helium) {
-		feat = (float *)psg_scratch(ctx, S_LOG, sizeof(float) * 8 * maxt);
-		if (!feat) return PSG_E_NOMEM;
-	}
-	// the long segments of the batch, listed in order, and each tick's first
-	int32_t *ascan = aflag + (na + 1);
-	uint32_t *long_act = (uint32_t *)(ascan + (na + 1));
-	int32_t *tick_long = (int32_t *)(long_act + (na + 1));
-	k_act_class<<<blocks(na + 1, 256), 256, 0, st>>>(na, act_seg, aflag);
-	PSG_CHECK_LAUNCH();
-	{
-		size_t tmp = 0;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, aflag, ascan, (int)(na + 1), st));
-		void *dt = psg_scratch(ctx, S_CUB, tmp);
-		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, aflag, ascan, (int)(na + 1), st));
-	}
-	k_act_lists<<<blocks(na, 256), 256, 0, st>>>(na, aflag, ascan, long_act);
-	PSG_CHECK_LAUNCH();
-	k_tick_long<<<blocks(K + 1, 256), 256, 0, st>>>((int)K, tick_act, ascan, tick_long);
-	PSG_CHECK_LAUNCH();
-	ctx->launches += 4;
-	std::vector<int32_t> h_tick_long(K + 1);
-	PSG_CUDA(cudaMemcpyAsync(h_tick_long.data(), tick_long, sizeof(int32_t) * (K + 1), cudaMemcpyDeviceToHost, st));
-	PSG_CUDA(cudaStreamSynchronize(st));
-	// capped hits settled by the affine-map scan when the last batch had many
-	const bool aff = ctx->sat_frac > 1e-3;
-	for (size_t t = 0; t < K; t++) {
-		const unsigned long long c0 = h_scan[t * R], c1 = (t + 1 < K) ? h_scan[(t + 1) * R] : tot;
-		const int l0 = (int)(uint32_t)c0, m0 = (int)(uint32_t)(c0 >> 32);
-		const int nlong = (int)(uint32_t)c1 - l0, nmid = (int)(uint32_t)(c1 >> 32) - m0;
-		const int s0 = (int)(t * R) - l0 - m0;
-		const int nshort = (int)R - nlong - nmid;
-		const unsigned grid = (unsigned)(nlong + (nmid + 3) / 4 + (nshort + DEP_THREADS / 32 - 1) / (DEP_THREADS / 32));
-		psg_mark_begin(ctx, PSG_K_DEPOSIT);
-		if (grid && gen)
-			k_deposit<true, false><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0,
-					nmid, short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
-					want_heat, acc, nacc, d_nsat, d_lost);
-		else if (grid && aff)
-			k_deposit<false, true><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0,
-					nmid, short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
-					want_heat, acc, nacc, d_nsat, d_lost);
-		else if (grid)
-			k_deposit<false, false><<<grid, DEP_THREADS, 0, st>>>(d_rays, long_rays + l0, nlong, mid_rays + m0,
-					nmid, short_rays + s0, nshort, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
-					want_heat, acc, nacc, d_nsat, d_lost);
-		PSG_CHECK_LAUNCH();
-		psg_mark_end(ctx);
-		const int nact_t = h_tick_act[t + 1] - h_tick_act[t];
-		psg_mark_begin(ctx, PSG_K_UPDATE);
-		if (nact_t > 0 && helium) {
-			if (P.ygrec)
-				k_update_he<true><<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
-						want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
-						ctx->d_rho, ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, hstiff, nstiff + t,
-						ctx->d_status);
-			else
-				k_update_he<false><<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc,
-						want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
-						ctx->d_rho, ctx->d_yeMET, P, first_tick + (int64_t)t, tick_time, hstiff, nstiff + t,
-						ctx->d_status);
-			PSG_CHECK_LAUNCH();
-			k_update_he_stiff<<<dev_sms, 64, 0, st>>>(hstiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
-					P, first_tick + (int64_t)t, ctx->d_status);
-			PSG_CHECK_LAUNCH();
-			ctx->launches += 2;
-		} else if (nact_t > 0) {
-			const int64_t tick = first_tick + (int64_t)t;
-			const int nl = h_tick_long[t + 1] - h_tick_long[t];
-			const int lb = (nl + 7) / 8;
-			const unsigned rgrid = (unsigned)(lb + (int)blocks(nact_t, 256));
-			const double *gcarry = euler ? ctx->d_gcarry : nullptr;
-			double *keep_g = (surr || feat) ? act_g : nullptr, *keep_heat = (surr || feat) ? act_heat : nullptr;
-#define PSG_REDUCE(ISO_, REC_)                                                                              \
-	k_reduce<ISO_, REC_><<<rgrid, 256, 0, st>>>((int)t, tick_act, act_ipar, act_seg, acc, want_heat, \
-			long_act + h_tick_long[t], nl, lb, ctx->d_hits, keep_g, keep_heat, ctx->d_lambdaH, ctx->d_ie,      \
-			ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, tick, tick_time,          \
-			ctx->d_status)
-			if (iso && !euler) {
-				if (P.ygrec) PSG_REDUCE(true, true);
-				else PSG_REDUCE(true, false);
-			} else {
-				if (P.ygrec) PSG_REDUCE(false, true);
-				else PSG_REDUCE(false, false);
-			}
-#undef PSG_REDUCE
-			PSG_CHECK_LAUNCH();
-			ctx->launches++;
-			if (euler) {
-				k_update_euler<<<blocks(nact_t, 128), 128, 0, st>>>((int)t, tick_act, urec, ctx->d_lambdaH, ctx->d_ie,
-						ctx->d_lasthit, ctx->d_gcarry, P, tick, ctx->d_status);
-				PSG_CHECK_LAUNCH();
-				ctx->launches++;
-			} else if (!iso) {
-				const unsigned qgrid = (unsigned)std::min<size_t>(blocks(nact_t, 256), (size_t)dev_sms * 8);
-				if (feat) {
-					k_log_pre<<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, act_g, act_heat,
-							ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, tick, tick_time, feat);
-					PSG_CHECK_LAUNCH();
-				}
-				if (surr) {
-					// the network first; the integrator takes its rejects
-					rc = psg_surrogate_tick(ctx, (int)t, nact_t, tick_act, act_ipar, act_g, act_heat, P, tick,
-							tick_time, rej, nrej + t, dev_sms);
-					if (rc) return rc;
-					ctx->launches++;
-				}
-				if (P.ygrec) {
-					k_update_queue<true><<<qgrid, 32 * UPD_WARPS, 0, st>>>((int)t, tick_act, urec, ctx->d_lambdaH,
-							ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, tick, cursors + t, stiff, nstiff + t, nullptr,
-							nullptr, ctx->d_status);
-					PSG_CHECK_LAUNCH();
-					k_update_stiff<true><<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie,
-							ctx->d_lasthit, P, tick, ctx->d_status);
-				} else {
-					k_update_queue<false><<<qgrid, 32 * UPD_WARPS, 0, st>>>((int)t, tick_act, urec, ctx->d_lambdaH,
-							ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, tick, cursors + t, stiff, nstiff + t,
-							surr ? rej : nullptr, surr ? nrej + t : nullptr, ctx->d_status);
-					PSG_CHECK_LAUNCH();
-					k_update_stiff<false><<<dev_sms, 64, 0, st>>>(stiff, nstiff + t, ctx->d_lambdaH, ctx->d_ie,
-							ctx->d_lasthit, P, tick, ctx->d_status);
-				}
-				PSG_CHECK_LAUNCH();
-				ctx->launches += 2;
-				if (feat) {
-					k_log_post<<<blocks(nact_t, 256), 256, 0, st>>>((int)t, tick_act, act_ipar, ctx->d_lambdaH,
-							ctx->d_ie, ctx->d_yeMET, P, feat, ctx->log_buf, ctx->log_cap, ctx->log_count);
-					PSG_CHECK_LAUNCH();
-				}
-			}
-		}
-		psg_mark_end(ctx);
-		ctx->launches++;
-	}
-	PSG_CUDA(cudaEventRecord(ctx->ev[2], st));
-	unsigned long long nsat = 0;
-	PSG_CUDA(cudaMemcpyAsync(&nsat, d_nsat, sizeof(nsat), cudaMemcpyDeviceToHost, st));
-	rc = check_status(ctx);      // (synchronises the stream)
+	ctx->launches++;
+	PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 1, 0, 2 * sizeof(unsigned long long), st));
+	PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 6, 0, sizeof(unsigned long long), st));
+	// per-launch timing needs the launches issued one by one; so does the
+	// library segmented sort of very long hit lists (its size is the hits')
+	const bool graph = ctx->use_graphs && !ctx->timing && pl.maxcount <= PSG_SORT_MAX;
+	rc = graph ? launch_batch_graph(ctx, pl, ctx->d_batch) : enqueue_any(ctx, pl, ctx->d_batch);
 	if (rc) return rc;
-	ctx->sat_frac = nhit ? (double)nsat / (double)nhit : 0.0;
+	PSG_CUDA(cudaEventRecord(ctx->ev[2], st));
+	// the batch's counters and status, one synchronisation
+	unsigned long long cnt[9];
+	uint32_t stw = 0;
+	PSG_CUDA(cudaMemcpyAsync(cnt, ctx->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaMemcpyAsync(&stw, ctx->d_status, sizeof(stw), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
+	ctx->host_syncs++;
+	if (stw) {
+		PSG_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), st));
+		return psg_fail(ctx, PSG_E_DEVICE, "device status 0x%x:%s%s%s", stw,
+				(stw & PSG_ST_NAN) ? " non-finite state" : "",
+				(stw & PSG_ST_SOLVER) ? " integrator step limit" : "",
+				(stw & PSG_ST_IE_NEG) ? " negative internal energy" : "");
+	}
+	const unsigned long long nsat = cnt[1];
+	ctx->sat_frac = tf.nhit ? (double)nsat / (double)tf.nhit : 0.0;
 	if (stats) {
-		double lost = 0;
-		PSG_CUDA(cudaMemcpyAsync(&lost, d_lost, sizeof(lost), cudaMemcpyDeviceToHost, st));
-		PSG_CUDA(cudaStreamSynchronize(st));
+		double lost = 0.0;
+		memcpy(&lost, &cnt[2], sizeof(double));
 		float trace_ms = 0.f, tick_ms = 0.f;
 		cudaEventElapsedTime(&trace_ms, ctx->ev[0], ctx->ev[1]);
 		cudaEventElapsedTime(&tick_ms, ctx->ev[1], ctx->ev[2]);
-		stats->hits = (double)nhit;
+		stats->hits = (double)tf.nhit;
 		stats->saturated = (double)nsat;
-		stats->active = (double)nact;
+		stats->active = (double)cnt[6];
 		stats->lost_photons = lost;
 		stats->trace_ms = trace_ms;
 		stats->tick_ms = tick_ms;
 		stats->launches = (double)ctx->launches;
-		stats->surrogate_accepted = 0.0;
+		stats->surrogate_accepted = pl.surr ? (double)cnt[8] : 0.0;
 		stats->rec_rays = stats->rec_photons = 0.0;
-		if (surr) {
-			unsigned long long acc_n = 0;
-			PSG_CUDA(cudaMemcpyAsync(&acc_n, ctx->d_counters + 8, sizeof(acc_n), cudaMemcpyDeviceToHost, st));
-			PSG_CUDA(cudaStreamSynchronize(st));
-			stats->surrogate_accepted = (double)acc_n;
-		}
+		stats->host_syncs = (double)ctx->host_syncs;
 		for (int k = 0; k < PSG_K_NKERNELS; k++) stats->kernel_ms[k] = stats->kernel_launches[k] = 0.0;
 		for (int i = 0; i < ctx->nkev; i++) {
 			float ms = 0.f;
@@ -1689,6 +2083,88 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 		return psg_run_ticks_rec(ctx, d_rays, R, K, first_tick, tick_time, stats);
 	}
 	return psg_run_ticks_core(ctx, d_rays, R, K, first_tick, tick_time, stats);
+}
+
+// ---- the autotuner -------------------------------------------------------------
+extern "C" int psg_autotune(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K, int64_t first_tick,
+		double tick_time, int reps, psg_tune *out, double *best_ms) {
+	if (!ctx) return PSG_E_INVAL;
+	if (!d_rays || R == 0 || K == 0) return psg_fail(ctx, PSG_E_INVAL, "psg_autotune: empty batch");
+	if (!ctx->have_physics || !ctx->have_tree)
+		return psg_fail(ctx, PSG_E_INVAL, "psg_autotune: set physics, load particles and build the tree first");
+	if (reps < 1) reps = 1;
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	const int timing0 = ctx->timing;
+	ctx->timing = 0;
+	const double sat0 = ctx->sat_frac;
+	int rc = psg_state_save(ctx);
+	if (rc) return rc;
+	// one shape: a warm-up batch (it captures the shape's graph), then reps
+	// timed batches; the state goes back after every one
+	auto trial = [&](const psg_tune &t, double *ms) -> int {
+		ctx->tune = t;
+		double best = 1e300;
+		for (int r = 0; r <= reps; r++) {
+			PSG_CUDA(cudaEventRecord(ctx->ev[5], ctx->stream));
+			const int rc1 = psg_run_ticks_device(ctx, d_rays, R, K, first_tick, tick_time, nullptr);
+			PSG_CUDA(cudaEventRecord(ctx->ev[6], ctx->stream));
+			PSG_CUDA(cudaEventSynchronize(ctx->ev[6]));
+			const int rc2 = psg_state_restore(ctx);
+			ctx->sat_frac = sat0;
+			if (rc1) return rc1;
+			if (rc2) return rc2;
+			float e = 0.f;
+			PSG_CUDA(cudaEventElapsedTime(&e, ctx->ev[5], ctx->ev[6]));
+			if (r > 0) best = std::min(best, (double)e);
+		}
+		*ms = best;
+		return PSG_OK;
+	};
+	psg_tune cur = ctx->tune;
+	double cur_ms = 0.0;
+	rc = trial(cur, &cur_ms);
+	// a candidate is kept when it is at least 1% faster (timing noise)
+	auto consider = [&](const psg_tune &t) -> int {
+		double ms = 0.0;
+		const int r = trial(t, &ms);
+		if (r) return r;
+		if (ms < 0.99 * cur_ms) {
+			cur = t;
+			cur_ms = ms;
+		}
+		return PSG_OK;
+	};
+	// traversal warps per block (the packet: one ray per warp, warps per block)
+	const int warps[] = {2, 4, 8};
+	for (int w : warps) {
+		if (rc || w == cur.trace_warps) continue;
+		psg_tune t = cur;
+		t.trace_warps = w;
+		rc = consider(t);
+	}
+	// deposit groups: which rays take a warp, a 128-thread group, a block
+	const int thr[][2] = {{64, 256}, {96, 384}, {128, 512}, {192, 768}};
+	for (auto &th : thr) {
+		if (rc || (th[0] == cur.deposit_long && th[1] == cur.deposit_mid)) continue;
+		psg_tune t = cur;
+		t.deposit_long = th[0];
+		t.deposit_mid = th[1];
+		rc = consider(t);
+	}
+	// the integrator's registers (occupancy against spills)
+	for (int mb : {1, 3}) {
+		if (rc || mb == cur.update_minblocks) continue;
+		psg_tune t = cur;
+		t.update_minblocks = mb;
+		rc = consider(t);
+	}
+	ctx->tune = cur;
+	ctx->timing = timing0;
+	if (rc) return rc;
+	psg_tune_store(ctx->device, &cur);
+	if (out) *out = cur;
+	if (best_ms) *best_ms = cur_ms;
+	return PSG_OK;
 }
 
 extern "C" int psg_run_ticks(psg_context *ctx, const psg_ray *rays, size_t R, size_t K,

@@ -127,9 +127,9 @@ __device__ __forceinline__ void test_candidates(const RayGeom &g, const int *lis
 // 4 + 28 entries per tree level; TR_STACK leaves room for 21 levels and an
 // overflow would raise PSG_ST_STACK instead of losing cells.
 #define TR_STACK 1024
-#define TR_WARPS 4
+#define TR_MAX_WARPS 16      // warps per block: ctx->tune.trace_warps, at most this
 
-__global__ void __launch_bounds__(32 * TR_WARPS) k_trace_stack(const psg_ray *__restrict__ rays, size_t nray,
+__global__ void __launch_bounds__(32 * TR_MAX_WARPS) k_trace_stack(const psg_ray *__restrict__ rays, size_t nray,
 		const float4 *__restrict__ wlo, const float4 *__restrict__ whi,
 		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx, int ppc,
 		uint32_t *__restrict__ count, size_t scap, uint32_t *__restrict__ slab_ipar,
@@ -255,6 +255,7 @@ __global__ void k_offsets64(const uint32_t *__restrict__ scan32, const uint32_t 
 	off64[r] = scan32[r];
 	off32[r] = (int32_t)scan32[r];
 	if (r < nray) atomicMax(maxcount, (unsigned long long)count[r]);
+	else maxcount[1] = scan32[r];       // the hit total, read with the longest list
 }
 
 __global__ void k_sort_keys(size_t nhit, const double *__restrict__ d, unsigned long long *__restrict__ keys,
@@ -321,7 +322,8 @@ __global__ void k_break_ties(size_t nray, const int64_t *__restrict__ off, uint3
 // order (loop.c:783-787) with ties broken by the caller's particle index. With want_kern the b column is replaced by the
 // column-density factor sph_depth(b/h)/h^2 of loop.c:429-445.
 template <int TPR, int IPT>
-__global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__ list, int nlist,
+__global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__ list,
+		const unsigned long long *__restrict__ d_nlist,
 		const int64_t *__restrict__ off, size_t scap, const uint32_t *__restrict__ slab_ipar,
 		const double *__restrict__ slab_d, const double *__restrict__ slab_b, uint32_t *__restrict__ out_ipar,
 		double *__restrict__ out_d, double *__restrict__ out_b, int want_kern, const float4 *__restrict__ psml,
@@ -336,8 +338,11 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 	};
 	extern __shared__ __align__(16) char sort_smem[];
 	Smem &sm = *reinterpret_cast<Smem *>(sort_smem);
-	if ((int)blockIdx.x >= nlist) return;
-	const size_t r = list[blockIdx.x];
+	// a persistent grid: the class's ray count is read here, so the launch
+	// needs no count from the host
+	const unsigned long long nlist = *d_nlist;
+	for (unsigned long long li = blockIdx.x; li < nlist; li += gridDim.x) {
+	const size_t r = list[li];
 	const int64_t h0 = off[r];
 	const int n = (int)(off[r + 1] - h0);
 	const uint32_t *raw_ipar = slab_ipar + r * scap;
@@ -424,6 +429,8 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 			out_b[h0 + i] = b;
 		}
 	}
+	__syncthreads();     // shared memory is reused by the next ray
+	}
 }
 
 template <int TPR, int IPT>
@@ -455,10 +462,12 @@ inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs);
 
 }  // namespace
 
-// Traces nray device-resident rays. Leaves in scratch: S_OFFSETS (int64
-// offsets[nray+1], then int32 offsets[nray+1]), S_HIT_IPAR (sorted caller
-// indices), S_RAW_D (sorted d) and S_HIT_KERN (sorted b).
-int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_kern) {
+// The traversal of nray device-resident rays into per-ray slabs, the hit
+// counts' scan and the offsets (S_OFFSETS: int64 offsets[nray+1], then
+// int32 offsets[nray+1]). One host synchronisation reads the longest list,
+// the status word and the hit total; a ray that outgrew its slab grows the
+// slabs and reruns the traversal once.
+int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTraceFill *tf) {
 	if (!ctx->have_tree) return psg_fail(ctx, PSG_E_INVAL, "trace: no tree (psg_build_tree first)");
 	cudaStream_t st = ctx->stream;
 	uint32_t *count = (uint32_t *)psg_scratch(ctx, S_COUNT, sizeof(uint32_t) * 2 * (nray + 1));
@@ -469,15 +478,14 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	int32_t *off32 = (int32_t *)(offmem + sizeof(int64_t) * (nray + 1));
 	unsigned long long *d_max = ctx->d_counters + 4;
 	unsigned long long *next_ray = ctx->d_counters + 9;
-	int sms = 148;
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+	const int sms = ctx->sms;
 	const int ppc = ctx->ppc;
-	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ppc + 32) * TR_WARPS;
+	const int trw = std::max(1, std::min(TR_MAX_WARPS, ctx->tune.trace_warps));
+	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ppc + 32) * trw;
 	if (smem > 48 * 1024)
 		PSG_CUDA(cudaFuncSetAttribute(k_trace_stack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-	// one traversal into per-ray slabs; if a ray outgrew its slab, grow and rerun
 	size_t scap = 0;
-	unsigned long long maxcount = 0;
+	unsigned long long hdr[2] = {0, 0};      // longest list, hit total
 	for (int attempt = 0; attempt < 2; attempt++) {
 		scap = ctx->slab_cap ? ctx->slab_cap : 1024;
 		const size_t slots = nray * scap;
@@ -485,14 +493,14 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 		double *slab_f64 = (double *)psg_scratch(ctx, S_REC_F64, sizeof(double) * 2 * (slots ? slots : 1));
 		if (!slab_ipar || !slab_f64) return PSG_E_NOMEM;
 		PSG_CUDA(cudaMemsetAsync(count + nray, 0, sizeof(uint32_t), st));
-		PSG_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st));
+		PSG_CUDA(cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned long long), st));
 		psg_mark_begin(ctx, PSG_K_TRACE_FILL);
 		if (nray) {
 			PSG_CUDA(cudaMemsetAsync(next_ray, 0, sizeof(unsigned long long), st));
 			int per_sm = 1;
-			PSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_stack, 32 * TR_WARPS, smem));
-			const unsigned tgrid = (unsigned)std::min<size_t>(blocks(nray, TR_WARPS), (size_t)std::max(per_sm, 1) * sms);
-			k_trace_stack<<<tgrid, 32 * TR_WARPS, smem, st>>>(d_rays, nray, ctx->d_wide_lo,
+			PSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_stack, 32 * trw, smem));
+			const unsigned tgrid = (unsigned)std::min<size_t>(blocks(nray, trw), (size_t)std::max(per_sm, 1) * sms);
+			k_trace_stack<<<tgrid, 32 * trw, smem, st>>>(d_rays, nray, ctx->d_wide_lo,
 					ctx->d_wide_hi, ctx->d_leaf_psml, ctx->d_leaf_idx, ppc, count, scap, slab_ipar,
 					slab_f64, slab_f64 + slots, next_ray, ctx->d_status);
 			ctx->launches++;
@@ -507,108 +515,163 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 		k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32, d_max);
 		PSG_CHECK_LAUNCH();
 		ctx->launches++;
-		PSG_CUDA(cudaMemcpyAsync(&maxcount, d_max, sizeof(maxcount), cudaMemcpyDeviceToHost, st));
+		PSG_CUDA(cudaMemcpyAsync(hdr, d_max, sizeof(hdr), cudaMemcpyDeviceToHost, st));
 		uint32_t stw = 0;
 		PSG_CUDA(cudaMemcpyAsync(&stw, ctx->d_status, sizeof(stw), cudaMemcpyDeviceToHost, st));
 		PSG_CUDA(cudaStreamSynchronize(st));
+		ctx->host_syncs++;
 		if (stw & PSG_ST_STACK) {
 			PSG_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), st));
 			return psg_fail(ctx, PSG_E_OVERFLOW, "trace: traversal stack overflow (tree deeper than supported)");
 		}
-		if (maxcount <= scap) break;
+		if (hdr[0] <= scap) break;
 		size_t want = 1024;
-		while (want < maxcount + maxcount / 4) want <<= 1;
+		while (want < hdr[0] + hdr[0] / 4) want <<= 1;
 		ctx->slab_cap = want;
 		if (attempt == 1) return psg_fail(ctx, PSG_E_OVERFLOW, "trace: hit lists grew between passes");
 	}
 	if (!ctx->slab_cap) ctx->slab_cap = scap;
-	int64_t nhit64 = 0;
-	PSG_CUDA(cudaMemcpyAsync(&nhit64, off64 + nray, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-	PSG_CUDA(cudaStreamSynchronize(st));
-	const size_t nhit = (size_t)nhit64;
-	if (nhit >= (size_t)INT32_MAX)
-		return psg_fail(ctx, PSG_E_OVERFLOW, "trace: %zu hits in one batch exceed 2^31", nhit);
-	const size_t hb = nhit ? nhit : 1;
+	if (hdr[1] >= (unsigned long long)INT32_MAX)
+		return psg_fail(ctx, PSG_E_OVERFLOW, "trace: %llu hits in one batch exceed 2^31", hdr[1]);
+	tf->nhit = (size_t)hdr[1];
+	tf->maxcount = hdr[0];
+	tf->scap = scap;
+	return PSG_OK;
+}
+
+// Buffers of the sorted hit lists for up to cap hits: S_HIT_IPAR, S_RAW_D
+// (sorted d at + cap), S_HIT_KERN (b, or the column-density factor), and
+// the class lists. Allocates; call before a stream capture.
+int psg_trace_sort_prepare(psg_context *ctx, size_t nray, size_t cap, unsigned long long maxcount) {
+	const size_t hb = cap ? cap : 1;
 	uint32_t *hit_ipar = (uint32_t *)psg_scratch(ctx, S_HIT_IPAR, sizeof(uint32_t) * hb);
 	double *hit_db = (double *)psg_scratch(ctx, S_RAW_D, sizeof(double) * 2 * hb);
 	double *hit_b = (double *)psg_scratch(ctx, S_HIT_KERN, sizeof(double) * hb);
-	if (!hit_ipar || !hit_db || !hit_b) return PSG_E_NOMEM;
-	double *hit_d = hit_db + hb;
+	uint32_t *lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * SORT_NCLS * (nray + 1));
+	if (!hit_ipar || !hit_db || !hit_b || !lists) return PSG_E_NOMEM;
+	ctx->hit_cap = hb;
+	if (maxcount > PSG_SORT_MAX) {
+		uint32_t *raw_ipar = (uint32_t *)psg_scratch(ctx, S_RAW_IPAR, sizeof(uint32_t) * hb);
+		double *raw_db = (double *)psg_scratch(ctx, S_RAW_B, sizeof(double) * 2 * hb);
+		unsigned long long *keys = (unsigned long long *)psg_scratch(ctx, S_KEYS, sizeof(unsigned long long) * 2 * hb);
+		uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
+		if (!raw_ipar || !raw_db || !keys || !vals) return PSG_E_NOMEM;
+	}
+	// shared-memory limits and resident blocks per multiprocessor of the
+	// eight class kernels (their persistent grids), once per context
+	if (!ctx->sort_grid[0]) {
+		int c = 0;
+#define PSG_SORT_ATTR(T, I)                                                                                    \
+	{                                                                                                        \
+		if (sort_smem_bytes<T, I>() > 48 * 1024)                                                             \
+			PSG_CUDA(cudaFuncSetAttribute(k_sort_block<T, I>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+					(int)sort_smem_bytes<T, I>()));                                                          \
+		int per_sm = 1;                                                                                      \
+		PSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sort_block<T, I>, T,               \
+				sort_smem_bytes<T, I>()));                                                                   \
+		ctx->sort_grid[c++] = (unsigned)std::max(per_sm, 1) * (unsigned)ctx->sms;                             \
+	}
+		PSG_SORT_ATTR(32, 2) PSG_SORT_ATTR(32, 4) PSG_SORT_ATTR(64, 4) PSG_SORT_ATTR(128, 4)
+		PSG_SORT_ATTR(128, 8) PSG_SORT_ATTR(256, 8) PSG_SORT_ATTR(256, 16) PSG_SORT_ATTR(512, 16)
+#undef PSG_SORT_ATTR
+	}
+	return PSG_OK;
+}
+
+// The per-ray sort by (d, ipar) of the filled slabs into the CSR lists.
+// With every list at most PSG_SORT_MAX long it issues only launches whose
+// sizes are fixed by nray (persistent class kernels read their ray counts on
+// the device), so it can be captured in a graph; a longer list takes the
+// library segmented sort, sized by nhit.
+int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned long long maxcount,
+		int want_kern) {
+	cudaStream_t st = ctx->stream;
+	const size_t hb = ctx->hit_cap;
+	const size_t scap = ctx->slab_cap;
 	const size_t slots = nray * scap;
+	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
+	int32_t *off32 = (int32_t *)((char *)ctx->scratch[S_OFFSETS].p + sizeof(int64_t) * (nray + 1));
+	uint32_t *hit_ipar = (uint32_t *)ctx->scratch[S_HIT_IPAR].p;
+	double *hit_d = (double *)ctx->scratch[S_RAW_D].p + hb;
+	double *hit_b = (double *)ctx->scratch[S_HIT_KERN].p;
 	uint32_t *slab_ipar = (uint32_t *)ctx->scratch[S_REC_U32].p;
 	double *slab_d = (double *)ctx->scratch[S_REC_F64].p;
 	double *slab_b = slab_d + slots;
-	if (nhit) {
-		psg_mark_begin(ctx, PSG_K_SORT);
-		if (maxcount <= PSG_SORT_MAX) {
-			uint32_t *lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * SORT_NCLS * (nray + 1));
-			if (!lists) return PSG_E_NOMEM;
-			unsigned long long *d_ncls = ctx->d_counters + 16;
-			PSG_CUDA(cudaMemsetAsync(d_ncls, 0, SORT_NCLS * sizeof(unsigned long long), st));
-			k_sort_classify<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, lists, nray + 1, d_ncls);
+	if (nray == 0) return PSG_OK;
+	psg_mark_begin(ctx, PSG_K_SORT);
+	if (maxcount <= PSG_SORT_MAX) {
+		uint32_t *lists = (uint32_t *)ctx->scratch[S_RAYLIST].p;
+		unsigned long long *d_ncls = ctx->d_counters + 16;
+		PSG_CUDA(cudaMemsetAsync(d_ncls, 0, SORT_NCLS * sizeof(unsigned long long), st));
+		k_sort_classify<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, lists, nray + 1, d_ncls);
+		PSG_CHECK_LAUNCH();
+		const PhysParams PP = psg_phys_params(ctx);
+		const size_t stride = nray + 1;
+		auto launch_block = [&](auto kern, int tpr, size_t smem, int c) -> int {
+			const unsigned grid = (unsigned)std::min<size_t>(nray, (size_t)ctx->sort_grid[c]);
+			kern<<<grid, tpr, smem, st>>>(lists + c * stride, d_ncls + c, off64, scap, slab_ipar, slab_d,
+					slab_b, hit_ipar, hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order);
 			PSG_CHECK_LAUNCH();
-			unsigned long long ncls[SORT_NCLS];
-			PSG_CUDA(cudaMemcpyAsync(ncls, d_ncls, sizeof(ncls), cudaMemcpyDeviceToHost, st));
-			PSG_CUDA(cudaStreamSynchronize(st));
-			const PhysParams PP = psg_phys_params(ctx);
-			const size_t stride = nray + 1;
-			auto launch_block = [&](auto kern, int tpr, size_t smem, int c) -> int {
-				const unsigned long long nl = ncls[c];
-				if (!nl) return PSG_OK;
-				if (smem > 48 * 1024)
-					PSG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-				kern<<<(unsigned)nl, tpr, smem, st>>>(lists + c * stride, (int)nl, off64, scap, slab_ipar, slab_d,
-						slab_b, hit_ipar, hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order);
-				PSG_CHECK_LAUNCH();
-				ctx->launches++;
-				return PSG_OK;
-			};
-			int rcs = launch_block(k_sort_block<32, 2>, 32, sort_smem_bytes<32, 2>(), 0);
-			if (!rcs) rcs = launch_block(k_sort_block<32, 4>, 32, sort_smem_bytes<32, 4>(), 1);
-			if (!rcs) rcs = launch_block(k_sort_block<64, 4>, 64, sort_smem_bytes<64, 4>(), 2);
-			if (!rcs) rcs = launch_block(k_sort_block<128, 4>, 128, sort_smem_bytes<128, 4>(), 3);
-			if (!rcs) rcs = launch_block(k_sort_block<128, 8>, 128, sort_smem_bytes<128, 8>(), 4);
-			if (!rcs) rcs = launch_block(k_sort_block<256, 8>, 256, sort_smem_bytes<256, 8>(), 5);
-			if (!rcs) rcs = launch_block(k_sort_block<256, 16>, 256, sort_smem_bytes<256, 16>(), 6);
-			if (!rcs) rcs = launch_block(k_sort_block<512, 16>, 512, sort_smem_bytes<512, 16>(), 7);
-			if (rcs) return rcs;
 			ctx->launches++;
-		} else {
-			// a ray longer than the shared-memory sort takes: library segmented sort
-			uint32_t *raw_ipar = (uint32_t *)psg_scratch(ctx, S_RAW_IPAR, sizeof(uint32_t) * hb);
-			double *raw_db = (double *)psg_scratch(ctx, S_RAW_B, sizeof(double) * 2 * hb);
-			unsigned long long *keys = (unsigned long long *)psg_scratch(ctx, S_KEYS, sizeof(unsigned long long) * 2 * hb);
-			uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
-			if (!raw_ipar || !raw_db || !keys || !vals) return PSG_E_NOMEM;
-			double *raw_d = raw_db, *raw_b = raw_db + hb;
-			k_compact_slabs<<<(unsigned)nray, 128, 0, st>>>(nray, scap, off64, slab_ipar, slab_d, slab_b,
-					raw_ipar, raw_d, raw_b);
+			return PSG_OK;
+		};
+		int rcs = launch_block(k_sort_block<32, 2>, 32, sort_smem_bytes<32, 2>(), 0);
+		if (!rcs) rcs = launch_block(k_sort_block<32, 4>, 32, sort_smem_bytes<32, 4>(), 1);
+		if (!rcs) rcs = launch_block(k_sort_block<64, 4>, 64, sort_smem_bytes<64, 4>(), 2);
+		if (!rcs) rcs = launch_block(k_sort_block<128, 4>, 128, sort_smem_bytes<128, 4>(), 3);
+		if (!rcs) rcs = launch_block(k_sort_block<128, 8>, 128, sort_smem_bytes<128, 8>(), 4);
+		if (!rcs) rcs = launch_block(k_sort_block<256, 8>, 256, sort_smem_bytes<256, 8>(), 5);
+		if (!rcs) rcs = launch_block(k_sort_block<256, 16>, 256, sort_smem_bytes<256, 16>(), 6);
+		if (!rcs) rcs = launch_block(k_sort_block<512, 16>, 512, sort_smem_bytes<512, 16>(), 7);
+		if (rcs) return rcs;
+		ctx->launches++;
+	} else if (nhit) {
+		// a ray longer than the shared-memory sort takes: library segmented sort
+		uint32_t *raw_ipar = (uint32_t *)ctx->scratch[S_RAW_IPAR].p;
+		double *raw_db = (double *)ctx->scratch[S_RAW_B].p;
+		unsigned long long *keys = (unsigned long long *)ctx->scratch[S_KEYS].p;
+		uint32_t *vals = (uint32_t *)ctx->scratch[S_VALS].p;
+		double *raw_d = raw_db, *raw_b = raw_db + hb;
+		k_compact_slabs<<<(unsigned)nray, 128, 0, st>>>(nray, scap, off64, slab_ipar, slab_d, slab_b,
+				raw_ipar, raw_d, raw_b);
+		PSG_CHECK_LAUNCH();
+		k_sort_keys<<<blocks(nhit, 256), 256, 0, st>>>(nhit, raw_d, keys, vals);
+		PSG_CHECK_LAUNCH();
+		size_t stmp = 0;
+		PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, stmp, keys, keys + hb, vals, vals + hb,
+				(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
+		void *dst = psg_scratch(ctx, S_CUB, stmp);
+		if (!dst) return PSG_E_NOMEM;
+		PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(dst, stmp, keys, keys + hb, vals, vals + hb,
+				(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
+		k_gather_sorted<<<blocks(nhit, 256), 256, 0, st>>>(nhit, vals + hb, raw_ipar, raw_d, raw_b,
+				hit_ipar, hit_d, hit_b);
+		PSG_CHECK_LAUNCH();
+		k_break_ties<<<blocks(nray, 128), 128, 0, st>>>(nray, off64, hit_ipar, hit_d, hit_b, ctx->d_order);
+		PSG_CHECK_LAUNCH();
+		ctx->launches += 4;
+		if (want_kern) {
+			k_hit_kernel<<<blocks(nhit, 256), 256, 0, st>>>(nhit, hit_ipar, ctx->d_psml, hit_b,
+					psg_phys_params(ctx));
 			PSG_CHECK_LAUNCH();
-			k_sort_keys<<<blocks(nhit, 256), 256, 0, st>>>(nhit, raw_d, keys, vals);
-			PSG_CHECK_LAUNCH();
-			size_t stmp = 0;
-			PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, stmp, keys, keys + hb, vals, vals + hb,
-					(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
-			void *dst = psg_scratch(ctx, S_CUB, stmp);
-			if (!dst) return PSG_E_NOMEM;
-			PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(dst, stmp, keys, keys + hb, vals, vals + hb,
-					(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
-			k_gather_sorted<<<blocks(nhit, 256), 256, 0, st>>>(nhit, vals + hb, raw_ipar, raw_d, raw_b,
-					hit_ipar, hit_d, hit_b);
-			PSG_CHECK_LAUNCH();
-			k_break_ties<<<blocks(nray, 128), 128, 0, st>>>(nray, off64, hit_ipar, hit_d, hit_b, ctx->d_order);
-			PSG_CHECK_LAUNCH();
-			ctx->launches += 4;
-			if (want_kern) {
-				k_hit_kernel<<<blocks(nhit, 256), 256, 0, st>>>(nhit, hit_ipar, ctx->d_psml, hit_b,
-						psg_phys_params(ctx));
-				PSG_CHECK_LAUNCH();
-				ctx->launches++;
-			}
+			ctx->launches++;
 		}
-		psg_mark_end(ctx);
 	}
+	psg_mark_end(ctx);
 	return PSG_OK;
+}
+
+// Traces nray device-resident rays: fill, buffers sized to the hits, sort.
+// Leaves in scratch: S_OFFSETS, S_HIT_IPAR (sorted leaf-order indices),
+// S_RAW_D (sorted d at + hit_cap) and S_HIT_KERN (sorted b, or with
+// want_kern the column-density factor).
+int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_kern) {
+	PsgTraceFill tf;
+	int rc = psg_trace_fill(ctx, d_rays, nray, &tf);
+	if (rc) return rc;
+	rc = psg_trace_sort_prepare(ctx, nray, tf.nhit, tf.maxcount);
+	if (rc) return rc;
+	return psg_trace_sort_enqueue(ctx, nray, tf.nhit, tf.maxcount, want_kern);
 }
 
 __global__ void k_caller_index(size_t n, const uint32_t *__restrict__ in, const uint32_t *__restrict__ order,
@@ -638,8 +701,7 @@ static int download_hits(psg_context *ctx, size_t nray, int64_t *offsets, psg_xt
 	if (nhit) {
 		std::vector<uint32_t> ip(nhit);
 		std::vector<double> d(nhit), b(nhit);
-		const size_t hb = nhit;
-		double *hit_d = (double *)ctx->scratch[S_RAW_D].p + hb;
+		double *hit_d = (double *)ctx->scratch[S_RAW_D].p + ctx->hit_cap;
 		// hits carry internal particle positions: the caller's indices
 		const uint32_t *hit_ipar = (const uint32_t *)ctx->scratch[S_HIT_IPAR].p;
 		if (ctx->d_order) {
