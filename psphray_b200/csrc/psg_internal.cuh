@@ -24,6 +24,7 @@
 #define PSG_ST_IE_NEG 4u       // internal energy would turn negative (solve.c:137-139)
 #define PSG_ST_STACK 8u        // traversal stack overflow
 #define PSG_ST_SURR 16u        // a surrogate tile's tensor-core step did not complete
+#define PSG_ST_SLAB 32u        // a hit list outgrew its slab in a call without host reads (redone)
 
 // scratch slots
 enum {
@@ -137,12 +138,15 @@ struct psg_context {
 	                                            // 3 longest list of a call, 4 longest hit list, 5 hit total,
 	                                            // 6 active particles, 7 hits of a call, 8 surrogate accepts,
 	                                            // 9 trace ray cursor, 10-13 recombination emission,
-	                                            // 14 recombination rays of a call, 16-23 sort size classes
+	                                            // 14 recombination rays of a call, 15 rays to trace,
+	                                            // 16-23 sort size classes, 24 largest tick total of a call
 	PsgBatchDev *d_batch = nullptr;             // per-call values read by the tick kernels (device)
 	int sms = 148;                              // multiprocessors of the device
 	size_t hit_cap = 0;                         // hits the sorted-list buffers hold
 	size_t batch_cap = 0;                       // hits the tick batches' per-hit buffers hold
 	unsigned sort_grid[8] = {};                 // persistent grids of the per-ray sort's classes
+	unsigned trace_grid = 0;                    // persistent grid of the traversal (psg_trace_fill_prepare)
+	size_t rec_tmp[2] = {0, 0};                 // library temporaries of the recombination emission
 	psg_tune tune{4, 96, 384, 1, 8};            // launch shapes (psg_set_tune, psg_autotune)
 	long host_syncs = 0;                        // host synchronisations of the current call
 	void *graphs = nullptr;                     // captured tick batches (psg_tick.cu)
@@ -217,6 +221,16 @@ int psg_surrogate_tick(psg_context *ctx, int t, const int32_t *tick_act, const u
 int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K, int64_t first_tick,
 		double tick_time, psg_tick_stats *stats);
 int psg_build_lte(psg_context *ctx, const psg_xs_table *xs);
+// the emission of a tick without host reads (its count stays on the
+// device), its buffers, and the next tick's emitter marks (psg_recomb.cu)
+int psg_rec_prepare(psg_context *ctx);
+int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out);
+int psg_rec_mark_enqueue(psg_context *ctx, size_t R, const PsgBatchDev *B);
+// the recombination ticks replayed from one captured tick (psg_tick.cu);
+// PSG_RETRY: run them one by one instead (first call, slabs too small)
+int psg_run_ticks_rec_graph(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K, int64_t first_tick,
+		double tick_time, psg_tick_stats *stats);
+#define PSG_RETRY 1
 #define PSG_LTE_NLOGT 128
 #define PSG_LTE_NFREQ 1024
 
@@ -230,6 +244,8 @@ int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTrac
 int psg_trace_sort_prepare(psg_context *ctx, size_t nray, size_t cap, unsigned long long maxcount);
 int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned long long maxcount, int want_kern);
 int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_kern);
+int psg_trace_fill_prepare(psg_context *ctx, size_t nray);
+int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray, const unsigned *nlim, size_t cap);
 
 // ---- device helpers ------------------------------------------------------------
 // Single-rounding float/double ops: the reference is compiled for x86-64 SSE

@@ -45,6 +45,15 @@ namespace {
 
 inline unsigned nblocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+__global__ void k_set_batch_rec(PsgBatchDev *b, int64_t tick, double tick_time, const psg_ray *rays,
+		const psg_ray *src, int64_t k) {
+	b->tick0 = tick;
+	b->tick_time = tick_time;
+	b->rays = rays;
+	b->src = src;
+	b->k = k;
+}
+
 __device__ __forceinline__ uint32_t caller_of(const uint32_t *__restrict__ order, uint32_t i) {
 	return order ? order[i] : i;
 }
@@ -63,11 +72,12 @@ __device__ __forceinline__ int lower_index(const double *cdf, int lo, int hi, do
 // tick, yGrecHII / xHI, placed in the caller's particle order (so that the
 // draws do not depend on the device's leaf order), and the caller -> leaf
 // map.
-__global__ void k_rec_weight(size_t n, int32_t prev, const int32_t *__restrict__ mark,
+__global__ void k_rec_weight(size_t n, const PsgBatchDev *__restrict__ B, const int32_t *__restrict__ mark,
 		const float *__restrict__ ygrec, const double *__restrict__ lambdaH, const uint32_t *__restrict__ order,
 		double *__restrict__ w, uint32_t *__restrict__ leaf_of) {
 	const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (p >= n) return;
+	const int32_t prev = (int32_t)(B->tick0 - 1);
 	double x = lambdaH[p];
 	if (x == 0.0) x = 1e-10;
 	const uint32_t c = caller_of(order, (uint32_t)p);
@@ -78,10 +88,11 @@ __global__ void k_rec_weight(size_t n, int32_t prev, const int32_t *__restrict__
 // nrec draws of species s from the cumulative weights (caller order):
 // key = s << 56 | caller index << 24 | draw, value = the particle (leaf
 // order); count[s] = nrec, or 0 when no weight is positive.
-__global__ void k_rec_draw(size_t n, int nrec, int s, uint32_t stream, const double *__restrict__ cdf, int64_t tick,
-		uint64_t seed, const uint32_t *__restrict__ leaf_of, unsigned long long *__restrict__ keys,
-		uint32_t *__restrict__ vals, unsigned *__restrict__ count) {
-	const double total = cdf[n - 1];
+__global__ void k_rec_draw(size_t n, int nrec, int s, uint32_t stream, const double *__restrict__ cdf,
+		const PsgBatchDev *__restrict__ B, uint64_t seed, const uint32_t *__restrict__ leaf_of,
+		unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals, unsigned *__restrict__ count) {
+	const int64_t tick = B->tick0;
+	const double total = tick > 1 ? cdf[n - 1] : 0.0;       // from the second tick on (loop.c:197)
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
 	if (k == 0) count[s] = total > 0.0 ? (unsigned)nrec : 0u;
 	if (k >= nrec || !(total > 0.0)) return;
@@ -95,11 +106,12 @@ __global__ void k_rec_draw(size_t n, int nrec, int s, uint32_t stream, const dou
 }
 
 // Threshold mode (loop.c:221-230): every marked particle above the threshold.
-__global__ void k_rec_flag(size_t n, int32_t prev, const int32_t *__restrict__ mark,
+__global__ void k_rec_flag(size_t n, const PsgBatchDev *__restrict__ B, const int32_t *__restrict__ mark,
 		const float *__restrict__ ygrec, double threshold, uint32_t *__restrict__ flag) {
 	const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (p >= n) return;
-	flag[p] = (mark[p] == prev && (double)ygrec[p] > threshold) ? 1u : 0u;
+	const int32_t prev = (int32_t)(B->tick0 - 1);
+	flag[p] = (B->tick0 > 1 && mark[p] == prev && (double)ygrec[p] > threshold) ? 1u : 0u;
 }
 
 __global__ void k_rec_compact(size_t n, int s, const uint32_t *__restrict__ flag, const uint32_t *__restrict__ pos,
@@ -131,10 +143,13 @@ __device__ __forceinline__ unsigned long long run_of(unsigned long long key) { r
 // its rays by (type, ipar), loop.c:236. Each ray's photons: the emitter's
 // yGrec of the species times NH (HII) or NHe (HeII, HeIII), split over the
 // run of rays that drew it (loop.c:277-290, 305-320).
-__global__ void k_rec_rays(int M, const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ vals,
-		int64_t tick, uint64_t seed, const float4 *__restrict__ psml, const float *__restrict__ mass, RecState Y,
+__global__ void k_rec_rays(const unsigned *__restrict__ count, const unsigned long long *__restrict__ keys,
+		const uint32_t *__restrict__ vals, const PsgBatchDev *__restrict__ B, uint64_t seed,
+		const float4 *__restrict__ psml, const float *__restrict__ mass, RecState Y,
 		const double *__restrict__ lambdaH, const float *__restrict__ ie, PhysParams P, LteView L, double length,
 		psg_ray *__restrict__ out, double *__restrict__ nph_sum) {
+	const int M = (int)(count[0] + count[1] + count[2]);
+	const int64_t tick = B->tick0;
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= M) return;
 	const uint32_t p = vals[i];
@@ -183,8 +198,10 @@ __global__ void k_rec_rays(int M, const unsigned long long *__restrict__ keys, c
 
 // The photons leave the emitter (loop.c:345-368): once per run, ray by ray
 // in float as the reference's compound assignment rounds, never below 0.
-__global__ void k_rec_purge(int M, const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ vals,
-		const psg_ray *__restrict__ rays, const float *__restrict__ mass, RecState Y, PhysParams P) {
+__global__ void k_rec_purge(const unsigned *__restrict__ count, const unsigned long long *__restrict__ keys,
+		const uint32_t *__restrict__ vals, const psg_ray *__restrict__ rays, const float *__restrict__ mass, RecState Y,
+		PhysParams P) {
+	const int M = (int)(count[0] + count[1] + count[2]);
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= M) return;
 	const unsigned long long run = run_of(keys[i]);
@@ -202,22 +219,27 @@ __global__ void k_rec_purge(int M, const unsigned long long *__restrict__ keys, 
 
 // The emitters of the next tick: every particle on the hit lists of the
 // tick's first nmark rays (its source rays and its first recombination ray).
-__global__ void k_rec_mark(int nmark, const int64_t *__restrict__ off, const uint32_t *__restrict__ hit_ipar,
-		int32_t tick, int32_t *__restrict__ mark) {
+__global__ void k_rec_mark(int R, const unsigned *__restrict__ count, const int64_t *__restrict__ off,
+		const uint32_t *__restrict__ hit_ipar, const PsgBatchDev *__restrict__ B, int32_t *__restrict__ mark) {
+	const int nmark = R + ((count[0] + count[1] + count[2]) > 0 ? 1 : 0);
+	const int32_t tick = (int32_t)B->tick0;
 	const int64_t end = off[nmark];
 	for (int64_t h = off[0] + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < end;
 			h += (int64_t)gridDim.x * blockDim.x)
 		mark[hit_ipar[h]] = tick;
 }
 
-// The tick's recombination rays into out (at most cap); *M_out their number.
-// One pass per species (HII; with helium also HeII and HeIII, loop.c:199):
-// weights or threshold flags, draws into the species' part of the key
-// array (unused entries stay all ones and sort last), then one sort.
-int emit_rec(psg_context *ctx, int64_t tick, size_t cap, psg_ray *out, size_t *M_out) {
-	cudaStream_t st = ctx->stream;
+}  // namespace
+
+// The tick's recombination rays into out (at most cap). One pass per
+// species (HII; with helium also HeII and HeIII, loop.c:199): weights or
+// threshold flags, draws into the species' part of the key array (unused
+// entries stay all ones and sort last), then one sort of the whole key
+// array. Launch sizes depend on n and the capacity only; the ray count lives
+// in d_count (counters 11-13) and the kernels read it: no host read, so a
+// tick can be captured. The tick number comes from B.
+int psg_rec_prepare(psg_context *ctx) {
 	const size_t n = ctx->n;
-	const PhysParams P = psg_phys_params(ctx);
 	const int threshold_mode = ctx->rec_nrec < 0;
 	const int nspec = ctx->flags.h_only ? 1 : 3;
 	const size_t kmax = threshold_mode ? n : (size_t)ctx->rec_nrec;     // per species
@@ -227,57 +249,68 @@ int emit_rec(psg_context *ctx, int64_t tick, size_t cap, psg_ray *out, size_t *M
 	if (!wm || !km) return PSG_E_NOMEM;
 	unsigned long long *keys = (unsigned long long *)km;
 	uint32_t *vals = (uint32_t *)(keys + 2 * ktot);
+	size_t t1 = 0, t2 = 0;
+	double *w = (double *)wm;
+	if (!threshold_mode) {
+		PSG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, t1, w, w + n, (int64_t)n, ctx->stream));
+	} else {
+		uint32_t *flag = (uint32_t *)wm;
+		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t1, flag, flag + n, (int64_t)n, ctx->stream));
+	}
+	PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t2, keys, keys + ktot, vals, vals + ktot, (int64_t)ktot, 0, 64,
+			ctx->stream));
+	ctx->rec_tmp[0] = t1;
+	ctx->rec_tmp[1] = t2;
+	if (!psg_scratch(ctx, S_CUB, std::max(t1, t2))) return PSG_E_NOMEM;
+	return PSG_OK;
+}
+
+int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out) {
+	cudaStream_t st = ctx->stream;
+	const size_t n = ctx->n;
+	const PhysParams P = psg_phys_params(ctx);
+	const int threshold_mode = ctx->rec_nrec < 0;
+	const int nspec = ctx->flags.h_only ? 1 : 3;
+	const size_t kmax = threshold_mode ? n : (size_t)ctx->rec_nrec;     // per species
+	const size_t ktot = kmax * nspec;
+	char *wm = (char *)ctx->scratch[S_RECW].p;
+	unsigned long long *keys = (unsigned long long *)ctx->scratch[S_RECK].p;
+	uint32_t *vals = (uint32_t *)(keys + 2 * ktot);
 	unsigned *d_count = (unsigned *)(ctx->d_counters + 11);      // [3]
 	double *d_nph = (double *)(ctx->d_counters + 10);
-	const int32_t prev = (int32_t)(tick - 1);
+	void *cubtmp = ctx->scratch[S_CUB].p;
 	const RecState Y{{ctx->d_ygrec, ctx->d_ygrecHe1, ctx->d_ygrecHe2}};
 	PSG_CUDA(cudaMemsetAsync(keys, 0xff, sizeof(unsigned long long) * ktot, st));
 	PSG_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned) * 4, st));
 	for (int s = 0; s < nspec; s++) {
+		size_t tmp = ctx->rec_tmp[0];
 		if (!threshold_mode) {
 			double *w = (double *)wm, *cdf = w + n;
 			uint32_t *leaf_of = (uint32_t *)(cdf + n);
-			k_rec_weight<<<nblocks(n, 256), 256, 0, st>>>(n, prev, ctx->d_srcmark, Y.yg[s], ctx->d_lambdaH,
+			k_rec_weight<<<nblocks(n, 256), 256, 0, st>>>(n, B, ctx->d_srcmark, Y.yg[s], ctx->d_lambdaH,
 					ctx->d_order, w, leaf_of);
 			PSG_CHECK_LAUNCH();
-			size_t tmp = 0;
-			PSG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, w, cdf, (int64_t)n, st));
-			void *dt = psg_scratch(ctx, S_CUB, tmp);
-			if (!dt) return PSG_E_NOMEM;
-			PSG_CUDA(cub::DeviceScan::InclusiveSum(dt, tmp, w, cdf, (int64_t)n, st));
+			PSG_CUDA(cub::DeviceScan::InclusiveSum(cubtmp, tmp, w, cdf, (int64_t)n, st));
 			// streams: 4 the HII emitters, 7 and 8 those of HeII and HeIII
 			k_rec_draw<<<nblocks(kmax, 128), 128, 0, st>>>(n, (int)kmax, s, s == 0 ? 4u : 6u + (uint32_t)s, cdf,
-					tick, ctx->rec_seed, leaf_of, keys + s * kmax, vals + s * kmax, d_count);
+					B, ctx->rec_seed, leaf_of, keys + s * kmax, vals + s * kmax, d_count);
 			PSG_CHECK_LAUNCH();
 		} else {
 			uint32_t *flag = (uint32_t *)wm, *pos = flag + n;
-			k_rec_flag<<<nblocks(n, 256), 256, 0, st>>>(n, prev, ctx->d_srcmark, Y.yg[s], ctx->rec_threshold, flag);
+			k_rec_flag<<<nblocks(n, 256), 256, 0, st>>>(n, B, ctx->d_srcmark, Y.yg[s], ctx->rec_threshold, flag);
 			PSG_CHECK_LAUNCH();
-			size_t tmp = 0;
-			PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag, pos, (int64_t)n, st));
-			void *dt = psg_scratch(ctx, S_CUB, tmp);
-			if (!dt) return PSG_E_NOMEM;
-			PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, flag, pos, (int64_t)n, st));
+			PSG_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, tmp, flag, pos, (int64_t)n, st));
 			k_rec_compact<<<nblocks(n, 256), 256, 0, st>>>(n, s, flag, pos, ctx->d_order, keys + s * kmax,
 					vals + s * kmax, d_count);
 			PSG_CHECK_LAUNCH();
 		}
 		ctx->launches += 3;
 	}
-	unsigned cnt[3] = {0, 0, 0};
-	PSG_CUDA(cudaMemcpyAsync(cnt, d_count, sizeof(unsigned) * 3, cudaMemcpyDeviceToHost, st));
-	PSG_CUDA(cudaStreamSynchronize(st));
-	ctx->host_syncs++;
-	const size_t M = (size_t)cnt[0] + cnt[1] + cnt[2];
-	if (M > cap) return psg_fail(ctx, PSG_E_OVERFLOW, "recombination rays: %zu > capacity %zu", M, cap);
-	*M_out = M;
-	if (M == 0) return PSG_OK;
-	size_t tmp = 0;
-	PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, keys + ktot, vals, vals + ktot, (int64_t)ktot, 0, 64,
-			st));
-	void *dt = psg_scratch(ctx, S_CUB, tmp);
-	if (!dt) return PSG_E_NOMEM;
-	PSG_CUDA(cub::DeviceRadixSort::SortPairs(dt, tmp, keys, keys + ktot, vals, vals + ktot, (int64_t)ktot, 0, 64, st));
+	{
+		size_t tmp = ctx->rec_tmp[1];
+		PSG_CUDA(cub::DeviceRadixSort::SortPairs(cubtmp, tmp, keys, keys + ktot, vals, vals + ktot, (int64_t)ktot, 0,
+				64, st));
+	}
 	LteView L;
 	L.cdf = ctx->d_lte;
 	for (int s = 0; s < 3; s++) {
@@ -286,16 +319,39 @@ int emit_rec(psg_context *ctx, int64_t tick, size_t cap, psg_ray *out, size_t *M
 	}
 	L.disabled = ctx->rec_disable_lte;
 	const double length = ctx->boxsize * 2.0 * 0.1;     // MAX_REC_RAY_LENGTH, loop.c:169
-	k_rec_rays<<<nblocks(M, 128), 128, 0, st>>>((int)M, keys + ktot, vals + ktot, tick, ctx->rec_seed, ctx->d_psml,
+	k_rec_rays<<<nblocks(ktot, 128), 128, 0, st>>>(d_count, keys + ktot, vals + ktot, B, ctx->rec_seed, ctx->d_psml,
 			ctx->d_mass, Y, ctx->d_lambdaH, ctx->d_ie, P, L, length, out, d_nph);
 	PSG_CHECK_LAUNCH();
-	k_rec_purge<<<nblocks(M, 128), 128, 0, st>>>((int)M, keys + ktot, vals + ktot, out, ctx->d_mass, Y, P);
+	k_rec_purge<<<nblocks(ktot, 128), 128, 0, st>>>(d_count, keys + ktot, vals + ktot, out, ctx->d_mass, Y, P);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 2;
 	return PSG_OK;
 }
 
-}  // namespace
+// The eager form: emission, then the count read back (one synchronisation).
+static int emit_rec(psg_context *ctx, const PsgBatchDev *B, size_t cap, psg_ray *out, size_t *M_out) {
+	int rc = psg_rec_prepare(ctx);
+	if (!rc) rc = psg_rec_emit_enqueue(ctx, B, out);
+	if (rc) return rc;
+	unsigned cnt[3] = {0, 0, 0};
+	PSG_CUDA(cudaMemcpyAsync(cnt, ctx->d_counters + 11, sizeof(unsigned) * 3, cudaMemcpyDeviceToHost, ctx->stream));
+	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
+	ctx->host_syncs++;
+	const size_t M = (size_t)cnt[0] + cnt[1] + cnt[2];
+	if (M > cap) return psg_fail(ctx, PSG_E_OVERFLOW, "recombination rays: %zu > capacity %zu", M, cap);
+	*M_out = M;
+	return PSG_OK;
+}
+
+// The emitters of the next tick (k_rec_mark), R source rays.
+int psg_rec_mark_enqueue(psg_context *ctx, size_t R, const PsgBatchDev *B) {
+	k_rec_mark<<<4 * ctx->sms, 256, 0, ctx->stream>>>((int)R, (const unsigned *)(ctx->d_counters + 11),
+			(const int64_t *)ctx->scratch[S_OFFSETS].p, (const uint32_t *)ctx->scratch[S_HIT_IPAR].p, B,
+			ctx->d_srcmark);
+	PSG_CHECK_LAUNCH();
+	ctx->launches++;
+	return PSG_OK;
+}
 
 // lte_init() / lte_fill() lte.c:30-72 for the three species (HI, HeI,
 // HeII): 128 rows of log T from 3 to 10, 1024 energies from the threshold
@@ -340,17 +396,23 @@ int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t 
 	double *d_nph = (double *)(ctx->d_counters + 10);
 	PSG_CUDA(cudaMemsetAsync(d_nph, 0, sizeof(double), st));
 	psg_tick_stats acc{}, one{};
-	const int sms = ctx->sms;
 	double rec_rays = 0.0, syncs = 0.0;
 	long launches = 0;
+	if (ctx->rec_nrec > 0 && ctx->use_graphs && !ctx->timing) {
+		// the ticks replayed from a captured tick, no host read between them
+		const int rc = psg_run_ticks_rec_graph(ctx, d_rays, R, K, first_tick, tick_time, stats);
+		if (rc != PSG_RETRY) return rc;
+	}
 	for (size_t k = 0; k < K; k++) {
 		const int64_t tick = first_tick + (int64_t)k;
 		PSG_CUDA(cudaMemcpyAsync(buf, d_rays + k * R, sizeof(psg_ray) * R, cudaMemcpyDeviceToDevice, st));
 		ctx->launches = 0;
 		ctx->host_syncs = 0;
 		size_t M = 0;
-		if (tick > 1 && ctx->rec_nrec != 0) {      // loop.c:197
-			const int rc = emit_rec(ctx, tick, cap, buf + R, &M);
+		if (ctx->rec_nrec != 0) {      // (no rays at the first tick, loop.c:197: k_rec_draw, k_rec_flag)
+			k_set_batch_rec<<<1, 1, 0, st>>>(ctx->d_batch, tick, tick_time, buf, d_rays, (int64_t)k);
+			PSG_CHECK_LAUNCH();
+			const int rc = emit_rec(ctx, ctx->d_batch, cap, buf + R, &M);
 			if (rc) return rc;
 		}
 		const long emit_launches = ctx->launches;
@@ -361,10 +423,9 @@ int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t 
 		rec_rays += (double)M;
 		int rc = psg_run_ticks_core(ctx, buf, R + M, 1, tick, tick_time, &one);
 		if (rc) return rc;
-		const int nmark = (int)(R + (M > 0 ? 1 : 0));
-		k_rec_mark<<<4 * sms, 256, 0, st>>>(nmark, (const int64_t *)ctx->scratch[S_OFFSETS].p,
-				(const uint32_t *)ctx->scratch[S_HIT_IPAR].p, (int32_t)tick, ctx->d_srcmark);
-		PSG_CHECK_LAUNCH();
+		if (ctx->rec_nrec == 0) PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 11, 0, 4 * sizeof(unsigned), st));
+		rc = psg_rec_mark_enqueue(ctx, R, ctx->d_batch);
+		if (rc) return rc;
 		launches += emit_launches + (long)one.launches + 1;
 		acc.hits += one.hits;
 		acc.saturated += one.saturated;

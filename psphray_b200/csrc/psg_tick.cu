@@ -1940,47 +1940,76 @@ int enqueue_any(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	return pl.key64 ? enqueue_batch<unsigned long long>(ctx, pl, B) : enqueue_batch<uint32_t>(ctx, pl, B);
 }
 
-// Replays the batch's graph, capturing it first if no graph of this key
-// exists. A failed capture is discarded before anything of it runs.
-int launch_batch_graph(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
+// Replays the graph of `key`, capturing what `enqueue` issues first if no
+// graph of this key exists. A failed capture is discarded before anything
+// of it runs. times: how many launches of the graph.
+template <typename F>
+int launch_graph(psg_context *ctx, std::vector<unsigned long long> key, F enqueue, size_t times = 1) {
 	GraphCache *gc = (GraphCache *)ctx->graphs;
 	if (!gc) {
 		gc = new GraphCache();
 		ctx->graphs = gc;
 	}
-	std::vector<unsigned long long> key = batch_key(ctx, pl, B);
-	for (auto &e : gc->e) {
-		if (e.key == key) {
-			PSG_CUDA(cudaGraphLaunch(e.exec, ctx->stream));
-			ctx->launches += e.launches;
-			return PSG_OK;
-		}
-	}
+	GraphEntry *hit = nullptr;
+	for (auto &e : gc->e)
+		if (e.key == key) hit = &e;
 	cudaStream_t st = ctx->stream;
-	PSG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-	const long l0 = ctx->launches;
-	int rc = enqueue_any(ctx, pl, B);
-	cudaGraph_t g = nullptr;
-	const cudaError_t ec = cudaStreamEndCapture(st, &g);
-	if (rc || ec != cudaSuccess) {
-		if (g) cudaGraphDestroy(g);
-		cudaGetLastError();
+	if (!hit) {
+		PSG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+		const long l0 = ctx->launches;
+		const int rc = enqueue();
+		cudaGraph_t g = nullptr;
+		const cudaError_t ec = cudaStreamEndCapture(st, &g);
+		if (rc || ec != cudaSuccess) {
+			if (g) cudaGraphDestroy(g);
+			cudaGetLastError();
+			ctx->launches = l0;
+			return rc ? rc : psg_cuda_fail(ctx, ec, "cudaStreamEndCapture", __FILE__, __LINE__);
+		}
+		GraphEntry e;
+		e.key = std::move(key);
+		e.launches = ctx->launches - l0;
 		ctx->launches = l0;
-		return rc ? rc : psg_cuda_fail(ctx, ec, "cudaStreamEndCapture", __FILE__, __LINE__);
+		const cudaError_t ei = cudaGraphInstantiate(&e.exec, g, 0);
+		cudaGraphDestroy(g);
+		if (ei != cudaSuccess) return psg_cuda_fail(ctx, ei, "cudaGraphInstantiate", __FILE__, __LINE__);
+		if (gc->e.size() >= 6) {
+			cudaGraphExecDestroy(gc->e.front().exec);
+			gc->e.erase(gc->e.begin());
+		}
+		gc->e.push_back(std::move(e));
+		hit = &gc->e.back();
 	}
-	GraphEntry e;
-	e.key = std::move(key);
-	e.launches = ctx->launches - l0;
-	const cudaError_t ei = cudaGraphInstantiate(&e.exec, g, 0);
-	cudaGraphDestroy(g);
-	if (ei != cudaSuccess) return psg_cuda_fail(ctx, ei, "cudaGraphInstantiate", __FILE__, __LINE__);
-	if (gc->e.size() >= 6) {
-		cudaGraphExecDestroy(gc->e.front().exec);
-		gc->e.erase(gc->e.begin());
+	for (size_t i = 0; i < times; i++) {
+		PSG_CUDA(cudaGraphLaunch(hit->exec, st));
+		ctx->launches += hit->launches;
 	}
-	gc->e.push_back(std::move(e));
-	PSG_CUDA(cudaGraphLaunch(gc->e.back().exec, st));
 	return PSG_OK;
+}
+
+// ---- recombination ticks without host reads -----------------------------------
+// The ticks of a call not on the spot, each: the tick's source rays into
+// the ray buffer, the recombination rays emitted behind them (their count
+// stays on the device), the traversal of all of them up to that count, the
+// batch of one tick, the next tick's emitter marks, the counters and the
+// tick number advanced on the device. Captured once, launched once per
+// tick; the host waits once per call.
+__global__ void k_rec_src(const PsgBatchDev *__restrict__ B, size_t R, psg_ray *__restrict__ buf) {
+	const psg_ray *src = B->src + (size_t)B->k * R;
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < R; i += (size_t)gridDim.x * blockDim.x)
+		buf[i] = src[i];
+}
+__global__ void k_rec_nlim(size_t R, const unsigned *__restrict__ count, unsigned long long *__restrict__ nlim,
+		unsigned long long *__restrict__ recsum) {
+	const unsigned M = count[0] + count[1] + count[2];
+	*(unsigned *)nlim = (unsigned)R + M;
+	*recsum += M;
+}
+__global__ void k_rec_tick_end(const int64_t *__restrict__ off, size_t nray, unsigned long long *__restrict__ hitsum,
+		PsgBatchDev *__restrict__ B) {
+	*hitsum += (unsigned long long)off[nray];
+	B->tick0 += 1;
+	B->k += 1;
 }
 
 }  // namespace
@@ -2026,7 +2055,8 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 	// per-launch timing needs the launches issued one by one; so does the
 	// library segmented sort of very long hit lists (its size is the hits')
 	const bool graph = ctx->use_graphs && !ctx->timing && pl.maxcount <= PSG_SORT_MAX;
-	rc = graph ? launch_batch_graph(ctx, pl, ctx->d_batch) : enqueue_any(ctx, pl, ctx->d_batch);
+	rc = graph ? launch_graph(ctx, batch_key(ctx, pl, ctx->d_batch), [&] { return enqueue_any(ctx, pl, ctx->d_batch); })
+			: enqueue_any(ctx, pl, ctx->d_batch);
 	if (rc) return rc;
 	PSG_CUDA(cudaEventRecord(ctx->ev[2], st));
 	// the batch's counters and status, one synchronisation
@@ -2083,6 +2113,121 @@ extern "C" int psg_run_ticks_device(psg_context *ctx, const psg_ray *d_rays, siz
 		return psg_run_ticks_rec(ctx, d_rays, R, K, first_tick, tick_time, stats);
 	}
 	return psg_run_ticks_core(ctx, d_rays, R, K, first_tick, tick_time, stats);
+}
+
+int psg_run_ticks_rec_graph(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t K, int64_t first_tick,
+		double tick_time, psg_tick_stats *stats) {
+	if (!ctx->have_physics || !ctx->have_tree) return PSG_RETRY;
+	const int nspec = ctx->flags.h_only ? 1 : 3;
+	const size_t cap_rec = (size_t)ctx->rec_nrec * nspec;
+	const size_t nray = R + cap_rec;
+	// the slabs and hit buffers as an earlier call left them: the first call
+	// runs its ticks one by one, which sizes them
+	if (ctx->rec_nrec <= 0 || !ctx->slab_cap || ctx->slab_cap > PSG_SORT_MAX || !ctx->batch_cap ||
+			nray >= (size_t)INT32_MAX)
+		return PSG_RETRY;
+	PSG_CUDA(cudaSetDevice(ctx->device));
+	cudaStream_t st = ctx->stream;
+	ctx->nkev = 0;
+	ctx->launches = 0;
+	ctx->host_syncs = 0;
+	psg_ray *buf = (psg_ray *)psg_scratch(ctx, S_RECRAYS, sizeof(psg_ray) * nray);
+	if (!buf) return PSG_E_NOMEM;
+	int rc = psg_trace_fill_prepare(ctx, nray);
+	if (!rc) rc = psg_rec_prepare(ctx);
+	if (rc) return rc;
+	PsgTraceFill tf{ctx->batch_cap, ctx->slab_cap, ctx->slab_cap};
+	BatchPlan pl;
+	rc = plan_batch(ctx, nray, 1, tf, pl);
+	if (rc) return rc;
+	rc = psg_state_save(ctx);      // (the undo if a tick outgrows the buffers)
+	if (rc) return rc;
+	PsgBatchDev *B = ctx->d_batch;
+	k_set_batch<<<1, 1, 0, st>>>(B, first_tick, tick_time, buf, d_rays);
+	PSG_CHECK_LAUNCH();
+	unsigned long long *cnt = ctx->d_counters;
+	PSG_CUDA(cudaMemsetAsync(cnt + 1, 0, 3 * sizeof(unsigned long long), st));      // 1-3
+	PSG_CUDA(cudaMemsetAsync(cnt + 6, 0, 2 * sizeof(unsigned long long), st));      // 6, 7
+	PSG_CUDA(cudaMemsetAsync(cnt + 10, 0, sizeof(unsigned long long), st));
+	PSG_CUDA(cudaMemsetAsync(cnt + 14, 0, sizeof(unsigned long long), st));
+	PSG_CUDA(cudaMemsetAsync(cnt + 24, 0, sizeof(unsigned long long), st));
+	const int64_t *off64 = (const int64_t *)ctx->scratch[S_OFFSETS].p;
+	const unsigned *nlim = (const unsigned *)(cnt + 15);
+	auto tick_enqueue = [&]() -> int {
+		k_rec_src<<<(unsigned)std::min<size_t>(blocks(R, 256), 4 * (size_t)ctx->sms), 256, 0, st>>>(B, R, buf);
+		PSG_CHECK_LAUNCH();
+		int r = psg_rec_emit_enqueue(ctx, B, buf + R);
+		if (r) return r;
+		k_rec_nlim<<<1, 1, 0, st>>>(R, (const unsigned *)(cnt + 11), cnt + 15, cnt + 14);
+		PSG_CHECK_LAUNCH();
+		r = psg_trace_fill_enqueue(ctx, buf, nray, nlim, pl.cap);
+		if (r) return r;
+		r = enqueue_any(ctx, pl, B);
+		if (r) return r;
+		r = psg_rec_mark_enqueue(ctx, R, B);
+		if (r) return r;
+		k_rec_tick_end<<<1, 1, 0, st>>>(off64, nray, cnt + 7, B);
+		PSG_CHECK_LAUNCH();
+		ctx->launches += 3;
+		return PSG_OK;
+	};
+	std::vector<unsigned long long> key = batch_key(ctx, pl, B);
+	key.push_back(0x5245432d5449434bull);      // a recombination tick
+	key.push_back(R);
+	key.push_back(cap_rec);
+	key.push_back((unsigned long long)(uintptr_t)buf);
+	key.push_back((unsigned long long)(uintptr_t)ctx->d_lte);
+	key.push_back(ctx->rec_seed);
+	key.push_back((unsigned long long)ctx->rec_disable_lte);
+	key.push_back((unsigned long long)(uintptr_t)ctx->d_srcmark);
+	key.push_back(ctx->trace_grid);
+	key.push_back((unsigned long long)ctx->tune.trace_warps);
+	rc = launch_graph(ctx, std::move(key), tick_enqueue, K);
+	if (rc) return rc;
+	unsigned long long c[32];
+	uint32_t stw = 0;
+	PSG_CUDA(cudaMemcpyAsync(c, cnt, sizeof(c), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaMemcpyAsync(&stw, ctx->d_status, sizeof(stw), cudaMemcpyDeviceToHost, st));
+	PSG_CUDA(cudaStreamSynchronize(st));
+	ctx->host_syncs++;
+	if (stw & PSG_ST_SLAB) {
+		// a tick outgrew the slabs or the hit buffers: undo the call, size
+		// both for what was seen, and let the ticks run one by one
+		PSG_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), st));
+		rc = psg_state_restore(ctx);
+		if (rc) return rc;
+		if (c[3] > ctx->slab_cap) {
+			size_t want = 1024;
+			while (want < c[3] + c[3] / 4) want <<= 1;
+			ctx->slab_cap = want;
+		}
+		if (c[24] > ctx->batch_cap) ctx->batch_cap = ((size_t)(c[24] + c[24] / 8) + 65535) & ~(size_t)65535;
+		return PSG_RETRY;
+	}
+	if (stw) {
+		PSG_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), st));
+		return psg_fail(ctx, PSG_E_DEVICE, "device status 0x%x:%s%s%s", stw,
+				(stw & PSG_ST_NAN) ? " non-finite state" : "",
+				(stw & PSG_ST_SOLVER) ? " integrator step limit" : "",
+				(stw & PSG_ST_IE_NEG) ? " negative internal energy" : "");
+	}
+	const unsigned *last = (const unsigned *)&c[11];
+	ctx->rec_last = (size_t)last[0] + last[1] + last[2];
+	ctx->rec_last_R = R;
+	ctx->rec_last_kmax = cap_rec;
+	ctx->sat_frac = c[7] ? (double)c[1] / (double)c[7] : 0.0;
+	if (stats) {
+		memset(stats, 0, sizeof(*stats));
+		stats->hits = (double)c[7];
+		stats->saturated = (double)c[1];
+		stats->active = (double)c[6];
+		memcpy(&stats->lost_photons, &c[2], sizeof(double));
+		stats->launches = (double)ctx->launches;
+		stats->rec_rays = (double)c[14];
+		memcpy(&stats->rec_photons, &c[10], sizeof(double));
+		stats->host_syncs = (double)ctx->host_syncs;
+	}
+	return PSG_OK;
 }
 
 // ---- the autotuner -------------------------------------------------------------

@@ -134,8 +134,11 @@ __global__ void __launch_bounds__(32 * TR_MAX_WARPS) k_trace_stack(const psg_ray
 		const float4 *__restrict__ lpsml, const uint32_t *__restrict__ lidx, int ppc,
 		uint32_t *__restrict__ count, size_t scap, uint32_t *__restrict__ slab_ipar,
 		double *__restrict__ slab_d, double *__restrict__ slab_b, unsigned long long *__restrict__ next_ray,
-		uint32_t *__restrict__ status) {
+		uint32_t *__restrict__ status, const unsigned *__restrict__ nlim) {
 	extern __shared__ int tr_smem[];
+	// rays past *nlim (when given: the recombination path's emitted count)
+	// are not traced; their counts stay as zeroed
+	if (nlim) nray = min(nray, (size_t)*nlim);
 	const int lane = threadIdx.x & 31;
 	const int wib = threadIdx.x >> 5;
 	int *stack = tr_smem + wib * (TR_STACK + 32 * ppc + 32);
@@ -246,16 +249,29 @@ __global__ void k_compact_slabs(size_t nray, size_t scap, const int64_t *__restr
 	}
 }
 
+// With cap (a call without host reads), a total above the hit buffers'
+// capacity empties every list instead (nothing downstream reads past cap)
+// and flags the status word for the host to redo the call; the call's
+// largest total is kept in *tickmax.
 __global__ void k_offsets64(const uint32_t *__restrict__ scan32, const uint32_t *__restrict__ count,
 		size_t nray, int64_t *__restrict__ off64, int32_t *__restrict__ off32,
-		unsigned long long *__restrict__ maxcount) {
+		unsigned long long *__restrict__ maxcount, size_t cap, unsigned long long *__restrict__ tickmax,
+		uint32_t *__restrict__ status) {
 	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (r > nray) return;
 	// scan32 holds the exclusive scan over nray+1 entries (count[nray] = 0)
-	off64[r] = scan32[r];
-	off32[r] = (int32_t)scan32[r];
-	if (r < nray) atomicMax(maxcount, (unsigned long long)count[r]);
-	else maxcount[1] = scan32[r];       // the hit total, read with the longest list
+	const bool over = cap && (size_t)scan32[nray] > cap;
+	off64[r] = over ? 0 : scan32[r];
+	off32[r] = over ? 0 : (int32_t)scan32[r];
+	if (r < nray) {
+		atomicMax(maxcount, (unsigned long long)count[r]);
+	} else {
+		maxcount[1] = scan32[r];       // the hit total, read with the longest list
+		if (cap) {
+			atomicMax(tickmax, (unsigned long long)scan32[r]);
+			if (over) atomicOr(status, PSG_ST_SLAB);
+		}
+	}
 }
 
 __global__ void k_sort_keys(size_t nhit, const double *__restrict__ d, unsigned long long *__restrict__ keys,
@@ -462,6 +478,83 @@ inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs);
 
 }  // namespace
 
+// Hit counts clamped to the slab capacity for the offsets (the slabs hold
+// no more); the longest list of the call kept in *callmax, and a clamped list
+// flagged in the status word (PSG_ST_SLAB) so the host redoes the call
+// with larger slabs.
+__global__ void k_count_clamp(size_t nray, size_t scap, uint32_t *__restrict__ count,
+		unsigned long long *__restrict__ callmax, uint32_t *__restrict__ status) {
+	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (r >= nray) return;
+	const uint32_t c = count[r];
+	if (c > scap) {
+		count[r] = (uint32_t)scap;
+		atomicOr(status, PSG_ST_SLAB);
+	}
+	if (c) atomicMax(callmax, (unsigned long long)c);
+}
+
+// The traversal without any host read (the recombination path's ticks):
+// the slabs as they are, rays up to *nlim, counts clamped to the slabs, a
+// total above cap flagged (k_offsets64).
+// Issues launches only; the caller has sized the slabs (S_COUNT, S_OFFSETS,
+// S_REC_U32/F64, S_CUB).
+int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray, const unsigned *nlim, size_t cap) {
+	cudaStream_t st = ctx->stream;
+	uint32_t *count = (uint32_t *)ctx->scratch[S_COUNT].p;
+	uint32_t *scan = count + (nray + 1);
+	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
+	int32_t *off32 = (int32_t *)((char *)ctx->scratch[S_OFFSETS].p + sizeof(int64_t) * (nray + 1));
+	unsigned long long *d_max = ctx->d_counters + 4;
+	unsigned long long *next_ray = ctx->d_counters + 9;
+	const size_t scap = ctx->slab_cap;
+	const size_t slots = nray * scap;
+	uint32_t *slab_ipar = (uint32_t *)ctx->scratch[S_REC_U32].p;
+	double *slab_f64 = (double *)ctx->scratch[S_REC_F64].p;
+	const int trw = std::max(1, std::min(TR_MAX_WARPS, ctx->tune.trace_warps));
+	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ctx->ppc + 32) * trw;
+	PSG_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t) * (nray + 1), st));
+	PSG_CUDA(cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned long long), st));
+	PSG_CUDA(cudaMemsetAsync(next_ray, 0, sizeof(unsigned long long), st));
+	k_trace_stack<<<ctx->trace_grid, 32 * trw, smem, st>>>(d_rays, nray, ctx->d_wide_lo, ctx->d_wide_hi,
+			ctx->d_leaf_psml, ctx->d_leaf_idx, ctx->ppc, count, scap, slab_ipar, slab_f64, slab_f64 + slots, next_ray,
+			ctx->d_status, nlim);
+	PSG_CHECK_LAUNCH();
+	k_count_clamp<<<blocks(nray, 256), 256, 0, st>>>(nray, scap, count, ctx->d_counters + 3, ctx->d_status);
+	PSG_CHECK_LAUNCH();
+	size_t tmp = ctx->scratch[S_CUB].bytes;
+	PSG_CUDA(cub::DeviceScan::ExclusiveSum(ctx->scratch[S_CUB].p, tmp, count, scan, (int)(nray + 1), st));
+	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32, d_max, cap,
+			ctx->d_counters + 24, ctx->d_status);
+	PSG_CHECK_LAUNCH();
+	ctx->launches += 3;
+	return PSG_OK;
+}
+
+// Sizes the buffers psg_trace_fill_enqueue uses for nray rays (allocates;
+// before a capture) and its persistent grid.
+int psg_trace_fill_prepare(psg_context *ctx, size_t nray) {
+	const size_t scap = ctx->slab_cap;
+	const size_t slots = nray * scap;
+	if (!psg_scratch(ctx, S_COUNT, sizeof(uint32_t) * 2 * (nray + 1)) ||
+			!psg_scratch(ctx, S_OFFSETS, (sizeof(int64_t) + sizeof(int32_t)) * (nray + 1) + 256) ||
+			!psg_scratch(ctx, S_REC_U32, sizeof(uint32_t) * (slots ? slots : 1)) ||
+			!psg_scratch(ctx, S_REC_F64, sizeof(double) * 2 * (slots ? slots : 1)))
+		return PSG_E_NOMEM;
+	uint32_t *count = (uint32_t *)ctx->scratch[S_COUNT].p;
+	size_t tmp = 0;
+	PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, count, count + (nray + 1), (int)(nray + 1), ctx->stream));
+	if (!psg_scratch(ctx, S_CUB, tmp)) return PSG_E_NOMEM;
+	const int trw = std::max(1, std::min(TR_MAX_WARPS, ctx->tune.trace_warps));
+	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ctx->ppc + 32) * trw;
+	if (smem > 48 * 1024)
+		PSG_CUDA(cudaFuncSetAttribute(k_trace_stack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	int per_sm = 1;
+	PSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_stack, 32 * trw, smem));
+	ctx->trace_grid = (unsigned)std::min<size_t>(blocks(nray, trw), (size_t)std::max(per_sm, 1) * ctx->sms);
+	return PSG_OK;
+}
+
 // The traversal of nray device-resident rays into per-ray slabs, the hit
 // counts' scan and the offsets (S_OFFSETS: int64 offsets[nray+1], then
 // int32 offsets[nray+1]). One host synchronisation reads the longest list,
@@ -502,7 +595,7 @@ int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTrac
 			const unsigned tgrid = (unsigned)std::min<size_t>(blocks(nray, trw), (size_t)std::max(per_sm, 1) * sms);
 			k_trace_stack<<<tgrid, 32 * trw, smem, st>>>(d_rays, nray, ctx->d_wide_lo,
 					ctx->d_wide_hi, ctx->d_leaf_psml, ctx->d_leaf_idx, ppc, count, scap, slab_ipar,
-					slab_f64, slab_f64 + slots, next_ray, ctx->d_status);
+					slab_f64, slab_f64 + slots, next_ray, ctx->d_status, nullptr);
 			ctx->launches++;
 		}
 		PSG_CHECK_LAUNCH();
@@ -512,7 +605,8 @@ int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTrac
 		void *dt = psg_scratch(ctx, S_CUB, tmp);
 		if (!dt) return PSG_E_NOMEM;
 		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, count, scan, (int)(nray + 1), st));
-		k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32, d_max);
+		k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32, d_max, 0, nullptr,
+				nullptr);
 		PSG_CHECK_LAUNCH();
 		ctx->launches++;
 		PSG_CUDA(cudaMemcpyAsync(hdr, d_max, sizeof(hdr), cudaMemcpyDeviceToHost, st));
