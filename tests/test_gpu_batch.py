@@ -124,3 +124,40 @@ def test_autotune_keeps_state_and_results(phys_noniso):
     assert np.array_equal(sa["lasthit"], sb["lasthit"]) and np.array_equal(sa["hits"], sb["hits"])
     assert np.max(np.abs(sa["lambdaH"] - sb["lambdaH"])) <= 1e-6
     assert np.max(np.abs(sa["ie"] - sb["ie"]) / sb["ie"]) <= 1e-4
+
+
+@pytest.mark.parametrize("iso", [True, False])
+def test_recombination_graph_equals_one_by_one(units, iso):
+    """Not on the spot (nrec recombination rays per tick emitted on the
+    device): from the second call on, a call's ticks replay one captured
+    tick with no host read between them (one wait per call); the same calls
+    issued launch by launch, tick by tick (per-launch timing on), must give
+    the identical state, counters and emitted rays."""
+    from psphray_b200 import api, fields
+    p = api.Physics(units, isothermal=iso, on_the_spot=False)
+    wa = fields.make_workload("iliev32", n_side=20, nray=64, seed=3)
+    wb = fields.make_workload("iliev32", n_side=20, nray=64, seed=3)
+    a, b = _ctx(p, wa.field), _ctx(p, wb.field)
+    try:
+        for c in (a, b):
+            c.set_recombination(nrec=40, seed=11)
+        b.set_timing(True)
+        sa = _batches(a, wa, 5, 4)
+        sb = _batches(b, wb, 5, 4)
+        ga, gb = a.state(), b.state()
+        ra, rb = a.rec_state(), b.rec_state()
+        rays_a, rays_b = a.rec_rays(), b.rec_rays()
+    finally:
+        a.close()
+        b.close()
+    for k in ("lambdaH", "ie", "hits", "lasthit"):
+        assert np.array_equal(ga[k], gb[k]), k
+    for x, y in zip(ra, rb):
+        assert np.array_equal(x, y)
+    assert np.array_equal(rays_a[0].view(np.uint8), rays_b[0].view(np.uint8))
+    assert np.array_equal(rays_a[1], rays_b[1])
+    for k in ("hits", "active", "rec_rays", "saturated"):
+        assert [s[k] for s in sa] == [s[k] for s in sb], k
+    assert [s["rec_photons"] for s in sa] == pytest.approx([s["rec_photons"] for s in sb], rel=1e-12)
+    assert all(s["host_syncs"] == 1 for s in sa[1:]), [s["host_syncs"] for s in sa]
+    assert sa[-1]["rec_rays"] == 4 * 40
