@@ -11,6 +11,7 @@ typedef struct gsl_ran_discrete_t {
 	double *P;
 } gsl_ran_discrete_t;
 void oracle_shim_set_uniform(double u);
+void oracle_shim_queue_uniforms(const double *u, size_t n);
 gsl_ran_discrete_t *gsl_ran_discrete_preproc(size_t K, const double *P);
 size_t gsl_ran_discrete(const gsl_rng *r, const gsl_ran_discrete_t *g);
 void gsl_ran_discrete_free(gsl_ran_discrete_t *g);

@@ -73,8 +73,16 @@ void stat_write(int n) { (void)n; bypassed("stat_write"); }
 void stat_reset() { bypassed("stat_reset"); }
 void stat_stop() { bypassed("stat_stop"); }
 void psystem_write_output(int n) { (void)n; bypassed("psystem_write_output"); }
-void psystem_weight_srcs(double w[]) { (void)w; bypassed("psystem_weight_srcs"); }
-double spec_gen_freq(const int id) { (void)id; bypassed("spec_gen_freq"); return 0; }
+/* (psystem_weight_srcs() is the reference's own, sources.c built in
+ * ref_sources.c; the source rays' energy is not compared: one fixed energy) */
+static double harness_spec_freq = 0.0;
+double spec_gen_freq(const int id) {
+	(void)id;
+	if (!(harness_spec_freq > 0.0)) bypassed("spec_gen_freq");
+	return harness_spec_freq;
+}
+int spec_get(const char *name) { (void)name; bypassed("spec_get"); return 0; }
+double spec_N_from_lum(const int id, double lum) { (void)id; (void)lum; bypassed("spec_N_from_lum"); return 0; }
 double eos_get_cloud_fraction(const double d) { (void)d; bypassed("eos_get_cloud_fraction"); return 0; }
 double eos_get_egyhot(const double d) { (void)d; bypassed("eos_get_egyhot"); return 0; }
 
@@ -341,3 +349,60 @@ int ref_step_evolve(Step *steps, size_t n) {
 	return 0;
 }
 size_t ref_sizeof_step(void) { return sizeof(Step); }
+
+/* ---- source rays: emit_rays() loop.c:163-373, on the spot ---------------- */
+/* Point sources with luminosity histories (psystem.h:7-25): source i has
+ * nhist[i] entries of (hist_ticks, hist_ngd) from offset hist_off[i]. */
+void ref_set_sources(int n, const double *pos, const int64_t *hist_ticks, const double *hist_ngd,
+		const int *hist_off, const int *nhist, const int64_t *lastemit) {
+	psys.srcs = calloc((size_t)n, sizeof(Source));
+	psys.nsrcs = (size_t)n;
+	for (int i = 0; i < n; i++) {
+		Source *S = &psys.srcs[i];
+		for (int d = 0; d < 3; d++) S->pos[d] = pos[3 * i + d];
+		S->type = PSYS_SRC_POINT;
+		S->specid = 0;
+		S->lastemit = (intptr_t)lastemit[i];
+		S->ticks = malloc(sizeof(intptr_t) * (size_t)nhist[i]);
+		S->Ngamma_dots = malloc(sizeof(double) * (size_t)nhist[i]);
+		for (int k = 0; k < nhist[i]; k++) {
+			S->ticks[k] = (intptr_t)hist_ticks[hist_off[i] + k];
+			S->Ngamma_dots[k] = hist_ngd[hist_off[i] + k];
+		}
+		S->ticks_length = S->ticks_size = (size_t)nhist[i];
+		S->Ngamma_dots_length = S->Ngamma_dots_size = (size_t)nhist[i];
+		S->cursor = 0;
+	}
+}
+
+void ref_get_sources(int64_t *lastemit, int64_t *cursor) {
+	for (size_t i = 0; i < psys.nsrcs; i++) {
+		lastemit[i] = (int64_t)psys.srcs[i].lastemit;
+		cursor[i] = (int64_t)psys.srcs[i].cursor;
+	}
+}
+
+/* One tick of emit_rays() with nray source rays, its source draws made at
+ * the uniforms u[0..nray) in draw order (the shim's queue); returns the
+ * rays' count and, in the reference's final ray order (sorted by source),
+ * each ray's source and photons. The energy is freq for every ray; the
+ * directions are not compared. */
+int ref_emit_source_rays(int nray, int64_t tick, double tick_time, double freq, const double *u, int64_t *isrc,
+		double *nph) {
+	const int saved = CFG_ON_THE_SPOT;
+	CFG_ON_THE_SPOT = 1;
+	psys.tick = (intptr_t)tick;
+	psys.tick_time = tick_time;
+	harness_epoch.nray = (size_t)nray;
+	harness_spec_freq = freq;
+	oracle_shim_queue_uniforms(u, (size_t)nray);
+	emit_rays();
+	oracle_shim_queue_uniforms(NULL, 0);
+	harness_spec_freq = 0.0;
+	CFG_ON_THE_SPOT = saved;
+	for (size_t i = 0; i < r_length; i++) {
+		isrc[i] = (int64_t)r[i].isrc;
+		nph[i] = r[i].Nph;
+	}
+	return (int)r_length;
+}

@@ -79,6 +79,11 @@ class Reference:
         lib.ref_lte_row.restype = C.c_int
         lib.ref_lte_gen_freq.argtypes = [C.c_int, C.c_double, C.c_double]
         lib.ref_lte_gen_freq.restype = C.c_double
+        lib.ref_set_sources.argtypes = [C.c_int] + [C.c_void_p] * 6
+        lib.ref_get_sources.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_emit_source_rays.argtypes = [C.c_int, C.c_int64, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]
+        lib.ref_emit_source_rays.restype = C.c_int
         assert lib.ref_sizeof_step() == C.sizeof(Step)
         self.units = units
         lib.ref_setup(rates_path.encode(), units.h, units.hmf, units.length_cmh,
@@ -251,3 +256,37 @@ class Reference:
 
     def xs_get(self, col: str, freq: float) -> float:
         return self.lib.ref_xs_get(self.ids[col], freq)
+
+    # ---- source rays: emit_rays() loop.c:163-373 with psystem_weight_srcs()
+    def set_sources(self, sources) -> None:
+        """Point sources: objects with pos, lastemit and either ngamma_dot or
+        a history (ticks, ngamma_dots), as psystem.h's Source."""
+        pos, hticks, hngd, off, nh, last = [], [], [], [], [], []
+        for src in sources:
+            t = list(src.ticks) if getattr(src, "ticks", None) is not None else [0]
+            v = list(src.ngamma_dots) if getattr(src, "ngamma_dots", None) is not None else [src.ngamma_dot]
+            off.append(len(hticks)); nh.append(len(t))
+            hticks += t; hngd += v
+            pos += [float(x) for x in src.pos]
+            last.append(int(src.lastemit))
+        self._src_keep = [np.ascontiguousarray(pos, np.float64), np.ascontiguousarray(hticks, np.int64),
+                          np.ascontiguousarray(hngd, np.float64), np.ascontiguousarray(off, np.int32),
+                          np.ascontiguousarray(nh, np.int32), np.ascontiguousarray(last, np.int64)]
+        self.nsrc = len(sources)
+        self.lib.ref_set_sources(self.nsrc, *[a.ctypes.data for a in self._src_keep])
+
+    def sources_state(self):
+        lastemit = np.zeros(self.nsrc, np.int64); cursor = np.zeros(self.nsrc, np.int64)
+        self.lib.ref_get_sources(lastemit.ctypes.data, cursor.ctypes.data)
+        return lastemit, cursor
+
+    def emit_source_rays(self, nray: int, tick: int, tick_time: float, u, freq: float = 1.0):
+        """One tick's source rays with the draws made at the uniforms u (ray
+        order): each ray's source and photons, in the reference's ray order
+        (by source)."""
+        u = np.ascontiguousarray(u, np.float64)
+        assert len(u) == nray
+        isrc = np.zeros(nray, np.int64); nph = np.zeros(nray)
+        n = self.lib.ref_emit_source_rays(int(nray), int(tick), float(tick_time), float(freq), u.ctypes.data,
+                                          isrc.ctypes.data, nph.ctypes.data)
+        return isrc[:n], nph[:n]

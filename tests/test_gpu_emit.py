@@ -86,3 +86,32 @@ def test_emit_errors(gpu_ctx, phys):
             fresh.set_sources([Src((0, 0, 0), 1.0, specid=5)], SPECTRA, seed=1)   # bad spectrum id
     finally:
         fresh.close()
+
+
+def test_emit_vs_reference_emit_rays(gpu_ctx, phys, reference):
+    """The device emitter against the reference's own emit_rays() with its
+    source draws made at the device's uniforms (tests/test_emit_reference.py
+    has the harness): per tick, the source of every ray and its photons
+    (the reference's weights from the luminosity histories and lastemit,
+    split evenly over a source's rays), and after the ticks each source's
+    lastemit and history cursor, bit for bit."""
+    from test_emit_reference import SEED, by_source, point_sources, reference_emission
+    g = load_golden("uniform16.npz")
+    f = golden_field(g)
+    gpu_ctx.set_physics(phys)
+    gpu_ctx.load(f)
+    R, tick_time, ticks = 400, 0.01, list(range(1, 9))
+    ref, (r_last, r_cur) = reference_emission(reference, R, ticks, tick_time)
+    srcs = point_sources()
+    gpu_ctx.set_sources(srcs, [(np.array([13.6 * phys.units.EV]), np.array([1.0]))], seed=SEED)
+    pos = np.array([s.pos for s in srcs], np.float32)
+    for t, (isrc, nph) in zip(ticks, ref):
+        rays = gpu_ctx.emit_rays(R, 1, t, tick_time)
+        which = np.array([int(np.nonzero((pos == s).all(1))[0][0]) for s in rays["s"]])
+        a_src, a_nph = by_source(which, rays["Nph"])
+        b_src, b_nph = by_source(isrc, nph)
+        assert np.array_equal(a_src, b_src), t
+        assert np.array_equal(a_nph, b_nph), t
+    lastemit, cursor = gpu_ctx.sources_state()
+    assert np.array_equal(lastemit, r_last)
+    assert np.array_equal(cursor.astype(np.int64), r_cur)
