@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "psg_internal.cuh"
+#include "psg_scan.cuh"
 #include "psg_helium.cuh"
 #include "psg_solve.cuh"
 #include "psg_surrogate.cuh"
@@ -86,87 +87,132 @@ namespace {
 inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 
-// (tick, ipar) keys for the by-particle order, tick in the bits above
-// `shift`; one warp per ray. KT is 32-bit whenever both fit.
-template <typename KT>
-__global__ void k_slot_keys(size_t nray, int nray_per_tick, int shift, const int64_t *__restrict__ off,
-		const uint32_t *__restrict__ ipar, KT *__restrict__ keys, uint32_t *__restrict__ vals) {
+// ---- the by-particle order without a key sort ------------------------------
+// The slots of a batch: every hit of tick t on particle p gets a place in the
+// (t, p, hit index) order. Counting instead of sorting: per (t, p) key the
+// number of hits (atomics; the counters are zero before and after), one
+// exclusive scan of the (count, count > 0) pairs over the K*N keys gives each
+// key its first slot and its active-particle index, a second pass places
+// every hit in its key's run (any order), and a last pass puts each run in
+// hit-index order -- the order a stable key sort gives, so the per-particle
+// sums downstream add in the same order as before, bit for bit.
+
+// one warp per ray: count the ray's hits per key (tick * N + particle)
+__global__ void k_slot_count(size_t nray, int R, uint32_t N, const int64_t *__restrict__ off,
+		const uint32_t *__restrict__ ipar, uint32_t *__restrict__ cnt) {
 	const size_t r = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32;
 	const int lane = threadIdx.x & 31;
 	if (r >= nray) return;
-	const KT t = (KT)(r / (size_t)nray_per_tick);
-	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32) {
-		keys[h] = (t << shift) | (KT)ipar[h];
-		vals[h] = (uint32_t)h;
-	}
+	const size_t base = (r / (size_t)R) * N;
+	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32) atomicAdd(&cnt[base + ipar[h]], 1u);
 }
 
-// The key sort runs over the buffers' capacity (a size fixed between
-// batches, so a captured batch replays for any hit count): entries past the
-// batch's hits (nhit = off[nray], read here) take the largest key and sort
-// last.
-template <typename KT>
-__global__ void k_pad_keys(size_t cap, const int64_t *__restrict__ off, size_t nray, KT *__restrict__ keys,
+// one warp per ray: every hit into its key's run (rank from the counter,
+// which returns to zero); vals[slot] = the hit
+__global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__restrict__ off,
+		const uint32_t *__restrict__ ipar, uint32_t *__restrict__ cnt, const unsigned long long *__restrict__ base,
 		uint32_t *__restrict__ vals) {
-	const size_t nhit = (size_t)off[nray];
-	for (size_t h = nhit + blockIdx.x * (size_t)blockDim.x + threadIdx.x; h < cap; h += (size_t)gridDim.x * blockDim.x) {
-		keys[h] = ~(KT)0;
-		vals[h] = (uint32_t)h;
+	const size_t r = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32;
+	const int lane = threadIdx.x & 31;
+	if (r >= nray) return;
+	const size_t kb = (r / (size_t)R) * N;
+	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32) {
+		const size_t key = kb + ipar[h];
+		const uint32_t rank = atomicSub(&cnt[key], 1u) - 1u;
+		vals[(uint32_t)base[key] + rank] = (uint32_t)h;
 	}
 }
 
-template <typename KT>
-__global__ void k_slots(size_t cap, const int64_t *__restrict__ off, size_t nray, const KT *__restrict__ skeys,
-		const uint32_t *__restrict__ svals, uint32_t *__restrict__ slot, int32_t *__restrict__ head) {
-	const size_t nhit = (size_t)off[nray];
-	for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < cap; k += (size_t)gridDim.x * blockDim.x) {
-		if (k < nhit) {
-			slot[svals[k]] = (uint32_t)k;
-			head[k] = (k == 0 || skeys[k] != skeys[k - 1]) ? 1 : 0;
-		} else {
-			head[k] = 0;
+// the active (tick, particle) pairs in key order: their particle and first
+// slot, the first pair of every tick and the totals
+__global__ void k_act_build(size_t KN, uint32_t N, int K, const unsigned long long *__restrict__ base,
+		uint32_t *__restrict__ act_ipar, uint32_t *__restrict__ act_seg, int32_t *__restrict__ tick_act,
+		unsigned long long *__restrict__ nact_out) {
+	for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < KN; k += (size_t)gridDim.x * blockDim.x) {
+		const unsigned long long b0 = base[k], b1 = base[k + 1];
+		const uint32_t a = (uint32_t)(b0 >> 32);
+		if ((uint32_t)(b1 >> 32) != a) {
+			act_ipar[a] = (uint32_t)(k % N);
+			act_seg[a] = (uint32_t)b0;
 		}
+		if (k % N == 0) tick_act[k / N] = (int32_t)a;
 	}
-}
-
-template <typename KT>
-__global__ void k_active(const int64_t *__restrict__ off, size_t nray, int shift, const KT *__restrict__ skeys,
-		const int32_t *__restrict__ head, const int32_t *__restrict__ scan, uint32_t *__restrict__ act_ipar,
-		uint32_t *__restrict__ act_seg, KT *__restrict__ act_key) {
-	const size_t nhit = (size_t)off[nray];
-	for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nhit; k += (size_t)gridDim.x * blockDim.x) {
-		if (!head[k]) continue;
-		const int a = scan[k];
-		act_ipar[a] = (uint32_t)(skeys[k] & (((KT)1 << shift) - 1));
-		act_seg[a] = (uint32_t)k;
-		act_key[a] = skeys[k];
-	}
-}
-
-// first active entry of every tick (and the total at index nticks); the
-// active total is the heads' scan at the last hit, read here
-template <typename KT>
-__global__ void k_tick_bounds(int nticks, int shift, const KT *__restrict__ act_key, const int64_t *__restrict__ off,
-		size_t nray, const int32_t *__restrict__ head, const int32_t *__restrict__ scan,
-		uint32_t *__restrict__ act_seg, int32_t *__restrict__ tick_act, unsigned long long *__restrict__ nact_out) {
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t > nticks) return;
-	const size_t nhit = (size_t)off[nray];
-	const int nact = nhit ? scan[nhit - 1] + head[nhit - 1] : 0;
-	int lo = 0, hi = nact;
-	if (t < nticks) {
-		const KT want = (KT)t << shift;
-		while (lo < hi) {
-			const int mid = (lo + hi) / 2;
-			if (act_key[mid] < want) lo = mid + 1; else hi = mid;
-		}
-	} else {
-		lo = nact;
-	}
-	tick_act[t] = lo;
-	if (t == nticks) {
-		act_seg[nact] = (uint32_t)nhit;
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		const unsigned long long tot = base[KN];
+		const uint32_t nact = (uint32_t)(tot >> 32);
+		tick_act[K] = (int32_t)nact;
+		act_seg[nact] = (uint32_t)tot;
 		atomicAdd(nact_out, (unsigned long long)nact);     // over the call's batches
+	}
+}
+
+// Runs of at most 32 hits, a thread each: insertion sort of the run's hit
+// indices, then each hit's slot. Longer runs are left to k_slot_canon_long.
+__global__ void k_slot_canon(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
+		uint32_t *__restrict__ vals, uint32_t *__restrict__ slot) {
+	const uint32_t na = (uint32_t)tick_act[K];
+	for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
+		const uint32_t n = s1 - s0;
+		if (n > 32) continue;
+		uint32_t v[32];
+		for (uint32_t i = 0; i < n; i++) {
+			const uint32_t x = vals[s0 + i];
+			uint32_t j = i;
+			while (j > 0 && v[j - 1] > x) {
+				v[j] = v[j - 1];
+				j--;
+			}
+			v[j] = x;
+		}
+		for (uint32_t i = 0; i < n; i++) {
+			vals[s0 + i] = v[i];
+			slot[v[i]] = s0 + i;
+		}
+	}
+}
+
+// Runs longer than 32 (particles next to a source), a block each: bitonic
+// sort in shared memory (runs up to SLOT_LONG_MAX hits: at most a tick's
+// rays; a longer run raises PSG_ST_SLOT).
+#define SLOT_LONG_MAX 32768
+__global__ void __launch_bounds__(1024) k_slot_canon_long(const int32_t *__restrict__ tick_long, int K,
+		const uint32_t *__restrict__ long_act, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals,
+		uint32_t *__restrict__ slot, int cap_pow2, uint32_t *__restrict__ status) {
+	extern __shared__ uint32_t sv[];
+	const int ne = tick_long[K];
+	for (int e = blockIdx.x; e < ne; e += gridDim.x) {
+		const uint32_t a = long_act[e];
+		const uint32_t s0 = act_seg[a], n = act_seg[a + 1] - s0;
+		if ((int)n > cap_pow2) {
+			if (threadIdx.x == 0) atomicOr(status, PSG_ST_SLOT);
+			continue;
+		}
+		int P = 1;
+		while (P < (int)n) P <<= 1;
+		for (int i = threadIdx.x; i < P; i += blockDim.x) sv[i] = i < (int)n ? vals[s0 + i] : 0xFFFFFFFFu;
+		__syncthreads();
+		for (int k = 2; k <= P; k <<= 1) {
+			for (int j = k >> 1; j > 0; j >>= 1) {
+				for (int i = threadIdx.x; i < P; i += blockDim.x) {
+					const int ixj = i ^ j;
+					if (ixj > i) {
+						const uint32_t x = sv[i], y = sv[ixj];
+						const bool up = (i & k) == 0;
+						if ((x > y) == up) {
+							sv[i] = y;
+							sv[ixj] = x;
+						}
+					}
+				}
+				__syncthreads();
+			}
+		}
+		for (int i = threadIdx.x; i < (int)n; i += blockDim.x) {
+			vals[s0 + i] = sv[i];
+			slot[sv[i]] = s0 + (uint32_t)i;
+		}
+		__syncthreads();
 	}
 }
 
@@ -794,16 +840,16 @@ __global__ void k_act_class(size_t cap, const int32_t *__restrict__ tick_act, in
 		flag[a] = (a < na && act_seg[a + 1] - act_seg[a] > 32) ? 1 : 0;
 }
 __global__ void k_act_lists(const int32_t *__restrict__ tick_act, int K, const int32_t *__restrict__ flag,
-		const int32_t *__restrict__ scan, uint32_t *__restrict__ long_act) {
+		const unsigned long long *__restrict__ scan, uint32_t *__restrict__ long_act) {
 	const size_t na = (size_t)tick_act[K];
 	for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a < na; a += (size_t)gridDim.x * blockDim.x)
-		if (flag[a]) long_act[scan[a]] = (uint32_t)a;
+		if (flag[a]) long_act[(uint32_t)scan[a]] = (uint32_t)a;
 }
 // first long entry of every tick
-__global__ void k_tick_long(int K, const int32_t *__restrict__ tick_act, const int32_t *__restrict__ scan,
+__global__ void k_tick_long(int K, const int32_t *__restrict__ tick_act, const unsigned long long *__restrict__ scan,
 		int32_t *__restrict__ out) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t <= K) out[t] = scan[tick_act[t]];
+	if (t <= K) out[t] = (int32_t)scan[tick_act[t]];
 }
 
 // One active particle's non-isothermal update, prepared by k_reduce<false>
@@ -1509,10 +1555,11 @@ struct BatchPlan {
 	size_t cap = 0;             // hits the per-hit buffers hold (>= the batch's hits)
 	size_t pcap = 0;            // particles one tick can update (min(n, cap))
 	unsigned long long maxcount = 0;
-	int shift = 1, tbits = 0, key64 = 0, nacc = 1, want_heat = 0;
+	size_t KN = 0;              // slot keys: ticks x particles
+	int long_cap = 0;           // longest run of one particle's hits the slot order sorts in shared memory
+	int nacc = 1, want_heat = 0;
 	bool gen = false, helium = false, iso = false, euler = false, surr = false, aff = false, feat_on = false;
-	// CUB temporary sizes
-	size_t sort_tmp = 0, head_tmp = 0, cls_tmp = 0, act_tmp = 0;
+
 	// grids
 	unsigned dep_grid = 0, red_grid = 0, queue_grid = 0, he_grid = 0, euler_grid = 0, log_grid = 0;
 	int queue_minb = 1;         // the integrator's register limit: resident blocks per SM
@@ -1539,26 +1586,22 @@ unsigned occ_grid(const psg_context *ctx, KF kern, int threads, size_t smem = 0)
 
 // Layout of the per-batch scratch slots.
 struct ActView {
-	int32_t *head, *hscan;
 	uint32_t *act_ipar, *act_seg;
 	int32_t *tick_act;
-	void *act_key;
 };
 ActView act_view(psg_context *ctx, const BatchPlan &pl) {
 	ActView v;
-	const size_t hb = pl.cap;
 	char *actm = (char *)ctx->scratch[S_ACT].p;
-	v.head = (int32_t *)actm;
-	v.hscan = v.head + (hb + 1);
-	v.act_ipar = (uint32_t *)(v.hscan + (hb + 1));
-	v.act_seg = v.act_ipar + (hb + 1);
-	v.tick_act = (int32_t *)(((uintptr_t)(v.act_seg + hb + 1) + 15) & ~(uintptr_t)15);
-	v.act_key = (void *)(((uintptr_t)(v.tick_act + pl.K + 1) + 15) & ~(uintptr_t)15);
+	v.act_ipar = (uint32_t *)actm;
+	v.act_seg = v.act_ipar + (pl.cap + 1);
+	v.tick_act = (int32_t *)(((uintptr_t)(v.act_seg + pl.cap + 1) + 15) & ~(uintptr_t)15);
 	return v;
 }
-size_t act_bytes(const BatchPlan &pl) {
-	return sizeof(int32_t) * 4 * (pl.cap + 1) + sizeof(int32_t) * (pl.K + 2) +
-			(pl.key64 ? 8 : 4) * (pl.cap + 1) + 1024;
+size_t act_bytes(const BatchPlan &pl) { return sizeof(uint32_t) * 2 * (pl.cap + 1) + sizeof(int32_t) * (pl.K + 2) + 64; }
+// S_SLOTCNT: the per-key counters (K * N, u32), then the keys' scan (K * N + 1, u64)
+size_t slotcnt_bytes(const BatchPlan &pl) { return 16 * ((4 * pl.KN + 15) / 16) + 8 * (pl.KN + 1) + 64; }
+unsigned long long *slot_base(psg_context *ctx, const BatchPlan &pl) {
+	return (unsigned long long *)((char *)ctx->scratch[S_SLOTCNT].p + 16 * ((4 * pl.KN + 15) / 16));
 }
 struct UpdView {
 	double *act_g, *act_heat;
@@ -1603,9 +1646,15 @@ int plan_batch(psg_context *ctx, size_t R, size_t K, const PsgTraceFill &tf, Bat
 	}
 	pl.cap = std::max<size_t>(ctx->batch_cap, 1);
 	pl.pcap = std::max<size_t>(std::min(ctx->n, pl.cap), 1);
-	while (pl.shift < 32 && (1ull << pl.shift) < (unsigned long long)ctx->n) pl.shift++;
-	while ((1ull << pl.tbits) < (unsigned long long)K) pl.tbits++;
-	pl.key64 = pl.shift + pl.tbits > 32;
+	pl.KN = K * ctx->n;
+	if (pl.KN >= (1ull << 31))
+		return psg_fail(ctx, PSG_E_OVERFLOW, "psg_run_ticks: %zu ticks x %zu particles: fewer ticks per call", K,
+				ctx->n);
+	{
+		int P = 1;
+		while (P < (int)std::min<size_t>(R, SLOT_LONG_MAX)) P <<= 1;
+		pl.long_cap = P;
+	}
 	pl.want_heat = !ctx->flags.isothermal;
 	pl.gen = !ctx->flags.h_only || ctx->flags.secondary_ionization;
 	pl.helium = !ctx->flags.h_only;
@@ -1623,19 +1672,20 @@ int plan_batch(psg_context *ctx, size_t R, size_t K, const PsgTraceFill &tf, Bat
 	int rc = psg_trace_sort_prepare(ctx, nray, cap, pl.maxcount);
 	if (rc) return rc;
 	// slots and the active lists
-	const size_t ksz = pl.key64 ? 8 : 4;
-	const size_t key_bytes = std::max(ksz * 2 * cap, pl.maxcount > PSG_SORT_MAX ? 16 * cap : (size_t)0);
-	if (!psg_scratch(ctx, S_KEYS, key_bytes) || !psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * cap) ||
-			!psg_scratch(ctx, S_SLOT, sizeof(uint32_t) * cap) ||
-			!psg_scratch(ctx, S_ACC, sizeof(double) * cap * pl.nacc) || !psg_scratch(ctx, S_ACT, act_bytes(pl)))
+	if (!psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * cap) || !psg_scratch(ctx, S_SLOT, sizeof(uint32_t) * cap) ||
+			!psg_scratch(ctx, S_ACC, sizeof(double) * cap * pl.nacc) || !psg_scratch(ctx, S_ACT, act_bytes(pl)) ||
+			!psg_scratch(ctx, S_SLOTCNT, slotcnt_bytes(pl)))
 		return PSG_E_NOMEM;
+	if (pl.long_cap * sizeof(uint32_t) > 48 * 1024)
+		PSG_CUDA(cudaFuncSetAttribute(k_slot_canon_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				(int)(pl.long_cap * sizeof(uint32_t))));
 	// ray classes (S_COUNT: class flags and scan; S_RAYLIST: the three lists,
 	// a room of nray each, inside the sort's class lists)
 	if (!psg_scratch(ctx, S_COUNT, sizeof(unsigned long long) * 2 * (nray + 1))) return PSG_E_NOMEM;
 	if (ctx->scratch[S_RAYLIST].bytes < sizeof(uint32_t) * 3 * (nray + 1)) return PSG_E_NOMEM;
 	// updates
 	if (!psg_scratch(ctx, S_UPD, upd_bytes(pl)) ||
-			!psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (3 * (cap + 1) + K + 1) + 512))
+			!psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (4 * (cap + 2) + K + 1) + 512))
 		return PSG_E_NOMEM;
 	if (pl.helium) {
 		if (!psg_scratch(ctx, S_REC, sizeof(HeStiffItem) * pl.pcap)) return PSG_E_NOMEM;
@@ -1643,28 +1693,10 @@ int plan_batch(psg_context *ctx, size_t R, size_t K, const PsgTraceFill &tf, Bat
 		if (!psg_scratch(ctx, S_REC, sizeof(UpdRec) * pl.pcap)) return PSG_E_NOMEM;
 	}
 	if (pl.feat_on && !psg_scratch(ctx, S_LOG, sizeof(float) * 8 * pl.pcap)) return PSG_E_NOMEM;
-	// library temporaries (one buffer, used one after another in stream order)
-	{
-		ActView av = act_view(ctx, pl);
-		size_t t1 = 0, t2 = 0, t3 = 0, t4 = 0;
-		const int endbit = pl.shift + pl.tbits;
-		if (pl.key64) {
-			unsigned long long *keys = (unsigned long long *)ctx->scratch[S_KEYS].p;
-			PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t1, keys, keys + cap, (uint32_t *)nullptr,
-					(uint32_t *)nullptr, (int64_t)cap, 0, endbit, ctx->stream));
-		} else {
-			uint32_t *keys = (uint32_t *)ctx->scratch[S_KEYS].p;
-			PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t1, keys, keys + cap, (uint32_t *)nullptr,
-					(uint32_t *)nullptr, (int64_t)cap, 0, endbit, ctx->stream));
-		}
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t2, av.head, av.hscan, (int)cap, ctx->stream));
-		unsigned long long *cls = (unsigned long long *)ctx->scratch[S_COUNT].p;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t3, cls, cls + (nray + 1), (int)nray, ctx->stream));
-		int32_t *aflag = (int32_t *)ctx->scratch[S_ALONG].p;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t4, aflag, aflag + (cap + 1), (int)(cap + 1), ctx->stream));
-		pl.sort_tmp = t1; pl.head_tmp = t2; pl.cls_tmp = t3; pl.act_tmp = t4;
-		if (!psg_scratch(ctx, S_CUB, std::max(std::max(t1, t2), std::max(t3, t4)))) return PSG_E_NOMEM;
-	}
+	// the scans' tile sums (one buffer, scans one after another in stream order)
+	if (!psg_scratch(ctx, S_SCAN, sizeof(unsigned long long) * (scan_tiles(std::max(std::max(pl.KN, cap + 1),
+			nray + 1)) + 1)))
+		return PSG_E_NOMEM;
 	// grids of the persistent kernels
 	pl.dep_grid = pl.gen ? occ_grid(ctx, k_deposit<true, false>, DEP_THREADS)
 			: (pl.aff ? occ_grid(ctx, k_deposit<false, true>, DEP_THREADS) : occ_grid(ctx, k_deposit<false, false>,
@@ -1686,7 +1718,6 @@ int plan_batch(psg_context *ctx, size_t R, size_t K, const PsgTraceFill &tf, Bat
 // Everything of the batch after the traversal. No host reads, no
 // allocation: the launch shapes depend on the plan alone; per-call values
 // come from B.
-template <typename KT>
 int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	cudaStream_t st = ctx->stream;
 	const size_t R = pl.R, K = pl.K, nray = pl.nray, cap = pl.cap;
@@ -1697,40 +1728,32 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
 	uint32_t *hit_ipar = (uint32_t *)ctx->scratch[S_HIT_IPAR].p;
 	double *hit_kern = (double *)ctx->scratch[S_HIT_KERN].p;
-	void *cubtmp = ctx->scratch[S_CUB].p;
 
-	// by-particle order of all hits: (tick, ipar) keys over the capacity
+	// by-particle order of all hits: per (tick, particle) key its run of
+	// slots, counted, placed, then put in hit order
 	psg_mark_begin(ctx, PSG_K_SLOTS);
-	KT *keys = (KT *)ctx->scratch[S_KEYS].p;
 	uint32_t *vals = (uint32_t *)ctx->scratch[S_VALS].p;
 	uint32_t *slot = (uint32_t *)ctx->scratch[S_SLOT].p;
 	double *acc = (double *)ctx->scratch[S_ACC].p;
 	ActView av = act_view(ctx, pl);
-	KT *act_key = (KT *)av.act_key;
+	uint32_t *kcnt = (uint32_t *)ctx->scratch[S_SLOTCNT].p;
+	unsigned long long *kbase = slot_base(ctx, pl);
+	unsigned long long *tiles = (unsigned long long *)ctx->scratch[S_SCAN].p;
+	const uint32_t N = (uint32_t)ctx->n;
 	const unsigned cgrid = (unsigned)std::min<size_t>(blocks(cap, 256), (size_t)sms * 16);
-	k_slot_keys<KT><<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, pl.shift, off64, hit_ipar, keys, vals);
+	PSG_CUDA(cudaMemsetAsync(kcnt, 0, sizeof(uint32_t) * pl.KN, st));
+	k_slot_count<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt);
 	PSG_CHECK_LAUNCH();
-	k_pad_keys<KT><<<cgrid, 256, 0, st>>>(cap, off64, nray, keys, vals);
-	PSG_CHECK_LAUNCH();
-	{
-		size_t tmp = pl.sort_tmp;
-		PSG_CUDA(cub::DeviceRadixSort::SortPairs(cubtmp, tmp, keys, keys + cap, vals, vals + cap, (int64_t)cap, 0,
-				pl.shift + pl.tbits, st));
-	}
-	k_slots<KT><<<cgrid, 256, 0, st>>>(cap, off64, nray, keys + cap, vals + cap, slot, av.head);
-	PSG_CHECK_LAUNCH();
-	{
-		size_t tmp = pl.head_tmp;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, tmp, av.head, av.hscan, (int)cap, st));
-	}
-	k_active<KT><<<cgrid, 256, 0, st>>>(off64, nray, pl.shift, keys + cap, av.head, av.hscan, av.act_ipar,
-			av.act_seg, act_key);
+	PSG_CUDA(scan_enqueue(st, kcnt, pl.KN, kbase, tiles, SlotPair()));
+	k_slot_place<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt, kbase, vals);
 	PSG_CHECK_LAUNCH();
 	unsigned long long *d_nact = ctx->d_counters + 6;
-	k_tick_bounds<KT><<<blocks(K + 1, 128), 128, 0, st>>>((int)K, pl.shift, act_key, off64, nray, av.head, av.hscan,
-			av.act_seg, av.tick_act, d_nact);
+	k_act_build<<<(unsigned)std::min<size_t>(blocks(pl.KN, 256), (size_t)sms * 16), 256, 0, st>>>(pl.KN, N, (int)K,
+			kbase, av.act_ipar, av.act_seg, av.tick_act, d_nact);
 	PSG_CHECK_LAUNCH();
-	ctx->launches += 6;
+	k_slot_canon<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, av.act_seg, vals, slot);
+	PSG_CHECK_LAUNCH();
+	ctx->launches += 8;
 	unsigned long long *d_nsat = ctx->d_counters + 1;      // (zeroed by the caller, per call)
 	psg_mark_end(ctx);
 
@@ -1743,10 +1766,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	UpdView uv = upd_view(ctx, pl);
 	k_ray_class<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, ctx->tune.deposit_long, ctx->tune.deposit_mid, cls);
 	PSG_CHECK_LAUNCH();
-	{
-		size_t tmp = pl.cls_tmp;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, tmp, cls, cls_scan, (int)nray, st));
-	}
+	PSG_CUDA(scan_enqueue(st, cls, nray, cls_scan, tiles, Widen()));
 	k_ray_lists<<<blocks(nray, 256), 256, 0, st>>>(nray, cls, cls_scan, long_rays, mid_rays, short_rays);
 	PSG_CHECK_LAUNCH();
 	k_tick_rays<<<blocks(K, 128), 128, 0, st>>>((int)K, R, nray, cls, cls_scan, uv.tick_rays);
@@ -1761,20 +1781,23 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	HeStiffItem *hstiff = pl.helium ? (HeStiffItem *)ctx->scratch[S_REC].p : nullptr;
 	float *feat = pl.feat_on ? (float *)ctx->scratch[S_LOG].p : nullptr;
 	int32_t *aflag = (int32_t *)ctx->scratch[S_ALONG].p;
-	int32_t *ascan = aflag + (cap + 1);
-	uint32_t *long_act = (uint32_t *)(ascan + (cap + 1));
+	unsigned long long *ascan = (unsigned long long *)(((uintptr_t)(aflag + cap + 1) + 15) & ~(uintptr_t)15);
+	uint32_t *long_act = (uint32_t *)(ascan + (cap + 2));
 	int32_t *tick_long = (int32_t *)(long_act + (cap + 1));
 	k_act_class<<<cgrid, 256, 0, st>>>(cap, av.tick_act, (int)K, av.act_seg, aflag);
 	PSG_CHECK_LAUNCH();
-	{
-		size_t tmp = pl.act_tmp;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, tmp, aflag, ascan, (int)(cap + 1), st));
-	}
+	PSG_CUDA(scan_enqueue(st, aflag, cap + 1, ascan, tiles, Widen()));
 	k_act_lists<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, aflag, ascan, long_act);
 	PSG_CHECK_LAUNCH();
 	k_tick_long<<<blocks(K + 1, 256), 256, 0, st>>>((int)K, av.tick_act, ascan, tick_long);
 	PSG_CHECK_LAUNCH();
-	ctx->launches += 3;
+	// the slot order of the long runs (the short ones are in order already)
+	psg_mark_begin(ctx, PSG_K_SLOTS);
+	k_slot_canon_long<<<(unsigned)(2 * sms), 1024, sizeof(uint32_t) * pl.long_cap, st>>>(tick_long, (int)K, long_act,
+			av.act_seg, vals, slot, pl.long_cap, ctx->d_status);
+	PSG_CHECK_LAUNCH();
+	psg_mark_end(ctx);
+	ctx->launches += 6;
 
 	// the tick loop
 	double *d_lost = (double *)(ctx->d_counters + 2);
@@ -1902,7 +1925,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 std::vector<unsigned long long> batch_key(const psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	std::vector<unsigned long long> k;
 	k.push_back(pl.R); k.push_back(pl.K); k.push_back(pl.cap); k.push_back(pl.pcap);
-	k.push_back(pl.maxcount > PSG_SORT_MAX); k.push_back(pl.shift); k.push_back(pl.tbits);
+	k.push_back(pl.maxcount > PSG_SORT_MAX); k.push_back(pl.KN); k.push_back((unsigned long long)pl.long_cap);
 	k.push_back((unsigned long long)pl.nacc | (pl.want_heat << 4) | (pl.gen << 5) | (pl.helium << 6) | (pl.iso << 7) |
 			(pl.euler << 8) | (pl.surr << 9) | (pl.aff << 10) | (pl.feat_on << 11));
 	k.push_back((unsigned long long)(uintptr_t)ctx->stream);
@@ -1937,7 +1960,7 @@ std::vector<unsigned long long> batch_key(const psg_context *ctx, const BatchPla
 }
 
 int enqueue_any(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
-	return pl.key64 ? enqueue_batch<unsigned long long>(ctx, pl, B) : enqueue_batch<uint32_t>(ctx, pl, B);
+	return enqueue_batch(ctx, pl, B);
 }
 
 // Replays the graph of `key`, capturing what `enqueue` issues first if no

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "psg_internal.cuh"
+#include "psg_scan.cuh"
 #include "psg_solve.cuh"
 
 namespace {
@@ -253,7 +254,7 @@ __global__ void k_compact_slabs(size_t nray, size_t scap, const int64_t *__restr
 // capacity empties every list instead (nothing downstream reads past cap)
 // and flags the status word for the host to redo the call; the call's
 // largest total is kept in *tickmax.
-__global__ void k_offsets64(const uint32_t *__restrict__ scan32, const uint32_t *__restrict__ count,
+__global__ void k_offsets64(const unsigned long long *__restrict__ scan32, const uint32_t *__restrict__ count,
 		size_t nray, int64_t *__restrict__ off64, int32_t *__restrict__ off32,
 		unsigned long long *__restrict__ maxcount, size_t cap, unsigned long long *__restrict__ tickmax,
 		uint32_t *__restrict__ status) {
@@ -476,6 +477,13 @@ __global__ void k_sort_classify(size_t nray, const int64_t *__restrict__ off, ui
 
 inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+// S_COUNT during a traversal: the hit counts (nray + 1, u32), then their
+// exclusive scan (nray + 2, u64) at the next 16-byte boundary
+size_t count_bytes(size_t nray) { return 16 * ((sizeof(uint32_t) * (nray + 1) + 15) / 16) + 8 * (nray + 2) + 64; }
+unsigned long long *count_scan(uint32_t *count, size_t nray) {
+	return (unsigned long long *)((char *)count + 16 * ((sizeof(uint32_t) * (nray + 1) + 15) / 16));
+}
+
 }  // namespace
 
 // Hit counts clamped to the slab capacity for the offsets (the slabs hold
@@ -502,7 +510,7 @@ __global__ void k_count_clamp(size_t nray, size_t scap, uint32_t *__restrict__ c
 int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray, const unsigned *nlim, size_t cap) {
 	cudaStream_t st = ctx->stream;
 	uint32_t *count = (uint32_t *)ctx->scratch[S_COUNT].p;
-	uint32_t *scan = count + (nray + 1);
+	unsigned long long *scan = count_scan(count, nray);
 	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
 	int32_t *off32 = (int32_t *)((char *)ctx->scratch[S_OFFSETS].p + sizeof(int64_t) * (nray + 1));
 	unsigned long long *d_max = ctx->d_counters + 4;
@@ -522,8 +530,7 @@ int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray,
 	PSG_CHECK_LAUNCH();
 	k_count_clamp<<<blocks(nray, 256), 256, 0, st>>>(nray, scap, count, ctx->d_counters + 3, ctx->d_status);
 	PSG_CHECK_LAUNCH();
-	size_t tmp = ctx->scratch[S_CUB].bytes;
-	PSG_CUDA(cub::DeviceScan::ExclusiveSum(ctx->scratch[S_CUB].p, tmp, count, scan, (int)(nray + 1), st));
+	PSG_CUDA(scan_enqueue(st, count, nray + 1, scan, (unsigned long long *)ctx->scratch[S_SCAN].p, Widen()));
 	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32, d_max, cap,
 			ctx->d_counters + 24, ctx->d_status);
 	PSG_CHECK_LAUNCH();
@@ -536,15 +543,12 @@ int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray,
 int psg_trace_fill_prepare(psg_context *ctx, size_t nray) {
 	const size_t scap = ctx->slab_cap;
 	const size_t slots = nray * scap;
-	if (!psg_scratch(ctx, S_COUNT, sizeof(uint32_t) * 2 * (nray + 1)) ||
+	if (!psg_scratch(ctx, S_COUNT, count_bytes(nray)) ||
+			!psg_scratch(ctx, S_SCAN, sizeof(unsigned long long) * (scan_tiles(nray + 1) + 1)) ||
 			!psg_scratch(ctx, S_OFFSETS, (sizeof(int64_t) + sizeof(int32_t)) * (nray + 1) + 256) ||
 			!psg_scratch(ctx, S_REC_U32, sizeof(uint32_t) * (slots ? slots : 1)) ||
 			!psg_scratch(ctx, S_REC_F64, sizeof(double) * 2 * (slots ? slots : 1)))
 		return PSG_E_NOMEM;
-	uint32_t *count = (uint32_t *)ctx->scratch[S_COUNT].p;
-	size_t tmp = 0;
-	PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, count, count + (nray + 1), (int)(nray + 1), ctx->stream));
-	if (!psg_scratch(ctx, S_CUB, tmp)) return PSG_E_NOMEM;
 	const int trw = std::max(1, std::min(TR_MAX_WARPS, ctx->tune.trace_warps));
 	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ctx->ppc + 32) * trw;
 	if (smem > 48 * 1024)
@@ -563,10 +567,12 @@ int psg_trace_fill_prepare(psg_context *ctx, size_t nray) {
 int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTraceFill *tf) {
 	if (!ctx->have_tree) return psg_fail(ctx, PSG_E_INVAL, "trace: no tree (psg_build_tree first)");
 	cudaStream_t st = ctx->stream;
-	uint32_t *count = (uint32_t *)psg_scratch(ctx, S_COUNT, sizeof(uint32_t) * 2 * (nray + 1));
+	uint32_t *count = (uint32_t *)psg_scratch(ctx, S_COUNT, count_bytes(nray));
 	char *offmem = (char *)psg_scratch(ctx, S_OFFSETS, (sizeof(int64_t) + sizeof(int32_t)) * (nray + 1) + 256);
-	if (!count || !offmem) return PSG_E_NOMEM;
-	uint32_t *scan = count + (nray + 1);
+	unsigned long long *tiles = (unsigned long long *)psg_scratch(ctx, S_SCAN,
+			sizeof(unsigned long long) * (scan_tiles(nray + 1) + 1));
+	if (!count || !offmem || !tiles) return PSG_E_NOMEM;
+	unsigned long long *scan = count_scan(count, nray);
 	int64_t *off64 = (int64_t *)offmem;
 	int32_t *off32 = (int32_t *)(offmem + sizeof(int64_t) * (nray + 1));
 	unsigned long long *d_max = ctx->d_counters + 4;
@@ -600,11 +606,7 @@ int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTrac
 		}
 		PSG_CHECK_LAUNCH();
 		psg_mark_end(ctx);
-		size_t tmp = 0;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, count, scan, (int)(nray + 1), st));
-		void *dt = psg_scratch(ctx, S_CUB, tmp);
-		if (!dt) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, count, scan, (int)(nray + 1), st));
+		PSG_CUDA(scan_enqueue(st, count, nray + 1, scan, tiles, Widen()));
 		k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32, d_max, 0, nullptr,
 				nullptr);
 		PSG_CHECK_LAUNCH();
