@@ -133,6 +133,9 @@ def make(workload: str):
     return fields.make_workload(workload)
 
 
+_REF = None
+
+
 def cpu_baseline_reference(w, seconds: float = 15.0, threads: int | None = None, ticks=None):
     """The reference's own CPU code (oracle/_ref) on a bounded sample of the
     same workload: hits/s over its trace + deposit time, as its stat counters
@@ -149,7 +152,10 @@ def cpu_baseline_reference(w, seconds: float = 15.0, threads: int | None = None,
         # dense cells of the log-normal field reach; its hits/s clock covers
         # trace + deposit only, which do not depend on the solver, so the
         # sample runs its isothermal solver.
-        ref = Reference(RATES_HUI, w.field.units, isothermal=True, threads=threads)
+        global _REF
+        if _REF is None:       # the reference keeps its state in globals: one instance per process
+            _REF = Reference(RATES_HUI, w.field.units, isothermal=True, threads=threads)
+        ref = _REF
         ref.load(w.field)
         ref.build_tree(8)
         ref.reset_stats()
@@ -257,6 +263,126 @@ def run_reference(args):
         dist.destroy_process_group()
 
 
+def surrogate_leg(ctx, w, R, T, ts, surr_path, dev, stream, nsurr=4, tol=1e-3):
+    """The chemistry surrogate against the integrator: the same nsurr steps
+    of T ticks from one state, plain and with the network (trained weights
+    shipped in psphray_b200/data); GPU s per simulated Myr, the accepted
+    fraction and the x_HII difference between the two."""
+    import torch
+    from psphray_b200.surrogate import Surrogate
+    net = Surrogate.load(surr_path)
+    for src in w.schedule.sources:          # one tick's photons at the first tick, as in a run
+        src.lastemit = ts - 1
+    s_rays = [torch.from_numpy(w.schedule.rays_for_ticks(ts + i * T, T).view(np.uint8)).to(f"cuda:{dev}")
+              for i in range(nsurr)]
+    st0 = ctx.state()
+    keep = {k: st0[k] for k in ("lambdaH", "ie", "lasthit")}
+    res = {}
+    for mode in ("plain", "surrogate"):
+        ctx.set_state(**keep)
+        if mode == "surrogate":
+            net.install(ctx, tol=tol)
+        ms, acc, act = 0.0, 0.0, 0.0
+        for i in range(nsurr):
+            e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = ctx.run_ticks_device(s_rays[i].data_ptr(), R, T, ts + i * T, w.tick_time)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            acc += st["surrogate_accepted"]
+            act += st["active"]
+        res[mode] = (ms, acc / max(act, 1.0), 1.0 - ctx.lambdaH())
+        if mode == "surrogate":
+            Surrogate.uninstall(ctx)
+    myr = nsurr * T * w.tick_time / w.field.units.MYR
+    xp, xs = res["plain"][2], res["surrogate"][2]
+    rel = np.abs(xs - xp) / np.maximum(xp, 1e-6)
+    return {"tol": tol, "steps": nsurr, "ticks_per_step": T, "weights": os.path.basename(surr_path),
+            "gpu_s_per_sim_myr_plain": res["plain"][0] / 1e3 / myr,
+            "gpu_s_per_sim_myr_surrogate": res["surrogate"][0] / 1e3 / myr,
+            "accepted_fraction": res["surrogate"][1],
+            "x_HII_rel_diff": {"p50": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),
+                               "max": float(rel.max())}}
+
+
+def timed_steps(ctx, rays_dev, R, T, t_first, tick_time, stream, nsteps):
+    """nsteps batches of T ticks timed with CUDA events: (ms, hits, syncs)."""
+    import torch
+    ms = hits = syncs = 0.0
+    for s in range(nsteps):
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = ctx.run_ticks_device(rays_dev[s].data_ptr(), R, T, t_first + s * T, tick_time)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        hits += st["hits"]
+        syncs += st["host_syncs"]
+    return ms, hits, syncs
+
+
+def default_physics_leg(w, dev, stream, dev_rays, R, T, nrs):
+    """The reference's default physics together (config.c:25,28,31: helium,
+    secondary ionisation, recombination rays, not isothermal) on the same
+    particles (hydrogen mass fraction 0.76) and rays: hits/s."""
+    from psphray_b200 import api
+    from psphray_b200.units import Units
+    hu = Units(hmf=0.76)
+    hf = dataclasses.replace(w.field, units=hu)
+    c = api.Context(dev)
+    c.set_stream(stream.cuda_stream)
+    c.set_physics(api.Physics(hu, isothermal=w.isothermal, h_only=False, secondary_ionization=True,
+                              on_the_spot=False))
+    c.load(hf)
+    c.build_tree(8)
+    c.set_recombination(nrec=100)
+    c.run_ticks_device(dev_rays[0].data_ptr(), R, T, 1, w.tick_time)
+    ms, hits, syncs = timed_steps(c, dev_rays[1:], R, T, 1 + T, w.tick_time, stream, nrs)
+    c.close()
+    return {"value": hits / (ms / 1e3), "unit": "hits/s", "ms_per_tick": ms / (nrs * T), "hmf": 0.76,
+            "secondary_ionization": True, "on_the_spot": False, "nrec_per_species": 100, "steps": nrs,
+            "ticks_per_step": T, "host_syncs_per_step": syncs / nrs}
+
+
+def full_pipeline_leg(dev, stream, cpu: bool):
+    """The full pipeline's field (256^3 = 16.8M particles, sigma 1.5, 256
+    sources, 65536 rays per tick, not isothermal), one tick per step: hits/s
+    and GPU s per simulated Myr, plain and with the surrogate, and the
+    reference's own CPU code on a bounded sample of the same ticks."""
+    import torch
+    from psphray_b200 import api
+    w = make("lognormal256")
+    R, T = w.schedule.nray, 1
+    c = api.Context(dev)
+    c.set_stream(stream.cuda_stream)
+    c.set_physics(api.Physics(w.field.units, isothermal=w.isothermal))
+    c.load(w.field)
+    c.build_tree(8)
+    nst = 4
+    rays = [torch.from_numpy(w.schedule.rays_for_ticks(1 + s, 1).view(np.uint8)).to(f"cuda:{dev}")
+            for s in range(nst + 2)]
+    for s in range(2):
+        c.run_ticks_device(rays[s].data_ptr(), R, T, 1 + s, w.tick_time)
+    ms, hits, syncs = timed_steps(c, rays[2:], R, T, 3, w.tick_time, stream, nst)
+    value = hits / (ms / 1e3)
+    myr = nst * T * w.tick_time / w.field.units.MYR
+    out = {"workload": "lognormal256", "particles": w.field.n, "rays_per_tick": R, "value": value,
+           "unit": "hits/s", "ms_per_tick": ms / nst, "gpu_s_per_sim_myr": ms / 1e3 / myr,
+           "host_syncs_per_step": syncs / nst}
+    surr_path = os.path.join(ROOT, "psphray_b200", "data", "surrogate_lognormal128.npz")
+    if os.path.exists(surr_path):
+        out["surrogate"] = surrogate_leg(c, w, R, T, 3 + nst, surr_path, dev, stream, nsurr=3)
+    c.close()
+    del rays
+    torch.cuda.empty_cache()
+    if cpu:
+        base = cpu_baseline_reference(make("lognormal256"), seconds=10.0, ticks=1)
+        out["cpu_baseline"] = base
+        out["vs_cpu"] = value / base["value"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -269,6 +395,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch shapes")
+    ap.add_argument("--no-full-pipeline", action="store_true", help="skip the 16.8M-particle leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -381,46 +508,10 @@ def main():
     # on the integrator and with the network (trained weights shipped in
     # psphray_b200/data), GPU s per simulated Myr and the x_HII difference
     surrogate = None
-    surr_path = os.path.join(ROOT, "psphray_b200", "data", f"surrogate_{args.workload}.npz")
+    surr_path = os.path.join(ROOT, "psphray_b200", "data", "surrogate_lognormal128.npz")
     if not w.isothermal and os.path.exists(surr_path):
-        from psphray_b200.surrogate import Surrogate
-        net = Surrogate.load(surr_path)
-        nsurr, tol = 4, 1e-3
         ts = t1 + (args.steps + 2) * T
-        for src in w.schedule.sources:          # one tick's photons at the first tick, as in a run
-            src.lastemit = ts - 1
-        s_rays = [torch.from_numpy(w.schedule.rays_for_ticks(ts + i * T, T).view(np.uint8)).to(f"cuda:{dev}")
-                  for i in range(nsurr)]
-        st0 = ctx.state()
-        keep = {k: st0[k] for k in ("lambdaH", "ie", "lasthit")}
-        res = {}
-        for mode in ("plain", "surrogate"):
-            ctx.set_state(**keep)
-            if mode == "surrogate":
-                net.install(ctx, tol=tol)
-            ms, acc, act = 0.0, 0.0, 0.0
-            for i in range(nsurr):
-                e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                st = ctx.run_ticks_device(s_rays[i].data_ptr(), R, T, ts + i * T, w.tick_time)
-                e1.record(stream)
-                e1.synchronize()
-                ms += e0.elapsed_time(e1)
-                acc += st["surrogate_accepted"]
-                act += st["active"]
-            res[mode] = (ms, acc / max(act, 1.0), 1.0 - ctx.lambdaH())
-            if mode == "surrogate":
-                Surrogate.uninstall(ctx)
-        myr = nsurr * T * w.tick_time / w.field.units.MYR
-        xp, xs = res["plain"][2], res["surrogate"][2]
-        rel = np.abs(xs - xp) / np.maximum(xp, 1e-6)
-        surrogate = {"tol": tol, "steps": nsurr, "ticks_per_step": T,
-                     "gpu_s_per_sim_myr_plain": res["plain"][0] / 1e3 / myr,
-                     "gpu_s_per_sim_myr_surrogate": res["surrogate"][0] / 1e3 / myr,
-                     "accepted_fraction": res["surrogate"][1],
-                     "x_HII_rel_diff": {"p50": float(np.median(rel)), "p99": float(np.percentile(rel, 99)),
-                                        "max": float(rel.max())}}
-
+        surrogate = surrogate_leg(ctx, w, R, T, ts, surr_path, dev, stream)
     # the side legs (recombination rays, helium) load further contexts of the
     # same field; the 16.8 M-particle field is measured without them
     recombination = helium = None
@@ -480,6 +571,14 @@ def main():
         hctx.close()
         helium = {"value": h_hits / (h_ms / 1e3), "unit": "hits/s", "ms_per_tick": h_ms / (nrs * T),
                   "hmf": 0.76, "secondary_ionization": True, "steps": nrs, "ticks_per_step": T}
+
+    # the reference's default physics together, and the full pipeline's
+    # field (one-GPU runs on the default workload: they add a few minutes)
+    default_physics = full_pipeline = None
+    if args.workload in SIDE_LEGS:
+        default_physics = default_physics_leg(w, dev, stream, dev_rays, R, T, min(3, nsteps - 1))
+    if args.workload == "lognormal128" and world == 1 and not args.no_full_pipeline:
+        full_pipeline = full_pipeline_leg(dev, stream, cpu=rank == 0 and not args.no_cpu_baseline)
 
     # the per-kernel-group breakdown: the same steps again (later ticks) with
     # the library's per-launch events on -- kept out of the timed steps,
@@ -541,6 +640,8 @@ def main():
             "surrogate": surrogate,
             "recombination": recombination,
             "helium": helium,
+            "default_physics": default_physics,
+            "full_pipeline": full_pipeline,
             "e2e_device_emission": {"value": em_hits / em_t, "unit": "hits/s", "h2d_bytes_per_step": 0,
                                     "d2h_bytes_per_step": int(lam.nbytes)},
             "e2e": {"value": e2e_hits / e2e_t, "unit": "hits/s",
