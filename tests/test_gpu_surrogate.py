@@ -136,6 +136,25 @@ def test_surrogate_ticks(phys_noniso):
         # over 8 ticks most particles stay far inside 1%
         assert np.median(rel) < 1e-3
         assert np.percentile(rel, 99) < 2e-2
+        # and both against the FP64 oracle (the restatement's rtol-1e-10
+        # integration of the same 20 ticks): the plain path within its
+        # integrator tolerance, the surrogate's x_HII within 1% of the
+        # oracle's wherever x_HII is above 1e-3 (below, relative errors
+        # measure round-off of a fraction that is still neutral gas)
+        from oracle import Oracle
+        orc = Oracle(w.field, phys_noniso, isothermal=False)
+        orc.build_tree(8)
+        allr = np.concatenate([rb, rb2])
+        for t in range(1, 21):
+            orc.tick(allr[(t - 1) * 256:t * 256], t, w.tick_time)
+        xo = 1.0 - orc.lambdaH
+        m = xo > 1e-3
+        err_plain = np.abs(xb - xo)[m] / xo[m]
+        err_surr = np.abs(xc - xo)[m] / xo[m]
+        print("x_HII vs the FP64 oracle: plain max %.3g, surrogate max %.3g p99 %.3g" %
+              (err_plain.max(), err_surr.max(), np.percentile(err_surr, 99)))
+        assert err_plain.max() < 1e-3
+        assert err_surr.max() < 1e-2
     finally:
         for ctx in (a, b, c):
             ctx.close()
