@@ -122,7 +122,8 @@ struct psg_context {
 	double lte_freq_min[3] = {}, lte_freq_step[3] = {};
 	size_t rec_last = 0;         // recombination rays of the last tick (after the source rays in S_RECRAYS)
 	size_t rec_last_R = 0;       // source rays of that tick
-	size_t rec_last_kmax = 0;    // capacity of that tick's key arrays (S_RECK)
+	size_t rec_last_kmax = 0;    // capacity of that tick's item arrays (S_RECK)
+	int rec_last_threshold = 0;  // that tick ran in threshold mode (its items unsorted, in place)
 
 	// chemistry surrogate (not isothermal): weight blob, residual tolerance
 	void *d_surr = nullptr;
@@ -147,7 +148,6 @@ struct psg_context {
 	size_t batch_cap = 0;                       // hits the tick batches' per-hit buffers hold
 	unsigned sort_grid[8] = {};                 // persistent grids of the per-ray sort's classes
 	unsigned trace_grid = 0;                    // persistent grid of the traversal (psg_trace_fill_prepare)
-	size_t rec_tmp[2] = {0, 0};                 // library temporaries of the recombination emission
 	psg_tune tune{4, 96, 384, 1, 8};            // launch shapes (psg_set_tune, psg_autotune)
 	long host_syncs = 0;                        // host synchronisations of the current call
 	void *graphs = nullptr;                     // captured tick batches (psg_tick.cu)

@@ -27,13 +27,14 @@
 // psg_set_recombination. The reference draws from GSL's MT19937 and its
 // Walker tables (gsl_ran_discrete); the draws here are inverse-CDF draws
 // of the same distributions.
-#include <cub/cub.cuh>
-
 #include <math.h>
+#include <string.h>
 
 #include <vector>
 
 #include "psg_internal.cuh"
+#include "psg_bsort.cuh"
+#include "psg_scan.cuh"
 #include "psg_helium.cuh"
 #include "psg_philox.cuh"
 #include "psg_solve.cuh"
@@ -85,12 +86,21 @@ __global__ void k_rec_weight(size_t n, const PsgBatchDev *__restrict__ B, const 
 	leaf_of[c] = (uint32_t)p;
 }
 
-// nrec draws of species s from the cumulative weights (caller order):
-// key = s << 56 | caller index << 24 | draw, value = the particle (leaf
-// order); count[s] = nrec, or 0 when no weight is positive.
+// A recombination ray before the sort: key = species << 56 | caller index
+// << 24 | draw, val = the emitter (leaf order).
+struct RecItem {
+	unsigned long long key;
+	uint32_t val, spare;
+};
+struct RecItemLess {
+	__device__ __forceinline__ bool operator()(const RecItem &x, const RecItem &y) const { return x.key < y.key; }
+};
+
+// nrec draws of species s from the cumulative weights (caller order);
+// count[s] = nrec, or 0 when no weight is positive.
 __global__ void k_rec_draw(size_t n, int nrec, int s, uint32_t stream, const double *__restrict__ cdf,
 		const PsgBatchDev *__restrict__ B, uint64_t seed, const uint32_t *__restrict__ leaf_of,
-		unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals, unsigned *__restrict__ count) {
+		RecItem *__restrict__ items, unsigned *__restrict__ count) {
 	const int64_t tick = B->tick0;
 	const double total = tick > 1 ? cdf[n - 1] : 0.0;       // from the second tick on (loop.c:197)
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -101,28 +111,41 @@ __global__ void k_rec_draw(size_t n, int nrec, int s, uint32_t stream, const dou
 	const double target = rn_dmul(u01(x[0], x[1]), total);
 	int c = upper_index(cdf, 0, (int)n, target);
 	if (c >= (int)n) c = lower_index(cdf, 0, (int)n, total);   // the last particle with weight
-	keys[k] = ((unsigned long long)s << 56) | ((unsigned long long)c << 24) | (unsigned long long)k;
-	vals[k] = leaf_of[c];
+	items[k].key = ((unsigned long long)s << 56) | ((unsigned long long)c << 24) | (unsigned long long)k;
+	items[k].val = leaf_of[c];
 }
 
-// Threshold mode (loop.c:221-230): every marked particle above the threshold.
+// Threshold mode (loop.c:221-230): every marked particle above the
+// threshold, flagged in the caller's order (flag[c] for species s at
+// s * n + c), and the caller -> leaf map.
 __global__ void k_rec_flag(size_t n, const PsgBatchDev *__restrict__ B, const int32_t *__restrict__ mark,
-		const float *__restrict__ ygrec, double threshold, uint32_t *__restrict__ flag) {
+		const float *__restrict__ ygrec, double threshold, const uint32_t *__restrict__ order,
+		uint32_t *__restrict__ flag, uint32_t *__restrict__ leaf_of) {
 	const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (p >= n) return;
 	const int32_t prev = (int32_t)(B->tick0 - 1);
-	flag[p] = (B->tick0 > 1 && mark[p] == prev && (double)ygrec[p] > threshold) ? 1u : 0u;
+	const uint32_t c = caller_of(order, (uint32_t)p);
+	flag[c] = (B->tick0 > 1 && mark[p] == prev && (double)ygrec[p] > threshold) ? 1u : 0u;
+	leaf_of[c] = (uint32_t)p;
 }
 
-__global__ void k_rec_compact(size_t n, int s, const uint32_t *__restrict__ flag, const uint32_t *__restrict__ pos,
-		const uint32_t *__restrict__ order, unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals,
+// The flagged emitters of all species in (species, caller index) order --
+// the order the sort gives -- from the scan of the flags; count[s] per
+// species.
+__global__ void k_rec_place(size_t n, int nspec, const uint32_t *__restrict__ flag,
+		const unsigned long long *__restrict__ pos, const uint32_t *__restrict__ leaf_of, RecItem *__restrict__ items,
 		unsigned *__restrict__ count) {
-	const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (p >= n) return;
-	if (p == n - 1) count[s] = pos[p] + flag[p];
-	if (!flag[p]) return;
-	keys[pos[p]] = ((unsigned long long)s << 56) | ((unsigned long long)caller_of(order, (uint32_t)p) << 24);
-	vals[pos[p]] = (uint32_t)p;
+	const size_t total = n * (size_t)nspec;
+	const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	if (i == 0)
+		for (int s = 0; s < nspec; s++) count[s] = (unsigned)(pos[(size_t)(s + 1) * n] - pos[(size_t)s * n]);
+	if (i >= total || !flag[i]) return;
+	const size_t s = i / n, c = i - s * n;
+	RecItem r;
+	r.key = ((unsigned long long)s << 56) | ((unsigned long long)c << 24);
+	r.val = leaf_of[c];
+	r.spare = 0;
+	items[pos[i]] = r;
 }
 
 // The LTE tables of the three species (HI, HeI, HeII recombinations).
@@ -143,8 +166,8 @@ __device__ __forceinline__ unsigned long long run_of(unsigned long long key) { r
 // its rays by (type, ipar), loop.c:236. Each ray's photons: the emitter's
 // yGrec of the species times NH (HII) or NHe (HeII, HeIII), split over the
 // run of rays that drew it (loop.c:277-290, 305-320).
-__global__ void k_rec_rays(const unsigned *__restrict__ count, const unsigned long long *__restrict__ keys,
-		const uint32_t *__restrict__ vals, const PsgBatchDev *__restrict__ B, uint64_t seed,
+__global__ void k_rec_rays(const unsigned *__restrict__ count, const RecItem *__restrict__ items,
+		const PsgBatchDev *__restrict__ B, uint64_t seed,
 		const float4 *__restrict__ psml, const float *__restrict__ mass, RecState Y,
 		const double *__restrict__ lambdaH, const float *__restrict__ ie, PhysParams P, LteView L, double length,
 		psg_ray *__restrict__ out, double *__restrict__ nph_sum) {
@@ -152,12 +175,12 @@ __global__ void k_rec_rays(const unsigned *__restrict__ count, const unsigned lo
 	const int64_t tick = B->tick0;
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= M) return;
-	const uint32_t p = vals[i];
-	const unsigned long long run = run_of(keys[i]);
-	const int s = (int)(keys[i] >> 56);
+	const uint32_t p = items[i].val;
+	const unsigned long long run = run_of(items[i].key);
+	const int s = (int)(items[i].key >> 56);
 	int c = 1;
-	for (int j = i - 1; j >= 0 && run_of(keys[j]) == run; j--) c++;
-	for (int j = i + 1; j < M && run_of(keys[j]) == run; j++) c++;
+	for (int j = i - 1; j >= 0 && run_of(items[j].key) == run; j--) c++;
+	for (int j = i + 1; j < M && run_of(items[j].key) == run; j++) c++;
 	const double N = rn_dmul((double)mass[p], s == 0 ? P.H_PER_MASS : P.HE_PER_MASS);
 	psg_ray r;
 	r.Nph = rn_dmul(rn_dmul((double)Y.yg[s][p], N), __ddiv_rn(1.0, (double)c));
@@ -198,19 +221,18 @@ __global__ void k_rec_rays(const unsigned *__restrict__ count, const unsigned lo
 
 // The photons leave the emitter (loop.c:345-368): once per run, ray by ray
 // in float as the reference's compound assignment rounds, never below 0.
-__global__ void k_rec_purge(const unsigned *__restrict__ count, const unsigned long long *__restrict__ keys,
-		const uint32_t *__restrict__ vals, const psg_ray *__restrict__ rays, const float *__restrict__ mass, RecState Y,
-		PhysParams P) {
+__global__ void k_rec_purge(const unsigned *__restrict__ count, const RecItem *__restrict__ items,
+		const psg_ray *__restrict__ rays, const float *__restrict__ mass, RecState Y, PhysParams P) {
 	const int M = (int)(count[0] + count[1] + count[2]);
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= M) return;
-	const unsigned long long run = run_of(keys[i]);
-	if (i > 0 && run_of(keys[i - 1]) == run) return;
-	const uint32_t p = vals[i];
-	const int s = (int)(keys[i] >> 56);
+	const unsigned long long run = run_of(items[i].key);
+	if (i > 0 && run_of(items[i - 1].key) == run) return;
+	const uint32_t p = items[i].val;
+	const int s = (int)(items[i].key >> 56);
 	const double N = rn_dmul((double)mass[p], s == 0 ? P.H_PER_MASS : P.HE_PER_MASS);
 	float y = Y.yg[s][p];
-	for (int j = i; j < M && run_of(keys[j]) == run; j++) {
+	for (int j = i; j < M && run_of(items[j].key) == run; j++) {
 		y = (float)rn_dsub((double)y, __ddiv_rn(rays[j].Nph, N));
 		if (y < 0.0f) y = 0.0f;
 	}
@@ -229,39 +251,63 @@ __global__ void k_rec_mark(int R, const unsigned *__restrict__ count, const int6
 		mark[hit_ipar[h]] = tick;
 }
 
+// Work space of the emission (S_RECW) for n particles and nspec species:
+// draws -- the weights in caller order, their FP64 exclusive scan (n + 1),
+// the scan's tile sums, the caller -> leaf map; threshold mode -- the
+// flags of all species in caller order, their scan, its tile sums, the map.
+struct RecWork {
+	double *w, *ex, *tiles_d;
+	uint32_t *flag;
+	unsigned long long *pos, *tiles_u;
+	uint32_t *leaf_of;
+	size_t bytes;
+};
+RecWork rec_work(char *base, size_t n, int nspec, int threshold_mode) {
+	RecWork r{};
+	auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+	size_t o = 0;
+	if (!threshold_mode) {
+		r.w = (double *)(base + o); o = up(o + sizeof(double) * n);
+		r.ex = (double *)(base + o); o = up(o + sizeof(double) * (n + 1));
+		r.tiles_d = (double *)(base + o); o = up(o + sizeof(double) * (scan_tiles(n) + 1));
+	} else {
+		const size_t m = n * (size_t)nspec;
+		r.flag = (uint32_t *)(base + o); o = up(o + sizeof(uint32_t) * m);
+		r.pos = (unsigned long long *)(base + o); o = up(o + sizeof(unsigned long long) * (m + 1));
+		r.tiles_u = (unsigned long long *)(base + o); o = up(o + sizeof(unsigned long long) * (scan_tiles(m) + 1));
+	}
+	r.leaf_of = (uint32_t *)(base + o); o = up(o + sizeof(uint32_t) * n);
+	r.bytes = o;
+	return r;
+}
+
+// Where the tick's rays end, in tick order: the draws' sort leaves them in
+// the first or second half of S_RECK by its number of merge passes; the
+// threshold mode places them in the first half.
+RecItem *rec_sorted(psg_context *ctx, size_t ktot, int threshold_mode) {
+	RecItem *items = (RecItem *)ctx->scratch[S_RECK].p;
+	return (!threshold_mode && (dsort_passes(ktot) & 1)) ? items + ktot : items;
+}
+
 }  // namespace
 
 // The tick's recombination rays into out (at most cap). One pass per
-// species (HII; with helium also HeII and HeIII, loop.c:199): weights or
-// threshold flags, draws into the species' part of the key array (unused
-// entries stay all ones and sort last), then one sort of the whole key
-// array. Launch sizes depend on n and the capacity only; the ray count lives
-// in d_count (counters 11-13) and the kernels read it: no host read, so a
-// tick can be captured. The tick number comes from B.
+// species (HII; with helium also HeII and HeIII, loop.c:199): weights and
+// draws into the species' part of the item array (unused entries stay all
+// ones and sort last), then one merge sort of the whole array; or, with a
+// threshold, flags in caller order, one scan and the placement. Launch
+// sizes depend on n and the capacity only; the ray count lives in d_count
+// (counters 11-13) and the kernels read it: no host read, so a tick can be
+// captured. The tick number comes from B.
 int psg_rec_prepare(psg_context *ctx) {
 	const size_t n = ctx->n;
 	const int threshold_mode = ctx->rec_nrec < 0;
 	const int nspec = ctx->flags.h_only ? 1 : 3;
 	const size_t kmax = threshold_mode ? n : (size_t)ctx->rec_nrec;     // per species
 	const size_t ktot = kmax * nspec;
-	char *wm = (char *)psg_scratch(ctx, S_RECW, sizeof(double) * 2 * n + sizeof(uint32_t) * n + 512);
-	char *km = (char *)psg_scratch(ctx, S_RECK, (sizeof(unsigned long long) + sizeof(uint32_t)) * 2 * ktot + 1024);
-	if (!wm || !km) return PSG_E_NOMEM;
-	unsigned long long *keys = (unsigned long long *)km;
-	uint32_t *vals = (uint32_t *)(keys + 2 * ktot);
-	size_t t1 = 0, t2 = 0;
-	double *w = (double *)wm;
-	if (!threshold_mode) {
-		PSG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, t1, w, w + n, (int64_t)n, ctx->stream));
-	} else {
-		uint32_t *flag = (uint32_t *)wm;
-		PSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t1, flag, flag + n, (int64_t)n, ctx->stream));
-	}
-	PSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t2, keys, keys + ktot, vals, vals + ktot, (int64_t)ktot, 0, 64,
-			ctx->stream));
-	ctx->rec_tmp[0] = t1;
-	ctx->rec_tmp[1] = t2;
-	if (!psg_scratch(ctx, S_CUB, std::max(t1, t2))) return PSG_E_NOMEM;
+	const RecWork W = rec_work(nullptr, n, nspec, threshold_mode);
+	if (!psg_scratch(ctx, S_RECW, W.bytes) || !psg_scratch(ctx, S_RECK, sizeof(RecItem) * 2 * ktot + 1024))
+		return PSG_E_NOMEM;
 	return PSG_OK;
 }
 
@@ -273,44 +319,43 @@ int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out) {
 	const int nspec = ctx->flags.h_only ? 1 : 3;
 	const size_t kmax = threshold_mode ? n : (size_t)ctx->rec_nrec;     // per species
 	const size_t ktot = kmax * nspec;
-	char *wm = (char *)ctx->scratch[S_RECW].p;
-	unsigned long long *keys = (unsigned long long *)ctx->scratch[S_RECK].p;
-	uint32_t *vals = (uint32_t *)(keys + 2 * ktot);
+	const RecWork W = rec_work((char *)ctx->scratch[S_RECW].p, n, nspec, threshold_mode);
+	RecItem *items = (RecItem *)ctx->scratch[S_RECK].p;
 	unsigned *d_count = (unsigned *)(ctx->d_counters + 11);      // [3]
 	double *d_nph = (double *)(ctx->d_counters + 10);
-	void *cubtmp = ctx->scratch[S_CUB].p;
 	const RecState Y{{ctx->d_ygrec, ctx->d_ygrecHe1, ctx->d_ygrecHe2}};
-	PSG_CUDA(cudaMemsetAsync(keys, 0xff, sizeof(unsigned long long) * ktot, st));
 	PSG_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned) * 4, st));
-	for (int s = 0; s < nspec; s++) {
-		size_t tmp = ctx->rec_tmp[0];
-		if (!threshold_mode) {
-			double *w = (double *)wm, *cdf = w + n;
-			uint32_t *leaf_of = (uint32_t *)(cdf + n);
+	if (!threshold_mode) {
+		PSG_CUDA(cudaMemsetAsync(items, 0xff, sizeof(RecItem) * ktot, st));
+		for (int s = 0; s < nspec; s++) {
 			k_rec_weight<<<nblocks(n, 256), 256, 0, st>>>(n, B, ctx->d_srcmark, Y.yg[s], ctx->d_lambdaH,
-					ctx->d_order, w, leaf_of);
+					ctx->d_order, W.w, W.leaf_of);
 			PSG_CHECK_LAUNCH();
-			PSG_CUDA(cub::DeviceScan::InclusiveSum(cubtmp, tmp, w, cdf, (int64_t)n, st));
+			// cumulative weights: cdf[i] = ex[i + 1]
+			PSG_CUDA(scan_enqueue(st, W.w, n, W.ex, W.tiles_d, AsDouble()));
 			// streams: 4 the HII emitters, 7 and 8 those of HeII and HeIII
-			k_rec_draw<<<nblocks(kmax, 128), 128, 0, st>>>(n, (int)kmax, s, s == 0 ? 4u : 6u + (uint32_t)s, cdf,
-					B, ctx->rec_seed, leaf_of, keys + s * kmax, vals + s * kmax, d_count);
+			k_rec_draw<<<nblocks(kmax, 128), 128, 0, st>>>(n, (int)kmax, s, s == 0 ? 4u : 6u + (uint32_t)s, W.ex + 1,
+					B, ctx->rec_seed, W.leaf_of, items + s * kmax, d_count);
 			PSG_CHECK_LAUNCH();
-		} else {
-			uint32_t *flag = (uint32_t *)wm, *pos = flag + n;
-			k_rec_flag<<<nblocks(n, 256), 256, 0, st>>>(n, B, ctx->d_srcmark, Y.yg[s], ctx->rec_threshold, flag);
-			PSG_CHECK_LAUNCH();
-			PSG_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, tmp, flag, pos, (int64_t)n, st));
-			k_rec_compact<<<nblocks(n, 256), 256, 0, st>>>(n, s, flag, pos, ctx->d_order, keys + s * kmax,
-					vals + s * kmax, d_count);
-			PSG_CHECK_LAUNCH();
+			ctx->launches += 5;
 		}
-		ctx->launches += 3;
+		RecItem pad;
+		memset(&pad, 0xff, sizeof(pad));
+		PSG_CUDA(dsort_enqueue(st, items, items + ktot, ktot, pad, RecItemLess()));
+		ctx->launches += 1 + dsort_passes(ktot);
+	} else {
+		for (int s = 0; s < nspec; s++) {
+			k_rec_flag<<<nblocks(n, 256), 256, 0, st>>>(n, B, ctx->d_srcmark, Y.yg[s], ctx->rec_threshold,
+					ctx->d_order, W.flag + (size_t)s * n, W.leaf_of);
+			PSG_CHECK_LAUNCH();
+			ctx->launches++;
+		}
+		PSG_CUDA(scan_enqueue(st, W.flag, n * nspec, W.pos, W.tiles_u, Widen()));
+		k_rec_place<<<nblocks(n * nspec, 256), 256, 0, st>>>(n, nspec, W.flag, W.pos, W.leaf_of, items, d_count);
+		PSG_CHECK_LAUNCH();
+		ctx->launches += 4;
 	}
-	{
-		size_t tmp = ctx->rec_tmp[1];
-		PSG_CUDA(cub::DeviceRadixSort::SortPairs(cubtmp, tmp, keys, keys + ktot, vals, vals + ktot, (int64_t)ktot, 0,
-				64, st));
-	}
+	const RecItem *sorted = rec_sorted(ctx, ktot, threshold_mode);
 	LteView L;
 	L.cdf = ctx->d_lte;
 	for (int s = 0; s < 3; s++) {
@@ -319,10 +364,10 @@ int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out) {
 	}
 	L.disabled = ctx->rec_disable_lte;
 	const double length = ctx->boxsize * 2.0 * 0.1;     // MAX_REC_RAY_LENGTH, loop.c:169
-	k_rec_rays<<<nblocks(ktot, 128), 128, 0, st>>>(d_count, keys + ktot, vals + ktot, B, ctx->rec_seed, ctx->d_psml,
-			ctx->d_mass, Y, ctx->d_lambdaH, ctx->d_ie, P, L, length, out, d_nph);
+	k_rec_rays<<<nblocks(ktot, 128), 128, 0, st>>>(d_count, sorted, B, ctx->rec_seed, ctx->d_psml, ctx->d_mass, Y,
+			ctx->d_lambdaH, ctx->d_ie, P, L, length, out, d_nph);
 	PSG_CHECK_LAUNCH();
-	k_rec_purge<<<nblocks(ktot, 128), 128, 0, st>>>(d_count, keys + ktot, vals + ktot, out, ctx->d_mass, Y, P);
+	k_rec_purge<<<nblocks(ktot, 128), 128, 0, st>>>(d_count, sorted, out, ctx->d_mass, Y, P);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 2;
 	return PSG_OK;
@@ -420,6 +465,7 @@ int psg_run_ticks_rec(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t 
 		ctx->rec_last = M;
 		ctx->rec_last_R = R;
 		ctx->rec_last_kmax = cap;
+		ctx->rec_last_threshold = ctx->rec_nrec < 0;
 		rec_rays += (double)M;
 		int rc = psg_run_ticks_core(ctx, buf, R + M, 1, tick, tick_time, &one);
 		if (rc) return rc;
@@ -478,14 +524,14 @@ extern "C" int psg_get_rec_rays(psg_context *ctx, psg_ray *rays, int64_t *ipar, 
 	if (rays)
 		PSG_CUDA(cudaMemcpyAsync(rays, (psg_ray *)ctx->scratch[S_RECRAYS].p + ctx->rec_last_R, sizeof(psg_ray) * M,
 				cudaMemcpyDeviceToHost, ctx->stream));
-	std::vector<unsigned long long> keys(M);
+	std::vector<RecItem> items(M);
 	if (ipar || type)
-		PSG_CUDA(cudaMemcpyAsync(keys.data(), (unsigned long long *)ctx->scratch[S_RECK].p + kmax,
-				sizeof(unsigned long long) * M, cudaMemcpyDeviceToHost, ctx->stream));
+		PSG_CUDA(cudaMemcpyAsync(items.data(), rec_sorted(ctx, kmax, ctx->rec_last_threshold), sizeof(RecItem) * M,
+				cudaMemcpyDeviceToHost, ctx->stream));
 	PSG_CUDA(cudaStreamSynchronize(ctx->stream));
 	for (size_t i = 0; i < M; i++) {
-		if (ipar) ipar[i] = (int64_t)((keys[i] >> 24) & 0xFFFFFFFFull);
-		if (type) type[i] = (int32_t)(keys[i] >> 56);
+		if (ipar) ipar[i] = (int64_t)((items[i].key >> 24) & 0xFFFFFFFFull);
+		if (type) type[i] = (int32_t)(items[i].key >> 56);
 	}
 	return PSG_OK;
 }

@@ -1,5 +1,6 @@
 // Exclusive scans of 64-bit sums over device arrays, used by the traversal
-// (hit counts) and the tick batches (slots, ray and particle classes); no
+// (hit counts), the tick batches (slots, ray and particle classes) and the
+// recombination emission (cumulative weights in FP64, emitter flags); no
 // library device-wide scan on the per-step path.
 #pragma once
 
@@ -13,8 +14,9 @@ namespace {
 // traversal's hit counts, the ray and particle classes) in three passes:
 // tile sums, one block scanning the tile sums, each tile's own scan plus
 // its offset. Tiles of 256 threads x 16 items; the element type of the
-// input is mapped to a 64-bit value by Op; out has n + 1 entries (the total
-// last).
+// input is mapped to the sum's type V (unsigned 64-bit or double) by Op; out
+// has n + 1 entries (the total last). The order of the additions is fixed
+// by n alone, so a floating-point scan gives the same bits every run.
 #define SCAN_T 256
 #define SCAN_I 16
 struct SlotPair {        // a key's count c: c | (c > 0) << 32 (slots below, active pairs below)
@@ -26,13 +28,16 @@ struct Widen {
 	template <typename T>
 	__device__ __forceinline__ unsigned long long operator()(T c) const { return (unsigned long long)c; }
 };
-template <typename T, typename Op>
+struct AsDouble {
+	__device__ __forceinline__ double operator()(double x) const { return x; }
+};
+template <typename T, typename Op, typename V>
 __global__ void __launch_bounds__(SCAN_T) k_scan_tiles(const T *__restrict__ in, size_t n,
-		unsigned long long *__restrict__ tile_sum, Op op) {
-	using BR = cub::BlockReduce<unsigned long long, SCAN_T>;
+		V *__restrict__ tile_sum, Op op) {
+	using BR = cub::BlockReduce<V, SCAN_T>;
 	__shared__ typename BR::TempStorage tmp;
 	const size_t t0 = (size_t)blockIdx.x * SCAN_T * SCAN_I;
-	unsigned long long s = 0;
+	V s = 0;
 #pragma unroll
 	for (int u = 0; u < SCAN_I; u++) {
 		const size_t k = t0 + (size_t)u * SCAN_T + threadIdx.x;
@@ -42,16 +47,17 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_tiles(const T *__restrict__ in,
 	if (threadIdx.x == 0) tile_sum[blockIdx.x] = s;
 }
 // one block: exclusive scan of the tile sums in place; the total after them
-__global__ void __launch_bounds__(1024) k_scan_sums(unsigned long long *__restrict__ tile_sum, size_t ntile) {
-	using BS = cub::BlockScan<unsigned long long, 1024>;
+template <typename V>
+__global__ void __launch_bounds__(1024) k_scan_sums(V *__restrict__ tile_sum, size_t ntile) {
+	using BS = cub::BlockScan<V, 1024>;
 	__shared__ typename BS::TempStorage tmp;
-	__shared__ unsigned long long carry;
+	__shared__ V carry;
 	if (threadIdx.x == 0) carry = 0;
 	__syncthreads();
 	for (size_t b = 0; b < ntile; b += 1024) {
 		const size_t i = b + threadIdx.x;
-		const unsigned long long v = i < ntile ? tile_sum[i] : 0ull;
-		unsigned long long x, agg;
+		const V v = i < ntile ? tile_sum[i] : (V)0;
+		V x, agg;
 		BS(tmp).ExclusiveSum(v, x, agg);
 		if (i < ntile) tile_sum[i] = x + carry;
 		__syncthreads();
@@ -60,22 +66,22 @@ __global__ void __launch_bounds__(1024) k_scan_sums(unsigned long long *__restri
 	}
 	if (threadIdx.x == 0) tile_sum[ntile] = carry;
 }
-template <typename T, typename Op>
+template <typename T, typename Op, typename V>
 __global__ void __launch_bounds__(SCAN_T) k_scan_apply(const T *__restrict__ in, size_t n,
-		const unsigned long long *__restrict__ tile_sum, unsigned long long *__restrict__ out, Op op) {
-	using BS = cub::BlockScan<unsigned long long, SCAN_T>;
+		const V *__restrict__ tile_sum, V *__restrict__ out, Op op) {
+	using BS = cub::BlockScan<V, SCAN_T>;
 	__shared__ typename BS::TempStorage tmp;
 	const size_t t0 = (size_t)blockIdx.x * SCAN_T * SCAN_I;
 	// blocked layout: thread i holds items t0 + i*16 .. +15
-	unsigned long long v[SCAN_I];
-	unsigned long long s = 0;
+	V v[SCAN_I];
+	V s = 0;
 #pragma unroll
 	for (int u = 0; u < SCAN_I; u++) {
 		const size_t k = t0 + (size_t)threadIdx.x * SCAN_I + u;
-		v[u] = k < n ? op(in[k]) : 0ull;
+		v[u] = k < n ? op(in[k]) : (V)0;
 		s += v[u];
 	}
-	unsigned long long x;
+	V x;
 	BS(tmp).ExclusiveSum(s, x);
 	x += tile_sum[blockIdx.x];
 #pragma unroll
@@ -93,13 +99,12 @@ inline size_t scan_tiles(size_t n) {
 	const size_t t = (n + (size_t)SCAN_T * SCAN_I - 1) / ((size_t)SCAN_T * SCAN_I);
 	return t ? t : 1;
 }
-template <typename T, typename Op>
-cudaError_t scan_enqueue(cudaStream_t st, const T *in, size_t n, unsigned long long *out,
-		unsigned long long *tiles, Op op) {
+template <typename T, typename Op, typename V>
+cudaError_t scan_enqueue(cudaStream_t st, const T *in, size_t n, V *out, V *tiles, Op op) {
 	const size_t nt = scan_tiles(n);
-	k_scan_tiles<T, Op><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, op);
-	k_scan_sums<<<1, 1024, 0, st>>>(tiles, nt);
-	k_scan_apply<T, Op><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, out, op);
+	k_scan_tiles<T, Op, V><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, op);
+	k_scan_sums<V><<<1, 1024, 0, st>>>(tiles, nt);
+	k_scan_apply<T, Op, V><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, out, op);
 	return cudaGetLastError();
 }
 

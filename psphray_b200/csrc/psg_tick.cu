@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "psg_internal.cuh"
+#include "psg_bsort.cuh"
 #include "psg_scan.cuh"
 #include "psg_helium.cuh"
 #include "psg_solve.cuh"
@@ -173,19 +174,35 @@ __global__ void k_slot_canon(const int32_t *__restrict__ tick_act, int K, const 
 }
 
 // Runs longer than 32 (particles next to a source), a block each: bitonic
-// sort in shared memory (runs up to SLOT_LONG_MAX hits: at most a tick's
-// rays; a longer run raises PSG_ST_SLOT).
+// sort in shared memory, runs up to cap_pow2 hits (the tick's rays rounded
+// up to a power of two, at most SLOT_LONG_MAX). A longer run (more than
+// SLOT_LONG_MAX rays of one tick on one particle) is merge-sorted in global
+// memory with the upper half of vals (from half) as scratch.
 #define SLOT_LONG_MAX 32768
+struct U32Less {
+	__device__ __forceinline__ bool operator()(uint32_t x, uint32_t y) const { return x < y; }
+};
 __global__ void __launch_bounds__(1024) k_slot_canon_long(const int32_t *__restrict__ tick_long, int K,
 		const uint32_t *__restrict__ long_act, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals,
-		uint32_t *__restrict__ slot, int cap_pow2, uint32_t *__restrict__ status) {
+		uint32_t *__restrict__ slot, int cap_pow2, size_t half, uint32_t *__restrict__ status) {
 	extern __shared__ uint32_t sv[];
 	const int ne = tick_long[K];
 	for (int e = blockIdx.x; e < ne; e += gridDim.x) {
 		const uint32_t a = long_act[e];
 		const uint32_t s0 = act_seg[a], n = act_seg[a + 1] - s0;
 		if ((int)n > cap_pow2) {
-			if (threadIdx.x == 0) atomicOr(status, PSG_ST_SLOT);
+			if (cap_pow2 < 2048) {      // (the tile below needs 2048 entries; n <= the tick's rays)
+				if (threadIdx.x == 0) atomicOr(status, PSG_ST_SLOT);
+				continue;
+			}
+			const uint32_t *f = block_sort_global<1024>(vals + s0, vals + half + s0, (int64_t)n, sv, 0xFFFFFFFFu,
+					U32Less());
+			for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+				const uint32_t v = f[i];
+				vals[s0 + i] = v;
+				slot[v] = s0 + i;
+			}
+			__syncthreads();
 			continue;
 		}
 		int P = 1;
@@ -1794,7 +1811,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	// the slot order of the long runs (the short ones are in order already)
 	psg_mark_begin(ctx, PSG_K_SLOTS);
 	k_slot_canon_long<<<(unsigned)(2 * sms), 1024, sizeof(uint32_t) * pl.long_cap, st>>>(tick_long, (int)K, long_act,
-			av.act_seg, vals, slot, pl.long_cap, ctx->d_status);
+			av.act_seg, vals, slot, pl.long_cap, cap, ctx->d_status);
 	PSG_CHECK_LAUNCH();
 	psg_mark_end(ctx);
 	ctx->launches += 6;
@@ -2075,9 +2092,8 @@ int psg_run_ticks_core(psg_context *ctx, const psg_ray *d_rays, size_t R, size_t
 	ctx->launches++;
 	PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 1, 0, 2 * sizeof(unsigned long long), st));
 	PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 6, 0, sizeof(unsigned long long), st));
-	// per-launch timing needs the launches issued one by one; so does the
-	// library segmented sort of very long hit lists (its size is the hits')
-	const bool graph = ctx->use_graphs && !ctx->timing && pl.maxcount <= PSG_SORT_MAX;
+	// per-launch timing needs the launches issued one by one
+	const bool graph = ctx->use_graphs && !ctx->timing;
 	rc = graph ? launch_graph(ctx, batch_key(ctx, pl, ctx->d_batch), [&] { return enqueue_any(ctx, pl, ctx->d_batch); })
 			: enqueue_any(ctx, pl, ctx->d_batch);
 	if (rc) return rc;
@@ -2146,7 +2162,7 @@ int psg_run_ticks_rec_graph(psg_context *ctx, const psg_ray *d_rays, size_t R, s
 	const size_t nray = R + cap_rec;
 	// the slabs and hit buffers as an earlier call left them: the first call
 	// runs its ticks one by one, which sizes them
-	if (ctx->rec_nrec <= 0 || !ctx->slab_cap || ctx->slab_cap > PSG_SORT_MAX || !ctx->batch_cap ||
+	if (ctx->rec_nrec <= 0 || !ctx->slab_cap || !ctx->batch_cap ||
 			nray >= (size_t)INT32_MAX)
 		return PSG_RETRY;
 	PSG_CUDA(cudaSetDevice(ctx->device));
@@ -2238,6 +2254,7 @@ int psg_run_ticks_rec_graph(psg_context *ctx, const psg_ray *d_rays, size_t R, s
 	ctx->rec_last = (size_t)last[0] + last[1] + last[2];
 	ctx->rec_last_R = R;
 	ctx->rec_last_kmax = cap_rec;
+	ctx->rec_last_threshold = ctx->rec_nrec < 0;
 	ctx->sat_frac = c[7] ? (double)c[1] / (double)c[7] : 0.0;
 	if (stats) {
 		memset(stats, 0, sizeof(*stats));

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "psg_internal.cuh"
+#include "psg_bsort.cuh"
 #include "psg_scan.cuh"
 #include "psg_solve.cuh"
 
@@ -235,76 +236,28 @@ __global__ void __launch_bounds__(32 * TR_MAX_WARPS) k_trace_stack(const psg_ray
 	}
 }
 
-// Slabs into contiguous per-ray lists (traversal order), for the library
-// sort taken when a ray is longer than the shared-memory sort.
-__global__ void k_compact_slabs(size_t nray, size_t scap, const int64_t *__restrict__ off,
-		const uint32_t *__restrict__ slab_ipar, const double *__restrict__ slab_d, const double *__restrict__ slab_b,
-		uint32_t *__restrict__ ipar, double *__restrict__ d, double *__restrict__ b) {
-	const size_t r = blockIdx.x;
-	const int64_t h0 = off[r];
-	const int n = (int)(off[r + 1] - h0);
-	for (int i = threadIdx.x; i < n; i += blockDim.x) {
-		ipar[h0 + i] = slab_ipar[r * scap + i];
-		d[h0 + i] = slab_d[r * scap + i];
-		b[h0 + i] = slab_b[r * scap + i];
-	}
-}
-
 // With cap (a call without host reads), a total above the hit buffers'
 // capacity empties every list instead (nothing downstream reads past cap)
 // and flags the status word for the host to redo the call; the call's
 // largest total is kept in *tickmax.
-__global__ void k_offsets64(const unsigned long long *__restrict__ scan32, const uint32_t *__restrict__ count,
-		size_t nray, int64_t *__restrict__ off64, int32_t *__restrict__ off32,
+__global__ void k_offsets64(const unsigned long long *__restrict__ scan, const uint32_t *__restrict__ count,
+		size_t nray, int64_t *__restrict__ off64,
 		unsigned long long *__restrict__ maxcount, size_t cap, unsigned long long *__restrict__ tickmax,
 		uint32_t *__restrict__ status) {
 	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (r > nray) return;
-	// scan32 holds the exclusive scan over nray+1 entries (count[nray] = 0)
-	const bool over = cap && (size_t)scan32[nray] > cap;
-	off64[r] = over ? 0 : scan32[r];
-	off32[r] = over ? 0 : (int32_t)scan32[r];
+	// scan holds the exclusive scan over nray+1 entries (count[nray] = 0)
+	const bool over = cap && (size_t)scan[nray] > cap;
+	off64[r] = over ? 0 : scan[r];
 	if (r < nray) {
 		atomicMax(maxcount, (unsigned long long)count[r]);
 	} else {
-		maxcount[1] = scan32[r];       // the hit total, read with the longest list
+		maxcount[1] = scan[r];       // the hit total, read with the longest list
 		if (cap) {
-			atomicMax(tickmax, (unsigned long long)scan32[r]);
+			atomicMax(tickmax, (unsigned long long)scan[r]);
 			if (over) atomicOr(status, PSG_ST_SLAB);
 		}
 	}
-}
-
-__global__ void k_sort_keys(size_t nhit, const double *__restrict__ d, unsigned long long *__restrict__ keys,
-		uint32_t *__restrict__ vals) {
-	const size_t h = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (h >= nhit) return;
-	keys[h] = (unsigned long long)__double_as_longlong(d[h]);   // d >= 0: bit order is value order
-	vals[h] = (uint32_t)h;
-}
-
-__global__ void k_gather_sorted(size_t nhit, const uint32_t *__restrict__ perm,
-		const uint32_t *__restrict__ raw_ipar, const double *__restrict__ raw_d,
-		const double *__restrict__ raw_b, uint32_t *__restrict__ ipar, double *__restrict__ d,
-		double *__restrict__ b) {
-	const size_t h = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (h >= nhit) return;
-	const uint32_t j = perm[h];
-	ipar[h] = raw_ipar[j];
-	d[h] = raw_d[j];
-	b[h] = raw_b[j];
-}
-
-// Column-density factor of each hit, kernel = sph_depth(b/h) / h^2
-// (loop.c:429-445); b is overwritten.
-__global__ void k_hit_kernel(size_t nhit, const uint32_t *__restrict__ ipar, const float4 *__restrict__ psml,
-		double *__restrict__ b_to_kern, PhysParams P) {
-	const size_t h = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (h >= nhit) return;
-	const double sml = (double)psml[ipar[h]].w;
-	const double sml_inv = __ddiv_rn(1.0, sml);
-	const double r_h = rn_dmul(b_to_kern[h], sml_inv);
-	b_to_kern[h] = rn_dmul(sph_depth(P, r_h), rn_dmul(sml_inv, sml_inv));
 }
 
 // The caller's index of internal particle i (order: null when the arrays
@@ -313,22 +266,23 @@ __device__ __forceinline__ uint32_t caller_index(const uint32_t *__restrict__ or
 	return order ? order[i] : i;
 }
 
-// Runs of equal d inside a ray are put in the caller's ipar order (the
-// reference leaves their order to qsort); insertion sort, runs are almost
-// always length 1.
-__global__ void k_break_ties(size_t nray, const int64_t *__restrict__ off, uint32_t *__restrict__ ipar,
-		double *__restrict__ d, double *__restrict__ b, const uint32_t *__restrict__ order) {
-	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-	if (r >= nray) return;
-	const int64_t h0 = off[r], h1 = off[r + 1];
-	for (int64_t h = h0 + 1; h < h1; h++) {
-		if (d[h] != d[h - 1]) continue;
-		int64_t k = h;
-		while (k > h0 && d[k - 1] == d[k] && caller_index(order, ipar[k - 1]) > caller_index(order, ipar[k])) {
-			const uint32_t ti = ipar[k]; ipar[k] = ipar[k - 1]; ipar[k - 1] = ti;
-			const double tb = b[k]; b[k] = b[k - 1]; b[k - 1] = tb;
-			k--;
-		}
+// The hit at slab position p of a ray as the sorted list's entry h; with
+// want_kern its b becomes the column-density factor sph_depth(b/h)/h^2
+// (loop.c:429-445).
+__device__ __forceinline__ void put_sorted_hit(int64_t h, uint32_t p, const uint32_t *__restrict__ raw_ipar,
+		const double *__restrict__ raw_d, const double *__restrict__ raw_b, uint32_t *__restrict__ out_ipar,
+		double *__restrict__ out_d, double *__restrict__ out_b, int want_kern, const float4 *__restrict__ psml,
+		const PhysParams &P) {
+	const uint32_t ip = raw_ipar[p];
+	const double b = raw_b[p];
+	out_ipar[h] = ip;
+	out_d[h] = raw_d[p];
+	if (want_kern) {
+		const double sml = (double)psml[ip].w;
+		const double inv = __ddiv_rn(1.0, sml);
+		out_b[h] = rn_dmul(sph_depth(P, rn_dmul(b, inv)), rn_dmul(inv, inv));
+	} else {
+		out_b[h] = b;
 	}
 }
 
@@ -432,20 +386,8 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 		}
 	}
 	__syncthreads();
-	for (int i = threadIdx.x; i < n; i += TPR) {
-		const uint32_t p = sm.pos[i];
-		const uint32_t ip = raw_ipar[p];
-		const double b = raw_b[p];
-		out_ipar[h0 + i] = ip;
-		out_d[h0 + i] = raw_d[p];
-		if (want_kern) {
-			const double sml = (double)psml[ip].w;
-			const double inv = __ddiv_rn(1.0, sml);
-			out_b[h0 + i] = rn_dmul(sph_depth(P, rn_dmul(b, inv)), rn_dmul(inv, inv));
-		} else {
-			out_b[h0 + i] = b;
-		}
-	}
+	for (int i = threadIdx.x; i < n; i += TPR)
+		put_sorted_hit(h0 + i, sm.pos[i], raw_ipar, raw_d, raw_b, out_ipar, out_d, out_b, want_kern, psml, P);
 	__syncthreads();     // shared memory is reused by the next ray
 	}
 }
@@ -456,6 +398,46 @@ size_t sort_smem_bytes() {
 			16 * (TPR / 32) + 128;
 }
 
+// Rays with more hits than the largest class (PSG_SORT_MAX), a block of
+// LONG_NT threads each, persistent over their list: the hits as (d, caller
+// index << 32 | slab position) pairs in tmp (the two halves, at the ray's
+// list offset), sorted by block_sort_global on exactly the order of the
+// class sorts -- d, then the caller's index.
+#define LONG_NT 1024
+struct LongHit {
+	double d;
+	unsigned long long ck;
+};
+struct LongHitLess {
+	__device__ __forceinline__ bool operator()(const LongHit &x, const LongHit &y) const {
+		return x.d < y.d || (x.d == y.d && x.ck < y.ck);
+	}
+};
+__global__ void __launch_bounds__(LONG_NT) k_sort_long(const uint32_t *__restrict__ list,
+		const unsigned long long *__restrict__ d_nlist, const int64_t *__restrict__ off, size_t scap,
+		const uint32_t *__restrict__ slab_ipar, const double *__restrict__ slab_d, const double *__restrict__ slab_b,
+		uint32_t *__restrict__ out_ipar, double *__restrict__ out_d, double *__restrict__ out_b, int want_kern,
+		const float4 *__restrict__ psml, PhysParams P, const uint32_t *__restrict__ order, LongHit *tmp, size_t hb) {
+	__shared__ LongHit tile[2 * LONG_NT];
+	const LongHit pad{__longlong_as_double(0x7ff0000000000000ll), ~0ull};
+	const unsigned long long nlist = *d_nlist;
+	for (unsigned long long li = blockIdx.x; li < nlist; li += gridDim.x) {
+		const size_t r = list[li];
+		const int64_t h0 = off[r];
+		const int64_t n = off[r + 1] - h0;
+		const uint32_t *raw_ipar = slab_ipar + r * scap;
+		const double *raw_d = slab_d + r * scap, *raw_b = slab_b + r * scap;
+		LongHit *a = tmp + h0;
+		for (int64_t i = threadIdx.x; i < n; i += LONG_NT)
+			a[i] = LongHit{raw_d[i], (unsigned long long)caller_index(order, raw_ipar[i]) << 32 | (unsigned long long)i};
+		const LongHit *f = block_sort_global<LONG_NT>(a, tmp + hb + h0, n, tile, pad, LongHitLess());
+		for (int64_t i = threadIdx.x; i < n; i += LONG_NT)
+			put_sorted_hit(h0 + i, (uint32_t)f[i].ck, raw_ipar, raw_d, raw_b, out_ipar, out_d, out_b, want_kern,
+					psml, P);
+		__syncthreads();
+	}
+}
+
 // Size classes of the ray sort: class c holds rays with at most
 // kSortClassMax[c] hits (and more than the previous class's bound).
 // size classes of the per-ray sort (threads x items per thread):
@@ -464,11 +446,16 @@ size_t sort_smem_bytes() {
 __constant__ int kSortBounds[SORT_NCLS] = {64, 128, 256, 512, 1024, 2048, 4096, PSG_SORT_MAX};
 
 __global__ void k_sort_classify(size_t nray, const int64_t *__restrict__ off, uint32_t *__restrict__ lists,
-		size_t stride, unsigned long long *__restrict__ nclass) {
+		size_t stride, unsigned long long *__restrict__ nclass, unsigned long long *__restrict__ nlong) {
 	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (r >= nray) return;
 	const int64_t n = off[r + 1] - off[r];
 	if (n == 0) return;
+	if (n > PSG_SORT_MAX) {      // the long list, after the classes'
+		const unsigned long long k = atomicAdd(nlong, 1ull);
+		lists[SORT_NCLS * stride + k] = (uint32_t)r;
+		return;
+	}
 	int c = 0;
 	while (c < SORT_NCLS - 1 && n > kSortBounds[c]) c++;
 	const unsigned long long k = atomicAdd(&nclass[c], 1ull);
@@ -512,7 +499,6 @@ int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray,
 	uint32_t *count = (uint32_t *)ctx->scratch[S_COUNT].p;
 	unsigned long long *scan = count_scan(count, nray);
 	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
-	int32_t *off32 = (int32_t *)((char *)ctx->scratch[S_OFFSETS].p + sizeof(int64_t) * (nray + 1));
 	unsigned long long *d_max = ctx->d_counters + 4;
 	unsigned long long *next_ray = ctx->d_counters + 9;
 	const size_t scap = ctx->slab_cap;
@@ -531,7 +517,7 @@ int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray,
 	k_count_clamp<<<blocks(nray, 256), 256, 0, st>>>(nray, scap, count, ctx->d_counters + 3, ctx->d_status);
 	PSG_CHECK_LAUNCH();
 	PSG_CUDA(scan_enqueue(st, count, nray + 1, scan, (unsigned long long *)ctx->scratch[S_SCAN].p, Widen()));
-	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32, d_max, cap,
+	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, d_max, cap,
 			ctx->d_counters + 24, ctx->d_status);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 3;
@@ -545,7 +531,7 @@ int psg_trace_fill_prepare(psg_context *ctx, size_t nray) {
 	const size_t slots = nray * scap;
 	if (!psg_scratch(ctx, S_COUNT, count_bytes(nray)) ||
 			!psg_scratch(ctx, S_SCAN, sizeof(unsigned long long) * (scan_tiles(nray + 1) + 1)) ||
-			!psg_scratch(ctx, S_OFFSETS, (sizeof(int64_t) + sizeof(int32_t)) * (nray + 1) + 256) ||
+			!psg_scratch(ctx, S_OFFSETS, sizeof(int64_t) * (nray + 1) + 256) ||
 			!psg_scratch(ctx, S_REC_U32, sizeof(uint32_t) * (slots ? slots : 1)) ||
 			!psg_scratch(ctx, S_REC_F64, sizeof(double) * 2 * (slots ? slots : 1)))
 		return PSG_E_NOMEM;
@@ -560,21 +546,19 @@ int psg_trace_fill_prepare(psg_context *ctx, size_t nray) {
 }
 
 // The traversal of nray device-resident rays into per-ray slabs, the hit
-// counts' scan and the offsets (S_OFFSETS: int64 offsets[nray+1], then
-// int32 offsets[nray+1]). One host synchronisation reads the longest list,
+// counts' scan and the offsets (S_OFFSETS: int64 offsets[nray+1]). One host synchronisation reads the longest list,
 // the status word and the hit total; a ray that outgrew its slab grows the
 // slabs and reruns the traversal once.
 int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTraceFill *tf) {
 	if (!ctx->have_tree) return psg_fail(ctx, PSG_E_INVAL, "trace: no tree (psg_build_tree first)");
 	cudaStream_t st = ctx->stream;
 	uint32_t *count = (uint32_t *)psg_scratch(ctx, S_COUNT, count_bytes(nray));
-	char *offmem = (char *)psg_scratch(ctx, S_OFFSETS, (sizeof(int64_t) + sizeof(int32_t)) * (nray + 1) + 256);
+	char *offmem = (char *)psg_scratch(ctx, S_OFFSETS, sizeof(int64_t) * (nray + 1) + 256);
 	unsigned long long *tiles = (unsigned long long *)psg_scratch(ctx, S_SCAN,
 			sizeof(unsigned long long) * (scan_tiles(nray + 1) + 1));
 	if (!count || !offmem || !tiles) return PSG_E_NOMEM;
 	unsigned long long *scan = count_scan(count, nray);
 	int64_t *off64 = (int64_t *)offmem;
-	int32_t *off32 = (int32_t *)(offmem + sizeof(int64_t) * (nray + 1));
 	unsigned long long *d_max = ctx->d_counters + 4;
 	unsigned long long *next_ray = ctx->d_counters + 9;
 	const int sms = ctx->sms;
@@ -607,7 +591,7 @@ int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTrac
 		PSG_CHECK_LAUNCH();
 		psg_mark_end(ctx);
 		PSG_CUDA(scan_enqueue(st, count, nray + 1, scan, tiles, Widen()));
-		k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, off32, d_max, 0, nullptr,
+		k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, d_max, 0, nullptr,
 				nullptr);
 		PSG_CHECK_LAUNCH();
 		ctx->launches++;
@@ -643,16 +627,11 @@ int psg_trace_sort_prepare(psg_context *ctx, size_t nray, size_t cap, unsigned l
 	uint32_t *hit_ipar = (uint32_t *)psg_scratch(ctx, S_HIT_IPAR, sizeof(uint32_t) * hb);
 	double *hit_db = (double *)psg_scratch(ctx, S_RAW_D, sizeof(double) * 2 * hb);
 	double *hit_b = (double *)psg_scratch(ctx, S_HIT_KERN, sizeof(double) * hb);
-	uint32_t *lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * SORT_NCLS * (nray + 1));
+	uint32_t *lists = (uint32_t *)psg_scratch(ctx, S_RAYLIST, sizeof(uint32_t) * (SORT_NCLS + 1) * (nray + 1));
 	if (!hit_ipar || !hit_db || !hit_b || !lists) return PSG_E_NOMEM;
 	ctx->hit_cap = hb;
-	if (maxcount > PSG_SORT_MAX) {
-		uint32_t *raw_ipar = (uint32_t *)psg_scratch(ctx, S_RAW_IPAR, sizeof(uint32_t) * hb);
-		double *raw_db = (double *)psg_scratch(ctx, S_RAW_B, sizeof(double) * 2 * hb);
-		unsigned long long *keys = (unsigned long long *)psg_scratch(ctx, S_KEYS, sizeof(unsigned long long) * 2 * hb);
-		uint32_t *vals = (uint32_t *)psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * hb);
-		if (!raw_ipar || !raw_db || !keys || !vals) return PSG_E_NOMEM;
-	}
+	// the long rays' two halves of (d, key) pairs, at their list offsets
+	if (maxcount > PSG_SORT_MAX && !psg_scratch(ctx, S_KEYS, sizeof(LongHit) * 2 * hb)) return PSG_E_NOMEM;
 	// shared-memory limits and resident blocks per multiprocessor of the
 	// eight class kernels (their persistent grids), once per context
 	if (!ctx->sort_grid[0]) {
@@ -675,18 +654,17 @@ int psg_trace_sort_prepare(psg_context *ctx, size_t nray, size_t cap, unsigned l
 }
 
 // The per-ray sort by (d, ipar) of the filled slabs into the CSR lists.
-// With every list at most PSG_SORT_MAX long it issues only launches whose
-// sizes are fixed by nray (persistent class kernels read their ray counts on
-// the device), so it can be captured in a graph; a longer list takes the
-// library segmented sort, sized by nhit.
+// Launch sizes are fixed by nray (the persistent class kernels read their
+// ray counts on the device), so it can be captured in a graph; with
+// maxcount above PSG_SORT_MAX the long rays' kernel runs too.
 int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned long long maxcount,
 		int want_kern) {
+	(void)nhit;
 	cudaStream_t st = ctx->stream;
 	const size_t hb = ctx->hit_cap;
 	const size_t scap = ctx->slab_cap;
 	const size_t slots = nray * scap;
 	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
-	int32_t *off32 = (int32_t *)((char *)ctx->scratch[S_OFFSETS].p + sizeof(int64_t) * (nray + 1));
 	uint32_t *hit_ipar = (uint32_t *)ctx->scratch[S_HIT_IPAR].p;
 	double *hit_d = (double *)ctx->scratch[S_RAW_D].p + hb;
 	double *hit_b = (double *)ctx->scratch[S_HIT_KERN].p;
@@ -695,11 +673,12 @@ int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned 
 	double *slab_b = slab_d + slots;
 	if (nray == 0) return PSG_OK;
 	psg_mark_begin(ctx, PSG_K_SORT);
-	if (maxcount <= PSG_SORT_MAX) {
+	{
 		uint32_t *lists = (uint32_t *)ctx->scratch[S_RAYLIST].p;
-		unsigned long long *d_ncls = ctx->d_counters + 16;
+		unsigned long long *d_ncls = ctx->d_counters + 16, *d_nlong = ctx->d_counters + 25;
 		PSG_CUDA(cudaMemsetAsync(d_ncls, 0, SORT_NCLS * sizeof(unsigned long long), st));
-		k_sort_classify<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, lists, nray + 1, d_ncls);
+		PSG_CUDA(cudaMemsetAsync(d_nlong, 0, sizeof(unsigned long long), st));
+		k_sort_classify<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, lists, nray + 1, d_ncls, d_nlong);
 		PSG_CHECK_LAUNCH();
 		const PhysParams PP = psg_phys_params(ctx);
 		const size_t stride = nray + 1;
@@ -721,34 +700,12 @@ int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned 
 		if (!rcs) rcs = launch_block(k_sort_block<512, 16>, 512, sort_smem_bytes<512, 16>(), 7);
 		if (rcs) return rcs;
 		ctx->launches++;
-	} else if (nhit) {
-		// a ray longer than the shared-memory sort takes: library segmented sort
-		uint32_t *raw_ipar = (uint32_t *)ctx->scratch[S_RAW_IPAR].p;
-		double *raw_db = (double *)ctx->scratch[S_RAW_B].p;
-		unsigned long long *keys = (unsigned long long *)ctx->scratch[S_KEYS].p;
-		uint32_t *vals = (uint32_t *)ctx->scratch[S_VALS].p;
-		double *raw_d = raw_db, *raw_b = raw_db + hb;
-		k_compact_slabs<<<(unsigned)nray, 128, 0, st>>>(nray, scap, off64, slab_ipar, slab_d, slab_b,
-				raw_ipar, raw_d, raw_b);
-		PSG_CHECK_LAUNCH();
-		k_sort_keys<<<blocks(nhit, 256), 256, 0, st>>>(nhit, raw_d, keys, vals);
-		PSG_CHECK_LAUNCH();
-		size_t stmp = 0;
-		PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, stmp, keys, keys + hb, vals, vals + hb,
-				(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
-		void *dst = psg_scratch(ctx, S_CUB, stmp);
-		if (!dst) return PSG_E_NOMEM;
-		PSG_CUDA(cub::DeviceSegmentedSort::SortPairs(dst, stmp, keys, keys + hb, vals, vals + hb,
-				(int64_t)nhit, (int64_t)nray, off32, off32 + 1, st));
-		k_gather_sorted<<<blocks(nhit, 256), 256, 0, st>>>(nhit, vals + hb, raw_ipar, raw_d, raw_b,
-				hit_ipar, hit_d, hit_b);
-		PSG_CHECK_LAUNCH();
-		k_break_ties<<<blocks(nray, 128), 128, 0, st>>>(nray, off64, hit_ipar, hit_d, hit_b, ctx->d_order);
-		PSG_CHECK_LAUNCH();
-		ctx->launches += 4;
-		if (want_kern) {
-			k_hit_kernel<<<blocks(nhit, 256), 256, 0, st>>>(nhit, hit_ipar, ctx->d_psml, hit_b,
-					psg_phys_params(ctx));
+		if (maxcount > PSG_SORT_MAX) {
+			// rays longer than the shared-memory classes: a block each
+			const unsigned grid = (unsigned)std::min<size_t>(nray, (size_t)ctx->sms);
+			k_sort_long<<<grid, LONG_NT, 0, st>>>(lists + SORT_NCLS * stride, d_nlong, off64, scap, slab_ipar,
+					slab_d, slab_b, hit_ipar, hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order,
+					(LongHit *)ctx->scratch[S_KEYS].p, hb);
 			PSG_CHECK_LAUNCH();
 			ctx->launches++;
 		}
