@@ -16,7 +16,6 @@
 #define PSG_INVALID_BIT 0x80000000u
 // Longest hit list sorted in shared memory (16 bytes per hit); longer lists
 // take the library segmented sort.
-#define PSG_ST_SLOT 64u        // a particle was hit by more rays of one tick than the slot order handles
 #define PSG_SORT_MAX 8192
 
 // Bits of the device status word.

@@ -109,10 +109,11 @@ __global__ void k_slot_count(size_t nray, int R, uint32_t N, const int64_t *__re
 }
 
 // one warp per ray: every hit into its key's run (rank from the counter,
-// which returns to zero); vals[slot] = the hit
+// which returns to zero); vals[slot] = the hit, slot[hit] = its slot (final
+// for runs of one hit, rewritten by the run sorts below otherwise)
 __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__restrict__ off,
 		const uint32_t *__restrict__ ipar, uint32_t *__restrict__ cnt, const unsigned long long *__restrict__ base,
-		uint32_t *__restrict__ vals) {
+		uint32_t *__restrict__ vals, uint32_t *__restrict__ slot) {
 	const size_t r = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32;
 	const int lane = threadIdx.x & 31;
 	if (r >= nray) return;
@@ -120,7 +121,9 @@ __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__re
 	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32) {
 		const size_t key = kb + ipar[h];
 		const uint32_t rank = atomicSub(&cnt[key], 1u) - 1u;
-		vals[(uint32_t)base[key] + rank] = (uint32_t)h;
+		const uint32_t sl = (uint32_t)base[key] + rank;
+		vals[sl] = (uint32_t)h;
+		slot[h] = sl;
 	}
 }
 
@@ -147,15 +150,16 @@ __global__ void k_act_build(size_t KN, uint32_t N, int K, const unsigned long lo
 	}
 }
 
-// Runs of at most 32 hits, a thread each: insertion sort of the run's hit
-// indices, then each hit's slot. Longer runs are left to k_slot_canon_long.
+// Runs of 2 to 32 hits, a thread each: insertion sort of the run's hit
+// indices, then each hit's slot. Longer runs are left to the run sorts
+// below; a run of one is placed already.
 __global__ void k_slot_canon(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
 		uint32_t *__restrict__ vals, uint32_t *__restrict__ slot) {
 	const uint32_t na = (uint32_t)tick_act[K];
 	for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
 		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
 		const uint32_t n = s1 - s0;
-		if (n > 32) continue;
+		if (n > 32 || n < 2) continue;
 		uint32_t v[32];
 		for (uint32_t i = 0; i < n; i++) {
 			const uint32_t x = vals[s0 + i];
@@ -173,28 +177,65 @@ __global__ void k_slot_canon(const int32_t *__restrict__ tick_act, int K, const 
 	}
 }
 
-// Runs longer than 32 (particles next to a source), a block each: bitonic
-// sort in shared memory, runs up to cap_pow2 hits (the tick's rays rounded
-// up to a power of two, at most SLOT_LONG_MAX). A longer run (more than
-// SLOT_LONG_MAX rays of one tick on one particle) is merge-sorted in global
-// memory with the upper half of vals (from half) as scratch.
+// Runs longer than 32 (particles next to a source). Up to SLOT_WARP_MAX
+// hits, a warp each (bitonic sort in the warp's part of shared memory);
+// longer ones (listed apart) a block each: bitonic in shared memory up to
+// cap_pow2 (the tick's rays rounded up to a power of two, at most
+// SLOT_LONG_MAX), merge-sorted in global memory beyond that (more than
+// SLOT_LONG_MAX rays of one tick on one particle), with the upper half of
+// vals (from half) as scratch.
+#define SLOT_WARP_MAX 1024
 #define SLOT_LONG_MAX 32768
+#define SLOT_WARPS 8
 struct U32Less {
 	__device__ __forceinline__ bool operator()(uint32_t x, uint32_t y) const { return x < y; }
 };
-__global__ void __launch_bounds__(1024) k_slot_canon_long(const int32_t *__restrict__ tick_long, int K,
+__global__ void __launch_bounds__(32 * SLOT_WARPS) k_slot_canon_warp(const int32_t *__restrict__ tick_long, int K,
 		const uint32_t *__restrict__ long_act, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals,
-		uint32_t *__restrict__ slot, int cap_pow2, size_t half, uint32_t *__restrict__ status) {
-	extern __shared__ uint32_t sv[];
+		uint32_t *__restrict__ slot) {
+	__shared__ uint32_t sv_all[SLOT_WARPS][SLOT_WARP_MAX];
+	uint32_t *sv = sv_all[threadIdx.x >> 5];
+	const int lane = threadIdx.x & 31;
 	const int ne = tick_long[K];
-	for (int e = blockIdx.x; e < ne; e += gridDim.x) {
+	for (int e = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); e < ne; e += (int)((gridDim.x * blockDim.x) >> 5)) {
 		const uint32_t a = long_act[e];
 		const uint32_t s0 = act_seg[a], n = act_seg[a + 1] - s0;
-		if ((int)n > cap_pow2) {
-			if (cap_pow2 < 2048) {      // (the tile below needs 2048 entries; n <= the tick's rays)
-				if (threadIdx.x == 0) atomicOr(status, PSG_ST_SLOT);
-				continue;
+		if (n > SLOT_WARP_MAX) continue;
+		int P = 64;
+		while (P < (int)n) P <<= 1;
+		for (int i = lane; i < P; i += 32) sv[i] = i < (int)n ? vals[s0 + i] : 0xFFFFFFFFu;
+		__syncwarp();
+		for (int k = 2; k <= P; k <<= 1) {
+			for (int j = k >> 1; j > 0; j >>= 1) {
+				for (int i = lane; i < P; i += 32) {
+					const int ixj = i ^ j;
+					if (ixj > i) {
+						const uint32_t x = sv[i], y = sv[ixj];
+						if ((x > y) == ((i & k) == 0)) {
+							sv[i] = y;
+							sv[ixj] = x;
+						}
+					}
+				}
+				__syncwarp();
 			}
+		}
+		for (int i = lane; i < (int)n; i += 32) {
+			vals[s0 + i] = sv[i];
+			slot[sv[i]] = s0 + (uint32_t)i;
+		}
+		__syncwarp();
+	}
+}
+__global__ void __launch_bounds__(1024) k_slot_canon_long(const uint32_t *__restrict__ vl_list,
+		const unsigned *__restrict__ vl_count, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals,
+		uint32_t *__restrict__ slot, int cap_pow2, size_t half) {
+	extern __shared__ uint32_t sv[];
+	const int ne = (int)*vl_count;
+	for (int e = blockIdx.x; e < ne; e += gridDim.x) {
+		const uint32_t a = vl_list[e];
+		const uint32_t s0 = act_seg[a], n = act_seg[a + 1] - s0;
+		if ((int)n > cap_pow2) {      // (shared memory holds at least the merge sort's 2048-entry tile)
 			const uint32_t *f = block_sort_global<1024>(vals + s0, vals + half + s0, (int64_t)n, sv, 0xFFFFFFFFu,
 					U32Less());
 			for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
@@ -850,23 +891,39 @@ __global__ void k_ray_lists(size_t nray, const unsigned long long *__restrict__ 
 // The active count of the batch, nact = tick_act[K], is read on the device;
 // flags cover the capacity cap + 1 (zero past nact) so the scan's size is
 // fixed.
-__global__ void k_act_class(size_t cap, const int32_t *__restrict__ tick_act, int K,
-		const uint32_t *__restrict__ act_seg, int32_t *__restrict__ flag) {
-	const size_t na = (size_t)tick_act[K];
-	for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a <= cap; a += (size_t)gridDim.x * blockDim.x)
-		flag[a] = (a < na && act_seg[a + 1] - act_seg[a] > 32) ? 1 : 0;
+// The active pairs whose run is longer than 32 hits, per tick (their order
+// within a tick is free: each is summed and sorted on its own). Counted per
+// tick, the K counts scanned by one block, then listed; runs longer than
+// SLOT_WARP_MAX also go to the very-long list of the block sort.
+__device__ __forceinline__ int tick_of_pair(const int32_t *__restrict__ tick_act, int K, int a) {
+	int lo = 0, hi = K;      // last t with tick_act[t] <= a
+	while (hi - lo > 1) {
+		const int mid = (lo + hi) >> 1;
+		if (tick_act[mid] <= a) lo = mid;
+		else hi = mid;
+	}
+	return lo;
 }
-__global__ void k_act_lists(const int32_t *__restrict__ tick_act, int K, const int32_t *__restrict__ flag,
-		const unsigned long long *__restrict__ scan, uint32_t *__restrict__ long_act) {
-	const size_t na = (size_t)tick_act[K];
-	for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a < na; a += (size_t)gridDim.x * blockDim.x)
-		if (flag[a]) long_act[(uint32_t)scan[a]] = (uint32_t)a;
+__global__ void k_long_count(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
+		unsigned long long *__restrict__ tick_cnt) {
+	const int na = tick_act[K];
+	for (int a = (int)(blockIdx.x * blockDim.x + threadIdx.x); a < na; a += (int)(gridDim.x * blockDim.x))
+		if (act_seg[a + 1] - act_seg[a] > 32) atomicAdd(&tick_cnt[tick_of_pair(tick_act, K, a)], 1ull);
 }
-// first long entry of every tick
-__global__ void k_tick_long(int K, const int32_t *__restrict__ tick_act, const unsigned long long *__restrict__ scan,
-		int32_t *__restrict__ out) {
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t <= K) out[t] = (int32_t)scan[tick_act[t]];
+__global__ void k_long_place(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
+		const unsigned long long *__restrict__ tick_off, unsigned *__restrict__ cursor,
+		uint32_t *__restrict__ long_act, int32_t *__restrict__ tick_long, uint32_t *__restrict__ vl_list,
+		unsigned *__restrict__ vl_count) {
+	const int na = tick_act[K];
+	const int i0 = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+	for (int t = i0; t <= K; t += (int)(gridDim.x * blockDim.x)) tick_long[t] = (int32_t)tick_off[t];
+	for (int a = i0; a < na; a += (int)(gridDim.x * blockDim.x)) {
+		const uint32_t n = act_seg[a + 1] - act_seg[a];
+		if (n <= 32) continue;
+		const int t = tick_of_pair(tick_act, K, a);
+		long_act[tick_off[t] + atomicAdd(&cursor[t], 1u)] = (uint32_t)a;
+		if (n > SLOT_WARP_MAX) vl_list[atomicAdd(vl_count, 1u)] = (uint32_t)a;
+	}
 }
 
 // One active particle's non-isothermal update, prepared by k_reduce<false>
@@ -1620,6 +1677,43 @@ size_t slotcnt_bytes(const BatchPlan &pl) { return 16 * ((4 * pl.KN + 15) / 16) 
 unsigned long long *slot_base(psg_context *ctx, const BatchPlan &pl) {
 	return (unsigned long long *)((char *)ctx->scratch[S_SLOTCNT].p + 16 * ((4 * pl.KN + 15) / 16));
 }
+// S_ALONG: the long pairs (at most cap/33 + 1; cap + 1 reserved), the very
+// long ones, each tick's first long pair (K + 1), then, zeroed per batch,
+// the per-tick counts and their scan (K + 1, u64), the per-tick cursors and
+// the very-long count.
+struct LongLists {
+	uint32_t *long_act, *vl_list;
+	int32_t *tick_long;
+	unsigned long long *tick_off;
+	unsigned *cursor, *vl_count;
+	void *zero;
+	size_t zero_bytes;
+};
+LongLists long_lists_at(char *m, size_t cap, size_t K, size_t *bytes) {
+	auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+	LongLists l;
+	size_t o = 0;
+	l.long_act = (uint32_t *)(m + o); o = up(o + sizeof(uint32_t) * (cap + 1));
+	l.vl_list = (uint32_t *)(m + o); o = up(o + sizeof(uint32_t) * (cap / SLOT_WARP_MAX + 2));
+	l.tick_long = (int32_t *)(m + o); o = up(o + sizeof(int32_t) * (K + 1));
+	const size_t z0 = o;
+	l.tick_off = (unsigned long long *)(m + o); o += sizeof(unsigned long long) * (K + 1);
+	l.cursor = (unsigned *)(m + o); o += sizeof(unsigned) * (K + 1);
+	l.vl_count = (unsigned *)(m + o); o += sizeof(unsigned);
+	l.zero = m + z0;
+	l.zero_bytes = o - z0;
+	o = up(o);
+	if (bytes) *bytes = o;
+	return l;
+}
+LongLists long_lists(psg_context *ctx, const BatchPlan &pl) {
+	return long_lists_at((char *)ctx->scratch[S_ALONG].p, pl.cap, pl.K, nullptr);
+}
+size_t long_lists_bytes(const BatchPlan &pl) {
+	size_t b = 0;
+	long_lists_at(nullptr, pl.cap, pl.K, &b);
+	return b;
+}
 struct UpdView {
 	double *act_g, *act_heat;
 	unsigned *cursors, *nstiff, *nrej, *dep_ctr;
@@ -1693,16 +1787,16 @@ int plan_batch(psg_context *ctx, size_t R, size_t K, const PsgTraceFill &tf, Bat
 			!psg_scratch(ctx, S_ACC, sizeof(double) * cap * pl.nacc) || !psg_scratch(ctx, S_ACT, act_bytes(pl)) ||
 			!psg_scratch(ctx, S_SLOTCNT, slotcnt_bytes(pl)))
 		return PSG_E_NOMEM;
-	if (pl.long_cap * sizeof(uint32_t) > 48 * 1024)
+	if (std::max(pl.long_cap, 2048) * sizeof(uint32_t) > 48 * 1024)
 		PSG_CUDA(cudaFuncSetAttribute(k_slot_canon_long, cudaFuncAttributeMaxDynamicSharedMemorySize,
-				(int)(pl.long_cap * sizeof(uint32_t))));
+				(int)(std::max(pl.long_cap, 2048) * sizeof(uint32_t))));
 	// ray classes (S_COUNT: class flags and scan; S_RAYLIST: the three lists,
 	// a room of nray each, inside the sort's class lists)
 	if (!psg_scratch(ctx, S_COUNT, sizeof(unsigned long long) * 2 * (nray + 1))) return PSG_E_NOMEM;
 	if (ctx->scratch[S_RAYLIST].bytes < sizeof(uint32_t) * 3 * (nray + 1)) return PSG_E_NOMEM;
 	// updates
 	if (!psg_scratch(ctx, S_UPD, upd_bytes(pl)) ||
-			!psg_scratch(ctx, S_ALONG, sizeof(int32_t) * (4 * (cap + 2) + K + 1) + 512))
+			!psg_scratch(ctx, S_ALONG, long_lists_bytes(pl)))
 		return PSG_E_NOMEM;
 	if (pl.helium) {
 		if (!psg_scratch(ctx, S_REC, sizeof(HeStiffItem) * pl.pcap)) return PSG_E_NOMEM;
@@ -1762,7 +1856,8 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	k_slot_count<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt);
 	PSG_CHECK_LAUNCH();
 	PSG_CUDA(scan_enqueue(st, kcnt, pl.KN, kbase, tiles, SlotPair()));
-	k_slot_place<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt, kbase, vals);
+	k_slot_place<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt, kbase, vals,
+			slot);
 	PSG_CHECK_LAUNCH();
 	unsigned long long *d_nact = ctx->d_counters + 6;
 	k_act_build<<<(unsigned)std::min<size_t>(blocks(pl.KN, 256), (size_t)sms * 16), 256, 0, st>>>(pl.KN, N, (int)K,
@@ -1797,24 +1892,27 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	UpdRec *urec = (!pl.helium && pl.euler) ? (UpdRec *)ctx->scratch[S_REC].p : nullptr;
 	HeStiffItem *hstiff = pl.helium ? (HeStiffItem *)ctx->scratch[S_REC].p : nullptr;
 	float *feat = pl.feat_on ? (float *)ctx->scratch[S_LOG].p : nullptr;
-	int32_t *aflag = (int32_t *)ctx->scratch[S_ALONG].p;
-	unsigned long long *ascan = (unsigned long long *)(((uintptr_t)(aflag + cap + 1) + 15) & ~(uintptr_t)15);
-	uint32_t *long_act = (uint32_t *)(ascan + (cap + 2));
-	int32_t *tick_long = (int32_t *)(long_act + (cap + 1));
-	k_act_class<<<cgrid, 256, 0, st>>>(cap, av.tick_act, (int)K, av.act_seg, aflag);
+	LongLists ll = long_lists(ctx, pl);
+	PSG_CUDA(cudaMemsetAsync(ll.zero, 0, ll.zero_bytes, st));
+	k_long_count<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, av.act_seg, ll.tick_off);
 	PSG_CHECK_LAUNCH();
-	PSG_CUDA(scan_enqueue(st, aflag, cap + 1, ascan, tiles, Widen()));
-	k_act_lists<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, aflag, ascan, long_act);
+	k_scan_sums<unsigned long long><<<1, 1024, 0, st>>>(ll.tick_off, K);
 	PSG_CHECK_LAUNCH();
-	k_tick_long<<<blocks(K + 1, 256), 256, 0, st>>>((int)K, av.tick_act, ascan, tick_long);
+	k_long_place<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, av.act_seg, ll.tick_off, ll.cursor, ll.long_act,
+			ll.tick_long, ll.vl_list, ll.vl_count);
 	PSG_CHECK_LAUNCH();
+	int32_t *tick_long = ll.tick_long;
+	uint32_t *long_act = ll.long_act;
 	// the slot order of the long runs (the short ones are in order already)
 	psg_mark_begin(ctx, PSG_K_SLOTS);
-	k_slot_canon_long<<<(unsigned)(2 * sms), 1024, sizeof(uint32_t) * pl.long_cap, st>>>(tick_long, (int)K, long_act,
-			av.act_seg, vals, slot, pl.long_cap, cap, ctx->d_status);
+	k_slot_canon_warp<<<(unsigned)(4 * sms), 32 * SLOT_WARPS, 0, st>>>(tick_long, (int)K, long_act, av.act_seg, vals,
+			slot);
+	PSG_CHECK_LAUNCH();
+	k_slot_canon_long<<<(unsigned)sms, 1024, sizeof(uint32_t) * std::max(pl.long_cap, 2048), st>>>(ll.vl_list,
+			ll.vl_count, av.act_seg, vals, slot, pl.long_cap, cap);
 	PSG_CHECK_LAUNCH();
 	psg_mark_end(ctx);
-	ctx->launches += 6;
+	ctx->launches += 5;
 
 	// the tick loop
 	double *d_lost = (double *)(ctx->d_counters + 2);
