@@ -114,7 +114,11 @@ def test_surrogate_ticks(phys_noniso):
         assert rows.shape[0] > 1000
         s, hist = fit(a, rows, epochs=25, batch=512, lr=3e-3, log=lambda *_: None)
         assert hist[-1] < 0.05      # it learns: most of the targets' variance explained
-        # b: the same ticks on the plain integrator; c: with the surrogate
+        # b: the same ticks on the plain integrator; c: with the surrogate.
+        # A fresh schedule: the one above has emitted ticks 1-12 already,
+        # and replaying them would give rays of negative photon counts.
+        from psphray_b200 import fields
+        rays = fields.make_workload("lognormal128", n_side=24, nray=256, seed=3).schedule.rays_for_ticks
         rb = rays(1, 12)
         b.run_ticks(rb, 256, 12, 1, w.tick_time)
         # every prediction rejected (tolerance 0+): identical to the plain path
