@@ -287,9 +287,11 @@ __device__ __forceinline__ void put_sorted_hit(int64_t h, uint32_t p, const uint
 }
 
 // Per-ray sort by (d, ipar), one ray per block of TPR threads holding IPT
-// hits each: a block radix sort (6 passes of 4 bits) on d mapped to 24 bits
-// over the ray's own range of d (a monotone map); the few runs of equal keys
-// are then insertion-sorted on the exact (d, ipar) -- the reference's d
+// hits each: a block radix sort (passes of 4 bits) on d mapped to KEY_BITS
+// bits over the ray's own range of d (a monotone map) -- 12 bits for up to
+// 256 hits, 16 up to 2048, 20 beyond, so that about n^2 / 2^(bits+1) pairs
+// share a key -- and the few runs of equal keys are then insertion-sorted
+// on the exact (d, ipar) -- the reference's d
 // order (loop.c:783-787) with ties broken by the caller's particle index. With want_kern the b column is replaced by the
 // column-density factor sph_depth(b/h)/h^2 of loop.c:429-445.
 template <int TPR, int IPT>
@@ -346,17 +348,19 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 		dlo = fmin(dlo, sm.lo[w]);
 		dhi = fmax(dhi, sm.hi[w]);
 	}
-	const double scale = dhi > dlo ? 16777215.0 / (dhi - dlo) : 0.0;
+	constexpr int KEY_BITS = NMAX <= 256 ? 12 : (NMAX <= 2048 ? 16 : 20);
+	constexpr uint32_t KEY_MAX = (1u << KEY_BITS) - 1u;
+	const double scale = dhi > dlo ? (double)KEY_MAX / (dhi - dlo) : 0.0;
 	uint32_t k[IPT], v[IPT];
 #pragma unroll
 	for (int u = 0; u < IPT; u++) {
 		const int i = threadIdx.x * IPT + u;
 		// padding takes the largest key; the sort is stable and padding
 		// follows every real item, so it stays behind them
-		k[u] = i < n ? (uint32_t)((dv[u] - dlo) * scale) : 16777215u;
+		k[u] = i < n ? min((uint32_t)((dv[u] - dlo) * scale), KEY_MAX) : KEY_MAX;
 		v[u] = (uint32_t)i;
 	}
-	Sort(sm.sort).Sort(k, v, 0, 24);
+	Sort(sm.sort).Sort(k, v, 0, KEY_BITS);
 	__syncthreads();
 #pragma unroll
 	for (int u = 0; u < IPT; u++) {
