@@ -86,17 +86,19 @@ __device__ Item *block_sort_global(Item *a, Item *b, int64_t n, Item *tile, Item
 }
 
 // ---- device-wide: a grid of tiles, then one launch per merge pass ----------
-#define DSORT_NT 1024
+// Tiles of 2 x NT items, NT = 64, 256 or 1024 by the size (a handful of
+// recombination rays needs no 1024-thread block).
 #define DSORT_PER 8          // outputs per thread in a merge pass (divides every run width)
-template <typename Item, typename Less>
-__global__ void __launch_bounds__(DSORT_NT) k_dsort_tiles(Item *a, size_t n, Item pad, Less less) {
-	__shared__ Item tile[2 * DSORT_NT];
-	const size_t t0 = (size_t)blockIdx.x * 2 * DSORT_NT;
-	const int m = (int)min((size_t)2 * DSORT_NT, n - t0);
-	for (int i = threadIdx.x; i < 2 * DSORT_NT; i += DSORT_NT) tile[i] = i < m ? a[t0 + i] : pad;
+inline int dsort_nt(size_t n) { return n <= 128 ? 64 : (n <= 512 ? 256 : 1024); }
+template <int NT, typename Item, typename Less>
+__global__ void __launch_bounds__(NT) k_dsort_tiles(Item *a, size_t n, Item pad, Less less) {
+	__shared__ Item tile[2 * NT];
+	const size_t t0 = (size_t)blockIdx.x * 2 * NT;
+	const int m = (int)min((size_t)2 * NT, n - t0);
+	for (int i = threadIdx.x; i < 2 * NT; i += NT) tile[i] = i < m ? a[t0 + i] : pad;
 	__syncthreads();
-	tile_bitonic<DSORT_NT>(tile, less);
-	for (int i = threadIdx.x; i < m; i += DSORT_NT) a[t0 + i] = tile[i];
+	tile_bitonic<NT>(tile, less);
+	for (int i = threadIdx.x; i < m; i += NT) a[t0 + i] = tile[i];
 }
 template <typename Item, typename Less>
 __global__ void __launch_bounds__(256) k_dsort_merge(const Item *__restrict__ a, Item *__restrict__ b, size_t n,
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(256) k_dsort_merge(const Item *__restrict__ a,
 // Number of merge passes after the tiles; the result is in a when even.
 inline int dsort_passes(size_t n) {
 	int p = 0;
-	for (size_t w = 2 * DSORT_NT; w < n; w <<= 1) p++;
+	for (size_t w = 2 * (size_t)dsort_nt(n); w < n; w <<= 1) p++;
 	return p;
 }
 // Issues the sort of a[0, n) (b: scratch of n items) on st; launch sizes
@@ -120,9 +122,12 @@ inline int dsort_passes(size_t n) {
 template <typename Item, typename Less>
 cudaError_t dsort_enqueue(cudaStream_t st, Item *a, Item *b, size_t n, Item pad, Less less) {
 	if (n == 0) return cudaSuccess;
-	k_dsort_tiles<Item, Less><<<(unsigned)((n + 2 * DSORT_NT - 1) / (2 * DSORT_NT)), DSORT_NT, 0, st>>>(a, n, pad,
-			less);
-	for (size_t w = 2 * DSORT_NT; w < n; w <<= 1) {
+	const int nt = dsort_nt(n);
+	const unsigned tiles = (unsigned)((n + 2 * nt - 1) / (2 * nt));
+	if (nt == 64) k_dsort_tiles<64, Item, Less><<<tiles, 64, 0, st>>>(a, n, pad, less);
+	else if (nt == 256) k_dsort_tiles<256, Item, Less><<<tiles, 256, 0, st>>>(a, n, pad, less);
+	else k_dsort_tiles<1024, Item, Less><<<tiles, 1024, 0, st>>>(a, n, pad, less);
+	for (size_t w = 2 * (size_t)nt; w < n; w <<= 1) {
 		k_dsort_merge<Item, Less><<<(unsigned)((n + 256 * DSORT_PER - 1) / (256 * DSORT_PER)), 256, 0, st>>>(a, b, n,
 				w, less);
 		Item *s = a;

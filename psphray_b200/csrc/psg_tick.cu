@@ -109,11 +109,11 @@ __global__ void k_slot_count(size_t nray, int R, uint32_t N, const int64_t *__re
 }
 
 // one warp per ray: every hit into its key's run (rank from the counter,
-// which returns to zero); vals[slot] = the hit, slot[hit] = its slot (final
-// for runs of one hit, rewritten by the run sorts below otherwise)
+// which returns to zero); vals[slot] = the hit (slot[hit] is written by the
+// run sorts below)
 __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__restrict__ off,
 		const uint32_t *__restrict__ ipar, uint32_t *__restrict__ cnt, const unsigned long long *__restrict__ base,
-		uint32_t *__restrict__ vals, uint32_t *__restrict__ slot) {
+		uint32_t *__restrict__ vals) {
 	const size_t r = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32;
 	const int lane = threadIdx.x & 31;
 	if (r >= nray) return;
@@ -121,9 +121,7 @@ __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__re
 	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32) {
 		const size_t key = kb + ipar[h];
 		const uint32_t rank = atomicSub(&cnt[key], 1u) - 1u;
-		const uint32_t sl = (uint32_t)base[key] + rank;
-		vals[sl] = (uint32_t)h;
-		slot[h] = sl;
+		vals[(uint32_t)base[key] + rank] = (uint32_t)h;
 	}
 }
 
@@ -150,41 +148,81 @@ __global__ void k_act_build(size_t KN, uint32_t N, int K, const unsigned long lo
 	}
 }
 
-// Runs of 2 to 32 hits, a thread each: insertion sort of the run's hit
-// indices, then each hit's slot. Longer runs are left to the run sorts
-// below; a run of one is placed already.
-__global__ void k_slot_canon(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
-		uint32_t *__restrict__ vals, uint32_t *__restrict__ slot) {
+// Runs of up to 32 hits. A warp takes 32 consecutive pairs; their slots
+// are contiguous, so the warp loads them into shared memory with coalesced
+// reads, each lane insertion-sorts its own run there, and the warp writes
+// the span back together with every slot's hit -> slot entry. Longer runs
+// inside the span are copied unchanged (their own sorts follow); a span
+// over SLOT_SPAN slots takes the lane-by-lane form from device memory.
+#define SLOT_SPAN 1024
+#define CANON_WARPS 8
+__global__ void __launch_bounds__(32 * CANON_WARPS) k_slot_canon(const int32_t *__restrict__ tick_act, int K,
+		const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals, uint32_t *__restrict__ slot) {
+	__shared__ uint32_t buf[CANON_WARPS][SLOT_SPAN];
+	uint32_t *sv = buf[threadIdx.x >> 5];
+	const int lane = threadIdx.x & 31;
 	const uint32_t na = (uint32_t)tick_act[K];
-	for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
-		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
-		const uint32_t n = s1 - s0;
-		if (n > 32 || n < 2) continue;
-		uint32_t v[32];
-		for (uint32_t i = 0; i < n; i++) {
-			const uint32_t x = vals[s0 + i];
-			uint32_t j = i;
-			while (j > 0 && v[j - 1] > x) {
-				v[j] = v[j - 1];
-				j--;
-			}
-			v[j] = x;
+	const uint32_t stride = gridDim.x * CANON_WARPS * 32;
+	for (uint32_t a0 = (blockIdx.x * CANON_WARPS + (threadIdx.x >> 5)) * 32; a0 < na; a0 += stride) {
+		const uint32_t a = a0 + lane;
+		const uint32_t S0 = act_seg[a0], S1 = act_seg[min(a0 + 32, na)];
+		uint32_t s0 = 0, n = 0;
+		if (a < na) {
+			s0 = act_seg[a];
+			n = act_seg[a + 1] - s0;
 		}
-		for (uint32_t i = 0; i < n; i++) {
-			vals[s0 + i] = v[i];
-			slot[v[i]] = s0 + i;
+		if (S1 - S0 <= SLOT_SPAN) {
+			for (uint32_t i = lane; i < S1 - S0; i += 32) sv[i] = vals[S0 + i];
+			__syncwarp();
+			if (n >= 2 && n <= 32) {
+				uint32_t *r = sv + (s0 - S0);
+				for (uint32_t i = 1; i < n; i++) {
+					const uint32_t x = r[i];
+					uint32_t j = i;
+					while (j > 0 && r[j - 1] > x) {
+						r[j] = r[j - 1];
+						j--;
+					}
+					r[j] = x;
+				}
+			}
+			__syncwarp();
+			for (uint32_t i = lane; i < S1 - S0; i += 32) {
+				const uint32_t v = sv[i];
+				vals[S0 + i] = v;
+				slot[v] = S0 + i;
+			}
+			__syncwarp();
+		} else if (n <= 32) {
+			uint32_t v[32];
+			for (uint32_t i = 0; i < n; i++) {
+				const uint32_t x = vals[s0 + i];
+				uint32_t j = i;
+				while (j > 0 && v[j - 1] > x) {
+					v[j] = v[j - 1];
+					j--;
+				}
+				v[j] = x;
+			}
+			for (uint32_t i = 0; i < n; i++) {
+				vals[s0 + i] = v[i];
+				slot[v[i]] = s0 + i;
+			}
 		}
 	}
 }
 
-// Runs longer than 32 (particles next to a source). Up to SLOT_WARP_MAX
-// hits, a warp each (bitonic sort in the warp's part of shared memory);
-// longer ones (listed apart) a block each: bitonic in shared memory up to
-// cap_pow2 (the tick's rays rounded up to a power of two, at most
-// SLOT_LONG_MAX), merge-sorted in global memory beyond that (more than
-// SLOT_LONG_MAX rays of one tick on one particle), with the upper half of
-// vals (from half) as scratch.
-#define SLOT_WARP_MAX 1024
+// Runs longer than 32 (particles next to a source), in three tiers: up to
+// SLOT_WARP_MAX hits a warp each (bitonic sort in the warp's part of
+// shared memory); up to SLOT_MID_MAX a 256-thread block each (bitonic in
+// shared memory); longer ones a 1024-thread block each, bitonic in shared
+// memory up to cap_pow2 (the tick's rays rounded up to a power of two, at
+// most SLOT_LONG_MAX) and merge-sorted in global memory beyond that (more
+// than SLOT_LONG_MAX rays of one tick on one particle), with the upper half
+// of vals (from half) as scratch. The two block tiers take their runs from
+// lists of their own.
+#define SLOT_WARP_MAX 256
+#define SLOT_MID_MAX 2048
 #define SLOT_LONG_MAX 32768
 #define SLOT_WARPS 8
 struct U32Less {
@@ -227,6 +265,46 @@ __global__ void __launch_bounds__(32 * SLOT_WARPS) k_slot_canon_warp(const int32
 		__syncwarp();
 	}
 }
+// P <= PMAX elements of sv sorted by the block (bitonic); callers sync
+// before, the last stage syncs after
+template <int NT>
+__device__ __forceinline__ void block_bitonic_u32(uint32_t *sv, int P) {
+	for (int k = 2; k <= P; k <<= 1) {
+		for (int j = k >> 1; j > 0; j >>= 1) {
+			for (int i = threadIdx.x; i < P; i += NT) {
+				const int ixj = i ^ j;
+				if (ixj > i) {
+					const uint32_t x = sv[i], y = sv[ixj];
+					if ((x > y) == ((i & k) == 0)) {
+						sv[i] = y;
+						sv[ixj] = x;
+					}
+				}
+			}
+			__syncthreads();
+		}
+	}
+}
+__global__ void __launch_bounds__(256) k_slot_canon_mid(const uint32_t *__restrict__ list,
+		const unsigned *__restrict__ count, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals,
+		uint32_t *__restrict__ slot) {
+	__shared__ uint32_t sv[SLOT_MID_MAX];
+	const int ne = (int)*count;
+	for (int e = blockIdx.x; e < ne; e += gridDim.x) {
+		const uint32_t a = list[e];
+		const uint32_t s0 = act_seg[a], n = act_seg[a + 1] - s0;
+		int P = 2 * SLOT_WARP_MAX;
+		while (P < (int)n) P <<= 1;
+		for (int i = threadIdx.x; i < P; i += 256) sv[i] = i < (int)n ? vals[s0 + i] : 0xFFFFFFFFu;
+		__syncthreads();
+		block_bitonic_u32<256>(sv, P);
+		for (int i = threadIdx.x; i < (int)n; i += 256) {
+			vals[s0 + i] = sv[i];
+			slot[sv[i]] = s0 + (uint32_t)i;
+		}
+		__syncthreads();
+	}
+}
 __global__ void __launch_bounds__(1024) k_slot_canon_long(const uint32_t *__restrict__ vl_list,
 		const unsigned *__restrict__ vl_count, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals,
 		uint32_t *__restrict__ slot, int cap_pow2, size_t half) {
@@ -250,22 +328,7 @@ __global__ void __launch_bounds__(1024) k_slot_canon_long(const uint32_t *__rest
 		while (P < (int)n) P <<= 1;
 		for (int i = threadIdx.x; i < P; i += blockDim.x) sv[i] = i < (int)n ? vals[s0 + i] : 0xFFFFFFFFu;
 		__syncthreads();
-		for (int k = 2; k <= P; k <<= 1) {
-			for (int j = k >> 1; j > 0; j >>= 1) {
-				for (int i = threadIdx.x; i < P; i += blockDim.x) {
-					const int ixj = i ^ j;
-					if (ixj > i) {
-						const uint32_t x = sv[i], y = sv[ixj];
-						const bool up = (i & k) == 0;
-						if ((x > y) == up) {
-							sv[i] = y;
-							sv[ixj] = x;
-						}
-					}
-				}
-				__syncthreads();
-			}
-		}
+		block_bitonic_u32<1024>(sv, P);
 		for (int i = threadIdx.x; i < (int)n; i += blockDim.x) {
 			vals[s0 + i] = sv[i];
 			slot[sv[i]] = s0 + (uint32_t)i;
@@ -894,7 +957,7 @@ __global__ void k_ray_lists(size_t nray, const unsigned long long *__restrict__ 
 // The active pairs whose run is longer than 32 hits, per tick (their order
 // within a tick is free: each is summed and sorted on its own). Counted per
 // tick, the K counts scanned by one block, then listed; runs longer than
-// SLOT_WARP_MAX also go to the very-long list of the block sort.
+// SLOT_WARP_MAX also go to the lists of the two block sorts.
 __device__ __forceinline__ int tick_of_pair(const int32_t *__restrict__ tick_act, int K, int a) {
 	int lo = 0, hi = K;      // last t with tick_act[t] <= a
 	while (hi - lo > 1) {
@@ -912,8 +975,8 @@ __global__ void k_long_count(const int32_t *__restrict__ tick_act, int K, const 
 }
 __global__ void k_long_place(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
 		const unsigned long long *__restrict__ tick_off, unsigned *__restrict__ cursor,
-		uint32_t *__restrict__ long_act, int32_t *__restrict__ tick_long, uint32_t *__restrict__ vl_list,
-		unsigned *__restrict__ vl_count) {
+		uint32_t *__restrict__ long_act, int32_t *__restrict__ tick_long, uint32_t *__restrict__ mid_list,
+		unsigned *__restrict__ mid_count, uint32_t *__restrict__ vl_list, unsigned *__restrict__ vl_count) {
 	const int na = tick_act[K];
 	const int i0 = (int)(blockIdx.x * blockDim.x + threadIdx.x);
 	for (int t = i0; t <= K; t += (int)(gridDim.x * blockDim.x)) tick_long[t] = (int32_t)tick_off[t];
@@ -922,7 +985,8 @@ __global__ void k_long_place(const int32_t *__restrict__ tick_act, int K, const 
 		if (n <= 32) continue;
 		const int t = tick_of_pair(tick_act, K, a);
 		long_act[tick_off[t] + atomicAdd(&cursor[t], 1u)] = (uint32_t)a;
-		if (n > SLOT_WARP_MAX) vl_list[atomicAdd(vl_count, 1u)] = (uint32_t)a;
+		if (n > SLOT_MID_MAX) vl_list[atomicAdd(vl_count, 1u)] = (uint32_t)a;
+		else if (n > SLOT_WARP_MAX) mid_list[atomicAdd(mid_count, 1u)] = (uint32_t)a;
 	}
 }
 
@@ -1677,15 +1741,15 @@ size_t slotcnt_bytes(const BatchPlan &pl) { return 16 * ((4 * pl.KN + 15) / 16) 
 unsigned long long *slot_base(psg_context *ctx, const BatchPlan &pl) {
 	return (unsigned long long *)((char *)ctx->scratch[S_SLOTCNT].p + 16 * ((4 * pl.KN + 15) / 16));
 }
-// S_ALONG: the long pairs (at most cap/33 + 1; cap + 1 reserved), the very
-// long ones, each tick's first long pair (K + 1), then, zeroed per batch,
-// the per-tick counts and their scan (K + 1, u64), the per-tick cursors and
-// the very-long count.
+// S_ALONG: the long pairs (at most cap/33 + 1; cap + 1 reserved), the
+// middle and very long ones, each tick's first long pair (K + 1), then,
+// zeroed per batch, the per-tick counts and their scan (K + 1, u64), the
+// per-tick cursors and the two list counts.
 struct LongLists {
-	uint32_t *long_act, *vl_list;
+	uint32_t *long_act, *mid_list, *vl_list;
 	int32_t *tick_long;
 	unsigned long long *tick_off;
-	unsigned *cursor, *vl_count;
+	unsigned *cursor, *mid_count, *vl_count;
 	void *zero;
 	size_t zero_bytes;
 };
@@ -1694,12 +1758,14 @@ LongLists long_lists_at(char *m, size_t cap, size_t K, size_t *bytes) {
 	LongLists l;
 	size_t o = 0;
 	l.long_act = (uint32_t *)(m + o); o = up(o + sizeof(uint32_t) * (cap + 1));
-	l.vl_list = (uint32_t *)(m + o); o = up(o + sizeof(uint32_t) * (cap / SLOT_WARP_MAX + 2));
+	l.mid_list = (uint32_t *)(m + o); o = up(o + sizeof(uint32_t) * (cap / SLOT_WARP_MAX + 2));
+	l.vl_list = (uint32_t *)(m + o); o = up(o + sizeof(uint32_t) * (cap / SLOT_MID_MAX + 2));
 	l.tick_long = (int32_t *)(m + o); o = up(o + sizeof(int32_t) * (K + 1));
 	const size_t z0 = o;
 	l.tick_off = (unsigned long long *)(m + o); o += sizeof(unsigned long long) * (K + 1);
 	l.cursor = (unsigned *)(m + o); o += sizeof(unsigned) * (K + 1);
 	l.vl_count = (unsigned *)(m + o); o += sizeof(unsigned);
+	l.mid_count = (unsigned *)(m + o); o += sizeof(unsigned);
 	l.zero = m + z0;
 	l.zero_bytes = o - z0;
 	o = up(o);
@@ -1856,14 +1922,14 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	k_slot_count<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt);
 	PSG_CHECK_LAUNCH();
 	PSG_CUDA(scan_enqueue(st, kcnt, pl.KN, kbase, tiles, SlotPair()));
-	k_slot_place<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt, kbase, vals,
-			slot);
+	k_slot_place<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt, kbase, vals);
 	PSG_CHECK_LAUNCH();
 	unsigned long long *d_nact = ctx->d_counters + 6;
 	k_act_build<<<(unsigned)std::min<size_t>(blocks(pl.KN, 256), (size_t)sms * 16), 256, 0, st>>>(pl.KN, N, (int)K,
 			kbase, av.act_ipar, av.act_seg, av.tick_act, d_nact);
 	PSG_CHECK_LAUNCH();
-	k_slot_canon<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, av.act_seg, vals, slot);
+	k_slot_canon<<<(unsigned)std::min<size_t>(blocks(cap, 1024), (size_t)sms * 6), 32 * CANON_WARPS, 0, st>>>(
+			av.tick_act, (int)K, av.act_seg, vals, slot);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 8;
 	unsigned long long *d_nsat = ctx->d_counters + 1;      // (zeroed by the caller, per call)
@@ -1899,7 +1965,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	k_scan_sums<unsigned long long><<<1, 1024, 0, st>>>(ll.tick_off, K);
 	PSG_CHECK_LAUNCH();
 	k_long_place<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, av.act_seg, ll.tick_off, ll.cursor, ll.long_act,
-			ll.tick_long, ll.vl_list, ll.vl_count);
+			ll.tick_long, ll.mid_list, ll.mid_count, ll.vl_list, ll.vl_count);
 	PSG_CHECK_LAUNCH();
 	int32_t *tick_long = ll.tick_long;
 	uint32_t *long_act = ll.long_act;
@@ -1908,11 +1974,13 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	k_slot_canon_warp<<<(unsigned)(4 * sms), 32 * SLOT_WARPS, 0, st>>>(tick_long, (int)K, long_act, av.act_seg, vals,
 			slot);
 	PSG_CHECK_LAUNCH();
+	k_slot_canon_mid<<<(unsigned)(4 * sms), 256, 0, st>>>(ll.mid_list, ll.mid_count, av.act_seg, vals, slot);
+	PSG_CHECK_LAUNCH();
 	k_slot_canon_long<<<(unsigned)sms, 1024, sizeof(uint32_t) * std::max(pl.long_cap, 2048), st>>>(ll.vl_list,
 			ll.vl_count, av.act_seg, vals, slot, pl.long_cap, cap);
 	PSG_CHECK_LAUNCH();
 	psg_mark_end(ctx);
-	ctx->launches += 5;
+	ctx->launches += 6;
 
 	// the tick loop
 	double *d_lost = (double *)(ctx->d_counters + 2);
