@@ -24,7 +24,7 @@ RUN = os.path.join(HERE, "psg_run")
 CU_SOURCES = ["psg_context.cu", "psg_tree.cu", "psg_trace.cu", "psg_tick.cu", "psg_emit.cu", "psg_mlp.cu", "psg_surrogate.cu",
               "psg_recomb.cu"]
 C_SOURCES = ["psg_host.c", "psg_snapshot.c"]
-HEADERS = ["psg_internal.cuh", "psg_solve.cuh", "psg_surrogate.cuh", "psg_philox.cuh", "psg_helium.cuh"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")))
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

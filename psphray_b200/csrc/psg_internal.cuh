@@ -29,7 +29,7 @@
 // scratch slots
 enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
-	S_HIT_IPAR, S_HIT_KERN, S_SLOT, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
+	S_HIT_IPAR, S_HIT_KERN, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
 	S_EMIT, S_MAP, S_ALONG, S_MLP, S_LOG, S_SURR, S_REC, S_RECW, S_RECK, S_RECRAYS, S_SNAP, S_SCAN, S_SLOTCNT,
 	S_NSLOTS
 };

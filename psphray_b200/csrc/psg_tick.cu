@@ -2,19 +2,21 @@
 // (loop.c:647-776) for many ticks whose rays are traced in one batch.
 //
 // Hit lists depend only on geometry, so all rays of a batch of ticks are
-// traced together. Before the tick loop every hit gets a slot in a
-// by-particle order ((tick, ipar, hit) sorted), which turns the reference's
-// merge into the runs of equal (tick, ipar) and its float atomics into a
-// fixed-order FP64 sum per particle. Then per tick:
-//   deposit: one warp per ray walks its sorted hits 32 at a time; optical
-//     depths are summed with an FP64 warp scan, the transmitted photons before
-//     each hit are TM*exp(-scan), absorbed = TM_j*(1-e^-tau_j); the first hit
-//     whose absorption exceeds its neutral atoms (the cap of loop.c:482-485)
-//     or after which TM/Nph < 1e-10 (loop.c:585) is settled on its own and the
-//     scan restarts after it. Each hit writes photons/NH into its slot, or -1
-//     when the reference would not deposit there;
-//   update: one thread per particle hit in the tick sums its slots in order
-//     and advances (lambdaH, ie) by the step since its last hit.
+// traced together. Before the tick loop the hits are put in a by-particle
+// order ((tick, ipar, hit) sorted: the slot order, vals[slot] = hit), which
+// turns the reference's merge into the runs of equal (tick, ipar) and its
+// float atomics into a fixed-order FP64 sum per particle. Then per tick:
+//   deposit: a group of threads per ray (a warp, a 128-thread quarter or a
+//     512-thread block) walks its sorted hits; optical depths are summed with
+//     an FP64 group scan, the transmitted photons before each hit are
+//     TM*exp(-scan), absorbed = TM_j*(1-e^-tau_j); the first hit whose
+//     absorption exceeds its neutral atoms (the cap of loop.c:482-485) or
+//     after which TM/Nph < 1e-10 (loop.c:585) is settled on its own and the
+//     scan restarts after it. Each hit writes photons/NH at its own index (in
+//     ray order), or -1 when the reference would not deposit there;
+//   update: every particle hit in the tick sums its deposits in slot order
+//     (gathered through vals) and advances (lambdaH, ie) by the step since
+//     its last hit.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -109,8 +111,7 @@ __global__ void k_slot_count(size_t nray, int R, uint32_t N, const int64_t *__re
 }
 
 // one warp per ray: every hit into its key's run (rank from the counter,
-// which returns to zero); vals[slot] = the hit (slot[hit] is written by the
-// run sorts below)
+// which returns to zero); vals[slot] = the hit
 __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__restrict__ off,
 		const uint32_t *__restrict__ ipar, uint32_t *__restrict__ cnt, const unsigned long long *__restrict__ base,
 		uint32_t *__restrict__ vals) {
@@ -151,13 +152,13 @@ __global__ void k_act_build(size_t KN, uint32_t N, int K, const unsigned long lo
 // Runs of up to 32 hits. A warp takes 32 consecutive pairs; their slots
 // are contiguous, so the warp loads them into shared memory with coalesced
 // reads, each lane insertion-sorts its own run there, and the warp writes
-// the span back together with every slot's hit -> slot entry. Longer runs
-// inside the span are copied unchanged (their own sorts follow); a span
-// over SLOT_SPAN slots takes the lane-by-lane form from device memory.
+// the span back. Longer runs inside the span are copied unchanged (their
+// own sorts follow); a span over SLOT_SPAN slots takes the lane-by-lane
+// form from device memory.
 #define SLOT_SPAN 1024
 #define CANON_WARPS 8
 __global__ void __launch_bounds__(32 * CANON_WARPS) k_slot_canon(const int32_t *__restrict__ tick_act, int K,
-		const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals, uint32_t *__restrict__ slot) {
+		const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals) {
 	__shared__ uint32_t buf[CANON_WARPS][SLOT_SPAN];
 	uint32_t *sv = buf[threadIdx.x >> 5];
 	const int lane = threadIdx.x & 31;
@@ -187,13 +188,9 @@ __global__ void __launch_bounds__(32 * CANON_WARPS) k_slot_canon(const int32_t *
 				}
 			}
 			__syncwarp();
-			for (uint32_t i = lane; i < S1 - S0; i += 32) {
-				const uint32_t v = sv[i];
-				vals[S0 + i] = v;
-				slot[v] = S0 + i;
-			}
+			for (uint32_t i = lane; i < S1 - S0; i += 32) vals[S0 + i] = sv[i];
 			__syncwarp();
-		} else if (n <= 32) {
+		} else if (n >= 2 && n <= 32) {
 			uint32_t v[32];
 			for (uint32_t i = 0; i < n; i++) {
 				const uint32_t x = vals[s0 + i];
@@ -204,10 +201,7 @@ __global__ void __launch_bounds__(32 * CANON_WARPS) k_slot_canon(const int32_t *
 				}
 				v[j] = x;
 			}
-			for (uint32_t i = 0; i < n; i++) {
-				vals[s0 + i] = v[i];
-				slot[v[i]] = s0 + i;
-			}
+			for (uint32_t i = 0; i < n; i++) vals[s0 + i] = v[i];
 		}
 	}
 }
@@ -229,8 +223,7 @@ struct U32Less {
 	__device__ __forceinline__ bool operator()(uint32_t x, uint32_t y) const { return x < y; }
 };
 __global__ void __launch_bounds__(32 * SLOT_WARPS) k_slot_canon_warp(const int32_t *__restrict__ tick_long, int K,
-		const uint32_t *__restrict__ long_act, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals,
-		uint32_t *__restrict__ slot) {
+		const uint32_t *__restrict__ long_act, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals) {
 	__shared__ uint32_t sv_all[SLOT_WARPS][SLOT_WARP_MAX];
 	uint32_t *sv = sv_all[threadIdx.x >> 5];
 	const int lane = threadIdx.x & 31;
@@ -258,10 +251,7 @@ __global__ void __launch_bounds__(32 * SLOT_WARPS) k_slot_canon_warp(const int32
 				__syncwarp();
 			}
 		}
-		for (int i = lane; i < (int)n; i += 32) {
-			vals[s0 + i] = sv[i];
-			slot[sv[i]] = s0 + (uint32_t)i;
-		}
+		for (int i = lane; i < (int)n; i += 32) vals[s0 + i] = sv[i];
 		__syncwarp();
 	}
 }
@@ -286,8 +276,7 @@ __device__ __forceinline__ void block_bitonic_u32(uint32_t *sv, int P) {
 	}
 }
 __global__ void __launch_bounds__(256) k_slot_canon_mid(const uint32_t *__restrict__ list,
-		const unsigned *__restrict__ count, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals,
-		uint32_t *__restrict__ slot) {
+		const unsigned *__restrict__ count, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals) {
 	__shared__ uint32_t sv[SLOT_MID_MAX];
 	const int ne = (int)*count;
 	for (int e = blockIdx.x; e < ne; e += gridDim.x) {
@@ -298,16 +287,13 @@ __global__ void __launch_bounds__(256) k_slot_canon_mid(const uint32_t *__restri
 		for (int i = threadIdx.x; i < P; i += 256) sv[i] = i < (int)n ? vals[s0 + i] : 0xFFFFFFFFu;
 		__syncthreads();
 		block_bitonic_u32<256>(sv, P);
-		for (int i = threadIdx.x; i < (int)n; i += 256) {
-			vals[s0 + i] = sv[i];
-			slot[sv[i]] = s0 + (uint32_t)i;
-		}
+		for (int i = threadIdx.x; i < (int)n; i += 256) vals[s0 + i] = sv[i];
 		__syncthreads();
 	}
 }
 __global__ void __launch_bounds__(1024) k_slot_canon_long(const uint32_t *__restrict__ vl_list,
 		const unsigned *__restrict__ vl_count, const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals,
-		uint32_t *__restrict__ slot, int cap_pow2, size_t half) {
+		int cap_pow2, size_t half) {
 	extern __shared__ uint32_t sv[];
 	const int ne = (int)*vl_count;
 	for (int e = blockIdx.x; e < ne; e += gridDim.x) {
@@ -316,11 +302,7 @@ __global__ void __launch_bounds__(1024) k_slot_canon_long(const uint32_t *__rest
 		if ((int)n > cap_pow2) {      // (shared memory holds at least the merge sort's 2048-entry tile)
 			const uint32_t *f = block_sort_global<1024>(vals + s0, vals + half + s0, (int64_t)n, sv, 0xFFFFFFFFu,
 					U32Less());
-			for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-				const uint32_t v = f[i];
-				vals[s0 + i] = v;
-				slot[v] = s0 + i;
-			}
+			for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) vals[s0 + i] = f[i];
 			__syncthreads();
 			continue;
 		}
@@ -329,10 +311,7 @@ __global__ void __launch_bounds__(1024) k_slot_canon_long(const uint32_t *__rest
 		for (int i = threadIdx.x; i < P; i += blockDim.x) sv[i] = i < (int)n ? vals[s0 + i] : 0xFFFFFFFFu;
 		__syncthreads();
 		block_bitonic_u32<1024>(sv, P);
-		for (int i = threadIdx.x; i < (int)n; i += blockDim.x) {
-			vals[s0 + i] = sv[i];
-			slot[sv[i]] = s0 + (uint32_t)i;
-		}
+		for (int i = threadIdx.x; i < (int)n; i += blockDim.x) vals[s0 + i] = sv[i];
 		__syncthreads();
 	}
 }
@@ -349,7 +328,7 @@ __device__ __forceinline__ bool below_cutoff(double TM, double Nph) {
 // scan restarts after it (or, in the AFF form, the rest of the step goes to
 // settle_capped()). Transmitted photons before hit j are
 // TM*exp(-(sum of earlier tau)); after it, TM_j minus the absorbed photons,
-// as loop.c:580 updates TM. Each hit writes photons/NH to its slot, or -1
+// as loop.c:580 updates TM. Each hit writes photons/NH at its index, or -1
 // where the reference deposits nothing. wsum and wb carry the per-warp scan
 // totals (wb: the affine maps' offsets).
 struct DepShared {
@@ -368,10 +347,10 @@ __device__ __forceinline__ void group_sync(int bar) {
 	else asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(NT) : "memory");
 }
 
-// One hit's deposits sit together, nacc doubles per slot (photons/NH; with
-// heat the heat; with helium yGdepHeI and yGdepHeII), so that the scattered
-// store of a hit touches one 32-byte sector and the by-particle sums read
-// one contiguous run.
+// One hit's deposits sit together, nacc doubles per hit (photons/NH; with
+// heat the heat; with helium yGdepHeI and yGdepHeII), at the hit's index:
+// a ray's group stores contiguously, and the by-particle sums gather one
+// 8- to 32-byte record per deposit through the slot order.
 __device__ __forceinline__ void acc_store(double *__restrict__ acc, int nacc, uint32_t s, double y, double heat,
 		double y1, double y2) {
 	if (nacc == 4) {
@@ -494,7 +473,7 @@ __device__ __forceinline__ void settle_capped(int t, bool valid, double tau, dou
 
 template <int NT, bool AFF>
 __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
-		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern, const uint32_t *__restrict__ slot,
+		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
 		const double *__restrict__ lambdaH, const float *__restrict__ mass, const PhysParams &P, int want_heat,
 		double *__restrict__ acc, DepShared &sh, unsigned &nsat, double &lost, int bar) {
 	const int lane = t & 31, wid = t >> 5;
@@ -507,7 +486,6 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 	double TM = Nph;
 	bool done = skip_ray;
 	// the next step's loads are issued one step ahead
-	uint32_t np_slot = 0;
 	double np_kern = 0.0, np_lam = 0.0;
 	float np_mass = 1.0f;
 	{
@@ -515,7 +493,6 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 		if (h < h1) {
 			const uint32_t p = hipar[h];
 			np_kern = hkern[h];
-			np_slot = slot[h];
 			if (!done) { np_lam = lambdaH[p]; np_mass = mass[p]; }
 		}
 	}
@@ -524,13 +501,12 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 		const bool valid = h < h1;
 		const double kern_c = np_kern, lam_c = np_lam;
 		const float mass_c = np_mass;
-		const uint32_t slot_c = np_slot;
+		const uint32_t slot_c = (uint32_t)h;      // (a hit's deposits sit at its own index)
 		{
 			const int64_t hn = h + NT;
 			if (hn < h1) {
 				const uint32_t p = hipar[hn];
 				np_kern = hkern[hn];
-				np_slot = slot[hn];
 				if (!done) { np_lam = lambdaH[p]; np_mass = mass[p]; }
 			}
 		}
@@ -629,12 +605,12 @@ __device__ void deposit_ray(const psg_ray &ray, int64_t h0, int64_t h1, int t,
 // scan runs over the sum of the three species' optical depths; a hit
 // absorbs tau_s/tausum of the photons per species, each capped at its
 // atoms (loop.c:476-505); it writes yGdepHI, heat, yGdepHeI and yGdepHeII
-// increments (nacc of them per slot), with the secondary
+// increments (nacc of them per hit), with the secondary
 // ionisation and heating of loop.c:513-552 (whose HeII terms the
 // reference's statements drop, loop.c:523,542).
 template <int NT>
 __device__ void deposit_ray_gen(const psg_ray &ray, int64_t h0, int64_t h1, int t,
-		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern, const uint32_t *__restrict__ slot,
+		const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
 		const double *__restrict__ lambdaH, const float *__restrict__ mass, const PhysParams &P, int want_heat,
 		double *__restrict__ acc, int nacc, DepShared &sh, unsigned &nsat, double &lost, int bar) {
 	const int lane = t & 31, wid = t >> 5;
@@ -649,7 +625,6 @@ __device__ void deposit_ray_gen(const psg_ray &ray, int64_t h0, int64_t h1, int 
 	double TM = Nph;
 	bool done = skip_ray;
 	// the next step's loads are issued one step ahead
-	uint32_t np_slot = 0;
 	double np_kern = 0.0, np_lam = 0.0, np_l1 = 0.0, np_l2 = 0.0;
 	float np_mass = 1.0f;
 	{
@@ -657,7 +632,6 @@ __device__ void deposit_ray_gen(const psg_ray &ray, int64_t h0, int64_t h1, int 
 		if (h < h1) {
 			const uint32_t p = hipar[h];
 			np_kern = hkern[h];
-			np_slot = slot[h];
 			if (!done) { np_lam = lambdaH[p]; np_mass = mass[p]; np_l1 = P.lamHeI[p]; np_l2 = P.lamHeII[p]; }
 		}
 	}
@@ -666,13 +640,12 @@ __device__ void deposit_ray_gen(const psg_ray &ray, int64_t h0, int64_t h1, int 
 		const bool valid = h < h1;
 		const double kern_c = np_kern, lam_c = np_lam, l1_c = np_l1, l2_c = np_l2;
 		const float mass_c = np_mass;
-		const uint32_t slot_c = np_slot;
+		const uint32_t slot_c = (uint32_t)h;      // (a hit's deposits sit at its own index)
 		{
 			const int64_t hn = h + NT;
 			if (hn < h1) {
 				const uint32_t p = hipar[hn];
 				np_kern = hkern[hn];
-				np_slot = slot[hn];
 				if (!done) { np_lam = lambdaH[p]; np_mass = mass[p]; np_l1 = P.lamHeI[p]; np_l2 = P.lamHeII[p]; }
 			}
 		}
@@ -843,7 +816,7 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(int t, const TickRay
 		const uint32_t *__restrict__ long_rays, const uint32_t *__restrict__ mid_rays,
 		const uint32_t *__restrict__ short_rays,
 		const int64_t *__restrict__ off, const uint32_t *__restrict__ hipar, const double *__restrict__ hkern,
-		const uint32_t *__restrict__ slot, const double *__restrict__ lambdaH, const float *__restrict__ mass,
+		const double *__restrict__ lambdaH, const float *__restrict__ mass,
 		PhysParams P, int want_heat, double *__restrict__ acc, int nacc, unsigned long long *__restrict__ n_sat,
 		double *__restrict__ lost) {
 	__shared__ DepShared sh_block;
@@ -867,10 +840,10 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(int t, const TickRay
 		if (u < nlong) {
 			const uint32_t r = long_rays[T.l0 + u];
 			if (GEN)
-				deposit_ray_gen<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
+				deposit_ray_gen<DEP_THREADS>(rays[r], off[r], off[r + 1], tid, hipar, hkern, lambdaH, mass, P,
 						want_heat, acc, nacc, sh_block, nsat, tm_lost, 0);
 			else
-				deposit_ray<DEP_THREADS, AFF>(rays[r], off[r], off[r + 1], tid, hipar, hkern, slot, lambdaH, mass, P,
+				deposit_ray<DEP_THREADS, AFF>(rays[r], off[r], off[r + 1], tid, hipar, hkern, lambdaH, mass, P,
 						want_heat, acc, sh_block, nsat, tm_lost, 0);
 		} else if (u < nlong + nmid_blocks) {
 			const int q = tid >> 7;
@@ -878,10 +851,10 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(int t, const TickRay
 			if (m < nmid) {
 				const uint32_t r = mid_rays[T.m0 + m];
 				if (GEN)
-					deposit_ray_gen<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
+					deposit_ray_gen<128>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, lambdaH, mass, P,
 							want_heat, acc, nacc, sh_quarter[q], nsat, tm_lost, 1 + q);
 				else
-					deposit_ray<128, AFF>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, slot, lambdaH, mass, P,
+					deposit_ray<128, AFF>(rays[r], off[r], off[r + 1], tid & 127, hipar, hkern, lambdaH, mass, P,
 							want_heat, acc, sh_quarter[q], nsat, tm_lost, 1 + q);
 			}
 		} else {
@@ -890,10 +863,10 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(int t, const TickRay
 				const uint32_t r = short_rays[T.s0 + w];
 				if (off[r + 1] > off[r]) {
 					if (GEN)
-						deposit_ray_gen<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
+						deposit_ray_gen<32>(rays[r], off[r], off[r + 1], lane, hipar, hkern, lambdaH, mass, P,
 								want_heat, acc, nacc, sh_warp[wid], nsat, tm_lost, 0);
 					else
-						deposit_ray<32, AFF>(rays[r], off[r], off[r + 1], lane, hipar, hkern, slot, lambdaH, mass, P,
+						deposit_ray<32, AFF>(rays[r], off[r], off[r + 1], lane, hipar, hkern, lambdaH, mass, P,
 								want_heat, acc, sh_warp[wid], nsat, tm_lost, 0);
 				}
 			}
@@ -1059,9 +1032,9 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 
 // One long deposit segment [b0, b1) summed by a warp: lanes strided over
 // it (eight loads in flight per lane), then a fixed butterfly; every lane
-// ends with the totals.
-__device__ __forceinline__ void warp_segment_sum(const double *__restrict__ acc, int want_heat, uint32_t b0,
-		uint32_t b1, int lane, double &sg, double &sh, int &sn) {
+// ends with the totals. Slot k's deposits sit at hit vals[k].
+__device__ __forceinline__ void warp_segment_sum(const double *__restrict__ acc, const uint32_t *__restrict__ vals,
+		int want_heat, uint32_t b0, uint32_t b1, int lane, double &sg, double &sh, int &sn) {
 	sg = 0.0;
 	sh = 0.0;
 	sn = 0;
@@ -1069,28 +1042,34 @@ __device__ __forceinline__ void warp_segment_sum(const double *__restrict__ acc,
 	if (want_heat) {
 		const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
 		for (; k + 7 * 32 < b1; k += 8 * 32) {
+			uint32_t hv[8];
 			double2 v[8];
 #pragma unroll
-			for (int u = 0; u < 8; u++) v[u] = acc2[k + 32 * u];
+			for (int u = 0; u < 8; u++) hv[u] = vals[k + 32 * u];
+#pragma unroll
+			for (int u = 0; u < 8; u++) v[u] = acc2[hv[u]];
 #pragma unroll
 			for (int u = 0; u < 8; u++)
 				if (v[u].x >= 0.0) { sg += v[u].x; sh += v[u].y; sn++; }
 		}
 		for (; k < b1; k += 32) {
-			const double2 d = acc2[k];
+			const double2 d = acc2[vals[k]];
 			if (d.x >= 0.0) { sg += d.x; sh += d.y; sn++; }
 		}
 	} else {
 		for (; k + 7 * 32 < b1; k += 8 * 32) {
+			uint32_t hv[8];
 			double v[8];
 #pragma unroll
-			for (int u = 0; u < 8; u++) v[u] = acc[k + 32 * u];
+			for (int u = 0; u < 8; u++) hv[u] = vals[k + 32 * u];
+#pragma unroll
+			for (int u = 0; u < 8; u++) v[u] = acc[hv[u]];
 #pragma unroll
 			for (int u = 0; u < 8; u++)
 				if (v[u] >= 0.0) { sg += v[u]; sn++; }
 		}
 		for (; k < b1; k += 32) {
-			const double d = acc[k];
+			const double d = acc[vals[k]];
 			if (d >= 0.0) { sg += d; sn++; }
 		}
 	}
@@ -1106,7 +1085,8 @@ __device__ __forceinline__ void warp_segment_sum(const double *__restrict__ acc,
 // their sums for the integrator (act_g, act_heat) and the deposit counters.
 // The integrator sums the short ones itself while it builds its records.
 __global__ void __launch_bounds__(256) k_sum_long(int t, const uint32_t *__restrict__ act_ipar,
-		const uint32_t *__restrict__ act_seg, const double *__restrict__ acc, int want_heat,
+		const uint32_t *__restrict__ act_seg, const double *__restrict__ acc, const uint32_t *__restrict__ vals,
+		int want_heat,
 		const uint32_t *__restrict__ long_act, const int32_t *__restrict__ tick_long, int32_t *__restrict__ hits,
 		double *__restrict__ act_g, double *__restrict__ act_heat) {
 	const int lane = threadIdx.x & 31;
@@ -1116,7 +1096,7 @@ __global__ void __launch_bounds__(256) k_sum_long(int t, const uint32_t *__restr
 		const int a = (int)long_act[e];
 		double sg, sh;
 		int sn;
-		warp_segment_sum(acc, want_heat, act_seg[a], act_seg[a + 1], lane, sg, sh, sn);
+		warp_segment_sum(acc, vals, want_heat, act_seg[a], act_seg[a + 1], lane, sg, sh, sn);
 		if (lane == 0) {
 			act_g[a] = sg;
 			act_heat[a] = sh;
@@ -1134,7 +1114,7 @@ __global__ void __launch_bounds__(256) k_sum_long(int t, const uint32_t *__restr
 template <bool ISO, bool REC>
 __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
-		const double *__restrict__ acc, int want_heat,
+		const double *__restrict__ acc, const uint32_t *__restrict__ vals, int want_heat,
 		const uint32_t *__restrict__ long_act, const int32_t *__restrict__ tick_long,
 		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat,
 		double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit,
@@ -1151,7 +1131,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		const int a = (int)long_act[e];
 		double sg, sh;
 		int sn;
-		warp_segment_sum(acc, want_heat, act_seg[a], act_seg[a + 1], lane, sg, sh, sn);
+		warp_segment_sum(acc, vals, want_heat, act_seg[a], act_seg[a + 1], lane, sg, sh, sn);
 		if (lane == 0)
 			finish_particle<ISO, REC>(a, sg, sh, sn, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
 					hstep, rec, lo, gcarry, P, tick, tick_time, status);
@@ -1162,11 +1142,12 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		double g = 0.0, heat = 0.0;
 		int nh = 0;
 		for (uint32_t k = s0; k < s1; k++) {
+			const uint32_t hk = vals[k];
 			if (want_heat) {
-				const double2 d = reinterpret_cast<const double2 *>(acc)[k];
+				const double2 d = reinterpret_cast<const double2 *>(acc)[hk];
 				if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
 			} else {
-				const double d = acc[k];
+				const double d = acc[hk];
 				if (d >= 0.0) { g += d; nh++; }
 			}
 		}
@@ -1192,6 +1173,7 @@ struct StiffItem {
 struct UpdSrc {
 	const uint32_t *act_ipar, *act_seg;
 	const double *acc;
+	const uint32_t *vals;       // slot -> hit (a hit's deposits sit at its index)
 	const double *act_g, *act_heat;
 	int want_heat, pre_all;
 	int32_t *hits;
@@ -1237,11 +1219,12 @@ __global__ void __launch_bounds__(32 * UPD_WARPS, MINB) k_update_queue(int t, co
 			} else {
 				int nh = 0;
 				for (uint32_t q = s0; q < s1; q++) {
+					const uint32_t hq = src.vals[q];
 					if (src.want_heat) {
-						const double2 d = reinterpret_cast<const double2 *>(src.acc)[q];
+						const double2 d = reinterpret_cast<const double2 *>(src.acc)[hq];
 						if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
 					} else {
-						const double d = src.acc[q];
+						const double d = src.acc[hq];
 						if (d >= 0.0) { g += d; nh++; }
 					}
 				}
@@ -1302,7 +1285,7 @@ __global__ void __launch_bounds__(32 * UPD_WARPS, MINB) k_update_queue(int t, co
 				S.rec = 0.0;
 				rhs<REC, true>(P, cx, S.x, S.k1, &S.krec);
 				atol1 = DP_ATOL1_REL * fabs(ie0) + 1e-300;
-				dp_init_k1(S);
+				dp_init_k1(S, DP_RTOL_TICK);
 				// the particle's last step proposal is a better first
 				// step than the derivative estimate
 				if (r.hstep > 0.0f) S.h = fmin(1.0, fmax((double)r.hstep / r.time, 1e-8));
@@ -1313,7 +1296,7 @@ __global__ void __launch_bounds__(32 * UPD_WARPS, MINB) k_update_queue(int t, co
 		}
 		if (!__any_sync(0xffffffffu, have)) break;
 		if (have) {
-			const bool done = dp_step<REC>(P, cx, S, atol1);
+			const bool done = dp_step<REC>(P, cx, S, atol1, DP_RTOL_TICK);
 			if (!done && S.steps >= DP_SWITCH) {
 				// stiff: hand the particle to k_update_stiff and free the lane
 				const unsigned q = atomicAdd(nstiff, 1u);
@@ -1426,7 +1409,7 @@ __device__ __forceinline__ void he_write(const PhysParams &P, uint32_t p, const 
 template <bool REC>
 __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg, const double *__restrict__ acc,
-		int want_heat,
+		const uint32_t *__restrict__ vals, int want_heat,
 		int32_t *__restrict__ hits, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P,
 		const PsgBatchDev *__restrict__ B, HeStiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff,
@@ -1441,9 +1424,10 @@ __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__re
 	int nh = 0;
 	const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
 	for (uint32_t k = s0; k < s1; k++) {
-		const double2 a = acc2[2 * (size_t)k];
+		const size_t hk = vals[k];
+		const double2 a = acc2[2 * hk];
 		if (a.x >= 0.0) {
-			const double2 b = acc2[2 * (size_t)k + 1];
+			const double2 b = acc2[2 * hk + 1];
 			g0 += a.x;
 			g1 += b.x;
 			g2 += b.y;
@@ -1849,7 +1833,7 @@ int plan_batch(psg_context *ctx, size_t R, size_t K, const PsgTraceFill &tf, Bat
 	int rc = psg_trace_sort_prepare(ctx, nray, cap, pl.maxcount);
 	if (rc) return rc;
 	// slots and the active lists
-	if (!psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * cap) || !psg_scratch(ctx, S_SLOT, sizeof(uint32_t) * cap) ||
+	if (!psg_scratch(ctx, S_VALS, sizeof(uint32_t) * 2 * cap) ||
 			!psg_scratch(ctx, S_ACC, sizeof(double) * cap * pl.nacc) || !psg_scratch(ctx, S_ACT, act_bytes(pl)) ||
 			!psg_scratch(ctx, S_SLOTCNT, slotcnt_bytes(pl)))
 		return PSG_E_NOMEM;
@@ -1910,7 +1894,6 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	// slots, counted, placed, then put in hit order
 	psg_mark_begin(ctx, PSG_K_SLOTS);
 	uint32_t *vals = (uint32_t *)ctx->scratch[S_VALS].p;
-	uint32_t *slot = (uint32_t *)ctx->scratch[S_SLOT].p;
 	double *acc = (double *)ctx->scratch[S_ACC].p;
 	ActView av = act_view(ctx, pl);
 	uint32_t *kcnt = (uint32_t *)ctx->scratch[S_SLOTCNT].p;
@@ -1929,7 +1912,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 			kbase, av.act_ipar, av.act_seg, av.tick_act, d_nact);
 	PSG_CHECK_LAUNCH();
 	k_slot_canon<<<(unsigned)std::min<size_t>(blocks(cap, 1024), (size_t)sms * 6), 32 * CANON_WARPS, 0, st>>>(
-			av.tick_act, (int)K, av.act_seg, vals, slot);
+			av.tick_act, (int)K, av.act_seg, vals);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 8;
 	unsigned long long *d_nsat = ctx->d_counters + 1;      // (zeroed by the caller, per call)
@@ -1971,13 +1954,13 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	uint32_t *long_act = ll.long_act;
 	// the slot order of the long runs (the short ones are in order already)
 	psg_mark_begin(ctx, PSG_K_SLOTS);
-	k_slot_canon_warp<<<(unsigned)(4 * sms), 32 * SLOT_WARPS, 0, st>>>(tick_long, (int)K, long_act, av.act_seg, vals,
-			slot);
+	k_slot_canon_warp<<<(unsigned)(4 * sms), 32 * SLOT_WARPS, 0, st>>>(tick_long, (int)K, long_act, av.act_seg,
+			vals);
 	PSG_CHECK_LAUNCH();
-	k_slot_canon_mid<<<(unsigned)(4 * sms), 256, 0, st>>>(ll.mid_list, ll.mid_count, av.act_seg, vals, slot);
+	k_slot_canon_mid<<<(unsigned)(4 * sms), 256, 0, st>>>(ll.mid_list, ll.mid_count, av.act_seg, vals);
 	PSG_CHECK_LAUNCH();
 	k_slot_canon_long<<<(unsigned)sms, 1024, sizeof(uint32_t) * std::max(pl.long_cap, 2048), st>>>(ll.vl_list,
-			ll.vl_count, av.act_seg, vals, slot, pl.long_cap, cap);
+			ll.vl_count, av.act_seg, vals, pl.long_cap, cap);
 	PSG_CHECK_LAUNCH();
 	psg_mark_end(ctx);
 	ctx->launches += 6;
@@ -1988,15 +1971,15 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 		psg_mark_begin(ctx, PSG_K_DEPOSIT);
 		if (pl.gen)
 			k_deposit<true, false><<<pl.dep_grid, DEP_THREADS, 0, st>>>((int)t, uv.tick_rays, uv.dep_ctr, B,
-					long_rays, mid_rays, short_rays, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+					long_rays, mid_rays, short_rays, off64, hit_ipar, hit_kern, ctx->d_lambdaH, ctx->d_mass, P,
 					pl.want_heat, acc, pl.nacc, d_nsat, d_lost);
 		else if (pl.aff)
 			k_deposit<false, true><<<pl.dep_grid, DEP_THREADS, 0, st>>>((int)t, uv.tick_rays, uv.dep_ctr, B,
-					long_rays, mid_rays, short_rays, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+					long_rays, mid_rays, short_rays, off64, hit_ipar, hit_kern, ctx->d_lambdaH, ctx->d_mass, P,
 					pl.want_heat, acc, pl.nacc, d_nsat, d_lost);
 		else
 			k_deposit<false, false><<<pl.dep_grid, DEP_THREADS, 0, st>>>((int)t, uv.tick_rays, uv.dep_ctr, B,
-					long_rays, mid_rays, short_rays, off64, hit_ipar, hit_kern, slot, ctx->d_lambdaH, ctx->d_mass, P,
+					long_rays, mid_rays, short_rays, off64, hit_ipar, hit_kern, ctx->d_lambdaH, ctx->d_mass, P,
 					pl.want_heat, acc, pl.nacc, d_nsat, d_lost);
 		PSG_CHECK_LAUNCH();
 		ctx->launches++;
@@ -2005,11 +1988,11 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 		if (pl.helium) {
 			if (P.ygrec)
 				k_update_he<true><<<pl.he_grid, 128, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc,
-						pl.want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
+						vals, pl.want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
 						ctx->d_yeMET, P, B, hstiff, uv.nstiff + t, ctx->d_status);
 			else
 				k_update_he<false><<<pl.he_grid, 128, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc,
-						pl.want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
+						vals, pl.want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
 						ctx->d_yeMET, P, B, hstiff, uv.nstiff + t, ctx->d_status);
 			PSG_CHECK_LAUNCH();
 			k_update_he_stiff<<<sms, 64, 0, st>>>(hstiff, uv.nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
@@ -2024,7 +2007,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 			double *keep_g = pre_all ? uv.act_g : nullptr;
 			double *keep_heat = pre_all ? uv.act_heat : nullptr;
 #define PSG_REDUCE(ISO_, REC_)                                                                                 \
-	k_reduce<ISO_, REC_><<<pl.red_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc,      \
+	k_reduce<ISO_, REC_><<<pl.red_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc, vals,\
 			pl.want_heat, long_act, tick_long, ctx->d_hits, keep_g, keep_heat, ctx->d_lambdaH, ctx->d_ie,       \
 			ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, B, ctx->d_status)
 			if (pl.iso && !pl.euler) {
@@ -2034,7 +2017,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 				if (P.ygrec) PSG_REDUCE(false, true);
 				else PSG_REDUCE(false, false);
 			} else {
-				k_sum_long<<<pl.red_grid, 256, 0, st>>>((int)t, av.act_ipar, av.act_seg, acc, pl.want_heat, long_act,
+				k_sum_long<<<pl.red_grid, 256, 0, st>>>((int)t, av.act_ipar, av.act_seg, acc, vals, pl.want_heat, long_act,
 						tick_long, ctx->d_hits, uv.act_g, uv.act_heat);
 			}
 #undef PSG_REDUCE
@@ -2050,6 +2033,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 				us.act_ipar = av.act_ipar;
 				us.act_seg = av.act_seg;
 				us.acc = acc;
+				us.vals = vals;
 				us.act_g = uv.act_g;
 				us.act_heat = uv.act_heat;
 				us.want_heat = pl.want_heat;
