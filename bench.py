@@ -48,15 +48,18 @@ SIDE_LEGS = ("iliev32", "iliev64", "lognormal128")
 # Algorithmic bytes. Per hit (the whole path): pos 12 + sml 4 + lambdaH 8 +
 # mass 4 + FP64 absorbed photons 8. Per kernel group, per unit it processes:
 # trace fill reads pos+sml (16) and writes (ipar 4, d 8, b 8) per hit; the
-# sort reads and writes (ipar, d, b) and writes the kernel value; slots read
-# ipar and write a slot per hit; deposit reads (ipar 4, kern 8, slot 4) and
-# the hit particle's lambdaH 8 and mass 4 and writes an FP64 deposit per hit
-# (36 B), plus an FP64 heat when not isothermal (DEPOSIT_HEAT_BYTES); the
-# update reads ~60 B and writes ~40 B of particle state per active (tick,
-# particle) pair.
+# sort reads the slab (ipar, d, b: 20), writes the sorted lists (20) and
+# gathers the smoothing length (16) for the kernel value; the slot
+# order reads ipar twice (8), writes the hit into its run and reads and
+# writes it once more in the run sort (12), plus the per-(tick, particle)
+# counters and their scan (12 B per key, ~4 B per hit here): 24 B; deposit
+# reads (ipar 4, kern 8) and the hit particle's lambdaH 8 and mass 4 and
+# writes an FP64 deposit per hit (32 B), plus an FP64 heat when not
+# isothermal (DEPOSIT_HEAT_BYTES); the update reads ~60 B and writes ~40 B
+# of particle state per active (tick, particle) pair.
 BYTES_PER_HIT = 36
-GROUP_BYTES = {"trace_count": (16, "hit"), "trace_fill": (36, "hit"), "sort": (60, "hit"),
-               "slots": (48, "hit"), "deposit": (36, "hit"), "update": (100, "active particle")}
+GROUP_BYTES = {"trace_count": (16, "hit"), "trace_fill": (36, "hit"), "sort": (56, "hit"),
+               "slots": (24, "hit"), "deposit": (32, "hit"), "update": (100, "active particle")}
 DEPOSIT_HEAT_BYTES = 8
 
 
