@@ -250,7 +250,7 @@ __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const
 }
 
 // Adaptive Dormand-Prince 5(4) over s in [0,1]. LSODA runs the reference at
-// rtol 1e-4 (solve.c:151-152); 1e-6 and 1e-5 here (below). The state of one integration is a
+// rtol 1e-4 (solve.c:151-152); 1e-6 here. The state of one integration is a
 // DPState; dp_init() evaluates the first derivative and picks the first step
 // (about a 1% change of each component, components near zero measured
 // against atol/rtol), dp_step() attempts one step.
@@ -262,23 +262,18 @@ struct DPState {
 	int steps;
 };
 
-// psg_step_evolve integrates at DP_RTOL; the ticks' work queue at
-// DP_RTOL_TICK, ten times tighter than the reference's LSODA still (its
-// right-hand side is only continuous -- rates linear in log T between table
-// rows -- so integrations at different tolerances agree to ~1e-5 anyway).
 #define DP_RTOL 1e-6
-#define DP_RTOL_TICK 1e-5
 #define DP_ATOL0 1e-10
 #define DP_ATOL1_REL 1e-8
 
 // First step from the derivative S.k1 = f(S.x), already evaluated.
-__device__ __forceinline__ void dp_init_k1(DPState &S, double rtol = DP_RTOL) {
+__device__ __forceinline__ void dp_init_k1(DPState &S) {
 	S.t = 0.0;
 	S.steps = 0;
 	double h = 1.0;
 	const double atol1 = DP_ATOL1_REL * fabs(S.x[1]) + 1e-300;
 	for (int i = 0; i < 2; i++) {
-		const double scale = fabs(S.x[i]) + (i == 0 ? DP_ATOL0 : atol1) / rtol;
+		const double scale = fabs(S.x[i]) + (i == 0 ? DP_ATOL0 : atol1) / DP_RTOL;
 		const double f = fabs(S.k1[i]);
 		if (f > 0.0) h = fmin(h, 0.01 * scale / f);
 	}
@@ -305,8 +300,7 @@ __device__ __forceinline__ void dp_init(const PhysParams &P, const RhsCtx &cx, D
 
 // One attempted step; returns true once s = 1 is reached.
 template <bool REC = false>
-__device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, DPState &S, double atol1,
-		double rtol = DP_RTOL) {
+__device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, DPState &S, double atol1) {
 	const double a21 = 1. / 5, a31 = 3. / 40, a32 = 9. / 40, a41 = 44. / 45, a42 = -56. / 15, a43 = 32. / 9;
 	const double a51 = 19372. / 6561, a52 = -25360. / 2187, a53 = 64448. / 6561, a54 = -212. / 729;
 	const double a61 = 9017. / 3168, a62 = -355. / 33, a63 = 46732. / 5247, a64 = 49. / 176, a65 = -5103. / 18656;
@@ -335,7 +329,7 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 	double err = 0.0;
 	for (int i = 0; i < 2; i++) {
 		const double e = h * F(e7, k7[i], F(e6, k6[i], F(e5, k5[i], F(e4, k4[i], F(e3, k3[i], e1 * k1[i])))));
-		const double sc = (i == 0 ? DP_ATOL0 : atol1) + rtol * fmax(fabs(x[i]), fabs(yn[i]));
+		const double sc = (i == 0 ? DP_ATOL0 : atol1) + DP_RTOL * fmax(fabs(x[i]), fabs(yn[i]));
 		err += (e / sc) * (e / sc);
 	}
 #undef F

@@ -989,7 +989,7 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 	hits[p] += nh;
 	if (gcarry) g += gcarry[p];      // photons left over by an earlier explicit step (loop.c:745)
 	if (!ISO) {
-		if (act_g) {        // read by the surrogate and the update log only
+		if (act_g) {        // read by the integrator queue, the surrogate and the update log
 			act_g[a] = g;
 			act_heat[a] = heat;
 		}
@@ -1081,30 +1081,6 @@ __device__ __forceinline__ void warp_segment_sum(const double *__restrict__ acc,
 	}
 }
 
-// The tick's long segments only (more deposits than a warp), a warp each:
-// their sums for the integrator (act_g, act_heat) and the deposit counters.
-// The integrator sums the short ones itself while it builds its records.
-__global__ void __launch_bounds__(256) k_sum_long(int t, const uint32_t *__restrict__ act_ipar,
-		const uint32_t *__restrict__ act_seg, const double *__restrict__ acc, const uint32_t *__restrict__ vals,
-		int want_heat,
-		const uint32_t *__restrict__ long_act, const int32_t *__restrict__ tick_long, int32_t *__restrict__ hits,
-		double *__restrict__ act_g, double *__restrict__ act_heat) {
-	const int lane = threadIdx.x & 31;
-	const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
-	for (int e = tick_long[t] + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); e < tick_long[t + 1];
-			e += nwarp) {
-		const int a = (int)long_act[e];
-		double sg, sh;
-		int sn;
-		warp_segment_sum(acc, vals, want_heat, act_seg[a], act_seg[a + 1], lane, sg, sh, sn);
-		if (lane == 0) {
-			act_g[a] = sg;
-			act_heat[a] = sh;
-			hits[act_ipar[a]] += sn;
-		}
-	}
-}
-
 // Per-particle sums of one tick's deposits (photons/NH, heat, deposit count)
 // in slot order. Warps first take the tick's long segments, a warp each
 // (particles are in leaf order, so the long ones are neighbours; giving each
@@ -1167,16 +1143,11 @@ struct StiffItem {
 };
 #define UPD_WARPS 8
 // Where the integrator's records come from: the tick's active particles,
-// their deposit segments (short ones are summed while the record is built;
-// long ones, or all when `pre_all`, were summed into act_g/act_heat before)
-// and the particle state.
+// their summed deposits (act_g, act_heat, from k_reduce) and the particle
+// state.
 struct UpdSrc {
-	const uint32_t *act_ipar, *act_seg;
-	const double *acc;
-	const uint32_t *vals;       // slot -> hit (a hit's deposits sit at its index)
+	const uint32_t *act_ipar;
 	const double *act_g, *act_heat;
-	int want_heat, pre_all;
-	int32_t *hits;
 	const float *rho, *yeMET;
 };
 
@@ -1211,25 +1182,7 @@ __global__ void __launch_bounds__(32 * UPD_WARPS, MINB) k_update_queue(int t, co
 			const unsigned k = base + lane;
 			const int a = alist ? (int)alist[k] : lo + (int)k;
 			const uint32_t p = src.act_ipar[a];
-			double g = 0.0, heat = 0.0;
-			const uint32_t s0 = src.act_seg[a], s1 = src.act_seg[a + 1];
-			if (src.pre_all || s1 - s0 > 32) {
-				g = src.act_g[a];
-				heat = src.act_heat[a];
-			} else {
-				int nh = 0;
-				for (uint32_t q = s0; q < s1; q++) {
-					const uint32_t hq = src.vals[q];
-					if (src.want_heat) {
-						const double2 d = reinterpret_cast<const double2 *>(src.acc)[hq];
-						if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
-					} else {
-						const double d = src.acc[hq];
-						if (d >= 0.0) { g += d; nh++; }
-					}
-				}
-				src.hits[p] += nh;
-			}
+			const double g = src.act_g[a], heat = src.act_heat[a];
 			UpdRec r;
 			r.time = rn_dmul((double)(tick - lasthit[p]), tick_time);
 			r.lam0 = lambdaH[p];
@@ -1285,7 +1238,7 @@ __global__ void __launch_bounds__(32 * UPD_WARPS, MINB) k_update_queue(int t, co
 				S.rec = 0.0;
 				rhs<REC, true>(P, cx, S.x, S.k1, &S.krec);
 				atol1 = DP_ATOL1_REL * fabs(ie0) + 1e-300;
-				dp_init_k1(S, DP_RTOL_TICK);
+				dp_init_k1(S);
 				// the particle's last step proposal is a better first
 				// step than the derivative estimate
 				if (r.hstep > 0.0f) S.h = fmin(1.0, fmax((double)r.hstep / r.time, 1e-8));
@@ -1296,7 +1249,7 @@ __global__ void __launch_bounds__(32 * UPD_WARPS, MINB) k_update_queue(int t, co
 		}
 		if (!__any_sync(0xffffffffu, have)) break;
 		if (have) {
-			const bool done = dp_step<REC>(P, cx, S, atol1, DP_RTOL_TICK);
+			const bool done = dp_step<REC>(P, cx, S, atol1);
 			if (!done && S.steps >= DP_SWITCH) {
 				// stiff: hand the particle to k_update_stiff and free the lane
 				const unsigned q = atomicAdd(nstiff, 1u);
@@ -2001,11 +1954,12 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 			ctx->launches += 2;
 		} else {
 			const double *gcarry = pl.euler ? ctx->d_gcarry : nullptr;
-			// the integrator sums the short segments itself unless every sum
-			// is wanted first (the surrogate, the update log)
-			const bool pre_all = pl.surr || feat;
-			double *keep_g = pre_all ? uv.act_g : nullptr;
-			double *keep_heat = pre_all ? uv.act_heat : nullptr;
+			// not isothermal, every pair's sums first (a thread per short run,
+			// a warp per long one): the integrator then reads two doubles per
+			// particle instead of gathering its deposits in its latency-bound
+			// loop
+			double *keep_g = pl.iso ? nullptr : uv.act_g;
+			double *keep_heat = pl.iso ? nullptr : uv.act_heat;
 #define PSG_REDUCE(ISO_, REC_)                                                                                 \
 	k_reduce<ISO_, REC_><<<pl.red_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc, vals,\
 			pl.want_heat, long_act, tick_long, ctx->d_hits, keep_g, keep_heat, ctx->d_lambdaH, ctx->d_ie,       \
@@ -2013,12 +1967,9 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 			if (pl.iso && !pl.euler) {
 				if (P.ygrec) PSG_REDUCE(true, true);
 				else PSG_REDUCE(true, false);
-			} else if (pl.euler || pre_all) {
+			} else {
 				if (P.ygrec) PSG_REDUCE(false, true);
 				else PSG_REDUCE(false, false);
-			} else {
-				k_sum_long<<<pl.red_grid, 256, 0, st>>>((int)t, av.act_ipar, av.act_seg, acc, vals, pl.want_heat, long_act,
-						tick_long, ctx->d_hits, uv.act_g, uv.act_heat);
 			}
 #undef PSG_REDUCE
 			PSG_CHECK_LAUNCH();
@@ -2031,14 +1982,8 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 			} else if (!pl.iso) {
 				UpdSrc us;
 				us.act_ipar = av.act_ipar;
-				us.act_seg = av.act_seg;
-				us.acc = acc;
-				us.vals = vals;
 				us.act_g = uv.act_g;
 				us.act_heat = uv.act_heat;
-				us.want_heat = pl.want_heat;
-				us.pre_all = pre_all;
-				us.hits = ctx->d_hits;
 				us.rho = ctx->d_rho;
 				us.yeMET = ctx->d_yeMET;
 				if (feat) {
