@@ -11,9 +11,9 @@
 namespace {
 
 // Exclusive scans of the batch (the slots' (count, count > 0) pairs, the
-// traversal's hit counts, the ray and particle classes) in three passes:
-// tile sums, one block scanning the tile sums, each tile's own scan plus
-// its offset. Tiles of 256 threads x 16 items; the element type of the
+// traversal's hit counts, the ray and particle classes) in up to three
+// passes: tile sums, one block scanning the tile sums, each tile's own scan
+// plus its offset. Tiles of 256 threads x 16 items; the element type of the
 // input is mapped to the sum's type V (unsigned 64-bit or double) by Op; out
 // has n + 1 entries (the total last). The order of the additions is fixed
 // by n alone, so a floating-point scan gives the same bits every run.
@@ -66,12 +66,29 @@ __global__ void __launch_bounds__(1024) k_scan_sums(V *__restrict__ tile_sum, si
 	}
 	if (threadIdx.x == 0) tile_sum[ntile] = carry;
 }
-template <typename T, typename Op, typename V>
+// MODE 0: tile_sum holds the tiles' exclusive prefixes (and the total
+// after them); MODE 1: tile_sum holds the raw tile sums, and each block sums
+// the ones before it itself (few tiles); MODE 2: a single tile, no tile sums.
+template <typename T, typename Op, typename V, int MODE>
 __global__ void __launch_bounds__(SCAN_T) k_scan_apply(const T *__restrict__ in, size_t n,
 		const V *__restrict__ tile_sum, V *__restrict__ out, Op op) {
 	using BS = cub::BlockScan<V, SCAN_T>;
+	using BR = cub::BlockReduce<V, SCAN_T>;
 	__shared__ typename BS::TempStorage tmp;
+	__shared__ typename BR::TempStorage rtmp;
+	__shared__ V before_s;
 	const size_t t0 = (size_t)blockIdx.x * SCAN_T * SCAN_I;
+	V before = 0;
+	if (MODE == 0) {
+		before = tile_sum[blockIdx.x];
+	} else if (MODE == 1) {
+		V part = 0;
+		for (unsigned b = threadIdx.x; b < blockIdx.x; b += SCAN_T) part += tile_sum[b];
+		part = BR(rtmp).Sum(part);
+		if (threadIdx.x == 0) before_s = part;
+		__syncthreads();
+		before = before_s;
+	}
 	// blocked layout: thread i holds items t0 + i*16 .. +15
 	V v[SCAN_I];
 	V s = 0;
@@ -83,18 +100,24 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_apply(const T *__restrict__ in,
 	}
 	V x;
 	BS(tmp).ExclusiveSum(s, x);
-	x += tile_sum[blockIdx.x];
+	x += before;
 #pragma unroll
 	for (int u = 0; u < SCAN_I; u++) {
 		const size_t k = t0 + (size_t)threadIdx.x * SCAN_I + u;
 		if (k < n) out[k] = x;
 		x += v[u];
 	}
-	if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = tile_sum[gridDim.x];
+	// the total: the last thread's running sum after its items
+	if (blockIdx.x == gridDim.x - 1 && threadIdx.x == SCAN_T - 1) {
+		if (MODE == 0) out[n] = tile_sum[gridDim.x];
+		else out[n] = x;
+	}
 }
 
-// Issues the three passes on st: out[0..n] (n + 1 entries); tiles: scratch
-// of scan_tiles(n) + 1 entries.
+// Issues the scan on st: out[0..n] (n + 1 entries); tiles: scratch of
+// scan_tiles(n) + 1 entries. One launch for a single tile, two up to
+// SCAN_FEW tiles (each block sums the tile sums before it), three beyond.
+#define SCAN_FEW 256
 inline size_t scan_tiles(size_t n) {
 	const size_t t = (n + (size_t)SCAN_T * SCAN_I - 1) / ((size_t)SCAN_T * SCAN_I);
 	return t ? t : 1;
@@ -102,9 +125,16 @@ inline size_t scan_tiles(size_t n) {
 template <typename T, typename Op, typename V>
 cudaError_t scan_enqueue(cudaStream_t st, const T *in, size_t n, V *out, V *tiles, Op op) {
 	const size_t nt = scan_tiles(n);
-	k_scan_tiles<T, Op, V><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, op);
-	k_scan_sums<V><<<1, 1024, 0, st>>>(tiles, nt);
-	k_scan_apply<T, Op, V><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, out, op);
+	if (nt == 1) {
+		k_scan_apply<T, Op, V, 2><<<1, SCAN_T, 0, st>>>(in, n, tiles, out, op);
+	} else if (nt <= SCAN_FEW) {
+		k_scan_tiles<T, Op, V><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, op);
+		k_scan_apply<T, Op, V, 1><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, out, op);
+	} else {
+		k_scan_tiles<T, Op, V><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, op);
+		k_scan_sums<V><<<1, 1024, 0, st>>>(tiles, nt);
+		k_scan_apply<T, Op, V, 0><<<(unsigned)nt, SCAN_T, 0, st>>>(in, n, tiles, out, op);
+	}
 	return cudaGetLastError();
 }
 
