@@ -235,8 +235,8 @@ typedef struct {
 	int trace_warps;        /* warps per traversal block, 1-16 (default 4) */
 	int deposit_long;       /* rays with more hits than this take a 128-thread group (default 96) ... */
 	int deposit_mid;        /* ... more than this a 512-thread block (default 384); fewer take a warp */
-	int update_minblocks;   /* 3: the integrator's registers capped for 3 resident blocks per
-	                         * multiprocessor (spilling the rest); 1: uncapped (default) */
+	int update_minblocks;   /* 3 or 4: the integrator's registers capped for that many resident
+	                         * blocks per multiprocessor (spilling the rest); 1: uncapped (default) */
 	int leaf_size;          /* particles per octree leaf: the reference's CFG_OCTTREE_PPC, 8; the hit
 	                         * lists are bit-exact only with the reference's leaves, so it is reported,
 	                         * never searched */

@@ -1816,8 +1816,9 @@ int plan_batch(psg_context *ctx, size_t R, size_t K, const PsgTraceFill &tf, Bat
 			: (pl.aff ? occ_grid(ctx, k_deposit<false, true>, DEP_THREADS) : occ_grid(ctx, k_deposit<false, false>,
 					DEP_THREADS));
 	pl.red_grid = occ_grid(ctx, k_reduce<false, false>, 256);
-	pl.queue_minb = ctx->tune.update_minblocks >= 3 ? 3 : 1;
-	pl.queue_grid = pl.queue_minb == 3 ? occ_grid(ctx, k_update_queue<false, 3>, 32 * UPD_WARPS)
+	pl.queue_minb = ctx->tune.update_minblocks >= 4 ? 4 : (ctx->tune.update_minblocks == 3 ? 3 : 1);
+	pl.queue_grid = pl.queue_minb == 4 ? occ_grid(ctx, k_update_queue<false, 4>, 32 * UPD_WARPS)
+			: pl.queue_minb == 3 ? occ_grid(ctx, k_update_queue<false, 3>, 32 * UPD_WARPS)
 			: occ_grid(ctx, k_update_queue<false, 1>, 32 * UPD_WARPS);
 	pl.he_grid = occ_grid(ctx, k_update_he<false>, 128);
 	pl.euler_grid = occ_grid(ctx, k_update_euler, 128);
@@ -2010,7 +2011,8 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	k_update_queue<false, MINB_><<<pl.queue_grid, 32 * UPD_WARPS, 0, st>>>((int)t, av.tick_act, us,          \
 			ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, B, uv.cursors + t, uv.stiff,           \
 			uv.nstiff + t, pl.surr ? uv.rej : nullptr, pl.surr ? uv.nrej + t : nullptr, ctx->d_status)
-					if (pl.queue_minb == 3) PSG_QUEUE(3);
+					if (pl.queue_minb == 4) PSG_QUEUE(4);
+					else if (pl.queue_minb == 3) PSG_QUEUE(3);
 					else PSG_QUEUE(1);
 #undef PSG_QUEUE
 					PSG_CHECK_LAUNCH();
@@ -2432,7 +2434,7 @@ extern "C" int psg_autotune(psg_context *ctx, const psg_ray *d_rays, size_t R, s
 		rc = consider(t);
 	}
 	// the integrator's registers (occupancy against spills)
-	for (int mb : {1, 3}) {
+	for (int mb : {1, 3, 4}) {
 		if (rc || mb == cur.update_minblocks) continue;
 		psg_tune t = cur;
 		t.update_minblocks = mb;
