@@ -289,7 +289,7 @@ __device__ __forceinline__ void put_sorted_hit(int64_t h, uint32_t p, const uint
 // Per-ray sort by (d, ipar), one ray per block of TPR threads holding IPT
 // hits each: a block radix sort (passes of 4 bits) on d mapped to KEY_BITS
 // bits over the ray's own range of d (a monotone map) -- 12 bits for up to
-// 256 hits, 16 up to 2048, 20 beyond, so that about n^2 / 2^(bits+1) pairs
+// 1024 hits, 16 up to 4096, 20 beyond, so that about n^2 / 2^(bits+1) pairs
 // share a key -- and the few runs of equal keys are then insertion-sorted
 // on the exact (d, ipar) -- the reference's d
 // order (loop.c:783-787) with ties broken by the caller's particle index. With want_kern the b column is replaced by the
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 		dlo = fmin(dlo, sm.lo[w]);
 		dhi = fmax(dhi, sm.hi[w]);
 	}
-	constexpr int KEY_BITS = NMAX <= 256 ? 12 : (NMAX <= 2048 ? 16 : 20);
+	constexpr int KEY_BITS = NMAX <= 1024 ? 12 : (NMAX <= 4096 ? 16 : 20);
 	constexpr uint32_t KEY_MAX = (1u << KEY_BITS) - 1u;
 	const double scale = dhi > dlo ? (double)KEY_MAX / (dhi - dlo) : 0.0;
 	uint32_t k[IPT], v[IPT];
