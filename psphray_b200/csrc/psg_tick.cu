@@ -93,12 +93,12 @@ inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs);
 // ---- the by-particle order without a key sort ------------------------------
 // The slots of a batch: every hit of tick t on particle p gets a place in the
 // (t, p, hit index) order. Counting instead of sorting: per (t, p) key the
-// number of hits (atomics; the counters are zero before and after), one
-// exclusive scan of the (count, count > 0) pairs over the K*N keys gives each
-// key its first slot and its active-particle index, a second pass places
-// every hit in its key's run (any order), and a last pass puts each run in
-// hit-index order -- the order a stable key sort gives, so the per-particle
-// sums downstream add in the same order as before, bit for bit.
+// number of hits (atomics on counters zeroed per batch), one exclusive scan
+// of the (count, count > 0) pairs over the K*N keys gives each key its first
+// slot and its active-particle index, a second pass places every hit in its
+// key's run (any order), and a last pass puts each run in hit-index order --
+// the order a stable key sort gives, so the per-particle sums downstream add
+// in a fixed order.
 
 // one warp per ray: count the ray's hits per key (tick * N + particle)
 __global__ void k_slot_count(size_t nray, int R, uint32_t N, const int64_t *__restrict__ off,
@@ -110,33 +110,19 @@ __global__ void k_slot_count(size_t nray, int R, uint32_t N, const int64_t *__re
 	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32) atomicAdd(&cnt[base + ipar[h]], 1u);
 }
 
-// one warp per ray: every hit into its key's run (rank from the counter,
-// which returns to zero); vals[slot] = the hit
-__global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__restrict__ off,
-		const uint32_t *__restrict__ ipar, uint32_t *__restrict__ cnt, const unsigned long long *__restrict__ base,
-		uint32_t *__restrict__ vals) {
-	const size_t r = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32;
-	const int lane = threadIdx.x & 31;
-	if (r >= nray) return;
-	const size_t kb = (r / (size_t)R) * N;
-	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32) {
-		const size_t key = kb + ipar[h];
-		const uint32_t rank = atomicSub(&cnt[key], 1u) - 1u;
-		vals[(uint32_t)base[key] + rank] = (uint32_t)h;
-	}
-}
-
 // the active (tick, particle) pairs in key order: their particle and first
-// slot, the first pair of every tick and the totals
+// slot, the first pair of every tick and the totals; and every key's
+// counter set to the end of its run, for the placement below
 __global__ void k_act_build(size_t KN, uint32_t N, int K, const unsigned long long *__restrict__ base,
 		uint32_t *__restrict__ act_ipar, uint32_t *__restrict__ act_seg, int32_t *__restrict__ tick_act,
-		unsigned long long *__restrict__ nact_out) {
+		unsigned long long *__restrict__ nact_out, uint32_t *__restrict__ cnt) {
 	for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < KN; k += (size_t)gridDim.x * blockDim.x) {
 		const unsigned long long b0 = base[k], b1 = base[k + 1];
 		const uint32_t a = (uint32_t)(b0 >> 32);
 		if ((uint32_t)(b1 >> 32) != a) {
 			act_ipar[a] = (uint32_t)(k % N);
 			act_seg[a] = (uint32_t)b0;
+			cnt[k] = (uint32_t)b1;
 		}
 		if (k % N == 0) tick_act[k / N] = (int32_t)a;
 	}
@@ -147,6 +133,19 @@ __global__ void k_act_build(size_t KN, uint32_t N, int K, const unsigned long lo
 		act_seg[nact] = (uint32_t)tot;
 		atomicAdd(nact_out, (unsigned long long)nact);     // over the call's batches
 	}
+}
+
+// one warp per ray: every hit into its key's run, at the slot its counter
+// (the run's end, counting down) gives; vals[slot] = the hit. The counters
+// are left at the runs' first slots (zeroed before the next batch).
+__global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__restrict__ off,
+		const uint32_t *__restrict__ ipar, uint32_t *__restrict__ cnt, uint32_t *__restrict__ vals) {
+	const size_t r = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32;
+	const int lane = threadIdx.x & 31;
+	if (r >= nray) return;
+	const size_t kb = (r / (size_t)R) * N;
+	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32)
+		vals[atomicSub(&cnt[kb + ipar[h]], 1u) - 1u] = (uint32_t)h;
 }
 
 // Runs of up to 32 hits. A warp takes 32 consecutive pairs; their slots
@@ -1859,11 +1858,11 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	k_slot_count<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt);
 	PSG_CHECK_LAUNCH();
 	PSG_CUDA(scan_enqueue(st, kcnt, pl.KN, kbase, tiles, SlotPair()));
-	k_slot_place<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt, kbase, vals);
-	PSG_CHECK_LAUNCH();
 	unsigned long long *d_nact = ctx->d_counters + 6;
 	k_act_build<<<(unsigned)std::min<size_t>(blocks(pl.KN, 256), (size_t)sms * 16), 256, 0, st>>>(pl.KN, N, (int)K,
-			kbase, av.act_ipar, av.act_seg, av.tick_act, d_nact);
+			kbase, av.act_ipar, av.act_seg, av.tick_act, d_nact, kcnt);
+	PSG_CHECK_LAUNCH();
+	k_slot_place<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt, vals);
 	PSG_CHECK_LAUNCH();
 	k_slot_canon<<<(unsigned)std::min<size_t>(blocks(cap, 1024), (size_t)sms * 6), 32 * CANON_WARPS, 0, st>>>(
 			av.tick_act, (int)K, av.act_seg, vals);
