@@ -96,9 +96,10 @@ inline unsigned blocks(size_t n, int bs) { return (unsigned)((n + bs - 1) / bs);
 // number of hits (atomics on counters zeroed per batch), one exclusive scan
 // of the (count, count > 0) pairs over the K*N keys gives each key its first
 // slot and its active-particle index, a second pass places every hit in its
-// key's run (any order), and a last pass puts each run in hit-index order --
-// the order a stable key sort gives, so the per-particle sums downstream add
-// in a fixed order.
+// key's run (any order), and the runs longer than 32 are sorted into
+// hit-index order -- the order a stable key sort gives; the per-particle
+// sums read the shorter ones in hit order by selection (next_in_run), so
+// every sum adds in a fixed order.
 
 // one warp per ray: count the ray's hits per key (tick * N + particle)
 __global__ void k_slot_count(size_t nray, int R, uint32_t N, const int64_t *__restrict__ off,
@@ -146,63 +147,6 @@ __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__re
 	const size_t kb = (r / (size_t)R) * N;
 	for (int64_t h = off[r] + lane; h < off[r + 1]; h += 32)
 		vals[atomicSub(&cnt[kb + ipar[h]], 1u) - 1u] = (uint32_t)h;
-}
-
-// Runs of up to 32 hits. A warp takes 32 consecutive pairs; their slots
-// are contiguous, so the warp loads them into shared memory with coalesced
-// reads, each lane insertion-sorts its own run there, and the warp writes
-// the span back. Longer runs inside the span are copied unchanged (their
-// own sorts follow); a span over SLOT_SPAN slots takes the lane-by-lane
-// form from device memory.
-#define SLOT_SPAN 1024
-#define CANON_WARPS 8
-__global__ void __launch_bounds__(32 * CANON_WARPS) k_slot_canon(const int32_t *__restrict__ tick_act, int K,
-		const uint32_t *__restrict__ act_seg, uint32_t *__restrict__ vals) {
-	__shared__ uint32_t buf[CANON_WARPS][SLOT_SPAN];
-	uint32_t *sv = buf[threadIdx.x >> 5];
-	const int lane = threadIdx.x & 31;
-	const uint32_t na = (uint32_t)tick_act[K];
-	const uint32_t stride = gridDim.x * CANON_WARPS * 32;
-	for (uint32_t a0 = (blockIdx.x * CANON_WARPS + (threadIdx.x >> 5)) * 32; a0 < na; a0 += stride) {
-		const uint32_t a = a0 + lane;
-		const uint32_t S0 = act_seg[a0], S1 = act_seg[min(a0 + 32, na)];
-		uint32_t s0 = 0, n = 0;
-		if (a < na) {
-			s0 = act_seg[a];
-			n = act_seg[a + 1] - s0;
-		}
-		if (S1 - S0 <= SLOT_SPAN) {
-			for (uint32_t i = lane; i < S1 - S0; i += 32) sv[i] = vals[S0 + i];
-			__syncwarp();
-			if (n >= 2 && n <= 32) {
-				uint32_t *r = sv + (s0 - S0);
-				for (uint32_t i = 1; i < n; i++) {
-					const uint32_t x = r[i];
-					uint32_t j = i;
-					while (j > 0 && r[j - 1] > x) {
-						r[j] = r[j - 1];
-						j--;
-					}
-					r[j] = x;
-				}
-			}
-			__syncwarp();
-			for (uint32_t i = lane; i < S1 - S0; i += 32) vals[S0 + i] = sv[i];
-			__syncwarp();
-		} else if (n >= 2 && n <= 32) {
-			uint32_t v[32];
-			for (uint32_t i = 0; i < n; i++) {
-				const uint32_t x = vals[s0 + i];
-				uint32_t j = i;
-				while (j > 0 && v[j - 1] > x) {
-					v[j] = v[j - 1];
-					j--;
-				}
-				v[j] = x;
-			}
-			for (uint32_t i = 0; i < n; i++) vals[s0 + i] = v[i];
-		}
-	}
 }
 
 // Runs longer than 32 (particles next to a source), in three tiers: up to
@@ -1029,6 +973,20 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 	if (st) atomicOr(status, st);
 }
 
+// Runs of up to 32 hits stay in placement order (arbitrary); their sums go
+// in hit order all the same: each step takes the smallest hit index above
+// the last one (n^2 reads of the run's entries, all in L1; runs average
+// under 4 hits). Longer runs are sorted and read in order.
+__device__ __forceinline__ uint32_t next_in_run(const uint32_t *__restrict__ vals, uint32_t s0, uint32_t s1,
+		int64_t prev) {
+	uint32_t best = 0xFFFFFFFFu;
+	for (uint32_t q = s0; q < s1; q++) {
+		const uint32_t v = vals[q];
+		if ((int64_t)v > prev && v < best) best = v;
+	}
+	return best;
+}
+
 // One long deposit segment [b0, b1) summed by a warp: lanes strided over
 // it (eight loads in flight per lane), then a fixed butterfly; every lane
 // ends with the totals. Slot k's deposits sit at hit vals[k].
@@ -1116,8 +1074,10 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		if (s1 - s0 > 32) continue;
 		double g = 0.0, heat = 0.0;
 		int nh = 0;
+		int64_t prev = -1;
 		for (uint32_t k = s0; k < s1; k++) {
-			const uint32_t hk = vals[k];
+			const uint32_t hk = next_in_run(vals, s0, s1, prev);
+			prev = hk;
 			if (want_heat) {
 				const double2 d = reinterpret_cast<const double2 *>(acc)[hk];
 				if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
@@ -1375,8 +1335,11 @@ __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__re
 	double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
 	int nh = 0;
 	const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
+	const bool short_run = s1 - s0 <= 32;
+	int64_t prev = -1;
 	for (uint32_t k = s0; k < s1; k++) {
-		const size_t hk = vals[k];
+		const size_t hk = short_run ? next_in_run(vals, s0, s1, prev) : vals[k];
+		prev = (int64_t)hk;
 		const double2 a = acc2[2 * hk];
 		if (a.x >= 0.0) {
 			const double2 b = acc2[2 * hk + 1];
@@ -1863,9 +1826,6 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 			kbase, av.act_ipar, av.act_seg, av.tick_act, d_nact, kcnt);
 	PSG_CHECK_LAUNCH();
 	k_slot_place<<<blocks(nray * 32, 256), 256, 0, st>>>(nray, (int)R, N, off64, hit_ipar, kcnt, vals);
-	PSG_CHECK_LAUNCH();
-	k_slot_canon<<<(unsigned)std::min<size_t>(blocks(cap, 1024), (size_t)sms * 6), 32 * CANON_WARPS, 0, st>>>(
-			av.tick_act, (int)K, av.act_seg, vals);
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 8;
 	unsigned long long *d_nsat = ctx->d_counters + 1;      // (zeroed by the caller, per call)
