@@ -31,6 +31,7 @@ enum {
 	S_RAYS = 0, S_COUNT, S_OFFSETS, S_RAW_IPAR, S_RAW_D, S_RAW_B, S_KEYS, S_VALS,
 	S_HIT_IPAR, S_HIT_KERN, S_ACC, S_ACT, S_CUB, S_TREE, S_MISC, S_REC_U32, S_REC_F64, S_RAYLIST, S_UPD,
 	S_EMIT, S_MAP, S_ALONG, S_MLP, S_LOG, S_SURR, S_REC, S_RECW, S_RECK, S_RECRAYS, S_SNAP, S_SCAN, S_SLOTCNT,
+	S_SRCHIT,
 	S_NSLOTS
 };
 
@@ -123,6 +124,8 @@ struct psg_context {
 	size_t rec_last_R = 0;       // source rays of that tick
 	size_t rec_last_kmax = 0;    // capacity of that tick's item arrays (S_RECK)
 	int rec_last_threshold = 0;  // that tick ran in threshold mode (its items unsorted, in place)
+	size_t src_nray = 0;         // S_SRCHIT: the call's source rays traced and sorted before its ticks ran
+	size_t src_nhit = 0;         //   (offsets[src_nray + 1], ipar[src_nhit], kernel factor[src_nhit])
 
 	// chemistry surrogate (not isothermal): weight blob, residual tolerance
 	void *d_surr = nullptr;
@@ -242,10 +245,19 @@ struct PsgTraceFill {
 };
 int psg_trace_fill(psg_context *ctx, const psg_ray *d_rays, size_t nray, PsgTraceFill *tf);
 int psg_trace_sort_prepare(psg_context *ctx, size_t nray, size_t cap, unsigned long long maxcount);
-int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned long long maxcount, int want_kern);
+int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned long long maxcount, int want_kern,
+		size_t r0);
 int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_kern);
 int psg_trace_fill_prepare(psg_context *ctx, size_t nray);
 int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray, const unsigned *nlim, size_t cap);
+// A recombination tick whose R source rays were traced and sorted with the
+// call's (S_SRCHIT): their counts and sorted hits come from there, only the
+// emitted rays behind them (at most cap_rec, *nlim of them) are traversed.
+int psg_trace_rec_fill_enqueue(psg_context *ctx, const psg_ray *buf, size_t R, size_t cap_rec, const unsigned *nlim,
+		size_t cap, const PsgBatchDev *B);
+int psg_trace_rec_sort_enqueue(psg_context *ctx, size_t R, size_t nray, unsigned long long maxcount,
+		const PsgBatchDev *B);
+int psg_trace_src_batch(psg_context *ctx, const psg_ray *d_rays, size_t nray);
 
 // ---- device helpers ------------------------------------------------------------
 // Single-rounding float/double ops: the reference is compiled for x86-64 SSE

@@ -1600,6 +1600,7 @@ struct BatchPlan {
 	// grids
 	unsigned dep_grid = 0, red_grid = 0, queue_grid = 0, he_grid = 0, euler_grid = 0, log_grid = 0;
 	int queue_minb = 1;         // the integrator's register limit: resident blocks per SM
+	size_t src_R = 0;           // > 0: a recombination tick whose first src_R rays come traced and sorted (S_SRCHIT)
 };
 
 struct GraphEntry {
@@ -1800,7 +1801,8 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	const size_t R = pl.R, K = pl.K, nray = pl.nray, cap = pl.cap;
 	const PhysParams P = psg_phys_params(ctx);
 	const int sms = ctx->sms;
-	int rc = psg_trace_sort_enqueue(ctx, nray, pl.nhit, pl.maxcount, 1);
+	int rc = pl.src_R ? psg_trace_rec_sort_enqueue(ctx, pl.src_R, nray, pl.maxcount, B)
+			: psg_trace_sort_enqueue(ctx, nray, pl.nhit, pl.maxcount, 1, 0);
 	if (rc) return rc;
 	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
 	uint32_t *hit_ipar = (uint32_t *)ctx->scratch[S_HIT_IPAR].p;
@@ -2029,6 +2031,9 @@ std::vector<unsigned long long> batch_key(const psg_context *ctx, const BatchPla
 	k.push_back(ctx->hit_cap);
 	k.push_back((unsigned long long)ctx->tune.deposit_long << 32 | (unsigned)ctx->tune.deposit_mid);
 	k.push_back((unsigned long long)pl.queue_minb);
+	k.push_back(pl.src_R);
+	k.push_back(ctx->src_nray);
+	k.push_back(ctx->src_nhit);
 	return k;
 }
 
@@ -2098,7 +2103,7 @@ __global__ void k_rec_src(const PsgBatchDev *__restrict__ B, size_t R, psg_ray *
 __global__ void k_rec_nlim(size_t R, const unsigned *__restrict__ count, unsigned long long *__restrict__ nlim,
 		unsigned long long *__restrict__ recsum) {
 	const unsigned M = count[0] + count[1] + count[2];
-	*(unsigned *)nlim = (unsigned)R + M;
+	*(unsigned *)nlim = M;      // the emitted rays to traverse (the source rays come traced)
 	*recsum += M;
 }
 __global__ void k_rec_tick_end(const int64_t *__restrict__ off, size_t nray, unsigned long long *__restrict__ hitsum,
@@ -2228,11 +2233,17 @@ int psg_run_ticks_rec_graph(psg_context *ctx, const psg_ray *d_rays, size_t R, s
 	ctx->host_syncs = 0;
 	psg_ray *buf = (psg_ray *)psg_scratch(ctx, S_RECRAYS, sizeof(psg_ray) * nray);
 	if (!buf) return PSG_E_NOMEM;
-	int rc = psg_trace_fill_prepare(ctx, nray);
+	// the call's source rays do not depend on the ticks' updates: traced and
+	// sorted together first (one host wait), each tick traverses only the
+	// rays it emits
+	int rc = psg_trace_src_batch(ctx, d_rays, R * K);
+	if (rc) return rc;
+	rc = psg_trace_fill_prepare(ctx, nray);
 	if (!rc) rc = psg_rec_prepare(ctx);
 	if (rc) return rc;
 	PsgTraceFill tf{ctx->batch_cap, ctx->slab_cap, ctx->slab_cap};
 	BatchPlan pl;
+	pl.src_R = R;
 	rc = plan_batch(ctx, nray, 1, tf, pl);
 	if (rc) return rc;
 	rc = psg_state_save(ctx);      // (the undo if a tick outgrows the buffers)
@@ -2255,7 +2266,7 @@ int psg_run_ticks_rec_graph(psg_context *ctx, const psg_ray *d_rays, size_t R, s
 		if (r) return r;
 		k_rec_nlim<<<1, 1, 0, st>>>(R, (const unsigned *)(cnt + 11), cnt + 15, cnt + 14);
 		PSG_CHECK_LAUNCH();
-		r = psg_trace_fill_enqueue(ctx, buf, nray, nlim, pl.cap);
+		r = psg_trace_rec_fill_enqueue(ctx, buf, R, cap_rec, nlim, pl.cap, B);
 		if (r) return r;
 		r = enqueue_any(ctx, pl, B);
 		if (r) return r;

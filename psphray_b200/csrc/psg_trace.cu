@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 		const int64_t *__restrict__ off, size_t scap, const uint32_t *__restrict__ slab_ipar,
 		const double *__restrict__ slab_d, const double *__restrict__ slab_b, uint32_t *__restrict__ out_ipar,
 		double *__restrict__ out_d, double *__restrict__ out_b, int want_kern, const float4 *__restrict__ psml,
-		PhysParams P, const uint32_t *__restrict__ order) {
+		PhysParams P, const uint32_t *__restrict__ order, size_t slab_r0) {
 	constexpr int NMAX = TPR * IPT;
 	using Sort = cub::BlockRadixSort<uint32_t, TPR, IPT, uint32_t, 4>;
 	struct Smem {
@@ -318,8 +318,8 @@ __global__ void __launch_bounds__(TPR) k_sort_block(const uint32_t *__restrict__
 	const size_t r = list[li];
 	const int64_t h0 = off[r];
 	const int n = (int)(off[r + 1] - h0);
-	const uint32_t *raw_ipar = slab_ipar + r * scap;
-	const double *raw_d = slab_d + r * scap, *raw_b = slab_b + r * scap;
+	const uint32_t *raw_ipar = slab_ipar + (r - slab_r0) * scap;
+	const double *raw_d = slab_d + (r - slab_r0) * scap, *raw_b = slab_b + (r - slab_r0) * scap;
 	// keys: d mapped onto 24 bits over the ray's [min, max] (monotone, so
 	// equal keys only ever hide an order the fix-up below restores)
 	double dv[IPT];
@@ -421,7 +421,8 @@ __global__ void __launch_bounds__(LONG_NT) k_sort_long(const uint32_t *__restric
 		const unsigned long long *__restrict__ d_nlist, const int64_t *__restrict__ off, size_t scap,
 		const uint32_t *__restrict__ slab_ipar, const double *__restrict__ slab_d, const double *__restrict__ slab_b,
 		uint32_t *__restrict__ out_ipar, double *__restrict__ out_d, double *__restrict__ out_b, int want_kern,
-		const float4 *__restrict__ psml, PhysParams P, const uint32_t *__restrict__ order, LongHit *tmp, size_t hb) {
+		const float4 *__restrict__ psml, PhysParams P, const uint32_t *__restrict__ order, LongHit *tmp, size_t hb,
+		size_t slab_r0) {
 	__shared__ LongHit tile[2 * LONG_NT];
 	const LongHit pad{__longlong_as_double(0x7ff0000000000000ll), ~0ull};
 	const unsigned long long nlist = *d_nlist;
@@ -429,8 +430,8 @@ __global__ void __launch_bounds__(LONG_NT) k_sort_long(const uint32_t *__restric
 		const size_t r = list[li];
 		const int64_t h0 = off[r];
 		const int64_t n = off[r + 1] - h0;
-		const uint32_t *raw_ipar = slab_ipar + r * scap;
-		const double *raw_d = slab_d + r * scap, *raw_b = slab_b + r * scap;
+		const uint32_t *raw_ipar = slab_ipar + (r - slab_r0) * scap;
+		const double *raw_d = slab_d + (r - slab_r0) * scap, *raw_b = slab_b + (r - slab_r0) * scap;
 		LongHit *a = tmp + h0;
 		for (int64_t i = threadIdx.x; i < n; i += LONG_NT)
 			a[i] = LongHit{raw_d[i], (unsigned long long)caller_index(order, raw_ipar[i]) << 32 | (unsigned long long)i};
@@ -449,9 +450,10 @@ __global__ void __launch_bounds__(LONG_NT) k_sort_long(const uint32_t *__restric
 #define SORT_NCLS 8
 __constant__ int kSortBounds[SORT_NCLS] = {64, 128, 256, 512, 1024, 2048, 4096, PSG_SORT_MAX};
 
-__global__ void k_sort_classify(size_t nray, const int64_t *__restrict__ off, uint32_t *__restrict__ lists,
+// rays [r0, nray) into the size classes' lists
+__global__ void k_sort_classify(size_t r0, size_t nray, const int64_t *__restrict__ off, uint32_t *__restrict__ lists,
 		size_t stride, unsigned long long *__restrict__ nclass, unsigned long long *__restrict__ nlong) {
-	const size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+	const size_t r = r0 + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
 	if (r >= nray) return;
 	const int64_t n = off[r + 1] - off[r];
 	if (n == 0) return;
@@ -526,6 +528,128 @@ int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray,
 	PSG_CHECK_LAUNCH();
 	ctx->launches += 3;
 	return PSG_OK;
+}
+
+namespace {
+// The tick's source-ray counts from the call's traced source rays (the tick
+// is B->k of the call).
+__global__ void k_src_counts(const PsgBatchDev *__restrict__ B, size_t R, const int64_t *__restrict__ src_off,
+		uint32_t *__restrict__ count) {
+	const int64_t base = B->k * (int64_t)R;
+	for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < R; r += (size_t)gridDim.x * blockDim.x)
+		count[r] = (uint32_t)(src_off[base + (int64_t)r + 1] - src_off[base + (int64_t)r]);
+}
+// their sorted hits into the tick's lists, a warp per ray (nothing when the
+// tick's offsets were emptied for exceeding the capacity)
+__global__ void k_copy_src_hits(const PsgBatchDev *__restrict__ B, size_t R, const int64_t *__restrict__ src_off,
+		const uint32_t *__restrict__ src_ipar, const double *__restrict__ src_kern, const int64_t *__restrict__ off,
+		uint32_t *__restrict__ hit_ipar, double *__restrict__ hit_kern) {
+	const size_t r = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) / 32;
+	const int lane = threadIdx.x & 31;
+	if (r >= R) return;
+	const int64_t base = B->k * (int64_t)R + (int64_t)r;
+	const int64_t s0 = src_off[base];
+	const int64_t n = min(src_off[base + 1] - s0, off[r + 1] - off[r]);
+	const int64_t d0 = off[r];
+	for (int64_t i = lane; i < n; i += 32) {
+		hit_ipar[d0 + i] = src_ipar[s0 + i];
+		hit_kern[d0 + i] = src_kern[s0 + i];
+	}
+}
+}  // namespace
+
+struct SrcHits {
+	const int64_t *off;
+	const uint32_t *ipar;
+	const double *kern;
+};
+static SrcHits src_hits(psg_context *ctx) {
+	char *m = (char *)ctx->scratch[S_SRCHIT].p;
+	SrcHits h;
+	h.off = (const int64_t *)m;
+	h.kern = (const double *)(m + sizeof(int64_t) * (ctx->src_nray + 1));
+	h.ipar = (const uint32_t *)(h.kern + ctx->src_nhit);
+	return h;
+}
+
+// All source rays of a recombination call traced and sorted (with the
+// column-density factor) before its ticks run; kept in S_SRCHIT. One host
+// synchronisation (the traversal's).
+int psg_trace_src_batch(psg_context *ctx, const psg_ray *d_rays, size_t nray) {
+	PsgTraceFill tf;
+	int rc = psg_trace_fill(ctx, d_rays, nray, &tf);
+	if (!rc) rc = psg_trace_sort_prepare(ctx, nray, tf.nhit, tf.maxcount);
+	if (!rc) rc = psg_trace_sort_enqueue(ctx, nray, tf.nhit, tf.maxcount, 1, 0);
+	if (rc) return rc;
+	char *m = (char *)psg_scratch(ctx, S_SRCHIT, sizeof(int64_t) * (nray + 1) + (sizeof(double) + sizeof(uint32_t)) *
+			(tf.nhit ? tf.nhit : 1));
+	if (!m) return PSG_E_NOMEM;
+	ctx->src_nray = nray;
+	ctx->src_nhit = tf.nhit;
+	const SrcHits h = src_hits(ctx);
+	cudaStream_t st = ctx->stream;
+	PSG_CUDA(cudaMemcpyAsync((void *)h.off, ctx->scratch[S_OFFSETS].p, sizeof(int64_t) * (nray + 1),
+			cudaMemcpyDeviceToDevice, st));
+	if (tf.nhit) {
+		PSG_CUDA(cudaMemcpyAsync((void *)h.ipar, ctx->scratch[S_HIT_IPAR].p, sizeof(uint32_t) * tf.nhit,
+				cudaMemcpyDeviceToDevice, st));
+		PSG_CUDA(cudaMemcpyAsync((void *)h.kern, ctx->scratch[S_HIT_KERN].p, sizeof(double) * tf.nhit,
+				cudaMemcpyDeviceToDevice, st));
+	}
+	return PSG_OK;
+}
+
+// The traversal of a recombination tick: the source rays' counts from
+// S_SRCHIT, the emitted rays buf[R, R + *nlim) traversed (slabs from index
+// 0), then the scan and the offsets over all R + cap_rec rays.
+int psg_trace_rec_fill_enqueue(psg_context *ctx, const psg_ray *buf, size_t R, size_t cap_rec, const unsigned *nlim,
+		size_t cap, const PsgBatchDev *B) {
+	cudaStream_t st = ctx->stream;
+	const size_t nray = R + cap_rec;
+	uint32_t *count = (uint32_t *)ctx->scratch[S_COUNT].p;
+	unsigned long long *scan = count_scan(count, nray);
+	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
+	unsigned long long *d_max = ctx->d_counters + 4;
+	unsigned long long *next_ray = ctx->d_counters + 9;
+	const size_t scap = ctx->slab_cap;
+	const size_t slots = cap_rec * scap;
+	uint32_t *slab_ipar = (uint32_t *)ctx->scratch[S_REC_U32].p;
+	double *slab_f64 = (double *)ctx->scratch[S_REC_F64].p;
+	const int trw = std::max(1, std::min(TR_MAX_WARPS, ctx->tune.trace_warps));
+	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ctx->ppc + 32) * trw;
+	const SrcHits h = src_hits(ctx);
+	PSG_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t) * (nray + 1), st));
+	PSG_CUDA(cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned long long), st));
+	PSG_CUDA(cudaMemsetAsync(next_ray, 0, sizeof(unsigned long long), st));
+	k_src_counts<<<(unsigned)std::min<size_t>(blocks(R, 256), 4 * (size_t)ctx->sms), 256, 0, st>>>(B, R, h.off,
+			count);
+	PSG_CHECK_LAUNCH();
+	k_trace_stack<<<ctx->trace_grid, 32 * trw, smem, st>>>(buf + R, cap_rec, ctx->d_wide_lo, ctx->d_wide_hi,
+			ctx->d_leaf_psml, ctx->d_leaf_idx, ctx->ppc, count + R, scap, slab_ipar, slab_f64, slab_f64 + slots,
+			next_ray, ctx->d_status, nlim);
+	PSG_CHECK_LAUNCH();
+	k_count_clamp<<<blocks(cap_rec, 256), 256, 0, st>>>(cap_rec, scap, count + R, ctx->d_counters + 3,
+			ctx->d_status);
+	PSG_CHECK_LAUNCH();
+	PSG_CUDA(scan_enqueue(st, count, nray + 1, scan, (unsigned long long *)ctx->scratch[S_SCAN].p, Widen()));
+	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, d_max, cap,
+			ctx->d_counters + 24, ctx->d_status);
+	PSG_CHECK_LAUNCH();
+	ctx->launches += 5;
+	return PSG_OK;
+}
+
+// The per-ray order of a recombination tick: the source rays' sorted hits
+// copied from S_SRCHIT, the emitted rays (from R on) sorted from their slabs.
+int psg_trace_rec_sort_enqueue(psg_context *ctx, size_t R, size_t nray, unsigned long long maxcount,
+		const PsgBatchDev *B) {
+	const SrcHits h = src_hits(ctx);
+	k_copy_src_hits<<<blocks(R * 32, 256), 256, 0, ctx->stream>>>(B, R, h.off, h.ipar, h.kern,
+			(const int64_t *)ctx->scratch[S_OFFSETS].p, (uint32_t *)ctx->scratch[S_HIT_IPAR].p,
+			(double *)ctx->scratch[S_HIT_KERN].p);
+	PSG_CHECK_LAUNCH();
+	ctx->launches++;
+	return psg_trace_sort_enqueue(ctx, nray, 0, maxcount, 1, R);
 }
 
 // Sizes the buffers psg_trace_fill_enqueue uses for nray rays (allocates;
@@ -662,12 +786,12 @@ int psg_trace_sort_prepare(psg_context *ctx, size_t nray, size_t cap, unsigned l
 // ray counts on the device), so it can be captured in a graph; with
 // maxcount above PSG_SORT_MAX the long rays' kernel runs too.
 int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned long long maxcount,
-		int want_kern) {
+		int want_kern, size_t r0) {
 	(void)nhit;
 	cudaStream_t st = ctx->stream;
 	const size_t hb = ctx->hit_cap;
 	const size_t scap = ctx->slab_cap;
-	const size_t slots = nray * scap;
+	const size_t slots = (nray - r0) * scap;
 	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
 	uint32_t *hit_ipar = (uint32_t *)ctx->scratch[S_HIT_IPAR].p;
 	double *hit_d = (double *)ctx->scratch[S_RAW_D].p + hb;
@@ -675,21 +799,21 @@ int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned 
 	uint32_t *slab_ipar = (uint32_t *)ctx->scratch[S_REC_U32].p;
 	double *slab_d = (double *)ctx->scratch[S_REC_F64].p;
 	double *slab_b = slab_d + slots;
-	if (nray == 0) return PSG_OK;
+	if (nray <= r0) return PSG_OK;
 	psg_mark_begin(ctx, PSG_K_SORT);
 	{
 		uint32_t *lists = (uint32_t *)ctx->scratch[S_RAYLIST].p;
 		unsigned long long *d_ncls = ctx->d_counters + 16, *d_nlong = ctx->d_counters + 25;
 		PSG_CUDA(cudaMemsetAsync(d_ncls, 0, SORT_NCLS * sizeof(unsigned long long), st));
 		PSG_CUDA(cudaMemsetAsync(d_nlong, 0, sizeof(unsigned long long), st));
-		k_sort_classify<<<blocks(nray, 256), 256, 0, st>>>(nray, off64, lists, nray + 1, d_ncls, d_nlong);
+		k_sort_classify<<<blocks(nray - r0, 256), 256, 0, st>>>(r0, nray, off64, lists, nray + 1, d_ncls, d_nlong);
 		PSG_CHECK_LAUNCH();
 		const PhysParams PP = psg_phys_params(ctx);
 		const size_t stride = nray + 1;
 		auto launch_block = [&](auto kern, int tpr, size_t smem, int c) -> int {
-			const unsigned grid = (unsigned)std::min<size_t>(nray, (size_t)ctx->sort_grid[c]);
+			const unsigned grid = (unsigned)std::min<size_t>(nray - r0, (size_t)ctx->sort_grid[c]);
 			kern<<<grid, tpr, smem, st>>>(lists + c * stride, d_ncls + c, off64, scap, slab_ipar, slab_d,
-					slab_b, hit_ipar, hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order);
+					slab_b, hit_ipar, hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order, r0);
 			PSG_CHECK_LAUNCH();
 			ctx->launches++;
 			return PSG_OK;
@@ -706,10 +830,10 @@ int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned 
 		ctx->launches++;
 		if (maxcount > PSG_SORT_MAX) {
 			// rays longer than the shared-memory classes: a block each
-			const unsigned grid = (unsigned)std::min<size_t>(nray, (size_t)ctx->sms);
+			const unsigned grid = (unsigned)std::min<size_t>(nray - r0, (size_t)ctx->sms);
 			k_sort_long<<<grid, LONG_NT, 0, st>>>(lists + SORT_NCLS * stride, d_nlong, off64, scap, slab_ipar,
 					slab_d, slab_b, hit_ipar, hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order,
-					(LongHit *)ctx->scratch[S_KEYS].p, hb);
+					(LongHit *)ctx->scratch[S_KEYS].p, hb, r0);
 			PSG_CHECK_LAUNCH();
 			ctx->launches++;
 		}
@@ -728,7 +852,7 @@ int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int
 	if (rc) return rc;
 	rc = psg_trace_sort_prepare(ctx, nray, tf.nhit, tf.maxcount);
 	if (rc) return rc;
-	return psg_trace_sort_enqueue(ctx, nray, tf.nhit, tf.maxcount, want_kern);
+	return psg_trace_sort_enqueue(ctx, nray, tf.nhit, tf.maxcount, want_kern, 0);
 }
 
 __global__ void k_caller_index(size_t n, const uint32_t *__restrict__ in, const uint32_t *__restrict__ order,
