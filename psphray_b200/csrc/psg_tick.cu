@@ -149,7 +149,7 @@ __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__re
 		vals[atomicSub(&cnt[kb + ipar[h]], 1u) - 1u] = (uint32_t)h;
 }
 
-// Runs longer than 32 (particles next to a source), in three tiers: up to
+// Runs longer than RUN_SHORT (particles next to a source), in three tiers: up to
 // SLOT_WARP_MAX hits a warp each (bitonic sort in the warp's part of
 // shared memory); up to SLOT_MID_MAX a 256-thread block each (bitonic in
 // shared memory); longer ones a 1024-thread block each, bitonic in shared
@@ -158,6 +158,7 @@ __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__re
 // than SLOT_LONG_MAX rays of one tick on one particle), with the upper half
 // of vals (from half) as scratch. The two block tiers take their runs from
 // lists of their own.
+#define RUN_SHORT 8          // runs up to this many hits are summed by selection, longer ones sorted
 #define SLOT_WARP_MAX 256
 #define SLOT_MID_MAX 2048
 #define SLOT_LONG_MAX 32768
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(32 * SLOT_WARPS) k_slot_canon_warp(const int32
 		const uint32_t a = long_act[e];
 		const uint32_t s0 = act_seg[a], n = act_seg[a + 1] - s0;
 		if (n > SLOT_WARP_MAX) continue;
-		int P = 64;
+		int P = 16;
 		while (P < (int)n) P <<= 1;
 		for (int i = lane; i < P; i += 32) sv[i] = i < (int)n ? vals[s0 + i] : 0xFFFFFFFFu;
 		__syncwarp();
@@ -870,7 +871,7 @@ __global__ void k_ray_lists(size_t nray, const unsigned long long *__restrict__ 
 // The active count of the batch, nact = tick_act[K], is read on the device;
 // flags cover the capacity cap + 1 (zero past nact) so the scan's size is
 // fixed.
-// The active pairs whose run is longer than 32 hits, per tick (their order
+// The active pairs whose run is longer than RUN_SHORT hits, per tick (their order
 // within a tick is free: each is summed and sorted on its own). Counted per
 // tick, the K counts scanned by one block, then listed; runs longer than
 // SLOT_WARP_MAX also go to the lists of the two block sorts.
@@ -887,7 +888,7 @@ __global__ void k_long_count(const int32_t *__restrict__ tick_act, int K, const 
 		unsigned long long *__restrict__ tick_cnt) {
 	const int na = tick_act[K];
 	for (int a = (int)(blockIdx.x * blockDim.x + threadIdx.x); a < na; a += (int)(gridDim.x * blockDim.x))
-		if (act_seg[a + 1] - act_seg[a] > 32) atomicAdd(&tick_cnt[tick_of_pair(tick_act, K, a)], 1ull);
+		if (act_seg[a + 1] - act_seg[a] > RUN_SHORT) atomicAdd(&tick_cnt[tick_of_pair(tick_act, K, a)], 1ull);
 }
 __global__ void k_long_place(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
 		const unsigned long long *__restrict__ tick_off, unsigned *__restrict__ cursor,
@@ -898,7 +899,7 @@ __global__ void k_long_place(const int32_t *__restrict__ tick_act, int K, const 
 	for (int t = i0; t <= K; t += (int)(gridDim.x * blockDim.x)) tick_long[t] = (int32_t)tick_off[t];
 	for (int a = i0; a < na; a += (int)(gridDim.x * blockDim.x)) {
 		const uint32_t n = act_seg[a + 1] - act_seg[a];
-		if (n <= 32) continue;
+		if (n <= RUN_SHORT) continue;
 		const int t = tick_of_pair(tick_act, K, a);
 		long_act[tick_off[t] + atomicAdd(&cursor[t], 1u)] = (uint32_t)a;
 		if (n > SLOT_MID_MAX) vl_list[atomicAdd(vl_count, 1u)] = (uint32_t)a;
@@ -973,10 +974,10 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 	if (st) atomicOr(status, st);
 }
 
-// Runs of up to 32 hits stay in placement order (arbitrary); their sums go
-// in hit order all the same: each step takes the smallest hit index above
-// the last one (n^2 reads of the run's entries, all in L1; runs average
-// under 4 hits). Longer runs are sorted and read in order.
+// Runs of up to RUN_SHORT hits stay in placement order (arbitrary); their
+// sums go in hit order all the same: each step takes the smallest hit index
+// above the last one (at most 64 reads of the run's entries, in L1; runs
+// average under 4 hits). Longer runs are sorted and read in order.
 __device__ __forceinline__ uint32_t next_in_run(const uint32_t *__restrict__ vals, uint32_t s0, uint32_t s1,
 		int64_t prev) {
 	uint32_t best = 0xFFFFFFFFu;
@@ -1071,7 +1072,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 	}
 	for (int a = lo + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi; a += (int)(gridDim.x * blockDim.x)) {
 		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
-		if (s1 - s0 > 32) continue;
+		if (s1 - s0 > RUN_SHORT) continue;
 		double g = 0.0, heat = 0.0;
 		int nh = 0;
 		int64_t prev = -1;
@@ -1335,7 +1336,7 @@ __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__re
 	double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
 	int nh = 0;
 	const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
-	const bool short_run = s1 - s0 <= 32;
+	const bool short_run = s1 - s0 <= RUN_SHORT;
 	int64_t prev = -1;
 	for (uint32_t k = s0; k < s1; k++) {
 		const size_t hk = short_run ? next_in_run(vals, s0, s1, prev) : vals[k];
