@@ -159,6 +159,7 @@ __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__re
 // of vals (from half) as scratch. The two block tiers take their runs from
 // lists of their own.
 #define RUN_SHORT 8          // runs up to this many hits are summed by selection, longer ones sorted
+#define RUN_THREAD 32        // runs up to this many hits are summed by a thread, longer ones by a warp
 #define SLOT_WARP_MAX 256
 #define SLOT_MID_MAX 2048
 #define SLOT_LONG_MAX 32768
@@ -884,24 +885,42 @@ __device__ __forceinline__ int tick_of_pair(const int32_t *__restrict__ tick_act
 	}
 	return lo;
 }
+// (a warp's pairs are consecutive and mostly of one tick: one atomic per
+// tick per warp, the lanes ranked within it)
 __global__ void k_long_count(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
 		unsigned long long *__restrict__ tick_cnt) {
 	const int na = tick_act[K];
-	for (int a = (int)(blockIdx.x * blockDim.x + threadIdx.x); a < na; a += (int)(gridDim.x * blockDim.x))
-		if (act_seg[a + 1] - act_seg[a] > RUN_SHORT) atomicAdd(&tick_cnt[tick_of_pair(tick_act, K, a)], 1ull);
+	const int lane = threadIdx.x & 31;
+	const int stride = (int)(gridDim.x * blockDim.x);
+	for (int a0 = (int)(blockIdx.x * blockDim.x + threadIdx.x) - lane; a0 < na; a0 += stride) {
+		const int a = a0 + lane;
+		const bool is_long = a < na && act_seg[a + 1] - act_seg[a] > RUN_SHORT;
+		const int t = is_long ? tick_of_pair(tick_act, K, a) : -1;
+		const unsigned grp = __match_any_sync(0xffffffffu, t);
+		if (is_long && lane == __ffs(grp) - 1) atomicAdd(&tick_cnt[t], (unsigned long long)__popc(grp));
+	}
 }
 __global__ void k_long_place(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
 		const unsigned long long *__restrict__ tick_off, unsigned *__restrict__ cursor,
 		uint32_t *__restrict__ long_act, int32_t *__restrict__ tick_long, uint32_t *__restrict__ mid_list,
 		unsigned *__restrict__ mid_count, uint32_t *__restrict__ vl_list, unsigned *__restrict__ vl_count) {
 	const int na = tick_act[K];
+	const int lane = threadIdx.x & 31;
 	const int i0 = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-	for (int t = i0; t <= K; t += (int)(gridDim.x * blockDim.x)) tick_long[t] = (int32_t)tick_off[t];
-	for (int a = i0; a < na; a += (int)(gridDim.x * blockDim.x)) {
-		const uint32_t n = act_seg[a + 1] - act_seg[a];
-		if (n <= RUN_SHORT) continue;
-		const int t = tick_of_pair(tick_act, K, a);
-		long_act[tick_off[t] + atomicAdd(&cursor[t], 1u)] = (uint32_t)a;
+	const int stride = (int)(gridDim.x * blockDim.x);
+	for (int t = i0; t <= K; t += stride) tick_long[t] = (int32_t)tick_off[t];
+	for (int a0 = i0 - lane; a0 < na; a0 += stride) {
+		const int a = a0 + lane;
+		const uint32_t n = a < na ? act_seg[a + 1] - act_seg[a] : 0u;
+		const bool is_long = n > RUN_SHORT;
+		const int t = is_long ? tick_of_pair(tick_act, K, a) : -1;
+		const unsigned grp = __match_any_sync(0xffffffffu, t);
+		const int leader = __ffs(grp) - 1;
+		unsigned base = 0;
+		if (is_long && lane == leader) base = atomicAdd(&cursor[t], (unsigned)__popc(grp));
+		base = __shfl_sync(0xffffffffu, base, leader);
+		if (!is_long) continue;
+		long_act[tick_off[t] + base + __popc(grp & ((1u << lane) - 1u))] = (uint32_t)a;
 		if (n > SLOT_MID_MAX) vl_list[atomicAdd(vl_count, 1u)] = (uint32_t)a;
 		else if (n > SLOT_WARP_MAX) mid_list[atomicAdd(mid_count, 1u)] = (uint32_t)a;
 	}
@@ -1040,11 +1059,12 @@ __device__ __forceinline__ void warp_segment_sum(const double *__restrict__ acc,
 }
 
 // Per-particle sums of one tick's deposits (photons/NH, heat, deposit count)
-// in slot order. Warps first take the tick's long segments, a warp each
-// (particles are in leaf order, so the long ones are neighbours; giving each
-// its own warp keeps them from piling up on a few warps), then every thread
-// takes short ones, a thread each. The grid is persistent (both loops stride
-// over the tick's ranges, read on the device).
+// in hit order. Warps first take the tick's segments of more than RUN_THREAD
+// deposits, a warp each (particles are in leaf order, so the long ones are
+// neighbours; giving each its own warp keeps them from piling up on a few
+// warps), then every thread takes shorter ones, a thread each (sorted runs
+// read in order, runs of up to RUN_SHORT by selection). The grid is
+// persistent (both loops stride over the tick's ranges, read on the device).
 template <bool ISO, bool REC>
 __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
@@ -1063,6 +1083,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 	for (int e = tick_long[t] + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); e < tick_long[t + 1];
 			e += nwarp) {
 		const int a = (int)long_act[e];
+		if (act_seg[a + 1] - act_seg[a] <= RUN_THREAD) continue;      // (a thread's, below)
 		double sg, sh;
 		int sn;
 		warp_segment_sum(acc, vals, want_heat, act_seg[a], act_seg[a + 1], lane, sg, sh, sn);
@@ -1072,12 +1093,13 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 	}
 	for (int a = lo + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi; a += (int)(gridDim.x * blockDim.x)) {
 		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
-		if (s1 - s0 > RUN_SHORT) continue;
+		if (s1 - s0 > RUN_THREAD) continue;
+		const bool by_selection = s1 - s0 <= RUN_SHORT;      // (longer runs are sorted)
 		double g = 0.0, heat = 0.0;
 		int nh = 0;
 		int64_t prev = -1;
 		for (uint32_t k = s0; k < s1; k++) {
-			const uint32_t hk = next_in_run(vals, s0, s1, prev);
+			const uint32_t hk = by_selection ? next_in_run(vals, s0, s1, prev) : vals[k];
 			prev = hk;
 			if (want_heat) {
 				const double2 d = reinterpret_cast<const double2 *>(acc)[hk];
