@@ -158,7 +158,7 @@ __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__re
 // than SLOT_LONG_MAX rays of one tick on one particle), with the upper half
 // of vals (from half) as scratch. The two block tiers take their runs from
 // lists of their own.
-#define RUN_SHORT 8          // runs up to this many hits are summed by selection, longer ones sorted
+#define RUN_SHORT 16         // runs up to this many hits are summed by selection, longer ones sorted
 #define RUN_THREAD 32        // runs up to this many hits are summed by a thread, longer ones by a warp
 #define SLOT_WARP_MAX 256
 #define SLOT_MID_MAX 2048
@@ -995,7 +995,7 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 
 // Runs of up to RUN_SHORT hits stay in placement order (arbitrary); their
 // sums go in hit order all the same: each step takes the smallest hit index
-// above the last one (at most 64 reads of the run's entries, in L1; runs
+// above the last one (at most 256 reads of the run's entries, in L1; runs
 // average under 4 hits). Longer runs are sorted and read in order.
 __device__ __forceinline__ uint32_t next_in_run(const uint32_t *__restrict__ vals, uint32_t s0, uint32_t s1,
 		int64_t prev) {
@@ -1341,11 +1341,89 @@ __device__ __forceinline__ void he_write(const PhysParams &P, uint32_t p, const 
 	lasthit[p] = tick;
 }
 
+// The helium update's inputs: per active pair of the tick its summed
+// yGdepHI, yGdepHeI, yGdepHeII and heat, and its deposit counter. Runs of
+// more than RUN_THREAD hits a warp each (lanes strided, then a fixed
+// butterfly), the others a thread each (sorted runs read in order, runs of
+// up to RUN_SHORT in hit order by selection).
+__global__ void __launch_bounds__(256) k_sum_he(int t, const int32_t *__restrict__ tick_act,
+		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg, const double *__restrict__ acc,
+		const uint32_t *__restrict__ vals, int want_heat, const uint32_t *__restrict__ long_act,
+		const int32_t *__restrict__ tick_long, int32_t *__restrict__ hits, double *__restrict__ sum_g0,
+		double *__restrict__ sum_g1, double *__restrict__ sum_g2, double *__restrict__ sum_heat) {
+	const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
+	const int lane = threadIdx.x & 31;
+	const int nwarp = (int)((gridDim.x * blockDim.x) >> 5);
+	for (int e = tick_long[t] + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); e < tick_long[t + 1];
+			e += nwarp) {
+		const int a = (int)long_act[e];
+		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
+		if (s1 - s0 <= RUN_THREAD) continue;
+		double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
+		int nh = 0;
+		for (uint32_t k = s0 + lane; k < s1; k += 32) {
+			const size_t hk = vals[k];
+			const double2 x = acc2[2 * hk];
+			if (x.x >= 0.0) {
+				const double2 y = acc2[2 * hk + 1];
+				g0 += x.x;
+				g1 += y.x;
+				g2 += y.y;
+				if (want_heat) heat += x.y;
+				nh++;
+			}
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+			g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+			g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+			heat += __shfl_xor_sync(0xffffffffu, heat, o);
+			nh += __shfl_xor_sync(0xffffffffu, nh, o);
+		}
+		if (lane == 0) {
+			sum_g0[a] = g0;
+			sum_g1[a] = g1;
+			sum_g2[a] = g2;
+			sum_heat[a] = heat;
+			hits[act_ipar[a]] += nh;
+		}
+	}
+	const int hi = tick_act[t + 1];
+	for (int a = tick_act[t] + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi;
+			a += (int)(gridDim.x * blockDim.x)) {
+		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
+		if (s1 - s0 > RUN_THREAD) continue;
+		const bool by_selection = s1 - s0 <= RUN_SHORT;
+		double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
+		int nh = 0;
+		int64_t prev = -1;
+		for (uint32_t k = s0; k < s1; k++) {
+			const size_t hk = by_selection ? next_in_run(vals, s0, s1, prev) : vals[k];
+			prev = (int64_t)hk;
+			const double2 x = acc2[2 * hk];
+			if (x.x >= 0.0) {
+				const double2 y = acc2[2 * hk + 1];
+				g0 += x.x;
+				g1 += y.x;
+				g2 += y.y;
+				if (want_heat) heat += x.y;
+				nh++;
+			}
+		}
+		sum_g0[a] = g0;
+		sum_g1[a] = g1;
+		sum_g2[a] = g2;
+		sum_heat[a] = heat;
+		hits[act_ipar[a]] += nh;
+	}
+}
+
 template <bool REC>
 __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__restrict__ tick_act,
-		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg, const double *__restrict__ acc,
-		const uint32_t *__restrict__ vals, int want_heat,
-		int32_t *__restrict__ hits, double *__restrict__ lambdaH, float *__restrict__ ie,
+		const uint32_t *__restrict__ act_ipar, const double *__restrict__ sum_g0, const double *__restrict__ sum_g1,
+		const double *__restrict__ sum_g2, const double *__restrict__ sum_heat, double *__restrict__ lambdaH,
+		float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET, PhysParams P,
 		const PsgBatchDev *__restrict__ B, HeStiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff,
 		uint32_t *__restrict__ status) {
@@ -1354,27 +1432,9 @@ __global__ void __launch_bounds__(128, 4) k_update_he(int t, const int32_t *__re
 	const int hi = tick_act[t + 1];
 	for (int a = tick_act[t] + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi;
 			a += (int)(gridDim.x * blockDim.x)) {
-	const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
-	double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
-	int nh = 0;
-	const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
-	const bool short_run = s1 - s0 <= RUN_SHORT;
-	int64_t prev = -1;
-	for (uint32_t k = s0; k < s1; k++) {
-		const size_t hk = short_run ? next_in_run(vals, s0, s1, prev) : vals[k];
-		prev = (int64_t)hk;
-		const double2 a = acc2[2 * hk];
-		if (a.x >= 0.0) {
-			const double2 b = acc2[2 * hk + 1];
-			g0 += a.x;
-			g1 += b.x;
-			g2 += b.y;
-			if (want_heat) heat += a.y;
-			nh++;
-		}
-	}
+	double g0 = sum_g0[a], g1 = sum_g1[a], g2 = sum_g2[a];
+	const double heat = sum_heat[a];
 	const uint32_t p = act_ipar[a];
-	hits[p] += nh;
 	if (P.euler) {      // photons left over by an earlier explicit step (loop.c:745-747)
 		g0 += P.gcarry[p];
 		g1 += P.gcarryHe1[p];
@@ -1715,7 +1775,8 @@ UpdView upd_view(psg_context *ctx, const BatchPlan &pl) {
 	char *um = (char *)ctx->scratch[S_UPD].p;
 	v.act_g = (double *)um;
 	v.act_heat = v.act_g + pl.cap;
-	v.cursors = (unsigned *)(v.act_heat + pl.cap);
+	// (with helium two more per-pair sums follow act_heat: yGdepHeI, yGdepHeII)
+	v.cursors = (unsigned *)(v.act_heat + pl.cap * (pl.helium ? 3 : 1));
 	v.nstiff = v.cursors + (pl.K + 1);
 	v.nrej = v.nstiff + (pl.K + 1);
 	v.dep_ctr = v.nrej + (pl.K + 1);
@@ -1725,7 +1786,7 @@ UpdView upd_view(psg_context *ctx, const BatchPlan &pl) {
 	return v;
 }
 size_t upd_bytes(const BatchPlan &pl) {
-	return sizeof(double) * 2 * pl.cap + sizeof(unsigned) * 4 * (pl.K + 1) + sizeof(TickRays) * pl.K +
+	return sizeof(double) * (pl.helium ? 4 : 2) * pl.cap + sizeof(unsigned) * 4 * (pl.K + 1) + sizeof(TickRays) * pl.K +
 			(pl.iso ? 0 : sizeof(StiffItem) * pl.pcap) + (pl.surr ? sizeof(uint32_t) * pl.pcap : 0) + 512;
 }
 
@@ -1924,13 +1985,18 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 		psg_mark_end(ctx);
 		psg_mark_begin(ctx, PSG_K_UPDATE);
 		if (pl.helium) {
+			double *g1 = uv.act_heat + pl.cap, *g2 = g1 + pl.cap;
+			k_sum_he<<<pl.red_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc, vals,
+					pl.want_heat, long_act, tick_long, ctx->d_hits, uv.act_g, g1, g2, uv.act_heat);
+			PSG_CHECK_LAUNCH();
+			ctx->launches++;
 			if (P.ygrec)
-				k_update_he<true><<<pl.he_grid, 128, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc,
-						vals, pl.want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
+				k_update_he<true><<<pl.he_grid, 128, 0, st>>>((int)t, av.tick_act, av.act_ipar, uv.act_g, g1, g2,
+						uv.act_heat, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
 						ctx->d_yeMET, P, B, hstiff, uv.nstiff + t, ctx->d_status);
 			else
-				k_update_he<false><<<pl.he_grid, 128, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc,
-						vals, pl.want_heat, ctx->d_hits, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
+				k_update_he<false><<<pl.he_grid, 128, 0, st>>>((int)t, av.tick_act, av.act_ipar, uv.act_g, g1, g2,
+						uv.act_heat, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho,
 						ctx->d_yeMET, P, B, hstiff, uv.nstiff + t, ctx->d_status);
 			PSG_CHECK_LAUNCH();
 			k_update_he_stiff<<<sms, 64, 0, st>>>(hstiff, uv.nstiff + t, ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit,
