@@ -994,9 +994,10 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 }
 
 // Runs of up to RUN_SHORT hits stay in placement order (arbitrary); their
-// sums go in hit order all the same: each step takes the smallest hit index
-// above the last one (at most 256 reads of the run's entries, in L1; runs
-// average under 4 hits). Longer runs are sorted and read in order.
+// sums go in hit order all the same. Up to 4 hits by selection (each step
+// the smallest hit index above the last: at most 16 reads, in L1); up to 8
+// and 16 through a bitonic network in registers (fully unrolled: 24 and 80
+// compare-exchanges). Longer runs are sorted and read in order.
 __device__ __forceinline__ uint32_t next_in_run(const uint32_t *__restrict__ vals, uint32_t s0, uint32_t s1,
 		int64_t prev) {
 	uint32_t best = 0xFFFFFFFFu;
@@ -1005,6 +1006,55 @@ __device__ __forceinline__ uint32_t next_in_run(const uint32_t *__restrict__ val
 		if ((int64_t)v > prev && v < best) best = v;
 	}
 	return best;
+}
+template <int N>
+__device__ __forceinline__ void bitonic_regs(uint32_t (&v)[N]) {
+#pragma unroll
+	for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+		for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+			for (int i = 0; i < N; i++) {
+				const int l = i ^ j;
+				if (l > i) {
+					const uint32_t a = v[i], b = v[l];
+					const bool up = (i & k) == 0;
+					v[i] = up ? min(a, b) : max(a, b);
+					v[l] = up ? max(a, b) : min(a, b);
+				}
+			}
+		}
+	}
+}
+template <int N, typename F>
+__device__ __forceinline__ void visit_sorted_regs(const uint32_t *__restrict__ vals, uint32_t s0, uint32_t n, F f) {
+	uint32_t v[N];
+#pragma unroll
+	for (int i = 0; i < N; i++) v[i] = (uint32_t)i < n ? vals[s0 + i] : 0xFFFFFFFFu;
+	bitonic_regs<N>(v);
+#pragma unroll
+	for (int i = 0; i < N; i++)
+		if ((uint32_t)i < n) f(v[i]);
+}
+// f(hit) for every hit of the run [s0, s1) in hit order; runs longer than
+// RUN_SHORT are read as stored (sorted)
+template <typename F>
+__device__ __forceinline__ void visit_run(const uint32_t *__restrict__ vals, uint32_t s0, uint32_t s1, F f) {
+	const uint32_t n = s1 - s0;
+	if (n <= 4) {
+		int64_t prev = -1;
+		for (uint32_t i = 0; i < n; i++) {
+			const uint32_t h = next_in_run(vals, s0, s1, prev);
+			prev = h;
+			f(h);
+		}
+	} else if (n <= 8) {
+		visit_sorted_regs<8>(vals, s0, n, f);
+	} else if (n <= RUN_SHORT) {
+		visit_sorted_regs<RUN_SHORT>(vals, s0, n, f);
+	} else {
+		for (uint32_t k = s0; k < s1; k++) f(vals[k]);
+	}
 }
 
 // One long deposit segment [b0, b1) summed by a warp: lanes strided over
@@ -1094,13 +1144,9 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 	for (int a = lo + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi; a += (int)(gridDim.x * blockDim.x)) {
 		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
 		if (s1 - s0 > RUN_THREAD) continue;
-		const bool by_selection = s1 - s0 <= RUN_SHORT;      // (longer runs are sorted)
 		double g = 0.0, heat = 0.0;
 		int nh = 0;
-		int64_t prev = -1;
-		for (uint32_t k = s0; k < s1; k++) {
-			const uint32_t hk = by_selection ? next_in_run(vals, s0, s1, prev) : vals[k];
-			prev = hk;
+		visit_run(vals, s0, s1, [&](uint32_t hk) {
 			if (want_heat) {
 				const double2 d = reinterpret_cast<const double2 *>(acc)[hk];
 				if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
@@ -1108,7 +1154,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 				const double d = acc[hk];
 				if (d >= 0.0) { g += d; nh++; }
 			}
-		}
+		});
 		finish_particle<ISO, REC>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
 				hstep, rec, lo, gcarry, P, tick, tick_time, status);
 	}
@@ -1394,13 +1440,10 @@ __global__ void __launch_bounds__(256) k_sum_he(int t, const int32_t *__restrict
 			a += (int)(gridDim.x * blockDim.x)) {
 		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
 		if (s1 - s0 > RUN_THREAD) continue;
-		const bool by_selection = s1 - s0 <= RUN_SHORT;
 		double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
 		int nh = 0;
-		int64_t prev = -1;
-		for (uint32_t k = s0; k < s1; k++) {
-			const size_t hk = by_selection ? next_in_run(vals, s0, s1, prev) : vals[k];
-			prev = (int64_t)hk;
+		visit_run(vals, s0, s1, [&](uint32_t h) {
+			const size_t hk = h;
 			const double2 x = acc2[2 * hk];
 			if (x.x >= 0.0) {
 				const double2 y = acc2[2 * hk + 1];
@@ -1410,7 +1453,7 @@ __global__ void __launch_bounds__(256) k_sum_he(int t, const int32_t *__restrict
 				if (want_heat) heat += x.y;
 				nh++;
 			}
-		}
+		});
 		sum_g0[a] = g0;
 		sum_g1[a] = g1;
 		sum_g2[a] = g2;
