@@ -149,7 +149,7 @@ __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__re
 		vals[atomicSub(&cnt[kb + ipar[h]], 1u) - 1u] = (uint32_t)h;
 }
 
-// Runs longer than RUN_SHORT (particles next to a source), in three tiers: up to
+// Runs longer than the tuner's run_short (particles next to a source), in three tiers: up to
 // SLOT_WARP_MAX hits a warp each (bitonic sort in the warp's part of
 // shared memory); up to SLOT_MID_MAX a 256-thread block each (bitonic in
 // shared memory); longer ones a 1024-thread block each, bitonic in shared
@@ -158,7 +158,7 @@ __global__ void k_slot_place(size_t nray, int R, uint32_t N, const int64_t *__re
 // than SLOT_LONG_MAX rays of one tick on one particle), with the upper half
 // of vals (from half) as scratch. The two block tiers take their runs from
 // lists of their own.
-#define RUN_SHORT 16         // runs up to this many hits are summed by selection, longer ones sorted
+#define RUN_SHORT 16         // the longest run that may be left unsorted (psg_tune.run_short: 4, 8 or 16)
 #define RUN_THREAD 32        // runs up to this many hits are summed by a thread, longer ones by a warp
 #define SLOT_WARP_MAX 256
 #define SLOT_MID_MAX 2048
@@ -872,7 +872,7 @@ __global__ void k_ray_lists(size_t nray, const unsigned long long *__restrict__ 
 // The active count of the batch, nact = tick_act[K], is read on the device;
 // flags cover the capacity cap + 1 (zero past nact) so the scan's size is
 // fixed.
-// The active pairs whose run is longer than RUN_SHORT hits, per tick (their order
+// The active pairs whose run is longer than short_max hits, per tick (their order
 // within a tick is free: each is summed and sorted on its own). Counted per
 // tick, the K counts scanned by one block, then listed; runs longer than
 // SLOT_WARP_MAX also go to the lists of the two block sorts.
@@ -888,20 +888,20 @@ __device__ __forceinline__ int tick_of_pair(const int32_t *__restrict__ tick_act
 // (a warp's pairs are consecutive and mostly of one tick: one atomic per
 // tick per warp, the lanes ranked within it)
 __global__ void k_long_count(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
-		unsigned long long *__restrict__ tick_cnt) {
+		uint32_t short_max, unsigned long long *__restrict__ tick_cnt) {
 	const int na = tick_act[K];
 	const int lane = threadIdx.x & 31;
 	const int stride = (int)(gridDim.x * blockDim.x);
 	for (int a0 = (int)(blockIdx.x * blockDim.x + threadIdx.x) - lane; a0 < na; a0 += stride) {
 		const int a = a0 + lane;
-		const bool is_long = a < na && act_seg[a + 1] - act_seg[a] > RUN_SHORT;
+		const bool is_long = a < na && act_seg[a + 1] - act_seg[a] > short_max;
 		const int t = is_long ? tick_of_pair(tick_act, K, a) : -1;
 		const unsigned grp = __match_any_sync(0xffffffffu, t);
 		if (is_long && lane == __ffs(grp) - 1) atomicAdd(&tick_cnt[t], (unsigned long long)__popc(grp));
 	}
 }
 __global__ void k_long_place(const int32_t *__restrict__ tick_act, int K, const uint32_t *__restrict__ act_seg,
-		const unsigned long long *__restrict__ tick_off, unsigned *__restrict__ cursor,
+		uint32_t short_max, const unsigned long long *__restrict__ tick_off, unsigned *__restrict__ cursor,
 		uint32_t *__restrict__ long_act, int32_t *__restrict__ tick_long, uint32_t *__restrict__ mid_list,
 		unsigned *__restrict__ mid_count, uint32_t *__restrict__ vl_list, unsigned *__restrict__ vl_count) {
 	const int na = tick_act[K];
@@ -912,7 +912,7 @@ __global__ void k_long_place(const int32_t *__restrict__ tick_act, int K, const 
 	for (int a0 = i0 - lane; a0 < na; a0 += stride) {
 		const int a = a0 + lane;
 		const uint32_t n = a < na ? act_seg[a + 1] - act_seg[a] : 0u;
-		const bool is_long = n > RUN_SHORT;
+		const bool is_long = n > short_max;
 		const int t = is_long ? tick_of_pair(tick_act, K, a) : -1;
 		const unsigned grp = __match_any_sync(0xffffffffu, t);
 		const int leader = __ffs(grp) - 1;
@@ -993,7 +993,7 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 	if (st) atomicOr(status, st);
 }
 
-// Runs of up to RUN_SHORT hits stay in placement order (arbitrary); their
+// Runs of up to short_max (at most RUN_SHORT) hits stay in placement order; their
 // sums go in hit order all the same. Up to 4 hits by selection (each step
 // the smallest hit index above the last: at most 16 reads, in L1); up to 8
 // and 16 through a bitonic network in registers (fully unrolled: 24 and 80
@@ -1037,11 +1037,14 @@ __device__ __forceinline__ void visit_sorted_regs(const uint32_t *__restrict__ v
 		if ((uint32_t)i < n) f(v[i]);
 }
 // f(hit) for every hit of the run [s0, s1) in hit order; runs longer than
-// RUN_SHORT are read as stored (sorted)
+// short_max (4, 8 or 16: the tuner's run_short) are read as stored (sorted)
 template <typename F>
-__device__ __forceinline__ void visit_run(const uint32_t *__restrict__ vals, uint32_t s0, uint32_t s1, F f) {
+__device__ __forceinline__ void visit_run(const uint32_t *__restrict__ vals, uint32_t s0, uint32_t s1,
+		uint32_t short_max, F f) {
 	const uint32_t n = s1 - s0;
-	if (n <= 4) {
+	if (n > short_max) {
+		for (uint32_t k = s0; k < s1; k++) f(vals[k]);
+	} else if (n <= 4) {
 		int64_t prev = -1;
 		for (uint32_t i = 0; i < n; i++) {
 			const uint32_t h = next_in_run(vals, s0, s1, prev);
@@ -1050,10 +1053,8 @@ __device__ __forceinline__ void visit_run(const uint32_t *__restrict__ vals, uin
 		}
 	} else if (n <= 8) {
 		visit_sorted_regs<8>(vals, s0, n, f);
-	} else if (n <= RUN_SHORT) {
-		visit_sorted_regs<RUN_SHORT>(vals, s0, n, f);
 	} else {
-		for (uint32_t k = s0; k < s1; k++) f(vals[k]);
+		visit_sorted_regs<RUN_SHORT>(vals, s0, n, f);
 	}
 }
 
@@ -1113,12 +1114,12 @@ __device__ __forceinline__ void warp_segment_sum(const double *__restrict__ acc,
 // deposits, a warp each (particles are in leaf order, so the long ones are
 // neighbours; giving each its own warp keeps them from piling up on a few
 // warps), then every thread takes shorter ones, a thread each (sorted runs
-// read in order, runs of up to RUN_SHORT by selection). The grid is
+// read in order, shorter ones put in hit order by visit_run). The grid is
 // persistent (both loops stride over the tick's ranges, read on the device).
 template <bool ISO, bool REC>
 __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg,
-		const double *__restrict__ acc, const uint32_t *__restrict__ vals, int want_heat,
+		const double *__restrict__ acc, const uint32_t *__restrict__ vals, uint32_t short_max, int want_heat,
 		const uint32_t *__restrict__ long_act, const int32_t *__restrict__ tick_long,
 		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat,
 		double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit,
@@ -1146,7 +1147,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		if (s1 - s0 > RUN_THREAD) continue;
 		double g = 0.0, heat = 0.0;
 		int nh = 0;
-		visit_run(vals, s0, s1, [&](uint32_t hk) {
+		visit_run(vals, s0, s1, short_max, [&](uint32_t hk) {
 			if (want_heat) {
 				const double2 d = reinterpret_cast<const double2 *>(acc)[hk];
 				if (d.x >= 0.0) { g += d.x; heat += d.y; nh++; }
@@ -1391,10 +1392,10 @@ __device__ __forceinline__ void he_write(const PhysParams &P, uint32_t p, const 
 // yGdepHI, yGdepHeI, yGdepHeII and heat, and its deposit counter. Runs of
 // more than RUN_THREAD hits a warp each (lanes strided, then a fixed
 // butterfly), the others a thread each (sorted runs read in order, runs of
-// up to RUN_SHORT in hit order by selection).
+// up to short_max put in hit order by visit_run).
 __global__ void __launch_bounds__(256) k_sum_he(int t, const int32_t *__restrict__ tick_act,
 		const uint32_t *__restrict__ act_ipar, const uint32_t *__restrict__ act_seg, const double *__restrict__ acc,
-		const uint32_t *__restrict__ vals, int want_heat, const uint32_t *__restrict__ long_act,
+		const uint32_t *__restrict__ vals, uint32_t short_max, int want_heat, const uint32_t *__restrict__ long_act,
 		const int32_t *__restrict__ tick_long, int32_t *__restrict__ hits, double *__restrict__ sum_g0,
 		double *__restrict__ sum_g1, double *__restrict__ sum_g2, double *__restrict__ sum_heat) {
 	const double2 *acc2 = reinterpret_cast<const double2 *>(acc);
@@ -1442,7 +1443,7 @@ __global__ void __launch_bounds__(256) k_sum_he(int t, const int32_t *__restrict
 		if (s1 - s0 > RUN_THREAD) continue;
 		double g0 = 0.0, g1 = 0.0, g2 = 0.0, heat = 0.0;
 		int nh = 0;
-		visit_run(vals, s0, s1, [&](uint32_t h) {
+		visit_run(vals, s0, s1, short_max, [&](uint32_t h) {
 			const size_t hk = h;
 			const double2 x = acc2[2 * hk];
 			if (x.x >= 0.0) {
@@ -1985,11 +1986,12 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	float *feat = pl.feat_on ? (float *)ctx->scratch[S_LOG].p : nullptr;
 	LongLists ll = long_lists(ctx, pl);
 	PSG_CUDA(cudaMemsetAsync(ll.zero, 0, ll.zero_bytes, st));
-	k_long_count<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, av.act_seg, ll.tick_off);
+	k_long_count<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, av.act_seg, (uint32_t)ctx->tune.run_short, ll.tick_off);
 	PSG_CHECK_LAUNCH();
 	k_scan_sums<unsigned long long><<<1, 1024, 0, st>>>(ll.tick_off, K);
 	PSG_CHECK_LAUNCH();
-	k_long_place<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, av.act_seg, ll.tick_off, ll.cursor, ll.long_act,
+	k_long_place<<<cgrid, 256, 0, st>>>(av.tick_act, (int)K, av.act_seg, (uint32_t)ctx->tune.run_short, ll.tick_off,
+			ll.cursor, ll.long_act,
 			ll.tick_long, ll.mid_list, ll.mid_count, ll.vl_list, ll.vl_count);
 	PSG_CHECK_LAUNCH();
 	int32_t *tick_long = ll.tick_long;
@@ -2030,7 +2032,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 		if (pl.helium) {
 			double *g1 = uv.act_heat + pl.cap, *g2 = g1 + pl.cap;
 			k_sum_he<<<pl.red_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc, vals,
-					pl.want_heat, long_act, tick_long, ctx->d_hits, uv.act_g, g1, g2, uv.act_heat);
+					(uint32_t)ctx->tune.run_short, pl.want_heat, long_act, tick_long, ctx->d_hits, uv.act_g, g1, g2, uv.act_heat);
 			PSG_CHECK_LAUNCH();
 			ctx->launches++;
 			if (P.ygrec)
@@ -2056,7 +2058,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 			double *keep_heat = pl.iso ? nullptr : uv.act_heat;
 #define PSG_REDUCE(ISO_, REC_)                                                                                 \
 	k_reduce<ISO_, REC_><<<pl.red_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc, vals,\
-			pl.want_heat, long_act, tick_long, ctx->d_hits, keep_g, keep_heat, ctx->d_lambdaH, ctx->d_ie,       \
+			(uint32_t)ctx->tune.run_short, pl.want_heat, long_act, tick_long, ctx->d_hits, keep_g, keep_heat, ctx->d_lambdaH, ctx->d_ie,       \
 			ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, B, ctx->d_status)
 			if (pl.iso && !pl.euler) {
 				if (P.ygrec) PSG_REDUCE(true, true);
@@ -2163,6 +2165,7 @@ std::vector<unsigned long long> batch_key(const psg_context *ctx, const BatchPla
 	k.push_back(ctx->hit_cap);
 	k.push_back((unsigned long long)ctx->tune.deposit_long << 32 | (unsigned)ctx->tune.deposit_mid);
 	k.push_back((unsigned long long)pl.queue_minb);
+	k.push_back((unsigned long long)ctx->tune.run_short);
 	k.push_back(pl.src_R);
 	k.push_back(ctx->src_nray);
 	k.push_back(ctx->src_nhit);
@@ -2540,6 +2543,13 @@ extern "C" int psg_autotune(psg_context *ctx, const psg_ray *d_rays, size_t R, s
 		if (rc || mb == cur.update_minblocks) continue;
 		psg_tune t = cur;
 		t.update_minblocks = mb;
+		rc = consider(t);
+	}
+	// which runs are sorted before their sums, which put in order where summed
+	for (int rs : {4, 8, 16}) {
+		if (rc || rs == cur.run_short) continue;
+		psg_tune t = cur;
+		t.run_short = rs;
 		rc = consider(t);
 	}
 	ctx->tune = cur;
