@@ -248,6 +248,7 @@ int psg_trace_sort_prepare(psg_context *ctx, size_t nray, size_t cap, unsigned l
 int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned long long maxcount, int want_kern,
 		size_t r0);
 int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_kern);
+int psg_sort_classes(unsigned long long maxcount);
 int psg_trace_fill_prepare(psg_context *ctx, size_t nray);
 int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray, const unsigned *nlim, size_t cap);
 // A recombination tick whose R source rays were traced and sorted with the

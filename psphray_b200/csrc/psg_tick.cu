@@ -2166,6 +2166,7 @@ std::vector<unsigned long long> batch_key(const psg_context *ctx, const BatchPla
 	k.push_back((unsigned long long)ctx->tune.deposit_long << 32 | (unsigned)ctx->tune.deposit_mid);
 	k.push_back((unsigned long long)pl.queue_minb);
 	k.push_back((unsigned long long)ctx->tune.run_short);
+	k.push_back((unsigned long long)psg_sort_classes(pl.maxcount));
 	k.push_back(pl.src_R);
 	k.push_back(ctx->src_nray);
 	k.push_back(ctx->src_nhit);

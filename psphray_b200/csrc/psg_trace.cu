@@ -781,6 +781,14 @@ int psg_trace_sort_prepare(psg_context *ctx, size_t nray, size_t cap, unsigned l
 	return PSG_OK;
 }
 
+// The size classes a call with lists up to maxcount long can fill.
+int psg_sort_classes(unsigned long long maxcount) {
+	static const unsigned long long lower[SORT_NCLS] = {0, 64, 128, 256, 512, 1024, 2048, 4096};
+	int c = 0;
+	while (c < SORT_NCLS && maxcount > lower[c]) c++;
+	return c;
+}
+
 // The per-ray sort by (d, ipar) of the filled slabs into the CSR lists.
 // Launch sizes are fixed by nray (the persistent class kernels read their
 // ray counts on the device), so it can be captured in a graph; with
@@ -810,7 +818,11 @@ int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned 
 		PSG_CHECK_LAUNCH();
 		const PhysParams PP = psg_phys_params(ctx);
 		const size_t stride = nray + 1;
+		// a class whose rays all have more hits than the call's longest list
+		// is empty: not launched (psg_sort_classes; part of a graph's key)
+		const int ncls = psg_sort_classes(maxcount);
 		auto launch_block = [&](auto kern, int tpr, size_t smem, int c) -> int {
+			if (c >= ncls) return PSG_OK;
 			const unsigned grid = (unsigned)std::min<size_t>(nray - r0, (size_t)ctx->sort_grid[c]);
 			kern<<<grid, tpr, smem, st>>>(lists + c * stride, d_ncls + c, off64, scap, slab_ipar, slab_d,
 					slab_b, hit_ipar, hit_d, hit_b, want_kern, ctx->d_psml, PP, ctx->d_order, r0);
