@@ -250,7 +250,6 @@ int psg_trace_sort_enqueue(psg_context *ctx, size_t nray, size_t nhit, unsigned 
 int psg_trace_internal(psg_context *ctx, const psg_ray *d_rays, size_t nray, int want_kern);
 int psg_sort_classes(unsigned long long maxcount);
 int psg_trace_fill_prepare(psg_context *ctx, size_t nray);
-int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray, const unsigned *nlim, size_t cap);
 // A recombination tick whose R source rays were traced and sorted with the
 // call's (S_SRCHIT): their counts and sorted hits come from there, only the
 // emitted rays behind them (at most cap_rec, *nlim of them) are traversed.

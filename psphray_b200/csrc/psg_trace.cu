@@ -495,41 +495,6 @@ __global__ void k_count_clamp(size_t nray, size_t scap, uint32_t *__restrict__ c
 	if (c) atomicMax(callmax, (unsigned long long)c);
 }
 
-// The traversal without any host read (the recombination path's ticks):
-// the slabs as they are, rays up to *nlim, counts clamped to the slabs, a
-// total above cap flagged (k_offsets64).
-// Issues launches only; the caller has sized the slabs (S_COUNT, S_OFFSETS,
-// S_REC_U32/F64, S_CUB).
-int psg_trace_fill_enqueue(psg_context *ctx, const psg_ray *d_rays, size_t nray, const unsigned *nlim, size_t cap) {
-	cudaStream_t st = ctx->stream;
-	uint32_t *count = (uint32_t *)ctx->scratch[S_COUNT].p;
-	unsigned long long *scan = count_scan(count, nray);
-	int64_t *off64 = (int64_t *)ctx->scratch[S_OFFSETS].p;
-	unsigned long long *d_max = ctx->d_counters + 4;
-	unsigned long long *next_ray = ctx->d_counters + 9;
-	const size_t scap = ctx->slab_cap;
-	const size_t slots = nray * scap;
-	uint32_t *slab_ipar = (uint32_t *)ctx->scratch[S_REC_U32].p;
-	double *slab_f64 = (double *)ctx->scratch[S_REC_F64].p;
-	const int trw = std::max(1, std::min(TR_MAX_WARPS, ctx->tune.trace_warps));
-	const size_t smem = sizeof(int) * (TR_STACK + 32 * (size_t)ctx->ppc + 32) * trw;
-	PSG_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t) * (nray + 1), st));
-	PSG_CUDA(cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned long long), st));
-	PSG_CUDA(cudaMemsetAsync(next_ray, 0, sizeof(unsigned long long), st));
-	k_trace_stack<<<ctx->trace_grid, 32 * trw, smem, st>>>(d_rays, nray, ctx->d_wide_lo, ctx->d_wide_hi,
-			ctx->d_leaf_psml, ctx->d_leaf_idx, ctx->ppc, count, scap, slab_ipar, slab_f64, slab_f64 + slots, next_ray,
-			ctx->d_status, nlim);
-	PSG_CHECK_LAUNCH();
-	k_count_clamp<<<blocks(nray, 256), 256, 0, st>>>(nray, scap, count, ctx->d_counters + 3, ctx->d_status);
-	PSG_CHECK_LAUNCH();
-	PSG_CUDA(scan_enqueue(st, count, nray + 1, scan, (unsigned long long *)ctx->scratch[S_SCAN].p, Widen()));
-	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, d_max, cap,
-			ctx->d_counters + 24, ctx->d_status);
-	PSG_CHECK_LAUNCH();
-	ctx->launches += 3;
-	return PSG_OK;
-}
-
 namespace {
 // The tick's source-ray counts from the call's traced source rays (the tick
 // is B->k of the call).
@@ -652,7 +617,7 @@ int psg_trace_rec_sort_enqueue(psg_context *ctx, size_t R, size_t nray, unsigned
 	return psg_trace_sort_enqueue(ctx, nray, 0, maxcount, 1, R);
 }
 
-// Sizes the buffers psg_trace_fill_enqueue uses for nray rays (allocates;
+// Sizes the buffers psg_trace_rec_fill_enqueue uses for nray rays (allocates;
 // before a capture) and its persistent grid.
 int psg_trace_fill_prepare(psg_context *ctx, size_t nray) {
 	const size_t scap = ctx->slab_cap;
