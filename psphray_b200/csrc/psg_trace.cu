@@ -111,7 +111,7 @@ __device__ __forceinline__ void test_candidates(const RayGeom &g, const int *lis
 				const size_t o = r * scap + q;
 				slab_ipar[o] = idx;
 				slab_d[o] = dc;
-				slab_b[o] = __dsqrt_rn(fabs(r2));
+				slab_b[o] = r2;      // (b = sqrt|r2| is taken in the sort, with every lane busy)
 			}
 		}
 		nh += __popc(bal);
@@ -266,15 +266,15 @@ __device__ __forceinline__ uint32_t caller_index(const uint32_t *__restrict__ or
 	return order ? order[i] : i;
 }
 
-// The hit at slab position p of a ray as the sorted list's entry h; with
-// want_kern its b becomes the column-density factor sph_depth(b/h)/h^2
-// (loop.c:429-445).
+// The hit at slab position p of a ray as the sorted list's entry h (the slab
+// holds b^2; b = sqrt|b^2| here); with want_kern b becomes the
+// column-density factor sph_depth(b/h)/h^2 (loop.c:429-445).
 __device__ __forceinline__ void put_sorted_hit(int64_t h, uint32_t p, const uint32_t *__restrict__ raw_ipar,
 		const double *__restrict__ raw_d, const double *__restrict__ raw_b, uint32_t *__restrict__ out_ipar,
 		double *__restrict__ out_d, double *__restrict__ out_b, int want_kern, const float4 *__restrict__ psml,
 		const PhysParams &P) {
 	const uint32_t ip = raw_ipar[p];
-	const double b = raw_b[p];
+	const double b = __dsqrt_rn(fabs(raw_b[p]));      // the slab holds the squared distance
 	out_ipar[h] = ip;
 	out_d[h] = raw_d[p];
 	if (want_kern) {
