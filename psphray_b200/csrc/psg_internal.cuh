@@ -227,7 +227,8 @@ int psg_build_lte(psg_context *ctx, const psg_xs_table *xs);
 // the emission of a tick without host reads (its count stays on the
 // device), its buffers, and the next tick's emitter marks (psg_recomb.cu)
 int psg_rec_prepare(psg_context *ctx);
-int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out);
+int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out, unsigned long long *nlim,
+		unsigned long long *recsum);
 int psg_rec_mark_enqueue(psg_context *ctx, size_t R, const PsgBatchDev *B);
 // the recombination ticks replayed from one captured tick (psg_tick.cu);
 // PSG_RETRY: run them one by one instead (first call, slabs too small)

@@ -166,7 +166,8 @@ __device__ __forceinline__ unsigned long long run_of(unsigned long long key) { r
 // its rays by (type, ipar), loop.c:236. Each ray's photons: the emitter's
 // yGrec of the species times NH (HII) or NHe (HeII, HeIII), split over the
 // run of rays that drew it (loop.c:277-290, 305-320).
-__global__ void k_rec_rays(const unsigned *__restrict__ count, const RecItem *__restrict__ items,
+__global__ void k_rec_rays(const unsigned *__restrict__ count, unsigned long long *__restrict__ nlim,
+		unsigned long long *__restrict__ recsum, const RecItem *__restrict__ items,
 		const PsgBatchDev *__restrict__ B, uint64_t seed,
 		const float4 *__restrict__ psml, const float *__restrict__ mass, RecState Y,
 		const double *__restrict__ lambdaH, const float *__restrict__ ie, PhysParams P, LteView L, double length,
@@ -174,6 +175,10 @@ __global__ void k_rec_rays(const unsigned *__restrict__ count, const RecItem *__
 	const int M = (int)(count[0] + count[1] + count[2]);
 	const int64_t tick = B->tick0;
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i == 0 && nlim) {      // (a captured tick: the traversal's ray limit and the call's ray total)
+		*(unsigned *)nlim = (unsigned)M;
+		*recsum += (unsigned long long)M;
+	}
 	if (i >= M) return;
 	const uint32_t p = items[i].val;
 	const unsigned long long run = run_of(items[i].key);
@@ -311,7 +316,8 @@ int psg_rec_prepare(psg_context *ctx) {
 	return PSG_OK;
 }
 
-int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out) {
+int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out, unsigned long long *nlim,
+		unsigned long long *recsum) {
 	cudaStream_t st = ctx->stream;
 	const size_t n = ctx->n;
 	const PhysParams P = psg_phys_params(ctx);
@@ -364,7 +370,8 @@ int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out) {
 	}
 	L.disabled = ctx->rec_disable_lte;
 	const double length = ctx->boxsize * 2.0 * 0.1;     // MAX_REC_RAY_LENGTH, loop.c:169
-	k_rec_rays<<<nblocks(ktot, 128), 128, 0, st>>>(d_count, sorted, B, ctx->rec_seed, ctx->d_psml, ctx->d_mass, Y,
+	k_rec_rays<<<nblocks(ktot, 128), 128, 0, st>>>(d_count, nlim, recsum, sorted, B, ctx->rec_seed, ctx->d_psml,
+			ctx->d_mass, Y,
 			ctx->d_lambdaH, ctx->d_ie, P, L, length, out, d_nph);
 	PSG_CHECK_LAUNCH();
 	k_rec_purge<<<nblocks(ktot, 128), 128, 0, st>>>(d_count, sorted, out, ctx->d_mass, Y, P);
@@ -376,7 +383,7 @@ int psg_rec_emit_enqueue(psg_context *ctx, const PsgBatchDev *B, psg_ray *out) {
 // The eager form: emission, then the count read back (one synchronisation).
 static int emit_rec(psg_context *ctx, const PsgBatchDev *B, size_t cap, psg_ray *out, size_t *M_out) {
 	int rc = psg_rec_prepare(ctx);
-	if (!rc) rc = psg_rec_emit_enqueue(ctx, B, out);
+	if (!rc) rc = psg_rec_emit_enqueue(ctx, B, out, nullptr, nullptr);
 	if (rc) return rc;
 	unsigned cnt[3] = {0, 0, 0};
 	PSG_CUDA(cudaMemcpyAsync(cnt, ctx->d_counters + 11, sizeof(unsigned) * 3, cudaMemcpyDeviceToHost, ctx->stream));

@@ -2001,11 +2001,17 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 	k_slot_canon_warp<<<(unsigned)(4 * sms), 32 * SLOT_WARPS, 0, st>>>(tick_long, (int)K, long_act, av.act_seg,
 			vals);
 	PSG_CHECK_LAUNCH();
-	k_slot_canon_mid<<<(unsigned)(4 * sms), 256, 0, st>>>(ll.mid_list, ll.mid_count, av.act_seg, vals);
-	PSG_CHECK_LAUNCH();
-	k_slot_canon_long<<<(unsigned)sms, 1024, sizeof(uint32_t) * std::max(pl.long_cap, 2048), st>>>(ll.vl_list,
-			ll.vl_count, av.act_seg, vals, pl.long_cap, cap);
-	PSG_CHECK_LAUNCH();
+	// (a particle's run of one tick holds at most the tick's R hits: the
+	// block tiers are launched only where R reaches them)
+	if (R > SLOT_WARP_MAX) {
+		k_slot_canon_mid<<<(unsigned)(4 * sms), 256, 0, st>>>(ll.mid_list, ll.mid_count, av.act_seg, vals);
+		PSG_CHECK_LAUNCH();
+	}
+	if (R > SLOT_MID_MAX) {
+		k_slot_canon_long<<<(unsigned)sms, 1024, sizeof(uint32_t) * std::max(pl.long_cap, 2048), st>>>(ll.vl_list,
+				ll.vl_count, av.act_seg, vals, pl.long_cap, cap);
+		PSG_CHECK_LAUNCH();
+	}
 	psg_mark_end(ctx);
 	ctx->launches += 6;
 
@@ -2236,12 +2242,6 @@ __global__ void k_rec_src(const PsgBatchDev *__restrict__ B, size_t R, psg_ray *
 	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < R; i += (size_t)gridDim.x * blockDim.x)
 		buf[i] = src[i];
 }
-__global__ void k_rec_nlim(size_t R, const unsigned *__restrict__ count, unsigned long long *__restrict__ nlim,
-		unsigned long long *__restrict__ recsum) {
-	const unsigned M = count[0] + count[1] + count[2];
-	*(unsigned *)nlim = M;      // the emitted rays to traverse (the source rays come traced)
-	*recsum += M;
-}
 __global__ void k_rec_tick_end(const int64_t *__restrict__ off, size_t nray, unsigned long long *__restrict__ hitsum,
 		PsgBatchDev *__restrict__ B) {
 	*hitsum += (unsigned long long)off[nray];
@@ -2398,10 +2398,8 @@ int psg_run_ticks_rec_graph(psg_context *ctx, const psg_ray *d_rays, size_t R, s
 	auto tick_enqueue = [&]() -> int {
 		k_rec_src<<<(unsigned)std::min<size_t>(blocks(R, 256), 4 * (size_t)ctx->sms), 256, 0, st>>>(B, R, buf);
 		PSG_CHECK_LAUNCH();
-		int r = psg_rec_emit_enqueue(ctx, B, buf + R);
+		int r = psg_rec_emit_enqueue(ctx, B, buf + R, cnt + 15, cnt + 14);
 		if (r) return r;
-		k_rec_nlim<<<1, 1, 0, st>>>(R, (const unsigned *)(cnt + 11), cnt + 15, cnt + 14);
-		PSG_CHECK_LAUNCH();
 		r = psg_trace_rec_fill_enqueue(ctx, buf, R, cap_rec, nlim, pl.cap, B);
 		if (r) return r;
 		r = enqueue_any(ctx, pl, B);

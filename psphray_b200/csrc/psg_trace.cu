@@ -496,13 +496,26 @@ __global__ void k_count_clamp(size_t nray, size_t scap, uint32_t *__restrict__ c
 }
 
 namespace {
-// The tick's source-ray counts from the call's traced source rays (the tick
-// is B->k of the call).
-__global__ void k_src_counts(const PsgBatchDev *__restrict__ B, size_t R, const int64_t *__restrict__ src_off,
-		uint32_t *__restrict__ count) {
+// The counts of a recombination tick after its traversal: the source rays'
+// from the call's traced source rays (the tick is B->k of the call), the
+// emitted rays' clamped to the slabs (as k_count_clamp).
+__global__ void k_rec_counts(const PsgBatchDev *__restrict__ B, size_t R, const int64_t *__restrict__ src_off,
+		size_t cap_rec, size_t scap, uint32_t *__restrict__ count, unsigned long long *__restrict__ callmax,
+		uint32_t *__restrict__ status) {
 	const int64_t base = B->k * (int64_t)R;
-	for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < R; r += (size_t)gridDim.x * blockDim.x)
-		count[r] = (uint32_t)(src_off[base + (int64_t)r + 1] - src_off[base + (int64_t)r]);
+	for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < R + cap_rec;
+			r += (size_t)gridDim.x * blockDim.x) {
+		if (r < R) {
+			count[r] = (uint32_t)(src_off[base + (int64_t)r + 1] - src_off[base + (int64_t)r]);
+			continue;
+		}
+		const uint32_t c = count[r];
+		if (c > scap) {
+			count[r] = (uint32_t)scap;
+			atomicOr(status, PSG_ST_SLAB);
+		}
+		if (c) atomicMax(callmax, (unsigned long long)c);
+	}
 }
 // their sorted hits into the tick's lists, a warp per ray (nothing when the
 // tick's offsets were emptied for exceeding the capacity)
@@ -564,9 +577,9 @@ int psg_trace_src_batch(psg_context *ctx, const psg_ray *d_rays, size_t nray) {
 	return PSG_OK;
 }
 
-// The traversal of a recombination tick: the source rays' counts from
-// S_SRCHIT, the emitted rays buf[R, R + *nlim) traversed (slabs from index
-// 0), then the scan and the offsets over all R + cap_rec rays.
+// The traversal of a recombination tick: the emitted rays buf[R, R + *nlim)
+// traversed (slabs from index 0), the source rays' counts from S_SRCHIT,
+// then the scan and the offsets over all R + cap_rec rays.
 int psg_trace_rec_fill_enqueue(psg_context *ctx, const psg_ray *buf, size_t R, size_t cap_rec, const unsigned *nlim,
 		size_t cap, const PsgBatchDev *B) {
 	cudaStream_t st = ctx->stream;
@@ -586,15 +599,12 @@ int psg_trace_rec_fill_enqueue(psg_context *ctx, const psg_ray *buf, size_t R, s
 	PSG_CUDA(cudaMemsetAsync(count, 0, sizeof(uint32_t) * (nray + 1), st));
 	PSG_CUDA(cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned long long), st));
 	PSG_CUDA(cudaMemsetAsync(next_ray, 0, sizeof(unsigned long long), st));
-	k_src_counts<<<(unsigned)std::min<size_t>(blocks(R, 256), 4 * (size_t)ctx->sms), 256, 0, st>>>(B, R, h.off,
-			count);
-	PSG_CHECK_LAUNCH();
 	k_trace_stack<<<ctx->trace_grid, 32 * trw, smem, st>>>(buf + R, cap_rec, ctx->d_wide_lo, ctx->d_wide_hi,
 			ctx->d_leaf_psml, ctx->d_leaf_idx, ctx->ppc, count + R, scap, slab_ipar, slab_f64, slab_f64 + slots,
 			next_ray, ctx->d_status, nlim);
 	PSG_CHECK_LAUNCH();
-	k_count_clamp<<<blocks(cap_rec, 256), 256, 0, st>>>(cap_rec, scap, count + R, ctx->d_counters + 3,
-			ctx->d_status);
+	k_rec_counts<<<(unsigned)std::min<size_t>(blocks(nray, 256), 4 * (size_t)ctx->sms), 256, 0, st>>>(B, R, h.off,
+			cap_rec, scap, count, ctx->d_counters + 3, ctx->d_status);
 	PSG_CHECK_LAUNCH();
 	PSG_CUDA(scan_enqueue(st, count, nray + 1, scan, (unsigned long long *)ctx->scratch[S_SCAN].p, Widen()));
 	k_offsets64<<<blocks(nray + 1, 256), 256, 0, st>>>(scan, count, nray, off64, d_max, cap,
