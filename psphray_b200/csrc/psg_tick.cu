@@ -2529,7 +2529,8 @@ extern "C" int psg_autotune(psg_context *ctx, const psg_ray *d_rays, size_t R, s
 		rc = consider(t);
 	}
 	// deposit groups: which rays take a warp, a 128-thread group, a block
-	const int thr[][2] = {{64, 256}, {96, 384}, {128, 512}, {192, 768}, {256, 1024}, {384, 1536}};
+	const int thr[][2] = {{64, 256}, {96, 384}, {128, 512}, {192, 768}, {256, 1024}, {384, 1536}, {512, 2048},
+			{768, 3072}};
 	for (auto &th : thr) {
 		if (rc || (th[0] == cur.deposit_long && th[1] == cur.deposit_mid)) continue;
 		psg_tune t = cur;
