@@ -125,7 +125,8 @@ struct psg_context {
 	size_t rec_last_kmax = 0;    // capacity of that tick's item arrays (S_RECK)
 	int rec_last_threshold = 0;  // that tick ran in threshold mode (its items unsorted, in place)
 	size_t src_nray = 0;         // S_SRCHIT: the call's source rays traced and sorted before its ticks ran
-	size_t src_nhit = 0;         //   (offsets[src_nray + 1], ipar[src_nhit], kernel factor[src_nhit])
+	size_t src_nhit = 0;         //   (offsets[src_nray + 1], kernel factor[src_nhit], ipar[src_nhit]; src_nhit
+	                             //   a grow-only capacity)
 
 	// chemistry surrogate (not isothermal): weight blob, residual tolerance
 	void *d_surr = nullptr;

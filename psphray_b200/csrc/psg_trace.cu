@@ -559,11 +559,17 @@ int psg_trace_src_batch(psg_context *ctx, const psg_ray *d_rays, size_t nray) {
 	if (!rc) rc = psg_trace_sort_prepare(ctx, nray, tf.nhit, tf.maxcount);
 	if (!rc) rc = psg_trace_sort_enqueue(ctx, nray, tf.nhit, tf.maxcount, 1, 0);
 	if (rc) return rc;
+	// the layout depends on a grow-only capacity, not on this call's hit
+	// total, so that calls of similar totals share one captured tick graph
+	if (tf.nhit > ctx->src_nhit || nray != ctx->src_nray) {
+		size_t c = std::max(tf.nhit + tf.nhit / 8, ctx->src_nhit);
+		c = (c + 65535) & ~(size_t)65535;
+		ctx->src_nhit = c;
+	}
 	char *m = (char *)psg_scratch(ctx, S_SRCHIT, sizeof(int64_t) * (nray + 1) + (sizeof(double) + sizeof(uint32_t)) *
-			(tf.nhit ? tf.nhit : 1));
+			ctx->src_nhit);
 	if (!m) return PSG_E_NOMEM;
 	ctx->src_nray = nray;
-	ctx->src_nhit = tf.nhit;
 	const SrcHits h = src_hits(ctx);
 	cudaStream_t st = ctx->stream;
 	PSG_CUDA(cudaMemcpyAsync((void *)h.off, ctx->scratch[S_OFFSETS].p, sizeof(int64_t) * (nray + 1),
