@@ -243,13 +243,17 @@ typedef struct {
 	int run_short;          /* a particle's deposits of one tick up to this many (4, 8 or 16; default
 	                         * 16) are put in hit order where they are summed; longer runs are sorted
 	                         * first. The sums are the same either way. */
+	int update_order;       /* 1 (default): the integrator claims first the particles that look slow
+	                         * (no carried step proposal, a proposal under a quarter of the step, or
+	                         * more photons absorbed than neutral atoms), then the rest; 0: in particle
+	                         * order. Which lane integrates a particle changes, its result does not. */
 } psg_tune;
 int psg_set_tune(psg_context *ctx, const psg_tune *tune);
 int psg_get_tune(psg_context *ctx, psg_tune *tune);
 /* Times candidate shapes on one batch of the caller's device rays (R rays
  * per tick, K ticks, as psg_run_ticks_device), each `reps` times, one
  * dimension after another (traversal warps, deposit thresholds, integrator
- * registers, short-run threshold), and keeps the fastest. The particle state is restored after
+ * registers, short-run threshold, integrator order), and keeps the fastest. The particle state is restored after
  * every trial, so the call does not advance the run. The result becomes the
  * context's shapes and the device's cached shapes, which contexts created
  * later on that device start from. *best_ms: the kept shape's batch time. */

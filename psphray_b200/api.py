@@ -151,7 +151,8 @@ def read_snapshot(path: str) -> dict:
 class Tune(C.Structure):
     """psg_tune: launch shapes that do not change results."""
     _fields_ = [("trace_warps", C.c_int), ("deposit_long", C.c_int), ("deposit_mid", C.c_int),
-                ("update_minblocks", C.c_int), ("leaf_size", C.c_int), ("run_short", C.c_int)]
+                ("update_minblocks", C.c_int), ("leaf_size", C.c_int), ("run_short", C.c_int),
+                ("update_order", C.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -194,6 +194,7 @@ int check_tune(const psg_tune *t) {
 	if (t->deposit_long < 32 || t->deposit_mid < t->deposit_long || t->deposit_mid > 1 << 20) return 0;
 	if (t->update_minblocks != 1 && t->update_minblocks != 3 && t->update_minblocks != 4) return 0;
 	if (t->run_short != 4 && t->run_short != 8 && t->run_short != 16) return 0;
+	if (t->update_order != 0 && t->update_order != 1) return 0;
 	return t->leaf_size == 8;
 }
 }  // namespace
@@ -217,7 +218,7 @@ extern "C" int psg_set_tune(psg_context *ctx, const psg_tune *tune) {
 	if (!ctx) return PSG_E_INVAL;
 	if (!tune || !check_tune(tune))
 		return psg_fail(ctx, PSG_E_INVAL, "psg_set_tune: trace_warps 1-16, 32 <= deposit_long <= deposit_mid, "
-				"update_minblocks 1, 3 or 4, leaf_size 8, run_short 4, 8 or 16");
+				"update_minblocks 1, 3 or 4, leaf_size 8, run_short 4, 8 or 16, update_order 0 or 1");
 	ctx->tune = *tune;
 	return PSG_OK;
 }

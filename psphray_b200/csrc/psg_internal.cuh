@@ -151,7 +151,7 @@ struct psg_context {
 	size_t batch_cap = 0;                       // hits the tick batches' per-hit buffers hold
 	unsigned sort_grid[8] = {};                 // persistent grids of the per-ray sort's classes
 	unsigned trace_grid = 0;                    // persistent grid of the traversal (psg_trace_fill_prepare)
-	psg_tune tune{4, 96, 384, 1, 8, 16};        // launch shapes (psg_set_tune, psg_autotune)
+	psg_tune tune{4, 96, 384, 1, 8, 16, 1};        // launch shapes (psg_set_tune, psg_autotune)
 	long host_syncs = 0;                        // host synchronisations of the current call
 	void *graphs = nullptr;                     // captured tick batches (psg_tick.cu)
 	int use_graphs = 1;                         // replay captured batches (0: issue launches one by one)

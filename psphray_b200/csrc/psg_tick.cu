@@ -939,15 +939,24 @@ struct __align__(16) UpdRec {
 };
 static_assert(sizeof(UpdRec) == 80, "UpdRec layout");
 
+// An integration that looks long (the integrator queue claims these first):
+// no step proposal carried over, a proposal under a quarter of the step, or
+// more photons absorbed than the particle has neutral atoms.
+__device__ __forceinline__ bool upd_looks_slow(float hstep, double time, double g, double lam0) {
+	return !(hstep > 0.0f) || 4.0 * (double)hstep < time || g > lam0;
+}
+
 // The particle's summed deposits of the tick: isothermal, the closed-form
-// update_pars() step (loop.c:653-770); otherwise the sums for the integrator.
+// update_pars() step (loop.c:653-770); otherwise the sums for the integrator
+// (with act_slow, whether the integrator should claim it first).
 template <bool ISO, bool REC>
 __device__ __forceinline__ void finish_particle(int a, double g, double heat, int nh,
 		const uint32_t *__restrict__ act_ipar, int32_t *__restrict__ hits, double *__restrict__ act_g,
 		double *__restrict__ act_heat, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, const float *__restrict__ rho, const float *__restrict__ yeMET,
 		const float *__restrict__ hstep, UpdRec *__restrict__ rec, int lo, const double *__restrict__ gcarry,
-		const PhysParams &P, int64_t tick, double tick_time, uint32_t *__restrict__ status) {
+		uint8_t *__restrict__ act_slow, const PhysParams &P, int64_t tick, double tick_time,
+		uint32_t *__restrict__ status) {
 	const uint32_t p = act_ipar[a];
 	hits[p] += nh;
 	if (gcarry) g += gcarry[p];      // photons left over by an earlier explicit step (loop.c:745)
@@ -956,6 +965,8 @@ __device__ __forceinline__ void finish_particle(int a, double g, double heat, in
 			act_g[a] = g;
 			act_heat[a] = heat;
 		}
+		if (act_slow)
+			act_slow[a] = upd_looks_slow(hstep[p], rn_dmul((double)(tick - lasthit[p]), tick_time), g, lambdaH[p]);
 		if (!rec) return;      // sums only: the integrator builds its own records
 		UpdRec r;
 		r.time = rn_dmul((double)(tick - lasthit[p]), tick_time);
@@ -1124,7 +1135,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		int32_t *__restrict__ hits, double *__restrict__ act_g, double *__restrict__ act_heat,
 		double *__restrict__ lambdaH, float *__restrict__ ie, int64_t *__restrict__ lasthit,
 		const float *__restrict__ rho, const float *__restrict__ yeMET, const float *__restrict__ hstep,
-		UpdRec *__restrict__ rec, const double *__restrict__ gcarry, PhysParams P,
+		UpdRec *__restrict__ rec, const double *__restrict__ gcarry, uint8_t *__restrict__ act_slow, PhysParams P,
 		const PsgBatchDev *__restrict__ B, uint32_t *__restrict__ status) {
 	const int64_t tick = B->tick0 + t;
 	const double tick_time = B->tick_time;
@@ -1140,7 +1151,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 		warp_segment_sum(acc, vals, want_heat, act_seg[a], act_seg[a + 1], lane, sg, sh, sn);
 		if (lane == 0)
 			finish_particle<ISO, REC>(a, sg, sh, sn, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
-					hstep, rec, lo, gcarry, P, tick, tick_time, status);
+					hstep, rec, lo, gcarry, act_slow, P, tick, tick_time, status);
 	}
 	for (int a = lo + (int)(blockIdx.x * blockDim.x + threadIdx.x); a < hi; a += (int)(gridDim.x * blockDim.x)) {
 		const uint32_t s0 = act_seg[a], s1 = act_seg[a + 1];
@@ -1157,7 +1168,7 @@ __global__ void __launch_bounds__(256) k_reduce(int t, const int32_t *__restrict
 			}
 		});
 		finish_particle<ISO, REC>(a, g, heat, nh, act_ipar, hits, act_g, act_heat, lambdaH, ie, lasthit, rho, yeMET,
-				hstep, rec, lo, gcarry, P, tick, tick_time, status);
+				hstep, rec, lo, gcarry, act_slow, P, tick, tick_time, status);
 	}
 }
 
@@ -1178,6 +1189,7 @@ struct UpdSrc {
 	const uint32_t *act_ipar;
 	const double *act_g, *act_heat;
 	const float *rho, *yeMET;
+	const uint8_t *slow;      // per active pair: claim in the first pass (with cursor2)
 };
 
 // Every warp owns two buffers of 32 records in shared memory: it claims
@@ -1187,12 +1199,23 @@ struct UpdSrc {
 // gathers of a chunk are paid once per 32 particles, not per integrator
 // step, and no record goes through device memory. MINB caps the registers
 // for that many resident blocks per multiprocessor (psg_tune).
+//
+// With cursor2 (psg_tune.update_order) the tick's particles are claimed in
+// two passes: first, from cursor, those that look slow (src.slow, set by
+// k_reduce before this kernel starts, so both passes see the same flags:
+// no step proposal carried over -- new, or handed to the stiff finish last
+// time --, a proposal under a quarter of this step, or more photons absorbed
+// than neutral atoms), then, from cursor2, the others; each claim keeps its
+// chunk's particles of the pass. Long integrations then start early instead
+// of trailing the kernel on a few lanes. Which lane integrates a particle
+// changes, not its result.
 template <bool REC, int MINB>
 __global__ void __launch_bounds__(32 * UPD_WARPS, MINB) k_update_queue(int t, const int32_t *__restrict__ tick_act,
 		const UpdSrc src, double *__restrict__ lambdaH, float *__restrict__ ie,
 		int64_t *__restrict__ lasthit, float *__restrict__ hstep, PhysParams P, const PsgBatchDev *__restrict__ B,
-		unsigned *__restrict__ cursor, StiffItem *__restrict__ stiff, unsigned *__restrict__ nstiff,
-		const uint32_t *__restrict__ alist, const unsigned *__restrict__ nalist, uint32_t *__restrict__ status) {
+		unsigned *__restrict__ cursor, unsigned *__restrict__ cursor2, StiffItem *__restrict__ stiff,
+		unsigned *__restrict__ nstiff, const uint32_t *__restrict__ alist, const unsigned *__restrict__ nalist,
+		uint32_t *__restrict__ status) {
 	__shared__ UpdRec buf[UPD_WARPS][2][32];
 	const int64_t tick = B->tick0 + t;
 	const double tick_time = B->tick_time;
@@ -1202,32 +1225,48 @@ __global__ void __launch_bounds__(32 * UPD_WARPS, MINB) k_update_queue(int t, co
 	const int lane = threadIdx.x & 31;
 	const unsigned lt_mask = (1u << lane) - 1u;
 	UpdRec (*WB)[32] = buf[threadIdx.x >> 5];
+	int pass = 0;        // warp-uniform: 0 the slow-looking particles (or all), 1 the others
+	// fills WB[b] with the next particles of the pass, packed from slot 0;
+	// returns how many (0: none left)
 	auto fetch = [&](int b) -> int {
-		unsigned base = 0;
-		if (lane == 0) base = atomicAdd(cursor, 32u);
-		base = __shfl_sync(0xffffffffu, base, 0);
-		const int cnt = base >= n ? 0 : (int)min(32u, n - base);
-		if (lane < cnt) {
-			const unsigned k = base + lane;
-			const int a = alist ? (int)alist[k] : lo + (int)k;
-			const uint32_t p = src.act_ipar[a];
-			const double g = src.act_g[a], heat = src.act_heat[a];
+		for (;;) {
+			unsigned base = 0;
+			if (lane == 0) base = atomicAdd(pass ? cursor2 : cursor, 32u);
+			base = __shfl_sync(0xffffffffu, base, 0);
+			if (base >= n) {
+				if (cursor2 && pass == 0) {
+					pass = 1;
+					continue;
+				}
+				return 0;
+			}
+			const int cnt = (int)min(32u, n - base);
+			bool keep = false;
 			UpdRec r;
-			r.time = rn_dmul((double)(tick - lasthit[p]), tick_time);
-			r.lam0 = lambdaH[p];
-			r.g = g;
-			r.heat = heat;
-			r.ie0 = ie[p];
-			r.rho = src.rho[p];
-			r.yeMET = src.yeMET[p];
-			r.hstep = hstep[p];
-			r.p = p;
-			r.pad0 = 0u;
-			r.k0 = r.k1 = r.krec = 0.0;
-			WB[b][lane] = r;
+			if (lane < cnt) {
+				const unsigned k = base + lane;
+				const int a = alist ? (int)alist[k] : lo + (int)k;
+				keep = !cursor2 || (src.slow[a] != 0) == (pass == 0);
+				if (keep) {
+					const uint32_t p = src.act_ipar[a];
+					r.time = rn_dmul((double)(tick - lasthit[p]), tick_time);
+					r.lam0 = lambdaH[p];
+					r.g = src.act_g[a];
+					r.heat = src.act_heat[a];
+					r.ie0 = ie[p];
+					r.rho = src.rho[p];
+					r.yeMET = src.yeMET[p];
+					r.hstep = hstep[p];
+					r.p = p;
+					r.pad0 = 0u;
+					r.k0 = r.k1 = r.krec = 0.0;
+				}
+			}
+			const unsigned km = __ballot_sync(0xffffffffu, keep);
+			if (keep) WB[b][__popc(km & lt_mask)] = r;
+			__syncwarp();
+			if (km) return __popc(km);
 		}
-		__syncwarp();
-		return cnt;
 	};
 	int avail[2];
 	avail[0] = fetch(0);
@@ -1809,10 +1848,11 @@ size_t long_lists_bytes(const BatchPlan &pl) {
 }
 struct UpdView {
 	double *act_g, *act_heat;
-	unsigned *cursors, *nstiff, *nrej, *dep_ctr;
+	unsigned *cursors, *nstiff, *nrej, *dep_ctr, *cursors2;
 	TickRays *tick_rays;
 	StiffItem *stiff;
 	uint32_t *rej;
+	uint8_t *act_slow;        // not isothermal: per active pair, the integrator's first pass
 };
 UpdView upd_view(psg_context *ctx, const BatchPlan &pl) {
 	UpdView v;
@@ -1824,14 +1864,16 @@ UpdView upd_view(psg_context *ctx, const BatchPlan &pl) {
 	v.nstiff = v.cursors + (pl.K + 1);
 	v.nrej = v.nstiff + (pl.K + 1);
 	v.dep_ctr = v.nrej + (pl.K + 1);
-	v.tick_rays = (TickRays *)(((uintptr_t)(v.dep_ctr + pl.K + 1) + 31) & ~(uintptr_t)31);
+	v.cursors2 = v.dep_ctr + (pl.K + 1);       // the integrator's second pass (update_order)
+	v.tick_rays = (TickRays *)(((uintptr_t)(v.cursors2 + pl.K + 1) + 31) & ~(uintptr_t)31);
 	v.stiff = (StiffItem *)(((uintptr_t)(v.tick_rays + pl.K) + 15) & ~(uintptr_t)15);
 	v.rej = (uint32_t *)(v.stiff + (pl.iso ? 0 : pl.pcap));
+	v.act_slow = (uint8_t *)(v.rej + (pl.surr ? pl.pcap : 0));
 	return v;
 }
 size_t upd_bytes(const BatchPlan &pl) {
-	return sizeof(double) * (pl.helium ? 4 : 2) * pl.cap + sizeof(unsigned) * 4 * (pl.K + 1) + sizeof(TickRays) * pl.K +
-			(pl.iso ? 0 : sizeof(StiffItem) * pl.pcap) + (pl.surr ? sizeof(uint32_t) * pl.pcap : 0) + 512;
+	return sizeof(double) * (pl.helium ? 4 : 2) * pl.cap + sizeof(unsigned) * 5 * (pl.K + 1) + sizeof(TickRays) * pl.K +
+			(pl.iso ? 0 : sizeof(StiffItem) * pl.pcap + pl.cap) + (pl.surr ? sizeof(uint32_t) * pl.pcap : 0) + 512;
 }
 
 // Sizes, capacities and every buffer of the batch (allocates; before any
@@ -1979,7 +2021,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 
 	// the long-segment lists and (not isothermal) the integrator's work
 	// cursors, stiff lists and the deposit's unit counters
-	PSG_CUDA(cudaMemsetAsync(uv.cursors, 0, sizeof(unsigned) * 4 * (K + 1), st));
+	PSG_CUDA(cudaMemsetAsync(uv.cursors, 0, sizeof(unsigned) * 5 * (K + 1), st));
 	if (pl.surr) PSG_CUDA(cudaMemsetAsync(ctx->d_counters + 8, 0, sizeof(unsigned long long), st));
 	UpdRec *urec = (!pl.helium && pl.euler) ? (UpdRec *)ctx->scratch[S_REC].p : nullptr;
 	HeStiffItem *hstiff = pl.helium ? (HeStiffItem *)ctx->scratch[S_REC].p : nullptr;
@@ -2062,10 +2104,13 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 			// loop
 			double *keep_g = pl.iso ? nullptr : uv.act_g;
 			double *keep_heat = pl.iso ? nullptr : uv.act_heat;
+			// the integrator's two passes (update_order; not over the surrogate's rejects)
+			const bool two_pass = !pl.iso && !pl.euler && ctx->tune.update_order && !pl.surr;
+			uint8_t *slow_flags = two_pass ? uv.act_slow : nullptr;
 #define PSG_REDUCE(ISO_, REC_)                                                                                 \
 	k_reduce<ISO_, REC_><<<pl.red_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, av.act_seg, acc, vals,\
 			(uint32_t)ctx->tune.run_short, pl.want_heat, long_act, tick_long, ctx->d_hits, keep_g, keep_heat, ctx->d_lambdaH, ctx->d_ie,       \
-			ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, P, B, ctx->d_status)
+			ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, ctx->d_hstep, urec, gcarry, slow_flags, P, B, ctx->d_status)
 			if (pl.iso && !pl.euler) {
 				if (P.ygrec) PSG_REDUCE(true, true);
 				else PSG_REDUCE(true, false);
@@ -2088,6 +2133,7 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 				us.act_heat = uv.act_heat;
 				us.rho = ctx->d_rho;
 				us.yeMET = ctx->d_yeMET;
+				us.slow = slow_flags;
 				if (feat) {
 					k_log_pre<<<pl.log_grid, 256, 0, st>>>((int)t, av.tick_act, av.act_ipar, uv.act_g, uv.act_heat,
 							ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_rho, ctx->d_yeMET, P, B, feat);
@@ -2100,17 +2146,18 @@ int enqueue_batch(psg_context *ctx, const BatchPlan &pl, const PsgBatchDev *B) {
 					if (rc) return rc;
 					ctx->launches++;
 				}
+				unsigned *cur2 = two_pass ? uv.cursors2 + t : nullptr;
 				if (P.ygrec) {
 					k_update_queue<true, 1><<<pl.queue_grid, 32 * UPD_WARPS, 0, st>>>((int)t, av.tick_act, us,
-							ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, B, uv.cursors + t, uv.stiff,
-							uv.nstiff + t, nullptr, nullptr, ctx->d_status);
+							ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, B, uv.cursors + t, cur2,
+							uv.stiff, uv.nstiff + t, nullptr, nullptr, ctx->d_status);
 					PSG_CHECK_LAUNCH();
 					k_update_stiff<true><<<sms, 64, 0, st>>>(uv.stiff, uv.nstiff + t, ctx->d_lambdaH, ctx->d_ie,
 							ctx->d_lasthit, P, B, (int)t, ctx->d_status);
 				} else {
 #define PSG_QUEUE(MINB_)                                                                                       \
 	k_update_queue<false, MINB_><<<pl.queue_grid, 32 * UPD_WARPS, 0, st>>>((int)t, av.tick_act, us,          \
-			ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, B, uv.cursors + t, uv.stiff,           \
+			ctx->d_lambdaH, ctx->d_ie, ctx->d_lasthit, ctx->d_hstep, P, B, uv.cursors + t, cur2, uv.stiff,     \
 			uv.nstiff + t, pl.surr ? uv.rej : nullptr, pl.surr ? uv.nrej + t : nullptr, ctx->d_status)
 					if (pl.queue_minb == 4) PSG_QUEUE(4);
 					else if (pl.queue_minb == 3) PSG_QUEUE(3);
@@ -2172,6 +2219,7 @@ std::vector<unsigned long long> batch_key(const psg_context *ctx, const BatchPla
 	k.push_back((unsigned long long)ctx->tune.deposit_long << 32 | (unsigned)ctx->tune.deposit_mid);
 	k.push_back((unsigned long long)pl.queue_minb);
 	k.push_back((unsigned long long)ctx->tune.run_short);
+	k.push_back((unsigned long long)ctx->tune.update_order);
 	k.push_back((unsigned long long)psg_sort_classes(pl.maxcount));
 	k.push_back(pl.src_R);
 	k.push_back(ctx->src_nray);
@@ -2550,6 +2598,13 @@ extern "C" int psg_autotune(psg_context *ctx, const psg_ray *d_rays, size_t R, s
 		if (rc || rs == cur.run_short) continue;
 		psg_tune t = cur;
 		t.run_short = rs;
+		rc = consider(t);
+	}
+	// the order in which the integrator claims the particles
+	for (int uo : {0, 1}) {
+		if (rc || uo == cur.update_order) continue;
+		psg_tune t = cur;
+		t.update_order = uo;
 		rc = consider(t);
 	}
 	ctx->tune = cur;
