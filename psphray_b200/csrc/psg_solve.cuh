@@ -39,6 +39,7 @@ struct PhysParams {
 	double ar_all_scale[PSG_AR_NCOLS];
 	int ar_nrows;
 	double ar_min, ar_step_inv, ar_step;
+	float ar_min_f, ar_step_inv_f, ar_step_f;   // the same in FP32 (the explicit stages' lookups)
 	const double *xs;      // [4][xs_nrows]: energy, sigma_HI, sigma_HeI, sigma_HeII
 	int xs_nrows;
 	double xs_min, xs_step_inv, xs_cut_HI, xs_cut_HeI, xs_cut_HeII;
@@ -197,39 +198,54 @@ __device__ __forceinline__ RhsCtx make_rhs_ctx(const PhysParams &P, double yeMET
 // rates, and fused multiply-adds (the last bits of an integrator's stage do
 // not matter; the isothermal closed form keeps the reference's roundings).
 // With REC, *rec receives d(yGrecHII)/ds. With T32 (the explicit
-// integrator's stages) the temperature and its logarithm, which only pick
-// the rate table's row and the interpolation weight, are computed in FP32:
-// the rates are FP32 table values anyway, and a 1e-7 relative error in log T
-// moves a rate by well under 1e-6 of itself (the integrator's rtol); the
-// state and its derivatives stay FP64. Without it (finite-difference
-// Jacobians, residual checks, the explicit build's steps) everything is FP64.
+// integrator's stages, not isothermal) the way from the state to the rates
+// is FP32: the temperature with the fast divide, its logarithm with the
+// fast log10 (a few ulp; the rate table is interpolated linearly, so an
+// error e in log T moves a rate by its slope times e, about 1e-5 of itself
+// at the steepest rows, the same order as FP32's own rounding of log T), the
+// row and weight, and the interpolation of the FP32 table values; each rate
+// is then scaled and combined in FP64, and the state and its derivatives
+// stay FP64. Without it (finite-difference Jacobians, residual checks, the
+// explicit build's steps) the lookup is FP64.
 template <bool REC = false, bool T32 = false>
 __device__ __forceinline__ void rhs(const PhysParams &P, const RhsCtx &cx, const double x[2], double dx[2],
 		double *rec = nullptr) {
 	const double xHI = x[0], xHII = 1.0 - x[0];
 	const double ye = xHII + P.he_e + cx.yeMET;
-	// the row of tabfun_get() and the offset into it (clamped rows: offset 0)
-	double logT;
-	if (T32 && !P.isothermal) {
-		const float Tf = (float)cx.T_num * (float)x[1] / (float)__fma_rn(P.hmf, ye, cx.T_den0);
-		logT = (double)log10f(Tf);
+	// the row of tabfun_get() and the offset into it (clamped rows, a NaN
+	// temperature included: offset 0)
+	long long idx;
+	double du = 0.0;
+	float duf = 0.0f;
+	if (T32) {
+		const float Tf = P.isothermal ? (float)cx.T
+				: __fdividef((float)cx.T_num * (float)x[1], (float)__fma_rn(P.hmf, ye, cx.T_den0));
+		const float lT = __log10f(Tf);
+		const float uf = (lT - P.ar_min_f) * P.ar_step_inv_f;
+		const int i = (int)uf;       // truncation; a NaN converts to 0, caught by uf == uf
+		if (!(uf == uf) || i < 0) {
+			idx = 0;
+		} else if (i >= P.ar_nrows - 1) {
+			idx = P.ar_nrows - 1;
+		} else {
+			idx = i;
+			duf = lT - __fmaf_rn((float)i, P.ar_step_f, P.ar_min_f);
+		}
 	} else {
-		logT = log10(P.isothermal ? cx.T : cx.T_num * x[1] / __fma_rn(P.hmf, ye, cx.T_den0));
-	}
-	long long idx = (long long)((logT - P.ar_min) * P.ar_step_inv);
-	double du;
-	if (idx < 0) {
-		idx = 0;
-		du = 0.0;
-	} else if (idx >= P.ar_nrows - 1) {
-		idx = P.ar_nrows - 1;
-		du = 0.0;
-	} else {
-		du = logT - __fma_rn((double)idx, P.ar_step, P.ar_min);
+		const double logT = log10(P.isothermal ? cx.T : cx.T_num * x[1] / __fma_rn(P.hmf, ye, cx.T_den0));
+		idx = (long long)((logT - P.ar_min) * P.ar_step_inv);
+		if (idx < 0) {
+			idx = 0;
+		} else if (idx >= P.ar_nrows - 1) {
+			idx = P.ar_nrows - 1;
+		} else {
+			du = logT - __fma_rn((double)idx, P.ar_step, P.ar_min);
+		}
 	}
 	const float4 *row = P.ar_ni + 4 * idx;
 	const float4 v0 = row[0], v1 = row[1], s0 = row[2], s1 = row[3];
-#define PSG_LIN(v, s, c) (__fma_rn((double)(s), du, (double)(v)) * P.ar_ni_scale[c])
+#define PSG_LIN(v, s, c)                                                                                  \
+	((T32 ? (double)__fmaf_rn((s), duf, (v)) : __fma_rn((double)(s), du, (double)(v))) * P.ar_ni_scale[c])
 	const double gamma = PSG_LIN(v0.x, s0.x, 0) * cx.nHt;
 	const double alpha = PSG_LIN(v0.y, s0.y, 1) * cx.nHt;       // case B on the spot, else A
 	dx[0] = __fma_rn(ye, __fma_rn(alpha, xHII, -gamma * xHI), -cx.g);
@@ -333,8 +349,9 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 		err += (e / sc) * (e / sc);
 	}
 #undef F
-	err = sqrt(0.5 * err);
-	if (err <= 1.0) {
+	// step-size control needs no double precision
+	const float errf = sqrtf((float)(0.5 * err));
+	if (errf <= 1.0f) {
 		S.t += h;
 		S.x[0] = yn[0]; S.x[1] = yn[1];
 		S.k1[0] = k7[0]; S.k1[1] = k7[1];
@@ -343,9 +360,8 @@ __device__ __forceinline__ bool dp_step(const PhysParams &P, const RhsCtx &cx, D
 			S.krec = r7;
 		}
 	}
-	// step-size control needs no double precision
-	const float fac = err > 0.0 ? fminf(5.0f, fmaxf(0.2f, 0.9f * __powf((float)err, -0.2f))) : 5.0f;
-	S.hnext = (cut && err <= 1.0) ? fmaxf((float)S.h, (float)h * fac) : (float)h * fac;
+	const float fac = errf > 0.0f ? fminf(5.0f, fmaxf(0.2f, 0.9f * __powf(errf, -0.2f))) : 5.0f;
+	S.hnext = (cut && errf <= 1.0f) ? fmaxf((float)S.h, (float)h * fac) : (float)h * fac;
 	S.h = fmax(h * (double)fac, 1e-14);
 	S.steps++;
 	return S.t >= 1.0;

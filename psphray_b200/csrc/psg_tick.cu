@@ -40,6 +40,9 @@ PhysParams psg_phys_params(const psg_context *ctx) {
 	P.ar_nrows = ctx->ar_nrows;
 	P.ar_min = ctx->ar_min;
 	P.ar_step_inv = ctx->ar_step_inv;
+	P.ar_min_f = (float)ctx->ar_min;
+	P.ar_step_f = (float)ctx->ar_step;
+	P.ar_step_inv_f = (float)ctx->ar_step_inv;
 	P.xs = ctx->d_xs;
 	P.xs_nrows = ctx->xs_nrows;
 	P.xs_min = ctx->xs_min;
